@@ -1,0 +1,402 @@
+// Batched LDPC decoder for sm_100a: layered normalised min-sum on int8 messages, bit-exact with
+// the reference's ldpc_decoder_avx512 / ldpc_decoder_avx2
+// (lib/phy/upper/channel_coding/ldpc/ldpc_decoder_impl.cpp:41-306,
+//  lib/phy/upper/channel_coding/ldpc/ldpc_decoder_avx512.cpp:69-253).
+//
+// Mapping: one CTA per codeblock, one thread per lifted check lane j (0 <= j < Z). For base-graph
+// row r, edge e (variable node v_e, lifted shift s_e), lane j reads soft bit (v_e, (j+s_e) mod Z):
+// the rows of a layer touch every lifted variable lane exactly once, so the Z lanes of a row are
+// independent and one __syncthreads separates consecutive rows (the layer schedule). Soft bits
+// live in shared memory; check-to-variable messages live in a per-codeblock global scratch slab
+// (edge-major, lane-minor: coalesced, L2 resident), indexed by (edge, check lane) rather than
+// the reference's rotated-back (variable slot, variable lane): the stored values are identical.
+//
+// Arithmetic, per lane and edge (all exactly as the reference's AVX-512 kernels):
+//   v2c = soft == +-127 ? soft : clamp(soft - c2v, -120, 120)
+//   min1/min2 over |v2c| starting at 120 (first minimum wins), sign = xor of v2c signs
+//   scale: m -> (m * 52428) >> 16     (floor(0.8 * 2^16) = 52428; m <= 120 always)
+//   c2v  = (sign xor sign(v2c)) ? -mag : mag,  mag = |v2c| == min1 ? scale(min2) : scale(min1)
+//          (equivalent to the reference's index test: a tie at min1 implies min1 == min2)
+//   soft = |v2c| == 127 ? v2c : promote(c2v + v2c) with |sum| > 120 -> +-127
+// After each iteration: hard bits (soft <= 0), fail if any soft bit is 0, else CRC over the
+// K*Z - F significant bits; CRC == 0 stops with iterations = it + 1.
+#include "pg_internal.h"
+
+#include <cstdio>
+
+namespace pg {
+#include "ldpc_base_graphs.inc"
+} // namespace pg
+
+namespace {
+
+constexpr int kThreads = 384;
+
+__constant__ uint8_t  c_edge_col[2][pg::kBg1Edges];
+__constant__ uint16_t c_edge_v[2][pg::kBg1Edges][8];
+__constant__ uint8_t  c_row_deg[2][pg::kBg1Rows];
+
+__device__ __forceinline__ int dev_set_index(int Z)
+{
+  const int a_tab[8] = {2, 3, 5, 7, 9, 11, 13, 15};
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int t = Z;
+    while ((t & 1) == 0 && t > a_tab[i]) {
+      t >>= 1;
+    }
+    if (t == a_tab[i]) {
+      return i;
+    }
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int scale_mag(int m)
+{
+  return (m * 52428) >> 16;
+}
+
+__device__ __forceinline__ int warp_max(int v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+__device__ __forceinline__ uint32_t warp_xor(uint32_t v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v ^= __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kThreads) ldpc_decode_kernel(const pg_ldpc_cb* __restrict__ descs,
+                                                              const int8_t* __restrict__ llrs,
+                                                              uint8_t* __restrict__ bits,
+                                                              int32_t* __restrict__ iterations,
+                                                              int8_t* __restrict__ c2v_all,
+                                                              const uint32_t* __restrict__ crc_pow)
+{
+  __shared__ __align__(16) int8_t soft[pg::kMaxNodes * pg::kMaxZ];
+  __shared__ uint32_t             edge[pg::kBg1Edges];
+  __shared__ uint32_t             hard[(22 * pg::kMaxZ) / 32];
+  __shared__ uint32_t             red[kThreads / 32];
+  __shared__ int                  s_last;
+  __shared__ int                  s_done;
+
+  const pg_ldpc_cb d   = descs[blockIdx.x];
+  const int        tid = threadIdx.x;
+  const int        bg  = d.base_graph;
+  const int        Z   = d.lifting_size;
+  const int        set = (Z >= 2 && Z <= pg::kMaxZ) ? dev_set_index(Z) : -1;
+  if ((bg != 1 && bg != 2) || set < 0) {
+    if (tid == 0) {
+      iterations[blockIdx.x] = -1;
+    }
+    return;
+  }
+  const int     g        = bg - 1;
+  const int     Kb       = bg == 1 ? 22 : 10;
+  const int     nrows    = bg == 1 ? pg::kBg1Rows : pg::kBg2Rows;
+  const int     nedges   = bg == 1 ? pg::kBg1Edges : pg::kBg2Edges;
+  const int     nfull    = bg == 1 ? 68 : 52;
+  const int     msg_len  = Kb * Z;
+  const int     n        = (int)d.nof_llrs;
+  const int8_t* in       = llrs + d.llr_offset;
+  int8_t*       c2v      = c2v_all + (size_t)blockIdx.x * pg::kC2vStride;
+  const int     nbytes   = (msg_len + 7) / 8;
+  uint8_t*      out      = bits + d.out_offset;
+  const int     crc_poly = d.crc_poly;
+  const int     nwords   = (msg_len + 31) / 32;
+
+  // Edge table of this lifting size: node offset (col * Z) and shift (V mod Z).
+  for (int e = tid; e < nedges; e += kThreads) {
+    const int col = c_edge_col[g][e];
+    const int s   = c_edge_v[g][e][set] % Z;
+    edge[e]       = ((uint32_t)(col * Z) << 16) | (uint32_t)s;
+  }
+  if (tid == 0) {
+    s_last = 0;
+    s_done = 0;
+  }
+  __syncthreads();
+
+  // Trim trailing zero LLRs (ldpc_decoder_impl.cpp:66-71).
+  int last = 0;
+  for (int i = tid; i < n; i += kThreads) {
+    if (in[i] != 0) {
+      last = i + 1;
+    }
+  }
+  last = warp_max(last);
+  if ((tid & 31) == 0 && last > 0) {
+    atomicMax(&s_last, last);
+  }
+
+  // Soft bits: 2Z punctured zeros, whole nodes clamped to +-64, a ragged tail as is
+  // (ldpc_decoder_impl.cpp:147-188).
+  const int nof_full = (n / Z) * Z;
+  for (int i = tid; i < nfull * Z; i += kThreads) {
+    int v = 0;
+    const int k = i - 2 * Z;
+    if (k >= 0 && k < n) {
+      v = in[k];
+      if (k < nof_full) {
+        v = max(-64, min(64, v));
+      }
+    }
+    soft[i] = (int8_t)v;
+  }
+  __syncthreads();
+
+  const int input_size = s_last;
+  if (input_size < msg_len) {
+    for (int b = tid; b < nbytes; b += kThreads) {
+      out[b] = 0xff;
+    }
+    if (tid == 0) {
+      iterations[blockIdx.x] = 0;
+    }
+    return;
+  }
+  int cb_len = max(input_size + 2 * Z, (Kb + 4) * Z);
+  cb_len     = ((cb_len + Z - 1) / Z) * Z;
+  const int nof_layers = min(cb_len / Z - Kb, nrows);
+
+  uint32_t g_poly = 0;
+  int      order  = 24;
+  if (crc_poly == PG_CRC16) {
+    order = 16;
+  }
+  const uint32_t* pow_tab = crc_pow + (size_t)(crc_poly <= PG_CRC24B ? crc_poly : 0) * pg::kCrcPowLen;
+  (void)g_poly;
+  const int crc_len = msg_len - (int)d.nof_filler_bits;
+
+  int result = 0;
+  const int max_it = d.max_iterations;
+  for (int it = 0; it < max_it; ++it) {
+    int e0 = 0;
+    for (int r = 0; r < nof_layers; ++r) {
+      const int deg = c_row_deg[g][r];
+      if (tid < Z) {
+        int      v2c[pg::kMaxRowDegree];
+        int      pos[pg::kMaxRowDegree];
+        int      min1 = 120, min2 = 120, sgn = 0;
+        int8_t*  c2v_row = c2v + (size_t)e0 * Z + tid;
+#pragma unroll
+        for (int e = 0; e < pg::kMaxRowDegree; ++e) {
+          if (e < deg) {
+            const uint32_t ed = edge[e0 + e];
+            int            p  = tid + (int)(ed & 0xffffu);
+            p                 = (p >= Z) ? p - Z : p;
+            p += (int)(ed >> 16);
+            pos[e]      = p;
+            const int x = soft[p];
+            const int c = (it > 0) ? (int)c2v_row[e * Z] : 0;
+            int       m = max(-120, min(120, x - c));
+            m           = (x >= 127 || x <= -127) ? x : m;
+            v2c[e]      = m;
+            const int a = abs(m);
+            min2        = min(min2, max(min1, a));
+            min1        = min(min1, a);
+            sgn ^= m;
+          }
+        }
+        const int s1 = scale_mag(min1);
+        const int s2 = scale_mag(min2);
+#pragma unroll
+        for (int e = 0; e < pg::kMaxRowDegree; ++e) {
+          if (e < deg) {
+            const int m   = v2c[e];
+            const int mag = (abs(m) == min1) ? s2 : s1;
+            const int c   = ((m ^ sgn) < 0) ? -mag : mag;
+            c2v_row[e * Z] = (int8_t)c;
+            int s          = c + m;
+            s              = (s > 120) ? 127 : ((s < -120) ? -127 : s);
+            s              = (m == 127 || m == -127) ? m : s;
+            soft[pos[e]]   = (int8_t)s;
+          }
+        }
+      }
+      e0 += deg;
+      __syncthreads();
+    }
+
+    // Hard decisions, zero check and CRC over the significant bits.
+    int      zero = 0;
+    uint32_t crc  = 0;
+    if (tid < nwords) {
+      const int4* p = reinterpret_cast<const int4*>(soft + 32 * tid);
+      const int4  a = p[0];
+      const int4  b = p[1];
+      const int   wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+      uint32_t    w     = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int idx = 32 * tid + 4 * k + j;
+          const int x   = (int)(int8_t)((uint32_t)wv[k] >> (8 * j));
+          if (idx < msg_len) {
+            w |= (uint32_t)(x <= 0) << (31 - (4 * k + j));
+            zero |= (x == 0);
+          }
+        }
+      }
+      hard[tid] = w;
+      if (crc_poly != PG_CRC_NONE) {
+        const int valid = crc_len - 32 * tid;
+        uint32_t  wc    = w;
+        if (valid <= 0) {
+          wc = 0;
+        } else if (valid < 32) {
+          wc &= ~((1u << (32 - valid)) - 1u);
+        }
+        const int e_w = crc_len - 32 * tid - 32 + order;
+        while (wc != 0) {
+          const int q = __ffs(wc) - 1;
+          crc ^= __ldg(pow_tab + e_w + q);
+          wc &= wc - 1;
+        }
+      }
+    }
+    zero = __syncthreads_or(zero);
+    crc  = warp_xor(crc);
+    if ((tid & 31) == 0) {
+      red[tid >> 5] = crc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kThreads / 32; ++w) {
+        t ^= red[w];
+      }
+      s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_done) {
+      result = it + 1;
+      break;
+    }
+  }
+
+  if (crc_poly == PG_CRC_NONE) {
+    // Syndrome check over the processed rows (ldpc_decoder_impl.cpp:329-387).
+    int bad = 0;
+    if (tid < Z) {
+      int e0 = 0;
+      for (int r = 0; r < nof_layers; ++r) {
+        const int deg    = c_row_deg[g][r];
+        int       parity = 0;
+        for (int e = 0; e < deg; ++e) {
+          const uint32_t ed = edge[e0 + e];
+          int            p  = tid + (int)(ed & 0xffffu);
+          p                 = (p >= Z) ? p - Z : p;
+          const int x       = soft[p + (int)(ed >> 16)];
+          bad |= (x == 0);
+          parity ^= (x <= 0);
+        }
+        bad |= parity;
+        e0 += deg;
+      }
+    }
+    bad = __syncthreads_or(bad);
+    // The hard words of the last iteration are in hard[]; a zero soft bit also fails.
+    int zero = 0;
+    if (tid < nwords) {
+      for (int k = 0; k < 32; ++k) {
+        const int idx = 32 * tid + k;
+        if (idx < msg_len && soft[idx] == 0) {
+          zero = 1;
+        }
+      }
+    }
+    zero   = __syncthreads_or(zero);
+    result = (!bad && !zero) ? max_it : 0;
+  }
+
+  for (int b = tid; b < nbytes; b += kThreads) {
+    out[b] = (uint8_t)(hard[b >> 2] >> (24 - 8 * (b & 3)));
+  }
+  if (tid == 0) {
+    iterations[blockIdx.x] = result;
+  }
+}
+
+} // namespace
+
+namespace pg {
+
+int lifting_set_index(int Z)
+{
+  static const int a_tab[8] = {2, 3, 5, 7, 9, 11, 13, 15};
+  if (Z < 2 || Z > kMaxZ) {
+    return -1;
+  }
+  for (int i = 0; i < 8; ++i) {
+    int t = Z;
+    while ((t % 2) == 0 && t > a_tab[i]) {
+      t /= 2;
+    }
+    if (t == a_tab[i]) {
+      return i;
+    }
+  }
+  return -1;
+}
+
+int ldpc_upload_tables(pg_context* ctx)
+{
+  uint8_t  col[2][kBg1Edges] = {};
+  uint16_t v[2][kBg1Edges][8] = {};
+  uint8_t  deg[2][kBg1Rows]   = {};
+  for (int e = 0; e < PG_BG1_EDGES; ++e) {
+    col[0][e] = PG_BG1_EDGE_COL[e];
+    for (int s = 0; s < 8; ++s) {
+      v[0][e][s] = PG_BG1_EDGE_V[e][s];
+    }
+  }
+  for (int e = 0; e < PG_BG2_EDGES; ++e) {
+    col[1][e] = PG_BG2_EDGE_COL[e];
+    for (int s = 0; s < 8; ++s) {
+      v[1][e][s] = PG_BG2_EDGE_V[e][s];
+    }
+  }
+  for (int r = 0; r < PG_BG1_ROWS; ++r) {
+    deg[0][r] = PG_BG1_ROW_DEG[r];
+  }
+  for (int r = 0; r < PG_BG2_ROWS; ++r) {
+    deg[1][r] = PG_BG2_ROW_DEG[r];
+  }
+  int rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_col, col, sizeof(col)), "cudaMemcpyToSymbol(edge_col)");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_v, v, sizeof(v)), "cudaMemcpyToSymbol(edge_v)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_row_deg, deg, sizeof(deg)), "cudaMemcpyToSymbol(row_deg)");
+  }
+  return rc;
+}
+
+int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                int32_t* iterations, cudaStream_t stream)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  if (ctx->timed) {
+    cudaEventRecord(ctx->ev_start, stream);
+  }
+  ldpc_decode_kernel<<<n, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, ctx->dev.c2v, ctx->dev.crc_pow);
+  if (ctx->timed) {
+    cudaEventRecord(ctx->ev_stop, stream);
+  }
+  return check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch");
+}
+
+} // namespace pg

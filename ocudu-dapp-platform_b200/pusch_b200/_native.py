@@ -1,0 +1,107 @@
+"""ctypes binding of the pusch_b200 C ABI (include/pusch_b200.h).
+
+The library is built in-tree (ocudu-dapp-platform_b200/csrc/Makefile) into
+pusch_b200/_lib/libpusch_b200.so. There is no CPU fallback: if the library is missing or no
+sm_100 device is present, creating a context raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpusch_b200.so")
+
+PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_CAPACITY, PG_ERR_TIMEOUT, PG_ERR_NO_DEVICE = range(6)
+PG_CRC16, PG_CRC24A, PG_CRC24B = 0, 1, 2
+PG_CRC_NONE = 255
+
+STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_INVALID", 2: "PG_ERR_CUDA", 3: "PG_ERR_CAPACITY", 4: "PG_ERR_TIMEOUT",
+                5: "PG_ERR_NO_DEVICE"}
+
+
+class PgConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_codeblocks", ctypes.c_int), ("max_llrs", ctypes.c_int)]
+
+
+class PgLdpcCb(ctypes.Structure):
+    _fields_ = [
+        ("llr_offset", ctypes.c_uint32),
+        ("nof_llrs", ctypes.c_uint32),
+        ("out_offset", ctypes.c_uint32),
+        ("lifting_size", ctypes.c_uint16),
+        ("nof_filler_bits", ctypes.c_uint16),
+        ("base_graph", ctypes.c_uint8),
+        ("crc_poly", ctypes.c_uint8),
+        ("max_iterations", ctypes.c_uint8),
+        ("reserved", ctypes.c_uint8),
+    ]
+
+
+assert ctypes.sizeof(PgLdpcCb) == 20
+
+# Every symbol the public header declares, with (restype, argtypes).
+_VP = ctypes.c_void_p
+SIGNATURES = {
+    "pg_abi_version": (ctypes.c_int, []),
+    "pg_create": (ctypes.c_int, [ctypes.POINTER(PgConfig), ctypes.POINTER(_VP)]),
+    "pg_destroy": (None, [_VP]),
+    "pg_last_error": (ctypes.c_char_p, [_VP]),
+    "pg_ldpc_decode_batch_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_ldpc_decode_batch_resident": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_ldpc_decode_batch_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP,
+                                                 ctypes.c_size_t, _VP]),
+    "pg_ldpc_output_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "pg_set_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "pg_last_kernel_ms": (ctypes.c_float, [_VP]),
+}
+
+_lib = None
+
+
+def load():
+    """Loads the library (once) and declares every exported signature."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"pusch_b200 native library not built: {LIB_PATH} (run __graft_entry__.build())")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+class PgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Context:
+    """Owns one pg_context (one CUDA device)."""
+
+    def __init__(self, device=0, max_codeblocks=1024, max_llrs=0):
+        self.lib = load()
+        cfg = PgConfig(device, max_codeblocks, max_llrs)
+        h = ctypes.c_void_p()
+        rc = self.lib.pg_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != PG_OK:
+            raise PgError(rc, "pg_create failed (is an sm_100 GPU visible?)")
+        self.handle = h
+        self.max_codeblocks = max_codeblocks
+
+    def check(self, rc):
+        if rc != PG_OK:
+            raise PgError(rc, self.lib.pg_last_error(self.handle).decode())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.pg_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,167 @@
+"""Transmit-side coding used by the project's seeded PUSCH simulator: CRC attachment and LDPC
+encoding (TS 38.212 Sections 5.1 and 5.3.2). Numpy, vectorised over codeblocks; this is input
+generation, not the measured receive path.
+
+The encoder is this project's own: the 4Z x 4Z core-parity block of the lifted parity-check
+matrix is inverted over GF(2) once per (base graph, Z); the extension parity bits then follow
+row by row from the lower-triangular identity structure of rows 4.. of both base graphs.
+"""
+import functools
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "..", "csrc", "ldpc_base_graphs.inc")
+
+CRC_POLYS = {0: (0x11021, 16), 1: (0x1864CFB, 24), 2: (0x1800063, 24)}  # CRC16, CRC24A, CRC24B
+
+
+@functools.lru_cache(maxsize=None)
+def base_graph(bg):
+    """Returns (row degrees, edge columns, edge V[8]) of base graph bg from the shared table."""
+    text = open(TABLE).read()
+
+    def arr(name):
+        m = re.search(r"PG_BG%d_%s\[[^\]]*\](?:\[8\])? = \{(.*?)\};" % (bg, name), text, re.S)
+        return [int(x) for x in re.findall(r"\d+", m.group(1))]
+
+    deg = np.array(arr("ROW_DEG"), np.int32)
+    col = np.array(arr("EDGE_COL"), np.int32)
+    v = np.array(arr("EDGE_V"), np.int32).reshape(-1, 8)
+    return deg, col, v
+
+
+def set_index(z):
+    for i, a in enumerate((2, 3, 5, 7, 9, 11, 13, 15)):
+        t = z
+        while t % 2 == 0 and t > a:
+            t //= 2
+        if t == a:
+            return i
+    raise ValueError(f"{z} is not a lifting size")
+
+
+@functools.lru_cache(maxsize=None)
+def lifted_edges(bg, z):
+    """Per row: list of (column, shift) with shift = V mod Z."""
+    deg, col, v = base_graph(bg)
+    s = set_index(z)
+    rows, e = [], 0
+    for d in deg:
+        rows.append([(int(col[e + k]), int(v[e + k, s] % z)) for k in range(d)])
+        e += d
+    return rows
+
+
+def _gf2_inverse(a):
+    """Inverse of a square GF(2) matrix given as a bool array (Gauss-Jordan on packed rows)."""
+    n = a.shape[0]
+    aug = np.concatenate([a.astype(np.uint8), np.eye(n, dtype=np.uint8)], axis=1)
+    packed = np.packbits(aug, axis=1).view(np.uint8)
+    words = packed.shape[1]
+    for c in range(n):
+        byte, bit = c // 8, 7 - (c % 8)
+        colbits = (packed[:, byte] >> bit) & 1
+        cand = np.nonzero(colbits[c:])[0]
+        if cand.size == 0:
+            raise ValueError("singular core parity block")
+        p = c + cand[0]
+        if p != c:
+            packed[[c, p]] = packed[[p, c]]
+            colbits = (packed[:, byte] >> bit) & 1
+        rows = np.nonzero(colbits)[0]
+        rows = rows[rows != c]
+        packed[rows] ^= packed[c]
+    del words
+    full = np.unpackbits(packed, axis=1)[:, : 2 * n]
+    return full[:, n:].astype(np.uint8)
+
+
+def _roll_rows(x, s):
+    """y[..., j] = x[..., (j + s) mod Z]: the lifted circulant applied to a node."""
+    return np.roll(x, -s, axis=-1)
+
+
+@functools.lru_cache(maxsize=None)
+def _core_inverse(bg, z):
+    kb = 22 if bg == 1 else 10
+    rows = lifted_edges(bg, z)
+    a = np.zeros((4 * z, 4 * z), np.uint8)
+    j = np.arange(z)
+    for r in range(4):
+        for c, s in rows[r]:
+            if kb <= c < kb + 4:
+                a[r * z + j, (c - kb) * z + (j + s) % z] = 1
+    return _gf2_inverse(a)
+
+
+def ldpc_encode(bg, z, msg):
+    """Encodes message bits msg[..., K_b*Z] (fillers as 0) into the shortened codeword
+    [..., N_short*Z] (the first 2Z systematic bits are not transmitted)."""
+    kb = 22 if bg == 1 else 10
+    m_rows = 46 if bg == 1 else 42
+    msg = np.asarray(msg, np.uint8)
+    lead = msg.shape[:-1]
+    nodes = np.zeros(lead + (kb + m_rows, z), np.uint8)
+    nodes[..., :kb, :] = msg.reshape(lead + (kb, z))
+    rows = lifted_edges(bg, z)
+    lam = np.zeros(lead + (4, z), np.uint8)
+    for r in range(4):
+        for c, s in rows[r]:
+            if c < kb:
+                lam[..., r, :] ^= _roll_rows(nodes[..., c, :], s)
+    inv = _core_inverse(bg, z)
+    rhs = lam.reshape(lead + (4 * z,)).astype(np.float32)
+    core = (rhs @ inv.T.astype(np.float32)).astype(np.int64) & 1
+    nodes[..., kb:kb + 4, :] = core.reshape(lead + (4, z)).astype(np.uint8)
+    for r in range(4, m_rows):
+        acc = np.zeros(lead + (z,), np.uint8)
+        ext = kb + r
+        for c, s in rows[r]:
+            if c == ext:
+                assert s == 0
+                continue
+            acc ^= _roll_rows(nodes[..., c, :], s)
+        nodes[..., ext, :] = acc
+    return nodes[..., 2:, :].reshape(lead + ((kb + m_rows - 2) * z,))
+
+
+@functools.lru_cache(maxsize=None)
+def _crc_table(poly):
+    g, order = CRC_POLYS[poly]
+    mask = (1 << order) - 1
+    tab = np.zeros(256, np.uint32)
+    for b in range(256):
+        r = b << (order - 8)
+        for _ in range(8):
+            r = ((r << 1) ^ g) & mask if r & (1 << (order - 1)) else (r << 1) & mask
+        tab[b] = r
+    return tab, order, mask
+
+
+def crc(poly, bits):
+    """CRC (init 0, MSB first) of bits[..., L]; vectorised over leading dimensions."""
+    bits = np.asarray(bits, np.uint8)
+    tab, order, mask = _crc_table(poly)
+    L = bits.shape[-1]
+    lead = bits.shape[:-1]
+    pad = (-L) % 8
+    # Leading zeros do not change a zero-initialised CRC.
+    b = np.concatenate([np.zeros(lead + (pad,), np.uint8), bits], axis=-1)
+    by = np.packbits(b, axis=-1).astype(np.uint32)
+    r = np.zeros(lead, np.uint32)
+    for k in range(by.shape[-1]):
+        idx = ((r >> (order - 8)) ^ by[..., k]) & 0xFF
+        r = ((r << 8) & mask) ^ tab[idx]
+    return r
+
+
+def attach_crc(poly, bits):
+    """bits[..., L] -> bits[..., L + order] with the CRC appended MSB first."""
+    _, order = CRC_POLYS[poly]
+    r = crc(poly, bits)
+    sh = np.arange(order - 1, -1, -1, dtype=np.uint32)
+    tail = ((r[..., None] >> sh) & 1).astype(np.uint8)
+    return np.concatenate([np.asarray(bits, np.uint8), tail], axis=-1)

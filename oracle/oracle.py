@@ -1,0 +1,140 @@
+"""Test infrastructure only: ctypes bindings to the two CPU checkers.
+
+* ``Ref``  - the reference's own CPU code compiled by oracle/Makefile into
+  oracle/_ref/libocudu_ref.so (the AVX-512 variant when the host has it, else AVX2; they
+  decode bit-identically).
+* ``Port`` - the plain-C restatement oracle/pusch_oracle.c (oracle/_build/libpusch_oracle.so).
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py use this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libocudu_ref.so")
+PORT_SO = os.path.join(HERE, "_build", "libpusch_oracle.so")
+
+CRC16, CRC24A, CRC24B, CRC24C, CRC11, CRC6 = range(6)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def kb(bg):
+    return 22 if bg == 1 else 10
+
+
+def n_short(bg):
+    return 66 if bg == 1 else 50
+
+
+class Ref:
+    """The reference's compiled CPU implementation."""
+
+    def __init__(self, path=REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run `make -C oracle ref`)")
+        lib = ctypes.CDLL(path)
+        lib.ref_ldpc_decode.argtypes = [ctypes.c_char_p] + [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_int,
+                                                                                  ctypes.c_void_p]
+        lib.ref_ldpc_decode.restype = ctypes.c_int
+        lib.ref_ldpc_auto_variant.restype = ctypes.c_char_p
+        lib.ref_crc_calculate.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.ref_crc_calculate.restype = ctypes.c_uint
+        lib.ref_crc_calculate_byte.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.ref_crc_calculate_byte.restype = ctypes.c_uint
+        lib.ref_ldpc_encode.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_ldpc_encode_rm.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p, ctypes.c_void_p]
+        lib.ref_rate_dematch.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        lib.ref_demodulate_soft.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p]
+        lib.ref_sch_segmentation.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        self.lib = lib
+        self.variant = lib.ref_ldpc_auto_variant().decode()
+
+    def ldpc_decode(self, bg, Z, llrs, filler=0, crc_poly=CRC24B, max_iter=10, nof_crc_bits=24, variant=None,
+                    prefill=0xFF):
+        """Returns (iterations or 0, packed K*Z bits)."""
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        K = kb(bg) * Z
+        out = np.full((K + 7) // 8, prefill, np.uint8)
+        v = (variant or self.variant).encode()
+        it = self.lib.ref_ldpc_decode(v, bg, Z, filler, nof_crc_bits, crc_poly, max_iter, _ptr(llrs), llrs.size,
+                                      _ptr(out))
+        if it < 0:
+            raise RuntimeError(f"decoder variant {v!r} unavailable on this CPU")
+        return it, out
+
+    def crc(self, poly, bits):
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        packed = np.packbits(bits) if bits.size else np.zeros(1, np.uint8)
+        return self.lib.ref_crc_calculate(poly, _ptr(packed), bits.size)
+
+    def ldpc_encode(self, bg, Z, msg_bits):
+        msg = np.packbits(np.ascontiguousarray(msg_bits, dtype=np.uint8))
+        cw = np.zeros(n_short(bg) * Z, np.uint8)
+        self.lib.ref_ldpc_encode(bg, Z, _ptr(msg), _ptr(cw))
+        return cw
+
+    def ldpc_encode_rm(self, bg, Z, msg_bits, E, rv=0, qm=1, Nref=0, filler=0):
+        msg = np.packbits(np.ascontiguousarray(msg_bits, dtype=np.uint8))
+        out = np.zeros(E, np.uint8)
+        self.lib.ref_ldpc_encode_rm(bg, Z, rv, qm, Nref, filler, E, _ptr(msg), _ptr(out))
+        return out
+
+    def rate_dematch(self, bg, Z, llrs, rv=0, qm=1, Nref=0, filler=0, new_data=True, out=None):
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        if out is None:
+            out = np.zeros(n_short(bg) * Z, np.int8)
+        self.lib.ref_rate_dematch(bg, Z, rv, qm, Nref, filler, int(bool(new_data)), _ptr(llrs), llrs.size, _ptr(out))
+        return out
+
+    def demodulate_soft(self, qm, symbols, noise_vars):
+        sym = np.ascontiguousarray(symbols, dtype=np.complex64)
+        nv = np.ascontiguousarray(noise_vars, dtype=np.float32)
+        out = np.zeros(sym.size * qm, np.int8)
+        self.lib.ref_demodulate_soft(qm, _ptr(sym), _ptr(nv), sym.size, _ptr(out))
+        return out
+
+    def sch_segmentation(self, tbs_bits, bg):
+        o = np.zeros(4, np.int32)
+        self.lib.ref_sch_segmentation(tbs_bits, bg, _ptr(o))
+        return dict(C=int(o[0]), Z=int(o[1]), K=int(o[2]), tb_crc=int(o[3]))
+
+
+class Port:
+    """The plain-C restatement (oracle/pusch_oracle.c)."""
+
+    def __init__(self, path=PORT_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built (run `make -C oracle oracle`)")
+        lib = ctypes.CDLL(path)
+        lib.pgo_crc.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        lib.pgo_crc.restype = ctypes.c_uint32
+        lib.pgo_ldpc_decode.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        lib.pgo_ldpc_decode.restype = ctypes.c_int
+        lib.pgo_rate_dematch.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        lib.pgo_ldpc_edge_shift.argtypes = [ctypes.c_int] * 3
+        self.lib = lib
+
+    def crc(self, poly, bits):
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        packed = np.packbits(bits) if bits.size else np.zeros(1, np.uint8)
+        return self.lib.pgo_crc(poly, _ptr(packed), bits.size)
+
+    def ldpc_decode(self, bg, Z, llrs, filler=0, crc_poly=CRC24B, max_iter=10):
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        K = kb(bg) * Z
+        out = np.zeros((K + 7) // 8, np.uint8)
+        it = self.lib.pgo_ldpc_decode(bg, Z, filler, crc_poly, max_iter, _ptr(llrs), llrs.size, _ptr(out))
+        return it, out
+
+    def rate_dematch(self, bg, Z, llrs, rv=0, qm=1, Nref=0, filler=0, new_data=True, out=None):
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        if out is None:
+            out = np.zeros(n_short(bg) * Z, np.int8)
+        self.lib.pgo_rate_dematch(bg, Z, rv, qm, Nref, filler, int(bool(new_data)), _ptr(llrs), llrs.size, _ptr(out))
+        return out

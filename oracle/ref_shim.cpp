@@ -1,0 +1,341 @@
+// Test infrastructure only (checker, never shipped): a flat C ABI over the reference's own
+// CPU implementation of the PUSCH receive-path stages, so tests and the CPU-baseline arm
+// can call it through ctypes. Every function builds the reference object through the
+// reference's public factory (the same factories upper_phy_factories.cpp wires) and calls
+// the reference interface unchanged:
+//   ldpc_decoder::decode            include/ocudu/phy/upper/channel_coding/ldpc/ldpc_decoder.h:57
+//   ldpc_encoder::encode            include/ocudu/phy/upper/channel_coding/ldpc/ldpc_encoder.h
+//   ldpc_rate_matcher::rate_match   include/ocudu/phy/upper/channel_coding/ldpc/ldpc_rate_matcher.h
+//   ldpc_rate_dematcher::rate_dematch include/ocudu/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher.h:36
+//   crc_calculator::calculate       include/ocudu/phy/upper/channel_coding/crc_calculator.h:67-77
+//   demodulation_mapper::demodulate_soft include/ocudu/phy/upper/channel_modulation/demodulation_mapper.h:48
+// The base-graph accessors expose the lifted shift table (TS 38.212 Tables 5.3.2-2/-3) so the
+// product's own compact table can be checked against it entry by entry.
+
+#include "ocudu/phy/upper/channel_coding/channel_coding_factories.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_decoder.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_encoder.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_encoder_buffer.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_rate_matcher.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_buffer.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_tx.h"
+#include "ocudu/phy/upper/channel_modulation/channel_modulation_factories.h"
+#include "ocudu/phy/upper/channel_modulation/demodulation_mapper.h"
+#include "ocudu/ran/sch/sch_segmentation.h"
+#include "lib/phy/upper/channel_coding/ldpc/ldpc_graph_impl.h"
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+using namespace ocudu;
+
+namespace {
+
+ldpc_base_graph_type to_bg(int bg)
+{
+  return bg == 2 ? ldpc_base_graph_type::BG2 : ldpc_base_graph_type::BG1;
+}
+
+crc_generator_poly to_poly(int p)
+{
+  switch (p) {
+    case 0:
+      return crc_generator_poly::CRC16;
+    case 1:
+      return crc_generator_poly::CRC24A;
+    case 2:
+      return crc_generator_poly::CRC24B;
+    case 3:
+      return crc_generator_poly::CRC24C;
+    case 4:
+      return crc_generator_poly::CRC11;
+    default:
+      return crc_generator_poly::CRC6;
+  }
+}
+
+modulation_scheme to_mod(int qm)
+{
+  switch (qm) {
+    case 1:
+      return modulation_scheme::BPSK;
+    case 2:
+      return modulation_scheme::QPSK;
+    case 4:
+      return modulation_scheme::QAM16;
+    case 6:
+      return modulation_scheme::QAM64;
+    default:
+      return modulation_scheme::QAM256;
+  }
+}
+
+// One decoder per (thread, variant): the reference objects are not thread safe.
+thread_local std::map<std::string, std::unique_ptr<ldpc_decoder>>   tl_decoders;
+thread_local std::map<int, std::unique_ptr<crc_calculator>>         tl_crc;
+thread_local std::unique_ptr<ldpc_rate_dematcher>                   tl_dematcher;
+thread_local std::unique_ptr<ldpc_encoder>                          tl_encoder;
+thread_local std::unique_ptr<ldpc_rate_matcher>                     tl_matcher;
+thread_local std::unique_ptr<demodulation_mapper>                   tl_demapper;
+
+crc_calculator* get_crc(int poly)
+{
+  auto it = tl_crc.find(poly);
+  if (it == tl_crc.end()) {
+    auto factory = create_crc_calculator_factory_sw("auto");
+    it           = tl_crc.emplace(poly, factory->create(to_poly(poly))).first;
+  }
+  return it->second.get();
+}
+
+ldpc_decoder* get_decoder(const char* variant)
+{
+  std::string key(variant);
+  auto        it = tl_decoders.find(key);
+  if (it == tl_decoders.end()) {
+    ldpc_decoder_factory::ldpc_decoder_factory_configuration cfg;
+    cfg.force_decoding      = false;
+    cfg.early_stop_syndrome = false;
+    auto factory            = create_ldpc_decoder_factory_sw(key, cfg);
+    if (!factory) {
+      return nullptr;
+    }
+    auto dec = factory->create();
+    if (!dec) {
+      return nullptr;
+    }
+    it = tl_decoders.emplace(key, std::move(dec)).first;
+  }
+  return it->second.get();
+}
+
+unsigned bg_k(int bg)
+{
+  return bg == 2 ? 10 : 22;
+}
+
+unsigned bg_n_short(int bg)
+{
+  return bg == 2 ? 50 : 66;
+}
+
+} // namespace
+
+extern "C" {
+
+/// Decodes one codeblock with the reference decoder of the given variant ("avx512", "avx2",
+/// "generic", "auto"). crc_poly < 0 disables CRC early stop. Output bits are packed MSB first
+/// (K*Z bits). Returns the iteration count (> 0) when the decoder reports success, 0 when it
+/// returns no value, and -1 when the variant is unavailable on this CPU.
+int ref_ldpc_decode(const char*   variant,
+                    int           bg,
+                    int           Z,
+                    int           nof_filler_bits,
+                    int           nof_crc_bits,
+                    int           crc_poly,
+                    int           max_iterations,
+                    const int8_t* llrs,
+                    int           nof_llrs,
+                    uint8_t*      out_packed)
+{
+  ldpc_decoder* dec = get_decoder(variant);
+  if (dec == nullptr) {
+    return -1;
+  }
+  ldpc_decoder::configuration cfg;
+  cfg.base_graph      = to_bg(bg);
+  cfg.lifting_size    = static_cast<ldpc::lifting_size_t>(Z);
+  cfg.nof_filler_bits = nof_filler_bits;
+  cfg.nof_crc_bits    = nof_crc_bits;
+  cfg.max_iterations  = max_iterations;
+
+  unsigned   K     = bg_k(bg) * Z;
+  bit_buffer out   = bit_buffer::from_bytes(span<uint8_t>(out_packed, (K + 7) / 8));
+  bit_buffer out_k = out.first(K);
+  span<const log_likelihood_ratio> in(reinterpret_cast<const log_likelihood_ratio*>(llrs), nof_llrs);
+  crc_calculator*                  crc = crc_poly < 0 ? nullptr : get_crc(crc_poly);
+  std::optional<unsigned>          res = dec->decode(out_k, in, crc, cfg);
+  return res.has_value() ? static_cast<int>(res.value()) : 0;
+}
+
+/// Returns the name of the decoder variant the reference's "auto" factory selects here.
+const char* ref_ldpc_auto_variant()
+{
+  static std::string name;
+  name = get_ldpc_decoder_type_str("auto");
+  return name.c_str();
+}
+
+/// CRC of nof_bits bits packed MSB first (crc_calculator::calculate on a bit_buffer).
+unsigned ref_crc_calculate(int crc_poly, const uint8_t* packed, int nof_bits)
+{
+  crc_calculator* crc = get_crc(crc_poly);
+  std::vector<uint8_t> tmp(packed, packed + (nof_bits + 7) / 8);
+  bit_buffer           buf = bit_buffer::from_bytes(span<uint8_t>(tmp)).first(nof_bits);
+  return crc->calculate(buf);
+}
+
+/// CRC of whole bytes (crc_calculator::calculate_byte).
+unsigned ref_crc_calculate_byte(int crc_poly, const uint8_t* bytes, int nof_bytes)
+{
+  return get_crc(crc_poly)->calculate_byte(span<const uint8_t>(bytes, nof_bytes));
+}
+
+/// Encodes K*Z message bits (packed MSB first; filler bits must be zero) into the full
+/// N = N_short*Z codeword, unpacked one bit per byte.
+int ref_ldpc_encode(int bg, int Z, const uint8_t* msg_packed, uint8_t* cw_unpacked)
+{
+  if (!tl_encoder) {
+    tl_encoder = create_ldpc_encoder_factory_sw("generic")->create();
+  }
+  unsigned               K = bg_k(bg) * Z;
+  std::vector<uint8_t>   tmp(msg_packed, msg_packed + (K + 7) / 8);
+  bit_buffer             msg = bit_buffer::from_bytes(span<uint8_t>(tmp)).first(K);
+  ldpc_encoder::configuration cfg;
+  cfg.base_graph   = to_bg(bg);
+  cfg.lifting_size = static_cast<ldpc::lifting_size_t>(Z);
+  cfg.Nref         = 0;
+  const ldpc_encoder_buffer& eb = tl_encoder->encode(msg, cfg);
+  unsigned                   N  = eb.get_codeblock_length();
+  eb.write_codeblock(span<uint8_t>(cw_unpacked, N), 0);
+  return static_cast<int>(N);
+}
+
+/// Encodes K*Z message bits and rate matches them to E bits (unpacked, one bit per byte),
+/// with the reference encoder and rate matcher.
+int ref_ldpc_encode_rm(int            bg,
+                       int            Z,
+                       int            rv,
+                       int            qm,
+                       int            Nref,
+                       int            nof_filler_bits,
+                       int            E,
+                       const uint8_t* msg_packed,
+                       uint8_t*       out_unpacked)
+{
+  if (!tl_encoder) {
+    tl_encoder = create_ldpc_encoder_factory_sw("generic")->create();
+  }
+  if (!tl_matcher) {
+    tl_matcher = create_ldpc_rate_matcher_factory_sw()->create();
+  }
+  unsigned             K = bg_k(bg) * Z;
+  std::vector<uint8_t> tmp(msg_packed, msg_packed + (K + 7) / 8);
+  bit_buffer           msg = bit_buffer::from_bytes(span<uint8_t>(tmp)).first(K);
+  ldpc_encoder::configuration cfg;
+  cfg.base_graph                 = to_bg(bg);
+  cfg.lifting_size               = static_cast<ldpc::lifting_size_t>(Z);
+  cfg.Nref                       = Nref;
+  const ldpc_encoder_buffer& eb  = tl_encoder->encode(msg, cfg);
+  codeblock_metadata         md  = {};
+  md.tb_common.base_graph        = to_bg(bg);
+  md.tb_common.lifting_size      = static_cast<ldpc::lifting_size_t>(Z);
+  md.tb_common.rv                = rv;
+  md.tb_common.mod               = to_mod(qm);
+  md.tb_common.Nref              = Nref;
+  md.cb_specific.full_length     = bg_n_short(bg) * Z;
+  md.cb_specific.rm_length       = E;
+  md.cb_specific.nof_filler_bits = nof_filler_bits;
+  std::vector<uint8_t> packed((E + 7) / 8);
+  bit_buffer           out = bit_buffer::from_bytes(span<uint8_t>(packed)).first(E);
+  tl_matcher->rate_match(out, eb, md);
+  for (int i = 0; i < E; ++i) {
+    out_unpacked[i] = out.extract(i, 1);
+  }
+  return 0;
+}
+
+/// Rate dematching of E LLRs into the N-LLR circular buffer (ldpc_rate_dematcher::rate_dematch).
+/// The output buffer is read before the call (soft combining when new_data == 0).
+int ref_rate_dematch(int           bg,
+                     int           Z,
+                     int           rv,
+                     int           qm,
+                     int           Nref,
+                     int           nof_filler_bits,
+                     int           new_data,
+                     const int8_t* in,
+                     int           E,
+                     int8_t*       out)
+{
+  if (!tl_dematcher) {
+    tl_dematcher = create_ldpc_rate_dematcher_factory_sw("auto")->create();
+  }
+  codeblock_metadata md          = {};
+  md.tb_common.base_graph        = to_bg(bg);
+  md.tb_common.lifting_size      = static_cast<ldpc::lifting_size_t>(Z);
+  md.tb_common.rv                = rv;
+  md.tb_common.mod               = to_mod(qm);
+  md.tb_common.Nref              = Nref;
+  md.cb_specific.full_length     = bg_n_short(bg) * Z;
+  md.cb_specific.rm_length       = E;
+  md.cb_specific.nof_filler_bits = nof_filler_bits;
+  unsigned N                     = bg_n_short(bg) * Z;
+  tl_dematcher->rate_dematch(span<log_likelihood_ratio>(reinterpret_cast<log_likelihood_ratio*>(out), N),
+                             span<const log_likelihood_ratio>(reinterpret_cast<const log_likelihood_ratio*>(in), E),
+                             new_data != 0,
+                             md);
+  return 0;
+}
+
+/// Soft demapping (demodulation_mapper::demodulate_soft): symbols are interleaved (re, im)
+/// float pairs; one noise variance per symbol; qm LLRs per symbol.
+int ref_demodulate_soft(int qm, const float* symbols, const float* noise_vars, int nof_symbols, int8_t* llrs)
+{
+  if (!tl_demapper) {
+    tl_demapper = create_demodulation_mapper_factory()->create();
+  }
+  tl_demapper->demodulate_soft(
+      span<log_likelihood_ratio>(reinterpret_cast<log_likelihood_ratio*>(llrs), nof_symbols * qm),
+      span<const cf_t>(reinterpret_cast<const cf_t*>(symbols), nof_symbols),
+      span<const float>(noise_vars, nof_symbols),
+      to_mod(qm));
+  return 0;
+}
+
+/// Lifted shift of base-graph edge (row, col) for lifting size Z, or -1 when there is no edge.
+int ref_ldpc_graph_shift(int bg, int Z, int row, int col)
+{
+  ldpc_graph_impl g(to_bg(bg), static_cast<ldpc::lifting_size_t>(Z));
+  uint16_t        v = g.get_lifted_node(row, col);
+  return v == ldpc::NO_EDGE ? -1 : static_cast<int>(v);
+}
+
+/// Writes the variable-node list of base-graph row `row` (in the decoder's edge order) and
+/// returns its length.
+int ref_ldpc_graph_row(int bg, int row, int* out_vars)
+{
+  ldpc_graph_impl                 g(to_bg(bg), ldpc::LS384);
+  const ldpc::BG_adjacency_row_t& r = g.get_adjacency_row(row);
+  int                             n = 0;
+  for (uint16_t v : r) {
+    if (v == ldpc::NO_EDGE) {
+      break;
+    }
+    out_vars[n++] = v;
+  }
+  return n;
+}
+
+/// TS 38.212 segmentation quantities as computed by the reference (sch_segmentation.h).
+/// Writes {C, Z, K(segment length), nof_tb_crc_bits}.
+int ref_sch_segmentation(int tbs_bits, int bg, int* out4)
+{
+  units::bits          tbs(tbs_bits);
+  ldpc_base_graph_type g   = to_bg(bg);
+  unsigned             C   = compute_nof_codeblocks(tbs, g);
+  unsigned             Zc  = compute_lifting_size(tbs, g, C);
+  unsigned             K   = compute_codeblock_size(g, Zc).value();
+  unsigned             crc = compute_tb_crc_size(tbs).value();
+  out4[0]                  = C;
+  out4[1]                  = Zc;
+  out4[2]                  = K;
+  out4[3]                  = crc;
+  return 0;
+}
+
+} // extern "C"

@@ -1,0 +1,159 @@
+"""Generates the golden fixtures in tests/golden/ from the reference's own compiled CPU code
+(oracle/_ref/libocudu_ref.so, built by `make -C oracle ref` from the reference sources).
+
+Inputs come from this project's seeded simulator; outputs (decoded bits, iteration counts, CRCs,
+dematched buffers, encoded codewords) come from the reference. Run in a container that holds the
+reference:
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "ocudu-dapp-platform_b200"))
+
+from oracle import Ref  # noqa: E402
+from pusch_b200 import codec  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def kb(bg):
+    return 22 if bg == 1 else 10
+
+
+def nshort(bg):
+    return 66 if bg == 1 else 50
+
+
+def make_cb(rng, bg, z, filler, crc_poly, e_len, ebn0, scale=4.0):
+    """A rate-dematched-style LLR buffer of length N: noisy LLRs for the first e_len positions of
+    the shortened codeword, +127 at filler positions, zeros after e_len."""
+    k = kb(bg) * z
+    order = 16 if crc_poly == 0 else 24
+    info = rng.integers(0, 2, k - filler - order, dtype=np.uint8)
+    msg = np.concatenate([codec.attach_crc(crc_poly, info), np.zeros(filler, np.uint8)])
+    cw = codec.ldpc_encode(bg, z, msg)
+    n = nshort(bg) * z
+    sigma = np.sqrt(1.0 / (2.0 * (k / max(e_len, 1)) * 10.0 ** (ebn0 / 10.0)))
+    y = (1.0 - 2.0 * cw) + sigma * rng.standard_normal(n)
+    llr = np.clip(np.rint(2.0 * y / sigma ** 2 * scale), -120, 120).astype(np.int8)
+    llr[e_len:] = 0
+    if filler:
+        llr[k - 2 * z - filler:k - 2 * z] = 127
+    return llr
+
+
+def ldpc_cases(ref, rng):
+    cases = []
+    # Config-2 shaped codeblocks: BG1/BG2 Z=384, full buffer, CRC24B, 10 iterations.
+    for i in range(8):
+        bg = 1 + (i % 2)
+        cases.append((bg, 384, 0, 2, 10, nshort(bg) * 384, 1.0 + 0.25 * i))
+    # Assorted lifting sizes, fillers, shortened inputs, CRC polynomials and iteration caps.
+    for bg, z, f, poly, it, frac, eb in [
+        (1, 2, 8, 0, 6, 1.0, 3.0), (2, 3, 5, 0, 6, 0.8, 2.0), (1, 7, 20, 0, 8, 0.6, 3.0),
+        (2, 15, 30, 1, 6, 0.7, 2.5), (1, 64, 100, 1, 6, 0.5, 4.0), (2, 208, 0, 2, 10, 0.9, 1.5),
+        (1, 288, 424, 1, 6, 0.45, 5.0), (2, 384, 72, 2, 4, 0.6, 3.0), (1, 384, 64, 2, 6, 0.5, 6.0),
+        (1, 160, 0, 2, 1, 1.0, 3.0), (2, 52, 12, 0, 20, 1.0, 0.5), (1, 384, 0, 2, 10, 1.0, -1.0),
+        (1, 120, 0, 255, 6, 0.8, 4.0), (2, 96, 8, 255, 6, 1.0, 0.0),
+    ]:
+        n = nshort(bg) * z
+        k = kb(bg) * z
+        e_len = max(int(frac * n), k + 2 * z)
+        cases.append((bg, z, f, poly, it, e_len, eb))
+    meta, llrs, bits, iters = [], [], [], []
+    for (bg, z, f, poly, it, e_len, eb) in cases:
+        cpoly = 2 if poly == 255 else poly
+        llr = make_cb(rng, bg, z, f, cpoly, e_len, eb)
+        nof_crc = 16 if cpoly == 0 else 24
+        got, out = ref.ldpc_decode(bg, z, llr, filler=f, crc_poly=(-1 if poly == 255 else poly), max_iter=it,
+                                   nof_crc_bits=nof_crc)
+        meta.append([bg, z, f, poly, it, llr.size])
+        llrs.append(llr)
+        bits.append(out)
+        iters.append(got)
+    # Special inputs: all zeros, and fewer than K*Z significant soft bits (both fail, all ones).
+    for bg, z in [(1, 384), (2, 64)]:
+        n = nshort(bg) * z
+        k = kb(bg) * z
+        for kind in ("zeros", "short"):
+            llr = np.zeros(n, np.int8)
+            if kind == "short":
+                llr[: k - 3] = rng.integers(-120, 121, k - 3)
+            got, out = ref.ldpc_decode(bg, z, llr, filler=0, crc_poly=2, max_iter=6, prefill=0xFF)
+            meta.append([bg, z, 0, 2, 6, n])
+            llrs.append(llr)
+            bits.append(out)
+            iters.append(got)
+    off = np.cumsum([0] + [x.size for x in llrs])
+    boff = np.cumsum([0] + [x.size for x in bits])
+    return dict(meta=np.array(meta, np.int32), llr_offsets=off.astype(np.int64), llrs=np.concatenate(llrs),
+                bit_offsets=boff.astype(np.int64), bits=np.concatenate(bits), iterations=np.array(iters, np.int32))
+
+
+def rm_cases(ref, rng):
+    meta, ins, prevs, outs = [], [], [], []
+    for t in range(30):
+        bg = 1 + t % 2
+        z = [384, 64, 16, 7, 2, 104, 36, 13, 22, 8][t % 10]
+        qm = [1, 2, 4, 6, 8][t % 5]
+        rv = (t // 5) % 4
+        k = kb(bg) * z
+        n = nshort(bg) * z
+        f = int(rng.integers(0, (k - 2 * z) // 3))
+        nref = 0 if t % 3 else int(rng.integers(k, n + 1))
+        e = qm * int(rng.integers(1, (13 * n) // (10 * qm)))
+        llr = rng.integers(-120, 121, e).astype(np.int8)
+        prev = rng.integers(-120, 121, n).astype(np.int8)
+        new_data = int(t % 4 != 3)
+        out = ref.rate_dematch(bg, z, llr, rv=rv, qm=qm, Nref=nref, filler=f, new_data=new_data, out=prev.copy())
+        meta.append([bg, z, rv, qm, nref, f, new_data, e])
+        ins.append(llr)
+        prevs.append(prev)
+        outs.append(out)
+    return dict(meta=np.array(meta, np.int32), in_offsets=np.cumsum([0] + [x.size for x in ins]).astype(np.int64),
+                ins=np.concatenate(ins), buf_offsets=np.cumsum([0] + [x.size for x in prevs]).astype(np.int64),
+                prevs=np.concatenate(prevs), outs=np.concatenate(outs))
+
+
+def crc_cases(ref, rng):
+    meta, bits, crcs = [], [], []
+    for poly in (0, 1, 2):
+        for length in (1, 7, 8, 9, 31, 33, 100, 1000, 3816, 8424, 8448):
+            b = rng.integers(0, 2, length, dtype=np.uint8)
+            meta.append([poly, length])
+            bits.append(b)
+            crcs.append(ref.crc(poly, b))
+    return dict(meta=np.array(meta, np.int32), offsets=np.cumsum([0] + [x.size for x in bits]).astype(np.int64),
+                bits=np.concatenate(bits), crcs=np.array(crcs, np.uint32))
+
+
+def enc_cases(ref, rng):
+    meta, msgs, cws = [], [], []
+    for bg, z in [(1, 384), (2, 384), (1, 2), (2, 7), (1, 288), (2, 208), (1, 15), (2, 52)]:
+        k = kb(bg) * z
+        m = rng.integers(0, 2, k, dtype=np.uint8)
+        meta.append([bg, z])
+        msgs.append(m)
+        cws.append(ref.ldpc_encode(bg, z, m))
+    return dict(meta=np.array(meta, np.int32), msg_offsets=np.cumsum([0] + [x.size for x in msgs]).astype(np.int64),
+                msgs=np.concatenate(msgs), cw_offsets=np.cumsum([0] + [x.size for x in cws]).astype(np.int64),
+                cws=np.concatenate(cws))
+
+
+def main():
+    ref = Ref()
+    rng = np.random.default_rng(20261203)
+    np.savez_compressed(os.path.join(OUT, "ldpc_decode.npz"), variant=ref.variant, **ldpc_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "rate_dematch.npz"), **rm_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "crc.npz"), **crc_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "ldpc_encode.npz"), **enc_cases(ref, rng))
+    print("golden fixtures written; reference LDPC variant:", ref.variant)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,50 @@
+"""Readers for the committed golden fixtures (tests/golden/*.npz)."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name))
+
+
+def ldpc_cases():
+    d = load("ldpc_decode.npz")
+    out = []
+    for i, m in enumerate(d["meta"]):
+        bg, z, f, poly, it, n = (int(x) for x in m)
+        llr = d["llrs"][d["llr_offsets"][i]:d["llr_offsets"][i + 1]]
+        bits = d["bits"][d["bit_offsets"][i]:d["bit_offsets"][i + 1]]
+        out.append(dict(bg=bg, z=z, filler=f, poly=poly, max_iter=it, llrs=llr, bits=bits,
+                        iterations=int(d["iterations"][i])))
+    return out
+
+
+def rm_cases():
+    d = load("rate_dematch.npz")
+    out = []
+    for i, m in enumerate(d["meta"]):
+        bg, z, rv, qm, nref, f, nd, e = (int(x) for x in m)
+        out.append(dict(bg=bg, z=z, rv=rv, qm=qm, nref=nref, filler=f, new_data=nd,
+                        llrs=d["ins"][d["in_offsets"][i]:d["in_offsets"][i + 1]],
+                        prev=d["prevs"][d["buf_offsets"][i]:d["buf_offsets"][i + 1]],
+                        out=d["outs"][d["buf_offsets"][i]:d["buf_offsets"][i + 1]]))
+    return out
+
+
+def crc_cases():
+    d = load("crc.npz")
+    return [dict(poly=int(m[0]), bits=d["bits"][d["offsets"][i]:d["offsets"][i + 1]], crc=int(d["crcs"][i]))
+            for i, m in enumerate(d["meta"])]
+
+
+def enc_cases():
+    d = load("ldpc_encode.npz")
+    return [dict(bg=int(m[0]), z=int(m[1]), msg=d["msgs"][d["msg_offsets"][i]:d["msg_offsets"][i + 1]],
+                 cw=d["cws"][d["cw_offsets"][i]:d["cw_offsets"][i + 1]]) for i, m in enumerate(d["meta"])]
+
+
+def kbits(bg, z):
+    return (22 if bg == 1 else 10) * z
