@@ -75,24 +75,143 @@ __device__ __forceinline__ uint32_t warp_xor(uint32_t v)
   return v;
 }
 
-__global__ void __launch_bounds__(kThreads) ldpc_decode_kernel(const pg_ldpc_cb* __restrict__ descs,
-                                                              const int8_t* __restrict__ llrs,
-                                                              uint8_t* __restrict__ bits,
-                                                              int32_t* __restrict__ iterations,
-                                                              int8_t* __restrict__ c2v_all,
-                                                              const uint32_t* __restrict__ crc_pow)
+// One layer (base-graph row) for check lane tid, specialised on the row degree so that the edge
+// loops unroll without predication. FIRST selects the first iteration, where every row's
+// check-to-variable messages are still zero (the reference copies the soft bits into the v2c
+// messages then: ldpc_decoder_impl.cpp:208-212).
+template <int DEG, bool FIRST, int ZT>
+__device__ __forceinline__ void row_update(const int tid, const int Zr, int8_t* __restrict__ soft,
+                                           const uint32_t* __restrict__ edge, int8_t* __restrict__ c2v_row)
 {
-  __shared__ __align__(16) int8_t soft[pg::kMaxNodes * pg::kMaxZ];
-  __shared__ uint32_t             edge[pg::kBg1Edges];
-  __shared__ uint32_t             hard[(22 * pg::kMaxZ) / 32];
-  __shared__ uint32_t             red[kThreads / 32];
-  __shared__ int                  s_last;
-  __shared__ int                  s_done;
+  const int Z = ZT > 0 ? ZT : Zr;
+  int       m[DEG];
+  unsigned  pos[DEG];
+  int       min1 = 120, min2 = 120, sgn = 0;
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    const uint32_t ed = edge[e];
+    const unsigned p0 = (unsigned)tid + (ed & 0xffffu);
+    const unsigned p  = min(p0, p0 - (unsigned)Z) + (ed >> 16);
+    pos[e]            = p;
+    const int x       = soft[p];
+    int       v       = x;
+    if (!FIRST) {
+      const int c = c2v_row[e * Z];
+      v           = max(-120, min(120, x - c));
+      v           = (x == 127 || x == -127) ? x : v;
+    }
+    m[e]        = v;
+    const int a = abs(v);
+    min2        = min(min2, max(min1, a));
+    min1        = min(min1, a);
+    sgn ^= v;
+  }
+  const int s1 = scale_mag(min1);
+  const int s2 = scale_mag(min2);
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    const int v    = m[e];
+    const int a    = abs(v);
+    const int mag  = (a == min1) ? s2 : s1;
+    const int c    = ((v ^ sgn) < 0) ? -mag : mag;
+    c2v_row[e * Z] = (int8_t)c;
+    int t          = c + v;
+    t              = (t > 120) ? 127 : ((t < -120) ? -127 : t);
+    t              = (a == 127) ? v : t;
+    soft[pos[e]]   = (int8_t)t;
+  }
+}
 
-  const pg_ldpc_cb d   = descs[blockIdx.x];
+// Degree-19 rows (BG1 rows 0-3): the same update as a rolled loop with the v2c messages staged in
+// shared memory (one byte per edge and lane), so the wide rows do not raise the register budget
+// of the whole kernel; the soft-bit addresses are recomputed in the second pass.
+template <bool FIRST, int ZT>
+__device__ __forceinline__ void row_update_wide(const int deg, const int tid, const int Zr, int8_t* __restrict__ soft,
+                                                const uint32_t* __restrict__ edge, int8_t* __restrict__ c2v_row,
+                                                int8_t* __restrict__ mbuf)
+{
+  const int Z    = ZT > 0 ? ZT : Zr;
+  int       min1 = 120, min2 = 120, sgn = 0;
+#pragma unroll 2
+  for (int e = 0; e < deg; ++e) {
+    const uint32_t ed = edge[e];
+    const unsigned p0 = (unsigned)tid + (ed & 0xffffu);
+    const unsigned p  = min(p0, p0 - (unsigned)Z) + (ed >> 16);
+    const int      x  = soft[p];
+    int            v  = x;
+    if (!FIRST) {
+      const int c = c2v_row[e * Z];
+      v           = max(-120, min(120, x - c));
+      v           = (x == 127 || x == -127) ? x : v;
+    }
+    mbuf[e * kThreads + tid] = (int8_t)v;
+    const int a              = abs(v);
+    min2                     = min(min2, max(min1, a));
+    min1                     = min(min1, a);
+    sgn ^= v;
+  }
+  const int s1 = scale_mag(min1);
+  const int s2 = scale_mag(min2);
+#pragma unroll 2
+  for (int e = 0; e < deg; ++e) {
+    const uint32_t ed  = edge[e];
+    const unsigned p0  = (unsigned)tid + (ed & 0xffffu);
+    const unsigned p   = min(p0, p0 - (unsigned)Z) + (ed >> 16);
+    const int      v   = mbuf[e * kThreads + tid];
+    const int      a   = abs(v);
+    const int      mag = (a == min1) ? s2 : s1;
+    const int      c   = ((v ^ sgn) < 0) ? -mag : mag;
+    c2v_row[e * Z]     = (int8_t)c;
+    int t              = c + v;
+    t                  = (t > 120) ? 127 : ((t < -120) ? -127 : t);
+    t                  = (a == 127) ? v : t;
+    soft[p]            = (int8_t)t;
+  }
+}
+
+// Base-graph row degrees: BG1 {3..10, 19}, BG2 {3..10}.
+template <bool FIRST, int ZT>
+__device__ __forceinline__ void row_dispatch(int deg, int tid, int Z, int8_t* soft, const uint32_t* edge, int8_t* c2v_row,
+                                             int8_t* mbuf)
+{
+  switch (deg) {
+    case 3: row_update<3, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 4: row_update<4, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 5: row_update<5, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 6: row_update<6, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 7: row_update<7, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 8: row_update<8, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 9: row_update<9, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    case 10: row_update<10, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
+    default: row_update_wide<FIRST, ZT>(deg, tid, Z, soft, edge, c2v_row, mbuf); break;
+  }
+}
+
+struct smem_t {
+  __align__(16) int8_t soft[pg::kMaxNodes * pg::kMaxZ];
+  uint32_t             edge[pg::kBg1Edges];
+  uint32_t             hard[(22 * pg::kMaxZ) / 32];
+  uint32_t             red[kThreads / 32];
+  int8_t               mbuf[pg::kMaxRowDegree * kThreads]; // v2c staging of the degree-19 rows
+  int                  s_last;
+  int                  s_done;
+};
+
+// Decodes codeblock blockIdx.x; ZT > 0 specialises the lifting size at compile time.
+template <int ZT>
+__device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm, const int8_t* __restrict__ llrs,
+                                                 uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
+                                                 int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow)
+{
+  int8_t*   soft   = sm.soft;
+  uint32_t* edge   = sm.edge;
+  uint32_t* hard   = sm.hard;
+  uint32_t* red    = sm.red;
+  int&      s_last = sm.s_last;
+  int&      s_done = sm.s_done;
   const int        tid = threadIdx.x;
   const int        bg  = d.base_graph;
-  const int        Z   = d.lifting_size;
+  const int        Z   = ZT > 0 ? ZT : (int)d.lifting_size;
   const int        set = (Z >= 2 && Z <= pg::kMaxZ) ? dev_set_index(Z) : -1;
   if ((bg != 1 && bg != 2) || set < 0) {
     if (tid == 0) {
@@ -184,43 +303,11 @@ __global__ void __launch_bounds__(kThreads) ldpc_decode_kernel(const pg_ldpc_cb*
     for (int r = 0; r < nof_layers; ++r) {
       const int deg = c_row_deg[g][r];
       if (tid < Z) {
-        int      v2c[pg::kMaxRowDegree];
-        int      pos[pg::kMaxRowDegree];
-        int      min1 = 120, min2 = 120, sgn = 0;
-        int8_t*  c2v_row = c2v + (size_t)e0 * Z + tid;
-#pragma unroll
-        for (int e = 0; e < pg::kMaxRowDegree; ++e) {
-          if (e < deg) {
-            const uint32_t ed = edge[e0 + e];
-            int            p  = tid + (int)(ed & 0xffffu);
-            p                 = (p >= Z) ? p - Z : p;
-            p += (int)(ed >> 16);
-            pos[e]      = p;
-            const int x = soft[p];
-            const int c = (it > 0) ? (int)c2v_row[e * Z] : 0;
-            int       m = max(-120, min(120, x - c));
-            m           = (x >= 127 || x <= -127) ? x : m;
-            v2c[e]      = m;
-            const int a = abs(m);
-            min2        = min(min2, max(min1, a));
-            min1        = min(min1, a);
-            sgn ^= m;
-          }
-        }
-        const int s1 = scale_mag(min1);
-        const int s2 = scale_mag(min2);
-#pragma unroll
-        for (int e = 0; e < pg::kMaxRowDegree; ++e) {
-          if (e < deg) {
-            const int m   = v2c[e];
-            const int mag = (abs(m) == min1) ? s2 : s1;
-            const int c   = ((m ^ sgn) < 0) ? -mag : mag;
-            c2v_row[e * Z] = (int8_t)c;
-            int s          = c + m;
-            s              = (s > 120) ? 127 : ((s < -120) ? -127 : s);
-            s              = (m == 127 || m == -127) ? m : s;
-            soft[pos[e]]   = (int8_t)s;
-          }
+        int8_t* c2v_row = c2v + (size_t)e0 * Z + tid;
+        if (it == 0) {
+          row_dispatch<true, ZT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+        } else {
+          row_dispatch<false, ZT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
         }
       }
       e0 += deg;
@@ -325,6 +412,23 @@ __global__ void __launch_bounds__(kThreads) ldpc_decode_kernel(const pg_ldpc_cb*
   }
   if (tid == 0) {
     iterations[blockIdx.x] = result;
+  }
+}
+
+
+__global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_cb* __restrict__ descs,
+                                                              const int8_t* __restrict__ llrs,
+                                                              uint8_t* __restrict__ bits,
+                                                              int32_t* __restrict__ iterations,
+                                                              int8_t* __restrict__ c2v_all,
+                                                              const uint32_t* __restrict__ crc_pow)
+{
+  __shared__ smem_t sm;
+  const pg_ldpc_cb  d = descs[blockIdx.x];
+  if (d.lifting_size == 384) {
+    decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow);
+  } else {
+    decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow);
   }
 }
 

@@ -52,6 +52,9 @@ class Ref:
         lib.ref_demodulate_soft.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                             ctypes.c_void_p]
         lib.ref_sch_segmentation.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        lib.ref_ldpc_decode_batch_mt.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        lib.ref_ldpc_decode_batch_mt.restype = ctypes.c_double
         self.lib = lib
         self.variant = lib.ref_ldpc_auto_variant().decode()
 
@@ -72,6 +75,18 @@ class Ref:
         bits = np.ascontiguousarray(bits, dtype=np.uint8)
         packed = np.packbits(bits) if bits.size else np.zeros(1, np.uint8)
         return self.lib.ref_crc_calculate(poly, _ptr(packed), bits.size)
+
+    def ldpc_decode_batch_mt(self, meta, llr_offsets, llrs, threads, variant=None):
+        """Multi-threaded batch decode in C++ (no interpreter in the loop). meta: int32 [n, 6]
+        {bg, Z, filler, crc_poly, max_iterations, nof_llrs}. Returns (iterations, wall seconds)."""
+        meta = np.ascontiguousarray(meta, dtype=np.int32)
+        offs = np.ascontiguousarray(llr_offsets, dtype=np.int64)
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        it = np.zeros(meta.shape[0], np.int32)
+        v = (variant or self.variant).encode()
+        dt = self.lib.ref_ldpc_decode_batch_mt(v, meta.shape[0], _ptr(meta), _ptr(offs), _ptr(llrs), _ptr(it),
+                                               threads)
+        return it, dt
 
     def ldpc_encode(self, bg, Z, msg_bits):
         msg = np.packbits(np.ascontiguousarray(msg_bits, dtype=np.uint8))

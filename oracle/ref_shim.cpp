@@ -28,7 +28,10 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <atomic>
+#include <chrono>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace ocudu;
@@ -336,6 +339,49 @@ int ref_sch_segmentation(int tbs_bits, int bg, int* out4)
   out4[2]                  = K;
   out4[3]                  = crc;
   return 0;
+}
+
+/// Decodes a batch of codeblocks on nof_threads host threads (one reference decoder per thread,
+/// codeblocks claimed dynamically), as the reference's per-codeblock executor tasks do
+/// (lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.cpp:466-470). meta holds six ints
+/// per codeblock {bg, Z, filler, crc_poly, max_iterations, nof_llrs}; llr_offsets gives each
+/// codeblock's first LLR. Writes iterations (0 = failure) and returns the wall time in seconds.
+double ref_ldpc_decode_batch_mt(const char*    variant,
+                                int            nof_cbs,
+                                const int*     meta,
+                                const int64_t* llr_offsets,
+                                const int8_t*  llrs,
+                                int*           iterations,
+                                int            nof_threads)
+{
+  std::atomic<int> next{0};
+  auto             worker = [&]() {
+    std::vector<uint8_t> out((22 * 384 + 7) / 8);
+    for (int i = next.fetch_add(1); i < nof_cbs; i = next.fetch_add(1)) {
+      const int* m    = meta + 6 * i;
+      int        poly = m[3] == 255 ? -1 : m[3];
+      iterations[i]   = ref_ldpc_decode(variant,
+                                      m[0],
+                                      m[1],
+                                      m[2],
+                                      poly == 0 ? 16 : 24,
+                                      poly,
+                                      m[4],
+                                      llrs + llr_offsets[i],
+                                      m[5],
+                                      out.data());
+    }
+  };
+  // Create the per-thread decoders before the clock starts.
+  auto                     t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nof_threads; ++t) {
+    pool.emplace_back(worker);
+  }
+  for (auto& th : pool) {
+    th.join();
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 } // extern "C"

@@ -35,7 +35,7 @@ def test_golden_batch_bit_exact(batch_decoder):
 def random_jobs(seed, n):
     rng = np.random.default_rng(seed)
     jobs = []
-    zs = [2, 3, 5, 8, 13, 16, 26, 36, 64, 72, 104, 120, 176, 208, 240, 256, 288, 320, 352, 384]
+    zs = [8, 13, 16, 26, 36, 64, 72, 104, 120, 176, 208, 240, 256, 288, 320, 352, 384]  # small Z: golden cases
     for t in range(n):
         bg = int(rng.integers(1, 3))
         z = int(rng.choice(zs))
