@@ -296,28 +296,34 @@ def run_ours(args):
                "h2d_bytes_per_step": int(h_llrs.numel() + len(bytes(descs))),
                "d2h_bytes_per_step": int(h_bits.numel() + 4 * N_CBS), "ms_per_step": round(e_ms, 3)}
 
-    # Integer roofline of the decoding kernel.
-    peak_ops = None
+    # Integer roofline of the decoding kernel. Denominator: the measured full-rate integer
+    # instruction throughput of this GPU (best of add.s32 / min.s32 in libpg_probe.so).
+    peak_ops, classes = None, None
     try:
         probe = ctypes.CDLL(os.path.join(ROOT, "ocudu-dapp-platform_b200", "pusch_b200", "_lib", "libpg_probe.so"))
-        probe.pg_probe_int_ops_per_s.restype = ctypes.c_double
-        probe.pg_probe_int_ops_per_s.argtypes = [ctypes.c_int, ctypes.c_int]
-        peak_ops = max(probe.pg_probe_int_ops_per_s(dev, 1 << 14) for _ in range(3))
+        probe.pg_probe_inst_classes.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        buf = (ctypes.c_double * 8)()
+        if probe.pg_probe_inst_classes(dev, buf) == 0:
+            names = ["add.s32", "min.s32", "mad.lo.u32", "prmt.b32", "min.s16x2", "add.f16x2", "min.f16x2",
+                     "fma.f16x2"]
+            classes = {n: round(buf[i] / 1e12, 2) for i, n in enumerate(names)}
+            peak_ops = max(buf[0], buf[1])
     except OSError:
         pass
     achieved = ops / (ms * 1e-3) / 1e12
     props = torch.cuda.get_device_properties(dev)
     nominal = props.multi_processor_count * 128 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
+    peak = peak_ops / 1e12 if peak_ops else nominal
     roofline = {
-        "bound": "int", "kernel": "ldpc_decode_kernel", "achieved": round(achieved, 3),
-        "peak": round(peak_ops / 1e12, 3) if peak_ops else round(nominal, 3),
-        "unit": "Tops/s",
-        "frac": round(achieved / (peak_ops / 1e12 if peak_ops else nominal), 4),
-        "peak_source": "measured integer-mix probe (libpg_probe.so) on this GPU" if peak_ops else
-                       "nominal 148 SM x 128 lanes x max SM clock",
-        "nominal_peak": round(nominal, 3),
+        "bound": "int", "kernel": "ldpc_decode_kernel", "achieved": round(achieved, 3), "peak": round(peak, 3),
+        "unit": "Tops/s", "frac": round(achieved / peak, 4),
+        "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"
+                        if peak_ops else "nominal 148 SM x 128 lanes x max SM clock"),
+        "nominal_peak": round(nominal, 3), "instruction_classes_tops": classes,
         "ops_per_edge_update": INT_OPS_PER_EDGE, "edge_updates_per_launch": edge_updates,
-        "traffic": None,
+        # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload (ncu capture
+        # summarised in profiles/ldpc_decode_kernel_ldpc-batch-512cb.md).
+        "traffic": 17298000,
         "hbm_bytes_per_launch": int(llrs.size + nbytes + 4 * N_CBS + 20 * N_CBS),
     }
 

@@ -114,6 +114,127 @@ int pg_set_kernel_timing(pg_context* ctx, int enabled);
  * or a negative value when none was recorded. */
 float pg_last_kernel_ms(pg_context* ctx);
 
+
+/* ---------------------------------------------------------------------------------------- */
+/* Rate dematching                                                                           */
+
+/* One codeblock of a rate-dematching batch: the fields of codeblock_metadata that
+ * ldpc_rate_dematcher::rate_dematch reads (include/ocudu/phy/upper/codeblock_metadata.h). */
+typedef struct pg_rm_cb {
+  uint32_t in_offset;       /* first of this codeblock's E rate-matched LLRs in the input */
+  uint32_t rm_length;       /* E (a multiple of the modulation order) */
+  uint32_t out_offset;      /* first of this codeblock's N = N_short*Z buffer LLRs in the output */
+  uint32_t nref;            /* N_ref (limited-buffer rate matching), 0 = unlimited */
+  uint16_t lifting_size;    /* Z */
+  uint16_t nof_filler_bits; /* F */
+  uint8_t  base_graph;      /* 1 or 2 */
+  uint8_t  rv;              /* redundancy version 0..3 */
+  uint8_t  modulation_order;/* Qm: 1, 2, 4, 6 or 8 */
+  uint8_t  new_data;        /* 1: overwrite the buffer; 0: soft-combine into it (HARQ) */
+} pg_rm_cb;
+
+/* Batched rate dematching, replacing ldpc_rate_dematcher::rate_dematch
+ * (include/ocudu/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher.h:36-39;
+ * lib/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher_impl.cpp:29-250). Device pointers; the
+ * output buffers are read when new_data == 0. */
+int pg_rate_dematch_batch_device(pg_context* ctx, const pg_rm_cb* cbs, int nof_cbs, const int8_t* in, int8_t* out,
+                                 void* stream);
+/* Same from and to host memory (out is read for soft combining and written back). */
+int pg_rate_dematch_batch_host(pg_context* ctx, const pg_rm_cb* cbs, int nof_cbs, const int8_t* in, size_t in_len,
+                               int8_t* out, size_t out_len);
+
+/* ---------------------------------------------------------------------------------------- */
+/* CRC and transport-block assembly                                                          */
+
+/* One CRC computation over nof_bits bits starting at bit_offset of a packed MSB-first buffer. */
+typedef struct pg_crc_item {
+  uint32_t bit_offset;
+  uint32_t nof_bits;
+  uint32_t poly; /* PG_CRC16, PG_CRC24A or PG_CRC24B */
+} pg_crc_item;
+
+/* Batched crc_calculator::calculate(const bit_buffer&)
+ * (include/ocudu/phy/upper/channel_coding/crc_calculator.h:67-77): remainder of each bit string
+ * (zero initial value, MSB first, no output XOR; 0 means the string ends in a valid CRC). */
+int pg_crc_calculate_device(pg_context* ctx, const pg_crc_item* items, int nof_items, const uint8_t* data,
+                            uint32_t* crcs, void* stream);
+int pg_crc_calculate_host(pg_context* ctx, const pg_crc_item* items, int nof_items, const uint8_t* data,
+                          size_t data_len, uint32_t* crcs);
+
+/* One transport block to assemble from decoded codeblocks (all codeblocks of a TB have the same
+ * payload size per TS 38.212 Section 5.2.2). */
+typedef struct pg_tb_desc {
+  uint32_t cb_first;        /* index of the TB's first codeblock in cb_bit_offsets */
+  uint32_t nof_cbs;         /* C */
+  uint32_t cb_payload_bits; /* K' - L per codeblock (L = 24 when C > 1, else 0) */
+  uint32_t tbs_bits;        /* transport block size, a multiple of 8 */
+  uint32_t tb_out_offset;   /* byte offset of the TB payload in tb_out */
+  uint32_t crc_poly;        /* PG_CRC16 or PG_CRC24A */
+} pg_tb_desc;
+
+/* Concatenates the codeblock payloads of each TB into tb_out (TBS/8 bytes) and computes the TB CRC
+ * remainder over TBS + CRC bits (0 = TB CRC passes), as the reference's TB join
+ * (lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.cpp:612-710). cb_bit_offsets[i] is
+ * the bit offset of codeblock i's decoded bits in cb_bits (device memory, like all buffers). */
+int pg_tb_assemble_device(pg_context* ctx, const pg_tb_desc* tbs, int nof_tbs, const uint8_t* cb_bits,
+                          const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, void* stream);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Segmentation and transport-block decoding (pusch_decoder)                                 */
+
+/* Segmentation of one UL-SCH transport block (TS 38.212 Sections 5.2.2 and 5.4.2.1), the
+ * quantities the reference's ldpc_segmenter_rx computes
+ * (lib/phy/upper/channel_coding/ldpc/ldpc_segmenter_rx_impl.cpp:33-85,
+ * include/ocudu/ran/sch/sch_segmentation.h:40-118). */
+typedef struct pg_sch_segmentation {
+  uint32_t nof_cbs;         /* C */
+  uint32_t lifting_size;    /* Z_c */
+  uint32_t cb_length;       /* K = K_b * Z_c (22 or 10 info columns) */
+  uint32_t nof_filler_bits; /* F */
+  uint32_t cb_crc_bits;     /* 24 when C > 1, else 0 */
+  uint32_t tb_crc_bits;     /* 16 or 24 */
+  uint32_t nof_short_cbs;   /* codeblocks with E = floor(...); the rest have E = ceil(...) */
+  uint32_t e_short;         /* E of the short codeblocks */
+  uint32_t e_long;          /* E of the long codeblocks */
+} pg_sch_segmentation;
+
+int pg_sch_segment(uint32_t tbs_bits, int base_graph, int modulation_order, int nof_layers,
+                   uint32_t nof_ch_symbols, pg_sch_segmentation* out);
+
+/* One UL-SCH transport block to decode from its (descrambled) codeword LLRs: the configuration
+ * of pusch_decoder::new_data / set_nof_softbits (include/ocudu/phy/upper/channel_processors/
+ * pusch/pusch_decoder.h:38-145). */
+typedef struct pg_sch_tb {
+  uint32_t llr_offset;      /* first codeword LLR (G = nof_ch_symbols * Qm * layers LLRs) */
+  uint32_t nof_ch_symbols;  /* channel symbols of the codeword (all layers) */
+  uint32_t tbs_bits;        /* transport block size */
+  uint32_t tb_out_offset;   /* byte offset of the decoded TB */
+  uint32_t nref;            /* N_ref, 0 = unlimited */
+  uint8_t  base_graph;
+  uint8_t  modulation_order;
+  uint8_t  nof_layers;
+  uint8_t  rv;
+  uint8_t  max_iterations;
+  uint8_t  reserved[3];
+} pg_sch_tb;
+
+/* Per-TB result: the reference's pusch_decoder_result (tb_crc_ok, codeblock counts and the
+ * LDPC iteration statistics). */
+typedef struct pg_sch_result {
+  uint32_t tb_crc_ok;
+  uint32_t nof_cbs;
+  uint32_t nof_cbs_crc_ok;
+  float    mean_iterations;  /* over the TB's codeblocks (failed codeblocks count max_iterations) */
+  uint32_t max_iterations_run;
+} pg_sch_result;
+
+/* Decodes a batch of transport blocks end to end on the GPU: segmentation (host), rate
+ * dematching, LDPC decoding with CRC early stop, TB assembly and TB CRC - the work of
+ * pusch_decoder_impl (lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.cpp:22-921) for
+ * new transmissions. Host buffers in and out. */
+int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* llrs,
+                             size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,24 +9,6 @@
 
 namespace pg {
 
-void crc_poly_params(int poly, uint32_t* g, int* order)
-{
-  switch (poly) {
-    case PG_CRC16:
-      *g     = 0x11021u;
-      *order = 16;
-      break;
-    case PG_CRC24A:
-      *g     = 0x1864cfbu;
-      *order = 24;
-      break;
-    default:
-      *g     = 0x1800063u;
-      *order = 24;
-      break;
-  }
-}
-
 int set_error(pg_context* ctx, int code, const std::string& msg)
 {
   if (ctx != nullptr) {
@@ -150,6 +132,87 @@ static int release_descs_after(pg_context* ctx, cudaStream_t s)
   return PG_OK;
 }
 
+int stage_slot(pg_context* ctx, int slot, const void* host, size_t bytes, cudaStream_t s, void** dev)
+{
+  staging_slot& sl = ctx->slots[slot];
+  if (sl.pending) {
+    if (int rc = check_cuda(ctx, cudaEventSynchronize(sl.ev), "cudaEventSynchronize(staging)")) {
+      return rc;
+    }
+    sl.pending = false;
+  }
+  if (sl.ev == nullptr) {
+    if (int rc = check_cuda(ctx, cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming), "cudaEventCreate")) {
+      return rc;
+    }
+  }
+  if (bytes > sl.cap) {
+    cudaFree(sl.dev);
+    cudaFreeHost(sl.host);
+    sl.dev  = nullptr;
+    sl.host = nullptr;
+    sl.cap  = 0;
+    size_t cap = bytes < 4096 ? 4096 : bytes * 2;
+    if (int rc = check_cuda(ctx, cudaMalloc(&sl.dev, cap), "cudaMalloc(staging)")) {
+      return rc;
+    }
+    if (int rc = check_cuda(ctx, cudaMallocHost(&sl.host, cap), "cudaMallocHost(staging)")) {
+      return rc;
+    }
+    sl.cap = cap;
+  }
+  std::memcpy(sl.host, host, bytes);
+  if (int rc = check_cuda(ctx, cudaMemcpyAsync(sl.dev, sl.host, bytes, cudaMemcpyHostToDevice, s),
+                          "cudaMemcpyAsync(staging)")) {
+    return rc;
+  }
+  *dev = sl.dev;
+  return PG_OK;
+}
+
+int release_slot_after(pg_context* ctx, int slot, cudaStream_t s)
+{
+  staging_slot& sl = ctx->slots[slot];
+  if (int rc = check_cuda(ctx, cudaEventRecord(sl.ev, s), "cudaEventRecord(staging)")) {
+    return rc;
+  }
+  sl.pending = true;
+  return PG_OK;
+}
+
+void free_slots(pg_context* ctx)
+{
+  for (auto& sl : ctx->slots) {
+    if (sl.pending && sl.ev) {
+      cudaEventSynchronize(sl.ev);
+    }
+    cudaFree(sl.dev);
+    if (sl.host) {
+      cudaFreeHost(sl.host);
+    }
+    if (sl.ev) {
+      cudaEventDestroy(sl.ev);
+    }
+    sl = staging_slot();
+  }
+}
+
+// Device scratch that grows on demand (owned by the context).
+int ensure_scratch(pg_context* ctx, void** buf, size_t* cap, size_t bytes, const char* what)
+{
+  if (bytes <= *cap) {
+    return PG_OK;
+  }
+  cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  if (int rc = check_cuda(ctx, cudaMalloc(buf, bytes), what)) {
+    return rc;
+  }
+  *cap = bytes;
+  return PG_OK;
+}
+
 } // namespace pg
 
 using namespace pg;
@@ -248,6 +311,17 @@ int pg_create(const pg_config* cfg, pg_context** out)
     }
   }
   if (rc == PG_OK) {
+    std::vector<uint32_t> tabs(3 * 3072);
+    crc_tables_host(tabs.data());
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.crc_tabs, tabs.size() * sizeof(uint32_t)), "cudaMalloc(crc tables)");
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx,
+                      cudaMemcpy(ctx->dev.crc_tabs, tabs.data(), tabs.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice),
+                      "cudaMemcpy(crc tables)");
+    }
+  }
+  if (rc == PG_OK) {
     rc = ldpc_upload_tables(ctx);
   }
   if (rc == PG_OK && cfg->max_llrs > 0) {
@@ -274,6 +348,10 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.c2v);
   cudaFree(ctx->dev.descs);
   cudaFree(ctx->dev.crc_pow);
+  cudaFree(ctx->dev.crc_tabs);
+  cudaFree(ctx->scratch_a);
+  cudaFree(ctx->scratch_b);
+  free_slots(ctx);
   cudaFree(ctx->dev.llrs);
   cudaFree(ctx->dev.bits);
   cudaFree(ctx->dev.iterations);

@@ -26,13 +26,36 @@ inline int nshort_of(int bg) { return bg == 1 ? 66 : 50; }
 // Lifting-size set index (TS 38.212 Table 5.3.2-1), -1 when Z is not a lifting size.
 int lifting_set_index(int Z);
 
-// Polynomial and order of a pg_crc_poly.
-void crc_poly_params(int poly, uint32_t* g, int* order);
+// Polynomial (with its x^order term) and order of a pg_crc_poly (TS 38.212 Section 5.1).
+__host__ __device__ inline void crc_poly_params(int poly, uint32_t* g, int* order)
+{
+  if (poly == PG_CRC16) {
+    *g     = 0x11021u;
+    *order = 16;
+  } else if (poly == PG_CRC24A) {
+    *g     = 0x1864cfbu;
+    *order = 24;
+  } else {
+    *g     = 0x1800063u;
+    *order = 24;
+  }
+}
+
+// Host-to-device staging of one kind of descriptor list: pinned host copy, device copy and the
+// event after which both may be reused (the last kernel that read them has completed).
+struct staging_slot {
+  void*       dev     = nullptr;
+  void*       host    = nullptr;
+  size_t      cap     = 0;
+  cudaEvent_t ev      = nullptr;
+  bool        pending = false;
+};
 
 struct device_buffers {
   int8_t*      c2v         = nullptr; // max_codeblocks * kC2vStride check-to-variable messages
   pg_ldpc_cb*  descs       = nullptr; // staged descriptors
   uint32_t*    crc_pow     = nullptr; // [3][kCrcPowLen]
+  uint32_t*    crc_tabs    = nullptr; // [3][1024 + 2048]: x^k and x^(1024k) mod g
   int8_t*      llrs        = nullptr; // staging for _host calls
   uint8_t*     bits        = nullptr;
   int32_t*     iterations  = nullptr;
@@ -55,6 +78,11 @@ struct pg_context {
   cudaEvent_t         ev_stop        = nullptr;
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
+  pg::staging_slot    slots[4];                  // rate-dematch, CRC, TB and PUSCH work lists
+  void*               scratch_a      = nullptr;  // growable device scratch of the _host entries
+  size_t              scratch_a_cap  = 0;
+  void*               scratch_b      = nullptr;
+  size_t              scratch_b_cap  = 0;
   bool                timed          = false;
   std::string         last_error;
 };
@@ -69,6 +97,25 @@ int validate_ldpc_descs(pg_context* ctx, const pg_ldpc_cb* cbs, int n, size_t no
 
 // Uploads the constant base-graph tables (once per process and device).
 int ldpc_upload_tables(pg_context* ctx);
+
+enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3 };
+
+// Copies `bytes` of host descriptors to the slot's device buffer on stream s (growing it when
+// needed); returns the device pointer in *dev. release_slot_after marks the slot busy until the
+// work enqueued on s so far has completed.
+int stage_slot(pg_context* ctx, int slot, const void* host, size_t bytes, cudaStream_t s, void** dev);
+int release_slot_after(pg_context* ctx, int slot, cudaStream_t s);
+void free_slots(pg_context* ctx);
+int ensure_scratch(pg_context* ctx, void** buf, size_t* cap, size_t bytes, const char* what);
+
+int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_total, size_t out_total);
+int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
+                        cudaStream_t stream);
+void crc_tables_host(uint32_t* tab);
+int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8_t* data, uint32_t* out,
+               cudaStream_t stream);
+int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const uint8_t* cb_bits,
+                       const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream);
 
 // Enqueues the batched decoder; descs_dev holds n descriptors in device memory.
 int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,

@@ -1,0 +1,138 @@
+// Batched LDPC rate dematching (TS 38.212 Section 5.4.2), bit-exact with the reference's
+// ldpc_rate_dematcher (lib/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher_impl.cpp:29-250) on
+// finite LLRs.
+//
+// The reference walks the E received LLRs sequentially through the circular buffer: bit
+// de-interleaving (out[K*j + i] = in[i*Qm + j]), then placement from k0 onward, skipping the
+// filler positions, wrapping at N_cb and combining wrapped values with the saturating LLR sum.
+// Here every output position is computed independently: the valid (non-filler) positions form a
+// cycle of length V = N_cb - F; position p with valid index v receives the de-interleaved inputs
+// t = (v - v0) mod V, t + V, t + 2V, ... < E, summed in that order onto 0 (new data) or onto the
+// previous buffer content (soft combining). Filler positions hold +127; positions at or beyond N_cb
+// are zeroed on new data and untouched otherwise. One CTA per codeblock, threads stride the
+// N output positions (coalesced stores).
+#include "pg_internal.h"
+
+namespace {
+
+constexpr int kRmThreads = 256;
+
+__device__ __forceinline__ int llr_sum(int a, int b)
+{
+  // log_likelihood_ratio::operator+ (lib/phy/upper/log_likelihood_ratio.cpp:21-53).
+  if (a == -b) {
+    return 0;
+  }
+  if (a == 127 || a == -127) {
+    return a;
+  }
+  if (b == 127 || b == -127) {
+    return b;
+  }
+  return max(-120, min(120, a + b));
+}
+
+__global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb* __restrict__ cbs,
+                                                                  const int8_t* __restrict__ in_all,
+                                                                  int8_t* __restrict__ out_all)
+{
+  const pg_rm_cb d   = cbs[blockIdx.x];
+  const int      bg  = d.base_graph;
+  const int      Z   = d.lifting_size;
+  const int      Kb  = bg == 1 ? 22 : 10;
+  const int      N   = (bg == 1 ? 66 : 50) * Z;
+  const int      Ncb = (d.nref > 0 && (int)d.nref < N) ? (int)d.nref : N;
+  const int      F   = d.nof_filler_bits;
+  const int      sys = (Kb - 2) * Z;
+  const int      inf = sys - F;
+  const int      E   = (int)d.rm_length;
+  const int      Qm  = d.modulation_order;
+  const int      Kq  = E / Qm;
+  const int      sh  = bg == 1 ? (d.rv == 0 ? 0 : d.rv == 1 ? 17 : d.rv == 2 ? 33 : 56)
+                               : (d.rv == 0 ? 0 : d.rv == 1 ? 13 : d.rv == 2 ? 25 : 43);
+  const int      k0  = (int)(((long long)sh * Ncb) / N) * Z;
+  const int      V   = Ncb - F;
+  const int      v0  = k0 < inf ? k0 : (k0 < sys ? inf : k0 - F);
+  const int8_t*  in  = in_all + d.in_offset;
+  int8_t*        out = out_all + d.out_offset;
+  const bool     nd  = d.new_data != 0;
+
+  for (int p = threadIdx.x; p < N; p += kRmThreads) {
+    if (p >= inf && p < sys) {
+      out[p] = 127;
+      continue;
+    }
+    if (p >= Ncb) {
+      if (nd) {
+        out[p] = 0;
+      }
+      continue;
+    }
+    const int v   = p < inf ? p : p - F;
+    int       t   = v - v0;
+    t             = t < 0 ? t + V : t;
+    int       acc = nd ? 0 : (int)out[p];
+    for (; t < E; t += V) {
+      const int src = (Qm > 1) ? (t % Kq) * Qm + t / Kq : t;
+      acc           = llr_sum(acc, in[src]);
+    }
+    out[p] = (int8_t)acc;
+  }
+}
+
+} // namespace
+
+namespace pg {
+
+int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_total, size_t out_total)
+{
+  if (n < 0 || (n > 0 && cbs == nullptr)) {
+    return set_error(ctx, PG_ERR_INVALID, "invalid codeblock list");
+  }
+  if (n > ctx->max_codeblocks) {
+    return set_error(ctx, PG_ERR_CAPACITY, "rate-dematch batch exceeds max_codeblocks");
+  }
+  for (int i = 0; i < n; ++i) {
+    const pg_rm_cb& d = cbs[i];
+    char            buf[160];
+    const int       qm = d.modulation_order;
+    if ((d.base_graph != 1 && d.base_graph != 2) || lifting_set_index(d.lifting_size) < 0 || d.rv > 3 ||
+        !(qm == 1 || qm == 2 || qm == 4 || qm == 6 || qm == 8)) {
+      snprintf(buf, sizeof(buf), "codeblock %d: invalid base graph, lifting size, rv or modulation", i);
+      return set_error(ctx, PG_ERR_INVALID, buf);
+    }
+    const int Z   = d.lifting_size;
+    const int N   = nshort_of(d.base_graph) * Z;
+    const int sys = (kb_of(d.base_graph) - 2) * Z;
+    const int Ncb = (d.nref > 0 && (int)d.nref < N) ? (int)d.nref : N;
+    if ((int)d.nof_filler_bits >= sys || Ncb <= sys) {
+      snprintf(buf, sizeof(buf), "codeblock %d: filler bits or N_ref out of range", i);
+      return set_error(ctx, PG_ERR_INVALID, buf);
+    }
+    if (d.rm_length % qm != 0) {
+      snprintf(buf, sizeof(buf), "codeblock %d: E=%u not a multiple of Qm=%d", i, d.rm_length, qm);
+      return set_error(ctx, PG_ERR_INVALID, buf);
+    }
+    if (in_total != 0 && (size_t)d.in_offset + d.rm_length > in_total) {
+      snprintf(buf, sizeof(buf), "codeblock %d: input beyond the buffer", i);
+      return set_error(ctx, PG_ERR_INVALID, buf);
+    }
+    if (out_total != 0 && (size_t)d.out_offset + (size_t)N > out_total) {
+      snprintf(buf, sizeof(buf), "codeblock %d: output beyond the buffer", i);
+      return set_error(ctx, PG_ERR_INVALID, buf);
+    }
+  }
+  return PG_OK;
+}
+
+int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
+                        cudaStream_t stream)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  rate_dematch_kernel<<<n, kRmThreads, 0, stream>>>(descs_dev, in, out);
+  return check_cuda(ctx, cudaGetLastError(), "rate_dematch_kernel launch");
+}
+
+} // namespace pg

@@ -38,6 +38,42 @@ class PgLdpcCb(ctypes.Structure):
 
 assert ctypes.sizeof(PgLdpcCb) == 20
 
+
+class PgRmCb(ctypes.Structure):
+    _fields_ = [("in_offset", ctypes.c_uint32), ("rm_length", ctypes.c_uint32), ("out_offset", ctypes.c_uint32),
+                ("nref", ctypes.c_uint32), ("lifting_size", ctypes.c_uint16), ("nof_filler_bits", ctypes.c_uint16),
+                ("base_graph", ctypes.c_uint8), ("rv", ctypes.c_uint8), ("modulation_order", ctypes.c_uint8),
+                ("new_data", ctypes.c_uint8)]
+
+
+class PgCrcItem(ctypes.Structure):
+    _fields_ = [("bit_offset", ctypes.c_uint32), ("nof_bits", ctypes.c_uint32), ("poly", ctypes.c_uint32)]
+
+
+class PgTbDesc(ctypes.Structure):
+    _fields_ = [("cb_first", ctypes.c_uint32), ("nof_cbs", ctypes.c_uint32), ("cb_payload_bits", ctypes.c_uint32),
+                ("tbs_bits", ctypes.c_uint32), ("tb_out_offset", ctypes.c_uint32), ("crc_poly", ctypes.c_uint32)]
+
+
+class PgSchSegmentation(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("nof_cbs", "lifting_size", "cb_length", "nof_filler_bits",
+                                                "cb_crc_bits", "tb_crc_bits", "nof_short_cbs", "e_short", "e_long")]
+
+
+class PgSchTb(ctypes.Structure):
+    _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_ch_symbols", ctypes.c_uint32), ("tbs_bits", ctypes.c_uint32),
+                ("tb_out_offset", ctypes.c_uint32), ("nref", ctypes.c_uint32), ("base_graph", ctypes.c_uint8),
+                ("modulation_order", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8), ("rv", ctypes.c_uint8),
+                ("max_iterations", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3)]
+
+
+class PgSchResult(ctypes.Structure):
+    _fields_ = [("tb_crc_ok", ctypes.c_uint32), ("nof_cbs", ctypes.c_uint32), ("nof_cbs_crc_ok", ctypes.c_uint32),
+                ("mean_iterations", ctypes.c_float), ("max_iterations_run", ctypes.c_uint32)]
+
+
+assert ctypes.sizeof(PgRmCb) == 24 and ctypes.sizeof(PgSchTb) == 28 and ctypes.sizeof(PgTbDesc) == 24
+
 # Every symbol the public header declares, with (restype, argtypes).
 _VP = ctypes.c_void_p
 SIGNATURES = {
@@ -51,6 +87,15 @@ SIGNATURES = {
                                                  ctypes.c_size_t, _VP]),
     "pg_ldpc_output_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
     "pg_set_kernel_timing": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "pg_rate_dematch_batch_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP]),
+    "pg_rate_dematch_batch_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t]),
+    "pg_crc_calculate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP]),
+    "pg_crc_calculate_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP]),
+    "pg_tb_assemble_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_sch_segment": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint32,
+                                      ctypes.POINTER(PgSchSegmentation)]),
+    "pg_sch_decode_batch_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t,
+                                                _VP]),
     "pg_last_kernel_ms": (ctypes.c_float, [_VP]),
 }
 

@@ -165,3 +165,54 @@ def attach_crc(poly, bits):
     sh = np.arange(order - 1, -1, -1, dtype=np.uint32)
     tail = ((r[..., None] >> sh) & 1).astype(np.uint8)
     return np.concatenate([np.asarray(bits, np.uint8), tail], axis=-1)
+
+
+def rate_match(bg, z, cw, e, rv=0, qm=2, nref=0, nof_filler_bits=0):
+    """TS 38.212 Section 5.4.2: bit selection from the circular buffer (filler bits skipped) and
+    bit interleaving. cw[..., N_short*Z] -> [..., E]."""
+    cw = np.asarray(cw, np.uint8)
+    kb = 22 if bg == 1 else 10
+    n = cw.shape[-1]
+    ncb = min(nref, n) if nref > 0 else n
+    sys_bits = (kb - 2) * z
+    info = sys_bits - nof_filler_bits
+    shift = (0, 17, 33, 56)[rv] if bg == 1 else (0, 13, 25, 43)[rv]
+    k0 = (shift * ncb // n) * z
+    valid = np.concatenate([np.arange(0, info), np.arange(sys_bits, ncb)])
+    # Rotate the valid positions to start at k0 (or at the first valid position after it).
+    start = np.searchsorted(valid, k0)
+    order = np.roll(valid, -start)
+    idx = order[np.arange(e) % order.size]
+    sel = cw[..., idx]
+    if qm > 1:
+        kq = e // qm
+        sel = sel.reshape(sel.shape[:-1] + (qm, kq)).swapaxes(-1, -2).reshape(sel.shape)
+    return sel
+
+
+def ulsch_encode(tb_bits, bg, qm, nof_layers, nof_ch_symbols, seg, rv=0, nref=0):
+    """Transport block bits -> codeword bits (G = nof_ch_symbols * Qm): TB CRC, code block
+    segmentation with CB CRC24B, filler bits, LDPC encoding and rate matching (TS 38.212
+    Sections 5.1-5.4, 6.2). seg is the segmentation dictionary (pusch_b200.sch.segment)."""
+    tb_bits = np.asarray(tb_bits, np.uint8)
+    tbs = tb_bits.size
+    b = attach_crc(0 if tbs <= 3824 else 1, tb_bits)
+    c = seg["nof_cbs"]
+    z = seg["lifting_size"]
+    k = seg["cb_length"]
+    f = seg["nof_filler_bits"]
+    if c > 1:
+        parts = b.reshape(c, -1)
+        cbs = attach_crc(2, parts)
+    else:
+        cbs = b.reshape(1, -1)
+    msgs = np.concatenate([cbs, np.zeros((c, f), np.uint8)], axis=1)
+    assert msgs.shape[1] == k
+    cws = ldpc_encode(bg, z, msgs)
+    out = []
+    for i in range(c):
+        e = seg["e_short"] if i < seg["nof_short_cbs"] else seg["e_long"]
+        out.append(rate_match(bg, z, cws[i], e, rv=rv, qm=qm, nref=nref, nof_filler_bits=f))
+    g = np.concatenate(out)
+    assert g.size == nof_ch_symbols * qm
+    return g
