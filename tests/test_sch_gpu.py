@@ -106,7 +106,7 @@ def oracle_tb_decode(port, llr, tbs, bg, qm, seg, max_iter, rv=0):
     (417976, 1, 8, 2, 2 * 12 * 3276, 14.0),
     (1320, 2, 4, 1, 600, 3.0),
     (3840, 2, 6, 2, 2400, None),
-    (40000, 1, 4, 2, 21000, 2.0),
+    (40016, 1, 4, 2, 21000, 2.0),
 ])
 def test_sch_decode_matches_oracle(ctx, port, tbs, bg, qm, nl, nsym, snr):
     rng = np.random.default_rng(tbs + qm)
@@ -127,7 +127,7 @@ def test_sch_decode_matches_oracle(ctx, port, tbs, bg, qm, nl, nsym, snr):
 def test_sch_decode_batch_mixed(ctx):
     rng = np.random.default_rng(9)
     jobs, truth = [], []
-    for tbs, bg, qm, nl, nsym in [(5888, 1, 2, 1, 13 * 612), (1320, 2, 4, 1, 600), (100000, 1, 6, 2, 40000),
+    for tbs, bg, qm, nl, nsym in [(5888, 1, 2, 1, 13 * 612), (1320, 2, 4, 1, 600), (100008, 1, 6, 2, 40000),
                                   (3840, 2, 6, 2, 2400), (24, 2, 2, 1, 48)]:
         tb, llr, _ = make_tb(rng, tbs, bg, qm, nl, nsym, None)
         jobs.append(SchTransportBlock(llr, tbs, bg, qm, nl))
