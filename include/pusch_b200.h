@@ -235,6 +235,34 @@ typedef struct pg_sch_result {
 int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* llrs,
                              size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
 
+/* ---------------------------------------------------------------------------------------- */
+/* Equalisation and soft demapping                                                           */
+
+enum pg_eq_algorithm { PG_EQ_ZF = 0, PG_EQ_MMSE = 1 };
+
+/* Channel equalisation, replacing channel_equalizer::equalize
+ * (include/ocudu/phy/upper/equalization/channel_equalizer.h:71-76;
+ * lib/phy/upper/equalization/channel_equalizer_generic_impl.cpp:511-653).
+ * ch_symbols: complex bf16 (cbf16_t, real in the low 16 bits) [port][re];
+ * ch_estimates: complex bf16 [port][layer][re]; noise_var_per_port: host array of nof_ports;
+ * outputs layer-interleaved: eq_symbols complex float [re][layer], eq_noise_vars [re][layer].
+ * One layer uses the per-port reduction (ZF and MMSE alike, as the reference); two and four
+ * layers use MMSE with the largest port noise variance. */
+int pg_equalize_device(pg_context* ctx, int algorithm, int nof_re, int nof_ports, int nof_layers,
+                       const uint32_t* ch_symbols, const uint32_t* ch_estimates, const float* noise_var_per_port,
+                       float tx_scaling, float* eq_symbols, float* eq_noise_vars, void* stream);
+int pg_equalize_host(pg_context* ctx, int algorithm, int nof_re, int nof_ports, int nof_layers,
+                     const uint32_t* ch_symbols, const uint32_t* ch_estimates, const float* noise_var_per_port,
+                     float tx_scaling, float* eq_symbols, float* eq_noise_vars);
+
+/* Soft demapping to int8 LLRs, replacing demodulation_mapper::demodulate_soft
+ * (include/ocudu/phy/upper/channel_modulation/demodulation_mapper.h:48-51). symbols: complex
+ * float; noise_vars: one per symbol; llrs: modulation_order per symbol (2, 4, 6 or 8). */
+int pg_demodulate_soft_device(pg_context* ctx, int modulation_order, int nof_symbols, const float* symbols,
+                              const float* noise_vars, int8_t* llrs, void* stream);
+int pg_demodulate_soft_host(pg_context* ctx, int modulation_order, int nof_symbols, const float* symbols,
+                            const float* noise_vars, int8_t* llrs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -117,6 +117,11 @@ int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8
 int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const uint8_t* cb_bits,
                        const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream);
 
+int demap_upload_tables(pg_context* ctx);
+int equalize_launch(pg_context* ctx, int nof_re, int nof_ports, int nof_layers, const uint32_t* y, const uint32_t* h,
+                    const float* nvar_port_host, float tx, float2* out, float* out_var, cudaStream_t s);
+int demap_launch(pg_context* ctx, int qm, int n, const float2* sym, const float* nvar, int8_t* llr, cudaStream_t s);
+
 // Enqueues the batched decoder; descs_dev holds n descriptors in device memory.
 int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                 int32_t* iterations, cudaStream_t stream);

@@ -97,6 +97,12 @@ SIGNATURES = {
     "pg_sch_decode_batch_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t,
                                                 _VP]),
     "pg_last_kernel_ms": (ctypes.c_float, [_VP]),
+    "pg_equalize_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,
+                                          ctypes.c_float, _VP, _VP, _VP]),
+    "pg_equalize_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP,
+                                        ctypes.c_float, _VP, _VP]),
+    "pg_demodulate_soft_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_demodulate_soft_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
 }
 
 _lib = None

@@ -55,6 +55,8 @@ class Ref:
         lib.ref_ldpc_decode_batch_mt.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         lib.ref_ldpc_decode_batch_mt.restype = ctypes.c_double
+        lib.ref_equalize.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_float, ctypes.c_void_p,
+                                                                                   ctypes.c_void_p]
         self.lib = lib
         self.variant = lib.ref_ldpc_auto_variant().decode()
 
@@ -114,6 +116,19 @@ class Ref:
         self.lib.ref_demodulate_soft(qm, _ptr(sym), _ptr(nv), sym.size, _ptr(out))
         return out
 
+    def equalize(self, algorithm, ch_symbols, ch_estimates, noise_var_per_port, tx_scaling=1.0):
+        """ch_symbols uint32 cbf16 [port][re], ch_estimates uint32 cbf16 [port][layer][re]."""
+        y = np.ascontiguousarray(ch_symbols, np.uint32)
+        h = np.ascontiguousarray(ch_estimates, np.uint32)
+        nports, nre = y.shape
+        nl = h.shape[1]
+        nv = np.ascontiguousarray(noise_var_per_port, np.float32)
+        eq = np.zeros((nre, nl), np.complex64)
+        var = np.zeros((nre, nl), np.float32)
+        self.lib.ref_equalize(algorithm, nre, nports, nl, _ptr(y), _ptr(h), _ptr(nv), ctypes.c_float(tx_scaling),
+                              _ptr(eq), _ptr(var))
+        return eq, var
+
     def sch_segmentation(self, tbs_bits, bg):
         o = np.zeros(4, np.int32)
         self.lib.ref_sch_segmentation(tbs_bits, bg, _ptr(o))
@@ -133,7 +148,16 @@ class Port:
         lib.pgo_ldpc_decode.restype = ctypes.c_int
         lib.pgo_rate_dematch.argtypes = [ctypes.c_int] * 7 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
         lib.pgo_ldpc_edge_shift.argtypes = [ctypes.c_int] * 3
+        lib.pgo_demodulate_soft.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p]
         self.lib = lib
+
+    def demodulate_soft(self, qm, symbols, noise_vars):
+        sym = np.ascontiguousarray(symbols, dtype=np.complex64)
+        nv = np.ascontiguousarray(noise_vars, dtype=np.float32)
+        out = np.zeros(sym.size * qm, np.int8)
+        self.lib.pgo_demodulate_soft(qm, _ptr(sym), _ptr(nv), sym.size, _ptr(out))
+        return out
 
     def crc(self, poly, bits):
         bits = np.ascontiguousarray(bits, dtype=np.uint8)

@@ -7,6 +7,7 @@
  */
 #include "pusch_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -375,4 +376,95 @@ void pgo_rate_dematch(int bg, int Z, int rv, int qm, int Nref, int nof_filler_bi
     fill(out + Ncb, N - Ncb, 0);
   }
   free(aux);
+}
+
+/* ------------------------------------------------------------------------------------------ */
+/* Soft demapping: lib/phy/upper/channel_modulation/demodulation_mapper_{qpsk,qam16,qam64,     */
+/* qam256}.cpp (AVX2 kernels) and avx2_helpers.h:103-253 (quantize_ps: scale by 120/R, clip,   */
+/* round to nearest even). The 64/256-QAM pieces are the max-log LLRs of the TS 38.211 Gray    */
+/* mapping, computed here per call from the constellation.                                   */
+
+static float rcp_noise(float n)
+{
+  return (n > 0.f) ? 1.0f / n : 0.0f;
+}
+
+static int8_t quantize_rne(float v, float scale)
+{
+  v = v * scale;
+  if (v != v) {
+    return 0;
+  }
+  if (v > 120.f) v = 120.f;
+  if (v < -120.f) v = -120.f;
+  return (int8_t)lrintf(v); /* default rounding mode: nearest, ties to even */
+}
+
+static int level_of(int code, int m)
+{
+  int t = 1;
+  for (int k = m - 1; k >= 1; --k) {
+    int bk = (code >> (m - 1 - k)) & 1;
+    t      = (1 << (m - k)) - (1 - 2 * bk) * t;
+  }
+  return (1 - 2 * ((code >> (m - 1)) & 1)) * t;
+}
+
+/* Max-log LLR (times noise) of dimension bit k for component x, in units of 1/sqrt(E). */
+static float maxlog_piece(float x, int m, int k, float unit, float energy)
+{
+  int   nlev = 1 << m;
+  float w    = 2.0f * unit;
+  int   idx  = (int)floorf(x / w) + nlev / 2;
+  if (idx < 0) idx = 0;
+  if (idx > nlev - 1) idx = nlev - 1;
+  double xm    = (idx - nlev / 2) * 2 + 1;
+  double best0 = 1e30, best1 = 1e30;
+  int    s0 = 0, s1 = 0;
+  for (int c = 0; c < nlev; ++c) {
+    int    bk = (c >> (m - 1 - k)) & 1;
+    int    l  = level_of(c, m);
+    double d  = (xm - l) * (xm - l);
+    if (bk == 0 && d < best0) { best0 = d; s0 = l; }
+    if (bk == 1 && d < best1) { best1 = d; s1 = l; }
+  }
+  float slope     = (float)(2 * (s0 - s1)) * unit;
+  float intercept = (float)(s1 * s1 - s0 * s0) / energy;
+  return slope * x + intercept;
+}
+
+void pgo_demodulate_soft(int qm, const float* symbols, const float* noise_vars, int nof_symbols, int8_t* llrs)
+{
+  for (int i = 0; i < nof_symbols; ++i) {
+    float  x[2] = {symbols[2 * i], symbols[2 * i + 1]};
+    float  rcp  = rcp_noise(noise_vars[i]);
+    int8_t* out = llrs + (size_t)i * qm;
+    if (qm == 2) {
+      float g = 2.0f * sqrtf(2.0f);
+      out[0]  = quantize_rne((g * x[0]) * rcp, 120.f / 24.f);
+      out[1]  = quantize_rne((g * x[1]) * rcp, 120.f / 24.f);
+    } else if (qm == 4) {
+      float s10 = 1.0f / sqrtf(10.0f);
+      for (int c = 0; c < 2; ++c) {
+        float first  = (4.0f * s10) * x[c];
+        float second = 2.0f * first - copysignf(0.8f, x[c]);
+        float v01    = fabsf(x[c]) > 2.0f * s10 ? second : first;
+        float v23    = 0.8f - fabsf(first);
+        int   z      = fabsf(x[c]) <= 1e-9f;
+        out[c]       = quantize_rne(z ? 0.f : v01 * rcp, 6.0f);
+        out[2 + c]   = quantize_rne(z ? 0.f : v23 * rcp, 6.0f);
+      }
+    } else {
+      int   m      = qm / 2;
+      float energy = qm == 6 ? 42.f : 170.f;
+      float unit   = 1.0f / sqrtf(energy);
+      for (int c = 0; c < 2; ++c) {
+        int z = fabsf(x[c]) <= 1e-9f;
+        for (int k = 0; k < m; ++k) {
+          float v        = maxlog_piece(x[c], m, k, unit, energy) * rcp;
+          out[2 * k + c] = quantize_rne(z ? 0.f : v, 6.0f);
+        }
+      }
+    }
+  }
 }

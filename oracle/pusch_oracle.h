@@ -33,6 +33,11 @@ int pgo_ldpc_decode(int bg, int Z, int nof_filler_bits, int crc_poly, int max_it
 void pgo_rate_dematch(int bg, int Z, int rv, int qm, int Nref, int nof_filler_bits, int new_data, const int8_t* in,
                       int E, int8_t* out);
 
+/* Soft demapping (modulation order 2, 4, 6, 8) with the arithmetic of the reference's AVX2
+ * kernels: max-log LLR times 1/noise, scaled to +-120, round half to even. symbols are
+ * interleaved (re, im) floats. */
+void pgo_demodulate_soft(int qm, const float* symbols, const float* noise_vars, int nof_symbols, int8_t* llrs);
+
 /* Saturating LLR sum with the reference's special cases. */
 int8_t pgo_llr_sum(int8_t a, int8_t b);
 

@@ -22,6 +22,9 @@
 #include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_tx.h"
 #include "ocudu/phy/upper/channel_modulation/channel_modulation_factories.h"
 #include "ocudu/phy/upper/channel_modulation/demodulation_mapper.h"
+#include "ocudu/phy/support/re_buffer.h"
+#include "ocudu/phy/upper/equalization/dynamic_ch_est_list.h"
+#include "ocudu/phy/upper/equalization/equalization_factories.h"
 #include "ocudu/ran/sch/sch_segmentation.h"
 #include "lib/phy/upper/channel_coding/ldpc/ldpc_graph_impl.h"
 #include <cstring>
@@ -382,6 +385,42 @@ double ref_ldpc_decode_batch_mt(const char*    variant,
     th.join();
   }
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+/// Channel equalisation with the reference's generic equaliser
+/// (channel_equalizer::equalize, include/ocudu/phy/upper/equalization/channel_equalizer.h:71-76).
+/// algorithm: 0 = ZF, 1 = MMSE. ch_symbols: cbf16 [port][re] as uint32 (real in the low half);
+/// ch_estimates: cbf16 [port][layer][re]; outputs layer-interleaved [re][layer].
+int ref_equalize(int             algorithm,
+                 int             nof_re,
+                 int             nof_ports,
+                 int             nof_layers,
+                 const uint32_t* ch_symbols,
+                 const uint32_t* ch_estimates,
+                 const float*    noise_var_per_port,
+                 float           tx_scaling,
+                 float*          eq_symbols,
+                 float*          eq_noise_vars)
+{
+  auto factory = create_channel_equalizer_generic_factory(algorithm == 0 ? channel_equalizer_algorithm_type::zf
+                                                                         : channel_equalizer_algorithm_type::mmse);
+  auto eq      = factory->create();
+  dynamic_re_buffer<cbf16_t> syms(nof_ports, nof_re);
+  dynamic_ch_est_list        est(nof_re, nof_ports, nof_layers);
+  for (int p = 0; p < nof_ports; ++p) {
+    std::memcpy(syms.get_slice(p).data(), ch_symbols + (size_t)p * nof_re, (size_t)nof_re * 4);
+    for (int l = 0; l < nof_layers; ++l) {
+      std::memcpy(est.get_channel(p, l).data(), ch_estimates + ((size_t)p * nof_layers + l) * nof_re,
+                  (size_t)nof_re * 4);
+    }
+  }
+  eq->equalize(span<cf_t>(reinterpret_cast<cf_t*>(eq_symbols), (size_t)nof_re * nof_layers),
+               span<float>(eq_noise_vars, (size_t)nof_re * nof_layers),
+               syms,
+               est,
+               span<const float>(noise_var_per_port, nof_ports),
+               tx_scaling);
+  return 0;
 }
 
 } // extern "C"

@@ -145,6 +145,51 @@ def enc_cases(ref, rng):
                 cws=np.concatenate(cws))
 
 
+def to_cbf16(x):
+    x = np.ascontiguousarray(x, np.complex64)
+    u = x.view(np.float32).reshape(x.shape + (2,)).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) & 0xFFFF
+    return (r[..., 0] | (r[..., 1] << 16)).astype(np.uint32)
+
+
+def demap_cases(ref, rng):
+    meta, syms, nvs, llrs = [], [], [], []
+    for qm in (2, 4, 6, 8):
+        n = 3000
+        s = ((rng.standard_normal(n) + 1j * rng.standard_normal(n)) * rng.uniform(0.2, 1.2)).astype(np.complex64)
+        s[:8] = 0
+        s[8:16] = 1e-10
+        nv = rng.uniform(1e-3, 1.0, n).astype(np.float32)
+        nv[16:20] = 0
+        nv[20] = np.inf
+        meta.append([qm, n])
+        syms.append(s)
+        nvs.append(nv)
+        llrs.append(ref.demodulate_soft(qm, s, nv))
+    return dict(meta=np.array(meta, np.int32), symbols=np.concatenate(syms), noise=np.concatenate(nvs),
+                llrs=np.concatenate(llrs))
+
+
+def eq_cases(ref, rng):
+    out = {}
+    for idx, (alg, p, l, nre) in enumerate([(1, 2, 1, 612), (1, 4, 1, 600), (1, 4, 2, 3276), (1, 2, 2, 500),
+                                           (0, 2, 1, 300), (1, 8, 2, 256), (1, 4, 4, 256)]):
+        y = to_cbf16((rng.standard_normal((p, nre)) + 1j * rng.standard_normal((p, nre))) / np.sqrt(2))
+        h = to_cbf16((rng.standard_normal((p, l, nre)) + 1j * rng.standard_normal((p, l, nre))) / np.sqrt(2))
+        h[:, :, :3] = 0  # zero channel: (0, inf) outputs
+        nv = rng.uniform(0.01, 0.3, p).astype(np.float32)
+        tx = float(rng.choice([1.0, 0.7071]))
+        eq, var = ref.equalize(alg, y, h, nv, tx)
+        out[f"c{idx}_meta"] = np.array([alg, p, l, nre], np.int32)
+        out[f"c{idx}_y"] = y
+        out[f"c{idx}_h"] = h
+        out[f"c{idx}_nv"] = nv
+        out[f"c{idx}_tx"] = np.array([tx], np.float32)
+        out[f"c{idx}_eq"] = eq
+        out[f"c{idx}_var"] = var
+    return out
+
+
 def main():
     ref = Ref()
     rng = np.random.default_rng(20261203)
@@ -152,6 +197,8 @@ def main():
     np.savez_compressed(os.path.join(OUT, "rate_dematch.npz"), **rm_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "crc.npz"), **crc_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "ldpc_encode.npz"), **enc_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "demap.npz"), **demap_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "equalize.npz"), **eq_cases(ref, rng))
     print("golden fixtures written; reference LDPC variant:", ref.variant)
 
 

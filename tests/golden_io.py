@@ -48,3 +48,30 @@ def enc_cases():
 
 def kbits(bg, z):
     return (22 if bg == 1 else 10) * z
+
+
+def demap_cases():
+    d = load("demap.npz")
+    out, off = [], 0
+    for qm, n in d["meta"]:
+        qm, n = int(qm), int(n)
+        out.append(dict(qm=qm, symbols=d["symbols"][off:off + n], noise=d["noise"][off:off + n],
+                        llrs=d["llrs"][off * 0:0]))
+        off += n
+    loff = 0
+    for c in out:
+        n = c["symbols"].size
+        c["llrs"] = d["llrs"][loff:loff + n * c["qm"]]
+        loff += n * c["qm"]
+    return out
+
+
+def eq_cases():
+    d = load("equalize.npz")
+    out, i = [], 0
+    while f"c{i}_meta" in d:
+        alg, p, l, nre = (int(x) for x in d[f"c{i}_meta"])
+        out.append(dict(alg=alg, ports=p, layers=l, nre=nre, y=d[f"c{i}_y"], h=d[f"c{i}_h"], nv=d[f"c{i}_nv"],
+                        tx=float(d[f"c{i}_tx"][0]), eq=d[f"c{i}_eq"], var=d[f"c{i}_var"]))
+        i += 1
+    return out
