@@ -263,6 +263,89 @@ int pg_demodulate_soft_device(pg_context* ctx, int modulation_order, int nof_sym
 int pg_demodulate_soft_host(pg_context* ctx, int modulation_order, int nof_symbols, const float* symbols,
                             const float* noise_vars, int8_t* llrs);
 
+/* ---------------------------------------------------------------------------------------- */
+/* PUSCH slot processing: DM-RS channel estimation, demodulation, decoding                   */
+
+/* One UE's PUSCH PDU, the device work-list entry of the slot kernels (the fields of
+ * pusch_processor::pdu_t the receive path reads: include/ocudu/phy/upper/channel_processors/
+ * pusch/pusch_processor.h). DM-RS type 1, one CDM group (layers 0 and 1), two CDM groups without
+ * data (no data on DM-RS symbols), no frequency hopping, no transform precoding, no UCI. */
+typedef struct pg_pusch_ue {
+  uint32_t grid_offset;      /* element offset of the UE's cell grid: cbf16 [port][14][grid_nof_subc] */
+  uint32_t grid_nof_subc;    /* subcarriers of that grid (12 x carrier PRBs) */
+  uint32_t llr_offset;       /* first codeword LLR of this UE in the LLR buffer */
+  uint32_t est_offset;       /* first complex float of this UE's frequency response buffer */
+  uint32_t tbs_bits;         /* transport block size */
+  uint32_t tb_out_offset;    /* byte offset of the decoded TB */
+  uint32_t nref;             /* N_ref for limited-buffer rate matching, 0 = unlimited */
+  float    dmrs_scaling;     /* DM-RS amplitude relative to data (sqrt(2) for two CDM groups) */
+  uint16_t rb_start;
+  uint16_t nof_rb;
+  uint16_t dmrs_symbol_mask; /* bit s set: OFDM symbol s carries DM-RS */
+  uint16_t n_id;             /* DM-RS scrambling identity */
+  uint16_t rnti;
+  uint16_t n_id_data;        /* data scrambling identity */
+  int16_t  dc_subcarrier;    /* grid subcarrier of DC (its channel estimate is zeroed), -1 = none */
+  uint8_t  slot;             /* slot index within the frame */
+  uint8_t  n_scid;
+  uint8_t  first_symbol;
+  uint8_t  nof_symbols;
+  uint8_t  nof_rx_ports;     /* 1, 2 or 4 */
+  uint8_t  nof_layers;       /* 1 or 2 */
+  uint8_t  modulation_order; /* 2, 4, 6 or 8 */
+  uint8_t  base_graph;
+  uint8_t  rv;
+  uint8_t  max_iterations;
+} pg_pusch_ue;
+
+/* Per (UE, receive port) estimator outputs (port_channel_estimator_results,
+ * include/ocudu/phy/upper/signal_processors/channel_estimator/port_channel_estimator.h:107-139). */
+typedef struct pg_port_result {
+  float noise_var;
+  float epre;
+  float snr;
+  float rsrp[2];
+} pg_port_result;
+
+/* Complex floats of one UE's frequency-response buffer: ports x DM-RS symbols x layers x 12 nof_rb. */
+size_t pg_pusch_est_size(const pg_pusch_ue* ue);
+
+/* DM-RS channel estimation for every (UE, receive port), replacing
+ * port_channel_estimator::compute with FD "filter", TD "interpolate", no CFO compensation
+ * (lib/phy/upper/signal_processors/channel_estimator/port_channel_estimator_average_impl.cpp:322-557)
+ * and the pilot generation of dmrs_pusch_estimator_impl (dmrs_pusch_estimator_impl.cpp:69-169).
+ * Writes the FP32 frequency response at every DM-RS symbol (est, layout
+ * [port][dmrs symbol][layer][subcarrier]) and one pg_port_result per (UE, port), port-major per UE
+ * (results[u * 4 + port]). Device pointers. */
+int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids, float* est,
+                             pg_port_result* results, void* stream);
+
+/* Per-symbol channel estimates of one UE as the reference's
+ * port_channel_estimator_results::get_symbol_ch_estimate returns them: cbf16 [port][symbol][layer]
+ * [12 nof_rb] for symbols 0..13 (time interpolation between DM-RS symbols, rounded to bf16).
+ * Device pointers. */
+int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, uint32_t* out,
+                                     void* stream);
+
+/* Demodulation of every UE: per data RE the channel estimate of its OFDM symbol (time interpolation
+ * between DM-RS symbols, rounded to bf16, DC subcarrier zeroed), equalisation (one layer: MRC with
+ * per-port noise; two layers: MMSE with the largest port noise), soft demapping and descrambling
+ * (c_init = RNTI * 2^15 + n_ID_data), writing ue.llr_offset.. of llrs in codeword order. Replaces
+ * pusch_demodulator::demodulate (lib/phy/upper/channel_processors/pusch/pusch_demodulator_impl.cpp:254-461).
+ * Device pointers; est and port_results as written by pg_pusch_estimate_device. */
+int pg_pusch_demodulate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids,
+                               const float* est, const pg_port_result* port_results, int8_t* llrs, void* stream);
+
+/* Whole PUSCH receive path for a batch of UEs (any number of cells): H2D of the grids, channel
+ * estimation, demodulation, rate dematching, LDPC decoding, TB assembly and CRC, D2H of the TBs and
+ * results - pusch_processor::process for new transmissions without UCI
+ * (lib/phy/upper/channel_processors/pusch/pusch_processor_impl.cpp:349-900). The library assigns
+ * the est_offset and llr_offset fields; tb_out_offset, grid_offset/grid_nof_subc are the caller's.
+ * grids: host cbf16 words; port_results: nof_ues * 4 entries (may be NULL). */
+int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids,
+                          size_t grid_words, uint8_t* tb_out, size_t tb_out_len, pg_port_result* port_results,
+                          pg_sch_result* results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -330,7 +330,10 @@ int demap_upload_tables(pg_context* ctx)
       }
     }
   }
-  int rc = check_cuda(ctx, cudaMemcpyToSymbol(c_slope, slope, sizeof(slope)), "cudaMemcpyToSymbol(slope)");
+  int rc = demod_upload_tables(ctx, slope, intercept, width);
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_slope, slope, sizeof(slope)), "cudaMemcpyToSymbol(slope)");
+  }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyToSymbol(c_intercept, intercept, sizeof(intercept)), "cudaMemcpyToSymbol");
   }

@@ -327,6 +327,9 @@ int pg_create(const pg_config* cfg, pg_context** out)
   if (rc == PG_OK) {
     rc = demap_upload_tables(ctx);
   }
+  if (rc == PG_OK) {
+    rc = est_upload_tables(ctx);
+  }
   if (rc == PG_OK && cfg->max_llrs > 0) {
     rc = ensure_host_capacity(ctx, (size_t)cfg->max_llrs, (size_t)cfg->max_codeblocks * ((22 * kMaxZ) / 8));
   }
@@ -352,6 +355,7 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.descs);
   cudaFree(ctx->dev.crc_pow);
   cudaFree(ctx->dev.crc_tabs);
+  cudaFree(ctx->dev.gold);
   cudaFree(ctx->scratch_a);
   cudaFree(ctx->scratch_b);
   free_slots(ctx);

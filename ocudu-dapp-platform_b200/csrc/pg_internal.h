@@ -19,6 +19,7 @@ constexpr int kMaxNodes      = 68;  // BG1 variable nodes before shortening
 constexpr int kMaxRowDegree  = 19;
 constexpr int kCrcPowLen     = 22 * kMaxZ + 64;  // x^e mod g for every exponent a codeblock CRC needs
 constexpr int kC2vStride     = kBg1Edges * kMaxZ; // check-to-variable bytes per codeblock
+constexpr uint32_t kGoldWords = (14u * 3276u * 2u * 8u + 64u * 32u) / 32u + 2u; // Gold-sequence words per basis
 
 inline int kb_of(int bg) { return bg == 1 ? 22 : 10; }
 inline int nshort_of(int bg) { return bg == 1 ? 66 : 50; }
@@ -56,6 +57,7 @@ struct device_buffers {
   pg_ldpc_cb*  descs       = nullptr; // staged descriptors
   uint32_t*    crc_pow     = nullptr; // [3][kCrcPowLen]
   uint32_t*    crc_tabs    = nullptr; // [3][1024 + 2048]: x^k and x^(1024k) mod g
+  uint32_t*    gold        = nullptr; // [32][kGoldWords]: x1 and the 31 unit-state x2 sequences
   int8_t*      llrs        = nullptr; // staging for _host calls
   uint8_t*     bits        = nullptr;
   int32_t*     iterations  = nullptr;
@@ -78,7 +80,7 @@ struct pg_context {
   cudaEvent_t         ev_stop        = nullptr;
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
-  pg::staging_slot    slots[4];                  // rate-dematch, CRC, TB and PUSCH work lists
+  pg::staging_slot    slots[5];                  // rate-dematch, CRC, TB, PUSCH and UE work lists
   void*               scratch_a      = nullptr;  // growable device scratch of the _host entries
   size_t              scratch_a_cap  = 0;
   void*               scratch_b      = nullptr;
@@ -98,7 +100,7 @@ int validate_ldpc_descs(pg_context* ctx, const pg_ldpc_cb* cbs, int n, size_t no
 // Uploads the constant base-graph tables (once per process and device).
 int ldpc_upload_tables(pg_context* ctx);
 
-enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3 };
+enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4 };
 
 // Copies `bytes` of host descriptors to the slot's device buffer on stream s (growing it when
 // needed); returns the device pointer in *dev. release_slot_after marks the slot busy until the
@@ -118,6 +120,20 @@ int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const 
                        const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream);
 
 int demap_upload_tables(pg_context* ctx);
+int est_upload_tables(pg_context* ctx);
+int demod_upload_tables(pg_context* ctx, const void* slope, const void* intercept, const void* width);
+uint32_t ue_codeword_bits(const pg_pusch_ue& u);
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
+                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
+                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s);
+// Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
+// uses scratch_b; results and TB payloads land in host memory.
+int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
+                           size_t nof_llrs, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
+int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* grids, float* est,
+                    pg_port_result* results, cudaStream_t s);
+int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1);
 int equalize_launch(pg_context* ctx, int nof_re, int nof_ports, int nof_layers, const uint32_t* y, const uint32_t* h,
                     const float* nvar_port_host, float tx, float2* out, float* out_var, cudaStream_t s);
 int demap_launch(pg_context* ctx, int qm, int n, const float2* sym, const float* nvar, int8_t* llr, cudaStream_t s);

@@ -268,6 +268,31 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
   if (ctx == nullptr || nof_tbs < 0 || (nof_tbs > 0 && (tbs == nullptr || results == nullptr || llrs == nullptr))) {
     return ctx ? set_error(ctx, PG_ERR_INVALID, "invalid arguments") : PG_ERR_INVALID;
   }
+  if (nof_tbs == 0) {
+    return PG_OK;
+  }
+  if (int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice")) {
+    return rc;
+  }
+  if (int rc = ensure_scratch(ctx, &ctx->scratch_a, &ctx->scratch_a_cap, std::max<size_t>(nof_llrs_total, 256),
+                              "cudaMalloc(llrs)")) {
+    return rc;
+  }
+  if (int rc = check_cuda(ctx, cudaMemcpyAsync(ctx->scratch_a, llrs, nof_llrs_total, cudaMemcpyHostToDevice, ctx->stream),
+                          "cudaMemcpyAsync(llrs)")) {
+    return rc;
+  }
+  return sch_decode_device_llrs(ctx, tbs, nof_tbs, static_cast<const int8_t*>(ctx->scratch_a), nof_llrs_total, tb_out,
+                                tb_out_len, results);
+}
+
+} // extern "C"
+
+namespace pg {
+
+int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
+                           size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results)
+{
   // Work lists: one rate-dematch and one LDPC descriptor per codeblock, one TB descriptor per TB.
   std::vector<pg_rm_cb>   rm;
   std::vector<pg_ldpc_cb> ldpc;
@@ -347,9 +372,9 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
   if (nof_tbs == 0) {
     return PG_OK;
   }
-  // Device buffers: [llrs | rm buffers | cb bits | cb bit offsets | tb out | tb crc | iterations].
+  // Device buffers (scratch_b): [rm buffers | cb bits | cb bit offsets | tb out | tb crc | iterations].
   auto   al       = [](size_t x) { return (x + 255) & ~(size_t)255; };
-  size_t o_rm     = al(nof_llrs_total);
+  size_t o_rm     = 0;
   size_t o_bits   = o_rm + al(rm_total);
   size_t o_offs   = o_bits + al(bits_total);
   size_t o_tb     = o_offs + al((size_t)ncb * 4);
@@ -359,13 +384,12 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
   cudaStream_t s  = ctx->stream;
   int          rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   if (rc == PG_OK) {
-    rc = ensure_scratch(ctx, &ctx->scratch_a, &ctx->scratch_a_cap, total, "cudaMalloc(sch scratch)");
+    rc = ensure_scratch(ctx, &ctx->scratch_b, &ctx->scratch_b_cap, total, "cudaMalloc(sch scratch)");
   }
   if (rc != PG_OK) {
     return rc;
   }
-  uint8_t* base = static_cast<uint8_t*>(ctx->scratch_a);
-  rc = check_cuda(ctx, cudaMemcpyAsync(base, llrs, nof_llrs_total, cudaMemcpyHostToDevice, s), "cudaMemcpyAsync(llrs)");
+  uint8_t* base = static_cast<uint8_t*>(ctx->scratch_b);
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyAsync(base + o_offs, cb_bit_off.data(), (size_t)ncb * 4, cudaMemcpyHostToDevice, s),
                     "cudaMemcpyAsync(offsets)");
@@ -378,7 +402,7 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
     rc = stage_slot(ctx, SLOT_RM, rm.data(), rm.size() * sizeof(pg_rm_cb), s, &d_rm);
   }
   if (rc == PG_OK) {
-    rc = rate_dematch_launch(ctx, static_cast<const pg_rm_cb*>(d_rm), ncb, reinterpret_cast<const int8_t*>(base),
+    rc = rate_dematch_launch(ctx, static_cast<const pg_rm_cb*>(d_rm), ncb, d_llrs,
                              reinterpret_cast<int8_t*>(base + o_rm), s);
   }
   if (rc == PG_OK) {
@@ -453,4 +477,4 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
   return PG_OK;
 }
 
-} // extern "C"
+} // namespace pg

@@ -1,0 +1,385 @@
+// PUSCH demodulation on sm_100a: per resource element, the channel estimate of the OFDM symbol
+// (time interpolation between the DM-RS symbols, rounded to bf16 as the reference's estimator
+// returns it, DC subcarrier zeroed), equalisation, soft demapping and descrambling, fused in one
+// kernel that writes the codeword LLRs in the reference's order: data symbols in time order,
+// subcarriers in frequency order, layers, bits (pusch_demodulator_impl.cpp:254-461 with
+// get_ch_data_estimates :510-545 and revert_scrambling :22-206).
+//
+// The descrambling sequence c_init = RNTI * 2^15 + n_ID is produced first, one 32-bit word per
+// thread from the Gold basis table (pg_device.cuh).
+#include "pg_internal.h"
+#include "pg_device.cuh"
+
+#include <algorithm>
+#include <vector>
+
+namespace {
+
+__constant__ float c_slope_d[3][4][16];
+__constant__ float c_intercept_d[3][4][16];
+__constant__ float c_width_d[3];
+
+struct cf {
+  float r, i;
+};
+__device__ __forceinline__ cf cmul(cf a, cf b)
+{
+  return {__fsub_rn(__fmul_rn(a.r, b.r), __fmul_rn(a.i, b.i)), __fadd_rn(__fmul_rn(a.r, b.i), __fmul_rn(a.i, b.r))};
+}
+__device__ __forceinline__ cf cconjmul(cf a, cf b)
+{
+  return {__fadd_rn(__fmul_rn(a.r, b.r), __fmul_rn(a.i, b.i)), __fsub_rn(__fmul_rn(a.i, b.r), __fmul_rn(a.r, b.i))};
+}
+__device__ __forceinline__ cf cadd(cf a, cf b)
+{
+  return {__fadd_rn(a.r, b.r), __fadd_rn(a.i, b.i)};
+}
+__device__ __forceinline__ cf csub(cf a, cf b)
+{
+  return {__fsub_rn(a.r, b.r), __fsub_rn(a.i, b.i)};
+}
+__device__ __forceinline__ cf cscale(cf a, float s)
+{
+  return {__fmul_rn(a.r, s), __fmul_rn(a.i, s)};
+}
+__device__ __forceinline__ float cnorm(cf a)
+{
+  return __fadd_rn(__fmul_rn(a.r, a.r), __fmul_rn(a.i, a.i));
+}
+__device__ __forceinline__ cf cbf16(uint32_t v)
+{
+  return {__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u)};
+}
+__device__ __forceinline__ float bf16_round(float f)
+{
+  uint32_t u = __float_as_uint(f);
+  if ((u & 0x7fffffffu) > 0x7f800000u) {
+    return f;
+  }
+  u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+  return __uint_as_float(u);
+}
+
+__device__ __forceinline__ int8_t quantize(float v, float scale)
+{
+  v = __fmul_rn(v, scale);
+  v = v > 120.f ? 120.f : (v < -120.f ? -120.f : v);
+  if (!(v == v)) {
+    return 0;
+  }
+  return (int8_t)__float2int_rn(v);
+}
+
+template <int QM>
+__device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* llr)
+{
+  const float rcp = (nvar > 0.f) ? __frcp_rn(nvar) : 0.f;
+  if (QM == 2) {
+    const float g = 2.0f * 1.41421353816986083984375f;
+    llr[0]        = quantize(__fmul_rn(__fmul_rn(g, xr), rcp), 5.0f);
+    llr[1]        = quantize(__fmul_rn(__fmul_rn(g, xi), rcp), 5.0f);
+    return;
+  }
+  if (QM == 4) {
+    const float s10  = 0.3162277638912200927734375f;
+    const float x[2] = {xr, xi};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      const float first  = __fmul_rn(4.0f * s10, x[c]);
+      const float second = __fsub_rn(__fmul_rn(2.0f, first), copysignf(0.8f, x[c]));
+      const float v01    = fabsf(x[c]) > 2.0f * s10 ? second : first;
+      const float v23    = __fsub_rn(0.8f, fabsf(first));
+      const bool  z      = fabsf(x[c]) <= 1e-9f;
+      llr[c]             = quantize(z ? 0.f : __fmul_rn(v01, rcp), 6.0f);
+      llr[2 + c]         = quantize(z ? 0.f : __fmul_rn(v23, rcp), 6.0f);
+    }
+    return;
+  }
+  constexpr int t     = QM == 6 ? 1 : 2;
+  constexpr int nint  = QM == 6 ? 8 : 16;
+  const float   width = c_width_d[t];
+  const float   x[2]  = {xr, xi};
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    int idx      = (int)floorf(__fdiv_rn(x[c], width)) + nint / 2;
+    idx          = idx < 0 ? 0 : (idx > nint - 1 ? nint - 1 : idx);
+    const bool z = fabsf(x[c]) <= 1e-9f;
+#pragma unroll
+    for (int b = 0; b < QM / 2; ++b) {
+      const float v  = __fmul_rn(__fadd_rn(__fmul_rn(c_slope_d[t][b][idx], x[c]), c_intercept_d[t][b][idx]), rcp);
+      llr[2 * b + c] = quantize(z ? 0.f : v, 6.0f);
+    }
+  }
+}
+
+__global__ void scrambling_kernel(const pg_pusch_ue* __restrict__ ues, const uint32_t* __restrict__ seq_offsets,
+                                  uint32_t* __restrict__ seq, const uint32_t* __restrict__ gold, uint32_t gold_words)
+{
+  const pg_pusch_ue ue     = ues[blockIdx.y];
+  int               d0 = 0, d1 = 0;
+  int               ndmrs = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+    ndmrs += (ue.dmrs_symbol_mask >> s) & 1;
+  }
+  (void)d0;
+  (void)d1;
+  const uint32_t g      = (uint32_t)(ue.nof_symbols - ndmrs) * 12u * ue.nof_rb * ue.nof_layers * ue.modulation_order;
+  const uint32_t words  = (g + 31) / 32;
+  const uint32_t c_init = ((uint32_t)ue.rnti << 15) + ue.n_id_data;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+    seq[seq_offsets[blockIdx.y] + w] = pg::gold_word(gold, gold_words, c_init, 32u * w);
+  }
+}
+
+template <int L, int P, int QM>
+__device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* __restrict__ grid,
+                                         const float2* __restrict__ est, const pg_port_result* __restrict__ pres,
+                                         int nd, float w, int sym, int re_idx, int j, const uint32_t* __restrict__ seq,
+                                         int8_t* __restrict__ llr_out)
+{
+  const int nsc     = 12 * ue.nof_rb;
+  const int sc      = 12 * ue.rb_start + j;
+  const bool is_dc  = sc == ue.dc_subcarrier;
+  cf        y[P];
+  cf        h[P][L];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    y[p] = cbf16(__ldg(grid + ((size_t)p * 14 + sym) * ue.grid_nof_subc + sc));
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const float2* f0 = est + (((size_t)p * nd) * L + l) * nsc;
+      float2        v  = f0[j];
+      if (nd == 2) {
+        const float2 v1 = f0[(size_t)L * nsc + j];
+        v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
+      }
+      h[p][l] = is_dc ? cf{0.f, 0.f} : cf{bf16_round(v.x), bf16_round(v.y)};
+    }
+  }
+  cf    s[L];
+  float nv[L];
+  if (L == 1) {
+    float ch_mod = 0.f, nacc = 0.f;
+    cf    acc    = {0.f, 0.f};
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const float n2 = cnorm(h[p][0]);
+      if (n2 < INFINITY) {
+        ch_mod = __fadd_rn(ch_mod, n2);
+        nacc   = __fadd_rn(nacc, __fmul_rn(n2, pres[p].noise_var));
+        acc    = cadd(acc, cconjmul(y[p], h[p][0]));
+      }
+    }
+    const bool  ok  = (ch_mod > 0.f) && (ch_mod < INFINITY);
+    const float rcp = __frcp_rn(ch_mod);
+    s[0]            = ok ? cscale(acc, rcp) : cf{0.f, 0.f};
+    nv[0]           = ok ? __fmul_rn(nacc, __fmul_rn(rcp, rcp)) : INFINITY;
+  } else {
+    float noise = pres[0].noise_var;
+#pragma unroll
+    for (int p = 1; p < P; ++p) {
+      noise = fmaxf(noise, pres[p].noise_var);
+    }
+    cf   G[L][L], Gi[L][L];
+    bool ok = pg::is_normal(noise) && noise >= 0.f;
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+#pragma unroll
+      for (int k = 0; k < L; ++k) {
+        cf acc = {0.f, 0.f};
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          acc = cadd(acc, cconjmul(h[p][i], h[p][k]));
+        }
+        G[i][k]  = acc;
+        Gi[i][k] = cf{i == k ? 1.f : 0.f, 0.f};
+      }
+      ok        = ok && (G[i][i].r > 0.f);
+      G[i][i].r = __fadd_rn(G[i][i].r, noise);
+    }
+#pragma unroll
+    for (int i = 0; i < L; ++i) {
+      const cf    piv  = G[i][i];
+      const float pn   = cnorm(piv);
+      ok               = ok && (pn > 0.f);
+      const cf    pinv = cscale(cf{piv.r, -piv.i}, __frcp_rn(pn));
+      Gi[i][i]         = cf{1.f, 0.f};
+#pragma unroll
+      for (int k = i + 1; k < L; ++k) {
+        G[i][k] = cmul(G[i][k], pinv);
+      }
+#pragma unroll
+      for (int k = 0; k <= i; ++k) {
+        Gi[i][k] = cmul(Gi[i][k], pinv);
+      }
+#pragma unroll
+      for (int r = 0; r < L; ++r) {
+        if (r != i) {
+          const cf f = G[r][i];
+#pragma unroll
+          for (int k = i; k < L; ++k) {
+            G[r][k] = csub(G[r][k], cmul(f, G[i][k]));
+          }
+#pragma unroll
+          for (int k = 0; k < i; ++k) {
+            Gi[r][k] = csub(Gi[r][k], cmul(f, Gi[i][k]));
+          }
+          const cf t = cmul(f, Gi[i][i]);
+          Gi[r][i]   = cf{-t.r, -t.i};
+        }
+      }
+    }
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      cf    acc  = {0.f, 0.f};
+      float corr = 0.f;
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        cf wv = {0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < L; ++k) {
+          wv = cadd(wv, cconjmul(Gi[k][l], h[p][k]));
+        }
+        acc  = cadd(acc, cmul(wv, y[p]));
+        corr = __fadd_rn(corr, cmul(wv, h[p][l]).r);
+      }
+      const float c = __frcp_rn(corr);
+      s[l]          = ok ? cscale(acc, c) : cf{0.f, 0.f};
+      nv[l]         = ok ? __fsub_rn(c, 1.f) : INFINITY;
+    }
+  }
+  // Demap, descramble, store: LLR index (re * L + l) * QM + b.
+  int8_t        llr[L * QM];
+#pragma unroll
+  for (int l = 0; l < L; ++l) {
+    demap<QM>(s[l].r, s[l].i, nv[l], llr + l * QM);
+  }
+  const uint32_t bit0 = (uint32_t)re_idx * L * QM;
+  const uint32_t wa   = __ldg(seq + (bit0 >> 5));
+  const uint32_t wb   = __ldg(seq + (bit0 >> 5) + 1);
+  const uint32_t sh   = bit0 & 31u;
+  const uint32_t cbits = sh ? ((wa >> sh) | (wb << (32 - sh))) : wa;
+  int8_t* out = llr_out + ue.llr_offset + bit0;
+#pragma unroll
+  for (int b = 0; b < L * QM; ++b) {
+    const int v = llr[b];
+    out[b]      = (int8_t)(((cbits >> b) & 1u) ? -v : v);
+  }
+}
+
+template <int L, int P>
+__device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const uint32_t* grid, const float2* est,
+                                                  const pg_port_result* pres, int nd, float w, int sym, int re_idx,
+                                                  int j, const uint32_t* seq, int8_t* llrs)
+{
+  switch (ue.modulation_order) {
+    case 2: demod_re<L, P, 2>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
+    case 4: demod_re<L, P, 4>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
+    case 6: demod_re<L, P, 6>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
+    default: demod_re<L, P, 8>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
+  }
+}
+
+__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues,
+                                                          const uint32_t* __restrict__ grids,
+                                                          const float2* __restrict__ est_all,
+                                                          const pg_port_result* __restrict__ port_results,
+                                                          const uint32_t* __restrict__ seq_offsets,
+                                                          const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs)
+{
+  const int         u  = blockIdx.y;
+  const pg_pusch_ue ue = ues[u];
+  const int         nsc = 12 * ue.nof_rb;
+  int               d0 = -1, d1 = -1, nd = 0, ndata = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+    if ((ue.dmrs_symbol_mask >> s) & 1) {
+      if (nd == 0) {
+        d0 = s;
+      } else if (nd == 1) {
+        d1 = s;
+      }
+      ++nd;
+    } else {
+      ++ndata;
+    }
+  }
+  const int total = ndata * nsc;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < total; r += gridDim.x * blockDim.x) {
+    const int di = r / nsc;
+    const int j  = r - di * nsc;
+    // OFDM symbol of data-symbol index di.
+    int sym = ue.first_symbol, cnt = -1;
+    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+      if (!((ue.dmrs_symbol_mask >> s) & 1)) {
+        if (++cnt == di) {
+          sym = s;
+          break;
+        }
+      }
+    }
+    const float             w    = nd == 2 ? (float)(sym - d0) / (float)(d1 - d0) : 0.f;
+    const uint32_t*         grid = grids + ue.grid_offset;
+    const float2*           est  = est_all + ue.est_offset;
+    const pg_port_result*   pres = port_results + (size_t)u * 4;
+    const uint32_t*         sq   = seq + seq_offsets[u];
+    if (ue.nof_layers == 1) {
+      switch (ue.nof_rx_ports) {
+        case 1: demod_dispatch_qm<1, 1>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
+        case 2: demod_dispatch_qm<1, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
+        default: demod_dispatch_qm<1, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
+      }
+    } else {
+      switch (ue.nof_rx_ports) {
+        case 2: demod_dispatch_qm<2, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
+        default: demod_dispatch_qm<2, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
+      }
+    }
+    (void)d1;
+  }
+}
+
+} // namespace
+
+namespace pg {
+
+int demod_upload_tables(pg_context* ctx, const void* slope, const void* intercept, const void* width)
+{
+  int rc = check_cuda(ctx, cudaMemcpyToSymbol(c_slope_d, slope, sizeof(c_slope_d)), "cudaMemcpyToSymbol");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_intercept_d, intercept, sizeof(c_intercept_d)), "cudaMemcpyToSymbol");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_width_d, width, sizeof(c_width_d)), "cudaMemcpyToSymbol");
+  }
+  return rc;
+}
+
+uint32_t ue_codeword_bits(const pg_pusch_ue& u)
+{
+  int ndmrs = 0;
+  for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
+    ndmrs += (u.dmrs_symbol_mask >> s) & 1;
+  }
+  return (uint32_t)(u.nof_symbols - ndmrs) * 12u * u.nof_rb * u.nof_layers * u.modulation_order;
+}
+
+// Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
+// device scratch sized by the caller from ue_codeword_bits.
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
+                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
+                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  scrambling_kernel<<<dim3(std::max(1u, std::min(64u, (max_words + 255) / 256)), n), 256, 0, s>>>(
+      ues_dev, seq_offsets_dev, seq_dev, ctx->dev.gold, kGoldWords);
+  if (int rc = check_cuda(ctx, cudaGetLastError(), "scrambling_kernel launch")) {
+    return rc;
+  }
+  pusch_demod_kernel<<<dim3(std::max(1u, std::min(1024u, (max_re + 255) / 256)), n), 256, 0, s>>>(
+      ues_dev, grids, reinterpret_cast<const float2*>(est), port_results, seq_offsets_dev, seq_dev, llrs);
+  return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
+}
+
+} // namespace pg

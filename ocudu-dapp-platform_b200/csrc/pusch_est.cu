@@ -1,0 +1,517 @@
+// DM-RS channel estimation for PUSCH on sm_100a, following the reference's
+// port_channel_estimator_average_impl with FD smoothing "filter", TD "interpolate" and no CFO
+// compensation (lib/phy/upper/signal_processors/channel_estimator/port_channel_estimator_average_impl.cpp:322-557,
+// port_channel_estimator_helpers.cpp:29-300, lib/phy/support/interpolator/interpolator_linear_impl.cpp:15-123)
+// and the pilot generation of dmrs_pusch_estimator_impl (dmrs_pusch_estimator_impl.cpp:69-169).
+//
+// One CTA per (UE, receive port). Per DM-RS symbol d and layer l (CDM group 0: layers 0 and 1):
+//   LS          lse = rx * conj(pilot_l); with two layers, adjacent pilot pairs are averaged
+//               (the frequency OCC [+1, -1] cancels the other layer); scaled by 1/beta;
+//   smoothing   the pilots are extended at both ends by nv virtual pilots (linear fit of magnitude
+//               and unwrapped phase of the nv outermost pilots) and convolved with the normalised
+//               raised-cosine taps (roll-off 0.2) resampled at the pilot stride;
+//   RSRP        sum |smoothed|^2 * beta^2;
+//   frequency   linear interpolation from the even subcarriers to every subcarrier;
+//   noise       sum over DM-RS symbols of |sum_l mean_d(smoothed) * beta * pilot_l - rx|^2.
+// Per port: rsrp /= N, epre = sum |rx|^2 / N, noise /= (N * nof_cdm - 1) floored at rsrp / 1e10,
+// snr = rsrp * layers / beta^2 / noise, with N = pilots per symbol x DM-RS symbols.
+// Pilot bits come from the Gold sequence c(n) of TS 38.211 Section 5.2.1, evaluated as
+// x1(n + Nc) xor (xor over the set bits i of c_init of the x2 sequence started from state e_i):
+// c is linear in c_init, so 32 precomputed basis sequences give any sequence word by word.
+#include "pg_internal.h"
+#include "pg_device.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace {
+
+constexpr int kEstThreads = 256;
+constexpr int kMaxV       = 12;
+constexpr int kMaxPil     = 6 * 275;
+constexpr int kMaxDmrs    = 2;
+
+__constant__ float c_rc_taps[3][16]; // normalised taps for 1, 2 and >= 3 PRBs (5, 11, 15 taps)
+
+__device__ __forceinline__ float2 cbf16_load(const uint32_t* p)
+{
+  const uint32_t v = __ldg(p);
+  return make_float2(__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u));
+}
+
+__device__ __forceinline__ uint32_t float_to_bf16_rne(float f)
+{
+  uint32_t u = __float_as_uint(f);
+  if ((u & 0x7fffffffu) > 0x7f800000u) {
+    return (u >> 16) | 0x40u; // quiet NaN
+  }
+  return (u + 0x7fffu + ((u >> 16) & 1u)) >> 16;
+}
+
+} // namespace
+
+namespace pg {
+
+// Host: x1 from (1, 0, ..., 0) and x2 from each unit state e_i, positions Nc .. Nc + 32*words.
+void gold_tables_host(std::vector<uint32_t>& tab, uint32_t words)
+{
+  tab.assign((size_t)32 * words, 0);
+  const uint32_t nc = 1600;
+  for (int seq = 0; seq < 32; ++seq) {
+    // State holds x(n) .. x(n+30) in bits 0..30.
+    uint32_t st = seq == 0 ? 1u : (1u << (seq - 1));
+    uint32_t* out = tab.data() + (size_t)seq * words;
+    for (uint32_t n = 0; n < nc + 32u * words; ++n) {
+      const uint32_t bit = st & 1u;
+      uint32_t       nb;
+      if (seq == 0) {
+        nb = ((st >> 3) ^ st) & 1u;
+      } else {
+        nb = ((st >> 3) ^ (st >> 2) ^ (st >> 1) ^ st) & 1u;
+      }
+      st = (st >> 1) | (nb << 30);
+      if (n >= nc) {
+        const uint32_t m = n - nc;
+        out[m >> 5] |= bit << (m & 31);
+      }
+    }
+  }
+}
+
+} // namespace pg
+
+namespace {
+
+struct est_smem {
+  float2   rx[kMaxDmrs][kMaxPil];
+  float2   ext[kMaxDmrs][2][kMaxPil + 2 * kMaxV];
+  float2   filt[kMaxDmrs][2][kMaxPil];
+  uint32_t bits[kMaxDmrs][(2 * kMaxPil) / 32 + 2];
+  float    red[3][kEstThreads / 32];
+};
+
+__device__ __forceinline__ float block_sum(float v, float* red, int slot_unused)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  (void)slot_unused;
+  if ((threadIdx.x & 31) == 0) {
+    red[threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  float t = 0.f;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kEstThreads / 32; ++i) {
+      t += red[i];
+    }
+  }
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
+{
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ float2 cmulconjf(float2 a, float2 b) // a * conj(b)
+{
+  return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+__device__ void virtual_pilots(float2* out, const float2* base, int nv, bool is_start)
+{
+  // Linear fit of |h| and of the unwrapped arg(h) over nv pilots (port_channel_estimator_helpers.cpp
+  // compute_v_pilots / add_v_pilots), evaluated at the nv positions before or after them.
+  float arg_prev = 0.f, acc = 0.f;
+  float mean_abs = 0.f, mean_arg = 0.f, sxa = 0.f, sxg = 0.f;
+  float args[kMaxV], abss[kMaxV];
+  for (int i = 0; i < nv; ++i) {
+    const float a = hypotf(base[i].x, base[i].y);
+    float       g = atan2f(base[i].y, base[i].x);
+    if (i > 0) {
+      // unwrap: keep consecutive differences within (-pi, pi].
+      float d = g - arg_prev;
+      if (d > 3.14159265358979f) {
+        acc -= 6.28318530717959f;
+      } else if (d < -3.14159265358979f) {
+        acc += 6.28318530717959f;
+      }
+    }
+    arg_prev = g;
+    abss[i]  = a;
+    args[i]  = g + acc;
+  }
+  for (int i = 0; i < nv; ++i) {
+    mean_abs += abss[i];
+    mean_arg += args[i];
+    sxa += abss[i] * (float)i;
+    sxg += args[i] * (float)i;
+  }
+  mean_abs /= (float)nv;
+  mean_arg /= (float)nv;
+  const float mean_x = (float)(nv * (nv - 1)) / 2.0f / (float)nv;
+  const float nxsq   = (float)((nv - 1) * nv * (2 * nv - 1)) / 6.0f;
+  const float den    = nxsq - (float)nv * mean_x * mean_x;
+  const float sa     = (sxa - mean_x * mean_abs * (float)nv) / den;
+  const float ia     = mean_abs - sa * mean_x;
+  const float sg     = (sxg - mean_x * mean_arg * (float)nv) / den;
+  const float ig     = mean_arg - sg * mean_x;
+  const int   voff   = is_start ? -nv : nv;
+  for (int i = 0; i < nv; ++i) {
+    const float iv  = (float)(i + voff);
+    const float rho = sa * iv + ia;
+    float       s, c;
+    sincosf(sg * iv + ig + (rho > 0.f ? 0.f : 3.14159265358979f), &s, &c);
+    out[i] = make_float2(fabsf(rho) * c, fabsf(rho) * s);
+  }
+}
+
+__global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pusch_ue* __restrict__ ues,
+                                                                     const uint32_t* __restrict__ grids,
+                                                                     float2* __restrict__ est_all,
+                                                                     pg_port_result* __restrict__ results,
+                                                                     const uint32_t* __restrict__ gold,
+                                                                     uint32_t gold_words)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  est_smem&         sm   = *reinterpret_cast<est_smem*>(smem_raw);
+  const int         u    = blockIdx.x;
+  const int         port = blockIdx.y;
+  const pg_pusch_ue ue   = ues[u];
+  if (port >= ue.nof_rx_ports) {
+    return;
+  }
+  const int tid  = threadIdx.x;
+  const int nl   = ue.nof_layers;
+  const int nrb  = ue.nof_rb;
+  const int npil = 6 * nrb;
+  const int nsc  = 12 * nrb;
+  int       dsym[kMaxDmrs];
+  int       nd = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && nd < kMaxDmrs; ++s) {
+    if ((ue.dmrs_symbol_mask >> s) & 1) {
+      dsym[nd++] = s;
+    }
+  }
+  const float     beta = ue.dmrs_scaling;
+  const uint32_t* grid = grids + ue.grid_offset + (size_t)port * 14 * ue.grid_nof_subc;
+
+  // Pilot bits c(2 m0) .. c(2 m0 + 2 npil - 1) per DM-RS symbol, m0 = 6 rb_start.
+  const int nwords = (2 * npil + 31) / 32;
+  for (int i = tid; i < nd * nwords; i += kEstThreads) {
+    const int      d      = i / nwords;
+    const int      w      = i - d * nwords;
+    const uint32_t c_init = (uint32_t)(((14ull * ue.slot + dsym[d] + 1) * (2ull * ue.n_id + 1) * (1ull << 17) +
+                                        (2ull * ue.n_id + ue.n_scid)) %
+                                       (1ull << 31));
+    sm.bits[d][w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 32u * w);
+  }
+  __syncthreads();
+
+  // LS estimates.
+  const float inv_beta = 1.0f / beta;
+  const float a        = 0.707106781186547524f; // 1/sqrt(2) (M_SQRT1_2 in float)
+  float       epre     = 0.f;
+  for (int i = tid; i < nd * npil; i += kEstThreads) {
+    const int    d   = i / npil;
+    const int    k   = i - d * npil;
+    const float2 y   = cbf16_load(grid + (size_t)dsym[d] * ue.grid_nof_subc + 12 * ue.rb_start + 2 * k);
+    sm.rx[d][k]      = y;
+    epre += y.x * y.x + y.y * y.y;
+    const uint32_t b0 = (sm.bits[d][(2 * k) >> 5] >> ((2 * k) & 31)) & 1u;
+    const uint32_t b1 = (sm.bits[d][(2 * k + 1) >> 5] >> ((2 * k + 1) & 31)) & 1u;
+    const float2   p0 = make_float2(b0 ? -a : a, b1 ? -a : a);
+    sm.ext[d][0][kMaxV + k] = cmulconjf(y, p0);
+    if (nl > 1) {
+      const float2 p1         = (k & 1) ? make_float2(-p0.x, -p0.y) : p0;
+      sm.ext[d][1][kMaxV + k] = cmulconjf(y, p1);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < nd * nl * (npil / 2); i += kEstThreads) {
+    const int d  = i / (nl * (npil / 2));
+    const int r  = i - d * nl * (npil / 2);
+    const int l  = r / (npil / 2);
+    const int k  = 2 * (r - l * (npil / 2));
+    float2    v0 = sm.ext[d][l][kMaxV + k], v1 = sm.ext[d][l][kMaxV + k + 1];
+    if (nl > 1) {
+      const float2 av = make_float2((v0.x + v1.x) / 2.0f, (v0.y + v1.y) / 2.0f);
+      v0 = v1 = av;
+    }
+    sm.ext[d][l][kMaxV + k]     = make_float2(v0.x * inv_beta, v0.y * inv_beta);
+    sm.ext[d][l][kMaxV + k + 1] = make_float2(v1.x * inv_beta, v1.y * inv_beta);
+  }
+  __syncthreads();
+
+  // Smoothing filter and virtual pilots.
+  const int  tsel  = nrb >= 3 ? 2 : nrb - 1;
+  const int  ntaps = tsel == 2 ? 15 : (tsel == 1 ? 11 : 5);
+  const int  mid   = ntaps / 2;
+  const int  nv    = nrb == 1 ? npil : mid;
+  if (tid < nd * nl * 2) {
+    const int d = tid / (nl * 2), l = (tid / 2) % nl, side = tid & 1;
+    if (side == 0) {
+      virtual_pilots(&sm.ext[d][l][kMaxV - nv], &sm.ext[d][l][kMaxV], nv, true);
+    } else {
+      virtual_pilots(&sm.ext[d][l][kMaxV + npil], &sm.ext[d][l][kMaxV + npil - nv], nv, false);
+    }
+  }
+  __syncthreads();
+  float rsrp_part[2] = {0.f, 0.f};
+  for (int i = tid; i < nd * nl * npil; i += kEstThreads) {
+    const int d = i / (nl * npil);
+    const int r = i - d * nl * npil;
+    const int l = r / npil;
+    const int k = r - l * npil;
+    float2    acc = make_float2(0.f, 0.f);
+    for (int t = 0; t < ntaps; ++t) {
+      const float2 x = sm.ext[d][l][kMaxV + k - mid + t];
+      acc.x += x.x * c_rc_taps[tsel][t];
+      acc.y += x.y * c_rc_taps[tsel][t];
+    }
+    sm.filt[d][l][k] = acc;
+    rsrp_part[l] += acc.x * acc.x + acc.y * acc.y;
+  }
+  __syncthreads();
+
+  // Frequency interpolation to every subcarrier and noise estimation.
+  float2* est = est_all + ue.est_offset + (size_t)port * nd * nl * nsc;
+  for (int i = tid; i < nd * nl * nsc; i += kEstThreads) {
+    const int d = i / (nl * nsc);
+    const int r = i - d * nl * nsc;
+    const int l = r / nsc;
+    const int j = r - l * nsc;
+    const int k = j >> 1;
+    float2    v = sm.filt[d][l][k];
+    if ((j & 1) && k + 1 < npil) {
+      const float2 n = sm.filt[d][l][k + 1];
+      v              = make_float2((n.x - v.x) * 0.5f + v.x, (n.y - v.y) * 0.5f + v.y);
+    }
+    est[((size_t)d * nl + l) * nsc + j] = v;
+  }
+  float       noise = 0.f;
+  const float sf    = beta / (float)nd;
+  for (int i = tid; i < nd * npil; i += kEstThreads) {
+    const int      d  = i / npil;
+    const int      k  = i - d * npil;
+    const uint32_t b0 = (sm.bits[d][(2 * k) >> 5] >> ((2 * k) & 31)) & 1u;
+    const uint32_t b1 = (sm.bits[d][(2 * k + 1) >> 5] >> ((2 * k + 1) & 31)) & 1u;
+    const float2   p0 = make_float2(b0 ? -a : a, b1 ? -a : a);
+    float2         pred = make_float2(0.f, 0.f);
+    for (int l = 0; l < nl; ++l) {
+      float2 s = make_float2(0.f, 0.f);
+      for (int dd = 0; dd < nd; ++dd) {
+        s.x += sm.filt[dd][l][k].x * sf;
+        s.y += sm.filt[dd][l][k].y * sf;
+      }
+      const float2 p = (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
+      const float2 q = cmulf(s, p);
+      pred.x += q.x;
+      pred.y += q.y;
+    }
+    const float2 e = make_float2(pred.x - sm.rx[d][k].x, pred.y - sm.rx[d][k].y);
+    noise += e.x * e.x + e.y * e.y;
+  }
+  const float tot_noise = block_sum(noise, sm.red[0], 0);
+  const float tot_epre  = block_sum(epre, sm.red[1], 1);
+  const float tot_r0    = block_sum(rsrp_part[0], sm.red[2], 2);
+  const float tot_r1    = block_sum(rsrp_part[1], sm.red[0], 0);
+  if (tid == 0) {
+    const float    n_pil = (float)(npil * nd);
+    pg_port_result pr;
+    pr.rsrp[0]        = tot_r0 * beta * beta / n_pil;
+    pr.rsrp[1]        = nl > 1 ? tot_r1 * beta * beta / n_pil : 0.f;
+    pr.epre           = tot_epre / n_pil;
+    const float ravg  = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
+    float       nvar  = (pg::is_normal(tot_noise) ? tot_noise : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
+    nvar              = fmaxf(ravg / 1e10f, nvar);
+    pr.noise_var      = nvar;
+    pr.snr            = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
+    results[(size_t)u * 4 + port] = pr;
+  }
+}
+
+// Per-symbol estimates of one UE: f[i] + (f[i+1] - f[i]) w rounded to bf16 (the reference's
+// apply_td_domain_strategy + conversion to cbf16_t).
+__global__ void symbol_estimates_kernel(pg_pusch_ue ue, const float2* __restrict__ est, uint32_t* __restrict__ out,
+                                        int nd, int dsym0, int dsym1)
+{
+  const int nsc = 12 * ue.nof_rb;
+  const int nl  = ue.nof_layers;
+  const int s   = blockIdx.y;
+  const int p   = blockIdx.z;
+  int       i0  = 0;
+  float     w   = 0.f;
+  if (nd == 2) {
+    w = (float)(s - dsym0) / (float)(dsym1 - dsym0);
+  }
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nl * nsc; t += gridDim.x * blockDim.x) {
+    const int     l  = t / nsc;
+    const int     j  = t - l * nsc;
+    const float2* f0 = est + (((size_t)p * nd + i0) * nl + l) * nsc;
+    float2        v  = f0[j];
+    if (nd == 2) {
+      const float2 v1 = f0[(size_t)nl * nsc + j];
+      v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
+    }
+    out[(((size_t)p * 14 + s) * nl + l) * nsc + j] = float_to_bf16_rne(v.x) | (float_to_bf16_rne(v.y) << 16);
+  }
+}
+
+} // namespace
+
+namespace pg {
+
+int est_upload_tables(pg_context* ctx)
+{
+  // Raised-cosine impulse, roll-off 0.2, 10 samples per symbol, 31 samples centred at 15; the
+  // taps of n PRBs (n = 1, 2, >= 3) are every second sample around the centre, normalised.
+  double rc[31];
+  for (int n = 0; n < 31; ++n) {
+    const double t = (n - 15) / 10.0, b = 0.2;
+    const double s = t == 0 ? 1.0 : std::sin(M_PI * t) / (M_PI * t);
+    const double q = 1 - (2 * b * t) * (2 * b * t);
+    rc[n]          = std::fabs(q) < 1e-12 ? 0.0 : s * std::cos(M_PI * b * t) / q;
+  }
+  float taps[3][16] = {};
+  for (int sel = 0; sel < 3; ++sel) {
+    const int nrb = sel + 1, ncoef = nrb * 10 + 1, nout = ncoef / 2 / 2, first = 15 - nout * 2, n = 2 * nout + 1;
+    float     tot = 0.f;
+    for (int i = 0; i < n; ++i) {
+      taps[sel][i] = (float)rc[first + 2 * i];
+      tot += taps[sel][i];
+    }
+    for (int i = 0; i < n; ++i) {
+      taps[sel][i] *= 1.0f / tot;
+    }
+  }
+  int rc2 = check_cuda(ctx, cudaMemcpyToSymbol(c_rc_taps, taps, sizeof(taps)), "cudaMemcpyToSymbol(rc taps)");
+  if (rc2 != PG_OK) {
+    return rc2;
+  }
+  std::vector<uint32_t> gold;
+  gold_tables_host(gold, kGoldWords);
+  rc2 = check_cuda(ctx, cudaMalloc(&ctx->dev.gold, gold.size() * 4), "cudaMalloc(gold)");
+  if (rc2 == PG_OK) {
+    rc2 = check_cuda(ctx, cudaMemcpy(ctx->dev.gold, gold.data(), gold.size() * 4, cudaMemcpyHostToDevice),
+                     "cudaMemcpy(gold)");
+  }
+  return rc2;
+}
+
+int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
+{
+  if (n < 0 || (n > 0 && ues == nullptr)) {
+    return set_error(ctx, PG_ERR_INVALID, "invalid UE list");
+  }
+  for (int i = 0; i < n; ++i) {
+    const pg_pusch_ue& u = ues[i];
+    int                nd = 0;
+    for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
+      nd += (u.dmrs_symbol_mask >> s) & 1;
+    }
+    const bool ok = u.nof_rb >= 1 && u.rb_start + u.nof_rb <= 275 && 12u * (u.rb_start + u.nof_rb) <= u.grid_nof_subc &&
+                    (u.nof_layers == 1 || u.nof_layers == 2) &&
+                    (u.nof_rx_ports == 1 || u.nof_rx_ports == 2 || u.nof_rx_ports == 4) &&
+                    u.nof_layers <= u.nof_rx_ports && nd >= 1 && nd <= kMaxDmrs && u.first_symbol + u.nof_symbols <= 14 &&
+                    u.dmrs_scaling > 0.f && (u.modulation_order == 2 || u.modulation_order == 4 ||
+                                             u.modulation_order == 6 || u.modulation_order == 8);
+    if (!ok) {
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": unsupported PUSCH configuration");
+    }
+  }
+  return PG_OK;
+}
+
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* grids, float* est,
+                    pg_port_result* results, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(pusch_estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(est_smem));
+    attr_set = true;
+  }
+  pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, sizeof(est_smem), s>>>(
+      ues_dev, grids, reinterpret_cast<float2*>(est), results, ctx->dev.gold, kGoldWords);
+  return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
+}
+
+int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1)
+{
+  int nd = 0;
+  for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
+    if ((u.dmrs_symbol_mask >> s) & 1) {
+      if (nd == 0) {
+        *d0 = s;
+      } else if (nd == 1) {
+        *d1 = s;
+      }
+      ++nd;
+    }
+  }
+  return nd;
+}
+
+} // namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+size_t pg_pusch_est_size(const pg_pusch_ue* ue)
+{
+  if (ue == nullptr) {
+    return 0;
+  }
+  int d0 = 0, d1 = 0;
+  return (size_t)ue->nof_rx_ports * dmrs_count(*ue, &d0, &d1) * ue->nof_layers * 12 * ue->nof_rb;
+}
+
+int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids, float* est,
+                             pg_port_result* results, void* stream)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (int rc = validate_ues(ctx, ues, nof_ues)) {
+    return rc;
+  }
+  if (nof_ues == 0) {
+    return PG_OK;
+  }
+  cudaStream_t s   = static_cast<cudaStream_t>(stream);
+  void*        dev = nullptr;
+  if (int rc = stage_slot(ctx, SLOT_UE, ues, (size_t)nof_ues * sizeof(pg_pusch_ue), s, &dev)) {
+    return rc;
+  }
+  if (int rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(dev), nof_ues, grids, est, results, s)) {
+    return rc;
+  }
+  return release_slot_after(ctx, SLOT_UE, s);
+}
+
+int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, uint32_t* out,
+                                     void* stream)
+{
+  if (ctx == nullptr || ue == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (int rc = validate_ues(ctx, ue, 1)) {
+    return rc;
+  }
+  int       d0 = 0, d1 = 0;
+  const int nd = dmrs_count(*ue, &d0, &d1);
+  symbol_estimates_kernel<<<dim3((ue->nof_layers * 12 * ue->nof_rb + 255) / 256, 14, ue->nof_rx_ports), 256, 0,
+                            static_cast<cudaStream_t>(stream)>>>(*ue, reinterpret_cast<const float2*>(est), out, nd,
+                                                                 d0, d1);
+  return check_cuda(ctx, cudaGetLastError(), "symbol_estimates_kernel launch");
+}
+
+} // extern "C"

@@ -103,6 +103,12 @@ SIGNATURES = {
                                         ctypes.c_float, _VP, _VP]),
     "pg_demodulate_soft_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_demodulate_soft_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
+    "pg_pusch_est_size": (ctypes.c_size_t, [_VP]),
+    "pg_pusch_estimate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_pusch_symbol_estimates_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_demodulate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_process_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _VP,
+                                             _VP]),
 }
 
 _lib = None

@@ -216,3 +216,23 @@ def ulsch_encode(tb_bits, bg, qm, nof_layers, nof_ch_symbols, seg, rv=0, nref=0)
     g = np.concatenate(out)
     assert g.size == nof_ch_symbols * qm
     return g
+
+
+def _level(bits, m):
+    """Per-dimension Gray level of TS 38.211 Section 5.1 from bits[..., m] (MSB first)."""
+    t = np.ones(bits.shape[:-1], np.int32)
+    for k in range(m - 1, 0, -1):
+        t = (1 << (m - k)) - (1 - 2 * bits[..., k].astype(np.int32)) * t
+    return (1 - 2 * bits[..., 0].astype(np.int32)) * t
+
+
+def modulate(bits, qm):
+    """Bits [N*qm] -> complex64 symbols [N] (TS 38.211 Section 5.1, unit average energy)."""
+    b = np.asarray(bits, np.uint8).reshape(-1, qm)
+    if qm == 1:
+        return ((1 - 2.0 * b[:, 0]) * (1 + 1j) / np.sqrt(2)).astype(np.complex64)
+    m = qm // 2
+    energy = {1: 2.0, 2: 10.0, 3: 42.0, 4: 170.0}[m]
+    i = _level(b[:, 0::2], m)
+    q = _level(b[:, 1::2], m)
+    return ((i + 1j * q) / np.sqrt(energy)).astype(np.complex64)

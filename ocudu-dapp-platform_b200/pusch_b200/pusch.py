@@ -1,0 +1,109 @@
+"""PUSCH slot processing on the B200: Python mirror of ``ocudu::pusch_processor::process``
+(include/ocudu/phy/upper/channel_processors/pusch/pusch_processor.h:199-203) for batches of UEs,
+and access to the individual stages (DM-RS channel estimation, demodulation) on device buffers.
+All compute runs on the GPU through the C ABI; torch tensors are only device-memory plumbing."""
+import ctypes
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native
+from ._native import PgSchResult
+from .sim import PuschSlot, PuschUe, nof_ch_symbols
+
+
+class PgPuschUe(ctypes.Structure):
+    _fields_ = [("grid_offset", ctypes.c_uint32), ("grid_nof_subc", ctypes.c_uint32), ("llr_offset", ctypes.c_uint32),
+                ("est_offset", ctypes.c_uint32), ("tbs_bits", ctypes.c_uint32), ("tb_out_offset", ctypes.c_uint32),
+                ("nref", ctypes.c_uint32), ("dmrs_scaling", ctypes.c_float), ("rb_start", ctypes.c_uint16),
+                ("nof_rb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16), ("n_id", ctypes.c_uint16),
+                ("rnti", ctypes.c_uint16), ("n_id_data", ctypes.c_uint16), ("dc_subcarrier", ctypes.c_int16),
+                ("slot", ctypes.c_uint8), ("n_scid", ctypes.c_uint8), ("first_symbol", ctypes.c_uint8),
+                ("nof_symbols", ctypes.c_uint8), ("nof_rx_ports", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8),
+                ("modulation_order", ctypes.c_uint8), ("base_graph", ctypes.c_uint8), ("rv", ctypes.c_uint8),
+                ("max_iterations", ctypes.c_uint8)]
+
+
+class PgPortResult(ctypes.Structure):
+    _fields_ = [("noise_var", ctypes.c_float), ("epre", ctypes.c_float), ("snr", ctypes.c_float),
+                ("rsrp", ctypes.c_float * 2)]
+
+
+def make_ue_descriptors(slot: PuschSlot, max_iterations=6, grid_offset=0, dc_subcarrier=-1, tb_offset=0):
+    """pg_pusch_ue array for the UEs of one simulated slot (grid at grid_offset words)."""
+    n = len(slot.ues)
+    arr = (PgPuschUe * n)()
+    llr, est, tbo = 0, 0, tb_offset
+    for i, ue in enumerate(slot.ues):
+        d = arr[i]
+        d.grid_offset = grid_offset
+        d.grid_nof_subc = 12 * slot.nof_prb_grid
+        d.llr_offset = llr
+        d.est_offset = est
+        d.tbs_bits = ue.tbs_bits
+        d.tb_out_offset = tbo
+        d.nref = 0
+        d.dmrs_scaling = slot.dmrs_scaling
+        d.rb_start, d.nof_rb = ue.rb_start, ue.nof_rb
+        d.dmrs_symbol_mask = sum(1 << s for s in ue.dmrs_symbols)
+        d.n_id, d.rnti, d.n_id_data = ue.n_id, ue.rnti, ue.n_id_data
+        d.dc_subcarrier = dc_subcarrier
+        d.slot, d.n_scid, d.first_symbol, d.nof_symbols = slot.slot, 0, ue.first_symbol, ue.nof_symbols
+        d.nof_rx_ports, d.nof_layers, d.modulation_order = slot.nof_ports, ue.nof_layers, ue.modulation_order
+        d.base_graph, d.rv, d.max_iterations = ue.base_graph, ue.rv, max_iterations
+        llr += nof_ch_symbols(ue) * ue.modulation_order
+        est += slot.nof_ports * len(ue.dmrs_symbols) * ue.nof_layers * 12 * ue.nof_rb
+        tbo += ue.tbs_bits // 8
+    return arr, llr, est, tbo
+
+
+@dataclass
+class PuschResult:
+    tb_crc_ok: bool
+    transport_block: Optional[np.ndarray]
+    nof_codeblocks: int
+    nof_codeblocks_crc_ok: int
+    mean_iterations: float
+    noise_var: np.ndarray
+    rsrp: np.ndarray
+    snr: np.ndarray
+
+
+class PuschProcessor:
+    def __init__(self, context: _native.Context):
+        self.ctx = context
+        self.lib = _native.load()
+
+    def process_slots(self, slots: Sequence[PuschSlot], max_iterations=6, dc_subcarrier=-1) -> List[PuschResult]:
+        """Decodes every UE of every slot (one cell per slot) in one batched call."""
+        descs, grids, off_words, tb_off, ue_list = [], [], 0, 0, []
+        for sl in slots:
+            arr, _, _, tbo = make_ue_descriptors(sl, max_iterations, off_words, dc_subcarrier, tb_off)
+            descs.extend(arr[i] for i in range(len(sl.ues)))
+            grids.append(np.ascontiguousarray(sl.grid, np.uint32).ravel())
+            off_words += grids[-1].size
+            tb_off = tbo
+            ue_list.extend(sl.ues)
+        n = len(descs)
+        arr = (PgPuschUe * n)(*descs)
+        grid = np.concatenate(grids)
+        tb = np.zeros(max(tb_off, 1), np.uint8)
+        pr = (PgPortResult * (4 * n))()
+        res = (PgSchResult * n)()
+        rc = self.lib.pg_pusch_process_host(self.ctx.handle, ctypes.addressof(arr), n,
+                                            grid.ctypes.data_as(ctypes.c_void_p), grid.size,
+                                            tb.ctypes.data_as(ctypes.c_void_p), tb.size, ctypes.addressof(pr),
+                                            ctypes.addressof(res))
+        self.ctx.check(rc)
+        out = []
+        for i in range(n):
+            r = res[i]
+            p = [pr[4 * i + k] for k in range(descs[i].nof_rx_ports)]
+            o = descs[i].tb_out_offset
+            out.append(PuschResult(bool(r.tb_crc_ok),
+                                   tb[o:o + descs[i].tbs_bits // 8].copy() if r.tb_crc_ok else None,
+                                   int(r.nof_cbs), int(r.nof_cbs_crc_ok), float(r.mean_iterations),
+                                   np.array([q.noise_var for q in p]), np.array([[q.rsrp[0], q.rsrp[1]] for q in p]),
+                                   np.array([q.snr for q in p])))
+        return out

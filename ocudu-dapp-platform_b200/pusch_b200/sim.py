@@ -56,3 +56,114 @@ def ldpc_batch(seed=0, n=512, z=384, ebn0_range=(1.0, 3.0), llr_scale=4.0, max_i
     return LdpcBatch(jobs, truth, ebn0, bgs, info,
                      dict(seed=seed, n=n, z=z, ebn0_range=ebn0_range, llr_scale=llr_scale,
                           max_iterations=max_iterations))
+
+
+# ----------------------------------------------------------------------------------------------
+# PUSCH slots.
+
+@dataclass
+class PuschUe:
+    """One UE's PUSCH PDU in a slot (the fields the receive path needs)."""
+    rb_start: int
+    nof_rb: int
+    nof_layers: int
+    modulation_order: int
+    tbs_bits: int
+    base_graph: int = 1
+    rnti: int = 0x4601
+    n_id: int = 0           # DM-RS scrambling identity
+    n_id_data: int = 0      # data scrambling identity
+    rv: int = 0
+    dmrs_symbols: tuple = (2,)
+    first_symbol: int = 0
+    nof_symbols: int = 14
+    snr_db: float = 10.0
+    channel: str = "flat"   # "flat": one CN(0,1) coefficient per (port, layer); "pdp": exponential PDP
+    rms_delay_ns: float = 100.0
+    nof_taps: int = 8
+
+
+@dataclass
+class PuschSlot:
+    grid: np.ndarray                 # uint32 complex bf16 [port][14][12*nof_prb_grid]
+    ues: list
+    truth: list                      # transport-block bits per UE
+    nof_ports: int
+    nof_prb_grid: int
+    slot: int
+    scs_khz: int = 30
+    dmrs_scaling: float = float(np.float32(10 ** (3 / 20)))  # two CDM groups without data: +3 dB DM-RS
+    channels: list = field(default_factory=list)
+    noise_vars: list = field(default_factory=list)
+
+
+def data_symbol_list(ue):
+    return [s for s in range(ue.first_symbol, ue.first_symbol + ue.nof_symbols) if s not in ue.dmrs_symbols]
+
+
+def nof_ch_symbols(ue):
+    """Channel symbols of the codeword over all layers (no data on DM-RS symbols)."""
+    return len(data_symbol_list(ue)) * 12 * ue.nof_rb * ue.nof_layers
+
+
+def channel_response(rng, ue, nof_ports, scs_khz):
+    """Frequency response H [port][layer][12*nof_rb] over the allocation, constant in time."""
+    nsc = 12 * ue.nof_rb
+    if ue.channel == "flat":
+        h = (rng.standard_normal((nof_ports, ue.nof_layers)) + 1j * rng.standard_normal((nof_ports, ue.nof_layers)))
+        return np.repeat((h / np.sqrt(2))[..., None], nsc, axis=-1)
+    # Exponential power-delay profile with the given RMS delay spread, nof_taps equally spaced taps
+    # up to 3 RMS delays, unit total power, independent Rayleigh taps per (port, layer).
+    tau = np.linspace(0, 3 * ue.rms_delay_ns * 1e-9, ue.nof_taps)
+    p = np.exp(-tau / (ue.rms_delay_ns * 1e-9))
+    p /= p.sum()
+    f = (np.arange(nsc) + 12 * ue.rb_start) * scs_khz * 1e3
+    taps = (rng.standard_normal((nof_ports, ue.nof_layers, ue.nof_taps))
+            + 1j * rng.standard_normal((nof_ports, ue.nof_layers, ue.nof_taps))) * np.sqrt(p / 2)
+    return np.einsum("plt,tf->plf", taps, np.exp(-2j * np.pi * tau[:, None] * f[None, :]))
+
+
+def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30):
+    """Seeded uplink slot: for each UE, random TB -> UL-SCH coding -> scrambling -> modulation ->
+    layer mapping -> RE mapping with DM-RS (type 1, amplitude +3 dB) -> channel -> AWGN; the
+    grid is rounded to complex bf16 (the reference's resource-grid storage)."""
+    from . import prg
+    from .demod import to_cbf16
+    from .sch import segment
+
+    rng = np.random.default_rng(seed)
+    nsc_grid = 12 * nof_prb_grid
+    grid = np.zeros((nof_ports, 14, nsc_grid), np.complex128)
+    truth, chans, nvs = [], [], []
+    beta = float(np.float32(10 ** (3 / 20)))
+    for ue in ues:
+        ncs = nof_ch_symbols(ue)
+        seg = segment(ue.tbs_bits, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs)
+        tb = rng.integers(0, 2, ue.tbs_bits, dtype=np.uint8)
+        cw = codec.ulsch_encode(tb, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs, seg, rv=ue.rv)
+        cw = cw ^ prg.scrambling(ue.rnti, ue.n_id_data, cw.size)
+        d = codec.modulate(cw, ue.modulation_order)              # [ncs]
+        nre_sym = 12 * ue.nof_rb
+        x = d.reshape(-1, ue.nof_layers)                          # [RE][layer]
+        h = channel_response(rng, ue, nof_ports, scs_khz)         # [P][L][nsc]
+        sc = slice(12 * ue.rb_start, 12 * (ue.rb_start + ue.nof_rb))
+        r = 0
+        for s in range(ue.first_symbol, ue.first_symbol + ue.nof_symbols):
+            if s in ue.dmrs_symbols:
+                pil = prg.dmrs_type1(slot, s, ue.n_id, ue.rb_start, ue.nof_rb, ue.nof_layers) * beta
+                tx = np.zeros((ue.nof_layers, nre_sym), np.complex128)
+                tx[:, 0::2] = pil
+            else:
+                tx = x[r:r + nre_sym].T
+                r += nre_sym
+            grid[:, s, sc] += np.einsum("plf,lf->pf", h, tx)
+        # Noise: SNR per receive port relative to unit per-layer signal power.
+        nv = 10 ** (-ue.snr_db / 10)
+        for s in range(ue.first_symbol, ue.first_symbol + ue.nof_symbols):
+            grid[:, s, sc] += np.sqrt(nv / 2) * (rng.standard_normal((nof_ports, nre_sym))
+                                                + 1j * rng.standard_normal((nof_ports, nre_sym)))
+        truth.append(tb)
+        chans.append(h)
+        nvs.append(nv)
+    return PuschSlot(to_cbf16(grid.astype(np.complex64)), list(ues), truth, nof_ports, nof_prb_grid, slot, scs_khz,
+                     beta, chans, nvs)

@@ -55,6 +55,9 @@ class Ref:
         lib.ref_ldpc_decode_batch_mt.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         lib.ref_ldpc_decode_batch_mt.restype = ctypes.c_double
+        lib.ref_port_estimate.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 9 + [ctypes.c_uint32, ctypes.c_float,
+                                                                                 ctypes.c_void_p, ctypes.c_void_p,
+                                                                                 ctypes.c_void_p]
         lib.ref_equalize.argtypes = [ctypes.c_int] * 4 + [ctypes.c_void_p] * 3 + [ctypes.c_float, ctypes.c_void_p,
                                                                                    ctypes.c_void_p]
         self.lib = lib
@@ -128,6 +131,22 @@ class Ref:
         self.lib.ref_equalize(algorithm, nre, nports, nl, _ptr(y), _ptr(h), _ptr(nv), ctypes.c_float(tx_scaling),
                               _ptr(eq), _ptr(var))
         return eq, var
+
+    def port_estimate(self, grid, port, slot, n_id, rb_start, nof_rb, nof_layers, dmrs_symbols, scaling, n_scid=0):
+        """The reference's port estimator (FD filter, TD interpolate). grid: uint32 cbf16
+        [nports][14][nsubc]. Returns (freq complex64 [nd][nl][12 nof_rb] (FP32 internal),
+        symbol estimates uint32 cbf16 [14][nl][12 nof_rb], dict of scalars)."""
+        g = np.ascontiguousarray(grid, np.uint32)
+        nports, _, nsubc = g.shape
+        nd = len(dmrs_symbols)
+        freq = np.zeros((nd, nof_layers, 12 * nof_rb), np.complex64)
+        sym = np.zeros((14, nof_layers, 12 * nof_rb), np.uint32)
+        sc = np.zeros(3 + nof_layers, np.float32)
+        mask = sum(1 << s for s in dmrs_symbols)
+        self.lib.ref_port_estimate(_ptr(g), nports, nsubc, port, slot, n_id, n_scid, rb_start, nof_rb, nof_layers, mask,
+                                   ctypes.c_float(scaling), _ptr(freq), _ptr(sym), _ptr(sc))
+        return freq, sym, dict(noise_var=float(sc[0]), epre=float(sc[1]), snr=float(sc[2]),
+                               rsrp=sc[3:].astype(np.float64))
 
     def sch_segmentation(self, tbs_bits, bg):
         o = np.zeros(4, np.int32)

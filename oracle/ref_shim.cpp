@@ -22,7 +22,18 @@
 #include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_tx.h"
 #include "ocudu/phy/upper/channel_modulation/channel_modulation_factories.h"
 #include "ocudu/phy/upper/channel_modulation/demodulation_mapper.h"
+#include "ocudu/phy/generic_functions/generic_functions_factories.h"
 #include "ocudu/phy/support/re_buffer.h"
+#include "ocudu/phy/support/resource_grid_reader.h"
+#include "ocudu/phy/support/time_alignment_estimator/time_alignment_estimator_factories.h"
+#include "ocudu/phy/upper/sequence_generators/sequence_generator_factories.h"
+#include "ocudu/phy/upper/signal_processors/channel_estimator/factories.h"
+#include "lib/phy/upper/signal_processors/dmrs_helper.h"
+// The estimator's FP32 frequency response (before the conversion to bf16 of its public
+// interface) is a private member; the checker reads it directly.
+#define private public
+#include "lib/phy/upper/signal_processors/channel_estimator/port_channel_estimator_average_impl.h"
+#undef private
 #include "ocudu/phy/upper/equalization/dynamic_ch_est_list.h"
 #include "ocudu/phy/upper/equalization/equalization_factories.h"
 #include "ocudu/ran/sch/sch_segmentation.h"
@@ -420,6 +431,167 @@ int ref_equalize(int             algorithm,
                est,
                span<const float>(noise_var_per_port, nof_ports),
                tx_scaling);
+  return 0;
+}
+
+} // extern "C"
+
+namespace {
+
+/// Read-only resource grid over caller memory: cbf16 [port][symbol][subcarrier].
+class array_grid_reader : public resource_grid_reader
+{
+public:
+  array_grid_reader(const uint32_t* data, unsigned nports, unsigned nsymb, unsigned nsubc) :
+    data_(reinterpret_cast<const cbf16_t*>(data)), nports_(nports), nsymb_(nsymb), nsubc_(nsubc)
+  {
+  }
+  unsigned     get_nof_ports() const override { return nports_; }
+  unsigned     get_nof_subc() const override { return nsubc_; }
+  unsigned     get_nof_symbols() const override { return nsymb_; }
+  bool         is_empty(unsigned) const override { return false; }
+  bool         is_empty() const override { return false; }
+  crb_interval get_allocation_range(unsigned, unsigned) const override { return {0, nsubc_ / 12}; }
+  span<cf_t>   get(span<cf_t> symbols, unsigned port, unsigned l, unsigned k_init, const bounded_bitset<MAX_NOF_SUBCARRIERS>& mask) const override
+  {
+    mask.for_each(0, mask.size(), [&](unsigned k) {
+      symbols.front() = to_cf(view(port, l)[k_init + k]);
+      symbols         = symbols.last(symbols.size() - 1);
+    });
+    return symbols;
+  }
+  span<cbf16_t> get(span<cbf16_t> symbols, unsigned port, unsigned l, unsigned k_init, const bounded_bitset<MAX_NOF_SUBCARRIERS>& mask) const override
+  {
+    mask.for_each(0, mask.size(), [&](unsigned k) {
+      symbols.front() = view(port, l)[k_init + k];
+      symbols         = symbols.last(symbols.size() - 1);
+    });
+    return symbols;
+  }
+  void get(span<cf_t> symbols, unsigned port, unsigned l, unsigned k_init, unsigned stride) const override
+  {
+    for (unsigned i = 0; i != symbols.size(); ++i) {
+      symbols[i] = to_cf(view(port, l)[k_init + i * stride]);
+    }
+  }
+  void get(span<cbf16_t> symbols, unsigned port, unsigned l, unsigned k_init) const override
+  {
+    std::copy_n(view(port, l).begin() + k_init, symbols.size(), symbols.begin());
+  }
+  span<const cbf16_t> get_view(unsigned port, unsigned l) const override { return view(port, l); }
+
+private:
+  span<const cbf16_t> view(unsigned port, unsigned l) const
+  {
+    return span<const cbf16_t>(data_ + ((size_t)port * nsymb_ + l) * nsubc_, nsubc_);
+  }
+  const cbf16_t* data_;
+  unsigned       nports_, nsymb_, nsubc_;
+};
+
+} // namespace
+
+extern "C" {
+
+/// One receive port of the reference's DM-RS PUSCH channel estimator
+/// (port_channel_estimator::compute, FD "filter", TD "interpolate", no CFO compensation), type-1
+/// DM-RS on layers 0..nof_layers-1, pilots generated as dmrs_pusch_estimator_impl does
+/// (pseudo-random c_init per symbol, OCC of port 1). grid: cbf16 [nports][14][nsubc].
+/// Outputs: freq (complex float [nof_dmrs][nof_layers][12*nof_rb], the FP32 response),
+/// sym_est (cbf16 [14][nof_layers][12*nof_rb], the public per-symbol estimates) and
+/// scalars {noise_var, epre, snr, rsrp[layer]...}.
+int ref_port_estimate(const uint32_t* grid,
+                      int             nports,
+                      int             nsubc,
+                      int             port,
+                      int             slot,
+                      int             n_id,
+                      int             n_scid,
+                      int             rb_start,
+                      int             nof_rb,
+                      int             nof_layers,
+                      uint32_t        dmrs_symbol_mask,
+                      float           scaling,
+                      float*          freq,
+                      uint32_t*       sym_est,
+                      float*          scalars)
+{
+  array_grid_reader reader(grid, nports, 14, nsubc);
+  auto              prg = create_pseudo_random_generator_sw_factory()->create();
+
+  port_channel_estimator::configuration cfg;
+  cfg.scs          = subcarrier_spacing::kHz30;
+  cfg.cp           = cyclic_prefix::NORMAL;
+  cfg.first_symbol = 0;
+  cfg.nof_symbols  = 14;
+  cfg.scaling      = scaling;
+  cfg.rx_ports.push_back(static_cast<uint8_t>(port));
+  bounded_bitset<MAX_NSYMB_PER_SLOT> symbols(14);
+  for (int s = 0; s < 14; ++s) {
+    if ((dmrs_symbol_mask >> s) & 1u) {
+      symbols.set(s);
+    }
+  }
+  crb_bitmap rb_mask(rb_start + nof_rb);
+  rb_mask.fill(rb_start, rb_start + nof_rb);
+  unsigned nof_dmrs = symbols.count();
+  unsigned npil     = 6 * nof_rb;
+
+  dmrs_symbol_list pilots({npil, nof_dmrs, static_cast<unsigned>(nof_layers)});
+  for (int s = 0, i = 0; s < 14; ++s) {
+    if (!symbols.test(s)) {
+      continue;
+    }
+    unsigned c_init = ((14 * slot + s + 1) * (2 * n_id + 1) * (1U << 17) + (2 * n_id + n_scid)) % (1U << 31);
+    prg->init(c_init);
+    dmrs_sequence_generate(pilots.get_symbol(i, 0), *prg, M_SQRT1_2, 0, 6, rb_mask);
+    ++i;
+  }
+  for (int l = 1; l < nof_layers; ++l) {
+    dmrs_pxsch_parameters params = get_pxsch_dmrs_params(dmrs_config_type::type1, l);
+    for (unsigned i = 0; i != nof_dmrs; ++i) {
+      span<cf_t>       d  = pilots.get_symbol(i, l);
+      span<const cf_t> d0 = pilots.get_symbol(i, 0);
+      std::copy(d0.begin(), d0.end(), d.begin());
+      if (params.w_f[0] != params.w_f[1]) {
+        for (unsigned k = 1; k < d.size(); k += 2) {
+          d[k] *= params.w_f[1];
+        }
+      }
+    }
+  }
+  for (int l = 0; l < nof_layers; ++l) {
+    dmrs_pxsch_parameters params = get_pxsch_dmrs_params(dmrs_config_type::type1, l);
+    cfg.dmrs_pattern.push_back({symbols, rb_mask, {}, std::nullopt, params.re_pattern});
+  }
+
+  auto ta_factory = create_time_alignment_estimator_dft_factory(create_dft_processor_factory_generic());
+  auto factory    = create_port_channel_estimator_factory_sw(ta_factory);
+  auto est        = factory->create(port_channel_estimator_fd_smoothing_strategy::filter,
+                             port_channel_estimator_td_interpolation_strategy::interpolate,
+                             false);
+  const port_channel_estimator_results& res = est->compute(reader, 0, pilots, cfg);
+
+  auto* impl = dynamic_cast<port_channel_estimator_average_impl*>(est.get());
+  for (unsigned d = 0; d != nof_dmrs; ++d) {
+    for (int l = 0; l < nof_layers; ++l) {
+      span<const cf_t> fr = impl->freq_response_hop0.get_symbol(d, l);
+      std::memcpy(freq + ((size_t)d * nof_layers + l) * 2 * fr.size(), fr.data(), fr.size() * sizeof(cf_t));
+    }
+  }
+  unsigned nsc = 12 * nof_rb;
+  for (int s = 0; s < 14; ++s) {
+    for (int l = 0; l < nof_layers; ++l) {
+      res.get_symbol_ch_estimate(
+          span<cbf16_t>(reinterpret_cast<cbf16_t*>(sym_est) + ((size_t)s * nof_layers + l) * nsc, nsc), s, l);
+    }
+  }
+  scalars[0] = res.get_noise_variance();
+  scalars[1] = res.get_epre();
+  scalars[2] = res.get_snr();
+  for (int l = 0; l < nof_layers; ++l) {
+    scalars[3 + l] = res.get_rsrp(l);
+  }
   return 0;
 }
 

@@ -190,6 +190,31 @@ def eq_cases(ref, rng):
     return out
 
 
+def est_cases(ref):
+    from pusch_b200 import sim
+    out = {}
+    cases = [dict(rb_start=3, nof_rb=51, nof_layers=1, ports=2, dmrs=(2,), channel="flat", snr=10.0),
+             dict(rb_start=10, nof_rb=20, nof_layers=2, ports=4, dmrs=(2, 11), channel="pdp", snr=20.0),
+             dict(rb_start=0, nof_rb=1, nof_layers=1, ports=1, dmrs=(3,), channel="flat", snr=5.0),
+             dict(rb_start=57, nof_rb=2, nof_layers=2, ports=2, dmrs=(2, 11), channel="pdp", snr=15.0)]
+    beta = float(np.float32(10 ** (3 / 20)))
+    for i, c in enumerate(cases):
+        ue = sim.PuschUe(rb_start=c["rb_start"], nof_rb=c["nof_rb"], nof_layers=c["nof_layers"], modulation_order=2,
+                         tbs_bits=24 if c["nof_rb"] < 3 else 1000, base_graph=2, dmrs_symbols=c["dmrs"],
+                         snr_db=c["snr"], channel=c["channel"], n_id=17 * i, rnti=0x4601 + i)
+        slot = sim.make_pusch_slot([ue], c["ports"], nof_prb_grid=60, slot=i + 1, seed=100 + i)
+        out[f"c{i}_meta"] = np.array([c["rb_start"], c["nof_rb"], c["nof_layers"], c["ports"], i + 1, 17 * i,
+                                      0x4601 + i, sum(1 << s for s in c["dmrs"])], np.int32)
+        out[f"c{i}_grid"] = slot.grid
+        for p in range(c["ports"]):
+            freq, sym, sc = ref.port_estimate(slot.grid, p, i + 1, 17 * i, c["rb_start"], c["nof_rb"], c["nof_layers"],
+                                              list(c["dmrs"]), beta)
+            out[f"c{i}_p{p}_freq"] = freq
+            out[f"c{i}_p{p}_sym"] = sym
+            out[f"c{i}_p{p}_scalars"] = np.array([sc["noise_var"], sc["epre"], sc["snr"], *sc["rsrp"]], np.float64)
+    return out
+
+
 def main():
     ref = Ref()
     rng = np.random.default_rng(20261203)
@@ -199,6 +224,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "ldpc_encode.npz"), **enc_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "demap.npz"), **demap_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "equalize.npz"), **eq_cases(ref, rng))
+    np.savez_compressed(os.path.join(OUT, "estimate.npz"), **est_cases(ref))
     print("golden fixtures written; reference LDPC variant:", ref.variant)
 
 

@@ -75,3 +75,18 @@ def eq_cases():
                         tx=float(d[f"c{i}_tx"][0]), eq=d[f"c{i}_eq"], var=d[f"c{i}_var"]))
         i += 1
     return out
+
+
+def est_cases():
+    d = load("estimate.npz")
+    out, i = [], 0
+    while f"c{i}_meta" in d:
+        rb0, nrb, nl, ports, slot, n_id, rnti, mask = (int(x) for x in d[f"c{i}_meta"])
+        dm = [s for s in range(14) if (mask >> s) & 1]
+        out.append(dict(rb_start=rb0, nof_rb=nrb, nof_layers=nl, ports=ports, slot=slot, n_id=n_id, rnti=rnti,
+                        dmrs=dm, grid=d[f"c{i}_grid"],
+                        freq=[d[f"c{i}_p{p}_freq"] for p in range(ports)],
+                        sym=[d[f"c{i}_p{p}_sym"] for p in range(ports)],
+                        scalars=[d[f"c{i}_p{p}_scalars"] for p in range(ports)]))
+        i += 1
+    return out
