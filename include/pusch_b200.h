@@ -97,6 +97,26 @@ int pg_ldpc_decode_batch_device(pg_context* ctx, const pg_ldpc_cb* cbs, int nof_
 int pg_ldpc_decode_batch_resident(pg_context* ctx, const pg_ldpc_cb* cbs_dev, int nof_cbs, const int8_t* llrs,
                                   uint8_t* bits, int32_t* iterations, void* stream);
 
+/* Largest batch pg_ldpc_decode_batch_static_scratch accepts: its check-to-variable scratch is a
+ * fixed device array of this many codeblocks of BG1 at Z = 384 (121,344 bytes each, 7.4 MiB). */
+#define PG_STATIC_SCRATCH_MAX_CODEBLOCKS 64
+
+/* No counterpart in the reference: an addition of this library. Same decode as
+ * pg_ldpc_decode_batch_resident (descriptors already in device memory, same results), but the
+ * call allocates no device memory and does not use the context's scratch: the check-to-variable
+ * messages live in a device array of the library module, reserved when the module loads, so the
+ * batch is bounded by PG_STATIC_SCRATCH_MAX_CODEBLOCKS instead of the context's max_codeblocks;
+ * larger batches fail with PG_ERR_CAPACITY. For callers that must not allocate while decoding:
+ * a real-time PHY worker under a slot deadline, where an allocation's driver locks and device
+ * synchronisation have no latency bound, and a process whose device memory was reserved at
+ * start-up, which must not meet out-of-memory during traffic.
+ * The first call on each device looks up the array's device address; make that first call before
+ * any stream capture begins. All calls on a device share the one array: calls whose kernels may
+ * overlap in time (different streams without ordering, several host threads) race on it, so
+ * order them on one stream or synchronise between them. */
+int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldpc_cb* cbs_dev, int nof_cbs, const int8_t* llrs,
+                                        uint8_t* bits, int32_t* iterations, void* stream);
+
 /* Same, from and to host memory (H2D of the LLRs and D2H of bits and iterations inside the
  * call). This is what the ldpc_decoder / pusch_resident_codeblock_decoder::decode_batch
  * adapters call (include/ocudu/phy/upper/channel_processors/pusch/

@@ -23,6 +23,7 @@
 #include "pg_internal.h"
 
 #include <cstdio>
+#include <mutex>
 
 namespace pg {
 #include "ldpc_base_graphs.inc"
@@ -504,3 +505,91 @@ int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_
 }
 
 } // namespace pg
+
+// ---------------------------------------------------------------------------------------------
+// Decoding with a module-static check-to-variable scratch (pg_ldpc_decode_batch_static_scratch).
+//
+// Some callers cannot allocate device memory while they decode: a PHY worker that has to finish
+// each slot by its deadline (cudaMalloc / cudaFree take driver locks and may synchronise the whole
+// device, so their latency has no useful bound), and a process that reserved its device memory
+// when it started and must not run into out-of-memory in the middle of traffic. For them the
+// scratch is a device array of this module, reserved by the driver when the module loads: room for
+// PG_STATIC_SCRATCH_MAX_CODEBLOCKS codeblocks of the largest graph (BG1, Z = 384).
+//
+// Nothing in the array has to start at zero: the first layered iteration of each codeblock writes
+// every check-to-variable message of the rows it processes before any later iteration reads one,
+// so what an earlier call left behind is never read. Every call on a device uses the same array;
+// kernels of two calls that run at the same time race on it.
+
+static __device__ __align__(256) int8_t g_static_c2v[(size_t)PG_STATIC_SCRATCH_MAX_CODEBLOCKS * pg::kC2vStride];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex    g_static_mu;
+int8_t*       g_static_c2v_addr[kStaticMaxDevices] = {};
+
+// Device address of g_static_c2v on ctx->device, looked up on the first call per device; the
+// caller has made ctx->device current.
+int static_scratch_address(pg_context* ctx, int8_t** out)
+{
+  if (ctx->device < 0 || ctx->device >= kStaticMaxDevices) {
+    return pg::set_error(ctx, PG_ERR_INVALID, "device ordinal beyond the static scratch table");
+  }
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (g_static_c2v_addr[ctx->device] == nullptr) {
+    int8_t* ptr = nullptr;
+    if (int rc = pg::check_cuda(ctx, cudaGetSymbolAddress((void**)&ptr, g_static_c2v),
+                                "cudaGetSymbolAddress(static check-to-variable scratch)")) {
+      return rc;
+    }
+    g_static_c2v_addr[ctx->device] = ptr;
+  }
+  *out = g_static_c2v_addr[ctx->device];
+  return PG_OK;
+}
+
+} // namespace
+
+extern "C" int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldpc_cb* cbs_dev, int nof_cbs,
+                                                   const int8_t* llrs, uint8_t* bits, int32_t* iterations,
+                                                   void* stream)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (nof_cbs < 0) {
+    return pg::set_error(ctx, PG_ERR_INVALID, "negative codeblock count");
+  }
+  if (nof_cbs > PG_STATIC_SCRATCH_MAX_CODEBLOCKS) {
+    return pg::set_error(ctx, PG_ERR_CAPACITY,
+                         "batch of " + std::to_string(nof_cbs) + " codeblocks exceeds the static scratch limit of " +
+                             std::to_string(PG_STATIC_SCRATCH_MAX_CODEBLOCKS) + " codeblocks per call");
+  }
+  if (nof_cbs == 0) {
+    return PG_OK;
+  }
+  if (cbs_dev == nullptr || llrs == nullptr || bits == nullptr || iterations == nullptr) {
+    return pg::set_error(ctx, PG_ERR_INVALID, "null device buffer");
+  }
+  int prev = -1;
+  if (int rc = pg::check_cuda(ctx, cudaGetDevice(&prev), "cudaGetDevice")) {
+    return rc;
+  }
+  if (prev != ctx->device) {
+    if (int rc = pg::check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice")) {
+      return rc;
+    }
+  }
+  int8_t* scratch = nullptr;
+  int     rc      = static_scratch_address(ctx, &scratch);
+  if (rc == PG_OK) {
+    ldpc_decode_kernel<<<nof_cbs, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(cbs_dev, llrs, bits, iterations,
+                                                                                     scratch, ctx->dev.crc_pow);
+    rc = pg::check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch (static scratch)");
+  }
+  if (prev != ctx->device) {
+    cudaSetDevice(prev);
+  }
+  return rc;
+}

@@ -83,6 +83,7 @@ SIGNATURES = {
     "pg_last_error": (ctypes.c_char_p, [_VP]),
     "pg_ldpc_decode_batch_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_ldpc_decode_batch_resident": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_ldpc_decode_batch_static_scratch": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_ldpc_decode_batch_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP,
                                                  ctypes.c_size_t, _VP]),
     "pg_ldpc_output_bytes": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
