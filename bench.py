@@ -1,21 +1,27 @@
 #!/usr/bin/env python3
-"""Benchmark of the B200 PUSCH receive path: the LDPC decoder batch workload.
+"""Benchmark of the B200 PUSCH receive path.
 
-Workload (one "step"): decode one batch of 512 codeblocks - BG1 Z=384 (K=8448, E=N=25344, rate
-1/3) and BG2 Z=384 (K=3840, E=N=19200, rate 1/5) mixed 50/50 by seed - of random bits with
-CRC24B, BPSK over AWGN at Eb/N0 ~ U[1, 3] dB, int8 LLRs saturated at +-127, at most 10
-iterations with CRC early stop. The metric is decoded information Gbit/s (K - 24 bits of every
-CRC-passing codeblock per second).
+Default workload (one "step"): the batched uneven slot - 16 cells of 100 MHz / 273 PRB, each with
+1-16 UEs on contiguous PRB allocations, QPSK-256QAM (MCS table 2), 1-2 layers, 4 rx ports,
+per-UE SNR U[0, 30] dB with link adaptation to BLER <= 10 %, DM-RS type 1 at symbols 2 and 11,
+exponential-PDP channels (100 ns RMS, 8 taps), max 6 LDPC iterations - decoded through one slot
+plan (DM-RS estimation, demodulation, rate dematching, LDPC, TB assembly and CRC; one CUDA graph
+replayed per step). The metric is decoded Mbit/s: the TBS of every UE whose TB CRC passes (and
+equals the transmitted bits), per second of device time, inputs resident in HBM, L2 flushed
+between steps.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+The line also carries: the plain per-UE GPU path on the same slot (one plan per UE, executed one
+after another with the host waiting for each UE's result); the end-to-end value through the host
+entry (pg_pusch_plan_execute_host: pinned host grids in, TBs and results out, every step); the
+integer roofline of the dominant kernel (ldpc_decode_kernel, CUDA-event time inside the step);
+the LDPC decoder batch (512 codeblocks, BG1/BG2 Z=384) in Gbit/s; clocks sampled during the timed
+region; and the reference's CPU receive path (oracle/_ref, the reference's own stage objects) on
+this host's cores as cpu_baseline.
 
-Our arm prints one JSON line with the device-timed value (inputs resident in HBM, one kernel
-launch per step, L2 flushed between steps), the end-to-end value through the host C ABI
-(pg_ldpc_decode_batch_host: pinned host LLRs in, bits and iteration counts out, every step),
-the integer-ALU roofline of the decoding kernel, clocks sampled during the timed region and the
-reference CPU decoder timed on this host. ``--impl reference`` times the reference's own CPU
-LDPC decoder (oracle/_ref, AVX-512/AVX2) on all host cores on the same workload.
-Under torchrun each rank decodes its own batch (seed + rank): weak scaling, no data-path
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload uneven|ldpc]
+
+``--impl reference`` times the reference's CPU receive path on all host cores on the same
+workload. Under torchrun each rank decodes its own slot (seed + rank): weak scaling, no data-path
 collective; rank 0 reports the aggregate over the max per-rank time.
 """
 import argparse
@@ -32,6 +38,13 @@ sys.path.insert(0, os.path.join(ROOT, "ocudu-dapp-platform_b200"))
 
 METRIC = "PUSCH Mbit/s/B200 batched+learned vs plain GPU at BLER≤10%; LDPC Gbit/s"
 N_CBS = 512
+N_CELLS = 16
+MAX_ITER = 6
+PUSCH_WORKLOAD = ("Batched uneven slot: 16 cells x 273 PRB (100 MHz, 30 kHz SCS), 1-16 UEs per cell on contiguous "
+                  "PRB allocations, QPSK-256QAM (MCS table 2) with link adaptation to BLER<=10%, 1-2 layers, 4 rx, "
+                  "per-UE SNR U[0,30] dB, DM-RS type 1 symbols {2,11}, exponential PDP (100 ns RMS, 8 taps), "
+                  "max 6 LDPC iterations, CRC early stop")
+KERNELS_PER_PLAN = 6  # estimate, demodulate, rate dematch, LDPC, TB assembly, results
 WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) and BG2 Z=384 (K=3840, rate 1/5) "
             "mixed 50/50 by seed, CRC24B, BPSK/AWGN Eb/N0 U[1,3] dB, int8 LLRs (scale 4/LLR unit, sat +-127), "
             "max 10 iterations, CRC early stop")
@@ -41,13 +54,16 @@ INT_OPS_PER_EDGE = 10  # algorithmic integer operations per edge update (see DES
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="uneven", choices=["uneven", "ldpc"])
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-ldpc", action="store_true")
     return p.parse_args()
 
 
@@ -139,6 +155,301 @@ def workload_stats(batch, iters):
     return bits_ok, bits_all, ops, edge_updates
 
 
+def pusch_edge_updates(ues, results):
+    """Algorithmic LDPC edge updates of one slot: per codeblock, the check rows its input covers
+    (trailing-zero trimming of the dematched buffer: E + F significant positions at rv 0) times
+    the row edges times Z, times the UE's iterations run (failed codeblocks count the maximum)."""
+    from pusch_b200 import codec
+    from pusch_b200.sch import segment
+    from pusch_b200.sim import nof_ch_symbols
+    total = 0
+    for ue, r in zip(ues, results):
+        g = nof_ch_symbols(ue) * ue.modulation_order
+        sg = segment(ue.tbs_bits, ue.base_graph, ue.modulation_order, ue.nof_layers, g // ue.modulation_order)
+        z, kb = sg["lifting_size"], (22 if ue.base_graph == 1 else 10)
+        n = (66 if ue.base_graph == 1 else 50) * z
+        deg, _, _ = codec.base_graph(ue.base_graph)
+        edges = 0
+        for c in range(sg["nof_cbs"]):
+            e = sg["e_short"] if c < sg["nof_short_cbs"] else sg["e_long"]
+            n_in = min(e + sg["nof_filler_bits"], n)
+            cb_len = max(n_in + 2 * z, kb * z + 4 * z)
+            cb_len = -(-cb_len // z) * z
+            rows = min(cb_len // z - kb, 46 if ue.base_graph == 1 else 42)
+            edges += int(deg[:rows].sum()) * z
+        total += edges * r.mean_iterations
+    return int(total)
+
+
+def int_peak(dev):
+    """Measured full-rate int32 instruction throughput (ops/s) of this GPU and the per-class
+    figures (libpg_probe.so), or (None, None)."""
+    import ctypes
+    try:
+        probe = ctypes.CDLL(os.path.join(ROOT, "ocudu-dapp-platform_b200", "pusch_b200", "_lib", "libpg_probe.so"))
+        probe.pg_probe_inst_classes.argtypes = [ctypes.c_int, ctypes.c_void_p]
+        buf = (ctypes.c_double * 8)()
+        if probe.pg_probe_inst_classes(dev, buf) == 0:
+            names = ["add.s32", "min.s32", "mad.lo.u32", "prmt.b32", "min.s16x2", "add.f16x2", "min.f16x2",
+                     "fma.f16x2"]
+            return max(buf[0], buf[1]), {n: round(buf[i] / 1e12, 2) for i, n in enumerate(names)}
+    except OSError:
+        pass
+    return None, None
+
+
+def reference_pusch(slots, seconds, cores, min_passes=1):
+    """The reference's CPU receive path (oracle/_ref: the reference's own stage objects, one UE
+    per thread) over the whole slot until `seconds` of decoding are timed. Returns (decoded bits
+    of the last pass, timed seconds, passes, UEs per pass)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Ref  # CPU baseline only
+    from pusch_b200.pusch import batch_descriptors
+    ref = Ref()
+    descs, grid, tb_bytes, ues = batch_descriptors(slots, max_iterations=MAX_ITER)
+    total, passes, bits = 0.0, 0, 0
+    while True:
+        ok, _, _, dt = ref.pusch_decode_mt(descs, grid, tb_bytes, cores)
+        total += dt
+        passes += 1
+        bits = int(sum(u.tbs_bits for u, o in zip(ues, ok) if o))
+        if passes >= min_passes and total >= seconds:
+            break
+    return bits, total, passes, len(ues)
+
+
+def run_reference_pusch(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    slots = pusch_workload(args.seed)
+    cores = host_cores()
+    reference_pusch(slots, 0.0, cores, min_passes=max(args.warmup, 1))
+    times, bits, n_ues = [], 0, 0
+    for _ in range(args.steps):
+        b, dt, _, n_ues = reference_pusch(slots, 0.0, cores, min_passes=1)
+        times.append(dt)
+        bits = b
+    ms = 1e3 * statistics.mean(times)
+    value = bits / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mbit/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32/int8", "data": "synthetic (seeded simulator)", "impl": "reference",
+        "config": {"workload": PUSCH_WORKLOAD, "cells": N_CELLS, "ues": n_ues},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mbit/s", "cores": cores, "kind": "reference",
+                         "sample": f"the full {N_CELLS}-cell slot ({n_ues} UEs) per step through the reference's CPU "
+                                   f"stage objects (oracle/_ref) on {cores} C++ threads, one UE per thread at a time"},
+        "e2e": {"value": round(value, 3), "unit": "Mbit/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def pusch_workload(seed):
+    from pusch_b200 import sim
+    return sim.uneven_cells(seed=seed, nof_cells=N_CELLS)
+
+
+def run_ours_pusch(args):
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    rank, world, dev = dist_setup()
+
+    from pusch_b200 import _native
+    from pusch_b200._native import PgSchResult
+    from pusch_b200.pusch import PuschSlotPlan, results_from
+
+    slots = pusch_workload(args.seed + rank)
+    truth = [t for sl in slots for t in sl.truth]
+    ctx = _native.Context(device=dev, max_codeblocks=64)
+    plan = PuschSlotPlan(ctx, slots, max_iterations=MAX_ITER, graph=True)
+    n = plan.n
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+    d_grid = torch.from_numpy(plan.grid.view(np.int32)).cuda()
+    d_tb = torch.zeros(max(plan.tb_bytes, 1), dtype=torch.uint8, device="cuda")
+    d_res = torch.zeros(n * ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
+
+    def step():
+        plan.execute_device(d_grid.data_ptr(), d_tb.data_ptr(), d_res.data_ptr(), None, sptr)
+
+    ctx.lib.pg_set_kernel_timing(ctx.handle, 1)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(dev)
+    clocks.wait_first_sample()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ldpc_ms = []
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+            stream.synchronize()
+            ldpc_ms.append(ctx.lib.pg_last_kernel_ms(ctx.handle))
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = statistics.mean(step_ms)
+
+    # Decoded bits: CRC-passing UEs whose TB equals the transmitted bits.
+    res_arr = (PgSchResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+    results = results_from(plan.descs, res_arr, None, d_tb.cpu().numpy())
+    good = [r.tb_crc_ok and bool((np.unpackbits(r.transport_block) == t).all()) for r, t in zip(results, truth)]
+    bits_ok = int(sum(u.tbs_bits for u, g in zip(plan.ues, good) if g))
+    bits_all = int(sum(u.tbs_bits for u in plan.ues))
+    bler = 1.0 - sum(good) / n
+
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+        b = torch.tensor([bits_ok], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(b)
+        total_bits = float(b.item())
+    else:
+        ms_max, total_bits = ms, float(bits_ok)
+    value = total_bits / (ms_max * 1e-3) / 1e6
+
+    # Plain per-UE GPU path: one plan per UE, each executed and waited for before the next UE.
+    plain = None
+    if not args.no_plain:
+        per_ue = []
+        for sl in slots:
+            for u in range(len(sl.ues)):
+                one = type(sl)(sl.grid, [sl.ues[u]], [sl.truth[u]], sl.nof_ports, sl.nof_prb_grid, sl.slot,
+                               sl.scs_khz, sl.dmrs_scaling)
+                per_ue.append(PuschSlotPlan(ctx, [one], max_iterations=MAX_ITER, graph=False))
+        grids = [torch.from_numpy(p.grid.view(np.int32)).cuda() for p in per_ue]
+        tbs = [torch.zeros(max(p.tb_bytes, 1), dtype=torch.uint8, device="cuda") for p in per_ue]
+        res1 = torch.zeros(ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
+
+        def plain_step():
+            for p, g, tb in zip(per_ue, grids, tbs):
+                p.execute_device(g.data_ptr(), tb.data_ptr(), res1.data_ptr(), None, sptr)
+                stream.synchronize()
+
+        with torch.cuda.stream(stream):
+            for _ in range(max(1, args.warmup)):
+                plain_step()
+            pms = []
+            for k in range(max(3, args.steps // 5)):
+                flush.fill_(k & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plain_step()
+                b.record(stream)
+                torch.cuda.synchronize()
+                pms.append(a.elapsed_time(b))
+        p_ms = statistics.mean(pms)
+        plain = {"value": round(bits_ok / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 3),
+                 "plans": len(per_ue), "kernels_per_step": KERNELS_PER_PLAN * len(per_ue),
+                 "what": "one plan per UE executed in turn, host waits for each UE's result (no batching, no graph)"}
+        for p in per_ue:
+            p.close()
+
+    # End to end through the host entry: pinned grids in, results and TBs out, every step.
+    e2e = None
+    if not args.no_e2e:
+        h_grid = torch.from_numpy(plan.grid.view(np.int32)).pin_memory()
+        h_tb = torch.zeros(max(plan.tb_bytes, 1), dtype=torch.uint8).pin_memory()
+        h_res = (PgSchResult * n)()
+        lib = ctx.lib
+
+        def e2e_step():
+            ctx.check(lib.pg_pusch_plan_execute_host(plan.handle, h_grid.data_ptr(), h_tb.data_ptr(), h_tb.numel(),
+                                                     ctypes.addressof(h_res), None))
+
+        for _ in range(max(args.warmup, 1)):
+            e2e_step()
+        et = []
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            e2e_step()
+            et.append(time.perf_counter() - t0)
+        e_ms = 1e3 * statistics.mean(et)
+        e_ok = [bool(h_res[i].tb_crc_ok) for i in range(n)]
+        assert e_ok == [r.tb_crc_ok for r in results]
+        if world > 1:
+            t = torch.tensor([e_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": round(total_bits / (e_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
+               "h2d_bytes_per_step": int(plan.grid.size * 4),
+               "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
+               "ms_per_step": round(e_ms, 3), "entry": "pg_pusch_plan_execute_host"}
+
+    # Integer roofline of the dominant kernel (ldpc_decode_kernel inside the step).
+    edge_updates = pusch_edge_updates(plan.ues, results)
+    ops = edge_updates * INT_OPS_PER_EDGE
+    valid_ms = [x for x in ldpc_ms if x > 0]
+    k_ms = statistics.mean(valid_ms) if valid_ms else float("nan")
+    peak_ops, classes = int_peak(dev)
+    props = torch.cuda.get_device_properties(dev)
+    nominal = props.multi_processor_count * 128 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
+    peak = peak_ops / 1e12 if peak_ops else nominal
+    achieved = ops / (k_ms * 1e-3) / 1e12
+    roofline = {
+        "bound": "int", "kernel": "ldpc_decode_kernel", "achieved": round(achieved, 3), "peak": round(peak, 3),
+        "unit": "Tops/s", "frac": round(achieved / peak, 4),
+        "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"
+                        if peak_ops else "nominal 148 SM x 128 lanes x max SM clock"),
+        "nominal_peak": round(nominal, 3), "instruction_classes_tops": classes,
+        "ops_per_edge_update": INT_OPS_PER_EDGE, "edge_updates_per_launch": edge_updates,
+        "kernel_ms": round(k_ms, 4), "kernel_share_of_step": round(k_ms / ms, 3),
+        "traffic": None,
+    }
+
+    ldpc_line = None
+    if not args.no_ldpc:
+        ldpc_line = ldpc_measure(args, dev, rank, world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = host_cores()
+        b, dt, passes, n_ues = reference_pusch(slots, args.cpu_seconds, cores)
+        cpu = {"value": round(b * passes / dt / 1e6, 3), "unit": "Mbit/s", "cores": cores, "kind": "reference",
+               "sample": f"{passes} passes over the full {N_CELLS}-cell slot ({n_ues} UEs) through the reference's "
+                         f"CPU stage objects (oracle/_ref) on {cores} C++ threads, {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32/int8", "data": "synthetic (seeded simulator)",
+            "config": {"workload": PUSCH_WORKLOAD, "cells_per_rank": N_CELLS, "ues_per_rank": n,
+                       "codeblocks_per_rank": int(plan.info.nof_codeblocks), "tb_bits_per_rank": bits_all,
+                       "decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
+                       "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
+                       "parallelism": f"replicas{world}", "estimator": "plain (LS + RC FIR + linear interpolation)"},
+            "plain_per_ue": plain, "learned": None,
+            "e2e": e2e, "roofline": roofline, "ldpc": ldpc_line, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": KERNELS_PER_PLAN * args.steps,
+            "step_ms": {"min": round(min(step_ms), 4), "max": round(max(step_ms), 4)},
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    ctx.close()
+    return 0
+
+
 def cpu_reference_decode(batch, seconds, cores, min_batches=1):
     """Decodes the batch with the reference's CPU decoder (oracle/_ref) on `cores` C++ threads,
     one reference decoder per thread with codeblocks claimed dynamically, until `seconds` of
@@ -197,19 +508,12 @@ def run_reference(args):
     return 0
 
 
-def run_ours(args):
+def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
+    """The LDPC decoder batch (512 codeblocks) on this rank's GPU; returns rank 0's JSON line."""
     import numpy as np
     import torch
 
-    rank, world, local_rank = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
-    dev = torch.cuda.current_device()
+    steps = steps or args.steps
 
     from pusch_b200 import sim
     from pusch_b200.ldpc import LdpcBatchDecoder, make_descriptors
@@ -239,9 +543,9 @@ def run_ours(args):
         torch.distributed.barrier()
     clocks = ClockSampler(dev)
     clocks.wait_first_sample()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     torch.cuda.synchronize()
-    for k in range(args.steps):
+    for k in range(steps):
         flush.fill_(k & 0xFF)
         evs[k][0].record(stream)
         step()
@@ -266,7 +570,7 @@ def run_ours(args):
 
     # End to end through the host C ABI: pinned LLRs in, bits + iterations out, every step.
     e2e = None
-    if not args.no_e2e:
+    if with_e2e and not args.no_e2e:
         h_llrs = torch.from_numpy(llrs).pin_memory()
         h_bits = torch.zeros(nbytes, dtype=torch.uint8).pin_memory()
         h_it = torch.zeros(N_CBS, dtype=torch.int32).pin_memory()
@@ -280,7 +584,7 @@ def run_ours(args):
         for _ in range(max(args.warmup, 1)):
             e2e_step()
         et = []
-        for _ in range(args.steps):
+        for _ in range(steps):
             flush.fill_(3)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -328,38 +632,72 @@ def run_ours(args):
     }
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if with_cpu and rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = host_cores()
         b, dt, ncb, variant = cpu_reference_decode(batch, args.cpu_seconds, cores)
         cpu = {"value": round(b / dt / 1e9, 4), "unit": "Gbit/s", "cores": cores, "kind": "reference",
                "sample": f"{ncb} codeblocks ({ncb // N_CBS} passes over the batch) with the reference "
                          f"ldpc_decoder_{variant} (oracle/_ref) on {cores} C++ threads, {dt:.1f} s"}
 
+    line = None
     if rank == 0:
         line = {
-            "metric": METRIC, "value": round(value, 4), "unit": "Gbit/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC, "value": round(value, 4), "unit": "Gbit/s", "n_gpus": world, "steps": steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int8", "data": "synthetic (seeded simulator)",
             "config": {"workload": WORKLOAD, "codeblocks_per_step": N_CBS * world,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas{world}",
                        "info_bits_all_per_rank": bits_all, "info_bits_passing_per_rank": bits_ok,
                        "crc_pass": int((iters > 0).sum()), "mean_iterations": round(float(iters[iters > 0].mean()), 3)},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": args.steps,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk, "gpu_launches": steps,
             "kernel_ms": {"min": round(min(kernel_ms), 4), "max": round(max(kernel_ms), 4)},
         }
+    dec.ctx.close()
+    return line
+
+
+def dist_setup():
+    import torch
+    rank, world, local_rank = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    return rank, world, torch.cuda.current_device()
+
+
+def run_ours_ldpc(args):
+    import torch
+    rank, world, dev = dist_setup()
+    line = ldpc_core(args, dev, rank, world)
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
-    dec.ctx.close()
     return 0
+
+
+def ldpc_measure(args, dev, rank, world):
+    """The LDPC batch as a sub-measurement of the PUSCH line (device-timed Gbit/s and roofline)."""
+    line = ldpc_core(args, dev, rank, world, with_cpu=False, with_e2e=False, steps=min(args.steps, 30))
+    if line is None:
+        return None
+    return {"value": line["value"], "unit": "Gbit/s", "ms_per_step": line["ms_per_step"],
+            "workload": WORKLOAD, "roofline": {k: line["roofline"][k] for k in ("achieved", "peak", "unit", "frac")},
+            "crc_pass": line["config"]["crc_pass"], "mean_iterations": line["config"]["mean_iterations"]}
+
+
 
 
 def main():
     args = parse_args()
     if args.impl == "reference":
-        return run_reference(args)
-    return run_ours(args)
+        return run_reference_pusch(args) if args.workload == "uneven" else run_reference(args)
+    return run_ours_pusch(args) if args.workload == "uneven" else run_ours_ldpc(args)
 
 
 if __name__ == "__main__":

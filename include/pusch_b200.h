@@ -366,6 +366,52 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
                           size_t grid_words, uint8_t* tb_out, size_t tb_out_len, pg_port_result* port_results,
                           pg_sch_result* results);
 
+/* ---------------------------------------------------------------------------------------- */
+/* Slot plans: one batch of PDUs (any number of UEs and cells) prepared once, executed per slot */
+
+/* A plan holds everything of pusch_processor::process that depends only on the PDUs
+ * (lib/phy/upper/channel_processors/pusch/pusch_processor_impl.cpp:349-900): segmentation, the
+ * work lists of every stage (uploaded to the device once), the device workspace and the
+ * descrambling sequences. Executing it enqueues DM-RS estimation, demodulation, rate dematching,
+ * LDPC decoding, TB assembly and CRC and the per-UE results on one stream with no host
+ * synchronisation. The plan keeps a pointer to its context, which must outlive it; a plan is used
+ * by one thread at a time. */
+typedef struct pg_pusch_plan pg_pusch_plan;
+
+typedef struct pg_pusch_plan_info_t {
+  uint32_t nof_ues;
+  uint32_t nof_codeblocks;
+  uint64_t tb_bytes;     /* transport-block output bytes (max tb_out_offset + TBS/8) */
+  uint64_t nof_llrs;     /* codeword LLRs of all UEs */
+  uint64_t grid_words;   /* cbf16 words of the grids buffer */
+  uint64_t device_bytes; /* device memory the plan holds */
+} pg_pusch_plan_info_t;
+
+/* ues: host array of nof_ues PDUs whose grids lie in a buffer of grid_words cbf16 words; the
+ * library assigns est_offset and llr_offset, the caller tb_out_offset, grid_offset and
+ * grid_nof_subc. */
+int  pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, size_t grid_words,
+                          pg_pusch_plan** out);
+void pg_pusch_plan_destroy(pg_pusch_plan* plan);
+int  pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info);
+
+/* enabled = 1: execute_device captures its launches into a CUDA graph on the first call (and
+ * again whenever its buffers or stream change) and replays the graph afterwards. Streams other
+ * than the legacy default stream only; on the default stream the launches are enqueued directly. */
+int pg_pusch_plan_set_graph(pg_pusch_plan* plan, int enabled);
+
+/* Enqueues the slot on stream: grids (device, grid_words cbf16 words) -> tb_out (device,
+ * tb_bytes; the assembled TB of every UE, valid where results[u].tb_crc_ok), results (device,
+ * one pg_sch_result per UE) and port_results (device, nof_ues * 4 entries, or NULL). */
+int pg_pusch_plan_execute_device(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, pg_sch_result* results,
+                                 pg_port_result* port_results, void* stream);
+
+/* The same from and to host memory: H2D of the grids, execution, D2H of results, port results
+ * (may be NULL) and TBs; returns when the results are in host memory. As the reference, a TB's
+ * payload is written to tb_out only when its CRC passes. */
+int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, size_t tb_out_len,
+                               pg_sch_result* results, pg_port_result* port_results);
+
 #ifdef __cplusplus
 }
 #endif

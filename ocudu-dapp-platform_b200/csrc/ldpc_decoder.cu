@@ -491,15 +491,29 @@ int ldpc_upload_tables(pg_context* ctx)
 int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                 int32_t* iterations, cudaStream_t stream)
 {
+  return ldpc_launch_scratch(ctx, descs_dev, n, llrs, bits, iterations, ctx->dev.c2v, stream);
+}
+
+int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                        int32_t* iterations, int8_t* c2v, cudaStream_t stream)
+{
   if (n == 0) {
     return PG_OK;
   }
-  if (ctx->timed) {
-    cudaEventRecord(ctx->ev_start, stream);
+  // Under stream capture the timing events become event-record nodes of the graph (external
+  // records); a plain record there would only mark a capture dependency.
+  unsigned int                rec_flags = cudaEventRecordDefault;
+  cudaStreamCaptureStatus     capturing = cudaStreamCaptureStatusNone;
+  if (ctx->timed && cudaStreamIsCapturing(stream, &capturing) == cudaSuccess &&
+      capturing == cudaStreamCaptureStatusActive) {
+    rec_flags = cudaEventRecordExternal;
   }
-  ldpc_decode_kernel<<<n, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, ctx->dev.c2v, ctx->dev.crc_pow);
   if (ctx->timed) {
-    cudaEventRecord(ctx->ev_stop, stream);
+    cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
+  }
+  ldpc_decode_kernel<<<n, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow);
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_stop, stream, rec_flags);
   }
   return check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch");
 }

@@ -489,6 +489,8 @@ float pg_last_kernel_ms(pg_context* ctx)
   float ms = -1.0f;
   if (cudaEventSynchronize(ctx->ev_stop) != cudaSuccess ||
       cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) != cudaSuccess) {
+    // Clear the error of the failed query, so that it is not reported by a later launch check.
+    (void)cudaGetLastError();
     return -1.0f;
   }
   return ms;

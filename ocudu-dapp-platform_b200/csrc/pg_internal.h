@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 namespace pg {
 
@@ -126,6 +127,25 @@ uint32_t ue_codeword_bits(const pg_pusch_ue& u);
 int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
                  const uint32_t* grids, const float* est, const pg_port_result* port_results,
                  const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s);
+// Host-side work lists of a batch of transport blocks: one rate-dematch and one LDPC descriptor
+// per codeblock, one TB descriptor per TB, the bit offset of each codeblock's decoded bits.
+struct sch_work {
+  std::vector<pg_rm_cb>   rm;
+  std::vector<pg_ldpc_cb> ldpc;
+  std::vector<pg_tb_desc> tbd;
+  std::vector<uint32_t>   cb_bit_off;
+  std::vector<int>        tb_first, tb_ncb;
+  size_t                  rm_total = 0, bits_total = 0;
+};
+int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t nof_llrs_total, size_t tb_out_len,
+                   sch_work& w);
+// Scrambling sequences of every UE (c_init = RNTI * 2^15 + n_ID), words at seq_offsets_dev[u].
+int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,
+                      const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s);
+// Demodulation with the scrambling sequences already generated.
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_re, const uint32_t* grids,
+                      const float* est, const pg_port_result* port_results, const uint32_t* seq_offsets_dev,
+                      const uint32_t* seq_dev, int8_t* llrs, cudaStream_t s);
 // Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
 // uses scratch_b; results and TB payloads land in host memory.
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
@@ -141,5 +161,8 @@ int demap_launch(pg_context* ctx, int qm, int n, const float2* sym, const float*
 // Enqueues the batched decoder; descs_dev holds n descriptors in device memory.
 int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                 int32_t* iterations, cudaStream_t stream);
+// Same with a caller-provided check-to-variable scratch of n * kC2vStride bytes.
+int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                        int32_t* iterations, int8_t* c2v, cudaStream_t stream);
 
 } // namespace pg

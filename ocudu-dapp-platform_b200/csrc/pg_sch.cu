@@ -290,16 +290,13 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
 
 namespace pg {
 
-int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
-                           size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results)
+int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t nof_llrs_total, size_t tb_out_len,
+                   sch_work& w)
 {
   // Work lists: one rate-dematch and one LDPC descriptor per codeblock, one TB descriptor per TB.
-  std::vector<pg_rm_cb>   rm;
-  std::vector<pg_ldpc_cb> ldpc;
-  std::vector<pg_tb_desc> tbd;
-  std::vector<uint32_t>   cb_bit_off;
-  std::vector<int>        tb_first(nof_tbs), tb_ncb(nof_tbs);
-  size_t                  rm_total = 0, bits_total = 0;
+  w = sch_work();
+  w.tb_first.resize(nof_tbs);
+  w.tb_ncb.resize(nof_tbs);
   for (int t = 0; t < nof_tbs; ++t) {
     const pg_sch_tb&    tb = tbs[t];
     pg_sch_segmentation sg;
@@ -307,8 +304,6 @@ int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, c
         tb.max_iterations == 0 || tb.tbs_bits % 8 != 0) {
       return set_error(ctx, PG_ERR_INVALID, "transport block " + std::to_string(t) + ": invalid configuration");
     }
-    const uint32_t g = tb.nof_ch_symbols * tb.modulation_order * 1u;
-    (void)g;
     const uint32_t tb_llrs = tb.nof_ch_symbols * tb.modulation_order;
     if ((size_t)tb.llr_offset + tb_llrs > nof_llrs_total) {
       return set_error(ctx, PG_ERR_INVALID, "transport block " + std::to_string(t) + ": LLRs beyond the buffer");
@@ -320,8 +315,8 @@ int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, c
     if (bout % sg.nof_cbs != 0) {
       return set_error(ctx, PG_ERR_INVALID, "transport block " + std::to_string(t) + ": TBS not segmentable evenly");
     }
-    tb_first[t]      = (int)ldpc.size();
-    tb_ncb[t]        = (int)sg.nof_cbs;
+    w.tb_first[t]    = (int)w.ldpc.size();
+    w.tb_ncb[t]      = (int)sg.nof_cbs;
     const uint32_t N = (tb.base_graph == 1 ? 66 : 50) * sg.lifting_size;
     uint32_t       cw_off = 0;
     for (uint32_t c = 0; c < sg.nof_cbs; ++c) {
@@ -329,7 +324,7 @@ int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, c
       pg_rm_cb       r{};
       r.in_offset        = tb.llr_offset + cw_off;
       r.rm_length        = e;
-      r.out_offset       = (uint32_t)rm_total;
+      r.out_offset       = (uint32_t)w.rm_total;
       r.nref             = tb.nref;
       r.lifting_size     = (uint16_t)sg.lifting_size;
       r.nof_filler_bits  = (uint16_t)sg.nof_filler_bits;
@@ -337,34 +332,52 @@ int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, c
       r.rv               = tb.rv;
       r.modulation_order = tb.modulation_order;
       r.new_data         = 1;
-      rm.push_back(r);
+      w.rm.push_back(r);
       pg_ldpc_cb l{};
-      l.llr_offset      = (uint32_t)rm_total;
+      l.llr_offset      = (uint32_t)w.rm_total;
       l.nof_llrs        = N;
-      l.out_offset      = (uint32_t)bits_total;
+      l.out_offset      = (uint32_t)w.bits_total;
       l.lifting_size    = (uint16_t)sg.lifting_size;
       l.nof_filler_bits = (uint16_t)sg.nof_filler_bits;
       l.base_graph      = tb.base_graph;
       l.crc_poly        = sg.nof_cbs > 1 ? PG_CRC24B : (tb.tbs_bits <= 3824 ? PG_CRC16 : PG_CRC24A);
       l.max_iterations  = tb.max_iterations;
-      ldpc.push_back(l);
-      cb_bit_off.push_back((uint32_t)(bits_total * 8));
-      rm_total += N;
-      bits_total += (sg.cb_length + 7) / 8;
+      w.ldpc.push_back(l);
+      w.cb_bit_off.push_back((uint32_t)(w.bits_total * 8));
+      w.rm_total += N;
+      w.bits_total += (sg.cb_length + 7) / 8;
       cw_off += e;
     }
     if (cw_off != tb_llrs) {
       return set_error(ctx, PG_ERR_INVALID, "transport block " + std::to_string(t) + ": E_r do not sum to G");
     }
     pg_tb_desc d{};
-    d.cb_first        = (uint32_t)tb_first[t];
+    d.cb_first        = (uint32_t)w.tb_first[t];
     d.nof_cbs         = sg.nof_cbs;
     d.cb_payload_bits = bout / sg.nof_cbs - sg.cb_crc_bits;
     d.tbs_bits        = tb.tbs_bits;
     d.tb_out_offset   = tb.tb_out_offset;
     d.crc_poly        = tb.tbs_bits <= 3824 ? PG_CRC16 : PG_CRC24A;
-    tbd.push_back(d);
+    w.tbd.push_back(d);
   }
+  return PG_OK;
+}
+
+int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
+                           size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results)
+{
+  sch_work w;
+  if (int rc = build_sch_work(ctx, tbs, nof_tbs, nof_llrs_total, tb_out_len, w)) {
+    return rc;
+  }
+  std::vector<pg_rm_cb>&   rm         = w.rm;
+  std::vector<pg_ldpc_cb>& ldpc       = w.ldpc;
+  std::vector<pg_tb_desc>& tbd        = w.tbd;
+  std::vector<uint32_t>&   cb_bit_off = w.cb_bit_off;
+  std::vector<int>&        tb_first   = w.tb_first;
+  std::vector<int>&        tb_ncb     = w.tb_ncb;
+  const size_t             rm_total   = w.rm_total;
+  const size_t             bits_total = w.bits_total;
   const int ncb = (int)ldpc.size();
   if (ncb > ctx->max_codeblocks) {
     return set_error(ctx, PG_ERR_CAPACITY, "batch of " + std::to_string(ncb) + " codeblocks exceeds max_codeblocks");

@@ -116,13 +116,10 @@ __global__ void scrambling_kernel(const pg_pusch_ue* __restrict__ ues, const uin
                                   uint32_t* __restrict__ seq, const uint32_t* __restrict__ gold, uint32_t gold_words)
 {
   const pg_pusch_ue ue     = ues[blockIdx.y];
-  int               d0 = 0, d1 = 0;
-  int               ndmrs = 0;
+  int               ndmrs  = 0;
   for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
     ndmrs += (ue.dmrs_symbol_mask >> s) & 1;
   }
-  (void)d0;
-  (void)d1;
   const uint32_t g      = (uint32_t)(ue.nof_symbols - ndmrs) * 12u * ue.nof_rb * ue.nof_layers * ue.modulation_order;
   const uint32_t words  = (g + 31) / 32;
   const uint32_t c_init = ((uint32_t)ue.rnti << 15) + ue.n_id_data;
@@ -363,23 +360,39 @@ uint32_t ue_codeword_bits(const pg_pusch_ue& u)
   return (uint32_t)(u.nof_symbols - ndmrs) * 12u * u.nof_rb * u.nof_layers * u.modulation_order;
 }
 
-// Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
-// device scratch sized by the caller from ue_codeword_bits.
-int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
-                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
-                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,
+                      const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s)
 {
   if (n == 0) {
     return PG_OK;
   }
   scrambling_kernel<<<dim3(std::max(1u, std::min(64u, (max_words + 255) / 256)), n), 256, 0, s>>>(
       ues_dev, seq_offsets_dev, seq_dev, ctx->dev.gold, kGoldWords);
-  if (int rc = check_cuda(ctx, cudaGetLastError(), "scrambling_kernel launch")) {
-    return rc;
+  return check_cuda(ctx, cudaGetLastError(), "scrambling_kernel launch");
+}
+
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_re, const uint32_t* grids,
+                      const float* est, const pg_port_result* port_results, const uint32_t* seq_offsets_dev,
+                      const uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
   }
   pusch_demod_kernel<<<dim3(std::max(1u, std::min(1024u, (max_re + 255) / 256)), n), 256, 0, s>>>(
       ues_dev, grids, reinterpret_cast<const float2*>(est), port_results, seq_offsets_dev, seq_dev, llrs);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
+}
+
+// Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
+// device scratch sized by the caller from ue_codeword_bits.
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
+                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
+                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+{
+  if (int rc = scrambling_launch(ctx, ues_dev, n, max_words, seq_offsets_dev, seq_dev, s)) {
+    return rc;
+  }
+  return demod_only_launch(ctx, ues_dev, n, max_re, grids, est, port_results, seq_offsets_dev, seq_dev, llrs, s);
 }
 
 } // namespace pg

@@ -389,7 +389,14 @@ int est_upload_tables(pg_context* ctx)
       taps[sel][i] *= 1.0f / tot;
     }
   }
-  int rc2 = check_cuda(ctx, cudaMemcpyToSymbol(c_rc_taps, taps, sizeof(taps)), "cudaMemcpyToSymbol(rc taps)");
+  int rc2 = check_cuda(ctx,
+                       cudaFuncSetAttribute(pusch_estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)sizeof(est_smem)),
+                       "cudaFuncSetAttribute(pusch_estimate_kernel)");
+  if (rc2 != PG_OK) {
+    return rc2;
+  }
+  rc2 = check_cuda(ctx, cudaMemcpyToSymbol(c_rc_taps, taps, sizeof(taps)), "cudaMemcpyToSymbol(rc taps)");
   if (rc2 != PG_OK) {
     return rc2;
   }
@@ -432,11 +439,6 @@ int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const ui
 {
   if (n == 0) {
     return PG_OK;
-  }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(pusch_estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(est_smem));
-    attr_set = true;
   }
   pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, sizeof(est_smem), s>>>(
       ues_dev, grids, reinterpret_cast<float2*>(est), results, ctx->dev.gold, kGoldWords);

@@ -1,0 +1,422 @@
+// Slot plans: the PUSCH receive path of a batch of UEs (any number of cells) prepared once on the
+// host and executed per slot as a fixed sequence of launches on one stream, with no host
+// synchronisation in between (pusch_processor_impl::process / process_data,
+// lib/phy/upper/channel_processors/pusch/pusch_processor_impl.cpp:349-900, for a whole slot of
+// PDUs at once).
+//
+// Creation does everything that depends only on the PDUs: segmentation and the work lists of every
+// stage (UE, rate-dematch, LDPC and TB descriptors, uploaded once), the device workspace (one
+// allocation: frequency responses, LLRs, dematched codeblocks, decoded bits, check-to-variable
+// scratch) and the descrambling sequences, which depend only on RNTI and n_ID.
+// Execution per slot: DM-RS estimation -> demodulation (equalise, demap, descramble) -> rate
+// dematching -> LDPC -> TB assembly and CRC -> per-UE results, optionally replayed as a CUDA graph
+// captured on the first execution.
+#include "pg_internal.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+using namespace pg;
+
+struct pg_pusch_plan {
+  pg_context*              ctx = nullptr;
+  int                      nof_ues = 0, nof_cbs = 0;
+  size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0;
+  uint32_t                 max_re = 0;
+  std::vector<pg_pusch_ue> ues;
+  // Device: descriptors, then workspace.
+  void*           dev      = nullptr;
+  pg_pusch_ue*    d_ues    = nullptr;
+  pg_rm_cb*       d_rm     = nullptr;
+  pg_ldpc_cb*     d_ldpc   = nullptr;
+  pg_tb_desc*     d_tb     = nullptr;
+  uint32_t*       d_cb_off = nullptr;
+  uint32_t*       d_seq_off = nullptr;
+  uint32_t*       d_seq    = nullptr;
+  float*          d_est    = nullptr;
+  pg_port_result* d_pr     = nullptr;
+  int8_t*         d_llr    = nullptr;
+  int8_t*         d_rm_out = nullptr;
+  uint8_t*        d_cb_bits = nullptr;
+  uint32_t*       d_tb_crc = nullptr;
+  int32_t*        d_iters  = nullptr;
+  int8_t*         d_c2v    = nullptr;
+  uint32_t*       d_grid   = nullptr; // grids of execute_host
+  uint8_t*        d_tb_out = nullptr; // TBs of execute_host
+  pg_sch_result*  d_res    = nullptr; // results of execute_host
+  // Pinned host buffers of execute_host: [results | port results | TBs].
+  void*           host     = nullptr;
+  // CUDA graph of execute_device.
+  bool            use_graph = false;
+  cudaGraphExec_t exec      = nullptr;
+  const void*     key[5]    = {};
+};
+
+namespace {
+
+// Per-UE pusch_decoder_result from the codeblock iteration counts and the TB CRC remainder:
+// C == 1: the codeblock CRC is the TB CRC; C > 1: every codeblock CRC and the TB CRC. A failed
+// codeblock counts max_iterations (pusch_decoder_impl.cpp:612-710).
+__global__ void sch_results_kernel(const pg_tb_desc* __restrict__ tbs, const pg_pusch_ue* __restrict__ ues, int n,
+                                   const int32_t* __restrict__ iters, const uint32_t* __restrict__ tb_crc,
+                                   pg_sch_result* __restrict__ out)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) {
+    return;
+  }
+  const pg_tb_desc d     = tbs[t];
+  const uint32_t   maxit = ues[t].max_iterations;
+  uint32_t         ok = 0, mx = 0;
+  float            sum = 0.f;
+  for (uint32_t c = 0; c < d.nof_cbs; ++c) {
+    const int32_t  it  = iters[d.cb_first + c];
+    const uint32_t run = it > 0 ? (uint32_t)it : maxit;
+    ok += it > 0 ? 1u : 0u;
+    sum += (float)run;
+    mx = run > mx ? run : mx;
+  }
+  pg_sch_result r;
+  r.tb_crc_ok          = (ok == d.nof_cbs && (d.nof_cbs == 1 || tb_crc[t] == 0)) ? 1u : 0u;
+  r.nof_cbs            = d.nof_cbs;
+  r.nof_cbs_crc_ok     = ok;
+  r.mean_iterations    = sum / (float)d.nof_cbs;
+  r.max_iterations_run = mx;
+  out[t]               = r;
+}
+
+size_t al(size_t x)
+{
+  return (x + 255) & ~(size_t)255;
+}
+
+int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_result* results,
+            pg_port_result* port_results, cudaStream_t s)
+{
+  pg_context* ctx = p->ctx;
+  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, grids, p->d_est, port_results, s);
+  if (rc == PG_OK) {
+    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->max_re, grids, p->d_est, port_results, p->d_seq_off,
+                           p->d_seq, p->d_llr, s);
+  }
+  if (rc == PG_OK) {
+    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s);
+  }
+  if (rc == PG_OK) {
+    rc = ldpc_launch_scratch(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
+  }
+  if (rc == PG_OK) {
+    rc = tb_assemble_launch(ctx, p->d_tb, p->nof_ues, p->d_cb_bits, p->d_cb_off, tb_out, p->d_tb_crc, s);
+  }
+  if (rc == PG_OK) {
+    sch_results_kernel<<<(p->nof_ues + 127) / 128, 128, 0, s>>>(p->d_tb, p->d_ues, p->nof_ues, p->d_iters, p->d_tb_crc,
+                                                                 results);
+    rc = check_cuda(ctx, cudaGetLastError(), "sch_results_kernel launch");
+  }
+  return rc;
+}
+
+void release(pg_pusch_plan* p)
+{
+  if (p->exec) {
+    cudaGraphExecDestroy(p->exec);
+  }
+  cudaFree(p->dev);
+  if (p->host) {
+    cudaFreeHost(p->host);
+  }
+  delete p;
+}
+
+} // namespace
+
+extern "C" {
+
+int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, size_t grid_words, pg_pusch_plan** out)
+{
+  if (ctx == nullptr || out == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (int rc = validate_ues(ctx, ues, nof_ues)) {
+    return rc;
+  }
+  if (nof_ues == 0) {
+    return set_error(ctx, PG_ERR_INVALID, "a plan needs at least one UE");
+  }
+  pg_pusch_plan* p = new (std::nothrow) pg_pusch_plan();
+  if (p == nullptr) {
+    return set_error(ctx, PG_ERR_CAPACITY, "out of host memory");
+  }
+  p->ctx        = ctx;
+  p->nof_ues    = nof_ues;
+  p->grid_words = grid_words;
+  p->ues.assign(ues, ues + nof_ues);
+
+  // UE layout: frequency responses, codeword LLRs and descrambling sequences back to back.
+  std::vector<uint32_t>  seq_off(nof_ues);
+  std::vector<pg_sch_tb> tbs(nof_ues);
+  size_t                 est_total = 0, seq_total = 0;
+  uint32_t               max_words = 0;
+  for (int i = 0; i < nof_ues; ++i) {
+    pg_pusch_ue& u = p->ues[i];
+    if ((size_t)u.grid_offset + (size_t)u.nof_rx_ports * 14 * u.grid_nof_subc > grid_words) {
+      release(p);
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": grid beyond the buffer");
+    }
+    const uint32_t g = ue_codeword_bits(u);
+    u.est_offset     = (uint32_t)est_total;
+    u.llr_offset     = (uint32_t)p->nof_llrs;
+    est_total += pg_pusch_est_size(&u);
+    p->nof_llrs += g;
+    seq_off[i]           = (uint32_t)seq_total;
+    const uint32_t words = (g + 31) / 32 + 2;
+    seq_total += words;
+    max_words = std::max(max_words, words);
+    int d0 = 0, d1 = 0;
+    p->max_re    = std::max(p->max_re, (uint32_t)(u.nof_symbols - dmrs_count(u, &d0, &d1)) * 12u * u.nof_rb);
+    p->tb_bytes  = std::max(p->tb_bytes, (size_t)u.tb_out_offset + u.tbs_bits / 8);
+    pg_sch_tb& t = tbs[i];
+    t            = pg_sch_tb{};
+    t.llr_offset       = u.llr_offset;
+    t.nof_ch_symbols   = g / u.modulation_order;
+    t.tbs_bits         = u.tbs_bits;
+    t.tb_out_offset    = u.tb_out_offset;
+    t.nref             = u.nref;
+    t.base_graph       = u.base_graph;
+    t.modulation_order = u.modulation_order;
+    t.nof_layers       = u.nof_layers;
+    t.rv               = u.rv;
+    t.max_iterations   = u.max_iterations;
+  }
+  sch_work w;
+  if (int rc = build_sch_work(ctx, tbs.data(), nof_ues, p->nof_llrs, p->tb_bytes, w)) {
+    release(p);
+    return rc;
+  }
+  p->nof_cbs = (int)w.ldpc.size();
+
+  // Device image: descriptors first (uploaded once), then the workspace.
+  const size_t o_ues    = 0;
+  const size_t o_rm     = o_ues + al((size_t)nof_ues * sizeof(pg_pusch_ue));
+  const size_t o_ldpc   = o_rm + al(w.rm.size() * sizeof(pg_rm_cb));
+  const size_t o_tb     = o_ldpc + al(w.ldpc.size() * sizeof(pg_ldpc_cb));
+  const size_t o_cb_off = o_tb + al(w.tbd.size() * sizeof(pg_tb_desc));
+  const size_t o_seqoff = o_cb_off + al(w.cb_bit_off.size() * 4);
+  const size_t desc_end = o_seqoff + al((size_t)nof_ues * 4);
+  const size_t o_seq    = desc_end;
+  const size_t o_est    = o_seq + al(seq_total * 4);
+  const size_t o_pr     = o_est + al(est_total * 8);
+  const size_t o_llr    = o_pr + al((size_t)nof_ues * 4 * sizeof(pg_port_result));
+  const size_t o_rmout  = o_llr + al(p->nof_llrs);
+  const size_t o_bits   = o_rmout + al(w.rm_total);
+  const size_t o_crc    = o_bits + al(w.bits_total);
+  const size_t o_it     = o_crc + al((size_t)nof_ues * 4);
+  const size_t o_c2v    = o_it + al((size_t)p->nof_cbs * 4);
+  const size_t o_grid   = o_c2v + al((size_t)p->nof_cbs * kC2vStride);
+  const size_t o_tbout  = o_grid + al(grid_words * 4);
+  const size_t o_res    = o_tbout + al(p->tb_bytes);
+  p->dev_bytes          = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
+
+  const size_t h_res  = 0;
+  const size_t h_pr   = h_res + al((size_t)nof_ues * sizeof(pg_sch_result));
+  const size_t h_tb   = h_pr + al((size_t)nof_ues * 4 * sizeof(pg_port_result));
+  const size_t h_size = std::max(h_tb + al(p->tb_bytes), desc_end);
+
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&p->dev, p->dev_bytes), "cudaMalloc(plan)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMallocHost(&p->host, h_size), "cudaMallocHost(plan)");
+  }
+  if (rc != PG_OK) {
+    release(p);
+    return rc;
+  }
+  uint8_t* b   = static_cast<uint8_t*>(p->dev);
+  p->d_ues     = reinterpret_cast<pg_pusch_ue*>(b + o_ues);
+  p->d_rm      = reinterpret_cast<pg_rm_cb*>(b + o_rm);
+  p->d_ldpc    = reinterpret_cast<pg_ldpc_cb*>(b + o_ldpc);
+  p->d_tb      = reinterpret_cast<pg_tb_desc*>(b + o_tb);
+  p->d_cb_off  = reinterpret_cast<uint32_t*>(b + o_cb_off);
+  p->d_seq_off = reinterpret_cast<uint32_t*>(b + o_seqoff);
+  p->d_seq     = reinterpret_cast<uint32_t*>(b + o_seq);
+  p->d_est     = reinterpret_cast<float*>(b + o_est);
+  p->d_pr      = reinterpret_cast<pg_port_result*>(b + o_pr);
+  p->d_llr     = reinterpret_cast<int8_t*>(b + o_llr);
+  p->d_rm_out  = reinterpret_cast<int8_t*>(b + o_rmout);
+  p->d_cb_bits = b + o_bits;
+  p->d_tb_crc  = reinterpret_cast<uint32_t*>(b + o_crc);
+  p->d_iters   = reinterpret_cast<int32_t*>(b + o_it);
+  p->d_c2v     = reinterpret_cast<int8_t*>(b + o_c2v);
+  p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
+  p->d_tb_out  = b + o_tbout;
+  p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);
+
+  // Descriptor image in pinned memory, one upload.
+  uint8_t* h = static_cast<uint8_t*>(p->host);
+  std::memset(h, 0, desc_end);
+  std::memcpy(h + o_ues, p->ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue));
+  std::memcpy(h + o_rm, w.rm.data(), w.rm.size() * sizeof(pg_rm_cb));
+  std::memcpy(h + o_ldpc, w.ldpc.data(), w.ldpc.size() * sizeof(pg_ldpc_cb));
+  std::memcpy(h + o_tb, w.tbd.data(), w.tbd.size() * sizeof(pg_tb_desc));
+  std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
+  std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
+  cudaStream_t s = ctx->stream;
+  rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemsetAsync(b + o_seq, 0, al(seq_total * 4), s), "cudaMemsetAsync(sequences)");
+  }
+  if (rc == PG_OK) {
+    rc = scrambling_launch(ctx, p->d_ues, nof_ues, max_words, p->d_seq_off, p->d_seq, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize(plan)");
+  }
+  if (rc != PG_OK) {
+    release(p);
+    return rc;
+  }
+  *out = p;
+  return PG_OK;
+}
+
+void pg_pusch_plan_destroy(pg_pusch_plan* plan)
+{
+  if (plan == nullptr) {
+    return;
+  }
+  cudaStreamSynchronize(plan->ctx->stream);
+  release(plan);
+}
+
+int pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info)
+{
+  if (plan == nullptr || info == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  info->nof_ues        = (uint32_t)plan->nof_ues;
+  info->nof_codeblocks = (uint32_t)plan->nof_cbs;
+  info->tb_bytes       = plan->tb_bytes;
+  info->nof_llrs       = plan->nof_llrs;
+  info->grid_words     = plan->grid_words;
+  info->device_bytes   = plan->dev_bytes;
+  return PG_OK;
+}
+
+int pg_pusch_plan_set_graph(pg_pusch_plan* plan, int enabled)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  plan->use_graph = enabled != 0;
+  return PG_OK;
+}
+
+int pg_pusch_plan_execute_device(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, pg_sch_result* results,
+                                 pg_port_result* port_results, void* stream)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (grids == nullptr || tb_out == nullptr || results == nullptr) {
+    return set_error(ctx, PG_ERR_INVALID, "null device buffer");
+  }
+  pg_port_result* pr = port_results != nullptr ? port_results : plan->d_pr;
+  cudaStream_t    s  = static_cast<cudaStream_t>(stream);
+  if (!plan->use_graph || s == nullptr) {
+    return enqueue(plan, grids, tb_out, results, pr, s);
+  }
+  const void* key[5] = {grids, tb_out, results, pr, stream};
+  if (plan->exec == nullptr || !std::equal(key, key + 5, plan->key)) {
+    if (plan->exec != nullptr) {
+      cudaGraphExecDestroy(plan->exec);
+      plan->exec = nullptr;
+    }
+    int rc = check_cuda(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    if (rc != PG_OK) {
+      return rc;
+    }
+    const int   rc_enq = enqueue(plan, grids, tb_out, results, pr, s);
+    cudaGraph_t graph  = nullptr;
+    rc                 = check_cuda(ctx, cudaStreamEndCapture(s, &graph), "cudaStreamEndCapture");
+    if (rc_enq != PG_OK || rc != PG_OK) {
+      if (graph != nullptr) {
+        cudaGraphDestroy(graph);
+      }
+      return rc_enq != PG_OK ? rc_enq : rc;
+    }
+    rc = check_cuda(ctx, cudaGraphInstantiate(&plan->exec, graph, 0), "cudaGraphInstantiate");
+    cudaGraphDestroy(graph);
+    if (rc != PG_OK) {
+      plan->exec = nullptr;
+      return rc;
+    }
+    std::copy(key, key + 5, plan->key);
+  }
+  return check_cuda(ctx, cudaGraphLaunch(plan->exec, s), "cudaGraphLaunch");
+}
+
+int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, size_t tb_out_len,
+                               pg_sch_result* results, pg_port_result* port_results)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (grids == nullptr || results == nullptr || (tb_out == nullptr && plan->tb_bytes > 0)) {
+    return set_error(ctx, PG_ERR_INVALID, "null host buffer");
+  }
+  if (tb_out_len < plan->tb_bytes) {
+    return set_error(ctx, PG_ERR_INVALID, "transport-block buffer smaller than the plan's TBs");
+  }
+  const int       n    = plan->nof_ues;
+  cudaStream_t    s    = ctx->stream;
+  uint8_t*        h    = static_cast<uint8_t*>(plan->host);
+  pg_sch_result*  hres = reinterpret_cast<pg_sch_result*>(h);
+  pg_port_result* hpr  = reinterpret_cast<pg_port_result*>(h + al((size_t)n * sizeof(pg_sch_result)));
+  uint8_t*        htb  = h + al((size_t)n * sizeof(pg_sch_result)) + al((size_t)n * 4 * sizeof(pg_port_result));
+  int rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, grids, plan->grid_words * 4, cudaMemcpyHostToDevice, s),
+                      "H2D grids");
+  if (rc == PG_OK) {
+    rc = pg_pusch_plan_execute_device(plan, plan->d_grid, plan->d_tb_out, plan->d_res, plan->d_pr, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(hres, plan->d_res, (size_t)n * sizeof(pg_sch_result), cudaMemcpyDeviceToHost, s),
+                    "D2H results");
+  }
+  if (rc == PG_OK && port_results != nullptr) {
+    rc = check_cuda(ctx,
+                    cudaMemcpyAsync(hpr, plan->d_pr, (size_t)n * 4 * sizeof(pg_port_result), cudaMemcpyDeviceToHost, s),
+                    "D2H port results");
+  }
+  if (rc == PG_OK && plan->tb_bytes > 0) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(htb, plan->d_tb_out, plan->tb_bytes, cudaMemcpyDeviceToHost, s), "D2H TBs");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  }
+  if (rc != PG_OK) {
+    return rc;
+  }
+  std::memcpy(results, hres, (size_t)n * sizeof(pg_sch_result));
+  if (port_results != nullptr) {
+    std::memcpy(port_results, hpr, (size_t)n * 4 * sizeof(pg_port_result));
+  }
+  // The reference writes a TB's payload only when its CRC passes.
+  for (int i = 0; i < n; ++i) {
+    if (hres[i].tb_crc_ok) {
+      const pg_pusch_ue& u = plan->ues[i];
+      std::memcpy(tb_out + u.tb_out_offset, htb + u.tb_out_offset, u.tbs_bits / 8);
+    }
+  }
+  return PG_OK;
+}
+
+} // extern "C"

@@ -72,6 +72,11 @@ class PgSchResult(ctypes.Structure):
                 ("mean_iterations", ctypes.c_float), ("max_iterations_run", ctypes.c_uint32)]
 
 
+class PgPuschPlanInfo(ctypes.Structure):
+    _fields_ = [("nof_ues", ctypes.c_uint32), ("nof_codeblocks", ctypes.c_uint32), ("tb_bytes", ctypes.c_uint64),
+                ("nof_llrs", ctypes.c_uint64), ("grid_words", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
+
+
 assert ctypes.sizeof(PgRmCb) == 24 and ctypes.sizeof(PgSchTb) == 28 and ctypes.sizeof(PgTbDesc) == 24
 
 # Every symbol the public header declares, with (restype, argtypes).
@@ -110,6 +115,12 @@ SIGNATURES = {
     "pg_pusch_demodulate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_process_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _VP,
                                              _VP]),
+    "pg_pusch_plan_create": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
+    "pg_pusch_plan_destroy": (None, [_VP]),
+    "pg_pusch_plan_info": (ctypes.c_int, [_VP, _VP]),
+    "pg_pusch_plan_set_graph": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "pg_pusch_plan_execute_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_plan_execute_host": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_size_t, _VP, _VP]),
 }
 
 _lib = None

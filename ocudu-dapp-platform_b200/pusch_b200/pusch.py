@@ -9,7 +9,7 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import _native
-from ._native import PgSchResult
+from ._native import PgPuschPlanInfo, PgSchResult
 from .sim import PuschSlot, PuschUe, nof_ch_symbols
 
 
@@ -107,3 +107,81 @@ class PuschProcessor:
                                    np.array([q.noise_var for q in p]), np.array([[q.rsrp[0], q.rsrp[1]] for q in p]),
                                    np.array([q.snr for q in p])))
         return out
+
+
+def batch_descriptors(slots: Sequence[PuschSlot], max_iterations=6, dc_subcarrier=-1):
+    """pg_pusch_ue array of every UE of every slot (one cell per slot), grids concatenated in slot
+    order, TBs packed back to back. Returns (descriptors, grid words, TB bytes, UE list)."""
+    descs, grids, off_words, tb_off, ue_list = [], [], 0, 0, []
+    for sl in slots:
+        arr, _, _, tbo = make_ue_descriptors(sl, max_iterations, off_words, dc_subcarrier, tb_off)
+        descs.extend(arr[i] for i in range(len(sl.ues)))
+        grids.append(np.ascontiguousarray(sl.grid, np.uint32).ravel())
+        off_words += grids[-1].size
+        tb_off = tbo
+        ue_list.extend(sl.ues)
+    arr = (PgPuschUe * len(descs))(*descs)
+    return arr, np.concatenate(grids), tb_off, ue_list
+
+
+class PuschSlotPlan:
+    """A pg_pusch_plan: the PDUs of one slot batch prepared once (segmentation, work lists,
+    workspace, descrambling sequences) and executed per slot - the batched form of
+    pusch_processor::process (pusch_processor.h:199-203)."""
+
+    def __init__(self, context: _native.Context, slots: Sequence[PuschSlot], max_iterations=6, dc_subcarrier=-1,
+                 graph=False):
+        self.ctx = context
+        self.lib = _native.load()
+        self.descs, self.grid, self.tb_bytes, self.ues = batch_descriptors(slots, max_iterations, dc_subcarrier)
+        self.n = len(self.ues)
+        h = ctypes.c_void_p()
+        self.ctx.check(self.lib.pg_pusch_plan_create(self.ctx.handle, ctypes.addressof(self.descs), self.n,
+                                                     self.grid.size, ctypes.byref(h)))
+        self.handle = h
+        info = PgPuschPlanInfo()
+        self.ctx.check(self.lib.pg_pusch_plan_info(self.handle, ctypes.byref(info)))
+        self.info = info
+        self.set_graph(graph)
+
+    def set_graph(self, enabled: bool):
+        self.ctx.check(self.lib.pg_pusch_plan_set_graph(self.handle, int(bool(enabled))))
+
+    def execute_device(self, grid_ptr, tb_ptr, results_ptr, port_results_ptr=None, stream_ptr=0):
+        self.ctx.check(self.lib.pg_pusch_plan_execute_device(self.handle, grid_ptr, tb_ptr, results_ptr,
+                                                             port_results_ptr, stream_ptr))
+
+    def execute_host(self, grid: Optional[np.ndarray] = None, with_port_results=True) -> List[PuschResult]:
+        grid = self.grid if grid is None else grid
+        tb = np.zeros(max(self.tb_bytes, 1), np.uint8)
+        res = (PgSchResult * self.n)()
+        pr = (PgPortResult * (4 * self.n))() if with_port_results else None
+        self.ctx.check(self.lib.pg_pusch_plan_execute_host(self.handle, grid.ctypes.data_as(ctypes.c_void_p),
+                                                           tb.ctypes.data_as(ctypes.c_void_p), tb.size,
+                                                           ctypes.addressof(res),
+                                                           ctypes.addressof(pr) if pr is not None else None))
+        return results_from(self.descs, res, pr, tb)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.pg_pusch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def results_from(descs, res, pr, tb) -> List[PuschResult]:
+    out = []
+    for i in range(len(descs)):
+        r = res[i]
+        p = [pr[4 * i + k] for k in range(descs[i].nof_rx_ports)] if pr is not None else []
+        o = descs[i].tb_out_offset
+        out.append(PuschResult(bool(r.tb_crc_ok), tb[o:o + descs[i].tbs_bits // 8].copy() if r.tb_crc_ok else None,
+                               int(r.nof_cbs), int(r.nof_cbs_crc_ok), float(r.mean_iterations),
+                               np.array([q.noise_var for q in p]), np.array([[q.rsrp[0], q.rsrp[1]] for q in p]),
+                               np.array([q.snr for q in p])))
+    return out

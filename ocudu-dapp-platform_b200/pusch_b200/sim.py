@@ -167,3 +167,73 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
         nvs.append(nv)
     return PuschSlot(to_cbf16(grid.astype(np.complex64)), list(ues), truth, nof_ports, nof_prb_grid, slot, scs_khz,
                      beta, chans, nvs)
+
+
+# ----------------------------------------------------------------------------------------------
+# Slot workloads of the benchmark configurations.
+
+def required_snr_db(qm, rate_x1024, nof_layers, nof_ports):
+    """Per-port SNR at which a PDU is expected to decode with BLER <= 10 %: the Shannon SNR of its
+    spectral efficiency per layer, less the combining gain of nof_ports receive ports over
+    nof_layers layers, plus an implementation gap of 8 dB (one layer) or 9 dB (two layers). The gap
+    is where this simulator's slots (exponential-PDP Rayleigh channels, DM-RS estimation, 6 LDPC
+    iterations, no HARQ) reached 10 % BLER in a sweep of 3,072 UEs over MCS table 2."""
+    se = qm * rate_x1024 / 1024.0
+    gap = 8.0 + (nof_layers - 1) * 1.0
+    return 10 * np.log10(2.0 ** se - 1.0) + gap - 10 * np.log10(nof_ports - nof_layers + 1)
+
+
+def ue_from_mcs(rb_start, nof_rb, nof_layers, table, index, dmrs_symbols, **kw):
+    """A PDU whose TBS and base graph follow TS 38.214 / TS 38.212 from (MCS table, index)."""
+    from . import mcs as mcs_tables
+    qm, r = mcs_tables.mcs(table, index)
+    a = mcs_tables.tbs(14, 12 * len(dmrs_symbols), 0, qm, r, nof_layers, nof_rb)
+    return PuschUe(rb_start=rb_start, nof_rb=nof_rb, nof_layers=nof_layers, modulation_order=qm, tbs_bits=a,
+                   base_graph=mcs_tables.base_graph(r, a), dmrs_symbols=tuple(dmrs_symbols), **kw)
+
+
+def single_ue_slot(seed=0):
+    """20 MHz / 30 kHz, 51 PRB, DM-RS symbol 2, 1 layer, 2 rx, QPSK (MCS table 1 index 5),
+    flat Rayleigh per rx port, 10 dB."""
+    ue = ue_from_mcs(0, 51, 1, 1, 5, (2,), snr_db=10.0, channel="flat")
+    return make_pusch_slot([ue], 2, nof_prb_grid=51, seed=seed)
+
+
+def full_cell_slot(seed=0, slot=0):
+    """100 MHz / 30 kHz, 273 PRB, DM-RS symbols 2 and 11, 2 layers, 4 rx, 256QAM (MCS table 2
+    index 20), exponential PDP (100 ns RMS, 8 taps), 25 dB."""
+    ue = ue_from_mcs(0, 273, 2, 2, 20, (2, 11), snr_db=25.0, channel="pdp")
+    return make_pusch_slot([ue], 4, nof_prb_grid=273, seed=seed, slot=slot)
+
+
+def uneven_cells(seed=0, nof_cells=16, nof_ports=4, snr_range=(0.0, 30.0), max_ues=16):
+    """The batched uneven slot: nof_cells cells of 273 PRB, each with 1..max_ues UEs on contiguous
+    PRB allocations that tile at most 273 PRB, 1 or 2 layers, per-UE SNR uniform in snr_range,
+    exponential-PDP channels. The MCS (table 2) of each UE is drawn among the indices its SNR
+    supports (required_snr_db), the highest few favoured; TBS and base graph follow from it."""
+    from . import mcs as mcs_tables
+    rng = np.random.default_rng(seed)
+    slots = []
+    for cell in range(nof_cells):
+        n_ues = int(rng.integers(1, max_ues + 1))
+        used = int(rng.integers(max(n_ues, 200), 274))
+        cuts = np.sort(rng.choice(np.arange(1, used), size=n_ues - 1, replace=False)) if n_ues > 1 else []
+        edges = [0, *[int(c) for c in cuts], used]
+        ues = []
+        for u in range(n_ues):
+            nof_rb = edges[u + 1] - edges[u]
+            layers = int(rng.integers(1, 3))
+            snr = float(rng.uniform(*snr_range))
+            ok = [i for i, (qm, r) in enumerate(mcs_tables.MCS_TABLE_2)
+                  if required_snr_db(qm, r, layers, nof_ports) <= snr]
+            if not ok and layers == 2:
+                layers = 1
+                ok = [i for i, (qm, r) in enumerate(mcs_tables.MCS_TABLE_2)
+                      if required_snr_db(qm, r, layers, nof_ports) <= snr]
+            top = max(ok) if ok else 0
+            index = int(rng.integers(max(0, top - 3), top + 1))
+            ues.append(ue_from_mcs(edges[u], nof_rb, layers, 2, index, (2, 11), snr_db=snr, channel="pdp",
+                                   rnti=0x4000 + 16 * cell + u, n_id=cell, n_id_data=cell))
+        slots.append(make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=cell % 20,
+                                     seed=int(rng.integers(0, 2 ** 31))))
+    return slots

@@ -148,6 +148,32 @@ class Ref:
         return freq, sym, dict(noise_var=float(sc[0]), epre=float(sc[1]), snr=float(sc[2]),
                                rsrp=sc[3:].astype(np.float64))
 
+    def pusch_decode_mt(self, descs, grid, tb_bytes, threads):
+        """The reference's CPU receive path over a pg_pusch_ue array (ctypes) and its grids.
+        Returns (ok flags, mean iterations, TB bytes, wall seconds)."""
+        n = len(descs)
+        g = np.ascontiguousarray(grid, np.uint32)
+        tb = np.zeros(max(tb_bytes, 1), np.uint8)
+        ok = np.zeros(n, np.int32)
+        it = np.zeros(n, np.float32)
+        self.lib.ref_pusch_decode_mt.restype = ctypes.c_double
+        self.lib.ref_pusch_decode_mt.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        dt = self.lib.ref_pusch_decode_mt(ctypes.addressof(descs), n, _ptr(g), _ptr(tb), _ptr(ok), _ptr(it), threads)
+        return ok.astype(bool), it, tb, float(dt)
+
+    def pusch_mcs(self, table, index):
+        r = ctypes.c_float()
+        qm = self.lib.ref_pusch_mcs(0 if table == 1 else 1, index, ctypes.byref(r))
+        return qm, float(r.value)
+
+    def tbs(self, nof_symb_sh, nof_dmrs_prb, nof_oh_prb, qm, rate_x1024, nof_layers, n_prb):
+        return int(self.lib.ref_tbs(nof_symb_sh, nof_dmrs_prb, nof_oh_prb, qm, ctypes.c_float(rate_x1024), nof_layers,
+                                    n_prb))
+
+    def base_graph(self, rate_x1024, tbs_bits):
+        return int(self.lib.ref_base_graph(ctypes.c_float(rate_x1024 / 1024.0), tbs_bits))
+
     def sch_segmentation(self, tbs_bits, bg):
         o = np.zeros(4, np.int32)
         self.lib.ref_sch_segmentation(tbs_bits, bg, _ptr(o))

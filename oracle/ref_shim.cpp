@@ -37,7 +37,13 @@
 #include "ocudu/phy/upper/equalization/dynamic_ch_est_list.h"
 #include "ocudu/phy/upper/equalization/equalization_factories.h"
 #include "ocudu/ran/sch/sch_segmentation.h"
+#include "ocudu/ran/pusch/pusch_mcs.h"
+#include "ocudu/ran/sch/ldpc_base_graph.h"
+#include "ocudu/ran/sch/tbs_calculator.h"
 #include "lib/phy/upper/channel_coding/ldpc/ldpc_graph_impl.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_rx.h"
+#include "ocudu/ocuduvec/bit.h"
+#include "../include/pusch_b200.h"
 #include <cstring>
 #include <map>
 #include <memory>
@@ -593,6 +599,248 @@ int ref_port_estimate(const uint32_t* grid,
     scalars[3 + l] = res.get_rsrp(l);
   }
   return 0;
+}
+
+/// PUSCH MCS (TS 38.214 Tables 5.1.3.1-1/2; table 0 = qam64, 1 = qam256), no transform
+/// precoding: returns Qm and writes the target code rate x 1024 (pusch_mcs_get_config).
+int ref_pusch_mcs(int table, int index, float* rate_x1024)
+{
+  const sch_mcs_description d = pusch_mcs_get_config(table == 0 ? pusch_mcs_table::qam64 : pusch_mcs_table::qam256,
+                                                     sch_mcs_index(static_cast<uint8_t>(index)), false, false);
+  *rate_x1024 = d.target_code_rate;
+  return static_cast<int>(get_bits_per_symbol(d.modulation));
+}
+
+/// Transport block size in bits (tbs_calculator_calculate, TS 38.214 Section 5.1.3.2).
+unsigned ref_tbs(int nof_symb_sh, int nof_dmrs_prb, int nof_oh_prb, int qm, float rate_x1024, int nof_layers, int n_prb)
+{
+  tbs_calculator_configuration cfg = {};
+  cfg.nof_symb_sh                  = nof_symb_sh;
+  cfg.nof_dmrs_prb                 = nof_dmrs_prb;
+  cfg.nof_oh_prb                   = nof_oh_prb;
+  cfg.mcs_descr.modulation         = to_mod(qm);
+  cfg.mcs_descr.target_code_rate   = rate_x1024;
+  cfg.nof_layers                   = nof_layers;
+  cfg.tb_scaling_field             = 0;
+  cfg.n_prb                        = n_prb;
+  return static_cast<unsigned>(units::bits(tbs_calculator_calculate(cfg)).value());
+}
+
+/// LDPC base graph (1 or 2) for a target code rate and payload size (TS 38.212 Section 7.2.2).
+int ref_base_graph(float rate, unsigned tbs_bits)
+{
+  return get_ldpc_base_graph(rate, units::bits(tbs_bits)) == ldpc_base_graph_type::BG1 ? 1 : 2;
+}
+
+/// The reference's CPU receive path for a batch of PUSCH PDUs, one UE at a time per thread, with
+/// the reference's own stage objects in the order pusch_processor_impl::process runs them
+/// (lib/phy/upper/channel_processors/pusch/pusch_processor_impl.cpp:349-900): DM-RS pilots and
+/// port_channel_estimator (FD filter, TD interpolate) per receive port, per data symbol
+/// get_symbol_ch_estimate + channel_equalizer (MMSE) + demodulation_mapper, descrambling with the
+/// pseudo-random generator, ldpc_segmenter_rx, then per codeblock ldpc_rate_dematcher and
+/// ldpc_decoder with CRC early stop, and the TB join of pusch_decoder_impl::join_and_notify
+/// (pusch_decoder_impl.cpp:612-710). No UCI, no HARQ combining. Threads claim UEs from a shared
+/// counter (independent UE-level work, as the reference's PUSCH processor pool runs them).
+/// ues: pg_pusch_ue array (include/pusch_b200.h layout); grids: cbf16 words; tb_out: TB bytes at
+/// each UE's tb_out_offset (written when the TB CRC passes); ok / iters: per UE. Returns wall s.
+double ref_pusch_decode_mt(const pg_pusch_ue* ues,
+                           int                nof_ues,
+                           const uint32_t*    grids,
+                           uint8_t*           tb_out,
+                           int32_t*           ok,
+                           float*             mean_iters,
+                           int                nof_threads)
+{
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    auto prg        = create_pseudo_random_generator_sw_factory()->create();
+    auto ta_factory = create_time_alignment_estimator_dft_factory(create_dft_processor_factory_generic());
+    auto est        = create_port_channel_estimator_factory_sw(ta_factory)
+                   ->create(port_channel_estimator_fd_smoothing_strategy::filter,
+                            port_channel_estimator_td_interpolation_strategy::interpolate,
+                            false);
+    auto eq    = create_channel_equalizer_generic_factory(channel_equalizer_algorithm_type::mmse)->create();
+    auto demap = create_demodulation_mapper_factory()->create();
+    auto seg   = create_ldpc_segmenter_rx_factory_sw()->create();
+    auto dem   = create_ldpc_rate_dematcher_factory_sw("auto")->create();
+    ldpc_decoder_factory::ldpc_decoder_factory_configuration dcfg_f = {false, false};
+    auto dec   = create_ldpc_decoder_factory_sw("auto", dcfg_f)->create();
+    auto crcf  = create_crc_calculator_factory_sw("auto");
+    auto crc16 = crcf->create(crc_generator_poly::CRC16);
+    auto crc24a = crcf->create(crc_generator_poly::CRC24A);
+    auto crc24b = crcf->create(crc_generator_poly::CRC24B);
+
+    for (int i = next++; i < nof_ues; i = next++) {
+      const pg_pusch_ue& u   = ues[i];
+      const unsigned     np  = u.nof_rx_ports;
+      const unsigned     nl  = u.nof_layers;
+      const unsigned     nsc = 12u * u.nof_rb;
+      const unsigned     qm  = u.modulation_order;
+      array_grid_reader  reader(grids + u.grid_offset, np, 14, u.grid_nof_subc);
+
+      // DM-RS pilots of every layer and the estimator configuration.
+      port_channel_estimator::configuration cfg;
+      cfg.scs          = subcarrier_spacing::kHz30;
+      cfg.cp           = cyclic_prefix::NORMAL;
+      cfg.first_symbol = u.first_symbol;
+      cfg.nof_symbols  = u.nof_symbols;
+      cfg.scaling      = u.dmrs_scaling;
+      for (unsigned p = 0; p < np; ++p) {
+        cfg.rx_ports.push_back(static_cast<uint8_t>(p));
+      }
+      bounded_bitset<MAX_NSYMB_PER_SLOT> symbols(14);
+      for (int s = 0; s < 14; ++s) {
+        if ((u.dmrs_symbol_mask >> s) & 1u) {
+          symbols.set(s);
+        }
+      }
+      crb_bitmap rb_mask(u.rb_start + u.nof_rb);
+      rb_mask.fill(u.rb_start, u.rb_start + u.nof_rb);
+      const unsigned   nof_dmrs = symbols.count();
+      dmrs_symbol_list pilots({6u * u.nof_rb, nof_dmrs, nl});
+      for (int s = 0, d = 0; s < 14; ++s) {
+        if (!symbols.test(s)) {
+          continue;
+        }
+        unsigned c_init =
+            ((14 * u.slot + s + 1) * (2 * u.n_id + 1) * (1U << 17) + (2 * u.n_id + u.n_scid)) % (1U << 31);
+        prg->init(c_init);
+        dmrs_sequence_generate(pilots.get_symbol(d, 0), *prg, M_SQRT1_2, 0, 6, rb_mask);
+        ++d;
+      }
+      for (unsigned l = 1; l < nl; ++l) {
+        dmrs_pxsch_parameters params = get_pxsch_dmrs_params(dmrs_config_type::type1, l);
+        for (unsigned d = 0; d != nof_dmrs; ++d) {
+          span<cf_t>       dst = pilots.get_symbol(d, l);
+          span<const cf_t> src = pilots.get_symbol(d, 0);
+          std::copy(src.begin(), src.end(), dst.begin());
+          if (params.w_f[0] != params.w_f[1]) {
+            for (unsigned k = 1; k < dst.size(); k += 2) {
+              dst[k] *= params.w_f[1];
+            }
+          }
+        }
+      }
+      for (unsigned l = 0; l < nl; ++l) {
+        dmrs_pxsch_parameters params = get_pxsch_dmrs_params(dmrs_config_type::type1, l);
+        cfg.dmrs_pattern.push_back({symbols, rb_mask, {}, std::nullopt, params.re_pattern});
+      }
+
+      // Channel estimates of every data symbol, layer and port; port noise variances.
+      std::vector<unsigned> data_syms;
+      for (unsigned s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
+        if (!symbols.test(s)) {
+          data_syms.push_back(s);
+        }
+      }
+      std::vector<cbf16_t> h((size_t)np * data_syms.size() * nl * nsc);
+      std::vector<float>   nvar(np);
+      for (unsigned p = 0; p < np; ++p) {
+        const port_channel_estimator_results& res = est->compute(reader, p, pilots, cfg);
+        nvar[p]                                   = res.get_noise_variance();
+        for (unsigned k = 0; k < data_syms.size(); ++k) {
+          for (unsigned l = 0; l < nl; ++l) {
+            res.get_symbol_ch_estimate(span<cbf16_t>(h.data() + (((size_t)p * data_syms.size() + k) * nl + l) * nsc, nsc),
+                                       data_syms[k], l);
+          }
+        }
+      }
+
+      // Equalisation and demapping per data symbol, then descrambling.
+      const unsigned                    g = data_syms.size() * nsc * nl * qm;
+      std::vector<log_likelihood_ratio> llr(g);
+      dynamic_re_buffer<cbf16_t>        y(np, nsc);
+      dynamic_ch_est_list               hl(nsc, np, nl);
+      std::vector<cf_t>                 eqs(nsc * nl);
+      std::vector<float>                eqv(nsc * nl);
+      for (unsigned k = 0; k < data_syms.size(); ++k) {
+        for (unsigned p = 0; p < np; ++p) {
+          span<const cbf16_t> row = reader.get_view(p, data_syms[k]);
+          std::copy_n(row.begin() + 12 * u.rb_start, nsc, y.get_slice(p).begin());
+          for (unsigned l = 0; l < nl; ++l) {
+            std::copy_n(h.data() + (((size_t)p * data_syms.size() + k) * nl + l) * nsc, nsc,
+                        hl.get_channel(p, l).begin());
+          }
+        }
+        eq->equalize(eqs, eqv, y, hl, nvar, 1.0F);
+        demap->demodulate_soft(span<log_likelihood_ratio>(llr).subspan((size_t)k * nsc * nl * qm, nsc * nl * qm), eqs, eqv,
+                               to_mod(qm));
+      }
+      prg->init((static_cast<unsigned>(u.rnti) << 15) + u.n_id_data);
+      prg->apply_xor(span<log_likelihood_ratio>(llr), span<const log_likelihood_ratio>(llr));
+
+      // Segmentation, dematching and decoding of every codeblock; TB join.
+      segmenter_config sc;
+      sc.transport_block_size = units::bytes(u.tbs_bits / 8);
+      sc.base_graph           = u.base_graph == 1 ? ldpc_base_graph_type::BG1 : ldpc_base_graph_type::BG2;
+      sc.rv                   = u.rv;
+      sc.mod                  = to_mod(qm);
+      sc.Nref                 = u.nref;
+      sc.nof_layers           = nl;
+      sc.nof_ch_symbols       = g / qm;
+      static_vector<described_rx_codeblock, MAX_NOF_SEGMENTS> cbs;
+      seg->segment(cbs, llr, sc);
+      const unsigned  C      = cbs.size();
+      crc_calculator* cb_crc = C > 1 ? crc24b.get() : (u.tbs_bits <= 3824 ? crc16.get() : crc24a.get());
+      std::vector<uint8_t> tb_bits;
+      bool                 all_ok = true;
+      unsigned             it_sum = 0;
+      for (unsigned c = 0; c < C; ++c) {
+        const codeblock_metadata& md = cbs[c].second;
+        const unsigned            N  = md.cb_specific.full_length;
+        const unsigned            z  = static_cast<unsigned>(md.tb_common.lifting_size);
+        const unsigned            K  = (u.base_graph == 1 ? 22 : 10) * z;
+        std::vector<log_likelihood_ratio> rm(N);
+        dem->rate_dematch(rm, cbs[c].first, true, md);
+        ldpc_decoder::configuration dc;
+        dc.base_graph      = sc.base_graph;
+        dc.lifting_size    = md.tb_common.lifting_size;
+        dc.nof_filler_bits = md.cb_specific.nof_filler_bits;
+        dc.nof_crc_bits    = md.cb_specific.nof_crc_bits;
+        dc.max_iterations  = u.max_iterations;
+        dynamic_bit_buffer           out(K);
+        std::optional<unsigned>      r = dec->decode(out, rm, cb_crc, dc);
+        all_ok                         = all_ok && r.has_value();
+        it_sum += r.has_value() ? *r : u.max_iterations;
+        const unsigned payload = K - md.cb_specific.nof_filler_bits - (C > 1 ? 24 : 0);
+        for (unsigned b = 0; b < payload; ++b) {
+          tb_bits.push_back(static_cast<uint8_t>(out.extract(b, 1)));
+        }
+      }
+      bool tb_ok = false;
+      if (C == 1) {
+        tb_ok = all_ok;
+      } else if (all_ok) {
+        dynamic_bit_buffer tb(u.tbs_bits);
+        ocuduvec::bit_pack(tb, span<const uint8_t>(tb_bits.data(), u.tbs_bits));
+        unsigned checksum = 0;
+        for (unsigned b = 0; b < 24; ++b) {
+          checksum = (checksum << 1) | tb_bits[u.tbs_bits + b];
+        }
+        tb_ok = crc24a->calculate(tb) == checksum;
+      }
+      ok[i]         = tb_ok ? 1 : 0;
+      mean_iters[i] = static_cast<float>(it_sum) / static_cast<float>(C);
+      if (tb_ok) {
+        for (unsigned b = 0; b < u.tbs_bits / 8; ++b) {
+          uint8_t v = 0;
+          for (unsigned j = 0; j < 8; ++j) {
+            v = static_cast<uint8_t>((v << 1) | tb_bits[8 * b + j]);
+          }
+          tb_out[u.tb_out_offset + b] = v;
+        }
+      }
+    }
+  };
+  const auto               t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> pool;
+  for (int t = 0; t < std::max(1, nof_threads); ++t) {
+    pool.emplace_back(worker);
+  }
+  for (auto& th : pool) {
+    th.join();
+  }
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 } // extern "C"
