@@ -54,7 +54,7 @@ INT_OPS_PER_EDGE = 10  # algorithmic integer operations per edge update (see DES
 def parse_args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="uneven", choices=["uneven", "ldpc"])
@@ -345,7 +345,7 @@ def run_ours_pusch(args):
             for _ in range(max(1, args.warmup)):
                 plain_step()
             pms = []
-            for k in range(max(3, args.steps // 5)):
+            for k in range(max(3, min(20, args.steps // 5))):
                 flush.fill_(k & 0xFF)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
@@ -375,7 +375,7 @@ def run_ours_pusch(args):
         for _ in range(max(args.warmup, 1)):
             e2e_step()
         et = []
-        for k in range(args.steps):
+        for k in range(min(args.steps, 200)):
             flush.fill_(k & 0xFF)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
@@ -683,7 +683,7 @@ def run_ours_ldpc(args):
 
 def ldpc_measure(args, dev, rank, world):
     """The LDPC batch as a sub-measurement of the PUSCH line (device-timed Gbit/s and roofline)."""
-    line = ldpc_core(args, dev, rank, world, with_cpu=False, with_e2e=False, steps=min(args.steps, 30))
+    line = ldpc_core(args, dev, rank, world, with_cpu=False, with_e2e=False, steps=min(args.steps, 100))
     if line is None:
         return None
     return {"value": line["value"], "unit": "Gbit/s", "ms_per_step": line["ms_per_step"],

@@ -119,6 +119,16 @@ __global__ void __launch_bounds__(kCrcThreads) crc_kernel(const pg_crc_item* __r
   }
 }
 
+// Transport-block assembly and TB CRC, split into chunks of kTbChunkWords 32-bit words so that a
+// large TB is spread over many CTAs (grid.x = TB, grid.y strides over its chunks). Each thread
+// gathers kTbWordsPerThread words of the TB from the codeblock payloads, stores them, and folds
+// its bytes with a byte-wise table (Sarwate) into the remainder of its piece alone; the piece's
+// contribution to the TB remainder is that value times x^(bits after the piece) mod g, and the
+// contributions meet by XOR (the CRC is linear) in tb_crc, which starts at zero.
+constexpr int kTbWordsPerThread = 4;
+constexpr int kTbChunkWords     = kCrcThreads * kTbWordsPerThread;
+constexpr int kTbGridY          = 16; // CTAs per TB: up to 16 chunks (512 Kbit) run in parallel
+
 __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_desc* __restrict__ tbs,
                                                                   const uint8_t* __restrict__ cb_bits,
                                                                   const uint32_t* __restrict__ cb_bit_offsets,
@@ -126,41 +136,68 @@ __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_de
                                                                   uint32_t* __restrict__ tb_crc,
                                                                   const uint32_t* __restrict__ tabs)
 {
+  __shared__ uint32_t byte_tab[256];
   __shared__ uint32_t red[kCrcThreads / 32];
   const pg_tb_desc    d = tbs[blockIdx.x];
   uint32_t            g;
   int                 order;
   pg::crc_poly_params(d.crc_poly, &g, &order);
-  const uint32_t* tab = tabs + (size_t)d.crc_poly * (1024 + 2048);
-  const uint32_t  P   = d.cb_payload_bits;
-  const uint32_t  L   = P * d.nof_cbs; // TBS + TB CRC bits
-  uint8_t*        out = tb_out + d.tb_out_offset;
-  const uint32_t  tb_bytes = d.tbs_bits / 8;
-  uint32_t        acc = 0;
-  for (uint32_t w = threadIdx.x; 32u * w < L; w += kCrcThreads) {
-    const uint32_t i0    = 32u * w;
-    const int      valid = (int)min(32u, L - i0);
-    // Gather the word from at most two codeblock payloads.
-    const uint32_t c0    = i0 / P;
-    const uint32_t o0    = i0 - c0 * P;
-    const int      n0    = (int)min((uint32_t)valid, P - o0);
-    uint32_t       bits  = load_bits(cb_bits, cb_bit_offsets[d.cb_first + c0] + o0, n0);
-    if (n0 < valid) {
-      const uint32_t rest = load_bits(cb_bits, cb_bit_offsets[d.cb_first + c0 + 1], valid - n0);
-      bits |= rest >> n0;
+  const uint32_t mask = (1u << order) - 1u;
+  {
+    // Remainder register after one byte i entered an all-zero register (MSB first).
+    uint32_t c = (uint32_t)threadIdx.x << (order - 8);
+    for (int k = 0; k < 8; ++k) {
+      c = ((c >> (order - 1)) & 1u) ? (((c << 1) ^ g) & mask) : ((c << 1) & mask);
     }
-    for (int b = 0; b < 4; ++b) {
-      const uint32_t byte = 4u * w + (uint32_t)b;
-      if (byte < tb_bytes) {
-        out[byte] = (uint8_t)(bits >> (24 - 8 * b));
-      }
-    }
-    const uint32_t e_lsb = L - i0 - (uint32_t)valid + (uint32_t)order - (uint32_t)(32 - valid);
-    acc ^= word_contribution(bits, valid, e_lsb, tab, g, order);
+    byte_tab[threadIdx.x] = c;
   }
-  const uint32_t crc = block_xor(acc, red);
-  if (threadIdx.x == 0) {
-    tb_crc[blockIdx.x] = crc;
+  __syncthreads();
+  const uint32_t* tab      = tabs + (size_t)d.crc_poly * (1024 + 2048);
+  const uint32_t  P        = d.cb_payload_bits;
+  const uint32_t  L        = P * d.nof_cbs; // TBS + TB CRC bits, a multiple of 8
+  const uint32_t  words    = (L + 31) / 32;
+  uint8_t*        out      = tb_out + d.tb_out_offset;
+  const uint32_t  tb_bytes = d.tbs_bits / 8;
+  for (uint32_t chunk = blockIdx.y; chunk * kTbChunkWords < words; chunk += gridDim.y) {
+    const uint32_t w0  = chunk * kTbChunkWords + threadIdx.x * kTbWordsPerThread;
+    uint32_t       rem = 0;
+    uint32_t       end_bit = 0;
+#pragma unroll
+    for (int k = 0; k < kTbWordsPerThread; ++k) {
+      const uint32_t w = w0 + (uint32_t)k;
+      if (w >= words) {
+        break;
+      }
+      const uint32_t i0    = 32u * w;
+      const int      valid = (int)min(32u, L - i0);
+      // Gather the word from at most two codeblock payloads.
+      const uint32_t c0   = i0 / P;
+      const uint32_t o0   = i0 - c0 * P;
+      const int      n0   = (int)min((uint32_t)valid, P - o0);
+      uint32_t       bits = load_bits(cb_bits, cb_bit_offsets[d.cb_first + c0] + o0, n0);
+      if (n0 < valid) {
+        const uint32_t rest = load_bits(cb_bits, cb_bit_offsets[d.cb_first + c0 + 1], valid - n0);
+        bits |= rest >> n0;
+      }
+      for (int b = 0; b < valid / 8; ++b) {
+        const uint32_t byte = 4u * w + (uint32_t)b;
+        const uint32_t v    = (bits >> (24 - 8 * b)) & 0xffu;
+        if (byte < tb_bytes) {
+          out[byte] = (uint8_t)v;
+        }
+        rem = ((rem << 8) & mask) ^ byte_tab[((rem >> (order - 8)) ^ v) & 0xffu];
+      }
+      end_bit = i0 + (uint32_t)valid;
+    }
+    uint32_t contrib = 0;
+    if (end_bit != 0 && rem != 0) {
+      contrib = gf2_mulmod(rem, xpow(tab, L - end_bit, g, order), g, order);
+    }
+    const uint32_t part = block_xor(contrib, red);
+    if (threadIdx.x == 0 && part != 0) {
+      atomicXor(tb_crc + blockIdx.x, part);
+    }
+    __syncthreads();
   }
 }
 
@@ -227,8 +264,12 @@ int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const 
   if (n == 0) {
     return PG_OK;
   }
-  tb_assemble_kernel<<<n, kCrcThreads, 0, stream>>>(tbs_dev, cb_bits, cb_bit_offsets, tb_out, tb_crc,
-                                                    ctx->dev.crc_tabs);
+  if (int rc = check_cuda(ctx, cudaMemsetAsync(tb_crc, 0, (size_t)n * sizeof(uint32_t), stream),
+                          "cudaMemsetAsync(tb crc)")) {
+    return rc;
+  }
+  tb_assemble_kernel<<<dim3(n, kTbGridY), kCrcThreads, 0, stream>>>(tbs_dev, cb_bits, cb_bit_offsets, tb_out, tb_crc,
+                                                                     ctx->dev.crc_tabs);
   return check_cuda(ctx, cudaGetLastError(), "tb_assemble_kernel launch");
 }
 

@@ -124,9 +124,12 @@ int demap_upload_tables(pg_context* ctx);
 int est_upload_tables(pg_context* ctx);
 int demod_upload_tables(pg_context* ctx, const void* slope, const void* intercept, const void* width);
 uint32_t ue_codeword_bits(const pg_pusch_ue& u);
-int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
-                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
-                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s);
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_re,
+                 const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                 const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
+                 cudaStream_t s);
+// Prefix sums (n + 1 entries) of the UEs' data REs; returns the total.
+uint32_t data_re_offsets(const pg_pusch_ue* ues, int n, uint32_t* off);
 // Host-side work lists of a batch of transport blocks: one rate-dematch and one LDPC descriptor
 // per codeblock, one TB descriptor per TB, the bit offset of each codeblock's decoded bits.
 struct sch_work {
@@ -143,16 +146,19 @@ int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t no
 int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,
                       const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s);
 // Demodulation with the scrambling sequences already generated.
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_re, const uint32_t* grids,
-                      const float* est, const pg_port_result* port_results, const uint32_t* seq_offsets_dev,
-                      const uint32_t* seq_dev, int8_t* llrs, cudaStream_t s);
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
+                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                      const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
+                      int8_t* llrs, cudaStream_t s);
 // Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
 // uses scratch_b; results and TB payloads land in host memory.
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
                            size_t nof_llrs, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
 int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
-int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* grids, float* est,
+// max_rb: the largest nof_rb of the UEs (sizes the kernel's shared memory).
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
                     pg_port_result* results, cudaStream_t s);
+int max_nof_rb(const pg_pusch_ue* ues, int n);
 int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1);
 int equalize_launch(pg_context* ctx, int nof_re, int nof_ports, int nof_layers, const uint32_t* y, const uint32_t* h,
                     const float* nvar_port_host, float tx, float2* out, float* out_var, cudaStream_t s);

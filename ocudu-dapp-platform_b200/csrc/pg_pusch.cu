@@ -11,8 +11,9 @@ namespace {
 struct slot_layout {
   std::vector<pg_pusch_ue> ues;
   std::vector<uint32_t>    seq_off;
+  std::vector<uint32_t>    offs; // [seq offsets (n) | data RE offsets (n + 1)]
   size_t                   est_total = 0, llr_total = 0, seq_total = 0;
-  uint32_t                 max_words = 0, max_re = 0;
+  uint32_t                 max_words = 0, total_re = 0;
 };
 
 // Assigns est/llr offsets and scrambling-sequence offsets.
@@ -33,12 +34,10 @@ void plan(const pg_pusch_ue* ues, int n, slot_layout& L, bool assign_offsets)
     const uint32_t words = (g + 31) / 32 + 2;
     L.seq_total += words;
     L.max_words = std::max(L.max_words, words);
-    int nd = 0;
-    for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
-      nd += (u.dmrs_symbol_mask >> s) & 1;
-    }
-    L.max_re = std::max(L.max_re, (uint32_t)(u.nof_symbols - nd) * 12u * u.nof_rb);
   }
+  L.offs.assign(2 * (size_t)n + 1, 0);
+  std::copy(L.seq_off.begin(), L.seq_off.end(), L.offs.begin());
+  L.total_re = data_re_offsets(L.ues.data(), n, L.offs.data() + n);
 }
 
 } // namespace
@@ -60,22 +59,23 @@ int pg_pusch_demodulate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_
   slot_layout L;
   plan(ues, nof_ues, L, false);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // Scratch: [sequence offsets | sequences].
-  const size_t bytes = 256 + (size_t)nof_ues * 4 + L.seq_total * 4;
+  // Scratch: [sequence offsets | data RE offsets | sequences].
+  const size_t noffs = L.offs.size();
+  const size_t bytes = 256 + noffs * 4 + L.seq_total * 4;
   if (int rc = ensure_scratch(ctx, &ctx->scratch_b, &ctx->scratch_b_cap, bytes, "cudaMalloc(demod scratch)")) {
     return rc;
   }
   uint32_t* d_off = static_cast<uint32_t*>(ctx->scratch_b);
-  uint32_t* d_seq = d_off + ((nof_ues + 63) / 64) * 64;
+  uint32_t* d_seq = d_off + ((noffs + 63) / 64) * 64;
   void*     d_ues = nullptr;
-  int       rc    = check_cuda(ctx, cudaMemcpyAsync(d_off, L.seq_off.data(), (size_t)nof_ues * 4, cudaMemcpyHostToDevice, s),
+  int       rc    = check_cuda(ctx, cudaMemcpyAsync(d_off, L.offs.data(), noffs * 4, cudaMemcpyHostToDevice, s),
                                "cudaMemcpyAsync(offsets)");
   if (rc == PG_OK) {
     rc = stage_slot(ctx, SLOT_UE, L.ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue), s, &d_ues);
   }
   if (rc == PG_OK) {
-    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.max_re, grids, est,
-                      port_results, d_off, d_seq, llrs, s);
+    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_re,
+                      d_off + nof_ues, grids, est, port_results, d_off, d_seq, llrs, s);
   }
   if (rc == PG_OK) {
     rc = release_slot_after(ctx, SLOT_UE, s);
@@ -116,7 +116,7 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
   const size_t o_est  = o_grid + al(grid_words * 4);
   const size_t o_pr   = o_est + al(L.est_total * 8);
   const size_t o_off  = o_pr + al((size_t)nof_ues * 4 * sizeof(pg_port_result));
-  const size_t o_seq  = o_off + al((size_t)nof_ues * 4);
+  const size_t o_seq  = o_off + al(L.offs.size() * 4);
   const size_t o_llr  = o_seq + al(L.seq_total * 4);
   const size_t total  = o_llr + al(L.llr_total);
   cudaStream_t s      = ctx->stream;
@@ -136,7 +136,7 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
   int8_t*         d_llr  = reinterpret_cast<int8_t*>(b + o_llr);
   rc = check_cuda(ctx, cudaMemcpyAsync(d_grid, grids, grid_words * 4, cudaMemcpyHostToDevice, s), "H2D grids");
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMemcpyAsync(d_off, L.seq_off.data(), (size_t)nof_ues * 4, cudaMemcpyHostToDevice, s),
+    rc = check_cuda(ctx, cudaMemcpyAsync(d_off, L.offs.data(), L.offs.size() * 4, cudaMemcpyHostToDevice, s),
                     "H2D offsets");
   }
   void* d_ues = nullptr;
@@ -144,11 +144,12 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
     rc = stage_slot(ctx, SLOT_UE, L.ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue), s, &d_ues);
   }
   if (rc == PG_OK) {
-    rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, d_grid, d_est, d_pr, s);
+    rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, max_nof_rb(ues, nof_ues), d_grid, d_est,
+                         d_pr, s);
   }
   if (rc == PG_OK) {
-    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.max_re, d_grid, d_est, d_pr,
-                      d_off, d_seq, d_llr, s);
+    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_re, d_off + nof_ues,
+                      d_grid, d_est, d_pr, d_off, d_seq, d_llr, s);
   }
   if (rc == PG_OK) {
     rc = release_slot_after(ctx, SLOT_UE, s);

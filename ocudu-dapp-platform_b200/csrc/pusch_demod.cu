@@ -71,7 +71,8 @@ __device__ __forceinline__ int8_t quantize(float v, float scale)
 }
 
 template <int QM>
-__device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* llr)
+__device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* llr, const float* s_slope,
+                                      const float* s_icpt, const float* s_width)
 {
   const float rcp = (nvar > 0.f) ? __frcp_rn(nvar) : 0.f;
   if (QM == 2) {
@@ -97,7 +98,7 @@ __device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* ll
   }
   constexpr int t     = QM == 6 ? 1 : 2;
   constexpr int nint  = QM == 6 ? 8 : 16;
-  const float   width = c_width_d[t];
+  const float   width = s_width[t];
   const float   x[2]  = {xr, xi};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
@@ -106,7 +107,9 @@ __device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* ll
     const bool z = fabsf(x[c]) <= 1e-9f;
 #pragma unroll
     for (int b = 0; b < QM / 2; ++b) {
-      const float v  = __fmul_rn(__fadd_rn(__fmul_rn(c_slope_d[t][b][idx], x[c]), c_intercept_d[t][b][idx]), rcp);
+      const float v  = __fmul_rn(__fadd_rn(__fmul_rn(s_slope[(t * 4 + b) * 16 + idx], x[c]),
+                                           s_icpt[(t * 4 + b) * 16 + idx]),
+                                 rcp);
       llr[2 * b + c] = quantize(z ? 0.f : v, 6.0f);
     }
   }
@@ -128,11 +131,17 @@ __global__ void scrambling_kernel(const pg_pusch_ue* __restrict__ ues, const uin
   }
 }
 
+struct demap_tables {
+  const float* slope;
+  const float* icpt;
+  const float* width;
+};
+
 template <int L, int P, int QM>
 __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* __restrict__ grid,
                                          const float2* __restrict__ est, const pg_port_result* __restrict__ pres,
                                          int nd, float w, int sym, int re_idx, int j, const uint32_t* __restrict__ seq,
-                                         int8_t* __restrict__ llr_out)
+                                         int8_t* __restrict__ llr_out, const demap_tables& tb)
 {
   const int nsc     = 12 * ue.nof_rb;
   const int sc      = 12 * ue.rb_start + j;
@@ -249,7 +258,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
   int8_t        llr[L * QM];
 #pragma unroll
   for (int l = 0; l < L; ++l) {
-    demap<QM>(s[l].r, s[l].i, nv[l], llr + l * QM);
+    demap<QM>(s[l].r, s[l].i, nv[l], llr + l * QM, tb.slope, tb.icpt, tb.width);
   }
   const uint32_t bit0 = (uint32_t)re_idx * L * QM;
   const uint32_t wa   = __ldg(seq + (bit0 >> 5));
@@ -267,27 +276,58 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
 template <int L, int P>
 __device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const uint32_t* grid, const float2* est,
                                                   const pg_port_result* pres, int nd, float w, int sym, int re_idx,
-                                                  int j, const uint32_t* seq, int8_t* llrs)
+                                                  int j, const uint32_t* seq, int8_t* llrs, const demap_tables& tb)
 {
   switch (ue.modulation_order) {
-    case 2: demod_re<L, P, 2>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
-    case 4: demod_re<L, P, 4>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
-    case 6: demod_re<L, P, 6>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
-    default: demod_re<L, P, 8>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs); break;
+    case 2: demod_re<L, P, 2>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 4: demod_re<L, P, 4>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 6: demod_re<L, P, 6>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    default: demod_re<L, P, 8>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
   }
 }
 
-__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues,
+// One thread per data resource element of the whole batch: re_off[u] .. re_off[u + 1] are the
+// data REs of UE u (data symbols x 12 nof_rb, symbol-major), so every CTA works on one or two
+// UEs and small UEs take no more threads than they have REs.
+__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, int nof_ues,
+                                                          const uint32_t* __restrict__ re_off,
                                                           const uint32_t* __restrict__ grids,
                                                           const float2* __restrict__ est_all,
                                                           const pg_port_result* __restrict__ port_results,
                                                           const uint32_t* __restrict__ seq_offsets,
                                                           const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs)
 {
-  const int         u  = blockIdx.y;
-  const pg_pusch_ue ue = ues[u];
+  __shared__ float s_slope[3 * 4 * 16];
+  __shared__ float s_icpt[3 * 4 * 16];
+  __shared__ float s_width[3];
+  for (int i = threadIdx.x; i < 3 * 4 * 16; i += blockDim.x) {
+    s_slope[i] = (&c_slope_d[0][0][0])[i];
+    s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
+  }
+  if (threadIdx.x < 3) {
+    s_width[threadIdx.x] = c_width_d[threadIdx.x];
+  }
+  __syncthreads();
+  const demap_tables tb = {s_slope, s_icpt, s_width};
+  const uint32_t     rg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rg >= __ldg(re_off + nof_ues)) {
+    return;
+  }
+  // UE of this RE: the last u with re_off[u] <= rg.
+  int lo = 0, hi = nof_ues - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(re_off + mid) <= rg) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  const int         u   = lo;
+  const pg_pusch_ue ue  = ues[u];
   const int         nsc = 12 * ue.nof_rb;
-  int               d0 = -1, d1 = -1, nd = 0, ndata = 0;
+  const int         r   = (int)(rg - __ldg(re_off + u));
+  int               d0 = -1, d1 = -1, nd = 0;
   for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
     if ((ue.dmrs_symbol_mask >> s) & 1) {
       if (nd == 0) {
@@ -296,42 +336,36 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
         d1 = s;
       }
       ++nd;
-    } else {
-      ++ndata;
     }
   }
-  const int total = ndata * nsc;
-  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < total; r += gridDim.x * blockDim.x) {
-    const int di = r / nsc;
-    const int j  = r - di * nsc;
-    // OFDM symbol of data-symbol index di.
-    int sym = ue.first_symbol, cnt = -1;
-    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-      if (!((ue.dmrs_symbol_mask >> s) & 1)) {
-        if (++cnt == di) {
-          sym = s;
-          break;
-        }
+  const int di = r / nsc;
+  const int j  = r - di * nsc;
+  // OFDM symbol of data-symbol index di.
+  int sym = ue.first_symbol, cnt = -1;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+    if (!((ue.dmrs_symbol_mask >> s) & 1)) {
+      if (++cnt == di) {
+        sym = s;
+        break;
       }
     }
-    const float             w    = nd == 2 ? (float)(sym - d0) / (float)(d1 - d0) : 0.f;
-    const uint32_t*         grid = grids + ue.grid_offset;
-    const float2*           est  = est_all + ue.est_offset;
-    const pg_port_result*   pres = port_results + (size_t)u * 4;
-    const uint32_t*         sq   = seq + seq_offsets[u];
-    if (ue.nof_layers == 1) {
-      switch (ue.nof_rx_ports) {
-        case 1: demod_dispatch_qm<1, 1>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
-        case 2: demod_dispatch_qm<1, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
-        default: demod_dispatch_qm<1, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
-      }
-    } else {
-      switch (ue.nof_rx_ports) {
-        case 2: demod_dispatch_qm<2, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
-        default: demod_dispatch_qm<2, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs); break;
-      }
+  }
+  const float           w    = nd == 2 ? (float)(sym - d0) / (float)(d1 - d0) : 0.f;
+  const uint32_t*       grid = grids + ue.grid_offset;
+  const float2*         est  = est_all + ue.est_offset;
+  const pg_port_result* pres = port_results + (size_t)u * 4;
+  const uint32_t*       sq   = seq + seq_offsets[u];
+  if (ue.nof_layers == 1) {
+    switch (ue.nof_rx_ports) {
+      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      default: demod_dispatch_qm<1, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
     }
-    (void)d1;
+  } else {
+    switch (ue.nof_rx_ports) {
+      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      default: demod_dispatch_qm<2, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+    }
   }
 }
 
@@ -371,28 +405,50 @@ int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
   return check_cuda(ctx, cudaGetLastError(), "scrambling_kernel launch");
 }
 
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_re, const uint32_t* grids,
-                      const float* est, const pg_port_result* port_results, const uint32_t* seq_offsets_dev,
-                      const uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
+                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                      const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
+                      int8_t* llrs, cudaStream_t s)
 {
-  if (n == 0) {
+  if (n == 0 || total_re == 0) {
     return PG_OK;
   }
-  pusch_demod_kernel<<<dim3(std::max(1u, std::min(1024u, (max_re + 255) / 256)), n), 256, 0, s>>>(
-      ues_dev, grids, reinterpret_cast<const float2*>(est), port_results, seq_offsets_dev, seq_dev, llrs);
+  pusch_demod_kernel<<<(total_re + 255) / 256, 256, 0, s>>>(ues_dev, n, re_off_dev, grids,
+                                                             reinterpret_cast<const float2*>(est), port_results,
+                                                             seq_offsets_dev, seq_dev, llrs);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 
 // Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
-// device scratch sized by the caller from ue_codeword_bits.
-int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t max_re,
-                 const uint32_t* grids, const float* est, const pg_port_result* port_results,
-                 const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs, cudaStream_t s)
+// device scratch sized by the caller from ue_codeword_bits, re_off_dev holds n + 1 prefix sums of
+// the UEs' data REs (data_re_offsets).
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_re,
+                 const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                 const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
+                 cudaStream_t s)
 {
   if (int rc = scrambling_launch(ctx, ues_dev, n, max_words, seq_offsets_dev, seq_dev, s)) {
     return rc;
   }
-  return demod_only_launch(ctx, ues_dev, n, max_re, grids, est, port_results, seq_offsets_dev, seq_dev, llrs, s);
+  return demod_only_launch(ctx, ues_dev, n, total_re, re_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
+                           llrs, s);
+}
+
+// Prefix sums of the UEs' data REs (data symbols x 12 nof_rb); returns the total.
+uint32_t data_re_offsets(const pg_pusch_ue* ues, int n, uint32_t* off)
+{
+  uint32_t t = 0;
+  for (int i = 0; i < n; ++i) {
+    off[i]        = t;
+    const auto& u = ues[i];
+    int         nd = 0;
+    for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
+      nd += (u.dmrs_symbol_mask >> s) & 1;
+    }
+    t += (uint32_t)(u.nof_symbols - nd) * 12u * u.nof_rb;
+  }
+  off[n] = t;
+  return t;
 }
 
 } // namespace pg

@@ -83,13 +83,36 @@ void gold_tables_host(std::vector<uint32_t>& tab, uint32_t words)
 
 namespace {
 
-struct est_smem {
-  float2   rx[kMaxDmrs][kMaxPil];
-  float2   ext[kMaxDmrs][2][kMaxPil + 2 * kMaxV];
-  float2   filt[kMaxDmrs][2][kMaxPil];
-  uint32_t bits[kMaxDmrs][(2 * kMaxPil) / 32 + 2];
-  float    red[3][kEstThreads / 32];
+// Dynamic shared memory of one CTA, sized for the largest allocation of the launch (npil_max
+// pilots per DM-RS symbol): pilot bits per DM-RS symbol, then the LS estimates of each (DM-RS
+// symbol, layer) extended by kMaxV virtual pilots at both ends, then the reduction scratch.
+struct est_layout {
+  uint32_t* bits; // [kMaxDmrs][bit_words]
+  float2*   ext;  // [kMaxDmrs][2][npil_max + 2 kMaxV]
+  float*    red;  // [3][kEstThreads / 32]
+  int       bit_words, ext_stride;
 };
+
+__host__ __device__ inline size_t est_smem_bytes(int npil_max)
+{
+  const size_t bit_words  = (size_t)(2 * npil_max) / 32 + 2;
+  const size_t ext_stride = (size_t)npil_max + 2 * kMaxV;
+  return 16 + kMaxDmrs * bit_words * 4 + kMaxDmrs * 2 * ext_stride * 8 + 3 * (kEstThreads / 32) * 4;
+}
+
+__device__ inline est_layout est_carve(unsigned char* raw, int npil_max)
+{
+  est_layout l;
+  l.bit_words  = (2 * npil_max) / 32 + 2;
+  l.ext_stride = npil_max + 2 * kMaxV;
+  l.bits       = reinterpret_cast<uint32_t*>(raw);
+  size_t off   = (size_t)kMaxDmrs * l.bit_words * 4;
+  off          = (off + 7) & ~(size_t)7;
+  l.ext        = reinterpret_cast<float2*>(raw + off);
+  off += (size_t)kMaxDmrs * 2 * l.ext_stride * 8;
+  l.red = reinterpret_cast<float*>(raw + off);
+  return l;
+}
 
 __device__ __forceinline__ float block_sum(float v, float* red, int slot_unused)
 {
@@ -175,10 +198,10 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
                                                                      float2* __restrict__ est_all,
                                                                      pg_port_result* __restrict__ results,
                                                                      const uint32_t* __restrict__ gold,
-                                                                     uint32_t gold_words)
+                                                                     uint32_t gold_words, int npil_max)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  est_smem&         sm   = *reinterpret_cast<est_smem*>(smem_raw);
+  const est_layout  sm   = est_carve(smem_raw, npil_max);
   const int         u    = blockIdx.x;
   const int         port = blockIdx.y;
   const pg_pusch_ue ue   = ues[u];
@@ -190,8 +213,11 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   const int nrb  = ue.nof_rb;
   const int npil = 6 * nrb;
   const int nsc  = 12 * nrb;
-  int       dsym[kMaxDmrs];
-  int       nd = 0;
+  if (npil > npil_max) {
+    return; // not reached: the host sizes the shared memory for the largest allocation
+  }
+  int dsym[kMaxDmrs];
+  int nd = 0;
   for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && nd < kMaxDmrs; ++s) {
     if ((ue.dmrs_symbol_mask >> s) & 1) {
       dsym[nd++] = s;
@@ -199,6 +225,11 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   }
   const float     beta = ue.dmrs_scaling;
   const uint32_t* grid = grids + ue.grid_offset + (size_t)port * 14 * ue.grid_nof_subc;
+  auto ext = [&](int d, int l) { return sm.ext + ((size_t)d * 2 + l) * sm.ext_stride; };
+  auto bit = [&](int d, int i) { return (sm.bits[d * sm.bit_words + (i >> 5)] >> (i & 31)) & 1u; };
+  auto rxp = [&](int d, int k) {
+    return cbf16_load(grid + (size_t)dsym[d] * ue.grid_nof_subc + 12 * ue.rb_start + 2 * k);
+  };
 
   // Pilot bits c(2 m0) .. c(2 m0 + 2 npil - 1) per DM-RS symbol, m0 = 6 rb_start.
   const int nwords = (2 * npil + 31) / 32;
@@ -208,7 +239,7 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
     const uint32_t c_init = (uint32_t)(((14ull * ue.slot + dsym[d] + 1) * (2ull * ue.n_id + 1) * (1ull << 17) +
                                         (2ull * ue.n_id + ue.n_scid)) %
                                        (1ull << 31));
-    sm.bits[d][w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 32u * w);
+    sm.bits[d * sm.bit_words + w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 32u * w);
   }
   __syncthreads();
 
@@ -217,18 +248,15 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   const float a        = 0.707106781186547524f; // 1/sqrt(2) (M_SQRT1_2 in float)
   float       epre     = 0.f;
   for (int i = tid; i < nd * npil; i += kEstThreads) {
-    const int    d   = i / npil;
-    const int    k   = i - d * npil;
-    const float2 y   = cbf16_load(grid + (size_t)dsym[d] * ue.grid_nof_subc + 12 * ue.rb_start + 2 * k);
-    sm.rx[d][k]      = y;
+    const int    d  = i / npil;
+    const int    k  = i - d * npil;
+    const float2 y  = rxp(d, k);
     epre += y.x * y.x + y.y * y.y;
-    const uint32_t b0 = (sm.bits[d][(2 * k) >> 5] >> ((2 * k) & 31)) & 1u;
-    const uint32_t b1 = (sm.bits[d][(2 * k + 1) >> 5] >> ((2 * k + 1) & 31)) & 1u;
-    const float2   p0 = make_float2(b0 ? -a : a, b1 ? -a : a);
-    sm.ext[d][0][kMaxV + k] = cmulconjf(y, p0);
+    const float2 p0 = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
+    ext(d, 0)[kMaxV + k] = cmulconjf(y, p0);
     if (nl > 1) {
-      const float2 p1         = (k & 1) ? make_float2(-p0.x, -p0.y) : p0;
-      sm.ext[d][1][kMaxV + k] = cmulconjf(y, p1);
+      const float2 p1      = (k & 1) ? make_float2(-p0.x, -p0.y) : p0;
+      ext(d, 1)[kMaxV + k] = cmulconjf(y, p1);
     }
   }
   __syncthreads();
@@ -237,100 +265,106 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
     const int r  = i - d * nl * (npil / 2);
     const int l  = r / (npil / 2);
     const int k  = 2 * (r - l * (npil / 2));
-    float2    v0 = sm.ext[d][l][kMaxV + k], v1 = sm.ext[d][l][kMaxV + k + 1];
+    float2*   e  = ext(d, l);
+    float2    v0 = e[kMaxV + k], v1 = e[kMaxV + k + 1];
     if (nl > 1) {
       const float2 av = make_float2((v0.x + v1.x) / 2.0f, (v0.y + v1.y) / 2.0f);
       v0 = v1 = av;
     }
-    sm.ext[d][l][kMaxV + k]     = make_float2(v0.x * inv_beta, v0.y * inv_beta);
-    sm.ext[d][l][kMaxV + k + 1] = make_float2(v1.x * inv_beta, v1.y * inv_beta);
+    e[kMaxV + k]     = make_float2(v0.x * inv_beta, v0.y * inv_beta);
+    e[kMaxV + k + 1] = make_float2(v1.x * inv_beta, v1.y * inv_beta);
   }
   __syncthreads();
 
   // Smoothing filter and virtual pilots.
-  const int  tsel  = nrb >= 3 ? 2 : nrb - 1;
-  const int  ntaps = tsel == 2 ? 15 : (tsel == 1 ? 11 : 5);
-  const int  mid   = ntaps / 2;
-  const int  nv    = nrb == 1 ? npil : mid;
+  const int tsel  = nrb >= 3 ? 2 : nrb - 1;
+  const int ntaps = tsel == 2 ? 15 : (tsel == 1 ? 11 : 5);
+  const int mid   = ntaps / 2;
+  const int nv    = nrb == 1 ? npil : mid;
   if (tid < nd * nl * 2) {
     const int d = tid / (nl * 2), l = (tid / 2) % nl, side = tid & 1;
+    float2*   e = ext(d, l);
     if (side == 0) {
-      virtual_pilots(&sm.ext[d][l][kMaxV - nv], &sm.ext[d][l][kMaxV], nv, true);
+      virtual_pilots(e + kMaxV - nv, e + kMaxV, nv, true);
     } else {
-      virtual_pilots(&sm.ext[d][l][kMaxV + npil], &sm.ext[d][l][kMaxV + npil - nv], nv, false);
+      virtual_pilots(e + kMaxV + npil, e + kMaxV + npil - nv, nv, false);
     }
   }
   __syncthreads();
-  float rsrp_part[2] = {0.f, 0.f};
+  // The smoothed pilots go straight to the even subcarriers of the output; the odd ones are filled
+  // below from their even neighbours, which this CTA reads back after a barrier.
+  float2* est          = est_all + ue.est_offset + (size_t)port * nd * nl * nsc;
+  float   rsrp_part[2] = {0.f, 0.f};
   for (int i = tid; i < nd * nl * npil; i += kEstThreads) {
-    const int d = i / (nl * npil);
-    const int r = i - d * nl * npil;
-    const int l = r / npil;
-    const int k = r - l * npil;
-    float2    acc = make_float2(0.f, 0.f);
+    const int     d   = i / (nl * npil);
+    const int     r   = i - d * nl * npil;
+    const int     l   = r / npil;
+    const int     k   = r - l * npil;
+    const float2* e   = ext(d, l);
+    float2        acc = make_float2(0.f, 0.f);
     for (int t = 0; t < ntaps; ++t) {
-      const float2 x = sm.ext[d][l][kMaxV + k - mid + t];
+      const float2 x = e[kMaxV + k - mid + t];
       acc.x += x.x * c_rc_taps[tsel][t];
       acc.y += x.y * c_rc_taps[tsel][t];
     }
-    sm.filt[d][l][k] = acc;
+    est[((size_t)d * nl + l) * nsc + 2 * k] = acc;
     rsrp_part[l] += acc.x * acc.x + acc.y * acc.y;
   }
   __syncthreads();
 
-  // Frequency interpolation to every subcarrier and noise estimation.
-  float2* est = est_all + ue.est_offset + (size_t)port * nd * nl * nsc;
-  for (int i = tid; i < nd * nl * nsc; i += kEstThreads) {
-    const int d = i / (nl * nsc);
-    const int r = i - d * nl * nsc;
-    const int l = r / nsc;
-    const int j = r - l * nsc;
-    const int k = j >> 1;
-    float2    v = sm.filt[d][l][k];
-    if ((j & 1) && k + 1 < npil) {
-      const float2 n = sm.filt[d][l][k + 1];
+  // Frequency interpolation to the odd subcarriers and noise estimation.
+  for (int i = tid; i < nd * nl * npil; i += kEstThreads) {
+    const int d   = i / (nl * npil);
+    const int r   = i - d * nl * npil;
+    const int l   = r / npil;
+    const int k   = r - l * npil;
+    float2*   row = est + ((size_t)d * nl + l) * nsc;
+    float2    v   = row[2 * k];
+    if (k + 1 < npil) {
+      const float2 n = row[2 * k + 2];
       v              = make_float2((n.x - v.x) * 0.5f + v.x, (n.y - v.y) * 0.5f + v.y);
     }
-    est[((size_t)d * nl + l) * nsc + j] = v;
+    row[2 * k + 1] = v;
   }
   float       noise = 0.f;
   const float sf    = beta / (float)nd;
   for (int i = tid; i < nd * npil; i += kEstThreads) {
-    const int      d  = i / npil;
-    const int      k  = i - d * npil;
-    const uint32_t b0 = (sm.bits[d][(2 * k) >> 5] >> ((2 * k) & 31)) & 1u;
-    const uint32_t b1 = (sm.bits[d][(2 * k + 1) >> 5] >> ((2 * k + 1) & 31)) & 1u;
-    const float2   p0 = make_float2(b0 ? -a : a, b1 ? -a : a);
-    float2         pred = make_float2(0.f, 0.f);
+    const int    d    = i / npil;
+    const int    k    = i - d * npil;
+    const float2 p0   = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
+    float2       pred = make_float2(0.f, 0.f);
     for (int l = 0; l < nl; ++l) {
-      float2 s = make_float2(0.f, 0.f);
+      float2 sacc = make_float2(0.f, 0.f);
       for (int dd = 0; dd < nd; ++dd) {
-        s.x += sm.filt[dd][l][k].x * sf;
-        s.y += sm.filt[dd][l][k].y * sf;
+        const float2 f = est[((size_t)dd * nl + l) * nsc + 2 * k];
+        sacc.x += f.x * sf;
+        sacc.y += f.y * sf;
       }
       const float2 p = (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
-      const float2 q = cmulf(s, p);
+      const float2 q = cmulf(sacc, p);
       pred.x += q.x;
       pred.y += q.y;
     }
-    const float2 e = make_float2(pred.x - sm.rx[d][k].x, pred.y - sm.rx[d][k].y);
+    const float2 y = rxp(d, k);
+    const float2 e = make_float2(pred.x - y.x, pred.y - y.y);
     noise += e.x * e.x + e.y * e.y;
   }
-  const float tot_noise = block_sum(noise, sm.red[0], 0);
-  const float tot_epre  = block_sum(epre, sm.red[1], 1);
-  const float tot_r0    = block_sum(rsrp_part[0], sm.red[2], 2);
-  const float tot_r1    = block_sum(rsrp_part[1], sm.red[0], 0);
+  float*      red       = sm.red;
+  const float tot_noise = block_sum(noise, red, 0);
+  const float tot_epre  = block_sum(epre, red + (kEstThreads / 32), 1);
+  const float tot_r0    = block_sum(rsrp_part[0], red + 2 * (kEstThreads / 32), 2);
+  const float tot_r1    = block_sum(rsrp_part[1], red, 0);
   if (tid == 0) {
     const float    n_pil = (float)(npil * nd);
     pg_port_result pr;
-    pr.rsrp[0]        = tot_r0 * beta * beta / n_pil;
-    pr.rsrp[1]        = nl > 1 ? tot_r1 * beta * beta / n_pil : 0.f;
-    pr.epre           = tot_epre / n_pil;
-    const float ravg  = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
-    float       nvar  = (pg::is_normal(tot_noise) ? tot_noise : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
-    nvar              = fmaxf(ravg / 1e10f, nvar);
-    pr.noise_var      = nvar;
-    pr.snr            = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
+    pr.rsrp[0]       = tot_r0 * beta * beta / n_pil;
+    pr.rsrp[1]       = nl > 1 ? tot_r1 * beta * beta / n_pil : 0.f;
+    pr.epre          = tot_epre / n_pil;
+    const float ravg = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
+    float       nvar = (pg::is_normal(tot_noise) ? tot_noise : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
+    nvar             = fmaxf(ravg / 1e10f, nvar);
+    pr.noise_var     = nvar;
+    pr.snr           = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
     results[(size_t)u * 4 + port] = pr;
   }
 }
@@ -391,7 +425,7 @@ int est_upload_tables(pg_context* ctx)
   }
   int rc2 = check_cuda(ctx,
                        cudaFuncSetAttribute(pusch_estimate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)sizeof(est_smem)),
+                                            (int)est_smem_bytes(kMaxPil)),
                        "cudaFuncSetAttribute(pusch_estimate_kernel)");
   if (rc2 != PG_OK) {
     return rc2;
@@ -434,15 +468,25 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
   return PG_OK;
 }
 
-int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* grids, float* est,
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
                     pg_port_result* results, cudaStream_t s)
 {
   if (n == 0) {
     return PG_OK;
   }
-  pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, sizeof(est_smem), s>>>(
-      ues_dev, grids, reinterpret_cast<float2*>(est), results, ctx->dev.gold, kGoldWords);
+  const int npil_max = 6 * std::max(1, std::min(max_rb, 275));
+  pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, est_smem_bytes(npil_max), s>>>(
+      ues_dev, grids, reinterpret_cast<float2*>(est), results, ctx->dev.gold, kGoldWords, npil_max);
   return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
+}
+
+int max_nof_rb(const pg_pusch_ue* ues, int n)
+{
+  int m = 1;
+  for (int i = 0; i < n; ++i) {
+    m = std::max(m, (int)ues[i].nof_rb);
+  }
+  return m;
 }
 
 int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1)
@@ -493,7 +537,8 @@ int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ue
   if (int rc = stage_slot(ctx, SLOT_UE, ues, (size_t)nof_ues * sizeof(pg_pusch_ue), s, &dev)) {
     return rc;
   }
-  if (int rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(dev), nof_ues, grids, est, results, s)) {
+  if (int rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(dev), nof_ues, max_nof_rb(ues, nof_ues), grids, est,
+                               results, s)) {
     return rc;
   }
   return release_slot_after(ctx, SLOT_UE, s);

@@ -23,7 +23,8 @@ struct pg_pusch_plan {
   pg_context*              ctx = nullptr;
   int                      nof_ues = 0, nof_cbs = 0;
   size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0;
-  uint32_t                 max_re = 0;
+  uint32_t                 total_re = 0;
+  int                      max_rb   = 1;
   std::vector<pg_pusch_ue> ues;
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
@@ -33,6 +34,7 @@ struct pg_pusch_plan {
   pg_tb_desc*     d_tb     = nullptr;
   uint32_t*       d_cb_off = nullptr;
   uint32_t*       d_seq_off = nullptr;
+  uint32_t*       d_re_off = nullptr;
   uint32_t*       d_seq    = nullptr;
   float*          d_est    = nullptr;
   pg_port_result* d_pr     = nullptr;
@@ -95,10 +97,10 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
             pg_port_result* port_results, cudaStream_t s)
 {
   pg_context* ctx = p->ctx;
-  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, grids, p->d_est, port_results, s);
+  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->max_rb, grids, p->d_est, port_results, s);
   if (rc == PG_OK) {
-    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->max_re, grids, p->d_est, port_results, p->d_seq_off,
-                           p->d_seq, p->d_llr, s);
+    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
+                           p->d_seq_off, p->d_seq, p->d_llr, s);
   }
   if (rc == PG_OK) {
     rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s);
@@ -177,8 +179,6 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     const uint32_t words = (g + 31) / 32 + 2;
     seq_total += words;
     max_words = std::max(max_words, words);
-    int d0 = 0, d1 = 0;
-    p->max_re    = std::max(p->max_re, (uint32_t)(u.nof_symbols - dmrs_count(u, &d0, &d1)) * 12u * u.nof_rb);
     p->tb_bytes  = std::max(p->tb_bytes, (size_t)u.tb_out_offset + u.tbs_bits / 8);
     pg_sch_tb& t = tbs[i];
     t            = pg_sch_tb{};
@@ -193,6 +193,9 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     t.rv               = u.rv;
     t.max_iterations   = u.max_iterations;
   }
+  p->max_rb = max_nof_rb(p->ues.data(), nof_ues);
+  std::vector<uint32_t> re_off(nof_ues + 1);
+  p->total_re = data_re_offsets(p->ues.data(), nof_ues, re_off.data());
   sch_work w;
   if (int rc = build_sch_work(ctx, tbs.data(), nof_ues, p->nof_llrs, p->tb_bytes, w)) {
     release(p);
@@ -207,7 +210,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_tb     = o_ldpc + al(w.ldpc.size() * sizeof(pg_ldpc_cb));
   const size_t o_cb_off = o_tb + al(w.tbd.size() * sizeof(pg_tb_desc));
   const size_t o_seqoff = o_cb_off + al(w.cb_bit_off.size() * 4);
-  const size_t desc_end = o_seqoff + al((size_t)nof_ues * 4);
+  const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
+  const size_t desc_end = o_reoff + al(re_off.size() * 4);
   const size_t o_seq    = desc_end;
   const size_t o_est    = o_seq + al(seq_total * 4);
   const size_t o_pr     = o_est + al(est_total * 8);
@@ -245,6 +249,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_tb      = reinterpret_cast<pg_tb_desc*>(b + o_tb);
   p->d_cb_off  = reinterpret_cast<uint32_t*>(b + o_cb_off);
   p->d_seq_off = reinterpret_cast<uint32_t*>(b + o_seqoff);
+  p->d_re_off  = reinterpret_cast<uint32_t*>(b + o_reoff);
   p->d_seq     = reinterpret_cast<uint32_t*>(b + o_seq);
   p->d_est     = reinterpret_cast<float*>(b + o_est);
   p->d_pr      = reinterpret_cast<pg_port_result*>(b + o_pr);
@@ -267,6 +272,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_tb, w.tbd.data(), w.tbd.size() * sizeof(pg_tb_desc));
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
+  std::memcpy(h + o_reoff, re_off.data(), re_off.size() * 4);
   cudaStream_t s = ctx->stream;
   rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
   if (rc == PG_OK) {

@@ -9,13 +9,14 @@
 // cycle of length V = N_cb - F; position p with valid index v receives the de-interleaved inputs
 // t = (v - v0) mod V, t + V, t + 2V, ... < E, summed in that order onto 0 (new data) or onto the
 // previous buffer content (soft combining). Filler positions hold +127; positions at or beyond N_cb
-// are zeroed on new data and untouched otherwise. One CTA per codeblock, threads stride the
-// N output positions (coalesced stores).
+// are zeroed on new data and untouched otherwise. kRmGridY CTAs per codeblock, threads stride
+// the N output positions (coalesced stores).
 #include "pg_internal.h"
 
 namespace {
 
 constexpr int kRmThreads = 256;
+constexpr int kRmGridY   = 8;
 
 __device__ __forceinline__ int llr_sum(int a, int b)
 {
@@ -57,7 +58,10 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   int8_t*        out = out_all + d.out_offset;
   const bool     nd  = d.new_data != 0;
 
-  for (int p = threadIdx.x; p < N; p += kRmThreads) {
+  // De-interleaver index src = (t mod Kq) * Qm + t div Kq with the quotient from a float
+  // reciprocal, corrected to the exact value (t < 2^24).
+  const float inv_kq = 1.0f / (float)(Kq > 0 ? Kq : 1);
+  for (int p = blockIdx.y * kRmThreads + threadIdx.x; p < N; p += gridDim.y * kRmThreads) {
     if (p >= inf && p < sys) {
       out[p] = 127;
       continue;
@@ -73,8 +77,20 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
     t             = t < 0 ? t + V : t;
     int       acc = nd ? 0 : (int)out[p];
     for (; t < E; t += V) {
-      const int src = (Qm > 1) ? (t % Kq) * Qm + t / Kq : t;
-      acc           = llr_sum(acc, in[src]);
+      int src = t;
+      if (Qm > 1) {
+        int q = __float2int_rz((float)t * inv_kq);
+        int r = t - q * Kq;
+        if (r < 0) {
+          --q;
+          r += Kq;
+        } else if (r >= Kq) {
+          ++q;
+          r -= Kq;
+        }
+        src = r * Qm + q;
+      }
+      acc = llr_sum(acc, in[src]);
     }
     out[p] = (int8_t)acc;
   }
@@ -131,7 +147,8 @@ int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const
   if (n == 0) {
     return PG_OK;
   }
-  rate_dematch_kernel<<<n, kRmThreads, 0, stream>>>(descs_dev, in, out);
+  // Each codeblock's N <= 25,344 output positions spread over kRmGridY CTAs.
+  rate_dematch_kernel<<<dim3(n, kRmGridY), kRmThreads, 0, stream>>>(descs_dev, in, out);
   return check_cuda(ctx, cudaGetLastError(), "rate_dematch_kernel launch");
 }
 
