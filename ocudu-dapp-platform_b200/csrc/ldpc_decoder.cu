@@ -22,6 +22,7 @@
 // K*Z - F significant bits; CRC == 0 stops with iterations = it + 1.
 #include "pg_internal.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <mutex>
 
@@ -198,11 +199,13 @@ struct smem_t {
   int                  s_done;
 };
 
-// Decodes codeblock blockIdx.x; ZT > 0 specialises the lifting size at compile time.
+// Decodes codeblock cb with check-to-variable slab `slab`; ZT > 0 specialises the lifting size
+// at compile time.
 template <int ZT>
 __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm, const int8_t* __restrict__ llrs,
                                                  uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
-                                                 int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow)
+                                                 int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
+                                                 const int cb, const int slab)
 {
   int8_t*   soft   = sm.soft;
   uint32_t* edge   = sm.edge;
@@ -216,7 +219,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   const int        set = (Z >= 2 && Z <= pg::kMaxZ) ? dev_set_index(Z) : -1;
   if ((bg != 1 && bg != 2) || set < 0) {
     if (tid == 0) {
-      iterations[blockIdx.x] = -1;
+      iterations[cb] = -1;
     }
     return;
   }
@@ -228,7 +231,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   const int     msg_len  = Kb * Z;
   const int     n        = (int)d.nof_llrs;
   const int8_t* in       = llrs + d.llr_offset;
-  int8_t*       c2v      = c2v_all + (size_t)blockIdx.x * pg::kC2vStride;
+  int8_t*       c2v      = c2v_all + (size_t)slab * pg::kC2vStride;
   const int     nbytes   = (msg_len + 7) / 8;
   uint8_t*      out      = bits + d.out_offset;
   const int     crc_poly = d.crc_poly;
@@ -246,31 +249,45 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   }
   __syncthreads();
 
-  // Trim trailing zero LLRs (ldpc_decoder_impl.cpp:66-71).
-  int last = 0;
-  for (int i = tid; i < n; i += kThreads) {
-    if (in[i] != 0) {
-      last = i + 1;
+  // One pass over the input: soft bits (2Z punctured zeros, whole nodes clamped to +-64, a ragged
+  // tail as is, ldpc_decoder_impl.cpp:147-188) and the last non-zero LLR (the trailing-zero trim,
+  // ldpc_decoder_impl.cpp:66-71), four LLRs per thread step.
+  const int nof_full = (n / Z) * Z;
+  const int soft_len = nfull * Z;
+  for (int i = tid; i < 2 * Z; i += kThreads) {
+    soft[i] = 0;
+  }
+  for (int i = 2 * Z + n + tid; i < soft_len; i += kThreads) {
+    soft[i] = 0;
+  }
+  int        last    = 0;
+  const bool aligned = (reinterpret_cast<uintptr_t>(in) & 3u) == 0;
+  for (int k0 = 4 * tid; k0 < n; k0 += 4 * kThreads) {
+    int v[4];
+    if (aligned && k0 + 3 < n) {
+      const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(in + k0));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        v[j] = (int)(int8_t)(w >> (8 * j));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        v[j] = k0 + j < n ? (int)in[k0 + j] : 0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = k0 + j;
+      if (k < n && 2 * Z + k < soft_len) {
+        last = v[j] != 0 ? k + 1 : last;
+        soft[2 * Z + k] = (int8_t)(k < nof_full ? max(-64, min(64, v[j])) : v[j]);
+      }
     }
   }
   last = warp_max(last);
   if ((tid & 31) == 0 && last > 0) {
     atomicMax(&s_last, last);
-  }
-
-  // Soft bits: 2Z punctured zeros, whole nodes clamped to +-64, a ragged tail as is
-  // (ldpc_decoder_impl.cpp:147-188).
-  const int nof_full = (n / Z) * Z;
-  for (int i = tid; i < nfull * Z; i += kThreads) {
-    int v = 0;
-    const int k = i - 2 * Z;
-    if (k >= 0 && k < n) {
-      v = in[k];
-      if (k < nof_full) {
-        v = max(-64, min(64, v));
-      }
-    }
-    soft[i] = (int8_t)v;
   }
   __syncthreads();
 
@@ -280,7 +297,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
       out[b] = 0xff;
     }
     if (tid == 0) {
-      iterations[blockIdx.x] = 0;
+      iterations[cb] = 0;
     }
     return;
   }
@@ -412,24 +429,52 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
     out[b] = (uint8_t)(hard[b >> 2] >> (24 - 8 * (b & 3)));
   }
   if (tid == 0) {
-    iterations[blockIdx.x] = result;
+    iterations[cb] = result;
   }
 }
 
 
+// counter == nullptr: one CTA per codeblock (blockIdx.x), slab blockIdx.x. Otherwise a persistent
+// grid: each CTA takes the next work index from *counter (zeroed before the launch), decodes
+// codeblock order[w] (or w) with its own slab blockIdx.x, and stops when the n codeblocks are
+// taken. Codeblocks are independent, so the order of work changes no result.
 __global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_cb* __restrict__ descs,
                                                               const int8_t* __restrict__ llrs,
                                                               uint8_t* __restrict__ bits,
                                                               int32_t* __restrict__ iterations,
                                                               int8_t* __restrict__ c2v_all,
-                                                              const uint32_t* __restrict__ crc_pow)
+                                                              const uint32_t* __restrict__ crc_pow,
+                                                              const uint32_t* __restrict__ order, int n,
+                                                              int* __restrict__ counter)
 {
   __shared__ smem_t sm;
-  const pg_ldpc_cb  d = descs[blockIdx.x];
-  if (d.lifting_size == 384) {
-    decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow);
-  } else {
-    decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow);
+  __shared__ int    s_work;
+  if (counter == nullptr) {
+    const pg_ldpc_cb d = descs[blockIdx.x];
+    if (d.lifting_size == 384) {
+      decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
+    } else {
+      decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
+    }
+    return;
+  }
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_work = atomicAdd(counter, 1);
+    }
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= n) {
+      break;
+    }
+    const int        cb = order != nullptr ? (int)order[w] : w;
+    const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size == 384) {
+      decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+    } else {
+      decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+    }
   }
 }
 
@@ -497,13 +542,35 @@ int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_
 int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                         int32_t* iterations, int8_t* c2v, cudaStream_t stream)
 {
+  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, nullptr, ctx->dev.ldpc_counter,
+                                stream);
+}
+
+int ldpc_resident_ctas(pg_context* ctx)
+{
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ldpc_decode_kernel, kThreads, 0) != cudaSuccess ||
+      per_sm < 1) {
+    (void)cudaGetLastError();
+    per_sm = 1;
+  }
+  return per_sm * ctx->sm_count;
+}
+
+int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                           int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
+                           cudaStream_t stream)
+{
   if (n == 0) {
     return PG_OK;
   }
+  if (int rc = check_cuda(ctx, cudaMemsetAsync(counter, 0, sizeof(int), stream), "cudaMemsetAsync(ldpc counter)")) {
+    return rc;
+  }
   // Under stream capture the timing events become event-record nodes of the graph (external
   // records); a plain record there would only mark a capture dependency.
-  unsigned int                rec_flags = cudaEventRecordDefault;
-  cudaStreamCaptureStatus     capturing = cudaStreamCaptureStatusNone;
+  unsigned int            rec_flags = cudaEventRecordDefault;
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
   if (ctx->timed && cudaStreamIsCapturing(stream, &capturing) == cudaSuccess &&
       capturing == cudaStreamCaptureStatusActive) {
     rec_flags = cudaEventRecordExternal;
@@ -511,7 +578,9 @@ int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, con
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  ldpc_decode_kernel<<<n, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow);
+  const int grid = std::min(n, ctx->ldpc_ctas);
+  ldpc_decode_kernel<<<grid, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, order, n,
+                                                    counter);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, stream, rec_flags);
   }
@@ -598,8 +667,8 @@ extern "C" int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldp
   int8_t* scratch = nullptr;
   int     rc      = static_scratch_address(ctx, &scratch);
   if (rc == PG_OK) {
-    ldpc_decode_kernel<<<nof_cbs, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(cbs_dev, llrs, bits, iterations,
-                                                                                     scratch, ctx->dev.crc_pow);
+    ldpc_decode_kernel<<<nof_cbs, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+        cbs_dev, llrs, bits, iterations, scratch, ctx->dev.crc_pow, nullptr, nof_cbs, nullptr);
     rc = pg::check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch (static scratch)");
   }
   if (prev != ctx->device) {

@@ -286,6 +286,12 @@ int pg_create(const pg_config* cfg, pg_context** out)
                     "cudaMalloc(iterations)");
   }
   if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_counter, sizeof(int)), "cudaMalloc(ldpc counter)");
+  }
+  if (rc == PG_OK) {
+    ctx->ldpc_ctas = ldpc_resident_ctas(ctx);
+  }
+  if (rc == PG_OK) {
     // x^e mod g(x) for CRC16, CRC24A and CRC24B.
     std::vector<uint32_t> pow(3 * (size_t)kCrcPowLen);
     for (int p = 0; p < 3; ++p) {
@@ -362,6 +368,7 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.llrs);
   cudaFree(ctx->dev.bits);
   cudaFree(ctx->dev.iterations);
+  cudaFree(ctx->dev.ldpc_counter);
   if (ctx->host_descs) {
     cudaFreeHost(ctx->host_descs);
   }

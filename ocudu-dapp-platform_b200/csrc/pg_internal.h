@@ -62,6 +62,7 @@ struct device_buffers {
   int8_t*      llrs        = nullptr; // staging for _host calls
   uint8_t*     bits        = nullptr;
   int32_t*     iterations  = nullptr;
+  int*         ldpc_counter = nullptr; // work counter of the persistent decoder
   size_t       llr_cap     = 0;
   size_t       bits_cap    = 0;
 };
@@ -72,6 +73,7 @@ struct pg_context {
   int                 device         = 0;
   int                 max_codeblocks = 0;
   int                 sm_count       = 0;
+  int                 ldpc_ctas      = 1;       // resident decoder CTAs on the device
   pg::device_buffers  dev;
   pg_ldpc_cb*         host_descs     = nullptr; // pinned staging for descriptors
   void*               host_stage     = nullptr; // pinned staging for _host calls
@@ -167,8 +169,15 @@ int demap_launch(pg_context* ctx, int qm, int n, const float2* sym, const float*
 // Enqueues the batched decoder; descs_dev holds n descriptors in device memory.
 int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                 int32_t* iterations, cudaStream_t stream);
-// Same with a caller-provided check-to-variable scratch of n * kC2vStride bytes.
+// Same with a caller-provided check-to-variable scratch of min(n, ldpc_ctas) * kC2vStride bytes.
 int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                         int32_t* iterations, int8_t* c2v, cudaStream_t stream);
+// Persistent launch: min(n, ldpc_ctas) CTAs take codeblocks order[0..n) (identity when order is
+// null) from *counter (device int, zeroed here on the stream); c2v holds one slab per CTA.
+int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                           int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
+                           cudaStream_t stream);
+// CTAs of ldpc_decode_kernel resident on the whole device.
+int ldpc_resident_ctas(pg_context* ctx);
 
 } // namespace pg

@@ -44,6 +44,8 @@ struct pg_pusch_plan {
   uint32_t*       d_tb_crc = nullptr;
   int32_t*        d_iters  = nullptr;
   int8_t*         d_c2v    = nullptr;
+  uint32_t*       d_order  = nullptr; // LDPC work order: largest codeblocks first
+  int*            d_counter = nullptr; // work counter of the persistent decoder
   uint32_t*       d_grid   = nullptr; // grids of execute_host
   uint8_t*        d_tb_out = nullptr; // TBs of execute_host
   pg_sch_result*  d_res    = nullptr; // results of execute_host
@@ -106,7 +108,8 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s);
   }
   if (rc == PG_OK) {
-    rc = ldpc_launch_scratch(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v, s);
+    rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
+                                p->d_order, p->d_counter, s);
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
@@ -202,6 +205,17 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     return rc;
   }
   p->nof_cbs = (int)w.ldpc.size();
+  // LDPC work order, largest first: a codeblock's cost grows with Z times the LLR positions it
+  // fills (E + F, at most N), which fix the check rows it runs.
+  std::vector<uint32_t> order(p->nof_cbs);
+  std::vector<uint64_t> cost(p->nof_cbs);
+  for (int c = 0; c < p->nof_cbs; ++c) {
+    const pg_ldpc_cb& l = w.ldpc[c];
+    order[c]            = (uint32_t)c;
+    cost[c]             = (uint64_t)l.lifting_size * std::min<uint64_t>(w.rm[c].rm_length + l.nof_filler_bits, l.nof_llrs);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
+  const int ldpc_slabs = std::max(1, std::min(p->nof_cbs, ctx->ldpc_ctas));
 
   // Device image: descriptors first (uploaded once), then the workspace.
   const size_t o_ues    = 0;
@@ -209,7 +223,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_ldpc   = o_rm + al(w.rm.size() * sizeof(pg_rm_cb));
   const size_t o_tb     = o_ldpc + al(w.ldpc.size() * sizeof(pg_ldpc_cb));
   const size_t o_cb_off = o_tb + al(w.tbd.size() * sizeof(pg_tb_desc));
-  const size_t o_seqoff = o_cb_off + al(w.cb_bit_off.size() * 4);
+  const size_t o_order  = o_cb_off + al(w.cb_bit_off.size() * 4);
+  const size_t o_seqoff = o_order + al(order.size() * 4);
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
   const size_t desc_end = o_reoff + al(re_off.size() * 4);
   const size_t o_seq    = desc_end;
@@ -220,8 +235,9 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_bits   = o_rmout + al(w.rm_total);
   const size_t o_crc    = o_bits + al(w.bits_total);
   const size_t o_it     = o_crc + al((size_t)nof_ues * 4);
-  const size_t o_c2v    = o_it + al((size_t)p->nof_cbs * 4);
-  const size_t o_grid   = o_c2v + al((size_t)p->nof_cbs * kC2vStride);
+  const size_t o_cnt    = o_it + al((size_t)p->nof_cbs * 4);
+  const size_t o_c2v    = o_cnt + al(sizeof(int));
+  const size_t o_grid   = o_c2v + al((size_t)ldpc_slabs * kC2vStride);
   const size_t o_tbout  = o_grid + al(grid_words * 4);
   const size_t o_res    = o_tbout + al(p->tb_bytes);
   p->dev_bytes          = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
@@ -259,6 +275,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_tb_crc  = reinterpret_cast<uint32_t*>(b + o_crc);
   p->d_iters   = reinterpret_cast<int32_t*>(b + o_it);
   p->d_c2v     = reinterpret_cast<int8_t*>(b + o_c2v);
+  p->d_order   = reinterpret_cast<uint32_t*>(b + o_order);
+  p->d_counter = reinterpret_cast<int*>(b + o_cnt);
   p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
   p->d_tb_out  = b + o_tbout;
   p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);
@@ -271,6 +289,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_ldpc, w.ldpc.data(), w.ldpc.size() * sizeof(pg_ldpc_cb));
   std::memcpy(h + o_tb, w.tbd.data(), w.tbd.size() * sizeof(pg_tb_desc));
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
+  std::memcpy(h + o_order, order.data(), order.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, re_off.data(), re_off.size() * 4);
   cudaStream_t s = ctx->stream;
