@@ -412,6 +412,21 @@ int pg_pusch_plan_execute_device(pg_pusch_plan* plan, const uint32_t* grids, uin
 int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, size_t tb_out_len,
                                pg_sch_result* results, pg_port_result* port_results);
 
+/* ---------------------------------------------------------------------------------------- */
+/* Learned channel estimator: tensor-core building blocks                                    */
+
+/* One 1-D convolution layer (kernel 5, zero 'same' padding) on the tensor cores: BF16 operands,
+ * FP32 accumulation. Activations are [C/8][rows][8] bf16 (8-channel chunks, one 16-byte row per
+ * position); samples are concatenated with at least two zero rows between them, and only rows
+ * with row_valid[r] != 0 are written. w: packed weights [5 taps][cin/8][cout][8] bf16
+ * (w[t][ci/8][co][ci%8] = W[co][ci][t]); bias: cout floats; res: optional residual added before
+ * the activation (same layout as y, may be NULL); relu != 0 applies max(0, .). (cin, cout) is
+ * (16, 64), (64, 64) or (64, 16). err: device int set to 1 if a tensor-core completion wait
+ * expired. No counterpart in the reference (the learned estimator is an addition). */
+int pg_conv1d_forward_device(pg_context* ctx, int cin, int cout, const void* x, const void* w, const float* bias,
+                             const void* res, void* y, const uint8_t* row_valid, int rows, int relu, int* err,
+                             void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -290,6 +290,7 @@ int pg_create(const pg_config* cfg, pg_context** out)
   }
   if (rc == PG_OK) {
     ctx->ldpc_ctas = ldpc_resident_ctas(ctx);
+    rc             = conv_setup(ctx);
   }
   if (rc == PG_OK) {
     // x^e mod g(x) for CRC16, CRC24A and CRC24B.

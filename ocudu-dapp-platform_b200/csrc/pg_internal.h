@@ -180,4 +180,10 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
 // CTAs of ldpc_decode_kernel resident on the whole device.
 int ldpc_resident_ctas(pg_context* ctx);
 
+// Tensor-core 1-D convolutions (tc_conv1d.cu): kernel attributes, and the forward launch over an
+// activation buffer of R rows ([C/8][R][8] bf16).
+int conv_setup(pg_context* ctx);
+int conv_forward_launch(pg_context* ctx, int cin, int cout, const void* x, const void* w, const float* bias,
+                        const void* res, void* y, const uint8_t* row_valid, int R, int relu, int* err, cudaStream_t s);
+
 } // namespace pg

@@ -121,6 +121,8 @@ SIGNATURES = {
     "pg_pusch_plan_set_graph": (ctypes.c_int, [_VP, ctypes.c_int]),
     "pg_pusch_plan_execute_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_execute_host": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_size_t, _VP, _VP]),
+    "pg_conv1d_forward_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP,
+                                                ctypes.c_int, ctypes.c_int, _VP, _VP]),
 }
 
 _lib = None
