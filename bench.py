@@ -45,6 +45,8 @@ PUSCH_WORKLOAD = ("Batched uneven slot: 16 cells x 273 PRB (100 MHz, 30 kHz SCS)
                   "per-UE SNR U[0,30] dB, DM-RS type 1 symbols {2,11}, exponential PDP (100 ns RMS, 8 taps), "
                   "max 6 LDPC iterations, CRC early stop")
 KERNELS_PER_PLAN = 6  # estimate, demodulate, rate dematch, LDPC, TB assembly, results
+LE_KERNELS = 16       # learned estimator: features, 14 convolution layers, apply
+LE_FLOPS_PER_ROW = 2 * 5 * (16 * 64 + 12 * 64 * 64 + 64 * 16)  # 14 layers, kernel 5, per subcarrier row
 WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) and BG2 Z=384 (K=3840, rate 1/5) "
             "mixed 50/50 by seed, CRC24B, BPSK/AWGN Eb/N0 U[1,3] dB, int8 LLRs (scale 4/LLR unit, sat +-127), "
             "max 10 iterations, CRC early stop")
@@ -64,6 +66,7 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-ldpc", action="store_true")
+    p.add_argument("--no-learned", action="store_true", help="plain estimator only")
     return p.parse_args()
 
 
@@ -181,6 +184,16 @@ def pusch_edge_updates(ues, results):
     return int(total)
 
 
+def bf16_peak():
+    """Dense bf16 tensor peak (TFLOP/s) measured on this pool (MEASURED_PEAKS.json, burst figure),
+    else the pool's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback (1.59 PFLOP/s earlier measurement on this pool)"
+
+
 def int_peak(dev):
     """Measured full-rate int32 instruction throughput (ops/s) of this GPU and the per-class
     figures (libpg_probe.so), or (None, None)."""
@@ -263,6 +276,8 @@ def run_ours_pusch(args):
     from pusch_b200._native import PgSchResult
     from pusch_b200.pusch import PuschSlotPlan, results_from
 
+    from pusch_b200 import learned as le_mod
+
     slots = pusch_workload(args.seed + rank)
     truth = [t for sl in slots for t in sl.truth]
     ctx = _native.Context(device=dev, max_codeblocks=64)
@@ -275,40 +290,63 @@ def run_ours_pusch(args):
     d_res = torch.zeros(n * ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
+    # The learned estimator (trained parameters committed with the package) refines every UE's
+    # channel estimates inside the plan; without parameters the plan runs the plain estimator.
+    params = None if args.no_learned else le_mod.load_params()
+    le_rows = plan.le_rows()
+    net = le_mod.LearnedEstimator(ctx, max_rows=le_rows, params=params) if params is not None else None
+
     def step():
         plan.execute_device(d_grid.data_ptr(), d_tb.data_ptr(), d_res.data_ptr(), None, sptr)
 
-    ctx.lib.pg_set_kernel_timing(ctx.handle, 1)
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            flush.fill_(1)
-            step()
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    clocks = ClockSampler(dev)
-    clocks.wait_first_sample()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    ldpc_ms = []
-    torch.cuda.synchronize()
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.fill_(k & 0xFF)
-            evs[k][0].record(stream)
-            step()
-            evs[k][1].record(stream)
-            stream.synchronize()
-            ldpc_ms.append(ctx.lib.pg_last_kernel_ms(ctx.handle))
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    ms = statistics.mean(step_ms)
+    def decoded():
+        """Decoded bits: CRC-passing UEs whose TB equals the transmitted bits."""
+        res_arr = (PgSchResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+        res = results_from(plan.descs, res_arr, None, d_tb.cpu().numpy())
+        ok = [r.tb_crc_ok and bool((np.unpackbits(r.transport_block) == t).all()) for r, t in zip(res, truth)]
+        return res, ok, int(sum(u.tbs_bits for u, g in zip(plan.ues, ok) if g))
 
-    # Decoded bits: CRC-passing UEs whose TB equals the transmitted bits.
-    res_arr = (PgSchResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
-    results = results_from(plan.descs, res_arr, None, d_tb.cpu().numpy())
-    good = [r.tb_crc_ok and bool((np.unpackbits(r.transport_block) == t).all()) for r, t in zip(results, truth)]
-    bits_ok = int(sum(u.tbs_bits for u, g in zip(plan.ues, good) if g))
+    def timed(nsteps, sample_clocks=False):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                flush.fill_(1)
+                step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        clocks = ClockSampler(dev) if sample_clocks else None
+        if clocks is not None:
+            clocks.wait_first_sample()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        k_ms, l_ms = [], []
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(nsteps):
+                flush.fill_(k & 0xFF)
+                evs[k][0].record(stream)
+                step()
+                evs[k][1].record(stream)
+                stream.synchronize()
+                k_ms.append(ctx.lib.pg_last_kernel_ms(ctx.handle))
+                l_ms.append(ctx.lib.pg_last_learned_ms(ctx.handle))
+        torch.cuda.synchronize()
+        clk = clocks.stop() if clocks is not None else None
+        return [a.elapsed_time(b) for a, b in evs], k_ms, l_ms, clk
+
+    ctx.lib.pg_set_kernel_timing(ctx.handle, 1)
+    # Batched path with the plain estimator (the comparison point of the learned one).
+    batched_plain = None
+    if net is not None:
+        p_step_ms, _, _, _ = timed(max(10, min(args.steps, 200)))
+        _, p_ok, p_bits = decoded()
+        p_ms = statistics.mean(p_step_ms)
+        batched_plain = {"value": round(p_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 4),
+                         "bler": round(1.0 - sum(p_ok) / n, 4),
+                         "what": "the same slot plan with the plain estimator (LS + RC FIR + linear interpolation)"}
+        plan.set_learned(net)
+    step_ms, ldpc_ms, learned_ms, clk = timed(args.steps, sample_clocks=True)
+    ms = statistics.mean(step_ms)
+    results, good, bits_ok = decoded()
     bits_all = int(sum(u.tbs_bits for u in plan.ues))
     bler = 1.0 - sum(good) / n
 
@@ -354,7 +392,9 @@ def run_ours_pusch(args):
                 torch.cuda.synchronize()
                 pms.append(a.elapsed_time(b))
         p_ms = statistics.mean(pms)
-        plain = {"value": round(bits_ok / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 3),
+        # The per-UE plans decode what the batched plan with the plain estimator decodes.
+        plain_bits = bits_ok if batched_plain is None else p_bits
+        plain = {"value": round(plain_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 3),
                  "plans": len(per_ue), "kernels_per_step": KERNELS_PER_PLAN * len(per_ue),
                  "what": "one plan per UE executed in turn, host waits for each UE's result (no batching, no graph)"}
         for p in per_ue:
@@ -393,7 +433,9 @@ def run_ours_pusch(args):
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
                "ms_per_step": round(e_ms, 3), "entry": "pg_pusch_plan_execute_host"}
 
-    # Integer roofline of the dominant kernel (ldpc_decode_kernel inside the step).
+    # Rooflines: the integer pipe of ldpc_decode_kernel and the tensor cores of the learned
+    # estimator's convolutions, both timed with CUDA events inside the step; "roofline" is the one
+    # that takes the larger share of the step.
     edge_updates = pusch_edge_updates(plan.ues, results)
     ops = edge_updates * INT_OPS_PER_EDGE
     valid_ms = [x for x in ldpc_ms if x > 0]
@@ -413,6 +455,21 @@ def run_ours_pusch(args):
         "kernel_ms": round(k_ms, 4), "kernel_share_of_step": round(k_ms / ms, 3),
         "traffic": None,
     }
+
+    rooflines = {"ldpc": roofline}
+    le_ms = statistics.mean([x for x in learned_ms if x > 0]) if net is not None else float("nan")
+    if net is not None:
+        flops = le_rows * LE_FLOPS_PER_ROW
+        peak_tf, peak_src = bf16_peak()
+        ach = flops / (le_ms * 1e-3) / 1e12
+        rooflines["learned"] = {
+            "bound": "tensor", "kernel": "conv1d_fwd_kernel (14 launches) + le_features/le_apply",
+            "achieved": round(ach, 2), "peak": peak_tf, "unit": "TFLOP/s", "frac": round(ach / peak_tf, 4),
+            "peak_source": peak_src, "flops_per_launch_chain": flops, "rows": le_rows,
+            "flops_per_row": LE_FLOPS_PER_ROW, "stage_ms": round(le_ms, 4), "stage_share_of_step": round(le_ms / ms, 3),
+            "traffic": None}
+        if le_ms > k_ms:
+            roofline = rooflines["learned"]
 
     ldpc_line = None
     if not args.no_ldpc:
@@ -435,14 +492,20 @@ def run_ours_pusch(args):
                        "codeblocks_per_rank": int(plan.info.nof_codeblocks), "tb_bits_per_rank": bits_all,
                        "decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
                        "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
-                       "parallelism": f"replicas{world}", "estimator": "plain (LS + RC FIR + linear interpolation)"},
-            "plain_per_ue": plain, "learned": None,
-            "e2e": e2e, "roofline": roofline, "ldpc": ldpc_line, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": KERNELS_PER_PLAN * args.steps,
+                       "parallelism": f"replicas{world}",
+                       "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
+                                     "plain LS + RC FIR + linear interpolation" if net is not None else
+                                     "plain (LS + RC FIR + linear interpolation)")},
+            "plain_per_ue": plain, "batched_plain": batched_plain,
+            "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": (KERNELS_PER_PLAN + (LE_KERNELS if net is not None else 0)) * args.steps,
             "step_ms": {"min": round(min(step_ms), 4), "max": round(max(step_ms), 4)},
         }
         print(json.dumps(line), flush=True)
     plan.close()
+    if net is not None:
+        net.close()
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

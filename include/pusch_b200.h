@@ -417,8 +417,8 @@ int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8
 
 /* One 1-D convolution layer (kernel 5, zero 'same' padding) on the tensor cores: BF16 operands,
  * FP32 accumulation. Activations are [C/8][rows][8] bf16 (8-channel chunks, one 16-byte row per
- * position); samples are concatenated with at least two zero rows between them, and only rows
- * with row_valid[r] != 0 are written. w: packed weights [5 taps][cin/8][cout][8] bf16
+ * position); samples are concatenated with at least two zero rows between them; rows with
+ * row_valid[r] != 0 receive the layer output, the other rows are written as zeros. w: packed weights [5 taps][cin/8][cout][8] bf16
  * (w[t][ci/8][co][ci%8] = W[co][ci][t]); bias: cout floats; res: optional residual added before
  * the activation (same layout as y, may be NULL); relu != 0 applies max(0, .). (cin, cout) is
  * (16, 64), (64, 64) or (64, 16). err: device int set to 1 if a tensor-core completion wait
@@ -426,6 +426,98 @@ int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8
 int pg_conv1d_forward_device(pg_context* ctx, int cin, int cout, const void* x, const void* w, const float* bias,
                              const void* res, void* y, const uint8_t* row_valid, int rows, int relu, int* err,
                              void* stream);
+
+/* Input gradient of a (cin -> cout) layer: dx = conv(dy, W') with the packed transposed weights
+ * w_t [5][cout/8][cin][8] (W'[ci][co][t] = W[co][ci][4 - t]), plus res (may be NULL), then zeroed
+ * where the forward ReLU output `mask` ([cin/8][rows][8], may be NULL) is not positive. dy is
+ * [cout/8][rows][8], dx [cin/8][rows][8]; rows that are not valid are written as zeros. No counterpart in the
+ * reference. */
+int pg_conv1d_backward_data_device(pg_context* ctx, int cin, int cout, const void* dy, const void* w_t,
+                                   const void* res, const void* mask, void* dx, const uint8_t* row_valid, int rows,
+                                   int* err, void* stream);
+
+/* Weight and bias gradients of a (cin -> cout) layer, ADDED to dw (FP32 [5][cin][cout]:
+ * dw[t][ci][co] += sum_r x[r + t - 2][ci] dy[r][co]) and db (FP32 [cout], may be NULL). x and dy in
+ * the activation layout; rows outside samples must be zero in both. No counterpart in the
+ * reference. */
+int pg_conv1d_backward_weights_device(pg_context* ctx, int cin, int cout, const void* x, const void* dy, int rows,
+                                      float* dw, float* db, int* err, void* stream);
+
+/* Device time in milliseconds of the learned-estimator stage (features, network, corrected
+ * estimates) of the most recent slot-plan execution of a timed context (pg_set_kernel_timing),
+ * or a negative value when none was recorded. No counterpart in the reference. */
+float pg_last_learned_ms(pg_context* ctx);
+
+/* ---------------------------------------------------------------------------------------- */
+/* Learned channel estimator                                                                 */
+
+/* No counterpart in the reference: an addition of this library. A residual 1-D convolutional
+ * network (input layer 16 -> 64 channels, 6 residual blocks of two 64 -> 64 layers, output layer
+ * 64 -> 16; kernel 5; BF16 weights and activations, FP32 accumulation on the tensor cores) that
+ * refines, per (UE, receive port, layer) allocation, the frequency responses of
+ * pg_pusch_estimate_device at the DM-RS symbols from the plain estimate, the LS estimates and the
+ * noise level. The plain estimator stays the per-allocation fallback (allocations can be left out;
+ * non-finite corrections are dropped). Parameters: per layer, weights [5][cin][cout] then bias
+ * [cout], FP32, layers in network order. A net is used by one thread and one plan at a time. */
+typedef struct pg_le_net pg_le_net;
+
+/* Optimiser of pg_le_train_step_device (Adam; weight decay on the weights only). */
+typedef struct pg_le_adam {
+  float lr;
+  float beta1;
+  float beta2;
+  float eps;
+  float weight_decay;
+} pg_le_adam;
+
+/* FP32 parameters of the network (256,848). */
+size_t pg_le_nof_params(void);
+/* Rows of the network's layout for a list of UEs (12 nof_rb per port and layer, plus gaps). */
+size_t pg_le_rows(const pg_pusch_ue* ues, int nof_ues);
+/* Creates a network with buffers for max_rows rows (about 2.1 KB of device memory per row). The
+ * parameters start at zero: set them with pg_le_set_params. */
+int  pg_le_create(pg_context* ctx, int max_rows, pg_le_net** out);
+void pg_le_destroy(pg_le_net* net);
+/* Host FP32 parameters in and out (count = pg_le_nof_params()); setting them resets Adam. */
+int pg_le_set_params(pg_le_net* net, const float* params, size_t count);
+int pg_le_get_params(pg_le_net* net, float* params, size_t count);
+/* Gradients accumulated by the last pg_le_backward_device (same layout as the parameters). */
+int pg_le_get_grads(pg_le_net* net, float* grads, size_t count);
+/* Waits for the device and returns PG_ERR_TIMEOUT if a tensor-core completion wait of any of the
+ * net's kernels expired since it was created. */
+int pg_le_status(pg_le_net* net);
+
+/* The network on given inputs: x [2][rows][8] bf16 features, row_valid per row, y [2][rows][8]
+ * bf16 outputs (device pointers). The activations stay in the net for pg_le_backward_device. */
+int pg_le_forward_device(pg_le_net* net, const void* x, const uint8_t* row_valid, int rows, void* y, void* stream);
+/* Gradients of every parameter for the output gradient dy [2][rows][8] bf16 of the last forward
+ * call (replaces the previous gradients). */
+int pg_le_backward_device(pg_le_net* net, const void* dy, int rows, void* stream);
+
+/* Refines est (as written by pg_pusch_estimate_ls_device, with its LS output ls and port results)
+ * in place for the UEs with use[u] != 0 (use may be NULL: every UE). ues: host array with the
+ * est_offset of each UE. */
+int pg_le_refine_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, float* est,
+                        const pg_port_result* port_results, const uint8_t* use, void* stream);
+/* One training step on a batch of UEs: features -> forward -> mean squared error of the
+ * correction against the true responses h_true (same layout as est) -> backward -> Adam.
+ * loss (device, 2 floats, may be NULL): the network's MSE and the plain estimator's MSE, both in
+ * units of the allocations' mean channel power. */
+int pg_le_train_step_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, const float* est,
+                            const pg_port_result* port_results, const float* h_true, const pg_le_adam* opt,
+                            float* loss, void* stream);
+
+/* DM-RS estimation as pg_pusch_estimate_device that also writes the LS estimates (same layout as
+ * est: the pilots' even subcarriers, zero on the odd ones) for the learned estimator; ls may be
+ * NULL. */
+int pg_pusch_estimate_ls_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids,
+                                float* est, float* ls, pg_port_result* results, void* stream);
+
+/* Uses net (NULL: none) to refine the plan's channel estimates between estimation and
+ * demodulation, for the UEs with use[u] != 0 (use: host array of nof_ues, or NULL for all).
+ * The net must hold pg_le_rows of those UEs; a captured graph is re-captured on the next
+ * execution. */
+int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t* use);
 
 #ifdef __cplusplus
 }

@@ -546,6 +546,18 @@ int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, con
                                 stream);
 }
 
+unsigned int timing_record_flags(pg_context* ctx, cudaStream_t s)
+{
+  // Under stream capture the timing events become event-record nodes of the graph (external
+  // records); a plain record there would only mark a capture dependency.
+  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+  if (ctx->timed && cudaStreamIsCapturing(s, &capturing) == cudaSuccess &&
+      capturing == cudaStreamCaptureStatusActive) {
+    return cudaEventRecordExternal;
+  }
+  return cudaEventRecordDefault;
+}
+
 int ldpc_resident_ctas(pg_context* ctx)
 {
   int per_sm = 0;
@@ -567,14 +579,7 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (int rc = check_cuda(ctx, cudaMemsetAsync(counter, 0, sizeof(int), stream), "cudaMemsetAsync(ldpc counter)")) {
     return rc;
   }
-  // Under stream capture the timing events become event-record nodes of the graph (external
-  // records); a plain record there would only mark a capture dependency.
-  unsigned int            rec_flags = cudaEventRecordDefault;
-  cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
-  if (ctx->timed && cudaStreamIsCapturing(stream, &capturing) == cudaSuccess &&
-      capturing == cudaStreamCaptureStatusActive) {
-    rec_flags = cudaEventRecordExternal;
-  }
+  const unsigned int rec_flags = timing_record_flags(ctx, stream);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }

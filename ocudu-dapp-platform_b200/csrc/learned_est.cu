@@ -1,0 +1,794 @@
+// Learned DM-RS channel estimator: a residual 1-D convolutional network over the subcarriers of
+// each (UE, receive port, layer) allocation that refines the frequency responses of the plain
+// estimator (LS + RC smoothing + linear interpolation, pusch_est.cu) at the DM-RS symbols. The
+// plain estimate stays the per-allocation fallback: the network only adds a correction, allocations
+// can be left out, and a correction that is not finite is dropped. No counterpart in the
+// reference (its estimator is port_channel_estimator_average_impl; the learned part is an
+// addition of this library).
+//
+// Network (14 layers, kernel 5, 'same' padding, BF16 activations, FP32 accumulation on the tensor
+// cores, tc_conv1d.cu):
+//   x (16 features) -> conv 16->64, ReLU -> 6 x [conv 64->64, ReLU -> conv 64->64, + block input,
+//   ReLU] -> conv 64->16 (linear); output channels 0..3 = correction of the DM-RS symbol 0 and 1
+//   responses (re, im), in units of the allocation's RMS channel amplitude.
+// Features per subcarrier k of an allocation of L = 12 nof_rb subcarriers, normalised by
+// g = beta / sqrt(RSRP_layer) (the inverse RMS amplitude of the plain estimate):
+//   0-3  plain estimate at DM-RS symbols 0 and 1 (re, im; symbol 1 repeats symbol 0 with one DM-RS symbol)
+//   4-7  LS estimate at the pilots (even k; zero on odd k), DM-RS symbols 0 and 1
+//   8    log10(noise_var g^2 / beta^2) / 2, clamped to [-4, 4] (the LS noise level)
+//   9    1 on pilot subcarriers
+//   10   max(0, 1 - k / 8), 11 max(0, 1 - (L - 1 - k) / 8)   (allocation edges)
+//   12   1 with two layers (pair-averaged LS), 13 1 with two DM-RS symbols, 14-15 zero
+// Row layout: the allocations one after another, two zero rows before each.
+//
+// Training (all on the GPU with this file's kernels and tc_conv1d.cu): features -> forward ->
+// MSE of the correction against g (H_true - plain) -> backward (input gradients through the
+// transposed convolutions with the ReLU masks, weight gradients on the tensor cores) -> Adam.
+#include "pg_internal.h"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+constexpr int kLayers = 14;
+constexpr int kBlocks = 6;
+constexpr int kCh     = 64;
+constexpr int kInCh   = 16;
+constexpr int kOutCh  = 16;
+constexpr int kTaps   = 5;
+constexpr int kGap    = 2; // zero rows before each allocation
+
+struct layer_desc {
+  int cin, cout;
+  int w_off; // floats: weights [5][cin][cout] at w_off, bias [cout] at w_off + 5 cin cout
+  int p_off; // bf16 elements of this layer's packed weights
+};
+
+struct layer_table {
+  layer_desc l[kLayers];
+  int        nparams = 0, npacked = 0;
+  layer_table()
+  {
+    int off = 0, poff = 0;
+    for (int i = 0; i < kLayers; ++i) {
+      const int cin  = i == 0 ? kInCh : kCh;
+      const int cout = i == kLayers - 1 ? kOutCh : kCh;
+      l[i]           = {cin, cout, off, poff};
+      off += kTaps * cin * cout + cout;
+      poff += kTaps * cin * cout;
+    }
+    nparams = off;
+    npacked = poff;
+  }
+};
+
+const layer_table& layers()
+{
+  static const layer_table t;
+  return t;
+}
+
+__constant__ layer_desc c_layers[kLayers];
+
+} // namespace
+
+using pg::le_seq;
+
+struct pg_le_net {
+  pg_context* ctx      = nullptr;
+  int         max_rows = 0;
+  int         step     = 0;
+  void*       dev      = nullptr;
+  float*      params   = nullptr;
+  float*      grads    = nullptr;
+  float*      adam_m   = nullptr;
+  float*      adam_v   = nullptr;
+  uint16_t*   wf       = nullptr; // packed forward weights
+  uint16_t*   wt       = nullptr; // packed transposed weights (input gradients)
+  uint16_t*   x        = nullptr; // [2][R][8]
+  uint16_t*   act[8]   = {};      // act[1..7]: [8][R][8] (act[0] = x)
+  uint16_t*   mid[kBlocks] = {};  // [8][R][8]
+  uint16_t*   y        = nullptr; // [2][R][8]
+  uint16_t*   dy       = nullptr; // [2][R][8]
+  uint16_t*   g0 = nullptr, *g1 = nullptr, *h = nullptr; // [8][R][8] gradients
+  uint8_t*    row_valid = nullptr;
+  pg::le_seq* seqs      = nullptr;
+  float*      gseq      = nullptr;
+  int*        err       = nullptr;
+  float*      loss      = nullptr; // [2]
+  int         max_seqs  = 0;
+};
+
+namespace {
+
+__device__ __forceinline__ int find_seq(const le_seq* __restrict__ seqs, int nseq, uint32_t r)
+{
+  int lo = 0, hi = nseq - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seqs[mid].row0 <= r) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+  const __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ float seq_gain(const le_seq& q, const pg_port_result* __restrict__ pr)
+{
+  const float rsrp = pr[q.pr].rsrp[q.layer];
+  return (rsrp > 0.f && isfinite(rsrp)) ? q.beta * rsqrtf(rsrp) : 0.f;
+}
+
+__global__ void le_features_kernel(const le_seq* __restrict__ seqs, int nseq, int R, const float2* __restrict__ est,
+                                   const float2* __restrict__ ls, const pg_port_result* __restrict__ pr,
+                                   uint4* __restrict__ x, uint8_t* __restrict__ row_valid, float* __restrict__ gseq)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) {
+    return;
+  }
+  const int    s = find_seq(seqs, nseq, (uint32_t)r);
+  const le_seq q = seqs[s];
+  const int    k = r - (int)q.row0;
+  uint4        c0 = make_uint4(0, 0, 0, 0), c1 = make_uint4(0, 0, 0, 0);
+  const bool   valid = k >= 0 && k < (int)q.len;
+  if (valid) {
+    const float  g   = seq_gain(q, pr);
+    const size_t o0  = q.est0 + (size_t)k;
+    const size_t o1  = o0 + (q.nd > 1 ? q.dstride : 0u);
+    const float2 p0 = est[o0], p1 = est[o1], l0 = ls[o0], l1 = ls[o1];
+    const float  nv  = pr[q.pr].noise_var;
+    float        nf  = 0.f;
+    if (g > 0.f) {
+      nf = log10f(fmaxf(nv * g * g / (q.beta * q.beta), 1e-12f)) * 0.5f;
+      nf = fminf(4.f, fmaxf(-4.f, isfinite(nf) ? nf : 0.f));
+    }
+    const float L = (float)q.len;
+    c0            = make_uint4(pack_bf16x2(g * p0.x, g * p0.y), pack_bf16x2(g * p1.x, g * p1.y),
+                               pack_bf16x2(g * l0.x, g * l0.y), pack_bf16x2(g * l1.x, g * l1.y));
+    c1 = make_uint4(pack_bf16x2(g > 0.f ? nf : 0.f, (k & 1) ? 0.f : 1.f),
+                    pack_bf16x2(fmaxf(0.f, 1.f - (float)k / 8.f), fmaxf(0.f, 1.f - (L - 1.f - (float)k) / 8.f)),
+                    pack_bf16x2(q.nof_layers > 1 ? 1.f : 0.f, q.nd > 1 ? 1.f : 0.f), 0u);
+    if (g <= 0.f) {
+      c0 = make_uint4(0, 0, 0, 0);
+      c1 = make_uint4(0, 0, 0, 0);
+    }
+    if (k == 0) {
+      gseq[s] = g;
+    }
+  }
+  x[r]                = c0;
+  x[(size_t)R + r]    = c1;
+  row_valid[r]        = valid ? 1 : 0;
+}
+
+__device__ __forceinline__ void unpack4(const uint4 v, float* o)
+{
+  const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    o[j] = __bfloat162float(b[j]);
+  }
+}
+
+// est += correction / g on the DM-RS symbols of every valid row (finite corrections only).
+__global__ void le_apply_kernel(const le_seq* __restrict__ seqs, int nseq, int R, const uint4* __restrict__ y,
+                                const float* __restrict__ gseq, float2* __restrict__ est)
+{
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= R) {
+    return;
+  }
+  const int    s = find_seq(seqs, nseq, (uint32_t)r);
+  const le_seq q = seqs[s];
+  const int    k = r - (int)q.row0;
+  const float  g = gseq[s];
+  if (k < 0 || k >= (int)q.len || !(g > 0.f)) {
+    return;
+  }
+  float o[4];
+  unpack4(y[r], o);
+  const float inv = 1.f / g;
+  for (int d = 0; d < q.nd; ++d) {
+    const float dx = o[2 * d] * inv, dyv = o[2 * d + 1] * inv;
+    if (isfinite(dx) && isfinite(dyv)) {
+      float2& e = est[q.est0 + (size_t)d * q.dstride + k];
+      e.x += dx;
+      e.y += dyv;
+    }
+  }
+}
+
+// MSE of the correction against g (H - plain): dy = 2 (y - t) inv_n on the used channels, zero
+// elsewhere; loss[0] += sum (y - t)^2 inv_n, loss[1] += sum t^2 inv_n (the plain estimator's error).
+__global__ void le_loss_kernel(const le_seq* __restrict__ seqs, int nseq, int R, const uint4* __restrict__ y,
+                               const float* __restrict__ gseq, const float2* __restrict__ est,
+                               const float2* __restrict__ h_true, float inv_n, uint4* __restrict__ dy,
+                               float* __restrict__ loss)
+{
+  const int r   = blockIdx.x * blockDim.x + threadIdx.x;
+  float     l0  = 0.f, l1 = 0.f;
+  if (r < R) {
+    const int    s = find_seq(seqs, nseq, (uint32_t)r);
+    const le_seq q = seqs[s];
+    const int    k = r - (int)q.row0;
+    const float  g = gseq[s];
+    float        d4[4] = {0.f, 0.f, 0.f, 0.f};
+    if (k >= 0 && k < (int)q.len && g > 0.f) {
+      float o[4];
+      unpack4(y[r], o);
+      for (int d = 0; d < q.nd; ++d) {
+        const size_t i  = q.est0 + (size_t)d * q.dstride + k;
+        const float2 p  = est[i], h = h_true[i];
+        const float  tx = g * (h.x - p.x), ty = g * (h.y - p.y);
+        const float  ex = o[2 * d] - tx, ey = o[2 * d + 1] - ty;
+        d4[2 * d]       = 2.f * ex * inv_n;
+        d4[2 * d + 1]   = 2.f * ey * inv_n;
+        l0 += (ex * ex + ey * ey) * inv_n;
+        l1 += (tx * tx + ty * ty) * inv_n;
+      }
+    }
+    dy[r]             = make_uint4(pack_bf16x2(d4[0], d4[1]), pack_bf16x2(d4[2], d4[3]), 0u, 0u);
+    dy[(size_t)R + r] = make_uint4(0, 0, 0, 0);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    l0 += __shfl_xor_sync(0xffffffffu, l0, o);
+    l1 += __shfl_xor_sync(0xffffffffu, l1, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (l0 != 0.f || l1 != 0.f)) {
+    atomicAdd(&loss[0], l0);
+    atomicAdd(&loss[1], l1);
+  }
+}
+
+__device__ __forceinline__ uint16_t bf16_bits(float f)
+{
+  const __nv_bfloat16 b = __float2bfloat16_rn(f);
+  return *reinterpret_cast<const uint16_t*>(&b);
+}
+
+// Adam step (when update != 0) on every parameter, then the packed BF16 copies of the weights for
+// the forward and the input-gradient convolutions; the gradients are cleared for the next step.
+__global__ void le_adam_kernel(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m,
+                               float* __restrict__ v, uint16_t* __restrict__ wf, uint16_t* __restrict__ wt, int total,
+                               int update, float lr, float b1, float b2, float eps, float wd, float bc1, float bc2)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) {
+    return;
+  }
+  int li = 0;
+#pragma unroll 1
+  while (li + 1 < kLayers && c_layers[li + 1].w_off <= i) {
+    ++li;
+  }
+  const layer_desc L  = c_layers[li];
+  const int        j  = i - L.w_off;
+  const int        nw = kTaps * L.cin * L.cout;
+  float            w  = p[i];
+  if (update) {
+    const float gr = grad[i];
+    const float mm = b1 * m[i] + (1.f - b1) * gr;
+    const float vv = b2 * v[i] + (1.f - b2) * gr * gr;
+    m[i]           = mm;
+    v[i]           = vv;
+    const float upd = (mm / bc1) / (sqrtf(vv / bc2) + eps) + (j < nw ? wd * w : 0.f);
+    w -= lr * upd;
+    p[i]    = w;
+    grad[i] = 0.f;
+  }
+  if (j < nw) {
+    const int t  = j / (L.cin * L.cout);
+    const int r  = j - t * L.cin * L.cout;
+    const int ci = r / L.cout;
+    const int co = r - ci * L.cout;
+    const uint16_t b = bf16_bits(w);
+    wf[L.p_off + ((t * (L.cin / 8) + ci / 8) * L.cout + co) * 8 + (ci & 7)]              = b;
+    wt[L.p_off + (((kTaps - 1 - t) * (L.cout / 8) + co / 8) * L.cin + ci) * 8 + (co & 7)] = b;
+  }
+}
+
+size_t al(size_t x)
+{
+  return (x + 255) & ~(size_t)255;
+}
+
+int check_err_status(pg_le_net* net)
+{
+  int e = 0;
+  if (int rc = pg::check_cuda(net->ctx, cudaMemcpy(&e, net->err, sizeof(int), cudaMemcpyDeviceToHost),
+                              "D2H learned-estimator status")) {
+    return rc;
+  }
+  return e != 0 ? pg::set_error(net->ctx, PG_ERR_TIMEOUT, "a tensor-core completion wait expired") : PG_OK;
+}
+
+int forward(pg_le_net* net, int R, cudaStream_t s)
+{
+  pg_context*        ctx = net->ctx;
+  const layer_table& T   = layers();
+  auto w  = [&](int i) { return (const void*)(net->wf + T.l[i].p_off); };
+  auto b  = [&](int i) { return (const float*)(net->params + T.l[i].w_off + kTaps * T.l[i].cin * T.l[i].cout); };
+  int  rc = pg::conv_forward_launch(ctx, kInCh, kCh, net->x, w(0), b(0), nullptr, nullptr, net->act[1],
+                                    net->row_valid, R, 1, net->err, s);
+  for (int k = 0; k < kBlocks && rc == PG_OK; ++k) {
+    rc = pg::conv_forward_launch(ctx, kCh, kCh, net->act[k + 1], w(1 + 2 * k), b(1 + 2 * k), nullptr, nullptr,
+                                 net->mid[k], net->row_valid, R, 1, net->err, s);
+    if (rc == PG_OK) {
+      rc = pg::conv_forward_launch(ctx, kCh, kCh, net->mid[k], w(2 + 2 * k), b(2 + 2 * k), net->act[k + 1], nullptr,
+                                   net->act[k + 2], net->row_valid, R, 1, net->err, s);
+    }
+  }
+  if (rc == PG_OK) {
+    rc = pg::conv_forward_launch(ctx, kCh, kOutCh, net->act[kBlocks + 1], w(kLayers - 1), b(kLayers - 1), nullptr,
+                                 nullptr, net->y, net->row_valid, R, 0, net->err, s);
+  }
+  return rc;
+}
+
+// Gradients of every parameter (added to net->grads) from net->dy and the activations of the last
+// forward pass.
+int backward(pg_le_net* net, int R, cudaStream_t s)
+{
+  pg_context*        ctx = net->ctx;
+  const layer_table& T   = layers();
+  auto wt = [&](int i) { return (const void*)(net->wt + T.l[i].p_off); };
+  auto gw = [&](int i) { return net->grads + T.l[i].w_off; };
+  auto gb = [&](int i) { return net->grads + T.l[i].w_off + kTaps * T.l[i].cin * T.l[i].cout; };
+  const int last = kLayers - 1;
+  uint16_t* top  = net->act[kBlocks + 1];
+  int rc = pg::conv_wgrad_launch(ctx, kCh, kOutCh, top, net->dy, R, gw(last), gb(last), net->err, s);
+  if (rc == PG_OK) {
+    rc = pg::conv_forward_launch(ctx, kOutCh, kCh, net->dy, wt(last), nullptr, nullptr, top, net->g0, net->row_valid,
+                                 R, 0, net->err, s);
+  }
+  uint16_t* G = net->g0;
+  uint16_t* Gn = net->g1;
+  for (int k = kBlocks - 1; k >= 0 && rc == PG_OK; --k) {
+    const int l2 = 2 + 2 * k, l1 = 1 + 2 * k;
+    rc = pg::conv_wgrad_launch(ctx, kCh, kCh, net->mid[k], G, R, gw(l2), gb(l2), net->err, s);
+    if (rc == PG_OK) {
+      rc = pg::conv_forward_launch(ctx, kCh, kCh, G, wt(l2), nullptr, nullptr, net->mid[k], net->h, net->row_valid, R,
+                                   0, net->err, s);
+    }
+    if (rc == PG_OK) {
+      rc = pg::conv_wgrad_launch(ctx, kCh, kCh, net->act[k + 1], net->h, R, gw(l1), gb(l1), net->err, s);
+    }
+    if (rc == PG_OK) {
+      rc = pg::conv_forward_launch(ctx, kCh, kCh, net->h, wt(l1), nullptr, G, net->act[k + 1], Gn, net->row_valid, R,
+                                   0, net->err, s);
+    }
+    std::swap(G, Gn);
+  }
+  if (rc == PG_OK) {
+    rc = pg::conv_wgrad_launch(ctx, kInCh, kCh, net->x, G, R, gw(0), gb(0), net->err, s);
+  }
+  return rc;
+}
+
+int pack_launch(pg_le_net* net, int update, const pg_le_adam* opt, cudaStream_t s)
+{
+  const int total = layers().nparams;
+  float     lr = 0.f, b1 = 0.9f, b2 = 0.999f, eps = 1e-8f, wd = 0.f, bc1 = 1.f, bc2 = 1.f;
+  if (update) {
+    ++net->step;
+    lr  = opt->lr;
+    b1  = opt->beta1;
+    b2  = opt->beta2;
+    eps = opt->eps;
+    wd  = opt->weight_decay;
+    bc1 = 1.f - std::pow(b1, (float)net->step);
+    bc2 = 1.f - std::pow(b2, (float)net->step);
+  }
+  le_adam_kernel<<<(total + 255) / 256, 256, 0, s>>>(net->params, net->grads, net->adam_m, net->adam_v, net->wf,
+                                                     net->wt, total, update, lr, b1, b2, eps, wd, bc1, bc2);
+  return pg::check_cuda(net->ctx, cudaGetLastError(), "le_adam_kernel launch");
+}
+
+} // namespace
+
+namespace pg {
+
+// Sequences of the UEs with use[u] != 0 (all when use is null); returns the rows they need.
+size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vector<le_seq>& out, size_t* terms)
+{
+  out.clear();
+  size_t row = 0, nterms = 0;
+  for (int u = 0; u < n; ++u) {
+    if (use != nullptr && use[u] == 0) {
+      continue;
+    }
+    const pg_pusch_ue& ue = ues[u];
+    int                d0 = 0, d1 = 0;
+    const int          nd = dmrs_count(ue, &d0, &d1);
+    const uint32_t     nsc = 12u * ue.nof_rb;
+    for (int p = 0; p < ue.nof_rx_ports; ++p) {
+      for (int l = 0; l < ue.nof_layers; ++l) {
+        le_seq q{};
+        row += kGap;
+        q.row0       = (uint32_t)row;
+        q.len        = nsc;
+        q.est0       = ue.est_offset + (uint32_t)(((p * nd) * ue.nof_layers + l) * nsc);
+        q.dstride    = (uint32_t)ue.nof_layers * nsc;
+        q.pr         = (uint32_t)(u * 4 + p);
+        q.beta       = ue.dmrs_scaling;
+        q.layer      = (uint8_t)l;
+        q.nof_layers = ue.nof_layers;
+        q.nd         = (uint8_t)std::min(nd, 2);
+        out.push_back(q);
+        row += nsc;
+        nterms += (size_t)nsc * 2 * q.nd;
+      }
+    }
+  }
+  if (terms != nullptr) {
+    *terms = nterms;
+  }
+  return out.empty() ? 0 : row;
+}
+
+int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, const float* ls, float* est,
+                     const pg_port_result* pr, cudaStream_t s)
+{
+  if (nseq == 0 || R == 0) {
+    return PG_OK;
+  }
+  le_features_kernel<<<(R + 255) / 256, 256, 0, s>>>(seqs_dev, nseq, R, reinterpret_cast<const float2*>(est),
+                                                     reinterpret_cast<const float2*>(ls), pr,
+                                                     reinterpret_cast<uint4*>(net->x), net->row_valid, net->gseq);
+  int rc = check_cuda(net->ctx, cudaGetLastError(), "le_features_kernel launch");
+  if (rc == PG_OK) {
+    rc = forward(net, R, s);
+  }
+  if (rc == PG_OK) {
+    le_apply_kernel<<<(R + 255) / 256, 256, 0, s>>>(seqs_dev, nseq, R, reinterpret_cast<const uint4*>(net->y),
+                                                    net->gseq, reinterpret_cast<float2*>(est));
+    rc = check_cuda(net->ctx, cudaGetLastError(), "le_apply_kernel launch");
+  }
+  return rc;
+}
+
+int le_capacity(const pg_le_net* net, size_t rows, int nseq)
+{
+  return rows <= (size_t)net->max_rows && nseq <= net->max_seqs ? PG_OK : PG_ERR_CAPACITY;
+}
+
+pg_context* le_context(const pg_le_net* net)
+{
+  return net->ctx;
+}
+
+} // namespace pg
+
+using namespace pg;
+
+extern "C" {
+
+size_t pg_le_nof_params(void)
+{
+  return (size_t)layers().nparams;
+}
+
+size_t pg_le_rows(const pg_pusch_ue* ues, int nof_ues)
+{
+  if (ues == nullptr || nof_ues <= 0) {
+    return 0;
+  }
+  std::vector<le_seq> s;
+  return le_build_seqs(ues, nof_ues, nullptr, s, nullptr);
+}
+
+int pg_le_create(pg_context* ctx, int max_rows, pg_le_net** out)
+{
+  if (ctx == nullptr || out == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  *out = nullptr;
+  if (max_rows <= 0) {
+    return set_error(ctx, PG_ERR_INVALID, "learned estimator: max_rows must be positive");
+  }
+  pg_le_net* n = new (std::nothrow) pg_le_net();
+  if (n == nullptr) {
+    return set_error(ctx, PG_ERR_CAPACITY, "out of host memory");
+  }
+  n->ctx      = ctx;
+  n->max_rows = max_rows;
+  n->max_seqs = max_rows / (12 + kGap) + 1;
+  const layer_table& T = layers();
+  const size_t R       = (size_t)max_rows;
+  const size_t P       = (size_t)T.nparams;
+  size_t       off     = 0;
+  auto take            = [&](size_t bytes) {
+    const size_t o = off;
+    off += al(bytes);
+    return o;
+  };
+  const size_t o_p = take(P * 4), o_g = take(P * 4), o_m = take(P * 4), o_v = take(P * 4);
+  const size_t o_wf = take((size_t)T.npacked * 2), o_wt = take((size_t)T.npacked * 2);
+  const size_t o_x = take(R * 32), o_y = take(R * 32), o_dy = take(R * 32);
+  size_t o_act[8] = {}, o_mid[kBlocks] = {};
+  for (int i = 1; i <= kBlocks + 1; ++i) {
+    o_act[i] = take(R * 128);
+  }
+  for (int i = 0; i < kBlocks; ++i) {
+    o_mid[i] = take(R * 128);
+  }
+  const size_t o_g0 = take(R * 128), o_g1 = take(R * 128), o_h = take(R * 128);
+  const size_t o_rv = take(R), o_seq = take((size_t)n->max_seqs * sizeof(le_seq)),
+               o_gs = take((size_t)n->max_seqs * 4), o_err = take(4), o_loss = take(8);
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&n->dev, off), "cudaMalloc(learned estimator)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemset(n->dev, 0, off), "cudaMemset(learned estimator)");
+  }
+  if (rc == PG_OK) {
+    layer_desc ld[kLayers];
+    std::copy(T.l, T.l + kLayers, ld);
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_layers, ld, sizeof(ld)), "cudaMemcpyToSymbol(layers)");
+  }
+  if (rc != PG_OK) {
+    cudaFree(n->dev);
+    delete n;
+    return rc;
+  }
+  uint8_t* b   = static_cast<uint8_t*>(n->dev);
+  n->params    = reinterpret_cast<float*>(b + o_p);
+  n->grads     = reinterpret_cast<float*>(b + o_g);
+  n->adam_m    = reinterpret_cast<float*>(b + o_m);
+  n->adam_v    = reinterpret_cast<float*>(b + o_v);
+  n->wf        = reinterpret_cast<uint16_t*>(b + o_wf);
+  n->wt        = reinterpret_cast<uint16_t*>(b + o_wt);
+  n->x         = reinterpret_cast<uint16_t*>(b + o_x);
+  n->y         = reinterpret_cast<uint16_t*>(b + o_y);
+  n->dy        = reinterpret_cast<uint16_t*>(b + o_dy);
+  for (int i = 1; i <= kBlocks + 1; ++i) {
+    n->act[i] = reinterpret_cast<uint16_t*>(b + o_act[i]);
+  }
+  n->act[0] = n->x;
+  for (int i = 0; i < kBlocks; ++i) {
+    n->mid[i] = reinterpret_cast<uint16_t*>(b + o_mid[i]);
+  }
+  n->g0        = reinterpret_cast<uint16_t*>(b + o_g0);
+  n->g1        = reinterpret_cast<uint16_t*>(b + o_g1);
+  n->h         = reinterpret_cast<uint16_t*>(b + o_h);
+  n->row_valid = b + o_rv;
+  n->seqs      = reinterpret_cast<le_seq*>(b + o_seq);
+  n->gseq      = reinterpret_cast<float*>(b + o_gs);
+  n->err       = reinterpret_cast<int*>(b + o_err);
+  n->loss      = reinterpret_cast<float*>(b + o_loss);
+  *out         = n;
+  return PG_OK;
+}
+
+void pg_le_destroy(pg_le_net* net)
+{
+  if (net == nullptr) {
+    return;
+  }
+  cudaDeviceSynchronize();
+  cudaFree(net->dev);
+  delete net;
+}
+
+int pg_le_set_params(pg_le_net* net, const float* params, size_t count)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (params == nullptr || count != (size_t)layers().nparams) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: parameter count mismatch");
+  }
+  cudaStream_t s  = net->ctx->stream;
+  int          rc = check_cuda(net->ctx, cudaMemcpyAsync(net->params, params, count * 4, cudaMemcpyHostToDevice, s),
+                               "H2D learned-estimator parameters");
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemsetAsync(net->adam_m, 0, count * 4, s), "cudaMemsetAsync(adam m)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemsetAsync(net->adam_v, 0, count * 4, s), "cudaMemsetAsync(adam v)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemsetAsync(net->grads, 0, count * 4, s), "cudaMemsetAsync(grads)");
+  }
+  if (rc == PG_OK) {
+    net->step = 0;
+    rc        = pack_launch(net, 0, nullptr, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  }
+  return rc;
+}
+
+static int copy_out(pg_le_net* net, const float* src, float* dst, size_t count)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (dst == nullptr || count != (size_t)layers().nparams) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: parameter count mismatch");
+  }
+  if (int rc = check_cuda(net->ctx, cudaDeviceSynchronize(), "cudaDeviceSynchronize")) {
+    return rc;
+  }
+  if (int rc = check_cuda(net->ctx, cudaMemcpy(dst, src, count * 4, cudaMemcpyDeviceToHost), "D2H parameters")) {
+    return rc;
+  }
+  return check_err_status(net);
+}
+
+int pg_le_get_params(pg_le_net* net, float* params, size_t count)
+{
+  return copy_out(net, net != nullptr ? net->params : nullptr, params, count);
+}
+
+int pg_le_get_grads(pg_le_net* net, float* grads, size_t count)
+{
+  return copy_out(net, net != nullptr ? net->grads : nullptr, grads, count);
+}
+
+int pg_le_status(pg_le_net* net)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (int rc = check_cuda(net->ctx, cudaDeviceSynchronize(), "cudaDeviceSynchronize")) {
+    return rc;
+  }
+  return check_err_status(net);
+}
+
+int pg_le_forward_device(pg_le_net* net, const void* x, const uint8_t* row_valid, int rows, void* y, void* stream)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (x == nullptr || row_valid == nullptr || y == nullptr || rows < 0) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: null buffer or negative row count");
+  }
+  if (rows > net->max_rows) {
+    return set_error(net->ctx, PG_ERR_CAPACITY, "learned estimator: more rows than max_rows");
+  }
+  cudaStream_t s  = static_cast<cudaStream_t>(stream);
+  int          rc = check_cuda(net->ctx, cudaMemcpyAsync(net->x, x, (size_t)rows * 32, cudaMemcpyDeviceToDevice, s),
+                               "D2D features");
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemcpyAsync(net->row_valid, row_valid, rows, cudaMemcpyDeviceToDevice, s),
+                    "D2D row mask");
+  }
+  if (rc == PG_OK) {
+    rc = forward(net, rows, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemcpyAsync(y, net->y, (size_t)rows * 32, cudaMemcpyDeviceToDevice, s), "D2D out");
+  }
+  return rc;
+}
+
+int pg_le_backward_device(pg_le_net* net, const void* dy, int rows, void* stream)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (dy == nullptr || rows < 0 || rows > net->max_rows) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: null gradient or bad row count");
+  }
+  cudaStream_t s  = static_cast<cudaStream_t>(stream);
+  int          rc = check_cuda(net->ctx, cudaMemsetAsync(net->grads, 0, (size_t)layers().nparams * 4, s),
+                               "cudaMemsetAsync(grads)");
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemcpyAsync(net->dy, dy, (size_t)rows * 32, cudaMemcpyDeviceToDevice, s),
+                    "D2D output gradient");
+  }
+  if (rc == PG_OK) {
+    rc = backward(net, rows, s);
+  }
+  return rc;
+}
+
+static int stage_seqs(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const uint8_t* use, int* nseq, int* R,
+                      size_t* terms, cudaStream_t s)
+{
+  if (int rc = validate_ues(net->ctx, ues, nof_ues)) {
+    return rc;
+  }
+  std::vector<le_seq> seqs;
+  const size_t        rows = le_build_seqs(ues, nof_ues, use, seqs, terms);
+  if (le_capacity(net, rows, (int)seqs.size()) != PG_OK) {
+    return set_error(net->ctx, PG_ERR_CAPACITY,
+                     "learned estimator: " + std::to_string(rows) + " rows exceed max_rows " +
+                         std::to_string(net->max_rows));
+  }
+  *nseq = (int)seqs.size();
+  *R    = (int)rows;
+  if (seqs.empty()) {
+    return PG_OK;
+  }
+  // Pageable source: the call returns once the descriptors have been copied out of `seqs`.
+  return check_cuda(net->ctx,
+                    cudaMemcpyAsync(net->seqs, seqs.data(), seqs.size() * sizeof(le_seq), cudaMemcpyHostToDevice, s),
+                    "H2D learned-estimator sequences");
+}
+
+int pg_le_refine_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, float* est,
+                        const pg_port_result* port_results, const uint8_t* use, void* stream)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (ls == nullptr || est == nullptr || port_results == nullptr) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: null device buffer");
+  }
+  cudaStream_t s    = static_cast<cudaStream_t>(stream);
+  int          nseq = 0, R = 0;
+  if (int rc = stage_seqs(net, ues, nof_ues, use, &nseq, &R, nullptr, s)) {
+    return rc;
+  }
+  return le_refine_launch(net, net->seqs, nseq, R, ls, est, port_results, s);
+}
+
+int pg_le_train_step_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, const float* est,
+                            const pg_port_result* port_results, const float* h_true, const pg_le_adam* opt,
+                            float* loss, void* stream)
+{
+  if (net == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (ls == nullptr || est == nullptr || port_results == nullptr || h_true == nullptr || opt == nullptr) {
+    return set_error(net->ctx, PG_ERR_INVALID, "learned estimator: null buffer");
+  }
+  cudaStream_t s    = static_cast<cudaStream_t>(stream);
+  int          nseq = 0, R = 0;
+  size_t       terms = 0;
+  if (int rc = stage_seqs(net, ues, nof_ues, nullptr, &nseq, &R, &terms, s)) {
+    return rc;
+  }
+  if (nseq == 0) {
+    return PG_OK;
+  }
+  le_features_kernel<<<(R + 255) / 256, 256, 0, s>>>(net->seqs, nseq, R, reinterpret_cast<const float2*>(est),
+                                                     reinterpret_cast<const float2*>(ls), port_results,
+                                                     reinterpret_cast<uint4*>(net->x), net->row_valid, net->gseq);
+  int rc = check_cuda(net->ctx, cudaGetLastError(), "le_features_kernel launch");
+  if (rc == PG_OK) {
+    rc = forward(net, R, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(net->ctx, cudaMemsetAsync(net->loss, 0, 8, s), "cudaMemsetAsync(loss)");
+  }
+  if (rc == PG_OK) {
+    le_loss_kernel<<<(R + 255) / 256, 256, 0, s>>>(net->seqs, nseq, R, reinterpret_cast<const uint4*>(net->y),
+                                                   net->gseq, reinterpret_cast<const float2*>(est),
+                                                   reinterpret_cast<const float2*>(h_true), 1.f / (float)terms,
+                                                   reinterpret_cast<uint4*>(net->dy), net->loss);
+    rc = check_cuda(net->ctx, cudaGetLastError(), "le_loss_kernel launch");
+  }
+  if (rc == PG_OK) {
+    rc = backward(net, R, s);
+  }
+  if (rc == PG_OK) {
+    rc = pack_launch(net, 1, opt, s);
+  }
+  if (rc == PG_OK && loss != nullptr) {
+    rc = check_cuda(net->ctx, cudaMemcpyAsync(loss, net->loss, 8, cudaMemcpyDeviceToDevice, s), "D2D loss");
+  }
+  return rc;
+}
+
+} // extern "C"

@@ -266,6 +266,12 @@ int pg_create(const pg_config* cfg, pg_context** out)
     rc = check_cuda(ctx, cudaEventCreate(&ctx->ev_stop), "cudaEventCreate");
   }
   if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventCreate(&ctx->ev_le_start), "cudaEventCreate");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventCreate(&ctx->ev_le_stop), "cudaEventCreate");
+  }
+  if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_desc, cudaEventDisableTiming), "cudaEventCreate");
   }
   if (rc == PG_OK) {
@@ -382,6 +388,12 @@ void pg_destroy(pg_context* ctx)
   if (ctx->ev_stop) {
     cudaEventDestroy(ctx->ev_stop);
   }
+  if (ctx->ev_le_start) {
+    cudaEventDestroy(ctx->ev_le_start);
+  }
+  if (ctx->ev_le_stop) {
+    cudaEventDestroy(ctx->ev_le_stop);
+  }
   if (ctx->ev_desc) {
     cudaEventDestroy(ctx->ev_desc);
   }
@@ -489,19 +501,31 @@ int pg_set_kernel_timing(pg_context* ctx, int enabled)
   return PG_OK;
 }
 
-float pg_last_kernel_ms(pg_context* ctx)
+static float elapsed_ms(cudaEvent_t a, cudaEvent_t b)
 {
-  if (ctx == nullptr || !ctx->timed) {
-    return -1.0f;
-  }
   float ms = -1.0f;
-  if (cudaEventSynchronize(ctx->ev_stop) != cudaSuccess ||
-      cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop) != cudaSuccess) {
+  if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
     // Clear the error of the failed query, so that it is not reported by a later launch check.
     (void)cudaGetLastError();
     return -1.0f;
   }
   return ms;
+}
+
+float pg_last_kernel_ms(pg_context* ctx)
+{
+  if (ctx == nullptr || !ctx->timed) {
+    return -1.0f;
+  }
+  return elapsed_ms(ctx->ev_start, ctx->ev_stop);
+}
+
+float pg_last_learned_ms(pg_context* ctx)
+{
+  if (ctx == nullptr || !ctx->timed || !ctx->le_recorded) {
+    return -1.0f;
+  }
+  return elapsed_ms(ctx->ev_le_start, ctx->ev_le_stop);
 }
 
 } // extern "C"

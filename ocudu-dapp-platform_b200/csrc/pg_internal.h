@@ -81,6 +81,9 @@ struct pg_context {
   cudaStream_t        stream         = nullptr; // stream of the _host calls
   cudaEvent_t         ev_start       = nullptr;
   cudaEvent_t         ev_stop        = nullptr;
+  cudaEvent_t         ev_le_start    = nullptr; // learned-estimator stage of slot plans (timed contexts)
+  cudaEvent_t         ev_le_stop     = nullptr;
+  bool                le_recorded    = false;
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
   pg::staging_slot    slots[5];                  // rate-dematch, CRC, TB, PUSCH and UE work lists
@@ -159,7 +162,7 @@ int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, c
 int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
 // max_rb: the largest nof_rb of the UEs (sizes the kernel's shared memory).
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
-                    pg_port_result* results, cudaStream_t s);
+                    float* ls, pg_port_result* results, cudaStream_t s);
 int max_nof_rb(const pg_pusch_ue* ues, int n);
 int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1);
 int equalize_launch(pg_context* ctx, int nof_re, int nof_ports, int nof_layers, const uint32_t* y, const uint32_t* h,
@@ -180,10 +183,41 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
 // CTAs of ldpc_decode_kernel resident on the whole device.
 int ldpc_resident_ctas(pg_context* ctx);
 
-// Tensor-core 1-D convolutions (tc_conv1d.cu): kernel attributes, and the forward launch over an
-// activation buffer of R rows ([C/8][R][8] bf16).
+// Tensor-core 1-D convolutions (tc_conv1d.cu): kernel attributes, the forward launch over an
+// activation buffer of R rows ([C/8][R][8] bf16; bias, res and mask may be null) and the weight
+// gradient (adds to dw[5][cin][cout] and, when db is not null, to db[cout]).
 int conv_setup(pg_context* ctx);
 int conv_forward_launch(pg_context* ctx, int cin, int cout, const void* x, const void* w, const float* bias,
-                        const void* res, void* y, const uint8_t* row_valid, int R, int relu, int* err, cudaStream_t s);
+                        const void* res, const void* mask, void* y, const uint8_t* row_valid, int R, int relu,
+                        int* err, cudaStream_t s);
+int conv_wgrad_launch(pg_context* ctx, int cin, int cout, const void* x, const void* dy, int R, float* dw, float* db,
+                      int* err, cudaStream_t s);
+
+// Learned channel estimator (learned_est.cu): one allocation sequence of the network's row layout
+// (a (UE, receive port, layer) allocation of 12 nof_rb rows).
+struct le_seq {
+  uint32_t row0;    // first row
+  uint32_t len;     // rows = 12 nof_rb
+  uint32_t est0;    // complex-float offset of (port, DM-RS symbol 0, layer) in est / ls / h_true
+  uint32_t dstride; // complex floats from DM-RS symbol 0 to 1 (layers x 12 nof_rb)
+  uint32_t pr;      // port-result index (u * 4 + port)
+  float    beta;    // DM-RS amplitude
+  uint8_t  layer, nof_layers, nd, pad;
+  uint32_t pad2;
+};
+static_assert(sizeof(le_seq) == 32, "le_seq layout");
+
+// Sequences of the UEs with use[u] != 0 (all when use is null), est_offset already assigned;
+// returns the rows of the layout (0 without sequences) and, in *terms, the loss terms.
+size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vector<le_seq>& out, size_t* terms);
+// PG_OK when the net's buffers hold `rows` rows and `nseq` sequences, else PG_ERR_CAPACITY.
+int le_capacity(const pg_le_net* net, size_t rows, int nseq);
+pg_context* le_context(const pg_le_net* net);
+// Features -> network -> est += correction, for sequences already in device memory.
+int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, const float* ls, float* est,
+                     const pg_port_result* pr, cudaStream_t s);
+// Event-record flags for timing events on stream s: under stream capture the records become event
+// nodes of the graph (external records).
+unsigned int timing_record_flags(pg_context* ctx, cudaStream_t s);
 
 } // namespace pg

@@ -196,6 +196,7 @@ __device__ void virtual_pilots(float2* out, const float2* base, int nv, bool is_
 __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pusch_ue* __restrict__ ues,
                                                                      const uint32_t* __restrict__ grids,
                                                                      float2* __restrict__ est_all,
+                                                                     float2* __restrict__ ls_all,
                                                                      pg_port_result* __restrict__ results,
                                                                      const uint32_t* __restrict__ gold,
                                                                      uint32_t gold_words, int npil_max)
@@ -275,6 +276,18 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
     e[kMaxV + k + 1] = make_float2(v1.x * inv_beta, v1.y * inv_beta);
   }
   __syncthreads();
+  if (ls_all != nullptr) {
+    // The LS estimates themselves (input of the learned estimator): the pilots' subcarriers
+    // (even) of the frequency-response layout, zero on the odd ones.
+    float2* ls = ls_all + ue.est_offset + (size_t)port * nd * nl * nsc;
+    for (int i = tid; i < nd * nl * nsc; i += kEstThreads) {
+      const int d = i / (nl * nsc);
+      const int r = i - d * nl * nsc;
+      const int l = r / nsc;
+      const int j = r - l * nsc;
+      ls[i]       = (j & 1) ? make_float2(0.f, 0.f) : ext(d, l)[kMaxV + (j >> 1)];
+    }
+  }
 
   // Smoothing filter and virtual pilots.
   const int tsel  = nrb >= 3 ? 2 : nrb - 1;
@@ -469,14 +482,15 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
 }
 
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
-                    pg_port_result* results, cudaStream_t s)
+                    float* ls, pg_port_result* results, cudaStream_t s)
 {
   if (n == 0) {
     return PG_OK;
   }
   const int npil_max = 6 * std::max(1, std::min(max_rb, 275));
   pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, est_smem_bytes(npil_max), s>>>(
-      ues_dev, grids, reinterpret_cast<float2*>(est), results, ctx->dev.gold, kGoldWords, npil_max);
+      ues_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls), results, ctx->dev.gold,
+      kGoldWords, npil_max);
   return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
 }
 
@@ -523,6 +537,12 @@ size_t pg_pusch_est_size(const pg_pusch_ue* ue)
 int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids, float* est,
                              pg_port_result* results, void* stream)
 {
+  return pg_pusch_estimate_ls_device(ctx, ues, nof_ues, grids, est, nullptr, results, stream);
+}
+
+int pg_pusch_estimate_ls_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids,
+                                float* est, float* ls, pg_port_result* results, void* stream)
+{
   if (ctx == nullptr) {
     return PG_ERR_INVALID;
   }
@@ -538,7 +558,7 @@ int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ue
     return rc;
   }
   if (int rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(dev), nof_ues, max_nof_rb(ues, nof_ues), grids, est,
-                               results, s)) {
+                               ls, results, s)) {
     return rc;
   }
   return release_slot_after(ctx, SLOT_UE, s);

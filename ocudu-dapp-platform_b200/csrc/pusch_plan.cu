@@ -22,7 +22,7 @@ using namespace pg;
 struct pg_pusch_plan {
   pg_context*              ctx = nullptr;
   int                      nof_ues = 0, nof_cbs = 0;
-  size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0;
+  size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0, est_total = 0;
   uint32_t                 total_re = 0;
   int                      max_rb   = 1;
   std::vector<pg_pusch_ue> ues;
@@ -51,6 +51,13 @@ struct pg_pusch_plan {
   pg_sch_result*  d_res    = nullptr; // results of execute_host
   // Pinned host buffers of execute_host: [results | port results | TBs].
   void*           host     = nullptr;
+  // Learned estimator: the net, the LS estimates and the sequences of the refined UEs.
+  pg_le_net*      le_net    = nullptr;
+  void*           le_dev    = nullptr;
+  float*          d_ls      = nullptr;
+  le_seq*         d_le_seqs = nullptr;
+  int             le_nseq   = 0;
+  int             le_rows   = 0;
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -99,7 +106,19 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
             pg_port_result* port_results, cudaStream_t s)
 {
   pg_context* ctx = p->ctx;
-  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->max_rb, grids, p->d_est, port_results, s);
+  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->max_rb, grids, p->d_est,
+                                    p->le_net != nullptr ? p->d_ls : nullptr, port_results, s);
+  if (rc == PG_OK && p->le_net != nullptr) {
+    const unsigned int flags = timing_record_flags(ctx, s);
+    if (ctx->timed) {
+      cudaEventRecordWithFlags(ctx->ev_le_start, s, flags);
+    }
+    rc = le_refine_launch(p->le_net, p->d_le_seqs, p->le_nseq, p->le_rows, p->d_ls, p->d_est, port_results, s);
+    if (ctx->timed) {
+      cudaEventRecordWithFlags(ctx->ev_le_stop, s, flags);
+      ctx->le_recorded = true;
+    }
+  }
   if (rc == PG_OK) {
     rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
                            p->d_seq_off, p->d_seq, p->d_llr, s);
@@ -131,6 +150,7 @@ void release(pg_pusch_plan* p)
     cudaGraphExecDestroy(p->exec);
   }
   cudaFree(p->dev);
+  cudaFree(p->le_dev);
   if (p->host) {
     cudaFreeHost(p->host);
   }
@@ -196,7 +216,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     t.rv               = u.rv;
     t.max_iterations   = u.max_iterations;
   }
-  p->max_rb = max_nof_rb(p->ues.data(), nof_ues);
+  p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
+  p->est_total = est_total;
   std::vector<uint32_t> re_off(nof_ues + 1);
   p->total_re = data_re_offsets(p->ues.data(), nof_ues, re_off.data());
   sch_work w;
@@ -340,6 +361,59 @@ int pg_pusch_plan_set_graph(pg_pusch_plan* plan, int enabled)
     return PG_ERR_INVALID;
   }
   plan->use_graph = enabled != 0;
+  return PG_OK;
+}
+
+int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t* use)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (net != nullptr && le_context(net) != ctx) {
+    return set_error(ctx, PG_ERR_INVALID, "the learned estimator belongs to another context");
+  }
+  if (int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize")) {
+    return rc;
+  }
+  if (plan->exec != nullptr) {
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  cudaFree(plan->le_dev);
+  plan->le_dev    = nullptr;
+  plan->le_net    = nullptr;
+  plan->d_ls      = nullptr;
+  plan->d_le_seqs = nullptr;
+  plan->le_nseq = plan->le_rows = 0;
+  if (net == nullptr) {
+    return PG_OK;
+  }
+  std::vector<le_seq> seqs;
+  const size_t        rows = le_build_seqs(plan->ues.data(), plan->nof_ues, use, seqs, nullptr);
+  if (le_capacity(net, rows, (int)seqs.size()) != PG_OK) {
+    return set_error(ctx, PG_ERR_CAPACITY,
+                     "learned estimator: the plan needs " + std::to_string(rows) + " rows, more than the net holds");
+  }
+  const size_t o_seq = al(plan->est_total * 8);
+  const size_t bytes = o_seq + al(std::max<size_t>(1, seqs.size()) * sizeof(le_seq));
+  int          rc    = check_cuda(ctx, cudaMalloc(&plan->le_dev, bytes), "cudaMalloc(plan learned estimator)");
+  if (rc == PG_OK && !seqs.empty()) {
+    rc = check_cuda(ctx,
+                    cudaMemcpy(static_cast<uint8_t*>(plan->le_dev) + o_seq, seqs.data(), seqs.size() * sizeof(le_seq),
+                               cudaMemcpyHostToDevice),
+                    "H2D plan learned-estimator sequences");
+  }
+  if (rc != PG_OK) {
+    cudaFree(plan->le_dev);
+    plan->le_dev = nullptr;
+    return rc;
+  }
+  plan->d_ls      = static_cast<float*>(plan->le_dev);
+  plan->d_le_seqs = reinterpret_cast<le_seq*>(static_cast<uint8_t*>(plan->le_dev) + o_seq);
+  plan->le_nseq   = (int)seqs.size();
+  plan->le_rows   = (int)rows;
+  plan->le_net    = net;
   return PG_OK;
 }
 

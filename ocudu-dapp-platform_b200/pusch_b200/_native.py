@@ -72,6 +72,11 @@ class PgSchResult(ctypes.Structure):
                 ("mean_iterations", ctypes.c_float), ("max_iterations_run", ctypes.c_uint32)]
 
 
+class PgLeAdam(ctypes.Structure):
+    _fields_ = [("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
+                ("weight_decay", ctypes.c_float)]
+
+
 class PgPuschPlanInfo(ctypes.Structure):
     _fields_ = [("nof_ues", ctypes.c_uint32), ("nof_codeblocks", ctypes.c_uint32), ("tb_bytes", ctypes.c_uint64),
                 ("nof_llrs", ctypes.c_uint64), ("grid_words", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
@@ -123,6 +128,25 @@ SIGNATURES = {
     "pg_pusch_plan_execute_host": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_size_t, _VP, _VP]),
     "pg_conv1d_forward_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP,
                                                 ctypes.c_int, ctypes.c_int, _VP, _VP]),
+    "pg_conv1d_backward_data_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP,
+                                                      ctypes.c_int, _VP, _VP]),
+    "pg_conv1d_backward_weights_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.c_int,
+                                                         _VP, _VP, _VP, _VP]),
+    "pg_last_learned_ms": (ctypes.c_float, [_VP]),
+    "pg_le_nof_params": (ctypes.c_size_t, []),
+    "pg_le_rows": (ctypes.c_size_t, [_VP, ctypes.c_int]),
+    "pg_le_create": (ctypes.c_int, [_VP, ctypes.c_int, _VP]),
+    "pg_le_destroy": (None, [_VP]),
+    "pg_le_set_params": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t]),
+    "pg_le_get_params": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t]),
+    "pg_le_get_grads": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t]),
+    "pg_le_status": (ctypes.c_int, [_VP]),
+    "pg_le_forward_device": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _VP, _VP]),
+    "pg_le_backward_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP]),
+    "pg_le_refine_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_le_train_step_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_estimate_ls_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),
 }
 
 _lib = None

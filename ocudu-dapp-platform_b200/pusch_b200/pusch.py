@@ -147,6 +147,20 @@ class PuschSlotPlan:
     def set_graph(self, enabled: bool):
         self.ctx.check(self.lib.pg_pusch_plan_set_graph(self.handle, int(bool(enabled))))
 
+    def set_learned(self, net, use=None):
+        """Refines the channel estimates with a LearnedEstimator (None: the plain estimator only)
+        for the UEs with use[u] true (all when use is None)."""
+        u = None if use is None else (ctypes.c_uint8 * self.n)(*[int(bool(v)) for v in use])
+        self.ctx.check(self.lib.pg_pusch_plan_set_learned(self.handle, net.handle if net is not None else None, u))
+
+    def le_rows(self, use=None):
+        """Rows a LearnedEstimator needs for this plan."""
+        if use is None:
+            return int(self.lib.pg_le_rows(ctypes.addressof(self.descs), self.n))
+        sel = [self.descs[i] for i in range(self.n) if use[i]]
+        arr = (PgPuschUe * len(sel))(*sel)
+        return int(self.lib.pg_le_rows(ctypes.addressof(arr), len(sel))) if sel else 0
+
     def execute_device(self, grid_ptr, tb_ptr, results_ptr, port_results_ptr=None, stream_ptr=0):
         self.ctx.check(self.lib.pg_pusch_plan_execute_device(self.handle, grid_ptr, tb_ptr, results_ptr,
                                                              port_results_ptr, stream_ptr))

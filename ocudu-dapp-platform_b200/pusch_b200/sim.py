@@ -81,6 +81,7 @@ class PuschUe:
     channel: str = "flat"   # "flat": one CN(0,1) coefficient per (port, layer); "pdp": exponential PDP
     rms_delay_ns: float = 100.0
     nof_taps: int = 8
+    doppler_hz: float = 0.0  # maximum Doppler shift of the "pdp" taps (0: constant in time)
 
 
 @dataclass
@@ -93,8 +94,9 @@ class PuschSlot:
     slot: int
     scs_khz: int = 30
     dmrs_scaling: float = float(np.float32(10 ** (3 / 20)))  # two CDM groups without data: +3 dB DM-RS
-    channels: list = field(default_factory=list)
+    channels: list = field(default_factory=list)      # per UE: [P][L][nsc] or [P][L][14][nsc]
     noise_vars: list = field(default_factory=list)
+    symbols: list = field(default_factory=list)       # per UE: transmitted data symbols [RE][layer]
 
 
 def data_symbol_list(ue):
@@ -106,8 +108,15 @@ def nof_ch_symbols(ue):
     return len(data_symbol_list(ue)) * 12 * ue.nof_rb * ue.nof_layers
 
 
+def symbol_start_s(scs_khz=30):
+    """Start time of each of the 14 OFDM symbols of a slot (normal cyclic prefix, equal symbols)."""
+    return np.arange(14) * (1e-3 / (scs_khz / 15) / 14)
+
+
 def channel_response(rng, ue, nof_ports, scs_khz):
-    """Frequency response H [port][layer][12*nof_rb] over the allocation, constant in time."""
+    """Frequency response over the allocation: H [port][layer][12*nof_rb], constant in time, or
+    [port][layer][14][12*nof_rb] for exponential-PDP taps with a Doppler shift (each tap a sum of
+    16 sinusoids with random arrival angles and phases: Rayleigh fading with Jakes' spectrum)."""
     nsc = 12 * ue.nof_rb
     if ue.channel == "flat":
         h = (rng.standard_normal((nof_ports, ue.nof_layers)) + 1j * rng.standard_normal((nof_ports, ue.nof_layers)))
@@ -118,9 +127,17 @@ def channel_response(rng, ue, nof_ports, scs_khz):
     p = np.exp(-tau / (ue.rms_delay_ns * 1e-9))
     p /= p.sum()
     f = (np.arange(nsc) + 12 * ue.rb_start) * scs_khz * 1e3
+    steer = np.exp(-2j * np.pi * tau[:, None] * f[None, :])
+    if ue.doppler_hz > 0:
+        m = 16
+        ang = rng.uniform(0, 2 * np.pi, (nof_ports, ue.nof_layers, ue.nof_taps, m))
+        ph = rng.uniform(0, 2 * np.pi, (nof_ports, ue.nof_layers, ue.nof_taps, m))
+        t = symbol_start_s(scs_khz)
+        a = np.exp(1j * (2 * np.pi * ue.doppler_hz * np.cos(ang)[..., None] * t + ph[..., None])).sum(3) / np.sqrt(m)
+        return np.einsum("plts,tf->plsf", a * np.sqrt(p)[None, None, :, None], steer)
     taps = (rng.standard_normal((nof_ports, ue.nof_layers, ue.nof_taps))
             + 1j * rng.standard_normal((nof_ports, ue.nof_layers, ue.nof_taps))) * np.sqrt(p / 2)
-    return np.einsum("plt,tf->plf", taps, np.exp(-2j * np.pi * tau[:, None] * f[None, :]))
+    return np.einsum("plt,tf->plf", taps, steer)
 
 
 def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30):
@@ -134,7 +151,7 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
     rng = np.random.default_rng(seed)
     nsc_grid = 12 * nof_prb_grid
     grid = np.zeros((nof_ports, 14, nsc_grid), np.complex128)
-    truth, chans, nvs = [], [], []
+    truth, chans, nvs, syms = [], [], [], []
     beta = float(np.float32(10 ** (3 / 20)))
     for ue in ues:
         ncs = nof_ch_symbols(ue)
@@ -156,7 +173,8 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
             else:
                 tx = x[r:r + nre_sym].T
                 r += nre_sym
-            grid[:, s, sc] += np.einsum("plf,lf->pf", h, tx)
+            hs = h[:, :, s, :] if h.ndim == 4 else h
+            grid[:, s, sc] += np.einsum("plf,lf->pf", hs, tx)
         # Noise: SNR per receive port relative to unit per-layer signal power.
         nv = 10 ** (-ue.snr_db / 10)
         for s in range(ue.first_symbol, ue.first_symbol + ue.nof_symbols):
@@ -165,8 +183,9 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
         truth.append(tb)
         chans.append(h)
         nvs.append(nv)
+        syms.append(x)
     return PuschSlot(to_cbf16(grid.astype(np.complex64)), list(ues), truth, nof_ports, nof_prb_grid, slot, scs_khz,
-                     beta, chans, nvs)
+                     beta, chans, nvs, syms)
 
 
 # ----------------------------------------------------------------------------------------------
@@ -206,13 +225,18 @@ def full_cell_slot(seed=0, slot=0):
     return make_pusch_slot([ue], 4, nof_prb_grid=273, seed=seed, slot=slot)
 
 
-def uneven_cells(seed=0, nof_cells=16, nof_ports=4, snr_range=(0.0, 30.0), max_ues=16):
+def uneven_cells(seed=0, nof_cells=16, nof_ports=4, snr_range=(0.0, 30.0), max_ues=16, delay_range_ns=None,
+                 doppler_range_hz=None, la_margin_db=0.0):
     """The batched uneven slot: nof_cells cells of 273 PRB, each with 1..max_ues UEs on contiguous
     PRB allocations that tile at most 273 PRB, 1 or 2 layers, per-UE SNR uniform in snr_range,
     exponential-PDP channels. The MCS (table 2) of each UE is drawn among the indices its SNR
-    supports (required_snr_db), the highest few favoured; TBS and base graph follow from it."""
+    supports (required_snr_db), the highest few favoured; TBS and base graph follow from it.
+    With delay_range_ns / doppler_range_hz, each UE's RMS delay spread and maximum Doppler shift
+    are drawn uniformly from them (from a second generator, so the rest of the slot is the same);
+    otherwise 100 ns and no Doppler. la_margin_db raises every link-adaptation threshold."""
     from . import mcs as mcs_tables
     rng = np.random.default_rng(seed)
+    rng_ch = np.random.default_rng([seed, 1])
     slots = []
     for cell in range(nof_cells):
         n_ues = int(rng.integers(1, max_ues + 1))
@@ -225,15 +249,20 @@ def uneven_cells(seed=0, nof_cells=16, nof_ports=4, snr_range=(0.0, 30.0), max_u
             layers = int(rng.integers(1, 3))
             snr = float(rng.uniform(*snr_range))
             ok = [i for i, (qm, r) in enumerate(mcs_tables.MCS_TABLE_2)
-                  if required_snr_db(qm, r, layers, nof_ports) <= snr]
+                  if required_snr_db(qm, r, layers, nof_ports) + la_margin_db <= snr]
             if not ok and layers == 2:
                 layers = 1
                 ok = [i for i, (qm, r) in enumerate(mcs_tables.MCS_TABLE_2)
-                      if required_snr_db(qm, r, layers, nof_ports) <= snr]
+                      if required_snr_db(qm, r, layers, nof_ports) + la_margin_db <= snr]
             top = max(ok) if ok else 0
             index = int(rng.integers(max(0, top - 3), top + 1))
+            ch = {}
+            if delay_range_ns is not None:
+                ch["rms_delay_ns"] = float(rng_ch.uniform(*delay_range_ns))
+            if doppler_range_hz is not None:
+                ch["doppler_hz"] = float(rng_ch.uniform(*doppler_range_hz))
             ues.append(ue_from_mcs(edges[u], nof_rb, layers, 2, index, (2, 11), snr_db=snr, channel="pdp",
-                                   rnti=0x4000 + 16 * cell + u, n_id=cell, n_id_data=cell))
+                                   rnti=0x4000 + 16 * cell + u, n_id=cell, n_id_data=cell, **ch))
         slots.append(make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=cell % 20,
                                      seed=int(rng.integers(0, 2 ** 31))))
     return slots

@@ -56,3 +56,29 @@ def conv1d_ref(x, w, b, res=None, relu=False, valid=None):
     if relu:
         y = np.maximum(y, 0)
     return y
+
+
+def pack_weights_t(w):
+    """Packed weights of the input-gradient convolution of a layer W[co][ci][5]:
+    W'[ci][co][t] = W[co][ci][4 - t], packed as [5][co/8][ci][8] bf16 bits."""
+    return pack_weights(np.ascontiguousarray(np.asarray(w)[:, :, ::-1].transpose(1, 0, 2)))
+
+
+def conv1d_backward_ref(x, w, dy):
+    """Float64 gradients of y = conv(x, W) (+ b) for 'same' zero padding on one sample:
+    dx[q][ci] = sum_{t,co} dy[q - t + 2][co] W[co][ci][t], dw[t][ci][co] = sum_r x[r + t - 2][ci] dy[r][co],
+    db[co] = sum_r dy[r][co]."""
+    rows, ci = x.shape
+    co = w.shape[0]
+    x = np.asarray(x, np.float64)
+    dy = np.asarray(dy, np.float64)
+    xp = np.zeros((rows + 4, ci))
+    xp[2:2 + rows] = x
+    dyp = np.zeros((rows + 4, co))
+    dyp[2:2 + rows] = dy
+    dx = np.zeros((rows, ci))
+    dw = np.zeros((5, ci, co))
+    for t in range(5):
+        dx += dyp[4 - t:4 - t + rows] @ np.asarray(w[:, :, t], np.float64)
+        dw[t] = xp[t:t + rows].T @ dy
+    return dx, dw, dy.sum(axis=0)

@@ -1,0 +1,147 @@
+"""Learned channel estimator on the GPU: forward pass and gradients of the tensor-core network
+against the float64 restatement (oracle/learned_ref.py, bf16 rounding at the same points), the
+refinement path (features -> network -> corrected estimates) against the restatement, and what
+training on the GPU gains over the plain estimator."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import learned_ref as lr
+from pusch_b200 import learned
+from pusch_b200 import tclayout as tl
+
+pytestmark = pytest.mark.gpu
+
+
+def chunked_dev(a):
+    import torch
+    return torch.from_numpy(tl.to_chunked(a).view(np.int16)).cuda()
+
+
+def random_rows(rng, lens):
+    rows = sum(n + 2 for n in lens) + 2
+    valid = np.zeros(rows, bool)
+    r = 0
+    for n in lens:
+        r += 2
+        valid[r:r + n] = True
+        r += n
+    return rows, valid
+
+
+def test_forward_and_gradients_match_oracle(ctx):
+    import torch
+    rng = np.random.default_rng(5)
+    rows, valid = random_rows(rng, [300, 37, 12, 600, 250])
+    params = learned.init_params(7)
+    params[-16 - 5 * 64 * 16:] *= 50.0
+    x = tl.bf16_round((rng.standard_normal((rows, 16)) * valid[:, None]).astype(np.float32))
+    dy = tl.bf16_round((rng.standard_normal((rows, 16)) * valid[:, None]).astype(np.float32))
+    net = learned.LearnedEstimator(ctx, max_rows=rows, params=params)
+    # Every device buffer stays referenced until the work that reads it has run.
+    x_dev, dy_dev = chunked_dev(x), chunked_dev(dy)
+    v_dev = torch.from_numpy(valid.astype(np.uint8)).cuda()
+    y_dev = torch.zeros((2, rows, 8), dtype=torch.int16, device="cuda")
+    net.forward(x_dev.data_ptr(), v_dev.data_ptr(), rows, y_dev.data_ptr())
+    net.backward(dy_dev.data_ptr(), rows)
+    y = tl.from_chunked(y_dev.cpu().numpy().view(np.uint16))
+    g = net.grads()
+    net.status()
+    y_ref, cache = lr.forward(params.astype(np.float64), x.astype(np.float64), valid, bf16_acts=True)
+    g_ref = lr.backward(cache, dy.astype(np.float64))
+    # Forward: bf16 storage of 14 layers; FP32 accumulation order is the only difference.
+    assert np.linalg.norm(y - y_ref) <= 2e-2 * np.linalg.norm(y_ref), np.abs(y - y_ref).max()
+    assert (y[~valid] == 0).all()
+    # Gradients, layer by layer (weights and biases).
+    offs, total = lr.layer_offsets()
+    for i, (cin, cout) in enumerate(lr.LAYERS):
+        a, b = offs[i], offs[i] + 5 * cin * cout + cout
+        err = np.linalg.norm(g[a:b] - g_ref[a:b]) / np.linalg.norm(g_ref[a:b])
+        assert err < 3e-2, (i, err)
+    net.close()
+
+
+def make_batch(ctx, seed, rows):
+    import torch
+    src = learned.DmrsTrainingSource(seed)
+    descs, grid, h_true, est_size, ues = src.batch(rows)
+    n = len(descs)
+    est = torch.empty(2 * est_size, dtype=torch.float32, device="cuda")
+    ls = torch.empty_like(est)
+    pr = torch.empty((n * 4, 5), dtype=torch.float32, device="cuda")
+    ctx.check(ctx.lib.pg_pusch_estimate_ls_device(ctx.handle, ctypes.addressof(descs), n, grid.data_ptr(),
+                                                  est.data_ptr(), ls.data_ptr(), pr.data_ptr(), None))
+    torch.cuda.synchronize()
+    return descs, est, ls, pr, h_true
+
+
+def test_refine_matches_oracle(ctx):
+    import torch
+    descs, est, ls, pr, h_true = make_batch(ctx, 3, 20_000)
+    n = len(descs)
+    params = learned.init_params(11)
+    params[-16 - 5 * 64 * 16:] *= 30.0
+    rows = int(ctx.lib.pg_le_rows(ctypes.addressof(descs), n))
+    net = learned.LearnedEstimator(ctx, max_rows=rows, params=params)
+    use = [i % 3 != 1 for i in range(n)]
+    est_h = est.cpu().numpy().view(np.complex64).astype(np.complex128)
+    ls_h = ls.cpu().numpy().view(np.complex64).astype(np.complex128)
+    prh = pr.cpu().numpy().reshape(n, 4, 5)
+    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr(), use=use)
+    got = est.cpu().numpy().view(np.complex64).astype(np.complex128)
+    net.status()
+    # Restatement over the used UEs only (the layout skips the others).
+    sel = [i for i in range(n) if use[i]]
+    ues = [dict(nof_rb=descs[i].nof_rb, nof_layers=descs[i].nof_layers, nof_rx_ports=4, nd=2) for i in sel]
+    seqs, R = lr.sequences(ues, [descs[i].est_offset for i in sel])
+    assert R + 0 == rows - sum(4 * descs[i].nof_layers * (12 * descs[i].nof_rb + 2) for i in range(n) if not use[i])
+    x, valid, gains = lr.features(seqs, R, est_h, ls_h, prh[sel, :, 0], prh[sel, :, 3:5],
+                                  [descs[i].dmrs_scaling for i in sel])
+    y, _ = lr.forward(params.astype(np.float64), x, valid, bf16_acts=True)
+    want = lr.refine(seqs, est_h, y, gains)
+    corr = want - est_h
+    err = np.linalg.norm(got - want) / max(np.linalg.norm(corr), 1e-12)
+    assert err < 3e-2, err
+    for i in range(n):
+        if not use[i]:
+            o = descs[i].est_offset
+            m = 4 * 2 * descs[i].nof_layers * 12 * descs[i].nof_rb
+            assert np.array_equal(got[o:o + m], est_h[o:o + m])
+    net.close()
+
+
+def nmse(est, h_true):
+    e = est.view(-1, 2) - h_true.view(-1, 2)
+    return float((e ** 2).sum() / (h_true ** 2).sum())
+
+
+def test_training_on_gpu_beats_plain_estimator(ctx):
+    """A short training run on the GPU (the library's own forward/backward kernels and Adam)
+    lowers the channel-estimate error below the plain estimator's on held-out batches."""
+    net, hist = learned.train(ctx, steps=400, rows_per_step=40_000, seed=1, lr=1e-3, log_every=100, verbose=False)
+    assert hist[-1][1] < hist[0][1]
+    descs, est, ls, pr, h_true = make_batch(ctx, 999, 60_000)
+    before = nmse(est, h_true)
+    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
+    after = nmse(est, h_true)
+    net.status()
+    assert after < 0.9 * before, (before, after)
+    net.close()
+
+
+def test_committed_weights_gain_over_plain(ctx):
+    """The committed trained parameters: the estimate error on held-out batches is well below the
+    plain estimator's."""
+    params = learned.load_params()
+    if params is None:
+        pytest.skip("no trained parameters committed")
+    descs, est, ls, pr, h_true = make_batch(ctx, 4242, 80_000)
+    rows = int(ctx.lib.pg_le_rows(ctypes.addressof(descs), len(descs)))
+    net = learned.LearnedEstimator(ctx, max_rows=rows, params=params)
+    before = nmse(est, h_true)
+    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
+    after = nmse(est, h_true)
+    net.status()
+    assert after < 0.7 * before, (before, after)
+    net.close()
