@@ -25,6 +25,7 @@
 // MSE of the correction against g (H_true - plain) -> backward (input gradients through the
 // transposed convolutions with the ReLU masks, weight gradients on the tensor cores) -> Adam.
 #include "pg_internal.h"
+#include "tc_common.cuh"
 
 #include <cuda_bf16.h>
 
@@ -34,6 +35,8 @@
 #include <vector>
 
 namespace {
+
+using namespace pg::tc;
 
 constexpr int kLayers = 14;
 constexpr int kBlocks = 6;
@@ -105,6 +108,8 @@ struct pg_le_net {
 };
 
 namespace {
+
+using namespace pg::tc;
 
 __device__ __forceinline__ int find_seq(const le_seq* __restrict__ seqs, int nseq, uint32_t r)
 {
@@ -306,6 +311,332 @@ size_t al(size_t x)
 {
   return (x + 255) & ~(size_t)255;
 }
+// ---------------------------------------------------------------------------------------------
+// Fused inference: the whole network per window of 384 rows in one kernel, activations in shared
+// memory, accumulators in tensor memory, each layer's weights brought in by 1-D bulk copies while
+// the previous layer computes. Every layer loses two exact rows at each window edge (its taps reach
+// two rows beyond), so after 14 layers the central 328 rows are exact and are the ones stored:
+// windows overlap by 56 rows. Buffers: X (16 input channels), A (block input and output; the second
+// layer of a block adds A and writes A in place, row by row), B (block middle); two zero rows
+// before and after the window in every buffer.
+//
+// Dataflow within a window (no CTA-wide barrier between layers): the window is three M tiles of 128
+// rows. A producer warp issues the MMAs of tile c of layer l as soon as the epilogues of layer l - 1
+// for tiles c - 1, c and c + 1 (the rows its taps read, and the accumulator columns it overwrites)
+// have arrived on their barriers, and commits them to tile c's barrier. Eight epilogue warps per
+// tile (two per TMEM lane quarter, one per half of the output channels) wait for that commit, add
+// bias and residual, apply the ReLU and the row mask, store bf16 to shared memory, make the stores
+// visible to the tensor cores and arrive. So the MMAs of one tile overlap the epilogues of the
+// others, across layer boundaries. The epilogue of layer l, tile c writes its destination buffer
+// only after its own MMAs, which waited for every MMA of layer l - 1 that read those rows.
+constexpr int      kFTiles     = 3;
+constexpr int      kFWin       = 128 * kFTiles;
+constexpr int      kFPad       = 2;
+constexpr int      kFRows      = kFWin + 2 * kFPad;
+constexpr int      kFMargin    = 2 * kLayers;
+constexpr int      kFOut       = kFWin - 2 * kFMargin;
+constexpr int      kFEpiWarps  = 8 * kFTiles;
+constexpr int      kFThreads   = 32 * (kFEpiWarps + 1); // + producer warp
+constexpr uint32_t kFChunkB    = kFRows * 16;
+constexpr uint32_t kFActB      = 8 * kFChunkB;
+constexpr uint32_t kFXB        = 2 * kFChunkB;
+constexpr uint32_t kFWB        = kTaps * 8 * kCh * 16;
+constexpr uint32_t kFOffX      = 2 * kFActB;
+constexpr uint32_t kFOffW      = kFOffX + kFXB;
+constexpr uint32_t kFOffBias   = kFOffW + 2 * kFWB;
+constexpr uint32_t kFOffVal    = kFOffBias + kLayers * kCh * 4;
+constexpr uint32_t kFOffBar    = kFOffVal + kFWin;
+constexpr int      kFBars      = 2 * kFTiles + 2; // MMA done [3], epilogue done [3], weights [2]
+constexpr size_t   kFSmem      = kFOffBar + 8 * kFBars + 16;
+constexpr uint32_t kFCopy      = 16384; // bytes per bulk copy
+constexpr uint32_t kFCols      = 256;   // TMEM columns: 64 per M tile
+static_assert(kFOffX % 16 == 0 && kFOffW % 16 == 0 && kFOffBias % 16 == 0 && kFOffBar % 8 == 0, "smem layout");
+static_assert(kFSmem <= 227 * 1024, "shared memory of the fused kernel");
+
+__device__ __forceinline__ uint32_t layer_weight_bytes(int l)
+{
+  return (uint32_t)(kTaps * c_layers[l].cin * c_layers[l].cout * 2);
+}
+
+// Bulk copy of layer l's packed weights into `dst`, completing on `bar`.
+__device__ __forceinline__ void fused_load_weights(const uint16_t* __restrict__ wf, int l, uint32_t dst, uint32_t bar)
+{
+  const uint32_t bytes = layer_weight_bytes(l);
+  const char*    src   = reinterpret_cast<const char*>(wf + c_layers[l].p_off);
+  mbar_expect_tx(bar, bytes);
+  for (uint32_t o = 0; o < bytes; o += kFCopy) {
+    bulk_g2s(dst + o, src + o, min(kFCopy, bytes - o), bar);
+  }
+}
+
+// The MMAs of M tile c of one layer, committed to `bar`. The descriptors are formed once; each
+// MMA adds its constant offset (16-byte units) to the start-address field, which stays below 2^14
+// (shared memory < 256 KB), so no carry reaches the LBO field.
+template <int CIN, int COUT>
+__device__ __forceinline__ void fused_issue_tile(int c, uint32_t src, uint32_t wb, uint32_t tmem, uint32_t bar)
+{
+  constexpr uint32_t idesc = make_idesc(128, COUT, false, false);
+  constexpr uint32_t wtap  = (uint32_t)(CIN / 8) * COUT * 16;
+  const uint64_t     a0    = make_desc(src + (uint32_t)(c * 128) * 16u, kFChunkB, 128);
+  const uint64_t     b0    = make_desc(wb, COUT * 16, 128);
+#pragma unroll
+  for (int t = 0; t < kTaps; ++t) {
+#pragma unroll
+    for (int kc = 0; kc < CIN / 16; ++kc) {
+      const uint64_t ad = a0 + (uint64_t)(((uint32_t)t * 16u + (uint32_t)(2 * kc) * kFChunkB) >> 4);
+      const uint64_t bd = b0 + (uint64_t)(((uint32_t)t * wtap + (uint32_t)(2 * kc) * COUT * 16) >> 4);
+      mma_bf16(tmem + (uint32_t)(c * 64), ad, bd, idesc, (t | kc) != 0 ? 1u : 0u);
+    }
+  }
+  mma_commit(bar);
+}
+
+// Bounded wait that gives up at once when another thread has recorded a failure.
+__device__ __forceinline__ bool fused_wait(uint32_t bar, uint32_t parity, volatile uint32_t* abort_sm,
+                                           int* __restrict__ err)
+{
+  if (*abort_sm != 0) {
+    return false;
+  }
+  if (mbar_wait_bounded(bar, parity)) {
+    return true;
+  }
+  *abort_sm = 1;
+  atomicExch(err, 1);
+  return false;
+}
+
+__global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const uint4* __restrict__ x,
+                                                                        const uint8_t* __restrict__ row_valid,
+                                                                        const uint16_t* __restrict__ wf,
+                                                                        const float* __restrict__ params, int R,
+                                                                        uint4* __restrict__ y, int* __restrict__ err)
+{
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint4*             xs       = reinterpret_cast<uint4*>(smem + kFOffX);
+  float*             bias_s   = reinterpret_cast<float*>(smem + kFOffBias);
+  uint8_t*           valid_s  = smem + kFOffVal;
+  uint64_t*          bars     = reinterpret_cast<uint64_t*>(smem + kFOffBar);
+  uint32_t*          tmem_sm  = reinterpret_cast<uint32_t*>(bars + kFBars);
+  volatile uint32_t* abort_sm = tmem_sm + 1;
+  const int          tid      = threadIdx.x;
+  const int          warp     = tid >> 5;
+  const int          lane     = tid & 31;
+  const int          ntiles   = (R + kFOut - 1) / kFOut;
+  if ((int)blockIdx.x >= ntiles) {
+    return;
+  }
+  for (int i = tid; i < 2 * 8 * 2 * kFPad; i += kFThreads) {
+    const int b = i / (8 * 2 * kFPad), c = (i / (2 * kFPad)) % 8, k = i % (2 * kFPad);
+    reinterpret_cast<uint4*>(smem + b * kFActB + c * kFChunkB)[k < kFPad ? k : kFWin + k] = make_uint4(0, 0, 0, 0);
+  }
+  for (int i = tid; i < kLayers * kCh; i += kFThreads) {
+    const int        l = i / kCh, co = i - l * kCh;
+    const layer_desc L = c_layers[l];
+    bias_s[i]          = co < L.cout ? params[L.w_off + kTaps * L.cin * L.cout + co] : 0.f;
+  }
+  const bool     producer = warp == kFEpiWarps;
+  const uint32_t bar_mma  = smem_u32(&bars[0]);           // + 8c
+  const uint32_t bar_epi  = smem_u32(&bars[kFTiles]);     // + 8c
+  const uint32_t bar_w    = smem_u32(&bars[2 * kFTiles]); // + 8b
+  const uint32_t wbuf0    = smem_u32(smem + kFOffW);
+  const uint32_t act0     = smem_u32(smem);
+  if (warp == 0) {
+    tmem_alloc(smem_u32(tmem_sm), kFCols);
+  }
+  if (producer && lane == 0) {
+    for (int c = 0; c < kFTiles; ++c) {
+      mbar_init(bar_mma + 8u * c, 1);
+      mbar_init(bar_epi + 8u * c, 8);
+    }
+    mbar_init(bar_w, 1);
+    mbar_init(bar_w + 8u, 1);
+    *abort_sm = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fused_load_weights(wf, 0, wbuf0, bar_w);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_sm;
+  // Epilogue role: tile mc, lane quarter q, channel half hh; window row r.
+  const int      mc   = warp / 8;
+  const int      q    = warp & 3;
+  const int      hh   = (warp >> 2) & 1;
+  const int      r    = mc * 128 + q * 32 + lane;
+  const uint32_t tad  = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(mc * 64 + hh * 32);
+  uint32_t       step = 0;     // layer steps of this CTA (all roles count alike)
+  uint32_t       w_issued = 1; // producer: weight loads issued (load k went to buffer k & 1)
+  uint32_t       mma_issued = 0; // producer: layer steps whose MMAs were issued
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int base = tile * kFOut - kFMargin; // global row of window row 0
+    for (int i = tid; i < 2 * kFRows; i += kFThreads) {
+      const int c = i / kFRows, rr = i - c * kFRows, g = base - kFPad + rr;
+      xs[i]       = (g >= 0 && g < R) ? x[(size_t)c * R + g] : make_uint4(0, 0, 0, 0);
+    }
+    for (int i = tid; i < kFWin; i += kFThreads) {
+      const int g = base + i;
+      valid_s[i]  = (g >= 0 && g < R) ? row_valid[g] : 0;
+    }
+    fence_async_shared();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (*abort_sm != 0) {
+      break;
+    }
+    if (producer) {
+      if (lane == 0) {
+        for (int l = 0; l < kLayers; ++l) {
+          const uint32_t s   = step + (uint32_t)l;
+          const uint32_t src = l == 0 ? smem_u32(xs) : act0 + ((l & 1) ? 0u : kFActB);
+          if (!fused_wait(bar_w + 8u * (s & 1), (s >> 1) & 1u, abort_sm, err)) {
+            break;
+          }
+          const uint32_t wb = wbuf0 + (s & 1) * kFWB;
+          // Layer 0 follows the window barrier; later layers wait for the epilogues of layer l - 1
+          // that tile c depends on (each barrier phase waited once: tiles 0 and 1 before tile 0,
+          // tile 2 before tile 1).
+          bool ok = true;
+          for (int c = 0; c < kFTiles && ok; ++c) {
+            if (l > 0) {
+              for (int d = (c == 0 ? 0 : c + 1); d <= min(c + 1, kFTiles - 1) && ok; ++d) {
+                ok = fused_wait(bar_epi + 8u * d, (s - 1) & 1u, abort_sm, err);
+              }
+              tc_fence_after();
+            }
+            if (!ok) {
+              break;
+            }
+            if (l == 0) {
+              fused_issue_tile<kInCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
+            } else if (l == kLayers - 1) {
+              fused_issue_tile<kCh, kOutCh>(c, src, wb, tmem, bar_mma + 8u * c);
+            } else {
+              fused_issue_tile<kCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
+            }
+          }
+          if (!ok) {
+            break;
+          }
+          mma_issued = s + 1;
+          // Every MMA of layer l - 1 has completed (its epilogues have arrived), so its weight
+          // buffer takes the next layer (layer 0 of the next window after the last layer).
+          if (l + 1 < kLayers || tile + (int)gridDim.x < ntiles) {
+            fused_load_weights(wf, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
+            ++w_issued;
+          }
+        }
+      }
+      __syncwarp();
+    } else {
+      const bool valid = valid_s[r] != 0;
+      for (int l = 0; l < kLayers; ++l) {
+        const uint32_t s  = step + (uint32_t)l;
+        const bool     ok = fused_wait(bar_mma + 8u * mc, s & 1u, abort_sm, err);
+        __syncwarp();
+        if (ok) {
+          tc_fence_after();
+          const float* bl = bias_s + l * kCh + hh * 32;
+          if (l < kLayers - 1) {
+            // 32 output channels (chunks 4 hh .. 4 hh + 3) of row r: one TMEM load, the residual
+            // and bias loads issued together, then straight-line arithmetic.
+            const bool     second = l >= 2 && (l & 1) == 0;
+            unsigned char* dst    = smem + ((l == 0 || second) ? 0u : kFActB);
+            uint4*         p      = reinterpret_cast<uint4*>(dst + (hh * 4) * kFChunkB) + (r + kFPad);
+            constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk column
+            uint4          res[4];
+            if (second) {
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                res[k] = p[k * kStep];
+              }
+            }
+            float v[32];
+            tmem_ld32(tad, v);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const float4 b0 = reinterpret_cast<const float4*>(bl)[2 * k];
+              const float4 b1 = reinterpret_cast<const float4*>(bl)[2 * k + 1];
+              const float  bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+              float        o[8];
+#pragma unroll
+              for (int j = 0; j < 8; ++j) {
+                o[j] = v[8 * k + j] + bb[j];
+              }
+              if (second) {
+                const __nv_bfloat16* rb = reinterpret_cast<const __nv_bfloat16*>(&res[k]);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                  o[j] += __bfloat162float(rb[j]);
+                }
+              }
+              uint4 pk = make_uint4(0, 0, 0, 0);
+              if (valid) {
+                pk = make_uint4(pack_bf16x2(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f)),
+                                pack_bf16x2(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f)),
+                                pack_bf16x2(fmaxf(o[4], 0.f), fmaxf(o[5], 0.f)),
+                                pack_bf16x2(fmaxf(o[6], 0.f), fmaxf(o[7], 0.f)));
+              }
+              p[k * kStep] = pk;
+            }
+            fence_async_shared();
+          } else if (hh == 0) {
+            float v[16];
+            tmem_ld16(tad, v);
+            const int g = base + r;
+            if (r >= kFMargin && r < kFMargin + kFOut && g < R) {
+#pragma unroll
+              for (int h = 0; h < 2; ++h) {
+                uint4 pk = make_uint4(0, 0, 0, 0);
+                if (valid) {
+                  const float* b8 = bl + 8 * h;
+                  const float* v8 = v + 8 * h;
+                  pk = make_uint4(pack_bf16x2(v8[0] + b8[0], v8[1] + b8[1]), pack_bf16x2(v8[2] + b8[2], v8[3] + b8[3]),
+                                  pack_bf16x2(v8[4] + b8[4], v8[5] + b8[5]), pack_bf16x2(v8[6] + b8[6], v8[7] + b8[7]));
+                }
+                y[(size_t)h * R + g] = pk;
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(bar_epi + 8u * mc);
+        }
+      }
+    }
+    step += kLayers;
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (*abort_sm != 0) {
+      break;
+    }
+  }
+  // After a failure: the producer waits (bounded) for the MMAs and weight loads it issued, so that
+  // nothing asynchronous is in flight when the tensor memory and shared memory go away.
+  if (producer && lane == 0 && *abort_sm != 0) {
+    if (mma_issued > 0) {
+      for (int c = 0; c < kFTiles; ++c) {
+        (void)mbar_wait_bounded(bar_mma + 8u * c, (mma_issued - 1) & 1u);
+      }
+    }
+    for (uint32_t k = mma_issued; k < w_issued; ++k) {
+      (void)mbar_wait_bounded(bar_w + 8u * (k & 1), (k >> 1) & 1u);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tmem_dealloc(tmem, kFCols);
+  }
+}
+
+int fused_forward(pg_le_net* net, int R, cudaStream_t s);
+
 
 int check_err_status(pg_le_net* net)
 {
@@ -338,6 +669,19 @@ int forward(pg_le_net* net, int R, cudaStream_t s)
                                  nullptr, net->y, net->row_valid, R, 0, net->err, s);
   }
   return rc;
+}
+
+int fused_forward(pg_le_net* net, int R, cudaStream_t s)
+{
+  if (R <= 0) {
+    return PG_OK;
+  }
+  const int ntiles = (R + kFOut - 1) / kFOut;
+  const int grid   = std::max(1, std::min(ntiles, net->ctx->sm_count));
+  le_fused_forward_kernel<<<grid, kFThreads, kFSmem, s>>>(reinterpret_cast<const uint4*>(net->x), net->row_valid,
+                                                          net->wf, net->params, R, reinterpret_cast<uint4*>(net->y),
+                                                          net->err);
+  return pg::check_cuda(net->ctx, cudaGetLastError(), "le_fused_forward_kernel launch");
 }
 
 // Gradients of every parameter (added to net->grads) from net->dy and the activations of the last
@@ -452,7 +796,7 @@ int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, co
                                                      reinterpret_cast<uint4*>(net->x), net->row_valid, net->gseq);
   int rc = check_cuda(net->ctx, cudaGetLastError(), "le_features_kernel launch");
   if (rc == PG_OK) {
-    rc = forward(net, R, s);
+    rc = fused_forward(net, R, s);
   }
   if (rc == PG_OK) {
     le_apply_kernel<<<(R + 255) / 256, 256, 0, s>>>(seqs_dev, nseq, R, reinterpret_cast<const uint4*>(net->y),
@@ -536,6 +880,12 @@ int pg_le_create(pg_context* ctx, int max_rows, pg_le_net** out)
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemset(n->dev, 0, off), "cudaMemset(learned estimator)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaFuncSetAttribute(le_fused_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kFSmem),
+                    "cudaFuncSetAttribute(le_fused_forward_kernel)");
   }
   if (rc == PG_OK) {
     layer_desc ld[kLayers];

@@ -19,137 +19,18 @@
 // Every wait on an mbarrier has an iteration limit; on expiry the kernel records an error code,
 // skips its epilogue, frees its tensor memory and returns.
 #include "pg_internal.h"
+#include "tc_common.cuh"
 
 #include <cuda_bf16.h>
 
 namespace {
 
-constexpr int      kTapCount     = 5;
-constexpr int      kTileRows     = 128;
-constexpr int      kHaloRows     = kTileRows + kTapCount - 1; // 132
-constexpr int      kConvThreads  = 128;
-constexpr uint32_t kWaitLimit    = 1u << 22;
+using namespace pg::tc;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p)
-{
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor, no swizzle (bits: start >> 4 [0,14), LBO >> 4 [16,30),
-// SBO >> 4 [32,46), version 1 [46,48), layout type 0 [61,64)).
-__device__ __forceinline__ uint64_t make_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3fffu);
-  d |= (uint64_t)((lbo >> 4) & 0x3fffu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3fffu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
-
-// Instruction descriptor of kind::f16: D f32, A and B bf16, majors, N >> 3 at bit 17, M >> 4 at 24.
-__host__ __device__ constexpr uint32_t make_idesc(int m, int n, bool a_mn_major, bool b_mn_major)
-{
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn_major ? 1u : 0u) << 15) | ((b_mn_major ? 1u : 0u) << 16) |
-         ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
-                                         uint32_t accumulate)
-{
-  asm volatile(
-      "{\n\t"
-      ".reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t"
-      "}\n" ::"r"(tmem_d),
-      "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar)
-{
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t mbar, uint32_t count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity)
-{
-  uint32_t ok;
-  asm volatile(
-      "{\n\t"
-      ".reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t"
-      "}\n"
-      : "=r"(ok)
-      : "r"(mbar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: true when the phase completed, false when the limit expired.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity)
-{
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
-    if (mbar_try_wait(mbar, parity)) {
-      return true;
-    }
-  }
-  return false;
-}
-
-__device__ __forceinline__ void fence_async_shared()
-{
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before()
-{
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_fence_after()
-{
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols)
-{
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols));
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
-{
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
-}
-
-// 16 consecutive FP32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
-{
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    v[i] = __uint_as_float(r[i]);
-  }
-}
-
-template <int N>
-__host__ __device__ constexpr uint32_t tmem_cols()
-{
-  return N <= 32 ? 32u : (N <= 64 ? 64u : (N <= 128 ? 128u : 256u));
-}
+constexpr int kTapCount    = 5;
+constexpr int kTileRows    = 128;
+constexpr int kHaloRows    = kTileRows + kTapCount - 1; // 132
+constexpr int kConvThreads = 128;
 
 // True for the bf16 values of the 8 lanes of v that are > 0 (ReLU outputs: +0 or positive).
 __device__ __forceinline__ void positive_mask(const uint4 v, bool* m)

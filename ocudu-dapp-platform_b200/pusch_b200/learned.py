@@ -408,9 +408,38 @@ def main(argv=None):
     e.add_argument("--cells", type=int, default=4)
     e.add_argument("--seed", type=int, default=100)
     e.add_argument("--json", default=None)
+    tm = sub.add_parser("time", help="time pg_le_refine_device on a batch of the training source")
+    tm.add_argument("--rows", type=int, default=270_000)
+    tm.add_argument("--reps", type=int, default=10)
     a = ap.parse_args(argv)
     ctx = _native.Context(0, 1024)
-    if a.cmd == "train":
+    if a.cmd == "time":
+        import torch
+        src = DmrsTrainingSource(5)
+        descs, grid, _, est_size, _ = src.batch(a.rows)
+        n = len(descs)
+        est = torch.empty(2 * est_size, dtype=torch.float32, device="cuda")
+        ls = torch.empty_like(est)
+        pr = torch.empty((4 * n, 5), dtype=torch.float32, device="cuda")
+        ctx.check(ctx.lib.pg_pusch_estimate_ls_device(ctx.handle, ctypes.addressof(descs), n, grid.data_ptr(),
+                                                      est.data_ptr(), ls.data_ptr(), pr.data_ptr(), None))
+        rows = int(ctx.lib.pg_le_rows(ctypes.addressof(descs), n))
+        net = LearnedEstimator(ctx, max_rows=rows, params=load_params())
+        for _ in range(3):
+            net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.reps):
+            net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
+        e1.record()
+        torch.cuda.synchronize()
+        net.status()
+        ms = e0.elapsed_time(e1) / a.reps
+        flops = rows * 2 * TAPS * sum(ci * co for ci, co in LAYERS)
+        print(f"rows {rows} refine {ms:.4f} ms {flops / (ms * 1e-3) / 1e12:.1f} TFLOP/s", flush=True)
+        net.close()
+    elif a.cmd == "train":
         t0 = time.time()
         net, hist = train(ctx, steps=a.steps, rows_per_step=a.rows, seed=a.seed, lr=a.lr, time_budget_s=a.time_budget)
         ues_seen = hist[-1][0] * a.rows / (4 * 1.5 * 12 * 92)
