@@ -5,20 +5,22 @@ Default workload (one "step"): the batched uneven slot - 16 cells of 100 MHz / 2
 1-16 UEs on contiguous PRB allocations, QPSK-256QAM (MCS table 2), 1-2 layers, 4 rx ports,
 per-UE SNR U[0, 30] dB with link adaptation to BLER <= 10 %, DM-RS type 1 at symbols 2 and 11,
 exponential-PDP channels (100 ns RMS, 8 taps), max 6 LDPC iterations - decoded through one slot
-plan (DM-RS estimation, demodulation, rate dematching, LDPC, TB assembly and CRC; one CUDA graph
-replayed per step). The metric is decoded Mbit/s: the TBS of every UE whose TB CRC passes (and
-equals the transmitted bits), per second of device time, inputs resident in HBM, L2 flushed
-between steps.
+plan: DM-RS estimation, the learned channel estimator's refinement (committed parameters),
+demodulation, rate dematching, LDPC, TB assembly and CRC; one CUDA graph replayed per step, launch
+shapes picked by the plan's autotuner. The metric is decoded Mbit/s: the TBS of every UE whose TB
+CRC passes (and equals the transmitted bits), per second of device time, inputs resident in HBM,
+L2 flushed between steps.
 
-The line also carries: the plain per-UE GPU path on the same slot (one plan per UE, executed one
-after another with the host waiting for each UE's result); the end-to-end value through the host
-entry (pg_pusch_plan_execute_host: pinned host grids in, TBs and results out, every step); the
-integer roofline of the dominant kernel (ldpc_decode_kernel, CUDA-event time inside the step);
-the LDPC decoder batch (512 codeblocks, BG1/BG2 Z=384) in Gbit/s; clocks sampled during the timed
-region; and the reference's CPU receive path (oracle/_ref, the reference's own stage objects) on
-this host's cores as cpu_baseline.
+The line also carries: the same plan with the plain estimator (batched_plain); the plain per-UE
+GPU path on the same slot (one plan per UE, executed one after another with the host waiting for
+each UE's result); the end-to-end value through the host entry (pg_pusch_plan_execute_host: pinned
+host grids in, TBs and results out, every step); the rooflines of the learned estimator's network
+(tensor cores) and of ldpc_decode_kernel (integer pipe), both timed with CUDA events inside the
+step; the LDPC decoder batch (512 codeblocks, BG1/BG2 Z=384) in Gbit/s; clocks sampled during the
+timed region; and the reference's CPU receive path (oracle/_ref, the reference's own stage objects)
+on this host's cores as cpu_baseline.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload uneven|ldpc]
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload uneven|ldpc] [--no-learned]
 
 ``--impl reference`` times the reference's CPU receive path on all host cores on the same
 workload. Under torchrun each rank decodes its own slot (seed + rank): weak scaling, no data-path
@@ -333,6 +335,12 @@ def run_ours_pusch(args):
         clk = clocks.stop() if clocks is not None else None
         return [a.elapsed_time(b) for a, b in evs], k_ms, l_ms, clk
 
+    # Launch shapes picked by the autotuner on this slot (with the estimator that is timed next).
+    if net is not None:
+        plan.set_learned(net)
+    tuning, _ = plan.autotune(d_grid.data_ptr(), reps=5)
+    if net is not None:
+        plan.set_learned(None)
     ctx.lib.pg_set_kernel_timing(ctx.handle, 1)
     # Batched path with the plain estimator (the comparison point of the learned one).
     batched_plain = None
@@ -492,7 +500,7 @@ def run_ours_pusch(args):
                        "codeblocks_per_rank": int(plan.info.nof_codeblocks), "tb_bits_per_rank": bits_all,
                        "decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
                        "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
-                       "parallelism": f"replicas{world}",
+                       "parallelism": f"replicas{world}", "launch_shapes": tuning.as_dict(),
                        "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
                                      "plain LS + RC FIR + linear interpolation" if net is not None else
                                      "plain (LS + RC FIR + linear interpolation)")},

@@ -400,6 +400,26 @@ int  pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info);
  * than the legacy default stream only; on the default stream the launches are enqueued directly. */
 int pg_pusch_plan_set_graph(pg_pusch_plan* plan, int enabled);
 
+/* Launch shapes of a plan's stages (the autotuner's search space). No counterpart in the
+ * reference, whose stages are sized per UE and per codeblock by its thread pools. */
+typedef struct pg_pusch_plan_tuning {
+  int rm_ctas_per_cb;       /* rate dematching: CTAs per codeblock, 1..32 (default 8) */
+  int demod_res_per_thread; /* demodulation: resource elements per thread, 1..8 (default 1) */
+  int demod_block;          /* demodulation: threads per CTA, 64, 128 or 256 (default 256) */
+  int ldpc_ctas_per_sm;     /* persistent LDPC decoder: CTAs per SM, 1 or 2 (default 2) */
+} pg_pusch_plan_tuning;
+
+int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out);
+/* Sets the shapes (validated); a captured graph is re-captured on the next execution. */
+int pg_pusch_plan_set_tuning(pg_pusch_plan* plan, const pg_pusch_plan_tuning* tuning);
+
+/* Autotuner: times whole-slot executions of the plan on `grids` (device) for candidate shapes of
+ * each stage (coordinate descent, two passes; each candidate the minimum of `reps` executions
+ * timed by CUDA events on the context's stream), keeps the fastest and returns it (best and
+ * best_ms may be NULL). Results do not depend on the shapes. Synchronises. */
+int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps, pg_pusch_plan_tuning* best,
+                           float* best_ms);
+
 /* Enqueues the slot on stream: grids (device, grid_words cbf16 words) -> tb_out (device,
  * tb_bytes; the assembled TB of every UE, valid where results[u].tb_crc_ok), results (device,
  * one pg_sch_result per UE) and port_results (device, nof_ues * 4 entries, or NULL). */

@@ -573,6 +573,13 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
                            cudaStream_t stream)
 {
+  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, counter, stream, ctx->ldpc_ctas);
+}
+
+int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                           int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
+                           cudaStream_t stream, int max_ctas)
+{
   if (n == 0) {
     return PG_OK;
   }
@@ -583,7 +590,7 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  const int grid = std::min(n, ctx->ldpc_ctas);
+  const int grid = std::max(1, std::min(n, std::min(max_ctas, ctx->ldpc_ctas)));
   ldpc_decode_kernel<<<grid, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, order, n,
                                                     counter);
   if (ctx->timed) {

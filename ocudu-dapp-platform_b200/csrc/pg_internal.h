@@ -119,6 +119,9 @@ int ensure_scratch(pg_context* ctx, void** buf, size_t* cap, size_t bytes, const
 int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_total, size_t out_total);
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
                         cudaStream_t stream);
+// Same with ctas_per_cb CTAs per codeblock (1..32).
+int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
+                        cudaStream_t stream, int ctas_per_cb);
 void crc_tables_host(uint32_t* tab);
 int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8_t* data, uint32_t* out,
                cudaStream_t stream);
@@ -155,6 +158,11 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s);
+// Same with `block` threads per CTA (64, 128 or 256) and res_per_thread REs per thread (1..8).
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
+                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                      const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
+                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread);
 // Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
 // uses scratch_b; results and TB payloads land in host memory.
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
@@ -180,6 +188,10 @@ int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, con
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
                            cudaStream_t stream);
+// Same with at most max_ctas CTAs.
+int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                           int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
+                           cudaStream_t stream, int max_ctas);
 // CTAs of ldpc_decode_kernel resident on the whole device.
 int ldpc_resident_ctas(pg_context* ctx);
 

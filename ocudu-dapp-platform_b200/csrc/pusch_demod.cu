@@ -289,30 +289,13 @@ __device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const u
 // One thread per data resource element of the whole batch: re_off[u] .. re_off[u + 1] are the
 // data REs of UE u (data symbols x 12 nof_rb, symbol-major), so every CTA works on one or two
 // UEs and small UEs take no more threads than they have REs.
-__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, int nof_ues,
-                                                          const uint32_t* __restrict__ re_off,
-                                                          const uint32_t* __restrict__ grids,
-                                                          const float2* __restrict__ est_all,
-                                                          const pg_port_result* __restrict__ port_results,
-                                                          const uint32_t* __restrict__ seq_offsets,
-                                                          const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs)
+__device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_ue* __restrict__ ues, int nof_ues,
+                                             const uint32_t* __restrict__ re_off, const uint32_t* __restrict__ grids,
+                                             const float2* __restrict__ est_all,
+                                             const pg_port_result* __restrict__ port_results,
+                                             const uint32_t* __restrict__ seq_offsets, const uint32_t* __restrict__ seq,
+                                             int8_t* __restrict__ llrs, const demap_tables& tb)
 {
-  __shared__ float s_slope[3 * 4 * 16];
-  __shared__ float s_icpt[3 * 4 * 16];
-  __shared__ float s_width[3];
-  for (int i = threadIdx.x; i < 3 * 4 * 16; i += blockDim.x) {
-    s_slope[i] = (&c_slope_d[0][0][0])[i];
-    s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
-  }
-  if (threadIdx.x < 3) {
-    s_width[threadIdx.x] = c_width_d[threadIdx.x];
-  }
-  __syncthreads();
-  const demap_tables tb = {s_slope, s_icpt, s_width};
-  const uint32_t     rg = blockIdx.x * blockDim.x + threadIdx.x;
-  if (rg >= __ldg(re_off + nof_ues)) {
-    return;
-  }
   // UE of this RE: the last u with re_off[u] <= rg.
   int lo = 0, hi = nof_ues - 1;
   while (lo < hi) {
@@ -369,6 +352,39 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
   }
 }
 
+// res_per_thread consecutive blocks of blockDim.x REs per CTA (a launch-shape tunable).
+__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, int nof_ues,
+                                                          const uint32_t* __restrict__ re_off,
+                                                          const uint32_t* __restrict__ grids,
+                                                          const float2* __restrict__ est_all,
+                                                          const pg_port_result* __restrict__ port_results,
+                                                          const uint32_t* __restrict__ seq_offsets,
+                                                          const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs,
+                                                          int res_per_thread)
+{
+  __shared__ float s_slope[3 * 4 * 16];
+  __shared__ float s_icpt[3 * 4 * 16];
+  __shared__ float s_width[3];
+  for (int i = threadIdx.x; i < 3 * 4 * 16; i += blockDim.x) {
+    s_slope[i] = (&c_slope_d[0][0][0])[i];
+    s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
+  }
+  if (threadIdx.x < 3) {
+    s_width[threadIdx.x] = c_width_d[threadIdx.x];
+  }
+  __syncthreads();
+  const demap_tables tb    = {s_slope, s_icpt, s_width};
+  const uint32_t     total = __ldg(re_off + nof_ues);
+  const uint32_t     base  = blockIdx.x * blockDim.x * (uint32_t)res_per_thread + threadIdx.x;
+  for (int k = 0; k < res_per_thread; ++k) {
+    const uint32_t rg = base + (uint32_t)k * blockDim.x;
+    if (rg >= total) {
+      break;
+    }
+    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, port_results, seq_offsets, seq, llrs, tb);
+  }
+}
+
 } // namespace
 
 namespace pg {
@@ -410,12 +426,26 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s)
 {
+  return demod_only_launch(ctx, ues_dev, n, total_re, re_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
+                           llrs, s, 256, 1);
+}
+
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
+                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+                      const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
+                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread)
+{
   if (n == 0 || total_re == 0) {
     return PG_OK;
   }
-  pusch_demod_kernel<<<(total_re + 255) / 256, 256, 0, s>>>(ues_dev, n, re_off_dev, grids,
-                                                             reinterpret_cast<const float2*>(est), port_results,
-                                                             seq_offsets_dev, seq_dev, llrs);
+  if (block != 64 && block != 128 && block != 256) {
+    block = 256;
+  }
+  res_per_thread       = std::max(1, std::min(8, res_per_thread));
+  const uint32_t per   = (uint32_t)block * (uint32_t)res_per_thread;
+  pusch_demod_kernel<<<(total_re + per - 1) / per, block, 0, s>>>(ues_dev, n, re_off_dev, grids,
+                                                                  reinterpret_cast<const float2*>(est), port_results,
+                                                                  seq_offsets_dev, seq_dev, llrs, res_per_thread);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 

@@ -58,6 +58,8 @@ struct pg_pusch_plan {
   le_seq*         d_le_seqs = nullptr;
   int             le_nseq   = 0;
   int             le_rows   = 0;
+  // Launch shapes (defaults, or the autotuner's choice).
+  pg_pusch_plan_tuning tuning = {8, 1, 256, 2};
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -121,14 +123,14 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
   }
   if (rc == PG_OK) {
     rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
-                           p->d_seq_off, p->d_seq, p->d_llr, s);
+                           p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread);
   }
   if (rc == PG_OK) {
-    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s);
+    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb);
   }
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
-                                p->d_order, p->d_counter, s);
+                                p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count);
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
@@ -414,6 +416,154 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
   plan->le_nseq   = (int)seqs.size();
   plan->le_rows   = (int)rows;
   plan->le_net    = net;
+  return PG_OK;
+}
+
+static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
+{
+  return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
+         t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
+         t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm * ctx->sm_count <= ctx->ldpc_ctas;
+}
+
+int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
+{
+  if (plan == nullptr || out == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  *out = plan->tuning;
+  return PG_OK;
+}
+
+int pg_pusch_plan_set_tuning(pg_pusch_plan* plan, const pg_pusch_plan_tuning* t)
+{
+  if (plan == nullptr || t == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (!tuning_valid(*t, plan->ctx)) {
+    return set_error(plan->ctx, PG_ERR_INVALID, "launch shapes out of range");
+  }
+  if (int rc = check_cuda(plan->ctx, cudaStreamSynchronize(plan->ctx->stream), "cudaStreamSynchronize")) {
+    return rc;
+  }
+  plan->tuning = *t;
+  if (plan->exec != nullptr) {
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  return PG_OK;
+}
+
+// Device time of `reps` executions (enqueued directly, no graph) with the plan's current shapes:
+// the minimum over the repetitions, after one untimed execution.
+static int time_plan(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb, pg_sch_result* res, int reps, float* best)
+{
+  pg_context*  ctx = p->ctx;
+  cudaStream_t s   = ctx->stream;
+  cudaEvent_t  a = nullptr, b = nullptr;
+  int          rc = check_cuda(ctx, cudaEventCreate(&a), "cudaEventCreate");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventCreate(&b), "cudaEventCreate");
+  }
+  const bool timed = ctx->timed;
+  ctx->timed       = false;
+  *best            = 1e30f;
+  for (int r = -1; r < reps && rc == PG_OK; ++r) {
+    rc = check_cuda(ctx, cudaEventRecord(a, s), "cudaEventRecord");
+    if (rc == PG_OK) {
+      rc = enqueue(p, grids, tb, res, p->d_pr, s);
+    }
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx, cudaEventRecord(b, s), "cudaEventRecord");
+    }
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx, cudaEventSynchronize(b), "cudaEventSynchronize");
+    }
+    float ms = 0.f;
+    if (rc == PG_OK && r >= 0 && cudaEventElapsedTime(&ms, a, b) == cudaSuccess) {
+      *best = std::min(*best, ms);
+    }
+  }
+  ctx->timed = timed;
+  if (a) {
+    cudaEventDestroy(a);
+  }
+  if (b) {
+    cudaEventDestroy(b);
+  }
+  return rc;
+}
+
+int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps, pg_pusch_plan_tuning* best_out,
+                           float* best_ms)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (grids == nullptr || reps < 1) {
+    return set_error(ctx, PG_ERR_INVALID, "autotune: null grids or no repetitions");
+  }
+  // Candidate shapes per stage; coordinate descent over the stages, two passes, each candidate
+  // timed on the plan's own slot (the outputs land in the plan's execute_host buffers).
+  static const int rm_c[]    = {2, 4, 8, 16, 32};
+  static const int res_c[]   = {1, 2, 4};
+  static const int blk_c[]   = {64, 128, 256};
+  static const int ldpc_c[]  = {1, 2};
+  pg_pusch_plan_tuning cur   = plan->tuning;
+  float                cur_ms = 0.f;
+  int rc = time_plan(plan, grids, plan->d_tb_out, plan->d_res, reps, &cur_ms);
+  auto try_set = [&](pg_pusch_plan_tuning cand) -> int {
+    if (!tuning_valid(cand, ctx)) {
+      return PG_OK;
+    }
+    const pg_pusch_plan_tuning keep = plan->tuning;
+    plan->tuning                    = cand;
+    float ms                        = 0.f;
+    const int r                     = time_plan(plan, grids, plan->d_tb_out, plan->d_res, reps, &ms);
+    if (r == PG_OK && ms < cur_ms) {
+      cur_ms = ms;
+      cur    = cand;
+    }
+    plan->tuning = keep;
+    return r;
+  };
+  for (int pass = 0; pass < 2 && rc == PG_OK; ++pass) {
+    for (int v : rm_c) {
+      pg_pusch_plan_tuning c = cur;
+      c.rm_ctas_per_cb       = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+    for (int v : res_c) {
+      pg_pusch_plan_tuning c = cur;
+      c.demod_res_per_thread = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+    for (int v : blk_c) {
+      pg_pusch_plan_tuning c = cur;
+      c.demod_block          = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+    for (int v : ldpc_c) {
+      pg_pusch_plan_tuning c = cur;
+      c.ldpc_ctas_per_sm     = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+  }
+  if (rc != PG_OK) {
+    return rc;
+  }
+  plan->tuning = cur;
+  if (plan->exec != nullptr) {
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  if (best_out != nullptr) {
+    *best_out = cur;
+  }
+  if (best_ms != nullptr) {
+    *best_ms = cur_ms;
+  }
   return PG_OK;
 }
 

@@ -13,6 +13,8 @@
 // the N output positions (coalesced stores).
 #include "pg_internal.h"
 
+#include <algorithm>
+
 namespace {
 
 constexpr int kRmThreads = 256;
@@ -144,11 +146,18 @@ int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_tot
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
                         cudaStream_t stream)
 {
+  return rate_dematch_launch(ctx, descs_dev, n, in, out, stream, kRmGridY);
+}
+
+int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
+                        cudaStream_t stream, int ctas_per_cb)
+{
   if (n == 0) {
     return PG_OK;
   }
-  // Each codeblock's N <= 25,344 output positions spread over kRmGridY CTAs.
-  rate_dematch_kernel<<<dim3(n, kRmGridY), kRmThreads, 0, stream>>>(descs_dev, in, out);
+  // Each codeblock's N <= 25,344 output positions spread over ctas_per_cb CTAs.
+  ctas_per_cb = std::max(1, std::min(32, ctas_per_cb));
+  rate_dematch_kernel<<<dim3(n, ctas_per_cb), kRmThreads, 0, stream>>>(descs_dev, in, out);
   return check_cuda(ctx, cudaGetLastError(), "rate_dematch_kernel launch");
 }
 

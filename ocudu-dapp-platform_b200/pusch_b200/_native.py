@@ -77,6 +77,14 @@ class PgLeAdam(ctypes.Structure):
                 ("weight_decay", ctypes.c_float)]
 
 
+class PgPuschPlanTuning(ctypes.Structure):
+    _fields_ = [("rm_ctas_per_cb", ctypes.c_int), ("demod_res_per_thread", ctypes.c_int),
+                ("demod_block", ctypes.c_int), ("ldpc_ctas_per_sm", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class PgPuschPlanInfo(ctypes.Structure):
     _fields_ = [("nof_ues", ctypes.c_uint32), ("nof_codeblocks", ctypes.c_uint32), ("tb_bytes", ctypes.c_uint64),
                 ("nof_llrs", ctypes.c_uint64), ("grid_words", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
@@ -147,6 +155,9 @@ SIGNATURES = {
     "pg_le_train_step_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_estimate_ls_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),
+    "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),
+    "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
+    "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
 }
 
 _lib = None

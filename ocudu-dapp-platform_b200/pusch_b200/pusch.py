@@ -153,6 +153,22 @@ class PuschSlotPlan:
         u = None if use is None else (ctypes.c_uint8 * self.n)(*[int(bool(v)) for v in use])
         self.ctx.check(self.lib.pg_pusch_plan_set_learned(self.handle, net.handle if net is not None else None, u))
 
+    def tuning(self):
+        t = _native.PgPuschPlanTuning()
+        self.ctx.check(self.lib.pg_pusch_plan_get_tuning(self.handle, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, t):
+        self.ctx.check(self.lib.pg_pusch_plan_set_tuning(self.handle, ctypes.byref(t)))
+
+    def autotune(self, grid_ptr, reps=5):
+        """Picks the fastest launch shapes for this plan's slot (pg_pusch_plan_autotune); returns
+        (PgPuschPlanTuning, best ms)."""
+        t = _native.PgPuschPlanTuning()
+        ms = ctypes.c_float()
+        self.ctx.check(self.lib.pg_pusch_plan_autotune(self.handle, grid_ptr, reps, ctypes.byref(t), ctypes.byref(ms)))
+        return t, ms.value
+
     def le_rows(self, use=None):
         """Rows a LearnedEstimator needs for this plan."""
         if use is None:

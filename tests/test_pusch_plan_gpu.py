@@ -88,3 +88,28 @@ def test_uneven_slot_bler(ctx):
     print("UEs", plan.n, "codeblocks", plan.info.nof_codeblocks, "BLER", 1 - ok / plan.n)
     assert ok >= 0.9 * plan.n
     plan.close()
+
+
+def test_autotuner_keeps_results(ctx):
+    """pg_pusch_plan_autotune picks valid launch shapes; every shape decodes to the same results."""
+    import torch
+    from pusch_b200._native import PgPuschPlanTuning
+    slots = sim.uneven_cells(seed=21, nof_cells=2)
+    plan = PuschSlotPlan(ctx, slots, max_iterations=6, graph=True)
+    ref = plan.execute_host()
+    d_grid = torch.from_numpy(plan.grid.view(np.int32)).cuda()
+    best, ms = plan.autotune(d_grid.data_ptr(), reps=3)
+    assert ms > 0
+    assert 1 <= best.rm_ctas_per_cb <= 32 and 1 <= best.demod_res_per_thread <= 8
+    assert best.demod_block in (64, 128, 256) and best.ldpc_ctas_per_sm in (1, 2)
+    assert plan.tuning().as_dict() == best.as_dict()
+    for shape in (best, PgPuschPlanTuning(3, 3, 64, 1), PgPuschPlanTuning(32, 8, 128, 2)):
+        plan.set_tuning(shape)
+        got = plan.execute_host()
+        for g, r in zip(got, ref):
+            assert g.tb_crc_ok == r.tb_crc_ok and g.mean_iterations == r.mean_iterations
+            if r.tb_crc_ok:
+                assert np.array_equal(g.transport_block, r.transport_block)
+    with pytest.raises(Exception):
+        plan.set_tuning(PgPuschPlanTuning(0, 1, 256, 2))
+    plan.close()
