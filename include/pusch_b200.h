@@ -406,7 +406,11 @@ typedef struct pg_pusch_plan_tuning {
   int rm_ctas_per_cb;       /* rate dematching: CTAs per codeblock, 1..32 (default 8) */
   int demod_res_per_thread; /* demodulation: resource elements per thread, 1..8 (default 1) */
   int demod_block;          /* demodulation: threads per CTA, 64, 128 or 256 (default 256) */
-  int ldpc_ctas_per_sm;     /* persistent LDPC decoder: CTAs per SM, 1 or 2 (default 2) */
+  int ldpc_ctas_per_sm;     /* persistent LDPC decoders: CTAs per SM, 1..4 (default 2; the one-lane-per-
+                               thread decoder holds at most 2) */
+  int ldpc_z384_two_lanes;  /* 1: Z = 384 codeblocks on the two-lanes-per-thread decoder (a lifting-size
+                               specialisation), 0: every codeblock on the one-lane-per-thread decoder
+                               (default 0) */
 } pg_pusch_plan_tuning;
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out);

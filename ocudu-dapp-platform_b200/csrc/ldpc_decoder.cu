@@ -22,6 +22,8 @@
 // K*Z - F significant bits; CRC == 0 stops with iterations = it + 1.
 #include "pg_internal.h"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -445,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_
                                                               int8_t* __restrict__ c2v_all,
                                                               const uint32_t* __restrict__ crc_pow,
                                                               const uint32_t* __restrict__ order, int n,
-                                                              int* __restrict__ counter)
+                                                              int* __restrict__ counter, int skip_z)
 {
   __shared__ smem_t sm;
   __shared__ int    s_work;
@@ -470,10 +472,414 @@ __global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_
     }
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size == skip_z) {
+      continue; // left to ldpc_decode_x2_kernel
+    }
     if (d.lifting_size == 384) {
       decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
     } else {
       decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Z = 384 decoder with two lifted lanes per thread. Thread j (0 <= j < 192) carries lanes j and
+// j + 192 as the two halves of one f16x2 register. Every value of the decoder is an integer of
+// magnitude at most 1,784 at any intermediate step, so f16 arithmetic (11-bit significand) on them
+// is exact, and the reference's int8 rules become exact f16x2 identities:
+//   v2c      = x == +-127 ? x : clamp(x - c, -120, 120)
+//            = min(max(clamp(x - c, -120, 120), 37x - 4572), 37x + 4572)   (fused multiply-adds;
+//              for |x| <= 120 the bounds lie outside [-120, 120], for x = +-127 they are +-127)
+//   min1/min2/sign: min.xorsign.abs keeps min(|.|) and accumulates the sign product in min1's sign
+//   c2v      = sign(product of the others) * (|v2c| == min1 ? s2 : s1),
+//              magnitude = s2 - (s2 - s1) * min(|v2c| - min1, 1), sign by XOR of sign bits
+//   soft     = |v2c| == 127 ? v2c : promote(c2v + v2c), promote(t) = clamp(8t - 7 clamp(t, +-120), +-127)
+//   scale    s = (m * 52428) >> 16 from a table indexed by the f16 bit pattern of m over 16.
+// Storage is int8 in offset binary (byte = value + 128): f16 bits 0x6400 | byte are 1024 + byte, so
+// one byte permute and one f16x2 subtraction of 1152 give the values, and an addition of 1152 and a
+// byte permute give the bytes back, exactly. Soft bits live twice in shared memory so that the
+// shifted pair of lanes is one 16-bit word: D[col][w] = (soft[col][w], soft[col][(w + 192) mod 384]);
+// check-to-variable messages are byte pairs per (edge, thread) in the global slab.
+constexpr int kX2Z       = 384;
+constexpr int kX2Half    = kX2Z / 2;
+constexpr int kX2Threads = kX2Half;
+constexpr int kScaleTab  = 1408;
+constexpr int kX2MaxPerSm = 4; // resident CTAs per SM (shared memory 55 KB, 80 registers)
+
+struct smem_x2_t {
+  uint16_t D[pg::kMaxNodes * kX2Z];
+  uint32_t edge[pg::kBg1Edges];
+  uint32_t hard[(22 * kX2Z) / 32];
+  uint32_t red[kX2Threads / 32];
+  int      s_last;
+  int      s_done;
+};
+
+__device__ __forceinline__ uint32_t h2_sub(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("sub.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_add(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("add.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_fma(uint32_t a, uint32_t b, uint32_t c)
+{
+  uint32_t r;
+  asm("fma.rn.f16x2 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_mul(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("mul.rn.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_min(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("min.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_max(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("max.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_min_xs(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("min.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+__device__ __forceinline__ uint32_t h2_max_xs(uint32_t a, uint32_t b)
+{
+  uint32_t r;
+  asm("max.xorsign.abs.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+
+// f16x2 constants (both halves equal).
+constexpr uint32_t kH120    = 0x57805780u; // 120
+constexpr uint32_t kHm120   = 0xd780d780u; // -120
+constexpr uint32_t kH127    = 0x57f057f0u; // 127
+constexpr uint32_t kHm127   = 0xd7f0d7f0u; // -127
+constexpr uint32_t kH37     = 0x50a050a0u; // 37
+constexpr uint32_t kHm4572  = 0xec77ec77u; // -4572
+constexpr uint32_t kH4572   = 0x6c776c77u; // 4572
+constexpr uint32_t kH8      = 0x48004800u; // 8
+constexpr uint32_t kHm7     = 0xc700c700u; // -7
+constexpr uint32_t kH1      = 0x3c003c00u; // 1
+constexpr uint32_t kH1152   = 0x64806480u; // 1152 = 1024 + 128
+constexpr uint32_t kAbs     = 0x7fff7fffu;
+constexpr uint32_t kSign    = 0x80008000u;
+
+// Offset-binary byte pair -> f16x2 integers, and back (low byte first).
+__device__ __forceinline__ uint32_t bytes_to_h2(uint32_t b)
+{
+  return h2_sub(__byte_perm(b, 0x6464u, 0x5140), kH1152);
+}
+__device__ __forceinline__ uint32_t h2_to_bytes_biased(uint32_t c)
+{
+  return h2_add(c, kH1152); // bytes 0 and 2 are the offset-binary values
+}
+
+__device__ __forceinline__ uint32_t x2_scale(const uint16_t* __restrict__ tab, uint32_t m)
+{
+  return (uint32_t)__ldg(tab + ((m & 0xffffu) >> 4)) | ((uint32_t)__ldg(tab + (m >> 20)) << 16);
+}
+
+// Partner position of p (same node, w + 192 mod 384).
+__device__ __forceinline__ uint32_t x2_partner(uint32_t p)
+{
+  const uint32_t w = p % kX2Z;
+  return p - w + (w < (uint32_t)kX2Half ? w + kX2Half : w - kX2Half);
+}
+
+template <int DEG, bool FIRST>
+__device__ __forceinline__ void row_update_x2(const int j, uint16_t* __restrict__ D, const uint32_t* __restrict__ edge,
+                                              uint16_t* __restrict__ c2v_row, const uint16_t* __restrict__ tab)
+{
+  uint32_t v[DEG];
+  uint32_t min1 = kH120, min2 = kH120;
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    const uint32_t ed = edge[e];
+    const unsigned p0 = (unsigned)j + (ed & 0xffffu);
+    const unsigned p  = min(p0, p0 - (unsigned)kX2Z) + (ed >> 16);
+    const uint32_t x  = bytes_to_h2(D[p]);
+    uint32_t       vv = x;
+    if (!FIRST) {
+      const uint32_t c = bytes_to_h2(c2v_row[e * kX2Half]);
+      const uint32_t d = h2_min(h2_max(h2_sub(x, c), kHm120), kH120);
+      vv               = h2_min(h2_max(d, h2_fma(x, kH37, kHm4572)), h2_fma(x, kH37, kH4572));
+    }
+    v[e]             = vv;
+    const uint32_t t = h2_max_xs(min1, vv);
+    min2             = h2_min_xs(min2, t);
+    min1             = h2_min_xs(min1, vv);
+  }
+  const uint32_t m1  = min1 & kAbs;
+  const uint32_t s1  = x2_scale(tab, m1);
+  const uint32_t s2  = x2_scale(tab, min2 & kAbs);
+  const uint32_t nds = h2_sub(s1, s2); // -(s2 - s1)
+  const uint32_t sgn = min1 & kSign;  // sign product of every v2c of the row
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    const uint32_t vv  = v[e];
+    const uint32_t k   = h2_min(h2_sub(vv & kAbs, m1), kH1);
+    const uint32_t mag = h2_fma(nds, k, s2);
+    const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
+    c2v_row[e * kX2Half] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+    const uint32_t t   = h2_add(c, vv);
+    const uint32_t cl  = h2_min(h2_max(t, kHm120), kH120);
+    uint32_t       u   = h2_fma(cl, kHm7, h2_mul(t, kH8));
+    u                  = h2_min(h2_max(u, kHm127), kH127);
+    u                  = h2_min(h2_max(u, h2_fma(vv, kH37, kHm4572)), h2_fma(vv, kH37, kH4572));
+    const uint32_t ub  = h2_to_bytes_biased(u);
+    const uint32_t ed  = edge[e];
+    const unsigned p0  = (unsigned)j + (ed & 0xffffu);
+    const unsigned p   = min(p0, p0 - (unsigned)kX2Z) + (ed >> 16);
+    D[p]               = (uint16_t)__byte_perm(ub, 0, 0x0020);
+    D[x2_partner(p)]   = (uint16_t)__byte_perm(ub, 0, 0x0002);
+  }
+}
+
+template <bool FIRST>
+__device__ __forceinline__ void row_dispatch_x2(int deg, int j, uint16_t* D, const uint32_t* edge, uint16_t* c2v_row,
+                                                const uint16_t* tab)
+{
+  switch (deg) {
+    case 3: row_update_x2<3, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 4: row_update_x2<4, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 5: row_update_x2<5, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 6: row_update_x2<6, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 7: row_update_x2<7, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 8: row_update_x2<8, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 9: row_update_x2<9, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 10: row_update_x2<10, FIRST>(j, D, edge, c2v_row, tab); break;
+    default: row_update_x2<19, FIRST>(j, D, edge, c2v_row, tab); break;
+  }
+}
+
+// Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`.
+__device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const int8_t* __restrict__ llrs,
+                                    uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
+                                    int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
+                                    const uint16_t* __restrict__ scale_tab, const int cb, const int slab)
+{
+  constexpr int Z   = kX2Z;
+  const int     tid = threadIdx.x;
+  const int     bg  = d.base_graph;
+  if (bg != 1 && bg != 2) {
+    if (tid == 0) {
+      iterations[cb] = -1;
+    }
+    return;
+  }
+  const int     g        = bg - 1;
+  const int     set      = 1; // Z = 384 = 3 * 2^7: set index 1 (a = 3)
+  const int     Kb       = bg == 1 ? 22 : 10;
+  const int     nrows    = bg == 1 ? pg::kBg1Rows : pg::kBg2Rows;
+  const int     nedges   = bg == 1 ? pg::kBg1Edges : pg::kBg2Edges;
+  const int     nfull    = bg == 1 ? 68 : 52;
+  const int     msg_len  = Kb * Z;
+  const int     n        = (int)d.nof_llrs;
+  const int8_t* in       = llrs + d.llr_offset;
+  uint16_t*     c2v      = reinterpret_cast<uint16_t*>(c2v_all + (size_t)slab * pg::kC2vStride);
+  const int     nbytes   = (msg_len + 7) / 8;
+  uint8_t*      out      = bits + d.out_offset;
+  const int     crc_poly = d.crc_poly;
+  const int     nwords   = (msg_len + 31) / 32;
+  uint16_t*     D        = sm.D;
+
+  for (int e = tid; e < nedges; e += kX2Threads) {
+    const int col = c_edge_col[g][e];
+    const int s   = c_edge_v[g][e][set] % Z;
+    sm.edge[e]    = ((uint32_t)(col * Z) << 16) | (uint32_t)s;
+  }
+  if (tid == 0) {
+    sm.s_last = 0;
+    sm.s_done = 0;
+  }
+  // Trailing-zero trim (ldpc_decoder_impl.cpp:66-71): the last non-zero LLR.
+  int last = 0;
+  for (int k = tid; k < n; k += kX2Threads) {
+    last = in[k] != 0 ? k + 1 : last;
+  }
+  last = warp_max(last);
+  __syncthreads();
+  if ((tid & 31) == 0 && last > 0) {
+    atomicMax(&sm.s_last, last);
+  }
+  // Soft bits (2Z punctured zeros, whole nodes clamped to +-64, a ragged tail as is, zeros after),
+  // both copies of each pair, offset binary.
+  const int nof_full = (n / Z) * Z;
+  auto soft_in = [&](int i) -> uint32_t {
+    const int k = i - 2 * Z;
+    int       v = 0;
+    if (k >= 0 && k < n) {
+      v = in[k];
+      v = k < nof_full ? max(-64, min(64, v)) : v;
+    }
+    return (uint32_t)(v + 128);
+  };
+  for (int i = tid; i < nfull * Z; i += kX2Threads) {
+    const int col = i / Z, w = i - col * Z;
+    const int w2  = w < kX2Half ? w + kX2Half : w - kX2Half;
+    D[i]          = (uint16_t)(soft_in(col * Z + w) | (soft_in(col * Z + w2) << 8));
+  }
+  __syncthreads();
+
+  const int input_size = sm.s_last;
+  if (input_size < msg_len) {
+    for (int b = tid; b < nbytes; b += kX2Threads) {
+      out[b] = 0xff;
+    }
+    if (tid == 0) {
+      iterations[cb] = 0;
+    }
+    return;
+  }
+  int cb_len = max(input_size + 2 * Z, (Kb + 4) * Z);
+  cb_len     = ((cb_len + Z - 1) / Z) * Z;
+  const int nof_layers = min(cb_len / Z - Kb, nrows);
+
+  int order = 24;
+  if (crc_poly == PG_CRC16) {
+    order = 16;
+  }
+  const uint32_t* pow_tab = crc_pow + (size_t)(crc_poly <= PG_CRC24B ? crc_poly : 0) * pg::kCrcPowLen;
+  const int       crc_len = msg_len - (int)d.nof_filler_bits;
+
+  int       result = 0;
+  const int max_it = d.max_iterations;
+  const int lane   = tid & 31;
+  for (int it = 0; it < max_it; ++it) {
+    int e0 = 0;
+    for (int r = 0; r < nof_layers; ++r) {
+      const int deg     = c_row_deg[g][r];
+      uint16_t* c2v_row = c2v + (size_t)e0 * kX2Half + tid;
+      if (it == 0) {
+        row_dispatch_x2<true>(deg, tid, D, sm.edge + e0, c2v_row, scale_tab);
+      } else {
+        row_dispatch_x2<false>(deg, tid, D, sm.edge + e0, c2v_row, scale_tab);
+      }
+      e0 += deg;
+      __syncthreads();
+    }
+
+    // Hard decisions (soft <= 0: offset byte <= 128; the low byte of D[i] is soft bit i), zero
+    // check and CRC: one 32-bit word per warp step, lane k holding bit k of the word (MSB first
+    // after the reversal); each set bit within the CRC length adds x^e mod g.
+    int      zero = 0;
+    uint32_t crc  = 0;
+    for (int wi = tid >> 5; wi < nwords; wi += kX2Threads / 32) {
+      const int      idx = 32 * wi + lane;
+      const uint32_t b   = idx < msg_len ? (D[idx] & 0xffu) : 0xffu;
+      const bool     bit = b <= 128u;
+      zero |= b == 128u;
+      const uint32_t w = __brev(__ballot_sync(0xffffffffu, bit));
+      if (lane == 0) {
+        sm.hard[wi] = w;
+      }
+      if (crc_poly != PG_CRC_NONE && bit && idx < crc_len) {
+        crc ^= __ldg(pow_tab + (crc_len - 1 - idx + order));
+      }
+    }
+    zero = __syncthreads_or(zero);
+    crc  = warp_xor(crc);
+    if (lane == 0) {
+      sm.red[tid >> 5] = crc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kX2Threads / 32; ++w) {
+        t ^= sm.red[w];
+      }
+      sm.s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
+    }
+    __syncthreads();
+    if (sm.s_done) {
+      result = it + 1;
+      break;
+    }
+  }
+
+  if (crc_poly == PG_CRC_NONE) {
+    // Syndrome check over the processed rows (ldpc_decoder_impl.cpp:329-387), both lanes.
+    int bad = 0;
+    int e0  = 0;
+    for (int r = 0; r < nof_layers; ++r) {
+      const int deg    = c_row_deg[g][r];
+      uint32_t  parity = 0;
+      for (int e = 0; e < deg; ++e) {
+        const uint32_t ed = sm.edge[e0 + e];
+        int            p  = tid + (int)(ed & 0xffffu);
+        p                 = (p >= Z) ? p - Z : p;
+        const uint32_t x  = D[p + (int)(ed >> 16)];
+        const uint32_t lo = x & 0xffu, hi = x >> 8;
+        bad |= (lo == 128u) | (hi == 128u);
+        parity ^= (uint32_t)(lo <= 128u) | ((uint32_t)(hi <= 128u) << 1);
+      }
+      bad |= parity != 0;
+      e0 += deg;
+    }
+    bad      = __syncthreads_or(bad);
+    int zero = 0;
+    for (int i = tid; i < msg_len; i += kX2Threads) {
+      zero |= (D[i] & 0xffu) == 128u;
+    }
+    zero   = __syncthreads_or(zero);
+    result = (!bad && !zero) ? max_it : 0;
+  }
+
+  for (int b = tid; b < nbytes; b += kX2Threads) {
+    out[b] = (uint8_t)(sm.hard[b >> 2] >> (24 - 8 * (b & 3)));
+  }
+  if (tid == 0) {
+    iterations[cb] = result;
+  }
+  __syncthreads();
+}
+
+// Persistent decoder of the Z = 384 codeblocks of a work list (the others are left to
+// ldpc_decode_kernel): each CTA takes the next work index from *counter, skips codeblocks of other
+// lifting sizes, and decodes with slab blockIdx.x.
+__global__ void __launch_bounds__(kX2Threads, 4) ldpc_decode_x2_kernel(const pg_ldpc_cb* __restrict__ descs,
+                                                                       const int8_t* __restrict__ llrs,
+                                                                       uint8_t* __restrict__ bits,
+                                                                       int32_t* __restrict__ iterations,
+                                                                       int8_t* __restrict__ c2v_all,
+                                                                       const uint32_t* __restrict__ crc_pow,
+                                                                       const uint16_t* __restrict__ scale_tab,
+                                                                       const uint32_t* __restrict__ order, int n,
+                                                                       int* __restrict__ counter)
+{
+  extern __shared__ __align__(16) unsigned char smem_x2_raw[];
+  smem_x2_t& sm = *reinterpret_cast<smem_x2_t*>(smem_x2_raw);
+  __shared__ int s_work;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_work = atomicAdd(counter, 1);
+    }
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= n) {
+      break;
+    }
+    const int        cb = order != nullptr ? (int)order[w] : w;
+    const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size == kX2Z) {
+      decode_codeblock_x2(d, sm, llrs, bits, iterations, c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
     }
   }
 }
@@ -523,7 +929,27 @@ int ldpc_upload_tables(pg_context* ctx)
   for (int r = 0; r < PG_BG2_ROWS; ++r) {
     deg[1][r] = PG_BG2_ROW_DEG[r];
   }
+  // Scale table of the two-lanes-per-thread decoder: f16 bits of (m * 52428) >> 16 at (f16 bits of
+  // m) >> 4, m = 0 .. 127.
+  uint16_t scale[kScaleTab] = {};
+  for (int m = 0; m <= 127; ++m) {
+    const uint16_t key = __half_as_ushort(__float2half_rn((float)m)) >> 4;
+    scale[key]         = __half_as_ushort(__float2half_rn((float)((m * 52428) >> 16)));
+  }
   int rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_col, col, sizeof(col)), "cudaMemcpyToSymbol(edge_col)");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_scale, sizeof(scale)), "cudaMalloc(scale table)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpy(ctx->dev.ldpc_scale, scale, sizeof(scale), cudaMemcpyHostToDevice),
+                    "cudaMemcpy(scale table)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaFuncSetAttribute(ldpc_decode_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(smem_x2_t)),
+                    "cudaFuncSetAttribute(ldpc_decode_x2_kernel)");
+  }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_v, v, sizeof(v)), "cudaMemcpyToSymbol(edge_v)");
   }
@@ -573,30 +999,47 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
                            cudaStream_t stream)
 {
-  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, counter, stream, ctx->ldpc_ctas);
+  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, counter, stream,
+                                kX2MaxPerSm * ctx->sm_count, PG_LDPC_KIND_ALL | PG_LDPC_ROUTE_X2);
 }
 
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
-                           cudaStream_t stream, int max_ctas)
+                           cudaStream_t stream, int max_ctas, int kinds)
 {
   if (n == 0) {
     return PG_OK;
   }
-  if (int rc = check_cuda(ctx, cudaMemsetAsync(counter, 0, sizeof(int), stream), "cudaMemsetAsync(ldpc counter)")) {
+  if (int rc = check_cuda(ctx, cudaMemsetAsync(counter, 0, 2 * sizeof(int), stream), "cudaMemsetAsync(ldpc counter)")) {
     return rc;
   }
   const unsigned int rec_flags = timing_record_flags(ctx, stream);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  const int grid = std::max(1, std::min(n, std::min(max_ctas, ctx->ldpc_ctas)));
-  ldpc_decode_kernel<<<grid, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, order, n,
-                                                    counter);
+  // With PG_LDPC_ROUTE_X2 the Z = 384 codeblocks go to the two-lanes-per-thread kernel and the
+  // others to ldpc_decode_kernel, both walking the same work list with their own counters and
+  // slabs 0 .. grid - 1; without it ldpc_decode_kernel decodes them all.
+  // ldpc_decode_kernel holds ldpc_ctas CTAs on the device (two per SM), the x2 kernel four per SM;
+  // the caller provides a slab per CTA (min(n, max_ctas) slabs).
+  const int grid    = std::max(1, std::min(n, std::min(max_ctas, ctx->ldpc_ctas)));
+  const int grid_x2 = std::max(1, std::min(n, std::min(max_ctas, kX2MaxPerSm * ctx->sm_count)));
+  int       rc      = PG_OK;
+  const bool x2 = (kinds & PG_LDPC_KIND_Z384) && (kinds & PG_LDPC_ROUTE_X2);
+  if (x2) {
+    ldpc_decode_x2_kernel<<<grid_x2, kX2Threads, sizeof(smem_x2_t), stream>>>(
+        descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
+    rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_x2_kernel launch");
+  }
+  if (rc == PG_OK && ((kinds & PG_LDPC_KIND_OTHER) || ((kinds & PG_LDPC_KIND_Z384) && !x2))) {
+    ldpc_decode_kernel<<<grid, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, order,
+                                                      n, counter, x2 ? kX2Z : 0);
+    rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch");
+  }
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, stream, rec_flags);
   }
-  return check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch");
+  return rc;
 }
 
 } // namespace pg
@@ -680,7 +1123,7 @@ extern "C" int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldp
   int     rc      = static_scratch_address(ctx, &scratch);
   if (rc == PG_OK) {
     ldpc_decode_kernel<<<nof_cbs, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-        cbs_dev, llrs, bits, iterations, scratch, ctx->dev.crc_pow, nullptr, nof_cbs, nullptr);
+        cbs_dev, llrs, bits, iterations, scratch, ctx->dev.crc_pow, nullptr, nof_cbs, nullptr, 0);
     rc = pg::check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch (static scratch)");
   }
   if (prev != ctx->device) {

@@ -292,7 +292,7 @@ int pg_create(const pg_config* cfg, pg_context** out)
                     "cudaMalloc(iterations)");
   }
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_counter, sizeof(int)), "cudaMalloc(ldpc counter)");
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_counter, 2 * sizeof(int)), "cudaMalloc(ldpc counter)");
   }
   if (rc == PG_OK) {
     ctx->ldpc_ctas = ldpc_resident_ctas(ctx);
@@ -376,6 +376,7 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.bits);
   cudaFree(ctx->dev.iterations);
   cudaFree(ctx->dev.ldpc_counter);
+  cudaFree(ctx->dev.ldpc_scale);
   if (ctx->host_descs) {
     cudaFreeHost(ctx->host_descs);
   }

@@ -62,7 +62,8 @@ struct device_buffers {
   int8_t*      llrs        = nullptr; // staging for _host calls
   uint8_t*     bits        = nullptr;
   int32_t*     iterations  = nullptr;
-  int*         ldpc_counter = nullptr; // work counter of the persistent decoder
+  int*         ldpc_counter = nullptr; // work counters of the persistent decoders (two ints)
+  uint16_t*    ldpc_scale   = nullptr; // scale table of the two-lanes-per-thread decoder
   size_t       llr_cap     = 0;
   size_t       bits_cap    = 0;
 };
@@ -188,10 +189,15 @@ int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, con
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
                            cudaStream_t stream);
-// Same with at most max_ctas CTAs.
+// Kinds of codeblocks a work list may hold: Z = 384 (two-lanes-per-thread decoder) and others.
+// PG_LDPC_ROUTE_X2 routes the Z = 384 codeblocks to the two-lanes-per-thread decoder; without it
+// ldpc_decode_kernel decodes every codeblock.
+enum { PG_LDPC_KIND_OTHER = 1, PG_LDPC_KIND_Z384 = 2, PG_LDPC_KIND_ALL = 3, PG_LDPC_ROUTE_X2 = 4 };
+// Same with at most max_ctas CTAs per decoder kernel, launching only the decoders of `kinds`.
+// counter: two device ints; c2v: one slab (kC2vStride bytes) per CTA.
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
-                           cudaStream_t stream, int max_ctas);
+                           cudaStream_t stream, int max_ctas, int kinds);
 // CTAs of ldpc_decode_kernel resident on the whole device.
 int ldpc_resident_ctas(pg_context* ctx);
 

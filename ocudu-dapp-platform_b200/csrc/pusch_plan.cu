@@ -25,6 +25,7 @@ struct pg_pusch_plan {
   size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0, est_total = 0;
   uint32_t                 total_re = 0;
   int                      max_rb   = 1;
+  int                      ldpc_kinds = 0; // PG_LDPC_KIND_* present in the plan
   std::vector<pg_pusch_ue> ues;
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
@@ -59,7 +60,7 @@ struct pg_pusch_plan {
   int             le_nseq   = 0;
   int             le_rows   = 0;
   // Launch shapes (defaults, or the autotuner's choice).
-  pg_pusch_plan_tuning tuning = {8, 1, 256, 2};
+  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, 0};
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -130,7 +131,8 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
   }
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
-                                p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count);
+                                p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count,
+                                p->ldpc_kinds | (p->tuning.ldpc_z384_two_lanes ? PG_LDPC_ROUTE_X2 : 0));
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
@@ -238,7 +240,12 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     cost[c]             = (uint64_t)l.lifting_size * std::min<uint64_t>(w.rm[c].rm_length + l.nof_filler_bits, l.nof_llrs);
   }
   std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
-  const int ldpc_slabs = std::max(1, std::min(p->nof_cbs, ctx->ldpc_ctas));
+  p->ldpc_kinds = 0;
+  for (const pg_ldpc_cb& l : w.ldpc) {
+    p->ldpc_kinds |= l.lifting_size == 384 ? PG_LDPC_KIND_Z384 : PG_LDPC_KIND_OTHER;
+  }
+  // One check-to-variable slab per decoder CTA: up to four per SM (the Z = 384 decoder).
+  const int ldpc_slabs = std::max(1, std::min(p->nof_cbs, 4 * ctx->sm_count));
 
   // Device image: descriptors first (uploaded once), then the workspace.
   const size_t o_ues    = 0;
@@ -423,7 +430,8 @@ static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
 {
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
          t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
-         t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm * ctx->sm_count <= ctx->ldpc_ctas;
+         t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm <= 4 &&
+         (t.ldpc_z384_two_lanes == 0 || t.ldpc_z384_two_lanes == 1);
 }
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
@@ -509,7 +517,7 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
   static const int rm_c[]    = {2, 4, 8, 16, 32};
   static const int res_c[]   = {1, 2, 4};
   static const int blk_c[]   = {64, 128, 256};
-  static const int ldpc_c[]  = {1, 2};
+  static const int ldpc_c[]  = {1, 2, 3, 4};
   pg_pusch_plan_tuning cur   = plan->tuning;
   float                cur_ms = 0.f;
   int rc = time_plan(plan, grids, plan->d_tb_out, plan->d_res, reps, &cur_ms);
@@ -547,6 +555,11 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
     for (int v : ldpc_c) {
       pg_pusch_plan_tuning c = cur;
       c.ldpc_ctas_per_sm     = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+    for (int v : {0, 1}) {
+      pg_pusch_plan_tuning c = cur;
+      c.ldpc_z384_two_lanes  = v;
       if (rc == PG_OK) rc = try_set(c);
     }
   }

@@ -152,3 +152,41 @@ def test_capacity_rejected(ctx):
         small.decode_batch(jobs)
     assert e.value.code == _native.PG_ERR_CAPACITY
     small.ctx.close()
+
+
+def test_z384_saturation_and_short_inputs_match_port(batch_decoder, port):
+    """Z = 384 codeblocks (the two-lanes-per-thread decoder) at high SNR, where soft bits saturate to
+    +-127 and the infinity rules decide, with fillers, every CRC and trimmed or too-short inputs."""
+    rng = np.random.default_rng(384)
+    jobs = []
+    for t in range(48):
+        bg = 1 + (t & 1)
+        z = 384
+        k = golden_io.kbits(bg, z)
+        nn = (66 if bg == 1 else 50) * z
+        poly = [0, 1, 2, 255][t % 4]
+        cpoly = 2 if poly == 255 else poly
+        order = 16 if cpoly == 0 else 24
+        f = int(rng.integers(0, 400)) if t % 3 else 0
+        msg = np.concatenate([codec.attach_crc(cpoly, rng.integers(0, 2, k - f - order, dtype=np.uint8)),
+                              np.zeros(f, np.uint8)])
+        cw = codec.ldpc_encode(bg, z, msg)
+        snr_db = rng.uniform(4, 12) if t % 5 else rng.uniform(-1, 2)
+        sigma = np.sqrt(1 / (2 * 10 ** (snr_db / 10)))
+        llr = np.clip(np.rint((1 - 2.0 * cw + sigma * rng.standard_normal(nn)) * 2 / sigma ** 2 * 4), -120,
+                      120).astype(np.int8)
+        if f:
+            llr[k - 2 * z - f:k - 2 * z] = 127
+        e = int(rng.integers(k + 2 * z, nn + 1)) if t % 7 else k  # the last ones: fewer LLRs than message bits
+        llr[e:] = 0
+        cfg = LdpcDecoderConfiguration(bg, z, f, order, int(rng.integers(1, 12)))
+        jobs.append(CodeblockJob(llr, cfg, poly))
+    outs, iters = batch_decoder.decode_batch(jobs)
+    for j, o, it in zip(jobs, outs, iters):
+        c = j.cfg
+        p = -1 if j.crc_poly == 255 else j.crc_poly
+        want_it, want_bits = port.ldpc_decode(c.base_graph, c.lifting_size, j.llrs, filler=c.nof_filler_bits,
+                                              crc_poly=p, max_iter=c.max_iterations)
+        k = golden_io.kbits(c.base_graph, c.lifting_size)
+        assert it == want_it, (c, j.crc_poly)
+        assert (unpack(o, k) == unpack(want_bits, k)).all(), (c, j.crc_poly)

@@ -101,9 +101,11 @@ def test_autotuner_keeps_results(ctx):
     best, ms = plan.autotune(d_grid.data_ptr(), reps=3)
     assert ms > 0
     assert 1 <= best.rm_ctas_per_cb <= 32 and 1 <= best.demod_res_per_thread <= 8
-    assert best.demod_block in (64, 128, 256) and best.ldpc_ctas_per_sm in (1, 2)
+    assert best.demod_block in (64, 128, 256) and best.ldpc_ctas_per_sm in (1, 2, 3, 4)
     assert plan.tuning().as_dict() == best.as_dict()
-    for shape in (best, PgPuschPlanTuning(3, 3, 64, 1), PgPuschPlanTuning(32, 8, 128, 2)):
+    assert best.ldpc_z384_two_lanes in (0, 1)
+    for shape in (best, PgPuschPlanTuning(3, 3, 64, 1, 0), PgPuschPlanTuning(32, 8, 128, 2, 1),
+                  PgPuschPlanTuning(8, 1, 256, 4, 1), PgPuschPlanTuning(8, 1, 256, 1, 1)):
         plan.set_tuning(shape)
         got = plan.execute_host()
         for g, r in zip(got, ref):
@@ -111,5 +113,5 @@ def test_autotuner_keeps_results(ctx):
             if r.tb_crc_ok:
                 assert np.array_equal(g.transport_block, r.transport_block)
     with pytest.raises(Exception):
-        plan.set_tuning(PgPuschPlanTuning(0, 1, 256, 2))
+        plan.set_tuning(PgPuschPlanTuning(0, 1, 256, 2, 0))
     plan.close()
