@@ -400,6 +400,17 @@ int  pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info);
  * than the legacy default stream only; on the default stream the launches are enqueued directly. */
 int pg_pusch_plan_set_graph(pg_pusch_plan* plan, int enabled);
 
+/* HARQ soft combining (the reference's rate-dematch soft buffer,
+ * lib/phy/upper/channel_coding/ldpc/ldpc_rate_dematcher_impl.cpp:98-194, and its rx_buffer per HARQ
+ * process, lib/phy/upper/rx_buffer_pool_impl.cpp, pusch_decoder_impl.cpp:412-430). The plan keeps
+ * each UE's dematched codeblocks on the device between executions: for the UEs with new_data[u] ==
+ * 0 the next execution combines the received LLRs into them (saturating sums, as the reference)
+ * instead of overwriting them, with redundancy version rv[u] (0..3). new_data or rv may be NULL
+ * (unchanged). Call it between executions (no execution of the plan in flight); it synchronises
+ * the context's stream. A plan holds one soft buffer per UE, valid until its next new-data
+ * execution. */
+int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const uint8_t* rv);
+
 /* Launch shapes of a plan's stages (the autotuner's search space). No counterpart in the
  * reference, whose stages are sized per UE and per codeblock by its thread pools. */
 typedef struct pg_pusch_plan_tuning {

@@ -27,6 +27,9 @@ struct pg_pusch_plan {
   int                      max_rb   = 1;
   int                      ldpc_kinds = 0; // PG_LDPC_KIND_* present in the plan
   std::vector<pg_pusch_ue> ues;
+  std::vector<pg_rm_cb>    rm;                 // rate-dematch descriptors (host copy, for HARQ updates)
+  std::vector<int>         tb_first, tb_ncb;   // codeblocks of each UE
+  size_t                   rm_total = 0;       // bytes of dematched codeblocks (the soft buffers)
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
   pg_pusch_ue*    d_ues    = nullptr;
@@ -229,7 +232,11 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     release(p);
     return rc;
   }
-  p->nof_cbs = (int)w.ldpc.size();
+  p->nof_cbs  = (int)w.ldpc.size();
+  p->rm       = w.rm;
+  p->tb_first = w.tb_first;
+  p->tb_ncb   = w.tb_ncb;
+  p->rm_total = w.rm_total;
   // LDPC work order, largest first: a codeblock's cost grows with Z times the LLR positions it
   // fills (E + F, at most N), which fix the check rows it runs.
   std::vector<uint32_t> order(p->nof_cbs);
@@ -426,6 +433,48 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
   return PG_OK;
 }
 
+int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const uint8_t* rv)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  for (int u = 0; u < plan->nof_ues && rv != nullptr; ++u) {
+    if (rv[u] > 3) {
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(u) + ": redundancy version above 3");
+    }
+  }
+  for (int u = 0; u < plan->nof_ues; ++u) {
+    if (rv != nullptr) {
+      plan->ues[u].rv = rv[u];
+    }
+    for (int c = plan->tb_first[u]; c < plan->tb_first[u] + plan->tb_ncb[u]; ++c) {
+      if (rv != nullptr) {
+        plan->rm[c].rv = rv[u];
+      }
+      if (new_data != nullptr) {
+        plan->rm[c].new_data = new_data[u] != 0 ? 1 : 0;
+      }
+    }
+  }
+  // The kernels read the descriptors when they run, so a captured graph stays valid.
+  cudaStream_t s  = ctx->stream;
+  int          rc = check_cuda(ctx,
+                               cudaMemcpyAsync(plan->d_rm, plan->rm.data(), plan->rm.size() * sizeof(pg_rm_cb),
+                                               cudaMemcpyHostToDevice, s),
+                               "H2D HARQ rate-dematch descriptors");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaMemcpyAsync(plan->d_ues, plan->ues.data(), plan->ues.size() * sizeof(pg_pusch_ue),
+                                    cudaMemcpyHostToDevice, s),
+                    "H2D HARQ UE descriptors");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  }
+  return rc;
+}
+
 static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
 {
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
@@ -520,7 +569,27 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
   static const int ldpc_c[]  = {1, 2, 3, 4};
   pg_pusch_plan_tuning cur   = plan->tuning;
   float                cur_ms = 0.f;
-  int rc = time_plan(plan, grids, plan->d_tb_out, plan->d_res, reps, &cur_ms);
+  // UEs set to combine would accumulate every timed execution into their soft buffers: keep a
+  // copy of the buffers and put it back afterwards.
+  bool combining = false;
+  for (const pg_rm_cb& c : plan->rm) {
+    combining = combining || c.new_data == 0;
+  }
+  int8_t* saved = nullptr;
+  int     rc    = PG_OK;
+  if (combining) {
+    rc = check_cuda(ctx, cudaMalloc(&saved, plan->rm_total), "cudaMalloc(soft-buffer copy)");
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx,
+                      cudaMemcpyAsync(saved, plan->d_rm_out, plan->rm_total, cudaMemcpyDeviceToDevice, ctx->stream),
+                      "D2D soft buffers");
+    }
+    if (rc != PG_OK) {
+      cudaFree(saved);
+      return rc;
+    }
+  }
+  rc = time_plan(plan, grids, plan->d_tb_out, plan->d_res, reps, &cur_ms);
   auto try_set = [&](pg_pusch_plan_tuning cand) -> int {
     if (!tuning_valid(cand, ctx)) {
       return PG_OK;
@@ -562,6 +631,14 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
       c.ldpc_z384_two_lanes  = v;
       if (rc == PG_OK) rc = try_set(c);
     }
+  }
+  if (saved != nullptr) {
+    const int r = check_cuda(
+      ctx, cudaMemcpyAsync(plan->d_rm_out, saved, plan->rm_total, cudaMemcpyDeviceToDevice, ctx->stream),
+      "D2D soft buffers");
+    const int r2 = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+    cudaFree(saved);
+    rc = rc != PG_OK ? rc : (r != PG_OK ? r : r2);
   }
   if (rc != PG_OK) {
     return rc;

@@ -155,6 +155,7 @@ SIGNATURES = {
     "pg_le_train_step_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_estimate_ls_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),
+    "pg_pusch_plan_set_harq": (ctypes.c_int, [_VP, _VP, _VP]),
     "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),

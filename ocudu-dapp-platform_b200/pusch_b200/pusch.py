@@ -153,6 +153,13 @@ class PuschSlotPlan:
         u = None if use is None else (ctypes.c_uint8 * self.n)(*[int(bool(v)) for v in use])
         self.ctx.check(self.lib.pg_pusch_plan_set_learned(self.handle, net.handle if net is not None else None, u))
 
+    def set_harq(self, new_data=None, rv=None):
+        """HARQ: for UEs with new_data[u] false the next execution soft-combines into the codeblock
+        buffers the plan kept from the previous one, with redundancy version rv[u]."""
+        nd = None if new_data is None else (ctypes.c_uint8 * self.n)(*[int(bool(v)) for v in new_data])
+        r = None if rv is None else (ctypes.c_uint8 * self.n)(*[int(v) for v in rv])
+        self.ctx.check(self.lib.pg_pusch_plan_set_harq(self.handle, nd, r))
+
     def tuning(self):
         t = _native.PgPuschPlanTuning()
         self.ctx.check(self.lib.pg_pusch_plan_get_tuning(self.handle, ctypes.byref(t)))

@@ -140,10 +140,11 @@ def channel_response(rng, ue, nof_ports, scs_khz):
     return np.einsum("plt,tf->plf", taps, steer)
 
 
-def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30):
+def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30, tb_bits=None):
     """Seeded uplink slot: for each UE, random TB -> UL-SCH coding -> scrambling -> modulation ->
     layer mapping -> RE mapping with DM-RS (type 1, amplitude +3 dB) -> channel -> AWGN; the
-    grid is rounded to complex bf16 (the reference's resource-grid storage)."""
+    grid is rounded to complex bf16 (the reference's resource-grid storage). tb_bits (one array per
+    UE) transmits given transport blocks instead, e.g. a HARQ retransmission with another rv."""
     from . import prg
     from .demod import to_cbf16
     from .sch import segment
@@ -157,6 +158,8 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
         ncs = nof_ch_symbols(ue)
         seg = segment(ue.tbs_bits, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs)
         tb = rng.integers(0, 2, ue.tbs_bits, dtype=np.uint8)
+        if tb_bits is not None:
+            tb = np.asarray(tb_bits[len(truth)], np.uint8)
         cw = codec.ulsch_encode(tb, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs, seg, rv=ue.rv)
         cw = cw ^ prg.scrambling(ue.rnti, ue.n_id_data, cw.size)
         d = codec.modulate(cw, ue.modulation_order)              # [ncs]
