@@ -454,7 +454,10 @@ def run_ours_pusch(args):
     peak = peak_ops / 1e12 if peak_ops else nominal
     achieved = ops / (k_ms * 1e-3) / 1e12
     roofline = {
-        "bound": "int", "kernel": "ldpc_decode_kernel", "achieved": round(achieved, 3), "peak": round(peak, 3),
+        "bound": "int",
+        "kernel": ("ldpc_decode_x2_kernel (Z=384) + ldpc_decode_kernel (other Z)"
+                   if tuning.as_dict().get("ldpc_z384_two_lanes") else "ldpc_decode_kernel"),
+        "achieved": round(achieved, 3), "peak": round(peak, 3),
         "unit": "Tops/s", "frac": round(achieved / peak, 4),
         "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"
                         if peak_ops else "nominal 148 SM x 128 lanes x max SM clock"),
@@ -471,7 +474,7 @@ def run_ours_pusch(args):
         peak_tf, peak_src = bf16_peak()
         ach = flops / (le_ms * 1e-3) / 1e12
         rooflines["learned"] = {
-            "bound": "tensor", "kernel": "conv1d_fwd_kernel (14 launches) + le_features/le_apply",
+            "bound": "tensor", "kernel": "le_fused_forward_kernel (14 layers in one launch) + le_features/le_apply",
             "achieved": round(ach, 2), "peak": peak_tf, "unit": "TFLOP/s", "frac": round(ach / peak_tf, 4),
             "peak_source": peak_src, "flops_per_launch_chain": flops, "rows": le_rows,
             "flops_per_row": LE_FLOPS_PER_ROW, "stage_ms": round(le_ms, 4), "stage_share_of_step": round(le_ms / ms, 3),
@@ -690,15 +693,20 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     nominal = props.multi_processor_count * 128 * (clk["sm_max_mhz"] or 1965.0) * 1e6 / 1e12
     peak = peak_ops / 1e12 if peak_ops else nominal
     roofline = {
-        "bound": "int", "kernel": "ldpc_decode_kernel", "achieved": round(achieved, 3), "peak": round(peak, 3),
+        "bound": "int",
+        "kernel": "ldpc_decode_x2_kernel (every codeblock of the batch has Z=384)",
+        "achieved": round(achieved, 3), "peak": round(peak, 3),
         "unit": "Tops/s", "frac": round(achieved / peak, 4),
         "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"
                         if peak_ops else "nominal 148 SM x 128 lanes x max SM clock"),
         "nominal_peak": round(nominal, 3), "instruction_classes_tops": classes,
         "ops_per_edge_update": INT_OPS_PER_EDGE, "edge_updates_per_launch": edge_updates,
-        # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this workload (ncu capture
-        # summarised in profiles/ldpc_decode_kernel_ldpc-batch-512cb.md).
-        "traffic": 17298000,
+        # dram__bytes_read.sum + dram__bytes_write.sum of one launch of ldpc_decode_x2_kernel on this
+        # workload, and its pipe utilisation (ncu --set full, one launch; summarised in
+        # profiles/ldpc_decode_kernel_ldpc-batch-512cb.md).
+        "traffic": 24246528,
+        "ncu_pipes_pct_of_active": {"alu": 55.5, "fma": 32.3, "lsu": 24.9, "issue_active": 59.6,
+                                    "sm_active_pct_of_elapsed": 60.4},
         "hbm_bytes_per_launch": int(llrs.size + nbytes + 4 * N_CBS + 20 * N_CBS),
     }
 

@@ -419,9 +419,9 @@ typedef struct pg_pusch_plan_tuning {
   int demod_block;          /* demodulation: threads per CTA, 64, 128 or 256 (default 256) */
   int ldpc_ctas_per_sm;     /* persistent LDPC decoders: CTAs per SM, 1..4 (default 2; the one-lane-per-
                                thread decoder holds at most 2) */
-  int ldpc_z384_two_lanes;  /* 1: Z = 384 codeblocks on the two-lanes-per-thread decoder (a lifting-size
-                               specialisation), 0: every codeblock on the one-lane-per-thread decoder
-                               (default 0) */
+  int ldpc_z384_two_lanes;  /* 1: every codeblock on the 192-thread decoder, two lifted lanes per
+                               thread for even Z > 192 (up to 384) and one lane per thread below;
+                               0: every codeblock on the 384-thread one-lane decoder (default 0) */
 } pg_pusch_plan_tuning;
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out);

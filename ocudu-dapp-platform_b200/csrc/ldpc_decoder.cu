@@ -129,7 +129,7 @@ __device__ __forceinline__ void row_update(const int tid, const int Zr, int8_t* 
 // Degree-19 rows (BG1 rows 0-3): the same update as a rolled loop with the v2c messages staged in
 // shared memory (one byte per edge and lane), so the wide rows do not raise the register budget
 // of the whole kernel; the soft-bit addresses are recomputed in the second pass.
-template <bool FIRST, int ZT>
+template <bool FIRST, int ZT, int NT>
 __device__ __forceinline__ void row_update_wide(const int deg, const int tid, const int Zr, int8_t* __restrict__ soft,
                                                 const uint32_t* __restrict__ edge, int8_t* __restrict__ c2v_row,
                                                 int8_t* __restrict__ mbuf)
@@ -148,7 +148,7 @@ __device__ __forceinline__ void row_update_wide(const int deg, const int tid, co
       v           = max(-120, min(120, x - c));
       v           = (x == 127 || x == -127) ? x : v;
     }
-    mbuf[e * kThreads + tid] = (int8_t)v;
+    mbuf[e * NT + tid] = (int8_t)v;
     const int a              = abs(v);
     min2                     = min(min2, max(min1, a));
     min1                     = min(min1, a);
@@ -161,7 +161,7 @@ __device__ __forceinline__ void row_update_wide(const int deg, const int tid, co
     const uint32_t ed  = edge[e];
     const unsigned p0  = (unsigned)tid + (ed & 0xffffu);
     const unsigned p   = min(p0, p0 - (unsigned)Z) + (ed >> 16);
-    const int      v   = mbuf[e * kThreads + tid];
+    const int      v   = mbuf[e * NT + tid];
     const int      a   = abs(v);
     const int      mag = (a == min1) ? s2 : s1;
     const int      c   = ((v ^ sgn) < 0) ? -mag : mag;
@@ -174,7 +174,7 @@ __device__ __forceinline__ void row_update_wide(const int deg, const int tid, co
 }
 
 // Base-graph row degrees: BG1 {3..10, 19}, BG2 {3..10}.
-template <bool FIRST, int ZT>
+template <bool FIRST, int ZT, int NT>
 __device__ __forceinline__ void row_dispatch(int deg, int tid, int Z, int8_t* soft, const uint32_t* edge, int8_t* c2v_row,
                                              int8_t* mbuf)
 {
@@ -187,24 +187,29 @@ __device__ __forceinline__ void row_dispatch(int deg, int tid, int Z, int8_t* so
     case 8: row_update<8, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
     case 9: row_update<9, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
     case 10: row_update<10, FIRST, ZT>(tid, Z, soft, edge, c2v_row); break;
-    default: row_update_wide<FIRST, ZT>(deg, tid, Z, soft, edge, c2v_row, mbuf); break;
+    default: row_update_wide<FIRST, ZT, NT>(deg, tid, Z, soft, edge, c2v_row, mbuf); break;
   }
 }
 
-struct smem_t {
-  __align__(16) int8_t soft[pg::kMaxNodes * pg::kMaxZ];
+// Shared memory of the one-lane decoder: NT threads, lifting sizes up to MAXZ (22 * MAXZ / 32 <= NT,
+// so that one thread per 32-bit hard-decision word covers the message).
+template <int NT, int MAXZ>
+struct smem_scalar_t {
+  __align__(16) int8_t soft[pg::kMaxNodes * MAXZ];
   uint32_t             edge[pg::kBg1Edges];
-  uint32_t             hard[(22 * pg::kMaxZ) / 32];
-  uint32_t             red[kThreads / 32];
-  int8_t               mbuf[pg::kMaxRowDegree * kThreads]; // v2c staging of the degree-19 rows
+  uint32_t             hard[(22 * MAXZ) / 32];
+  uint32_t             red[NT / 32];
+  int8_t               mbuf[pg::kMaxRowDegree * NT]; // v2c staging of the degree-19 rows
   int                  s_last;
   int                  s_done;
 };
+using smem_t = smem_scalar_t<kThreads, pg::kMaxZ>;
 
-// Decodes codeblock cb with check-to-variable slab `slab`; ZT > 0 specialises the lifting size
-// at compile time.
-template <int ZT>
-__device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm, const int8_t* __restrict__ llrs,
+// Decodes codeblock cb with check-to-variable slab `slab`, one lane per thread (NT threads, Z <=
+// MAXZ); ZT > 0 specialises the lifting size at compile time.
+template <int ZT, int NT, int MAXZ>
+__device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_scalar_t<NT, MAXZ>& sm,
+                                                 const int8_t* __restrict__ llrs,
                                                  uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
                                                  int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
                                                  const int cb, const int slab)
@@ -218,7 +223,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   const int        tid = threadIdx.x;
   const int        bg  = d.base_graph;
   const int        Z   = ZT > 0 ? ZT : (int)d.lifting_size;
-  const int        set = (Z >= 2 && Z <= pg::kMaxZ) ? dev_set_index(Z) : -1;
+  const int        set = (Z >= 2 && Z <= MAXZ) ? dev_set_index(Z) : -1;
   if ((bg != 1 && bg != 2) || set < 0) {
     if (tid == 0) {
       iterations[cb] = -1;
@@ -240,7 +245,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   const int     nwords   = (msg_len + 31) / 32;
 
   // Edge table of this lifting size: node offset (col * Z) and shift (V mod Z).
-  for (int e = tid; e < nedges; e += kThreads) {
+  for (int e = tid; e < nedges; e += NT) {
     const int col = c_edge_col[g][e];
     const int s   = c_edge_v[g][e][set] % Z;
     edge[e]       = ((uint32_t)(col * Z) << 16) | (uint32_t)s;
@@ -256,15 +261,15 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
   // ldpc_decoder_impl.cpp:66-71), four LLRs per thread step.
   const int nof_full = (n / Z) * Z;
   const int soft_len = nfull * Z;
-  for (int i = tid; i < 2 * Z; i += kThreads) {
+  for (int i = tid; i < 2 * Z; i += NT) {
     soft[i] = 0;
   }
-  for (int i = 2 * Z + n + tid; i < soft_len; i += kThreads) {
+  for (int i = 2 * Z + n + tid; i < soft_len; i += NT) {
     soft[i] = 0;
   }
   int        last    = 0;
   const bool aligned = (reinterpret_cast<uintptr_t>(in) & 3u) == 0;
-  for (int k0 = 4 * tid; k0 < n; k0 += 4 * kThreads) {
+  for (int k0 = 4 * tid; k0 < n; k0 += 4 * NT) {
     int v[4];
     if (aligned && k0 + 3 < n) {
       const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(in + k0));
@@ -295,7 +300,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
 
   const int input_size = s_last;
   if (input_size < msg_len) {
-    for (int b = tid; b < nbytes; b += kThreads) {
+    for (int b = tid; b < nbytes; b += NT) {
       out[b] = 0xff;
     }
     if (tid == 0) {
@@ -325,9 +330,9 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
       if (tid < Z) {
         int8_t* c2v_row = c2v + (size_t)e0 * Z + tid;
         if (it == 0) {
-          row_dispatch<true, ZT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+          row_dispatch<true, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
         } else {
-          row_dispatch<false, ZT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+          row_dispatch<false, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
         }
       }
       e0 += deg;
@@ -380,7 +385,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
     __syncthreads();
     if (tid == 0) {
       uint32_t t = 0;
-      for (int w = 0; w < kThreads / 32; ++w) {
+      for (int w = 0; w < NT / 32; ++w) {
         t ^= red[w];
       }
       s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
@@ -427,7 +432,7 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_t& sm
     result = (!bad && !zero) ? max_it : 0;
   }
 
-  for (int b = tid; b < nbytes; b += kThreads) {
+  for (int b = tid; b < nbytes; b += NT) {
     out[b] = (uint8_t)(hard[b >> 2] >> (24 - 8 * (b & 3)));
   }
   if (tid == 0) {
@@ -454,9 +459,9 @@ __global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_
   if (counter == nullptr) {
     const pg_ldpc_cb d = descs[blockIdx.x];
     if (d.lifting_size == 384) {
-      decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
+      decode_codeblock<384, kThreads, pg::kMaxZ>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
     } else {
-      decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
+      decode_codeblock<0, kThreads, pg::kMaxZ>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, blockIdx.x, blockIdx.x);
     }
     return;
   }
@@ -476,45 +481,61 @@ __global__ void __launch_bounds__(kThreads, 2) ldpc_decode_kernel(const pg_ldpc_
       continue; // left to ldpc_decode_x2_kernel
     }
     if (d.lifting_size == 384) {
-      decode_codeblock<384>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      decode_codeblock<384, kThreads, pg::kMaxZ>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
     } else {
-      decode_codeblock<0>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      decode_codeblock<0, kThreads, pg::kMaxZ>(d, sm, llrs, bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
     }
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Z = 384 decoder with two lifted lanes per thread. Thread j (0 <= j < 192) carries lanes j and
-// j + 192 as the two halves of one f16x2 register. Every value of the decoder is an integer of
-// magnitude at most 1,784 at any intermediate step, so f16 arithmetic (11-bit significand) on them
-// is exact, and the reference's int8 rules become exact f16x2 identities:
-//   v2c      = x == +-127 ? x : clamp(x - c, -120, 120)
-//            = min(max(clamp(x - c, -120, 120), 37x - 4572), 37x + 4572)   (fused multiply-adds;
-//              for |x| <= 120 the bounds lie outside [-120, 120], for x = +-127 they are +-127)
+// Two-lanes-per-thread decoder: one 192-thread CTA per codeblock, every lifting size.
+//
+// Pair mode (even Z > 192, H = Z / 2): thread j (0 <= j < H) carries check lanes j and j + H as
+// the two halves of one f16x2 register. For an edge of shift s the two variable lanes it reads,
+// (j + s) mod Z and (j + H + s) mod Z, differ by H, so soft bits live twice in shared memory and
+// the shifted pair is one 16-bit word: D[col][w] = (soft[col][w], soft[col][(w + H) mod Z]).
+// The reference's int8 rules become exact f16x2 identities:
+//   v2c      = x == +-127 ? x : clamp(x - c, -120, 120)       (reference)
+//   v        = min(max(clamp(x - c, -120, 120), 104x - 12984), 104x + 12984)  (fused
+//              multiply-adds; for |x| <= 120 the bounds lie outside [-120, 120], for x = +-127
+//              they are +-224; in the first iteration c = 0 and x is not clamped, and the bounds
+//              keep every |x| <= 126 as it is)
+//              so v = v2c, except that a saturated soft bit gives +-224 instead of +-127. Both
+//              exceed every magnitude the minimum search starts from (120) and keep the sign, so
+//              the row's minima, sign and messages are the same; and +-224 plus any message
+//              (|c2v| <= 96) stays above 120 in magnitude, so the soft update below gives +-127
+//              back without the reference's separate test of |v2c| == 127.
 //   min1/min2/sign: min.xorsign.abs keeps min(|.|) and accumulates the sign product in min1's sign
 //   c2v      = sign(product of the others) * (|v2c| == min1 ? s2 : s1),
-//              magnitude = s2 - (s2 - s1) * min(|v2c| - min1, 1), sign by XOR of sign bits
-//   soft     = |v2c| == 127 ? v2c : promote(c2v + v2c), promote(t) = clamp(8t - 7 clamp(t, +-120), +-127)
+//              magnitude = s2 + (s1 - s2) * (|v| != min1), the comparison as f16 1.0 / 0.0, sign by
+//              XOR of sign bits
+//   soft     = |v2c| == 127 ? v2c : promote(c2v + v2c) = promote(c2v + v),
+//              promote(t) = clamp(8t - 7 clamp(t, +-120), +-127)
 //   scale    s = (m * 52428) >> 16 from a table indexed by the f16 bit pattern of m over 16.
+// Every value used is an integer of magnitude at most 2,560 (even above 2,048), so f16 arithmetic
+// (11-bit significand) on it is exact; the bounds are exact where they decide (x = +-127).
 // Storage is int8 in offset binary (byte = value + 128): f16 bits 0x6400 | byte are 1024 + byte, so
 // one byte permute and one f16x2 subtraction of 1152 give the values, and an addition of 1152 and a
-// byte permute give the bytes back, exactly. Soft bits live twice in shared memory so that the
-// shifted pair of lanes is one 16-bit word: D[col][w] = (soft[col][w], soft[col][(w + 192) mod 384]);
-// check-to-variable messages are byte pairs per (edge, thread) in the global slab.
-constexpr int kX2Z       = 384;
-constexpr int kX2Half    = kX2Z / 2;
-constexpr int kX2Threads = kX2Half;
-constexpr int kScaleTab  = 1408;
-constexpr int kX2MaxPerSm = 4; // resident CTAs per SM (shared memory 55 KB, 80 registers)
+// byte permute give the bytes back, exactly. Check-to-variable messages are byte pairs per (edge,
+// thread) in the global slab.
+//
+// Scalar mode (Z <= 192): the one-lane arithmetic of ldpc_decode_kernel with 192 threads.
+constexpr int kX2Threads  = 192; // = kMaxZ / 2
+constexpr int kScaleTab   = 1408;
+constexpr int kX2MaxPerSm = 4;   // resident CTAs per SM (registers)
 
-struct smem_x2_t {
-  uint16_t D[pg::kMaxNodes * kX2Z];
-  uint32_t edge[pg::kBg1Edges];
-  uint32_t hard[(22 * kX2Z) / 32];
+struct __align__(16) smem_pair_t {
+  uint16_t D[pg::kMaxNodes * pg::kMaxZ]; // soft-bit pairs, column stride Z
+  uint32_t edge[pg::kBg1Edges];          // col*Z << 16 | s
+  uint32_t hard[(22 * pg::kMaxZ) / 32];
   uint32_t red[kX2Threads / 32];
   int      s_last;
   int      s_done;
 };
+using smem_x2_scalar_t = smem_scalar_t<kX2Threads, kX2Threads>;
+constexpr size_t kX2Smem = sizeof(smem_pair_t) > sizeof(smem_x2_scalar_t) ? sizeof(smem_pair_t)
+                                                                           : sizeof(smem_x2_scalar_t);
 
 __device__ __forceinline__ uint32_t h2_sub(uint32_t a, uint32_t b)
 {
@@ -570,20 +591,19 @@ constexpr uint32_t kH120    = 0x57805780u; // 120
 constexpr uint32_t kHm120   = 0xd780d780u; // -120
 constexpr uint32_t kH127    = 0x57f057f0u; // 127
 constexpr uint32_t kHm127   = 0xd7f0d7f0u; // -127
-constexpr uint32_t kH37     = 0x50a050a0u; // 37
-constexpr uint32_t kHm4572  = 0xec77ec77u; // -4572
-constexpr uint32_t kH4572   = 0x6c776c77u; // 4572
+constexpr uint32_t kH104    = 0x56805680u; // 104
+constexpr uint32_t kHm12984 = 0xf257f257u; // -12984
+constexpr uint32_t kH12984  = 0x72577257u; // 12984
 constexpr uint32_t kH8      = 0x48004800u; // 8
 constexpr uint32_t kHm7     = 0xc700c700u; // -7
-constexpr uint32_t kH1      = 0x3c003c00u; // 1
 constexpr uint32_t kH1152   = 0x64806480u; // 1152 = 1024 + 128
 constexpr uint32_t kAbs     = 0x7fff7fffu;
 constexpr uint32_t kSign    = 0x80008000u;
 
-// Offset-binary byte pair -> f16x2 integers, and back (low byte first).
+// Offset-binary byte pair -> f16x2 integers (low byte first).
 __device__ __forceinline__ uint32_t bytes_to_h2(uint32_t b)
 {
-  return h2_sub(__byte_perm(b, 0x6464u, 0x5140), kH1152);
+  return h2_sub(__byte_perm(b, 0x6464u, 0x5140u), kH1152);
 }
 __device__ __forceinline__ uint32_t h2_to_bytes_biased(uint32_t c)
 {
@@ -595,32 +615,53 @@ __device__ __forceinline__ uint32_t x2_scale(const uint16_t* __restrict__ tab, u
   return (uint32_t)__ldg(tab + ((m & 0xffffu) >> 4)) | ((uint32_t)__ldg(tab + (m >> 20)) << 16);
 }
 
-// Partner position of p (same node, w + 192 mod 384).
-__device__ __forceinline__ uint32_t x2_partner(uint32_t p)
+__device__ __forceinline__ uint32_t h2_ne(uint32_t a, uint32_t b)
 {
-  const uint32_t w = p % kX2Z;
-  return p - w + (w < (uint32_t)kX2Half ? w + kX2Half : w - kX2Half);
+  uint32_t r;
+  asm("set.ne.f16x2.f16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
 }
 
-template <int DEG, bool FIRST>
-__device__ __forceinline__ void row_update_x2(const int j, uint16_t* __restrict__ D, const uint32_t* __restrict__ edge,
-                                              uint16_t* __restrict__ c2v_row, const uint16_t* __restrict__ tab)
+// v2c of one edge (saturated soft bits as +-224) from its soft-bit pair x and its stored
+// check-to-variable pair.
+template <bool FIRST>
+__device__ __forceinline__ uint32_t pair_v2c(const uint32_t x, const uint16_t* __restrict__ c2v)
 {
-  uint32_t v[DEG];
-  uint32_t min1 = kH120, min2 = kH120;
+  uint32_t d = x;
+  if (!FIRST) {
+    d = h2_min(h2_max(h2_sub(x, bytes_to_h2(*c2v)), kHm120), kH120);
+  }
+  return h2_min(h2_max(d, h2_fma(x, kH104, kHm12984)), h2_fma(x, kH104, kH12984));
+}
+
+// One layer for thread j. Rows of degree up to 10 keep each edge's v2c, soft-bit position and
+// partner position from the first pass; the degree-19 rows keep the v2c of their first ten edges
+// and recompute the rest (the soft bits and messages they read are not yet overwritten), so that
+// they stay within the register budget of four CTAs per SM.
+template <int DEG, bool FIRST>
+__device__ __forceinline__ void row_update_pair(const unsigned j, const unsigned Z, const unsigned H,
+                                                uint16_t* __restrict__ D, const uint32_t* __restrict__ edge,
+                                                uint16_t* __restrict__ c2v_row, const uint16_t* __restrict__ tab)
+{
+  constexpr bool KEEP = DEG <= 10;
+  constexpr int  NV   = KEEP ? DEG : 10;
+  uint32_t       v[NV];
+  unsigned       pos[KEEP ? DEG : 1], par[KEEP ? DEG : 1];
+  uint32_t       min1 = kH120, min2 = kH120;
 #pragma unroll
   for (int e = 0; e < DEG; ++e) {
     const uint32_t ed = edge[e];
-    const unsigned p0 = (unsigned)j + (ed & 0xffffu);
-    const unsigned p  = min(p0, p0 - (unsigned)kX2Z) + (ed >> 16);
-    const uint32_t x  = bytes_to_h2(D[p]);
-    uint32_t       vv = x;
-    if (!FIRST) {
-      const uint32_t c = bytes_to_h2(c2v_row[e * kX2Half]);
-      const uint32_t d = h2_min(h2_max(h2_sub(x, c), kHm120), kH120);
-      vv               = h2_min(h2_max(d, h2_fma(x, kH37, kHm4572)), h2_fma(x, kH37, kH4572));
+    const unsigned p0 = j + (ed & 0xffffu);
+    const unsigned w  = min(p0, p0 - Z); // (j + s) mod Z
+    const unsigned p  = w + (ed >> 16);
+    if constexpr (KEEP) {
+      pos[e] = p;
+      par[e] = w < H ? p + H : p - H;
     }
-    v[e]             = vv;
+    const uint32_t vv = pair_v2c<FIRST>(bytes_to_h2(D[p]), c2v_row + e * kX2Threads);
+    if (e < NV) {
+      v[e < NV ? e : 0] = vv;
+    }
     const uint32_t t = h2_max_xs(min1, vv);
     min2             = h2_min_xs(min2, t);
     min1             = h2_min_xs(min1, vv);
@@ -628,63 +669,107 @@ __device__ __forceinline__ void row_update_x2(const int j, uint16_t* __restrict_
   const uint32_t m1  = min1 & kAbs;
   const uint32_t s1  = x2_scale(tab, m1);
   const uint32_t s2  = x2_scale(tab, min2 & kAbs);
-  const uint32_t nds = h2_sub(s1, s2); // -(s2 - s1)
+  const uint32_t nds = h2_sub(s1, s2);
   const uint32_t sgn = min1 & kSign;  // sign product of every v2c of the row
 #pragma unroll
   for (int e = 0; e < DEG; ++e) {
-    const uint32_t vv  = v[e];
-    const uint32_t k   = h2_min(h2_sub(vv & kAbs, m1), kH1);
-    const uint32_t mag = h2_fma(nds, k, s2);
+    unsigned p, q;
+    if constexpr (KEEP) {
+      p = pos[e];
+      q = par[e];
+    } else {
+      const uint32_t ed = edge[e];
+      const unsigned p0 = j + (ed & 0xffffu);
+      const unsigned w  = min(p0, p0 - Z);
+      p                 = w + (ed >> 16);
+      q                 = w < H ? p + H : p - H;
+    }
+    const uint32_t vv  = e < NV ? v[e < NV ? e : 0] : pair_v2c<FIRST>(bytes_to_h2(D[p]), c2v_row + e * kX2Threads);
+    const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
     const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
-    c2v_row[e * kX2Half] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+    c2v_row[e * kX2Threads] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
     const uint32_t t   = h2_add(c, vv);
     const uint32_t cl  = h2_min(h2_max(t, kHm120), kH120);
     uint32_t       u   = h2_fma(cl, kHm7, h2_mul(t, kH8));
     u                  = h2_min(h2_max(u, kHm127), kH127);
-    u                  = h2_min(h2_max(u, h2_fma(vv, kH37, kHm4572)), h2_fma(vv, kH37, kH4572));
     const uint32_t ub  = h2_to_bytes_biased(u);
-    const uint32_t ed  = edge[e];
-    const unsigned p0  = (unsigned)j + (ed & 0xffffu);
-    const unsigned p   = min(p0, p0 - (unsigned)kX2Z) + (ed >> 16);
-    D[p]               = (uint16_t)__byte_perm(ub, 0, 0x0020);
-    D[x2_partner(p)]   = (uint16_t)__byte_perm(ub, 0, 0x0002);
+    D[p] = (uint16_t)__byte_perm(ub, 0, 0x0020);
+    D[q] = (uint16_t)__byte_perm(ub, 0, 0x0002);
   }
 }
 
 template <bool FIRST>
-__device__ __forceinline__ void row_dispatch_x2(int deg, int j, uint16_t* D, const uint32_t* edge, uint16_t* c2v_row,
-                                                const uint16_t* tab)
+__device__ __forceinline__ void row_dispatch_pair(int deg, unsigned j, unsigned Z, unsigned H, uint16_t* D,
+                                                  const uint32_t* edge, uint16_t* c2v_row, const uint16_t* tab)
 {
   switch (deg) {
-    case 3: row_update_x2<3, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 4: row_update_x2<4, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 5: row_update_x2<5, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 6: row_update_x2<6, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 7: row_update_x2<7, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 8: row_update_x2<8, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 9: row_update_x2<9, FIRST>(j, D, edge, c2v_row, tab); break;
-    case 10: row_update_x2<10, FIRST>(j, D, edge, c2v_row, tab); break;
-    default: row_update_x2<19, FIRST>(j, D, edge, c2v_row, tab); break;
+    case 3: row_update_pair<3, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 4: row_update_pair<4, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 5: row_update_pair<5, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 6: row_update_pair<6, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 7: row_update_pair<7, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 8: row_update_pair<8, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 9: row_update_pair<9, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    case 10: row_update_pair<10, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
+    default: row_update_pair<19, FIRST>(j, Z, H, D, edge, c2v_row, tab); break;
   }
 }
 
-// Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`.
-__device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const int8_t* __restrict__ llrs,
-                                    uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
-                                    int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
-                                    const uint16_t* __restrict__ scale_tab, const int cb, const int slab)
+// Eight input LLRs from index k (any k; outside [0, n) they are zero) as soft bits in offset
+// binary, four per word: whole nodes (index < nof_full) clamped to +-64, a ragged tail as is
+// (ldpc_decoder_impl.cpp:147-188). last: one past the last non-zero LLR seen (the trailing-zero trim,
+// ldpc_decoder_impl.cpp:66-71).
+__device__ __forceinline__ void fetch8(const int8_t* __restrict__ in, int k, int n, int nof_full, bool aligned,
+                                       int& last, uint32_t& w0, uint32_t& w1)
 {
-  constexpr int Z   = kX2Z;
-  const int     tid = threadIdx.x;
-  const int     bg  = d.base_graph;
-  if (bg != 1 && bg != 2) {
+  int v[8];
+  if (aligned && k >= 0 && k + 8 <= n) {
+    const uint2 q = __ldg(reinterpret_cast<const uint2*>(in + k));
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      v[i]     = (int)(int8_t)(q.x >> (8 * i));
+      v[i + 4] = (int)(int8_t)(q.y >> (8 * i));
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = (k + i >= 0 && k + i < n) ? (int)__ldg(in + k + i) : 0;
+    }
+  }
+  w0 = 0;
+  w1 = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int kk = k + i;
+    last         = v[i] != 0 ? kk + 1 : last;
+    const int x  = kk < nof_full ? max(-64, min(64, v[i])) : v[i];
+    const uint32_t b = (uint32_t)(x + 128);
+    if (i < 4) {
+      w0 |= b << (8 * i);
+    } else {
+      w1 |= b << (8 * (i - 4));
+    }
+  }
+}
+
+// Decodes codeblock cb (even Z > 192) with check-to-variable slab `slab`.
+__device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, const int8_t* __restrict__ llrs,
+                                      uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
+                                      int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
+                                      const uint16_t* __restrict__ scale_tab, const int cb, const int slab)
+{
+  const int tid = threadIdx.x;
+  const int bg  = d.base_graph;
+  const int Z   = (int)d.lifting_size;
+  const int H   = Z >> 1;
+  const int set = (Z <= pg::kMaxZ) ? dev_set_index(Z) : -1;
+  if ((bg != 1 && bg != 2) || set < 0 || (Z & 15) != 0) {
     if (tid == 0) {
       iterations[cb] = -1;
     }
     return;
   }
   const int     g        = bg - 1;
-  const int     set      = 1; // Z = 384 = 3 * 2^7: set index 1 (a = 3)
   const int     Kb       = bg == 1 ? 22 : 10;
   const int     nrows    = bg == 1 ? pg::kBg1Rows : pg::kBg2Rows;
   const int     nedges   = bg == 1 ? pg::kBg1Edges : pg::kBg2Edges;
@@ -708,32 +793,41 @@ __device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const in
     sm.s_last = 0;
     sm.s_done = 0;
   }
-  // Trailing-zero trim (ldpc_decoder_impl.cpp:66-71): the last non-zero LLR.
-  int last = 0;
-  for (int k = tid; k < n; k += kX2Threads) {
-    last = in[k] != 0 ? k + 1 : last;
-  }
-  last = warp_max(last);
   __syncthreads();
-  if ((tid & 31) == 0 && last > 0) {
-    atomicMax(&sm.s_last, last);
-  }
-  // Soft bits (2Z punctured zeros, whole nodes clamped to +-64, a ragged tail as is, zeros after),
-  // both copies of each pair, offset binary.
-  const int nof_full = (n / Z) * Z;
-  auto soft_in = [&](int i) -> uint32_t {
-    const int k = i - 2 * Z;
-    int       v = 0;
-    if (k >= 0 && k < n) {
-      v = in[k];
-      v = k < nof_full ? max(-64, min(64, v)) : v;
+
+  // Soft bits, eight lanes of each half of a column per thread step (2Z punctured zeros, then the
+  // input), both copies: D[col][w0 + i] = (soft[w0 + i], soft[w0 + H + i]) and the swapped pair at
+  // w0 + H + i.
+  {
+    const int  per_col  = H / 8;
+    const int  nchunks  = nfull * per_col;
+    const int  nof_full = (n / Z) * Z;
+    const bool aligned  = (reinterpret_cast<uintptr_t>(in) & 7u) == 0;
+    int        last     = 0;
+#pragma unroll 4
+    for (int q = tid; q < nchunks; q += kX2Threads) {
+      const int col = q / per_col;
+      const int w0  = (q - col * per_col) * 8;
+      const int k   = (col - 2) * Z + w0;
+      uint32_t  l0, l1, h0, h1;
+      fetch8(in, k, n, nof_full, aligned, last, l0, l1);
+      fetch8(in, k + H, n, nof_full, aligned, last, h0, h1);
+      uint4 lo, hi;
+      lo.x = __byte_perm(l0, h0, 0x5140);
+      lo.y = __byte_perm(l0, h0, 0x7362);
+      lo.z = __byte_perm(l1, h1, 0x5140);
+      lo.w = __byte_perm(l1, h1, 0x7362);
+      hi.x = __byte_perm(h0, l0, 0x5140);
+      hi.y = __byte_perm(h0, l0, 0x7362);
+      hi.z = __byte_perm(h1, l1, 0x5140);
+      hi.w = __byte_perm(h1, l1, 0x7362);
+      *reinterpret_cast<uint4*>(D + col * Z + w0)     = lo;
+      *reinterpret_cast<uint4*>(D + col * Z + w0 + H) = hi;
     }
-    return (uint32_t)(v + 128);
-  };
-  for (int i = tid; i < nfull * Z; i += kX2Threads) {
-    const int col = i / Z, w = i - col * Z;
-    const int w2  = w < kX2Half ? w + kX2Half : w - kX2Half;
-    D[i]          = (uint16_t)(soft_in(col * Z + w) | (soft_in(col * Z + w2) << 8));
+    last = warp_max(last);
+    if ((tid & 31) == 0 && last > 0) {
+      atomicMax(&sm.s_last, last);
+    }
   }
   __syncthreads();
 
@@ -745,6 +839,7 @@ __device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const in
     if (tid == 0) {
       iterations[cb] = 0;
     }
+    __syncthreads();
     return;
   }
   int cb_len = max(input_size + 2 * Z, (Kb + 4) * Z);
@@ -758,18 +853,21 @@ __device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const in
   const uint32_t* pow_tab = crc_pow + (size_t)(crc_poly <= PG_CRC24B ? crc_poly : 0) * pg::kCrcPowLen;
   const int       crc_len = msg_len - (int)d.nof_filler_bits;
 
-  int       result = 0;
-  const int max_it = d.max_iterations;
-  const int lane   = tid & 31;
+  int            result = 0;
+  const int      max_it = d.max_iterations;
+  const int      lane   = tid & 31;
+  const unsigned j      = (unsigned)tid;
   for (int it = 0; it < max_it; ++it) {
     int e0 = 0;
     for (int r = 0; r < nof_layers; ++r) {
-      const int deg     = c_row_deg[g][r];
-      uint16_t* c2v_row = c2v + (size_t)e0 * kX2Half + tid;
-      if (it == 0) {
-        row_dispatch_x2<true>(deg, tid, D, sm.edge + e0, c2v_row, scale_tab);
-      } else {
-        row_dispatch_x2<false>(deg, tid, D, sm.edge + e0, c2v_row, scale_tab);
+      const int deg = c_row_deg[g][r];
+      if (tid < H) {
+        uint16_t* c2v_row = c2v + (size_t)e0 * kX2Threads + tid;
+        if (it == 0) {
+          row_dispatch_pair<true>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+        } else {
+          row_dispatch_pair<false>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+        }
       }
       e0 += deg;
       __syncthreads();
@@ -816,21 +914,22 @@ __device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const in
   if (crc_poly == PG_CRC_NONE) {
     // Syndrome check over the processed rows (ldpc_decoder_impl.cpp:329-387), both lanes.
     int bad = 0;
-    int e0  = 0;
-    for (int r = 0; r < nof_layers; ++r) {
-      const int deg    = c_row_deg[g][r];
-      uint32_t  parity = 0;
-      for (int e = 0; e < deg; ++e) {
-        const uint32_t ed = sm.edge[e0 + e];
-        int            p  = tid + (int)(ed & 0xffffu);
-        p                 = (p >= Z) ? p - Z : p;
-        const uint32_t x  = D[p + (int)(ed >> 16)];
-        const uint32_t lo = x & 0xffu, hi = x >> 8;
-        bad |= (lo == 128u) | (hi == 128u);
-        parity ^= (uint32_t)(lo <= 128u) | ((uint32_t)(hi <= 128u) << 1);
+    if (tid < H) {
+      int e0 = 0;
+      for (int r = 0; r < nof_layers; ++r) {
+        const int deg    = c_row_deg[g][r];
+        uint32_t  parity = 0;
+        for (int e = 0; e < deg; ++e) {
+          const uint32_t ed = sm.edge[e0 + e];
+          const unsigned p0 = j + (ed & 0xffffu);
+          const uint32_t x  = D[min(p0, p0 - (unsigned)Z) + (ed >> 16)];
+          const uint32_t lo = x & 0xffu, hi = x >> 8;
+          bad |= (lo == 128u) | (hi == 128u);
+          parity ^= (uint32_t)(lo <= 128u) | ((uint32_t)(hi <= 128u) << 1);
+        }
+        bad |= parity != 0;
+        e0 += deg;
       }
-      bad |= parity != 0;
-      e0 += deg;
     }
     bad      = __syncthreads_or(bad);
     int zero = 0;
@@ -850,21 +949,20 @@ __device__ void decode_codeblock_x2(const pg_ldpc_cb& d, smem_x2_t& sm, const in
   __syncthreads();
 }
 
-// Persistent decoder of the Z = 384 codeblocks of a work list (the others are left to
-// ldpc_decode_kernel): each CTA takes the next work index from *counter, skips codeblocks of other
-// lifting sizes, and decodes with slab blockIdx.x.
-__global__ void __launch_bounds__(kX2Threads, 4) ldpc_decode_x2_kernel(const pg_ldpc_cb* __restrict__ descs,
-                                                                       const int8_t* __restrict__ llrs,
-                                                                       uint8_t* __restrict__ bits,
-                                                                       int32_t* __restrict__ iterations,
-                                                                       int8_t* __restrict__ c2v_all,
-                                                                       const uint32_t* __restrict__ crc_pow,
-                                                                       const uint16_t* __restrict__ scale_tab,
-                                                                       const uint32_t* __restrict__ order, int n,
-                                                                       int* __restrict__ counter)
+// Persistent decoder of a work list, every lifting size: each CTA takes the next work index from
+// *counter, decodes codeblock order[w] (or w) in pair mode (even Z > 192) or scalar mode (Z <= 192)
+// with slab blockIdx.x, and stops when the n codeblocks are taken.
+__global__ void __launch_bounds__(kX2Threads, kX2MaxPerSm) ldpc_decode_x2_kernel(const pg_ldpc_cb* __restrict__ descs,
+                                                                        const int8_t* __restrict__ llrs,
+                                                                        uint8_t* __restrict__ bits,
+                                                                        int32_t* __restrict__ iterations,
+                                                                        int8_t* __restrict__ c2v_all,
+                                                                        const uint32_t* __restrict__ crc_pow,
+                                                                        const uint16_t* __restrict__ scale_tab,
+                                                                        const uint32_t* __restrict__ order, int n,
+                                                                        int* __restrict__ counter)
 {
   extern __shared__ __align__(16) unsigned char smem_x2_raw[];
-  smem_x2_t& sm = *reinterpret_cast<smem_x2_t*>(smem_x2_raw);
   __shared__ int s_work;
   for (;;) {
     if (threadIdx.x == 0) {
@@ -878,8 +976,13 @@ __global__ void __launch_bounds__(kX2Threads, 4) ldpc_decode_x2_kernel(const pg_
     }
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
-    if (d.lifting_size == kX2Z) {
-      decode_codeblock_x2(d, sm, llrs, bits, iterations, c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
+    if (d.lifting_size > kX2Threads) {
+      decode_codeblock_pair(d, *reinterpret_cast<smem_pair_t*>(smem_x2_raw), llrs, bits, iterations, c2v_all,
+                            crc_pow, scale_tab, cb, blockIdx.x);
+    } else {
+      decode_codeblock<0, kX2Threads, kX2Threads>(d, *reinterpret_cast<smem_x2_scalar_t*>(smem_x2_raw), llrs, bits,
+                                                  iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      __syncthreads();
     }
   }
 }
@@ -947,7 +1050,7 @@ int ldpc_upload_tables(pg_context* ctx)
   if (rc == PG_OK) {
     rc = check_cuda(ctx,
                     cudaFuncSetAttribute(ldpc_decode_x2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(smem_x2_t)),
+                                         (int)kX2Smem),
                     "cudaFuncSetAttribute(ldpc_decode_x2_kernel)");
   }
   if (rc == PG_OK) {
@@ -1017,23 +1120,19 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  // With PG_LDPC_ROUTE_X2 the Z = 384 codeblocks go to the two-lanes-per-thread kernel and the
-  // others to ldpc_decode_kernel, both walking the same work list with their own counters and
-  // slabs 0 .. grid - 1; without it ldpc_decode_kernel decodes them all.
-  // ldpc_decode_kernel holds ldpc_ctas CTAs on the device (two per SM), the x2 kernel four per SM;
-  // the caller provides a slab per CTA (min(n, max_ctas) slabs).
-  const int grid    = std::max(1, std::min(n, std::min(max_ctas, ctx->ldpc_ctas)));
-  const int grid_x2 = std::max(1, std::min(n, std::min(max_ctas, kX2MaxPerSm * ctx->sm_count)));
-  int       rc      = PG_OK;
-  const bool x2 = (kinds & PG_LDPC_KIND_Z384) && (kinds & PG_LDPC_ROUTE_X2);
-  if (x2) {
-    ldpc_decode_x2_kernel<<<grid_x2, kX2Threads, sizeof(smem_x2_t), stream>>>(
+  // With PG_LDPC_ROUTE_X2 the two-lanes-per-thread kernel decodes every codeblock (four CTAs per
+  // SM); without it ldpc_decode_kernel does (two per SM). The caller provides a slab per CTA
+  // (min(n, max_ctas) slabs, max_ctas <= four per SM).
+  int rc = PG_OK;
+  if (kinds & PG_LDPC_ROUTE_X2) {
+    const int grid_x2 = std::max(1, std::min(n, std::min(max_ctas, kX2MaxPerSm * ctx->sm_count)));
+    ldpc_decode_x2_kernel<<<grid_x2, kX2Threads, kX2Smem, stream>>>(
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
     rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_x2_kernel launch");
-  }
-  if (rc == PG_OK && ((kinds & PG_LDPC_KIND_OTHER) || ((kinds & PG_LDPC_KIND_Z384) && !x2))) {
+  } else {
+    const int grid = std::max(1, std::min(n, std::min(max_ctas, ctx->ldpc_ctas)));
     ldpc_decode_kernel<<<grid, kThreads, 0, stream>>>(descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, order,
-                                                      n, counter, x2 ? kX2Z : 0);
+                                                      n, counter, 0);
     rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch");
   }
   if (ctx->timed) {

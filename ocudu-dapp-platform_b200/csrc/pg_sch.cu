@@ -344,7 +344,7 @@ int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t no
       l.max_iterations  = tb.max_iterations;
       w.ldpc.push_back(l);
       w.cb_bit_off.push_back((uint32_t)(w.bits_total * 8));
-      w.rm_total += N;
+      w.rm_total += (N + 15u) & ~15u; // 16-byte aligned codeblocks: vector loads in the decoder
       w.bits_total += (sg.cb_length + 7) / 8;
       cw_off += e;
     }

@@ -35,7 +35,7 @@ def test_golden_batch_bit_exact(batch_decoder):
 def random_jobs(seed, n):
     rng = np.random.default_rng(seed)
     jobs = []
-    zs = [8, 13, 16, 26, 36, 64, 72, 104, 120, 176, 208, 240, 256, 288, 320, 352, 384]  # small Z: golden cases
+    zs = [8, 13, 16, 26, 36, 64, 72, 104, 120, 176, 192, 208, 224, 240, 256, 288, 320, 352, 384]
     for t in range(n):
         bg = int(rng.integers(1, 3))
         z = int(rng.choice(zs))
@@ -154,14 +154,15 @@ def test_capacity_rejected(ctx):
     small.ctx.close()
 
 
-def test_z384_saturation_and_short_inputs_match_port(batch_decoder, port):
-    """Z = 384 codeblocks (the two-lanes-per-thread decoder) at high SNR, where soft bits saturate to
-    +-127 and the infinity rules decide, with fillers, every CRC and trimmed or too-short inputs."""
+def test_pair_mode_saturation_and_short_inputs_match_port(batch_decoder, port):
+    """Lifting sizes above 192 (the pair mode of the two-lanes-per-thread decoder) at high SNR, where
+    soft bits saturate to +-127 and the infinity rules decide, with fillers, every CRC and trimmed or
+    too-short inputs."""
     rng = np.random.default_rng(384)
     jobs = []
-    for t in range(48):
+    for t in range(64):
         bg = 1 + (t & 1)
-        z = 384
+        z = [384, 208, 224, 240, 256, 288, 320, 352][(t >> 1) % 8]
         k = golden_io.kbits(bg, z)
         nn = (66 if bg == 1 else 50) * z
         poly = [0, 1, 2, 255][t % 4]

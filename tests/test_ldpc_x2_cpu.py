@@ -27,17 +27,59 @@ def fma16(a, b, c):
     return np.float16(np.float64(a) * np.float64(b) + np.float64(c))
 
 
+def kernel_v(x, c, first):
+    """The decoder's v (arrays): clamp(x - c) (not in the first iteration) bounded by
+    104x -+ 12984, each step rounded to f16 as the f16x2 instructions do."""
+    x16 = x.astype(np.float16)
+    d = x16 if first else np.clip(x16 - c.astype(np.float16), -120, 120).astype(np.float16)
+    lo = (x.astype(np.float64) * 104 - 12984).astype(np.float16)
+    hi = (x.astype(np.float64) * 104 + 12984).astype(np.float16)
+    return np.minimum(np.maximum(d, lo), hi)
+
+
+def kernel_soft(v, cnew):
+    t = (cnew.astype(np.float16) + v.astype(np.float16)).astype(np.float16)
+    cl = np.clip(t, -120, 120).astype(np.float16)
+    t8 = (t * np.float16(8)).astype(np.float16)
+    return np.clip((cl.astype(np.float64) * -7 + t8.astype(np.float64)).astype(np.float16), -127, 127)
+
+
 def test_identities_exact():
-    for x in list(range(-120, 121)) + [127, -127]:
-        lo, hi = fma16(x, 37, -4572), fma16(x, 37, 4572)
-        for c in range(-96, 97):
-            d = np.clip(np.float16(x) - np.float16(c), -120, 120)
-            v = min(max(d, lo), hi)
-            assert v == (x if abs(x) == 127 else max(-120, min(120, x - c))), (x, c)
-    for t in range(-223, 224):
+    """Over the reference's LLR domain ([-120, 120] and +-127; raw first-iteration tails up to
+    +-126 too) and every stored message c and new message cnew (|.| <= 96): the decoder's v equals
+    the reference's v2c except +-224 for +-127, which acts the same in the minimum search (start
+    120) and in the message magnitude test, and the soft update gives the reference's value."""
+    dom = np.array(list(range(-120, 121)) + [127, -127])
+    cnew = np.arange(-96, 97)
+    for first in (True, False):
+        xs = np.array(list(range(-126, 127)) + [127, -127]) if first else dom
+        cs = np.array([0]) if first else np.arange(-96, 97)
+        x, c = np.meshgrid(xs, cs, indexing="ij")
+        x, c = x.ravel(), c.ravel()
+        ref = x if first else np.where(np.abs(x) == 127, x, np.clip(x - c, -120, 120))
+        v = kernel_v(x, c, first).astype(np.float64)
+        sat = np.abs(ref) == 127
+        assert np.array_equal(v[sat], 224.0 * np.sign(ref[sat]))
+        assert np.array_equal(v[~sat], ref[~sat].astype(np.float64))
+        # Soft update for every new message.
+        vv, rr = np.repeat(v, cnew.size), np.repeat(ref, cnew.size)
+        cc = np.tile(cnew, v.size)
+        t = cc + rr
+        want = np.where(np.abs(rr) == 127, rr, np.where(t > 120, 127, np.where(t < -120, -127, t)))
+        got = kernel_soft(vv, cc).astype(np.float64)
+        assert np.array_equal(got, want.astype(np.float64))
+    # promote(t) = clamp(8t - 7 clamp(t, +-120), +-127) for every t the update can see.
+    for t in range(-320, 321):
         cl = np.clip(np.float16(t), -120, 120)
         u = np.clip(fma16(cl, -7, np.float16(t) * np.float16(8)), -127, 127)
         assert u == (127 if t > 120 else (-127 if t < -120 else t)), t
+    # The message magnitude: s2 + (s1 - s2) * (|v| != min1) picks s2 exactly when |v| == min1.
+    for m1 in range(0, 121):
+        for a in list(range(0, 121)) + [224]:
+            ne = np.float16(1.0 if np.float16(a) != np.float16(m1) else 0.0)
+            for s1, s2 in ((0, 0), (3, 7), (96, 96), (40, 95)):
+                mag = fma16(np.float16(s1) - np.float16(s2), ne, s2)
+                assert mag == (s2 if a == m1 else s1)
     for b in range(1, 256):  # offset-binary byte <-> f16 through 1024 + byte
         v = np.float16(np.array([0x6400 | b], np.uint16).view(np.float16)[0]) - np.float16(1152)
         assert v == b - 128
@@ -45,3 +87,71 @@ def test_identities_exact():
         assert back == b
     keys = [f16_bits(m) >> 4 for m in range(128)]
     assert len(set(keys)) == 128 and max(keys) < 1408
+
+
+LIFTING_ABOVE_192 = [208, 224, 240, 256, 288, 320, 352, 384]
+
+
+def pair_pos(ed, j, H):
+    """The decoder's pair_pos: shared-memory pair index | swapped << 16 (32-bit unsigned)."""
+    t = j + (ed & 0xFF)
+    u = (t - H) & 0xFFFFFFFF
+    w = min(t, u)
+    sw = ((ed >> 8) ^ (1 if u < t else 0)) & 1
+    return ((ed >> 9) + w) | (sw << 16)
+
+
+def test_pair_store_addressing_covers_both_lanes():
+    """Pair mode: for every lifting size above 192, every shift and every thread j < Z/2, the
+    pair read for an edge holds variable lanes (j + s) mod Z (low half after the swap) and
+    (j + Z/2 + s) mod Z (high half), and the threads of a row touch disjoint pairs."""
+    for Z in LIFTING_ABOVE_192:
+        H = Z // 2
+        assert H % 8 == 0 and Z % 16 == 0
+        col = 5
+        for s in range(Z):
+            f = 1 if s >= H else 0
+            ed = ((col * 192) << 9) | (f << 8) | (s - f * H)
+            seen = set()
+            for j in range(H):
+                p = pair_pos(ed, j, H)
+                idx, sw = p & 0xFFFF, p >> 16
+                wp = idx - col * 192
+                assert 0 <= wp < H
+                lanes = (wp, wp + H)  # D[col][w'] = (soft[w'], soft[w' + H])
+                lo, hi = (lanes[1], lanes[0]) if sw else lanes
+                assert lo == (j + s) % Z and hi == (j + H + s) % Z, (Z, s, j)
+                assert idx not in seen
+                seen.add(idx)
+
+
+def test_pair_soft_byte_column_division_exact():
+    """(i * ceil(2^24 / Z)) >> 24 is i // Z for every message bit i of both base graphs."""
+    for Z in LIFTING_ABOVE_192:
+        inv = ((1 << 24) + Z - 1) // Z
+        i = np.arange(22 * Z, dtype=np.int64)
+        assert ((i * inv) < 2 ** 32).all()
+        assert np.array_equal((i * inv) >> 24, i // Z)
+
+
+def test_pair_fill_layout():
+    """The soft-bit fill: chunk q of eight pairs (column q // (H/8)) reads LLR indices k .. k+7 and
+    k+H .. k+H+7 with k = (col - 2) Z + w0, and writes pairs D[col*192 + w0 + i] = (k + i, k + H + i);
+    over all chunks this is every soft bit of the nfull columns exactly once."""
+    for Z in LIFTING_ABOVE_192:
+        H = Z // 2
+        per_col = H // 8
+        for nfull in (68, 52):
+            got = {}
+            for q in range(nfull * per_col):
+                col = q // per_col
+                w0 = (q - col * per_col) * 8
+                k = (col - 2) * Z + w0
+                for i in range(8):
+                    got[col * 192 + w0 + i] = (k + i, k + H + i)
+            soft = set()
+            for idx, (a, b) in got.items():
+                col, wp = divmod(idx, 192)
+                assert a == col * Z + wp - 2 * Z and b == a + H
+                soft.update((a, b))
+            assert soft == set(range(-2 * Z, (nfull - 2) * Z))
