@@ -554,6 +554,67 @@ int pg_pusch_estimate_ls_device(pg_context* ctx, const pg_pusch_ue* ues, int nof
  * execution. */
 int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t* use);
 
+
+/* ---------------------------------------------------------------------------------------------
+ * UCI on PUSCH: HARQ-ACK and CSI Part 1 of up to 11 bits (short block codes). Messages of more
+ * than 11 bits (polar codes) and CSI Part 2 are not supported (PG_ERR_INVALID). */
+
+/* One codeword to demultiplex: the fields of ulsch_demultiplex::configuration
+ * (include/ocudu/phy/upper/channel_processors/pusch/ulsch_demultiplex.h:31-58) plus the buffers.
+ * The encoded sizes are multiples of modulation_order * nof_layers (as get_ulsch_information,
+ * lib/ran/pusch/ulsch_info.cpp, produces them). */
+typedef struct pg_ulsch_demux_config {
+  uint32_t llr_offset;             /* descrambled codeword soft bits of this PDU in the input */
+  uint32_t nof_llrs;               /* codeword soft bits of the allocation (checked) */
+  uint32_t sch_offset;             /* output offsets, soft bits */
+  uint32_t harq_ack_offset;
+  uint32_t csi_part1_offset;
+  uint32_t c_init;                 /* scrambling initial state, RNTI * 2^15 + n_ID (placeholders) */
+  uint32_t nof_harq_ack_rvd;       /* reserved HARQ-ACK soft bits, G^HARQ-ACK_rvd */
+  uint32_t nof_enc_harq_ack_bits;  /* G^HARQ-ACK */
+  uint32_t nof_enc_csi_part1_bits; /* G^CSI-1 */
+  uint16_t nof_prb;
+  uint16_t dmrs_symbol_mask;       /* bit s: slot symbol s carries DM-RS */
+  uint8_t  modulation_order;       /* 1, 2, 4, 6, 8 */
+  uint8_t  nof_layers;             /* 1..4 */
+  uint8_t  start_symbol_index;
+  uint8_t  nof_symbols;
+  uint8_t  dmrs_type;              /* 1 or 2 */
+  uint8_t  nof_cdm_groups_without_data;
+  uint8_t  nof_harq_ack_bits;      /* O^HARQ-ACK, 0..11 */
+  uint8_t  nof_csi_part1_bits;     /* O^CSI-1, 0..11 */
+} pg_ulsch_demux_config;
+
+/* Soft bits of the UL-SCH, HARQ-ACK and CSI Part 1 streams of one codeword (host computation, no
+ * GPU): sizes[0..2]. PG_ERR_INVALID when the configuration is inconsistent or unsupported. */
+int pg_ulsch_demultiplex_sizes(const pg_ulsch_demux_config* cfg, uint32_t* sizes);
+
+/* Demultiplexes n codewords of descrambled soft bits (device llrs, as pg_pusch_demodulate_device
+ * writes them) into UL-SCH, HARQ-ACK and CSI Part 1 streams (device buffers; the UCI ones may be
+ * NULL when no PDU carries that field) - ulsch_demultiplex::demultiplex followed by the codeword's
+ * blocks (lib/phy/upper/channel_processors/pusch/ulsch_demultiplex_impl.cpp:183-573): one- and
+ * two-bit messages get their placeholder bits re-scrambled, and the REs of one- and two-bit
+ * HARQ-ACK are zero in the UL-SCH stream. cfgs is a host array. */
+int pg_ulsch_demultiplex_device(pg_context* ctx, const pg_ulsch_demux_config* cfgs, int n, const int8_t* llrs,
+                                int8_t* sch, int8_t* harq_ack, int8_t* csi_part1, void* stream);
+
+/* One short-block UCI message: short_block_detector::detect
+ * (include/ocudu/phy/upper/channel_coding/short/short_block_detector.h), called by
+ * uci_decoder_impl::decode for 1..11 bits (lib/phy/upper/channel_processors/uci/uci_decoder_impl.cpp:101-111). */
+typedef struct pg_uci_short_block {
+  uint32_t llr_offset; /* demultiplexed soft bits */
+  uint32_t nof_llrs;   /* E */
+  uint32_t out_offset; /* nof_bits output bytes, one bit per byte */
+  uint8_t  nof_bits;   /* 1..11 */
+  uint8_t  modulation_order;
+  uint8_t  reserved[2];
+} pg_uci_short_block;
+
+/* Detects n messages (items: host array; llrs, bits, valid: device buffers). valid[i] = 1 when the
+ * reference's detection test passes; an invalid input span gives all-ones bits and valid 0. */
+int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* items, int n, const int8_t* llrs,
+                                     uint8_t* bits, uint8_t* valid, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -343,6 +343,9 @@ int pg_create(const pg_config* cfg, pg_context** out)
   if (rc == PG_OK) {
     rc = est_upload_tables(ctx);
   }
+  if (rc == PG_OK) {
+    rc = uci_upload_tables(ctx);
+  }
   if (rc == PG_OK && cfg->max_llrs > 0) {
     rc = ensure_host_capacity(ctx, (size_t)cfg->max_llrs, (size_t)cfg->max_codeblocks * ((22 * kMaxZ) / 8));
   }

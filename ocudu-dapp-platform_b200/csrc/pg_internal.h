@@ -87,7 +87,7 @@ struct pg_context {
   bool                le_recorded    = false;
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
-  pg::staging_slot    slots[5];                  // rate-dematch, CRC, TB, PUSCH and UE work lists
+  pg::staging_slot    slots[7];                  // rate-dematch, CRC, TB, PUSCH, UE and UCI work lists
   void*               scratch_a      = nullptr;  // growable device scratch of the _host entries
   size_t              scratch_a_cap  = 0;
   void*               scratch_b      = nullptr;
@@ -106,8 +106,9 @@ int validate_ldpc_descs(pg_context* ctx, const pg_ldpc_cb* cbs, int n, size_t no
 
 // Uploads the constant base-graph tables (once per process and device).
 int ldpc_upload_tables(pg_context* ctx);
+int uci_upload_tables(pg_context* ctx);
 
-enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4 };
+enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4, SLOT_UCI = 5, SLOT_UCI_SHORT = 6 };
 
 // Copies `bytes` of host descriptors to the slot's device buffer on stream s (growing it when
 // needed); returns the device pointer in *dev. release_slot_after marks the slot busy until the

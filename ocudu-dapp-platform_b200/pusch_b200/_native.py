@@ -85,6 +85,23 @@ class PgPuschPlanTuning(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PgUlschDemuxConfig(ctypes.Structure):
+    _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("sch_offset", ctypes.c_uint32),
+                ("harq_ack_offset", ctypes.c_uint32), ("csi_part1_offset", ctypes.c_uint32),
+                ("c_init", ctypes.c_uint32), ("nof_harq_ack_rvd", ctypes.c_uint32),
+                ("nof_enc_harq_ack_bits", ctypes.c_uint32), ("nof_enc_csi_part1_bits", ctypes.c_uint32),
+                ("nof_prb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16),
+                ("modulation_order", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8),
+                ("start_symbol_index", ctypes.c_uint8), ("nof_symbols", ctypes.c_uint8), ("dmrs_type", ctypes.c_uint8),
+                ("nof_cdm_groups_without_data", ctypes.c_uint8), ("nof_harq_ack_bits", ctypes.c_uint8),
+                ("nof_csi_part1_bits", ctypes.c_uint8)]
+
+
+class PgUciShortBlock(ctypes.Structure):
+    _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("out_offset", ctypes.c_uint32),
+                ("nof_bits", ctypes.c_uint8), ("modulation_order", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 2)]
+
+
 class PgPuschPlanInfo(ctypes.Structure):
     _fields_ = [("nof_ues", ctypes.c_uint32), ("nof_codeblocks", ctypes.c_uint32), ("tb_bytes", ctypes.c_uint64),
                 ("nof_llrs", ctypes.c_uint64), ("grid_words", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
@@ -156,6 +173,9 @@ SIGNATURES = {
     "pg_pusch_estimate_ls_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),
     "pg_pusch_plan_set_harq": (ctypes.c_int, [_VP, _VP, _VP]),
+    "pg_ulsch_demultiplex_sizes": (ctypes.c_int, [_VP, _VP]),
+    "pg_ulsch_demultiplex_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_uci_short_block_detect_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),

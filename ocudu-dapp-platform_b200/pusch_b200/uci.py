@@ -1,0 +1,99 @@
+"""UCI on PUSCH: UL-SCH demultiplexing of HARQ-ACK and CSI Part 1 and short-block detection,
+mirroring the reference's ulsch_demultiplex
+(include/ocudu/phy/upper/channel_processors/pusch/ulsch_demultiplex.h:31-90) and
+short_block_detector (include/ocudu/phy/upper/channel_coding/short/short_block_detector.h) over
+the library's GPU entries."""
+import ctypes
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from . import _native
+from ._native import PgUciShortBlock, PgUlschDemuxConfig
+
+CONFIG_FIELDS = [f for f, _ in PgUlschDemuxConfig._fields_]
+
+
+def make_config(**fields) -> PgUlschDemuxConfig:
+    """A pg_ulsch_demux_config from keyword fields (missing ones are zero)."""
+    c = PgUlschDemuxConfig()
+    for k, v in fields.items():
+        if k not in CONFIG_FIELDS:
+            raise KeyError(k)
+        setattr(c, k, int(v))
+    return c
+
+
+class UlschDemultiplexer:
+    def __init__(self, context: _native.Context):
+        self.ctx = context
+        self.lib = context.lib
+
+    def sizes(self, cfg: PgUlschDemuxConfig) -> Tuple[int, int, int]:
+        """Soft bits of the UL-SCH, HARQ-ACK and CSI Part 1 streams (host computation)."""
+        out = (ctypes.c_uint32 * 3)()
+        rc = self.lib.pg_ulsch_demultiplex_sizes(ctypes.byref(cfg), out)
+        if rc:
+            raise _native.PgError(rc, "inconsistent or unsupported UL-SCH demultiplexing configuration")
+        return tuple(int(x) for x in out)
+
+    def demultiplex_device(self, cfgs: Sequence[PgUlschDemuxConfig], llrs_ptr, sch_ptr, ack_ptr, csi_ptr,
+                           stream_ptr=0):
+        arr = (PgUlschDemuxConfig * max(1, len(cfgs)))(*cfgs)
+        self.ctx.check(self.lib.pg_ulsch_demultiplex_device(self.ctx.handle, ctypes.addressof(arr), len(cfgs),
+                                                            llrs_ptr, sch_ptr, ack_ptr, csi_ptr, stream_ptr))
+
+    def demultiplex(self, cfgs: Sequence[PgUlschDemuxConfig], llrs: Sequence[np.ndarray]):
+        """Host soft bits in, [(sch, harq_ack, csi_part1)] out (offsets are assigned here)."""
+        import torch
+        cfgs = [PgUlschDemuxConfig.from_buffer_copy(c) for c in cfgs]
+        off_in, offs, spans = 0, [0, 0, 0], []
+        for c, x in zip(cfgs, llrs):
+            s = self.sizes(c)
+            c.llr_offset = off_in
+            c.sch_offset, c.harq_ack_offset, c.csi_part1_offset = offs
+            spans.append([(offs[k], s[k]) for k in range(3)])
+            off_in += int(np.asarray(x).size)
+            offs = [offs[k] + s[k] for k in range(3)]
+        d_in = torch.from_numpy(np.ascontiguousarray(np.concatenate(llrs), dtype=np.int8)).cuda()
+        outs = [torch.zeros(max(1, offs[k]), dtype=torch.int8, device="cuda") for k in range(3)]
+        st = torch.cuda.current_stream()
+        self.demultiplex_device(cfgs, d_in.data_ptr(), outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
+                                st.cuda_stream)
+        st.synchronize()
+        host = [o.cpu().numpy() for o in outs]
+        return [tuple(host[k][o:o + n] for k, (o, n) in enumerate(sp)) for sp in spans]
+
+
+class ShortBlockDetector:
+    def __init__(self, context: _native.Context):
+        self.ctx = context
+        self.lib = context.lib
+
+    def detect(self, messages: Sequence[Tuple[int, int, np.ndarray]]) -> List[Tuple[np.ndarray, bool]]:
+        """messages: (nof_bits, modulation_order, soft bits); returns (bits, valid) per message."""
+        import torch
+        n = len(messages)
+        if n == 0:
+            return []
+        items = (PgUciShortBlock * n)()
+        off, out_off = 0, 0
+        for i, (K, qm, llr) in enumerate(messages):
+            items[i].llr_offset, items[i].nof_llrs, items[i].out_offset = off, int(np.asarray(llr).size), out_off
+            items[i].nof_bits, items[i].modulation_order = K, qm
+            off += int(np.asarray(llr).size)
+            out_off += K
+        d_in = torch.from_numpy(np.ascontiguousarray(np.concatenate([m[2] for m in messages]), dtype=np.int8)).cuda()
+        d_bits = torch.zeros(out_off, dtype=torch.uint8, device="cuda")
+        d_valid = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        st = torch.cuda.current_stream()
+        self.ctx.check(self.lib.pg_uci_short_block_detect_device(self.ctx.handle, ctypes.addressof(items), n,
+                                                                 d_in.data_ptr(), d_bits.data_ptr(),
+                                                                 d_valid.data_ptr(), st.cuda_stream))
+        st.synchronize()
+        bits, valid = d_bits.cpu().numpy(), d_valid.cpu().numpy()
+        out, o = [], 0
+        for i, (K, _, _) in enumerate(messages):
+            out.append((bits[o:o + K].copy(), bool(valid[i])))
+            o += K
+        return out

@@ -179,6 +179,44 @@ class Ref:
         self.lib.ref_sch_segmentation(tbs_bits, bg, _ptr(o))
         return dict(C=int(o[0]), Z=int(o[1]), K=int(o[2]), tb_crc=int(o[3]))
 
+    def ulsch_demultiplex(self, cfg, llrs, block_size=4096):
+        """The reference's ulsch_demultiplex on descrambled soft bits (ref_shim_uci.cpp). cfg: a dict
+        with the fields of pg_ulsch_demux_config. Returns (sch, harq_ack, csi_part1, complete)."""
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        G = llrs.size
+        sch, ack, csi = np.zeros(G, np.int8), np.zeros(G, np.int8), np.zeros(G, np.int8)
+        lens = np.zeros(4, np.int32)
+        f = self.lib.ref_ulsch_demultiplex
+        f.argtypes = [ctypes.c_int] * 13 + [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        f(cfg["modulation_order"], cfg["nof_layers"], cfg["nof_prb"], cfg["start_symbol_index"], cfg["nof_symbols"],
+          cfg["dmrs_symbol_mask"], cfg["dmrs_type"], cfg["nof_cdm_groups_without_data"], cfg["nof_harq_ack_rvd"],
+          cfg["nof_harq_ack_bits"], cfg["nof_enc_harq_ack_bits"], cfg["nof_csi_part1_bits"],
+          cfg["nof_enc_csi_part1_bits"], cfg["c_init"], _ptr(llrs), G, block_size, _ptr(sch), G, _ptr(ack), G,
+          _ptr(csi), G, _ptr(lens))
+        return sch[:lens[0]].copy(), ack[:lens[1]].copy(), csi[:lens[2]].copy(), bool(lens[3])
+
+    def short_block_encode(self, msg, E, qm):
+        msg = np.ascontiguousarray(msg, dtype=np.uint8)
+        out = np.zeros(E, np.uint8)
+        self.lib.ref_short_block_encode.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_void_p]
+        self.lib.ref_short_block_encode(msg.size, _ptr(msg), E, qm, _ptr(out))
+        return out
+
+    def short_block_detect(self, K, llrs, qm):
+        """The reference's short_block_detector::detect: (bits, valid)."""
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        out = np.zeros(K, np.uint8)
+        self.lib.ref_short_block_detect.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_void_p]
+        ok = self.lib.ref_short_block_detect(K, _ptr(llrs), llrs.size, qm, _ptr(out))
+        return out, bool(ok)
+
+    def uci_min_encoded_bits(self, K):
+        return int(self.lib.ref_uci_min_encoded_bits(K))
+
 
 class Port:
     """The plain-C restatement (oracle/pusch_oracle.c)."""
