@@ -47,7 +47,7 @@ PUSCH_WORKLOAD = ("Batched uneven slot: 16 cells x 273 PRB (100 MHz, 30 kHz SCS)
                   "per-UE SNR U[0,30] dB, DM-RS type 1 symbols {2,11}, exponential PDP (100 ns RMS, 8 taps), "
                   "max 6 LDPC iterations, CRC early stop")
 KERNELS_PER_PLAN = 6  # estimate, demodulate, rate dematch, LDPC, TB assembly, results
-LE_KERNELS = 16       # learned estimator: features, 14 convolution layers, apply
+LE_KERNELS = 3        # learned estimator: features, the fused 14-layer network, apply
 LE_FLOPS_PER_ROW = 2 * 5 * (16 * 64 + 12 * 64 * 64 + 64 * 16)  # 14 layers, kernel 5, per subcarrier row
 WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) and BG2 Z=384 (K=3840, rate 1/5) "
             "mixed 50/50 by seed, CRC24B, BPSK/AWGN Eb/N0 U[1,3] dB, int8 LLRs (scale 4/LLR unit, sat +-127), "
@@ -194,6 +194,15 @@ def bf16_peak():
             return float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops, burst)"
     except (OSError, KeyError, ValueError):
         return 1590.0, "fallback (1.59 PFLOP/s earlier measurement on this pool)"
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth (GB/s, MEASURED_PEAKS.json), else the pool's earlier measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def int_peak(dev):
@@ -455,7 +464,7 @@ def run_ours_pusch(args):
     achieved = ops / (k_ms * 1e-3) / 1e12
     roofline = {
         "bound": "int",
-        "kernel": ("ldpc_decode_x2_kernel (Z=384) + ldpc_decode_kernel (other Z)"
+        "kernel": ("ldpc_decode_x2_kernel (every codeblock; two lifted lanes per thread for Z > 192)"
                    if tuning.as_dict().get("ldpc_z384_two_lanes") else "ldpc_decode_kernel"),
         "achieved": round(achieved, 3), "peak": round(peak, 3),
         "unit": "Tops/s", "frac": round(achieved / peak, 4),
@@ -485,6 +494,7 @@ def run_ours_pusch(args):
     ldpc_line = None
     if not args.no_ldpc:
         ldpc_line = ldpc_measure(args, dev, rank, world)
+    uci_line = uci_measure(ctx, plan.ues, hbm_peak()) if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -508,7 +518,7 @@ def run_ours_pusch(args):
                                      "plain LS + RC FIR + linear interpolation" if net is not None else
                                      "plain (LS + RC FIR + linear interpolation)")},
             "plain_per_ue": plain, "batched_plain": batched_plain,
-            "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": (KERNELS_PER_PLAN + (LE_KERNELS if net is not None else 0)) * args.steps,
             "step_ms": {"min": round(min(step_ms), 4), "max": round(max(step_ms), 4)},
@@ -758,6 +768,89 @@ def run_ours_ldpc(args):
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     return 0
+
+
+def uci_measure(ctx, ues, peak_gbs):
+    """UCI on PUSCH for every UE of the slot: HARQ-ACK of 5 bits and CSI Part 1 of 8 bits on each
+    codeword (demultiplexed out of synthetic descrambled soft bits of the slot's codeword sizes),
+    then short-block detection of the 2 x UEs messages; CUDA-event time of both entries, and the
+    demultiplexer against the measured HBM bandwidth (it reads and writes every soft bit once)."""
+    import ctypes
+    import torch
+    from pusch_b200._native import PgUciShortBlock
+    from pusch_b200.sim import nof_ch_symbols
+    from pusch_b200.uci import make_config
+    cfgs, offs, in_off = [], [0, 0, 0], 0
+    lib = ctx.lib
+    for ue in ues:
+        bpr = ue.modulation_order * ue.nof_layers
+        g = nof_ch_symbols(ue) * ue.modulation_order
+        mask = sum(1 << s for s in ue.dmrs_symbols)
+        c = make_config(nof_llrs=g, c_init=(ue.rnti << 15) + ue.n_id_data, nof_prb=ue.nof_rb, dmrs_symbol_mask=mask,
+                        modulation_order=ue.modulation_order, nof_layers=ue.nof_layers, start_symbol_index=0,
+                        nof_symbols=14, dmrs_type=1, nof_cdm_groups_without_data=2, nof_harq_ack_bits=5,
+                        nof_csi_part1_bits=8, nof_enc_harq_ack_bits=bpr * max(3, 24 // bpr),
+                        nof_enc_csi_part1_bits=bpr * max(4, 48 // bpr))
+        sz = (ctypes.c_uint32 * 3)()
+        if lib.pg_ulsch_demultiplex_sizes(ctypes.byref(c), sz):
+            continue
+        c.llr_offset, c.sch_offset, c.harq_ack_offset, c.csi_part1_offset = in_off, offs[0], offs[1], offs[2]
+        in_off += g
+        offs = [offs[k] + sz[k] for k in range(3)]
+        cfgs.append((c, tuple(sz)))
+    if not cfgs:
+        return None
+    n = len(cfgs)
+    arr = (type(cfgs[0][0]) * n)(*[c for c, _ in cfgs])
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    d_in = torch.randint(-120, 121, (in_off,), dtype=torch.int8, device="cuda", generator=gen)
+    outs = [torch.zeros(max(1, offs[k]), dtype=torch.int8, device="cuda") for k in range(3)]
+    items = (PgUciShortBlock * (2 * n))()
+    for i, (c, sz) in enumerate(cfgs):
+        for j, (off, e, k) in enumerate(((c.harq_ack_offset, sz[1], 5), (offs[1] + c.csi_part1_offset, sz[2], 8))):
+            it = items[2 * i + j]
+            it.llr_offset, it.nof_llrs, it.out_offset = off, e, (2 * i + j) * 8
+            it.nof_bits, it.modulation_order = k, c.modulation_order
+    uci_in = torch.zeros(max(1, offs[1] + offs[2]), dtype=torch.int8, device="cuda")
+    d_bits = torch.zeros(16 * n, dtype=torch.uint8, device="cuda")
+    d_valid = torch.zeros(2 * n, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def demux():
+        ctx.check(lib.pg_ulsch_demultiplex_device(ctx.handle, ctypes.addressof(arr), n, d_in.data_ptr(),
+                                                  outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
+                                                  st.cuda_stream))
+
+    def detect():
+        ctx.check(lib.pg_uci_short_block_detect_device(ctx.handle, ctypes.addressof(items), 2 * n, uci_in.data_ptr(),
+                                                       d_bits.data_ptr(), d_valid.data_ptr(), st.cuda_stream))
+
+    demux()
+    torch.cuda.synchronize()
+    uci_in[:offs[1]] = outs[1][:offs[1]]
+    uci_in[offs[1]:offs[1] + offs[2]] = outs[2][:offs[2]]
+    times, kernel = {}, {}
+    lib.pg_set_kernel_timing(ctx.handle, 1)
+    for name, fn in (("demux", demux), ("detect", detect)):
+        for _ in range(3):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        ks = []
+        for a, b in ev:
+            a.record(st)
+            fn()
+            b.record(st)
+            b.synchronize()
+            ks.append(float(lib.pg_last_kernel_ms(ctx.handle)))
+        times[name] = statistics.mean(a.elapsed_time(b) for a, b in ev)
+        kernel[name] = statistics.mean(ks)
+    gbs = 2 * in_off / (kernel["demux"] * 1e-3) / 1e9
+    return {"ues": n, "harq_ack_bits": 5, "csi_part1_bits": 8, "soft_bits": int(in_off),
+            "call_ms": {k: round(v, 4) for k, v in times.items()},
+            "demux_kernel_ms": round(kernel["demux"], 4), "detect_kernel_ms": round(kernel["detect"], 4),
+            "demux_roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak_gbs, "unit": "GB/s",
+                               "frac": round(gbs / peak_gbs, 4), "bytes_per_launch": int(2 * in_off)},
+            "data": "synthetic descrambled soft bits of the slot's codeword sizes, L2 not flushed between launches"}
 
 
 def ldpc_measure(args, dev, rank, world):

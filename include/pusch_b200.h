@@ -127,10 +127,11 @@ int pg_ldpc_decode_batch_host(pg_context* ctx, const pg_ldpc_cb* cbs, int nof_cb
 /* Size in bytes of the decoded-bit output of one codeblock: ceil(K_b*Z/8). */
 int pg_ldpc_output_bytes(int base_graph, int lifting_size);
 
-/* Enables (1) or disables (0) CUDA-event timing of the decode kernel launches. */
+/* Enables (1) or disables (0) CUDA-event timing of the decode kernel launches (LDPC decoding,
+ * UL-SCH demultiplexing, short-block UCI detection). */
 int pg_set_kernel_timing(pg_context* ctx, int enabled);
 
-/* Device time of the most recent decode kernel in milliseconds (CUDA events on its stream),
+/* Device time of the most recent of those kernels in milliseconds (CUDA events on its stream),
  * or a negative value when none was recorded. */
 float pg_last_kernel_ms(pg_context* ctx);
 

@@ -83,14 +83,55 @@ __device__ __forceinline__ void copy_re(const int8_t* __restrict__ src, int8_t* 
   }
 }
 
-__global__ void ulsch_demux_kernel(const demux_ue* __restrict__ ues, const demux_sym* __restrict__ syms,
-                                   const int8_t* __restrict__ llrs, int8_t* __restrict__ sch, int8_t* __restrict__ ack,
-                                   int8_t* __restrict__ csi, const uint32_t* __restrict__ gold)
+// Copies n bytes from src to dst with the CTA: 32-bit destination words assembled from the two
+// aligned source words that cover them (funnel shift), bytes at both ends. Every aligned source word
+// read holds at least one byte of [src - 3, src + n).
+__device__ __forceinline__ void copy_bytes_cta(int8_t* __restrict__ dst, const int8_t* __restrict__ src, uint32_t n)
 {
-  const demux_sym sd = syms[blockIdx.x];
-  const demux_ue  ud = ues[sd.ue];
-  const int       bpr = ud.bpr;
-  for (uint32_t i = threadIdx.x; i < sd.nre; i += blockDim.x) {
+  const uint32_t head = min(n, (4u - (uint32_t)(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u);
+  if (threadIdx.x < head) {
+    dst[threadIdx.x] = src[threadIdx.x];
+  }
+  dst += head;
+  src += head;
+  n -= head;
+  const uint32_t  nw = n / 4;
+  const uint32_t  sh = (uint32_t)(reinterpret_cast<uintptr_t>(src) & 3u);
+  const uint32_t* sw = reinterpret_cast<const uint32_t*>(src - sh);
+  uint32_t*       dw = reinterpret_cast<uint32_t*>(dst);
+  // The last word and the tail go byte by byte, so that no word beyond src + n is read.
+  const uint32_t nfast = nw > 0 ? nw - 1 : 0;
+  for (uint32_t w = threadIdx.x; w < nfast; w += blockDim.x) {
+    const uint32_t lo = __ldg(sw + w);
+    const uint32_t hi = sh ? __ldg(sw + w + 1) : 0u;
+    dw[w]             = __funnelshift_r(lo, hi, 8u * sh);
+  }
+  for (uint32_t b = 4 * nfast + threadIdx.x; b < n; b += blockDim.x) {
+    dst[b] = src[b];
+  }
+}
+
+// One CTA per work item (symbol index, RE range [r0, r1) of at most kDemuxChunk REs), so that
+// every thread handles at most one RE and the CTA issues its loads in one round.
+constexpr uint32_t kDemuxChunk = 256;
+
+__global__ void ulsch_demux_kernel(const demux_ue* __restrict__ ues, const demux_sym* __restrict__ syms,
+                                   const uint2* __restrict__ items, const int8_t* __restrict__ llrs,
+                                   int8_t* __restrict__ sch, int8_t* __restrict__ ack, int8_t* __restrict__ csi,
+                                   const uint32_t* __restrict__ gold)
+{
+  const uint2     item = items[blockIdx.x];
+  const demux_sym sd   = syms[item.x];
+  const demux_ue  ud   = ues[sd.ue];
+  const int       bpr  = ud.bpr;
+  const uint32_t  r0 = item.y & 0xffffu, r1 = item.y >> 16;
+  if (sd.rvd_m == 0 && sd.ack_m == 0 && sd.csi_m == 0) {
+    // No UCI in this symbol: its soft bits go to UL-SCH unchanged.
+    copy_bytes_cta(sch + ud.sch_offset + sd.sch0 + r0 * (uint32_t)bpr, llrs + ud.llr_offset + sd.in0 + r0 * (uint32_t)bpr,
+                   (r1 - r0) * (uint32_t)bpr);
+    return;
+  }
+  for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
     const bool     rvd   = sel_at(i, sd.rvd_d, sd.rvd_m);
     const bool     ack3  = sel_at(i, sd.ack_d, sd.ack_m);
     const uint32_t avail = i - sel_below(i, sd.ack_d, sd.ack_m) - sel_below(i, sd.rvd_d, sd.rvd_m);
@@ -506,19 +547,39 @@ int pg_ulsch_demultiplex_device(pg_context* ctx, const pg_ulsch_demux_config* cf
   if (syms.empty()) {
     return PG_OK;
   }
-  std::vector<uint8_t> blob(ues.size() * sizeof(demux_ue) + syms.size() * sizeof(demux_sym));
-  std::memcpy(blob.data(), ues.data(), ues.size() * sizeof(demux_ue));
-  std::memcpy(blob.data() + ues.size() * sizeof(demux_ue), syms.data(), syms.size() * sizeof(demux_sym));
+  std::vector<uint2> items;
+  for (size_t k = 0; k < syms.size(); ++k) {
+    for (uint32_t r0 = 0; r0 < syms[k].nre; r0 += kDemuxChunk) {
+      const uint32_t r1 = std::min<uint32_t>(syms[k].nre, r0 + kDemuxChunk);
+      items.push_back(make_uint2((uint32_t)k, r0 | (r1 << 16)));
+    }
+  }
+  // [UEs | symbols | items], the items (8-byte vectors) on a 16-byte boundary.
+  const size_t         b_ues = ues.size() * sizeof(demux_ue), b_syms = syms.size() * sizeof(demux_sym);
+  const size_t         o_items = (b_ues + b_syms + 15) & ~(size_t)15;
+  std::vector<uint8_t> blob(o_items + items.size() * sizeof(uint2));
+  std::memcpy(blob.data(), ues.data(), b_ues);
+  std::memcpy(blob.data() + b_ues, syms.data(), b_syms);
+  std::memcpy(blob.data() + o_items, items.data(), items.size() * sizeof(uint2));
   cudaStream_t s   = static_cast<cudaStream_t>(stream);
   void*        dev = nullptr;
   if (int rc = stage_slot(ctx, SLOT_UCI, blob.data(), blob.size(), s, &dev)) {
     return rc;
   }
   const demux_ue*  d_ues  = static_cast<const demux_ue*>(dev);
-  const demux_sym* d_syms = reinterpret_cast<const demux_sym*>(static_cast<uint8_t*>(dev) + ues.size() * sizeof(demux_ue));
-  ulsch_demux_kernel<<<(unsigned)syms.size(), 256, 0, s>>>(d_ues, d_syms, llrs, sch, harq_ack, csi_part1,
-                                                            ctx->dev.gold);
-  return check_cuda(ctx, cudaGetLastError(), "ulsch_demux_kernel launch");
+  const demux_sym* d_syms  = reinterpret_cast<const demux_sym*>(static_cast<uint8_t*>(dev) + b_ues);
+  const uint2*     d_items = reinterpret_cast<const uint2*>(static_cast<uint8_t*>(dev) + o_items);
+  const unsigned int rec = timing_record_flags(ctx, s);
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_start, s, rec);
+  }
+  ulsch_demux_kernel<<<(unsigned)items.size(), kDemuxChunk, 0, s>>>(d_ues, d_syms, d_items, llrs, sch, harq_ack,
+                                                                     csi_part1, ctx->dev.gold);
+  const int rc = check_cuda(ctx, cudaGetLastError(), "ulsch_demux_kernel launch");
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
+  }
+  return rc;
 }
 
 int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* items, int n, const int8_t* llrs,
@@ -551,9 +612,17 @@ int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* 
     return rc;
   }
   const unsigned warps_per_cta = 4;
+  const unsigned int rec           = timing_record_flags(ctx, s);
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_start, s, rec);
+  }
   uci_short_block_kernel<<<(unsigned)((n + warps_per_cta - 1) / warps_per_cta), 32 * warps_per_cta, 0, s>>>(
       static_cast<const short_item*>(dev), n, llrs, bits, valid);
-  return check_cuda(ctx, cudaGetLastError(), "uci_short_block_kernel launch");
+  const int rc = check_cuda(ctx, cudaGetLastError(), "uci_short_block_kernel launch");
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
+  }
+  return rc;
 }
 
 } // extern "C"
