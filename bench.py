@@ -450,6 +450,43 @@ def run_ours_pusch(args):
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
                "ms_per_step": round(e_ms, 3), "entry": "pg_pusch_plan_execute_host"}
 
+        # The same through the Open Fronthaul payload: the grids as 9-bit BFP PRBs (the radio
+        # unit's gain of 1/16 into the fixed-point range and its compression, done here by the
+        # simulator), decompressed on the GPU.
+        from pusch_b200 import sim as sim_mod
+        h_comp = torch.from_numpy(sim_mod.bfp_compress(sim_mod.scale_grid_words(plan.grid.ravel(), 1.0 / 16),
+                                                       9)).pin_memory()
+
+        def bfp_step():
+            ctx.check(lib.pg_pusch_plan_execute_host_bfp(plan.handle, h_comp.data_ptr(), h_comp.numel(), 9,
+                                                         h_tb.data_ptr(), h_tb.numel(), ctypes.addressof(h_res), None))
+
+        for _ in range(max(args.warmup, 1)):
+            bfp_step()
+        bt = []
+        for k in range(min(args.steps, 200)):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            bfp_step()
+            bt.append(time.perf_counter() - t0)
+        b_ms = 1e3 * statistics.mean(bt)
+        tbh = h_tb.numpy()
+        b_bits = 0
+        for i, d in enumerate(plan.descs):
+            if h_res[i].tb_crc_ok and (np.unpackbits(tbh[d.tb_out_offset:d.tb_out_offset + d.tbs_bits // 8])
+                                       == truth[i]).all():
+                b_bits += d.tbs_bits
+        if world > 1:
+            t = torch.tensor([b_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            b_ms = float(t.item())
+        e2e["ofh_bfp9"] = {"value": round(b_bits / (b_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
+                           "h2d_bytes_per_step": int(h_comp.numel()),
+                           "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
+                           "ms_per_step": round(b_ms, 3), "decoded_bits": int(b_bits),
+                           "entry": "pg_pusch_plan_execute_host_bfp (9-bit BFP grids, decompressed on the GPU)"}
+
     # Rooflines: the integer pipe of ldpc_decode_kernel and the tensor cores of the learned
     # estimator's convolutions, both timed with CUDA events inside the step; "roofline" is the one
     # that takes the larger share of the step.
@@ -495,6 +532,7 @@ def run_ours_pusch(args):
     if not args.no_ldpc:
         ldpc_line = ldpc_measure(args, dev, rank, world)
     uci_line = uci_measure(ctx, plan.ues, hbm_peak()) if rank == 0 else None
+    bfp_line = bfp_measure(ctx, plan.grid.ravel(), hbm_peak()) if rank == 0 else None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -518,7 +556,7 @@ def run_ours_pusch(args):
                                      "plain LS + RC FIR + linear interpolation" if net is not None else
                                      "plain (LS + RC FIR + linear interpolation)")},
             "plain_per_ue": plain, "batched_plain": batched_plain,
-            "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "cpu_baseline": cpu,
+            "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "ofh_bfp": bfp_line, "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": (KERNELS_PER_PLAN + (LE_KERNELS if net is not None else 0)) * args.steps,
             "step_ms": {"min": round(min(step_ms), 4), "max": round(max(step_ms), 4)},
@@ -851,6 +889,33 @@ def uci_measure(ctx, ues, peak_gbs):
             "demux_roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak_gbs, "unit": "GB/s",
                                "frac": round(gbs / peak_gbs, 4), "bytes_per_launch": int(2 * in_off)},
             "data": "synthetic descrambled soft bits of the slot's codeword sizes, L2 not flushed between launches"}
+
+
+def bfp_measure(ctx, grid_words, peak_gbs):
+    """Open Fronthaul BFP decompression of the slot's grids (9-bit PRBs, the radio unit's gain of
+    1/16 and compression done by the simulator): kernel time through the context's kernel events
+    and the HBM roofline (compressed bytes read + complex bf16 words written, per launch)."""
+    import torch
+    from pusch_b200 import sim as sim_mod
+    comp = sim_mod.bfp_compress(sim_mod.scale_grid_words(grid_words, 1.0 / 16), 9)
+    nprb = grid_words.size // 12
+    d_in = torch.from_numpy(comp).cuda()
+    d_out = torch.empty(12 * nprb, dtype=torch.int32, device="cuda")
+    lib = ctx.lib
+    st = torch.cuda.current_stream()
+    lib.pg_set_kernel_timing(ctx.handle, 1)
+    ks = []
+    for k in range(23):
+        ctx.check(lib.pg_bfp_decompress_device(ctx.handle, d_in.data_ptr(), nprb, 9, d_out.data_ptr(), st.cuda_stream))
+        st.synchronize()
+        if k >= 3:
+            ks.append(float(lib.pg_last_kernel_ms(ctx.handle)))
+    ms = statistics.mean(ks)
+    nbytes = int(comp.size + 4 * 12 * nprb)
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    return {"prbs": int(nprb), "data_width": 9, "kernel_ms": round(ms, 4),
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak_gbs, "unit": "GB/s",
+                         "frac": round(gbs / peak_gbs, 4), "bytes_per_launch": nbytes}}
 
 
 def ldpc_measure(args, dev, rank, world):

@@ -616,6 +616,30 @@ typedef struct pg_uci_short_block {
 int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* items, int n, const int8_t* llrs,
                                      uint8_t* bits, uint8_t* valid, void* stream);
 
+
+/* ---------------------------------------------------------------------------------------------
+ * Open Fronthaul block-floating-point IQ (O-RAN.WG4.CUS Annex A.1.2): per PRB one exponent byte,
+ * then the I and Q samples of the 12 subcarriers, data_width bits each, packed big-endian. */
+
+/* Compressed bytes per PRB for data_width (1..16) bits: 1 + 3 * data_width; -1 when out of range. */
+int pg_bfp_prb_bytes(int data_width);
+
+/* Decompresses nof_prb consecutive PRBs (device bytes) into 12 * nof_prb complex bf16 words (device)
+ * - iq_decompressor::decompress for compression_type::BFP (include/ocudu/ofh/compression/iq_decompressor.h;
+ * lib/ofh/compression/iq_compression_bfp_impl.cpp:89-141, iq_compression_bfp_avx512.cpp:147-201),
+ * with the rounding of the reference's x86 implementation for the width. A whole grid is one call:
+ * its (port, symbol) rows are whole PRBs back to back. */
+int pg_bfp_decompress_device(pg_context* ctx, const uint8_t* compressed, uint32_t nof_prb, int data_width,
+                             uint32_t* iq, void* stream);
+
+/* pg_pusch_plan_execute_host with the grids given as BFP-compressed PRBs (host bytes, the plan's
+ * grid words / 12 PRBs in grid order): copies the compressed bytes, decompresses them on the GPU
+ * into the plan's grid buffer and runs the plan. The first call allocates the plan's buffer for the
+ * compressed bytes. */
+int pg_pusch_plan_execute_host_bfp(pg_pusch_plan* plan, const uint8_t* compressed, size_t compressed_len,
+                                   int data_width, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results,
+                                   pg_port_result* port_results);
+
 #ifdef __cplusplus
 }
 #endif

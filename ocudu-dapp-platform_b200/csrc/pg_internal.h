@@ -107,6 +107,10 @@ int validate_ldpc_descs(pg_context* ctx, const pg_ldpc_cb* cbs, int n, size_t no
 // Uploads the constant base-graph tables (once per process and device).
 int ldpc_upload_tables(pg_context* ctx);
 int uci_upload_tables(pg_context* ctx);
+// Open Fronthaul BFP: compressed bytes per PRB, and decompression of nof_prb PRBs into cbf16.
+int bfp_prb_bytes(int data_width);
+int bfp_decompress_launch(pg_context* ctx, const uint8_t* in, uint32_t nof_prb, int data_width, uint32_t* out,
+                          cudaStream_t s);
 
 enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4, SLOT_UCI = 5, SLOT_UCI_SHORT = 6 };
 

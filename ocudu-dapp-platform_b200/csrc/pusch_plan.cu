@@ -55,6 +55,9 @@ struct pg_pusch_plan {
   pg_sch_result*  d_res    = nullptr; // results of execute_host
   // Pinned host buffers of execute_host: [results | port results | TBs].
   void*           host     = nullptr;
+  // Compressed grids of execute_host_bfp (allocated on its first call).
+  uint8_t*        d_bfp     = nullptr;
+  size_t          d_bfp_cap = 0;
   // Learned estimator: the net, the LS estimates and the sequences of the refined UEs.
   pg_le_net*      le_net    = nullptr;
   void*           le_dev    = nullptr;
@@ -158,6 +161,7 @@ void release(pg_pusch_plan* p)
   }
   cudaFree(p->dev);
   cudaFree(p->le_dev);
+  cudaFree(p->d_bfp);
   if (p->host) {
     cudaFreeHost(p->host);
   }
@@ -702,6 +706,11 @@ int pg_pusch_plan_execute_device(pg_pusch_plan* plan, const uint32_t* grids, uin
   return check_cuda(ctx, cudaGraphLaunch(plan->exec, s), "cudaGraphLaunch");
 }
 
+// The part of the host entries after the grids are on the device: the plan on plan->d_grid, the
+// results and TBs back to the host.
+static int execute_host_tail(pg_pusch_plan* plan, uint8_t* tb_out, pg_sch_result* results,
+                             pg_port_result* port_results, int rc);
+
 int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8_t* tb_out, size_t tb_out_len,
                                pg_sch_result* results, pg_port_result* port_results)
 {
@@ -715,14 +724,69 @@ int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8
   if (tb_out_len < plan->tb_bytes) {
     return set_error(ctx, PG_ERR_INVALID, "transport-block buffer smaller than the plan's TBs");
   }
+  const int rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, grids, plan->grid_words * 4, cudaMemcpyHostToDevice,
+                                                 ctx->stream),
+                            "H2D grids");
+  return execute_host_tail(plan, tb_out, results, port_results, rc);
+}
+
+int pg_pusch_plan_execute_host_bfp(pg_pusch_plan* plan, const uint8_t* compressed, size_t compressed_len,
+                                   int data_width, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results,
+                                   pg_port_result* port_results)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (compressed == nullptr || results == nullptr || (tb_out == nullptr && plan->tb_bytes > 0)) {
+    return set_error(ctx, PG_ERR_INVALID, "null host buffer");
+  }
+  if (tb_out_len < plan->tb_bytes) {
+    return set_error(ctx, PG_ERR_INVALID, "transport-block buffer smaller than the plan's TBs");
+  }
+  if (data_width < 1 || data_width > 16) {
+    return set_error(ctx, PG_ERR_INVALID, "BFP data width must be 1 to 16 bits");
+  }
+  if (plan->grid_words % 12 != 0) {
+    return set_error(ctx, PG_ERR_INVALID, "the plan's grids are not whole PRBs");
+  }
+  const uint32_t nof_prb = (uint32_t)(plan->grid_words / 12);
+  const size_t   bytes   = (size_t)nof_prb * (size_t)bfp_prb_bytes(data_width);
+  if (compressed_len < bytes) {
+    return set_error(ctx, PG_ERR_INVALID, "compressed grids shorter than the plan's PRBs (" + std::to_string(bytes) +
+                                              " bytes)");
+  }
+  cudaStream_t s = ctx->stream;
+  if (plan->d_bfp_cap < bytes) {
+    if (int rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize")) {
+      return rc;
+    }
+    cudaFree(plan->d_bfp);
+    plan->d_bfp     = nullptr;
+    plan->d_bfp_cap = 0;
+    if (int rc = check_cuda(ctx, cudaMalloc(&plan->d_bfp, bytes), "cudaMalloc(compressed grids)")) {
+      return rc;
+    }
+    plan->d_bfp_cap = bytes;
+  }
+  int rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_bfp, compressed, bytes, cudaMemcpyHostToDevice, s),
+                      "H2D compressed grids");
+  if (rc == PG_OK) {
+    rc = bfp_decompress_launch(ctx, plan->d_bfp, nof_prb, data_width, plan->d_grid, s);
+  }
+  return execute_host_tail(plan, tb_out, results, port_results, rc);
+}
+
+static int execute_host_tail(pg_pusch_plan* plan, uint8_t* tb_out, pg_sch_result* results,
+                             pg_port_result* port_results, int rc)
+{
+  pg_context*     ctx  = plan->ctx;
   const int       n    = plan->nof_ues;
   cudaStream_t    s    = ctx->stream;
   uint8_t*        h    = static_cast<uint8_t*>(plan->host);
   pg_sch_result*  hres = reinterpret_cast<pg_sch_result*>(h);
   pg_port_result* hpr  = reinterpret_cast<pg_port_result*>(h + al((size_t)n * sizeof(pg_sch_result)));
   uint8_t*        htb  = h + al((size_t)n * sizeof(pg_sch_result)) + al((size_t)n * 4 * sizeof(pg_port_result));
-  int rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, grids, plan->grid_words * 4, cudaMemcpyHostToDevice, s),
-                      "H2D grids");
   if (rc == PG_OK) {
     rc = pg_pusch_plan_execute_device(plan, plan->d_grid, plan->d_tb_out, plan->d_res, plan->d_pr, s);
   }

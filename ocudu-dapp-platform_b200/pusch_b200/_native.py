@@ -174,6 +174,10 @@ SIGNATURES = {
     "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),
     "pg_pusch_plan_set_harq": (ctypes.c_int, [_VP, _VP, _VP]),
     "pg_ulsch_demultiplex_sizes": (ctypes.c_int, [_VP, _VP]),
+    "pg_bfp_prb_bytes": (ctypes.c_int, [ctypes.c_int]),
+    "pg_bfp_decompress_device": (ctypes.c_int, [_VP, _VP, ctypes.c_uint32, ctypes.c_int, _VP, _VP]),
+    "pg_pusch_plan_execute_host_bfp": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t, ctypes.c_int, _VP, ctypes.c_size_t,
+                                                      _VP, _VP]),
     "pg_ulsch_demultiplex_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_uci_short_block_detect_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),

@@ -199,10 +199,25 @@ class PuschSlotPlan:
                                                            ctypes.addressof(pr) if pr is not None else None))
         return results_from(self.descs, res, pr, tb)
 
+    def execute_host_bfp(self, compressed: np.ndarray, data_width: int, with_port_results=True) -> List[PuschResult]:
+        """execute_host with the grids as O-RAN BFP-compressed PRBs (pg_pusch_plan_execute_host_bfp)."""
+        compressed = np.ascontiguousarray(compressed, dtype=np.uint8)
+        n = self.n
+        res = (PgSchResult * n)()
+        pr = (PgPortResult * (4 * n))() if with_port_results else None
+        tb = np.zeros(max(self.tb_bytes, 1), np.uint8)
+        self.ctx.check(self.lib.pg_pusch_plan_execute_host_bfp(
+            self.handle, compressed.ctypes.data_as(ctypes.c_void_p), compressed.size, data_width,
+            tb.ctypes.data_as(ctypes.c_void_p), tb.size, ctypes.addressof(res),
+            ctypes.addressof(pr) if pr is not None else None))
+        return results_from(self.descs, res, pr, tb)
+
     def close(self):
-        if getattr(self, "handle", None):
+        # A plan outlived by its context (closed first, e.g. at interpreter exit) is not destroyed:
+        # the plan refers to the context's stream.
+        if getattr(self, "handle", None) and getattr(self.ctx, "handle", None):
             self.lib.pg_pusch_plan_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

@@ -269,3 +269,36 @@ def uneven_cells(seed=0, nof_cells=16, nof_ports=4, snr_range=(0.0, 30.0), max_u
         slots.append(make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=cell % 20,
                                      seed=int(rng.integers(0, 2 ** 31))))
     return slots
+
+
+# ----------------------------------------------------------------------------------------------
+# Open Fronthaul block floating point (O-RAN.WG4.CUS Annex A.1.2), the uplink U-plane payload a
+# radio unit sends: per PRB an exponent byte, then the 24 samples of `width` bits, big-endian.
+
+
+def bfp_compress(words, width):
+    """Compresses complex bf16 grid words (12 per PRB, real in the low half) to BFP bytes: samples
+    quantised to 16-bit fixed point (gain 2^15 - 1, rounded to nearest, saturated to int16), the
+    PRB's exponent the smallest right shift that fits every sample in `width` signed bits."""
+    w = np.ascontiguousarray(words, np.uint32).reshape(-1, 12)
+    nprb = w.shape[0]
+    f = np.stack([(w & 0xFFFF) << 16, w & 0xFFFF0000], axis=-1).astype(np.uint32).view(np.float32).reshape(nprb, 24)
+    q = np.clip(np.rint(f.astype(np.float64) * np.float32(32767.0)), -32768, 32767).astype(np.int32)
+    mag = np.max(np.where(q < 0, -q - 1, q), axis=1)          # largest magnitude of the signed values
+    need = np.where(mag > 0, np.floor(np.log2(np.maximum(mag, 1))).astype(np.int32) + 2, 1)
+    e = np.clip(need - width, 0, 15).astype(np.int32)
+    v = (q >> e[:, None]) & ((1 << width) - 1)
+    bits = ((v[:, :, None] >> np.arange(width - 1, -1, -1)) & 1).astype(np.uint8).reshape(nprb, 24 * width)
+    out = np.zeros((nprb, 1 + 3 * width), np.uint8)
+    out[:, 0] = e
+    out[:, 1:] = np.packbits(bits, axis=1)
+    return out.ravel()
+
+
+def scale_grid_words(words, factor):
+    """Complex bf16 grid words multiplied by a power of two (exact): the radio unit's gain that
+    brings the received signal into the fixed-point range before BFP compression."""
+    w = np.asarray(words, np.uint32)
+    f = np.stack([(w & 0xFFFF) << 16, w & 0xFFFF0000], axis=-1).astype(np.uint32).view(np.float32) * np.float32(factor)
+    h = (f.view(np.uint32) >> 16).astype(np.uint32)
+    return (h[..., 0] | (h[..., 1] << 16)).astype(np.uint32)

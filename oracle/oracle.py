@@ -214,6 +214,25 @@ class Ref:
         ok = self.lib.ref_short_block_detect(K, _ptr(llrs), llrs.size, qm, _ptr(out))
         return out, bool(ok)
 
+    def bfp_compress(self, width, iq_words, generic=False):
+        """The reference's BFP compressor on complex bf16 words (12 per PRB): compressed bytes."""
+        iq_words = np.ascontiguousarray(iq_words, dtype=np.uint32)
+        nprb = iq_words.size // 12
+        out = np.zeros(nprb * (1 + 3 * width), np.uint8)
+        self.lib.ref_bfp_compress.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                              ctypes.c_int]
+        self.lib.ref_bfp_compress(width, _ptr(iq_words), nprb, _ptr(out), int(generic))
+        return out
+
+    def bfp_decompress(self, width, data, nprb, generic=False):
+        """The reference's BFP decompressor: complex bf16 words (12 per PRB)."""
+        data = np.ascontiguousarray(data, dtype=np.uint8)
+        out = np.zeros(12 * nprb, np.uint32)
+        self.lib.ref_bfp_decompress.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                                ctypes.c_int]
+        rc = self.lib.ref_bfp_decompress(width, _ptr(data), nprb, _ptr(out), int(generic))
+        return out, int(rc)
+
     def uci_min_encoded_bits(self, K):
         return int(self.lib.ref_uci_min_encoded_bits(K))
 
