@@ -450,6 +450,37 @@ def run_ours_pusch(args):
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
                "ms_per_step": round(e_ms, 3), "entry": "pg_pusch_plan_execute_host"}
 
+        # Consecutive slots through the pipelined entries: each step's grids still go host to
+        # device and its results device to host, but the copy of slot k + 1 overlaps slot k.
+        def pipelined(steps):
+            t0 = time.perf_counter()
+            for k in range(steps):
+                ctx.check(lib.pg_pusch_plan_submit_host(plan.handle, h_grid.data_ptr()))
+                if k >= 1:
+                    ctx.check(lib.pg_pusch_plan_collect_host(plan.handle, h_tb.data_ptr(), h_tb.numel(),
+                                                             ctypes.addressof(h_res), None))
+            ctx.check(lib.pg_pusch_plan_collect_host(plan.handle, h_tb.data_ptr(), h_tb.numel(),
+                                                     ctypes.addressof(h_res), None))
+            return time.perf_counter() - t0
+
+        pipelined(max(args.warmup, 2))
+        np_steps = min(args.steps, 200)
+        p_ms = 1e3 * pipelined(np_steps) / np_steps
+        assert [bool(h_res[i].tb_crc_ok) for i in range(n)] == [r.tb_crc_ok for r in results]
+        if world > 1:
+            t = torch.tensor([p_ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            p_ms = float(t.item())
+        # The headline end-to-end figure is the pipelined one (consecutive slots, as a PHY runs them);
+        # the one-call-at-a-time figure stays beside it.
+        e2e = {"value": round(total_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
+               "h2d_bytes_per_step": int(plan.grid.size * 4),
+               "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
+               "ms_per_step": round(p_ms, 3),
+               "entry": "pg_pusch_plan_submit_host / pg_pusch_plan_collect_host (two slots in flight; every step "
+                        "copies its grids in and its results out)",
+               "synchronous": e2e}
+
         # The same through the Open Fronthaul payload: the grids as 9-bit BFP PRBs (the radio
         # unit's gain of 1/16 into the fixed-point range and its compression, done here by the
         # simulator), decompressed on the GPU.

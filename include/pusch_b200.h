@@ -617,6 +617,19 @@ int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* 
                                      uint8_t* bits, uint8_t* valid, void* stream);
 
 
+/* Pipelined host execution of consecutive slots: pg_pusch_plan_submit_host enqueues one slot and
+ * returns without waiting - the host-to-device copy of its grids runs on a stream of its own into
+ * a staging buffer, overlapping the previous slot's processing; the grids then move into the plan's
+ * grid buffer, the plan runs and its results come back to a pinned buffer of the slot.
+ * pg_pusch_plan_collect_host waits for the oldest submitted slot and writes its results as
+ * pg_pusch_plan_execute_host does. At most two slots are in flight (PG_ERR_INVALID beyond); the
+ * grids of a slot are read asynchronously, so they stay untouched until its collect returns (pinned
+ * host memory makes the copy asynchronous). The first submit allocates the staging and result
+ * buffers. Do not mix with the plan's other execute calls while slots are in flight. */
+int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids);
+int pg_pusch_plan_collect_host(pg_pusch_plan* plan, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results,
+                               pg_port_result* port_results);
+
 /* ---------------------------------------------------------------------------------------------
  * Open Fronthaul block-floating-point IQ (O-RAN.WG4.CUS Annex A.1.2): per PRB one exponent byte,
  * then the I and Q samples of the 12 subcarriers, data_width bits each, packed big-endian. */

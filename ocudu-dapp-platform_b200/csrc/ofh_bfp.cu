@@ -12,19 +12,19 @@
 // the float (2^e / 32767) - two roundings; for the other widths it falls back to the generic one,
 // which divides the integer sample * 2^e by 32767 - one rounding. The kernel does the same per width.
 //
-// Mapping: one CTA per 32 PRBs (384 threads, one per subcarrier). The CTA's compressed bytes are a
-// contiguous run of 32 * (1 + 3 * width) bytes, a multiple of 16, so they are staged into shared
-// memory with 16-byte loads (byte loads when the buffer is not 16-byte aligned); each thread then
-// reads its I and Q fields through a 32-bit big-endian window and writes one complex bf16 word,
-// coalesced across the CTA.
+// Mapping: one CTA per 128 PRBs (384 threads, four subcarriers each). The CTA's compressed bytes
+// are a contiguous run of 128 * (1 + 3 * width) bytes, a multiple of 16, so they are staged into
+// shared memory with 16-byte loads (byte loads when the buffer is not 16-byte aligned), all in
+// flight before the barrier; each thread then reads its I and Q fields through a 32-bit big-endian
+// window and writes complex bf16 words, coalesced across the CTA.
 #include "pg_internal.h"
 
 #include <cuda_bf16.h>
 
 namespace {
 
-constexpr int kBfpPrbs    = 32;
-constexpr int kBfpThreads = kBfpPrbs * 12;
+constexpr int kBfpPrbs    = 128;
+constexpr int kBfpThreads = 384; // each thread writes kBfpPrbs * 12 / 384 = 4 subcarriers
 constexpr int kBfpMaxPrbBytes = 1 + 3 * 16;
 
 __device__ __forceinline__ int bfp_field(const uint8_t* __restrict__ p, uint32_t bit, int w)
@@ -65,25 +65,29 @@ __global__ void __launch_bounds__(kBfpThreads) bfp_decompress_kernel(const uint8
     s[nbytes + tid] = 0; // the bytes a 32-bit window may read past the last field
   }
   __syncthreads();
-  const uint32_t p = (uint32_t)tid / 12u, k = (uint32_t)tid - p * 12u;
-  if (p >= np) {
-    return;
+#pragma unroll
+  for (int j = 0; j < kBfpPrbs * 12 / kBfpThreads; ++j) {
+    const uint32_t idx = (uint32_t)(tid + j * kBfpThreads);
+    const uint32_t p = idx / 12u, k = idx - p * 12u;
+    if (p >= np) {
+      break;
+    }
+    const uint8_t* prb = s + p * (uint32_t)prb_bytes;
+    const int      e   = prb[0] & 31;
+    const int      re  = bfp_field(prb + 1, 2u * k * (uint32_t)w, w);
+    const int      im  = bfp_field(prb + 1, (2u * k + 1u) * (uint32_t)w, w);
+    float          fr, fi;
+    if (mul_path) {
+      const float scale = __fdiv_rn((float)(1 << e), 32767.0f);
+      fr                = __fmul_rn((float)re, scale);
+      fi                = __fmul_rn((float)im, scale);
+    } else {
+      const int scaler = (int)(int16_t)(1 << e); // the reference's int16_t scaling factor
+      fr               = __fdiv_rn(__int2float_rn(re * scaler), 32767.0f);
+      fi               = __fdiv_rn(__int2float_rn(im * scaler), 32767.0f);
+    }
+    out[(size_t)p0 * 12u + idx] = bf16_bits(fr) | (bf16_bits(fi) << 16);
   }
-  const uint8_t* prb = s + p * (uint32_t)prb_bytes;
-  const int      e   = prb[0] & 31;
-  const int      re  = bfp_field(prb + 1, 2u * k * (uint32_t)w, w);
-  const int      im  = bfp_field(prb + 1, (2u * k + 1u) * (uint32_t)w, w);
-  float          fr, fi;
-  if (mul_path) {
-    const float scale = __fdiv_rn((float)(1 << e), 32767.0f);
-    fr                = __fmul_rn((float)re, scale);
-    fi                = __fmul_rn((float)im, scale);
-  } else {
-    const int scaler = (int)(int16_t)(1 << e); // the reference's int16_t scaling factor
-    fr               = __fdiv_rn(__int2float_rn(re * scaler), 32767.0f);
-    fi               = __fdiv_rn(__int2float_rn(im * scaler), 32767.0f);
-  }
-  out[(size_t)(p0 + p) * 12u + k] = bf16_bits(fr) | (bf16_bits(fi) << 16);
 }
 
 } // namespace

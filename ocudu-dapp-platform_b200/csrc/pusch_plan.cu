@@ -58,6 +58,17 @@ struct pg_pusch_plan {
   // Compressed grids of execute_host_bfp (allocated on its first call).
   uint8_t*        d_bfp     = nullptr;
   size_t          d_bfp_cap = 0;
+  // Pipelined host execution (submit_host / collect_host; allocated on the first submit): the
+  // staging buffer the next slot's grids are copied into while the current slot runs, the copy
+  // stream, and two pinned result slots.
+  uint32_t*       d_stage       = nullptr;
+  cudaStream_t    copy_stream   = nullptr;
+  cudaEvent_t     ev_h2d        = nullptr;
+  cudaEvent_t     ev_stage_free = nullptr;
+  cudaEvent_t     ev_done[2]    = {nullptr, nullptr};
+  void*           host_slot[2]  = {nullptr, nullptr};
+  uint64_t        submitted     = 0;
+  uint64_t        collected     = 0;
   // Learned estimator: the net, the LS estimates and the sequences of the refined UEs.
   pg_le_net*      le_net    = nullptr;
   void*           le_dev    = nullptr;
@@ -162,6 +173,20 @@ void release(pg_pusch_plan* p)
   cudaFree(p->dev);
   cudaFree(p->le_dev);
   cudaFree(p->d_bfp);
+  cudaFree(p->d_stage);
+  if (p->copy_stream) {
+    cudaStreamDestroy(p->copy_stream);
+  }
+  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1]}) {
+    if (e) {
+      cudaEventDestroy(e);
+    }
+  }
+  for (void* h : p->host_slot) {
+    if (h) {
+      cudaFreeHost(h);
+    }
+  }
   if (p->host) {
     cudaFreeHost(p->host);
   }
@@ -775,6 +800,145 @@ int pg_pusch_plan_execute_host_bfp(pg_pusch_plan* plan, const uint8_t* compresse
     rc = bfp_decompress_launch(ctx, plan->d_bfp, nof_prb, data_width, plan->d_grid, s);
   }
   return execute_host_tail(plan, tb_out, results, port_results, rc);
+}
+
+// Results of one slot from the pinned host buffer h (layout of plan->host) to the caller's buffers.
+static void copy_results_out(const pg_pusch_plan* plan, const uint8_t* h, uint8_t* tb_out, pg_sch_result* results,
+                             pg_port_result* port_results)
+{
+  const int             n    = plan->nof_ues;
+  const pg_sch_result*  hres = reinterpret_cast<const pg_sch_result*>(h);
+  const pg_port_result* hpr  = reinterpret_cast<const pg_port_result*>(h + al((size_t)n * sizeof(pg_sch_result)));
+  const uint8_t*        htb  = h + al((size_t)n * sizeof(pg_sch_result)) + al((size_t)n * 4 * sizeof(pg_port_result));
+  std::memcpy(results, hres, (size_t)n * sizeof(pg_sch_result));
+  if (port_results != nullptr) {
+    std::memcpy(port_results, hpr, (size_t)n * 4 * sizeof(pg_port_result));
+  }
+  // The reference writes a TB's payload only when its CRC passes.
+  for (int i = 0; i < n; ++i) {
+    if (hres[i].tb_crc_ok) {
+      const pg_pusch_ue& u = plan->ues[i];
+      std::memcpy(tb_out + u.tb_out_offset, htb + u.tb_out_offset, u.tbs_bits / 8);
+    }
+  }
+}
+
+// D2H of one slot's results, port results and TBs into the pinned host buffer h.
+static int enqueue_results_d2h(pg_pusch_plan* plan, uint8_t* h, cudaStream_t s)
+{
+  pg_context* ctx = plan->ctx;
+  const int   n   = plan->nof_ues;
+  uint8_t*    hpr = h + al((size_t)n * sizeof(pg_sch_result));
+  uint8_t*    htb = hpr + al((size_t)n * 4 * sizeof(pg_port_result));
+  int rc = check_cuda(ctx, cudaMemcpyAsync(h, plan->d_res, (size_t)n * sizeof(pg_sch_result), cudaMemcpyDeviceToHost, s),
+                      "D2H results");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(hpr, plan->d_pr, (size_t)n * 4 * sizeof(pg_port_result), cudaMemcpyDeviceToHost, s),
+                    "D2H port results");
+  }
+  if (rc == PG_OK && plan->tb_bytes > 0) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(htb, plan->d_tb_out, plan->tb_bytes, cudaMemcpyDeviceToHost, s), "D2H TBs");
+  }
+  return rc;
+}
+
+int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (grids == nullptr) {
+    return set_error(ctx, PG_ERR_INVALID, "null host buffer");
+  }
+  if (plan->submitted - plan->collected >= 2) {
+    return set_error(ctx, PG_ERR_INVALID, "two slots in flight: collect one before submitting another");
+  }
+  const size_t grid_bytes = plan->grid_words * 4;
+  const size_t n          = (size_t)plan->nof_ues;
+  const size_t h_bytes    = al(n * sizeof(pg_sch_result)) + al(n * 4 * sizeof(pg_port_result)) + al(plan->tb_bytes);
+  int          rc         = PG_OK;
+  if (plan->copy_stream == nullptr) {
+    rc = check_cuda(ctx, cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (cudaEvent_t* e : {&plan->ev_h2d, &plan->ev_stage_free, &plan->ev_done[0], &plan->ev_done[1]}) {
+      if (rc == PG_OK) {
+        rc = check_cuda(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
+      }
+    }
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx, cudaMalloc(&plan->d_stage, std::max<size_t>(grid_bytes, 4)), "cudaMalloc(staging grids)");
+    }
+    for (void** h : {&plan->host_slot[0], &plan->host_slot[1]}) {
+      if (rc == PG_OK) {
+        rc = check_cuda(ctx, cudaMallocHost(h, std::max<size_t>(h_bytes, 64)), "cudaMallocHost(result slot)");
+      }
+    }
+    if (rc != PG_OK) {
+      return rc;
+    }
+  }
+  cudaStream_t s    = ctx->stream;
+  const int    slot = (int)(plan->submitted & 1u);
+  // Copy stream: the staging buffer is free once the previous slot has moved it into the grid
+  // buffer; the H2D then overlaps whatever the compute stream runs.
+  rc = check_cuda(ctx, cudaStreamWaitEvent(plan->copy_stream, plan->ev_stage_free, 0), "cudaStreamWaitEvent");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_stage, grids, grid_bytes, cudaMemcpyHostToDevice, plan->copy_stream),
+                    "H2D grids");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventRecord(plan->ev_h2d, plan->copy_stream), "cudaEventRecord");
+  }
+  // Compute stream: the grids into the plan's grid buffer (after the previous slot's plan, same
+  // stream), the plan, the results back.
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamWaitEvent(s, plan->ev_h2d, 0), "cudaStreamWaitEvent");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, plan->d_stage, grid_bytes, cudaMemcpyDeviceToDevice, s),
+                    "D2D grids");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventRecord(plan->ev_stage_free, s), "cudaEventRecord");
+  }
+  if (rc == PG_OK) {
+    rc = pg_pusch_plan_execute_device(plan, plan->d_grid, plan->d_tb_out, plan->d_res, plan->d_pr, s);
+  }
+  if (rc == PG_OK) {
+    rc = enqueue_results_d2h(plan, static_cast<uint8_t*>(plan->host_slot[slot]), s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventRecord(plan->ev_done[slot], s), "cudaEventRecord");
+  }
+  if (rc == PG_OK) {
+    ++plan->submitted;
+  }
+  return rc;
+}
+
+int pg_pusch_plan_collect_host(pg_pusch_plan* plan, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results,
+                               pg_port_result* port_results)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (results == nullptr || (tb_out == nullptr && plan->tb_bytes > 0)) {
+    return set_error(ctx, PG_ERR_INVALID, "null host buffer");
+  }
+  if (tb_out_len < plan->tb_bytes) {
+    return set_error(ctx, PG_ERR_INVALID, "transport-block buffer smaller than the plan's TBs");
+  }
+  if (plan->collected == plan->submitted) {
+    return set_error(ctx, PG_ERR_INVALID, "no slot submitted");
+  }
+  const int slot = (int)(plan->collected & 1u);
+  if (int rc = check_cuda(ctx, cudaEventSynchronize(plan->ev_done[slot]), "cudaEventSynchronize")) {
+    return rc;
+  }
+  copy_results_out(plan, static_cast<const uint8_t*>(plan->host_slot[slot]), tb_out, results, port_results);
+  ++plan->collected;
+  return PG_OK;
 }
 
 static int execute_host_tail(pg_pusch_plan* plan, uint8_t* tb_out, pg_sch_result* results,

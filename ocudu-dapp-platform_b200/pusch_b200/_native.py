@@ -175,6 +175,8 @@ SIGNATURES = {
     "pg_pusch_plan_set_harq": (ctypes.c_int, [_VP, _VP, _VP]),
     "pg_ulsch_demultiplex_sizes": (ctypes.c_int, [_VP, _VP]),
     "pg_bfp_prb_bytes": (ctypes.c_int, [ctypes.c_int]),
+    "pg_pusch_plan_submit_host": (ctypes.c_int, [_VP, _VP]),
+    "pg_pusch_plan_collect_host": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t, _VP, _VP]),
     "pg_bfp_decompress_device": (ctypes.c_int, [_VP, _VP, ctypes.c_uint32, ctypes.c_int, _VP, _VP]),
     "pg_pusch_plan_execute_host_bfp": (ctypes.c_int, [_VP, _VP, ctypes.c_size_t, ctypes.c_int, _VP, ctypes.c_size_t,
                                                       _VP, _VP]),

@@ -199,6 +199,24 @@ class PuschSlotPlan:
                                                            ctypes.addressof(pr) if pr is not None else None))
         return results_from(self.descs, res, pr, tb)
 
+    def submit_host(self, grid: np.ndarray):
+        """Pipelined execution: enqueues one slot (pg_pusch_plan_submit_host). The grid array must stay
+        alive and unchanged until the matching collect_host returns."""
+        grid = np.ascontiguousarray(grid, dtype=np.uint32)
+        self._inflight = getattr(self, "_inflight", []) + [grid]
+        self.ctx.check(self.lib.pg_pusch_plan_submit_host(self.handle, grid.ctypes.data_as(ctypes.c_void_p)))
+
+    def collect_host(self, with_port_results=True) -> List[PuschResult]:
+        """Results of the oldest submitted slot (pg_pusch_plan_collect_host)."""
+        tb = np.zeros(max(self.tb_bytes, 1), np.uint8)
+        res = (PgSchResult * self.n)()
+        pr = (PgPortResult * (4 * self.n))() if with_port_results else None
+        self.ctx.check(self.lib.pg_pusch_plan_collect_host(self.handle, tb.ctypes.data_as(ctypes.c_void_p), tb.size,
+                                                           ctypes.addressof(res),
+                                                           ctypes.addressof(pr) if pr is not None else None))
+        self._inflight = self._inflight[1:]
+        return results_from(self.descs, res, pr, tb)
+
     def execute_host_bfp(self, compressed: np.ndarray, data_width: int, with_port_results=True) -> List[PuschResult]:
         """execute_host with the grids as O-RAN BFP-compressed PRBs (pg_pusch_plan_execute_host_bfp)."""
         compressed = np.ascontiguousarray(compressed, dtype=np.uint8)

@@ -115,3 +115,35 @@ def test_autotuner_keeps_results(ctx):
     with pytest.raises(Exception):
         plan.set_tuning(PgPuschPlanTuning(0, 1, 256, 2, 0))
     plan.close()
+
+
+def test_pipelined_host_execution(ctx):
+    """submit_host / collect_host over three slots with two in flight give, slot by slot, the
+    results of execute_host on the same grids; the in-flight limit and an empty collect are errors."""
+    from pusch_b200._native import PgError
+    slots = sim.uneven_cells(seed=13, nof_cells=2)
+    plan = PuschSlotPlan(ctx, slots, max_iterations=6)
+    grids = [plan.grid] + [np.concatenate([np.ascontiguousarray(sl.grid, np.uint32).ravel()
+                                           for sl in [same_config_slot(x, 200 + 10 * k + i) for i, x in enumerate(slots)]])
+                           for k in range(2)]
+    want = [plan.execute_host(g) for g in grids]
+    try:
+        with pytest.raises(PgError):
+            plan.collect_host()
+        plan.submit_host(grids[0])
+        plan.submit_host(grids[1])
+        with pytest.raises(PgError):
+            plan.submit_host(grids[2])
+        got = [plan.collect_host()]
+        plan.submit_host(grids[2])
+        got += [plan.collect_host(), plan.collect_host()]
+        for g_slot, w_slot in zip(got, want):
+            for g, w in zip(g_slot, w_slot):
+                assert (g.tb_crc_ok, g.nof_codeblocks_crc_ok, g.mean_iterations) == \
+                    (w.tb_crc_ok, w.nof_codeblocks_crc_ok, w.mean_iterations)
+                assert np.array_equal(g.noise_var, w.noise_var)
+                if g.tb_crc_ok:
+                    assert np.array_equal(g.transport_block, w.transport_block)
+        assert sum(r.tb_crc_ok for r in got[2]) >= 0.9 * plan.n
+    finally:
+        plan.close()
