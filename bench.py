@@ -367,15 +367,7 @@ def run_ours_pusch(args):
     bits_all = int(sum(u.tbs_bits for u in plan.ues))
     bler = 1.0 - sum(good) / n
 
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-        b = torch.tensor([bits_ok], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(b)
-        total_bits = float(b.item())
-    else:
-        ms_max, total_bits = ms, float(bits_ok)
+    ms_max, total_bits = max_over_ranks(ms, world), sum_over_ranks(bits_ok, world)
     value = total_bits / (ms_max * 1e-3) / 1e6
 
     # Plain per-UE GPU path: one plan per UE, each executed and waited for before the next UE.
@@ -441,10 +433,7 @@ def run_ours_pusch(args):
         e_ms = 1e3 * statistics.mean(et)
         e_ok = [bool(h_res[i].tb_crc_ok) for i in range(n)]
         assert e_ok == [r.tb_crc_ok for r in results]
-        if world > 1:
-            t = torch.tensor([e_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e_ms, world)
         e2e = {"value": round(total_bits / (e_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
                "h2d_bytes_per_step": int(plan.grid.size * 4),
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
@@ -467,10 +456,7 @@ def run_ours_pusch(args):
         np_steps = min(args.steps, 200)
         p_ms = 1e3 * pipelined(np_steps) / np_steps
         assert [bool(h_res[i].tb_crc_ok) for i in range(n)] == [r.tb_crc_ok for r in results]
-        if world > 1:
-            t = torch.tensor([p_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            p_ms = float(t.item())
+        p_ms = max_over_ranks(p_ms, world)
         # The headline end-to-end figure is the pipelined one (consecutive slots, as a PHY runs them);
         # the one-call-at-a-time figure stays beside it.
         e2e = {"value": round(total_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
@@ -508,10 +494,7 @@ def run_ours_pusch(args):
             if h_res[i].tb_crc_ok and (np.unpackbits(tbh[d.tb_out_offset:d.tb_out_offset + d.tbs_bits // 8])
                                        == truth[i]).all():
                 b_bits += d.tbs_bits
-        if world > 1:
-            t = torch.tensor([b_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            b_ms = float(t.item())
+        b_ms = max_over_ranks(b_ms, world)
         e2e["ofh_bfp9"] = {"value": round(b_bits / (b_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
                            "h2d_bytes_per_step": int(h_comp.numel()),
                            "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
@@ -710,15 +693,7 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     iters = d_it.cpu().numpy()
     bits_ok, bits_all, ops, edge_updates = workload_stats(batch, iters)
 
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-        b = torch.tensor([bits_ok], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(b)
-        total_bits = float(b.item())
-    else:
-        ms_max, total_bits = ms, float(bits_ok)
+    ms_max, total_bits = max_over_ranks(ms, world), sum_over_ranks(bits_ok, world)
     value = total_bits / (ms_max * 1e-3) / 1e9
 
     # End to end through the host C ABI: pinned LLRs in, bits + iterations out, every step.
@@ -745,10 +720,7 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
             et.append(time.perf_counter() - t0)
         assert (h_it.numpy() == iters).all()
         e_ms = 1e3 * statistics.mean(et)
-        if world > 1:
-            t = torch.tensor([e_ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = float(t.item())
+        e_ms = max_over_ranks(e_ms, world)
         e2e = {"value": round(total_bits / (e_ms * 1e-3) / 1e9, 4), "unit": "Gbit/s",
                "h2d_bytes_per_step": int(h_llrs.numel() + len(bytes(descs))),
                "d2h_bytes_per_step": int(h_bits.numel() + 4 * N_CBS), "ms_per_step": round(e_ms, 3)}
@@ -812,6 +784,26 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
         }
     dec.ctx.close()
     return line
+
+
+def max_over_ranks(x, world, device="cuda"):
+    """The largest x over the ranks (times are taken as the slowest rank's)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world, device="cuda"):
+    """The sum of x over the ranks (work done by the whole job)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t)
+    return float(t.item())
 
 
 def dist_setup():
