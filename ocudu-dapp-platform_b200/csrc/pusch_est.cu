@@ -27,7 +27,7 @@
 
 namespace {
 
-constexpr int kEstThreads = 256;
+constexpr int kEstThreads = 512;
 constexpr int kMaxV       = 12;
 constexpr int kMaxPil     = 6 * 275;
 constexpr int kMaxDmrs    = 2;
