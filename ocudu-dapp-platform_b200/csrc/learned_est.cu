@@ -93,6 +93,7 @@ struct pg_le_net {
   float*      adam_v   = nullptr;
   uint16_t*   wf       = nullptr; // packed forward weights
   uint16_t*   wt       = nullptr; // packed transposed weights (input gradients)
+  uint16_t*   wp       = nullptr; // packed weights of the fused inference kernel (taps along N)
   uint16_t*   x        = nullptr; // [2][R][8]
   uint16_t*   act[8]   = {};      // act[1..7]: [8][R][8] (act[0] = x)
   uint16_t*   mid[kBlocks] = {};  // [8][R][8]
@@ -267,9 +268,11 @@ __device__ __forceinline__ uint16_t bf16_bits(float f)
 }
 
 // Adam step (when update != 0) on every parameter, then the packed BF16 copies of the weights for
-// the forward and the input-gradient convolutions; the gradients are cleared for the next step.
+// the forward and the input-gradient convolutions and for the fused inference kernel; the gradients
+// are cleared for the next step.
 __global__ void le_adam_kernel(float* __restrict__ p, float* __restrict__ grad, float* __restrict__ m,
-                               float* __restrict__ v, uint16_t* __restrict__ wf, uint16_t* __restrict__ wt, int total,
+                               float* __restrict__ v, uint16_t* __restrict__ wf, uint16_t* __restrict__ wt,
+                               uint16_t* __restrict__ wp, int total,
                                int update, float lr, float b1, float b2, float eps, float wd, float bc1, float bc2)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -304,6 +307,7 @@ __global__ void le_adam_kernel(float* __restrict__ p, float* __restrict__ grad, 
     const uint16_t b = bf16_bits(w);
     wf[L.p_off + ((t * (L.cin / 8) + ci / 8) * L.cout + co) * 8 + (ci & 7)]              = b;
     wt[L.p_off + (((kTaps - 1 - t) * (L.cout / 8) + co / 8) * L.cin + ci) * 8 + (co & 7)] = b;
+    wp[L.p_off + (((ci / 8) * kTaps + (kTaps - 1 - t)) * L.cout + co) * 8 + (ci & 7)]     = b;
   }
 }
 
@@ -312,46 +316,59 @@ size_t al(size_t x)
   return (x + 255) & ~(size_t)255;
 }
 // ---------------------------------------------------------------------------------------------
-// Fused inference: the whole network per window of 384 rows in one kernel, activations in shared
+// Fused inference: the whole network per window of 512 rows in one kernel, activations in shared
 // memory, accumulators in tensor memory, each layer's weights brought in by 1-D bulk copies while
 // the previous layer computes. Every layer loses two exact rows at each window edge (its taps reach
-// two rows beyond), so after 14 layers the central 328 rows are exact and are the ones stored:
-// windows overlap by 56 rows. Buffers: X (16 input channels), A (block input and output; the second
-// layer of a block adds A and writes A in place, row by row), B (block middle); two zero rows
-// before and after the window in every buffer.
+// two rows beyond), so after 14 layers the central 456 rows are exact and are the ones stored:
+// windows overlap by 56 rows.
 //
-// Dataflow within a window (no CTA-wide barrier between layers): the window is three M tiles of 128
-// rows. A producer warp issues the MMAs of tile c of layer l as soon as the epilogues of layer l - 1
-// for tiles c - 1, c and c + 1 (the rows its taps read, and the accumulator columns it overwrites)
-// have arrived on their barriers, and commits them to tile c's barrier. Eight epilogue warps per
-// tile (two per TMEM lane quarter, one per half of the output channels) wait for that commit, add
-// bias and residual, apply the ReLU and the row mask, store bf16 to shared memory, make the stores
-// visible to the tensor cores and arrive. So the MMAs of one tile overlap the epilogues of the
-// others, across layer boundaries. The epilogue of layer l, tile c writes its destination buffer
-// only after its own MMAs, which waited for every MMA of layer l - 1 that read those rows.
-constexpr int      kFTiles     = 3;
-constexpr int      kFWin       = 128 * kFTiles;
-constexpr int      kFPad       = 2;
-constexpr int      kFRows      = kFWin + 2 * kFPad;
-constexpr int      kFMargin    = 2 * kLayers;
-constexpr int      kFOut       = kFWin - 2 * kFMargin;
-constexpr int      kFEpiWarps  = 8 * kFTiles;
-constexpr int      kFThreads   = 32 * (kFEpiWarps + 1); // + producer warp
-constexpr uint32_t kFChunkB    = kFRows * 16;
-constexpr uint32_t kFActB      = 8 * kFChunkB;
-constexpr uint32_t kFXB        = 2 * kFChunkB;
-constexpr uint32_t kFWB        = kTaps * 8 * kCh * 16;
-constexpr uint32_t kFOffX      = 2 * kFActB;
-constexpr uint32_t kFOffW      = kFOffX + kFXB;
-constexpr uint32_t kFOffBias   = kFOffW + 2 * kFWB;
-constexpr uint32_t kFOffVal    = kFOffBias + kLayers * kCh * 4;
-constexpr uint32_t kFOffBar    = kFOffVal + kFWin;
-constexpr int      kFBars      = 2 * kFTiles + 2; // MMA done [3], epilogue done [3], weights [2]
-constexpr size_t   kFSmem      = kFOffBar + 8 * kFBars + 16;
-constexpr uint32_t kFCopy      = 16384; // bytes per bulk copy
-constexpr uint32_t kFCols      = 256;   // TMEM columns: 64 per M tile
-static_assert(kFOffX % 16 == 0 && kFOffW % 16 == 0 && kFOffBias % 16 == 0 && kFOffBar % 8 == 0, "smem layout");
+// Row pairs: an MMA row (M) is a pair of rows (2 r', 2 r' + 1) and its 2 x 64 accumulator columns
+// are the output channels of both rows, so one MMA of N = 128 reads each A row once for two output
+// rows. Shared memory keeps each buffer in two phase planes (even rows, odd rows), 8-channel chunks
+// of row-pair lines of 16 bytes, with one pad pair before and after the window in each plane. The A
+// operand x[2 r' + s] (s = -2 .. 3) is plane s & 1 starting floor(s / 2) pairs from r', a plain
+// start-address offset. It feeds output row 2 r' through tap s + 2 and row 2 r' + 1 through tap
+// s + 1, so the B operand of shift s is [W(s + 2) | W(s + 1)]: the weights are packed with the taps
+// in descending order along N (taps 4, 3, 2, 1, 0, cout rows each) and B is 2 cout rows starting at
+// tap s + 2. The two end shifts feed one row each (s = -2 row 2 r' through tap 0, s = 3 row
+// 2 r' + 1 through tap 4) and are N = cout MMAs into their half of the accumulator; they come first
+// in each tile, without accumulation, and initialise the two halves. Per 128-pair tile and 16 input
+// channels: 4 MMAs of N = 128 and 2 of N = 64, against 10 of N = 64 with one row per MMA row.
+//
+// Buffers: A (block input and output; the second layer of a block adds A and writes A in place,
+// row by row) and B (block middle; the 16 input features share its first two chunks, dead once
+// layer 0's MMAs have completed, which precedes every write of B).
+//
+// Dataflow: the window is two M tiles of 128 pairs; the taps of either tile reach one pair into the
+// other, so every layer depends on both tiles of the previous one. A producer warp waits for the
+// epilogue barrier of layer l - 1, issues the MMAs of tile 0 and commits them to tile 0's barrier,
+// then those of tile 1. Sixteen epilogue warps (four per TMEM lane quarter, 32 accumulator columns
+// each) take tile 0 as soon as its MMAs complete - while tile 1's run - then tile 1: they add bias
+// and residual, apply the ReLU and the row mask, store bf16 to shared memory, make the stores
+// visible to the tensor cores and arrive once per layer. MMAs complete in issue order, so the
+// epilogue of layer l writes its destination only after every MMA of layer l - 1 that read it.
+constexpr int      kFTiles    = 2;
+constexpr int      kFPairs    = 128 * kFTiles;
+constexpr int      kFWin      = 2 * kFPairs;
+constexpr int      kFPRows    = kFPairs + 2; // + one pad pair before and after, per plane
+constexpr int      kFMargin   = 2 * kLayers;
+constexpr int      kFOut      = kFWin - 2 * kFMargin;
+constexpr int      kFEpiWarps = 16;
+constexpr int      kFThreads  = 32 * (kFEpiWarps + 1); // + producer warp
+constexpr uint32_t kFChunkB   = kFPRows * 16;         // one 8-channel chunk of one plane
+constexpr uint32_t kFActB     = 2 * 8 * kFChunkB;     // [plane][chunk][pair]
+constexpr uint32_t kFWB       = kTaps * 8 * kCh * 16;
+constexpr uint32_t kFOffW     = 2 * kFActB;
+constexpr uint32_t kFOffBias  = kFOffW + 2 * kFWB;
+constexpr uint32_t kFOffVal   = kFOffBias + kLayers * kCh * 4;
+constexpr uint32_t kFOffBar   = kFOffVal + kFWin;
+constexpr int      kFBars     = kFTiles + 3; // MMA done [2], epilogue done, weights [2]
+constexpr size_t   kFSmem     = kFOffBar + 8 * kFBars + 16;
+constexpr uint32_t kFCopy     = 16384; // bytes per bulk copy
+constexpr uint32_t kFCols     = 256;   // TMEM columns: 128 per M tile
+static_assert(kFOffW % 16 == 0 && kFOffBias % 16 == 0 && kFOffBar % 8 == 0, "smem layout");
 static_assert(kFSmem <= 227 * 1024, "shared memory of the fused kernel");
+static_assert(kFChunkB % 16 == 0 && kFSmem < (1u << 18), "descriptor start addresses: 14 bits of 16-byte units");
 
 __device__ __forceinline__ uint32_t layer_weight_bytes(int l)
 {
@@ -359,10 +376,10 @@ __device__ __forceinline__ uint32_t layer_weight_bytes(int l)
 }
 
 // Bulk copy of layer l's packed weights into `dst`, completing on `bar`.
-__device__ __forceinline__ void fused_load_weights(const uint16_t* __restrict__ wf, int l, uint32_t dst, uint32_t bar)
+__device__ __forceinline__ void fused_load_weights(const uint16_t* __restrict__ wp, int l, uint32_t dst, uint32_t bar)
 {
   const uint32_t bytes = layer_weight_bytes(l);
-  const char*    src   = reinterpret_cast<const char*>(wf + c_layers[l].p_off);
+  const char*    src   = reinterpret_cast<const char*>(wp + c_layers[l].p_off);
   mbar_expect_tx(bar, bytes);
   for (uint32_t o = 0; o < bytes; o += kFCopy) {
     bulk_g2s(dst + o, src + o, min(kFCopy, bytes - o), bar);
@@ -375,17 +392,31 @@ __device__ __forceinline__ void fused_load_weights(const uint16_t* __restrict__ 
 template <int CIN, int COUT>
 __device__ __forceinline__ void fused_issue_tile(int c, uint32_t src, uint32_t wb, uint32_t tmem, uint32_t bar)
 {
-  constexpr uint32_t idesc = make_idesc(128, COUT, false, false);
-  constexpr uint32_t wtap  = (uint32_t)(CIN / 8) * COUT * 16;
-  const uint64_t     a0    = make_desc(src + (uint32_t)(c * 128) * 16u, kFChunkB, 128);
-  const uint64_t     b0    = make_desc(wb, COUT * 16, 128);
+  constexpr uint32_t idesc_pair = make_idesc(128, 2 * COUT, false, false);
+  constexpr uint32_t idesc_one  = make_idesc(128, COUT, false, false);
+  constexpr uint32_t lbo_b      = (uint32_t)kTaps * COUT * 16; // between 8-channel chunks of the weights
+  const uint64_t     a0         = make_desc(src + (uint32_t)(c * 128) * 16u, kFChunkB, 128);
+  const uint64_t     b0         = make_desc(wb, lbo_b, 128);
+  const uint32_t     d          = tmem + (uint32_t)(c * 128);
 #pragma unroll
-  for (int t = 0; t < kTaps; ++t) {
+  for (int kc = 0; kc < CIN / 16; ++kc) {
 #pragma unroll
-    for (int kc = 0; kc < CIN / 16; ++kc) {
-      const uint64_t ad = a0 + (uint64_t)(((uint32_t)t * 16u + (uint32_t)(2 * kc) * kFChunkB) >> 4);
-      const uint64_t bd = b0 + (uint64_t)(((uint32_t)t * wtap + (uint32_t)(2 * kc) * COUT * 16) >> 4);
-      mma_bf16(tmem + (uint32_t)(c * 64), ad, bd, idesc, (t | kc) != 0 ? 1u : 0u);
+    for (int i = 0; i < 6; ++i) {
+      const int      s      = i == 0 ? 3 : i - 3; // 3, -2, -1, 0, 1, 2
+      const uint32_t plane  = (uint32_t)(s & 1);
+      const uint32_t pofs   = (uint32_t)(1 + (s >> 1)); // 1 + floor(s / 2), pairs
+      const uint32_t a_off  = (plane * 8u + 2u * (uint32_t)kc) * kFChunkB + pofs * 16u;
+      const uint32_t tap_hi = s == 3 ? 0u : (uint32_t)(2 - s); // first B tap block (descending taps)
+      const uint32_t b_off  = 2u * (uint32_t)kc * lbo_b + tap_hi * COUT * 16u;
+      const uint64_t ad     = a0 + (uint64_t)(a_off >> 4);
+      const uint64_t bd     = b0 + (uint64_t)(b_off >> 4);
+      if (s == 3) {
+        mma_bf16(d + COUT, ad, bd, idesc_one, kc != 0 ? 1u : 0u);
+      } else if (s == -2) {
+        mma_bf16(d, ad, bd, idesc_one, kc != 0 ? 1u : 0u);
+      } else {
+        mma_bf16(d, ad, bd, idesc_pair, 1u);
+      }
     }
   }
   mma_commit(bar);
@@ -406,14 +437,20 @@ __device__ __forceinline__ bool fused_wait(uint32_t bar, uint32_t parity, volati
   return false;
 }
 
+__device__ __forceinline__ uint32_t fused_line(int plane, int chunk, int pair) // byte offset in a buffer
+{
+  return ((uint32_t)(plane * 8 + chunk)) * kFChunkB + (uint32_t)pair * 16u;
+}
+
 __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const uint4* __restrict__ x,
                                                                         const uint8_t* __restrict__ row_valid,
-                                                                        const uint16_t* __restrict__ wf,
+                                                                        const uint16_t* __restrict__ wp,
                                                                         const float* __restrict__ params, int R,
                                                                         uint4* __restrict__ y, int* __restrict__ err)
 {
   extern __shared__ __align__(128) unsigned char smem[];
-  uint4*             xs       = reinterpret_cast<uint4*>(smem + kFOffX);
+  unsigned char*     buf_a    = smem;
+  unsigned char*     buf_b    = smem + kFActB;
   float*             bias_s   = reinterpret_cast<float*>(smem + kFOffBias);
   uint8_t*           valid_s  = smem + kFOffVal;
   uint64_t*          bars     = reinterpret_cast<uint64_t*>(smem + kFOffBar);
@@ -426,9 +463,11 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   if ((int)blockIdx.x >= ntiles) {
     return;
   }
-  for (int i = tid; i < 2 * 8 * 2 * kFPad; i += kFThreads) {
-    const int b = i / (8 * 2 * kFPad), c = (i / (2 * kFPad)) % 8, k = i % (2 * kFPad);
-    reinterpret_cast<uint4*>(smem + b * kFActB + c * kFChunkB)[k < kFPad ? k : kFWin + k] = make_uint4(0, 0, 0, 0);
+  // Pad pairs of every plane and chunk of both buffers: zero (those of B's first two chunks take
+  // the input features of the rows beyond the window, loaded with each window).
+  for (int i = tid; i < 2 * 2 * 8 * 2; i += kFThreads) {
+    const int b = i >> 5, pl = (i >> 4) & 1, ch = (i >> 1) & 7, e = i & 1;
+    *reinterpret_cast<uint4*>(smem + b * kFActB + fused_line(pl, ch, e ? kFPRows - 1 : 0)) = make_uint4(0, 0, 0, 0);
   }
   for (int i = tid; i < kLayers * kCh; i += kFThreads) {
     const int        l = i / kCh, co = i - l * kCh;
@@ -437,43 +476,44 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   }
   const bool     producer = warp == kFEpiWarps;
   const uint32_t bar_mma  = smem_u32(&bars[0]);           // + 8c
-  const uint32_t bar_epi  = smem_u32(&bars[kFTiles]);     // + 8c
-  const uint32_t bar_w    = smem_u32(&bars[2 * kFTiles]); // + 8b
+  const uint32_t bar_epi  = smem_u32(&bars[kFTiles]);
+  const uint32_t bar_w    = smem_u32(&bars[kFTiles + 1]); // + 8b
   const uint32_t wbuf0    = smem_u32(smem + kFOffW);
-  const uint32_t act0     = smem_u32(smem);
+  const uint32_t act_a    = smem_u32(buf_a);
+  const uint32_t act_b    = smem_u32(buf_b);
   if (warp == 0) {
     tmem_alloc(smem_u32(tmem_sm), kFCols);
   }
   if (producer && lane == 0) {
     for (int c = 0; c < kFTiles; ++c) {
       mbar_init(bar_mma + 8u * c, 1);
-      mbar_init(bar_epi + 8u * c, 8);
     }
+    mbar_init(bar_epi, kFEpiWarps);
     mbar_init(bar_w, 1);
     mbar_init(bar_w + 8u, 1);
     *abort_sm = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    fused_load_weights(wf, 0, wbuf0, bar_w);
+    fused_load_weights(wp, 0, wbuf0, bar_w);
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_sm;
-  // Epilogue role: tile mc, lane quarter q, channel half hh; window row r.
-  const int      mc   = warp / 8;
-  const int      q    = warp & 3;
-  const int      hh   = (warp >> 2) & 1;
-  const int      r    = mc * 128 + q * 32 + lane;
-  const uint32_t tad  = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(mc * 64 + hh * 32);
-  uint32_t       step = 0;     // layer steps of this CTA (all roles count alike)
-  uint32_t       w_issued = 1; // producer: weight loads issued (load k went to buffer k & 1)
+  // Epilogue role: TMEM lane quarter q, accumulator columns 32 cs .. 32 cs + 31 of each tile (plane
+  // cs >> 1, channel half cs & 1; in the last layer warps cs < 2 take plane cs, 16 columns).
+  const int      q          = warp & 3;
+  const int      cs         = (warp >> 2) & 3;
+  uint32_t       step       = 0; // layer steps of this CTA (all roles count alike)
+  uint32_t       w_issued   = 1; // producer: weight loads issued (load k went to buffer k & 1)
   uint32_t       mma_issued = 0; // producer: layer steps whose MMAs were issued
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int base = tile * kFOut - kFMargin; // global row of window row 0
-    for (int i = tid; i < 2 * kFRows; i += kFThreads) {
-      const int c = i / kFRows, rr = i - c * kFRows, g = base - kFPad + rr;
-      xs[i]       = (g >= 0 && g < R) ? x[(size_t)c * R + g] : make_uint4(0, 0, 0, 0);
+    // Input features: window rows -2 .. kFWin + 1 (pairs 0 .. kFPRows - 1 of both planes).
+    for (int i = tid; i < 2 * 2 * kFPRows; i += kFThreads) {
+      const int ch = i / (2 * kFPRows), w = i - ch * 2 * kFPRows - 2, g = base + w;
+      *reinterpret_cast<uint4*>(buf_b + fused_line(w & 1, ch, (w >> 1) + 1)) =
+          (g >= 0 && g < R) ? x[(size_t)ch * R + g] : make_uint4(0, 0, 0, 0);
     }
     for (int i = tid; i < kFWin; i += kFThreads) {
       const int g = base + i;
@@ -490,25 +530,19 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
       if (lane == 0) {
         for (int l = 0; l < kLayers; ++l) {
           const uint32_t s   = step + (uint32_t)l;
-          const uint32_t src = l == 0 ? smem_u32(xs) : act0 + ((l & 1) ? 0u : kFActB);
+          const uint32_t src = (l & 1) ? act_a : act_b;
           if (!fused_wait(bar_w + 8u * (s & 1), (s >> 1) & 1u, abort_sm, err)) {
             break;
           }
-          const uint32_t wb = wbuf0 + (s & 1) * kFWB;
-          // Layer 0 follows the window barrier; later layers wait for the epilogues of layer l - 1
-          // that tile c depends on (each barrier phase waited once: tiles 0 and 1 before tile 0,
-          // tile 2 before tile 1).
-          bool ok = true;
-          for (int c = 0; c < kFTiles && ok; ++c) {
-            if (l > 0) {
-              for (int d = (c == 0 ? 0 : c + 1); d <= min(c + 1, kFTiles - 1) && ok; ++d) {
-                ok = fused_wait(bar_epi + 8u * d, (s - 1) & 1u, abort_sm, err);
-              }
-              tc_fence_after();
-            }
-            if (!ok) {
+          // Layer 0 follows the window barrier; later layers wait for every epilogue of layer l - 1.
+          if (l > 0) {
+            if (!fused_wait(bar_epi, (s - 1) & 1u, abort_sm, err)) {
               break;
             }
+            tc_fence_after();
+          }
+          const uint32_t wb = wbuf0 + (s & 1) * kFWB;
+          for (int c = 0; c < kFTiles; ++c) {
             if (l == 0) {
               fused_issue_tile<kInCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
             } else if (l == kLayers - 1) {
@@ -517,35 +551,38 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
               fused_issue_tile<kCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
             }
           }
-          if (!ok) {
-            break;
-          }
           mma_issued = s + 1;
           // Every MMA of layer l - 1 has completed (its epilogues have arrived), so its weight
           // buffer takes the next layer (layer 0 of the next window after the last layer).
           if (l + 1 < kLayers || tile + (int)gridDim.x < ntiles) {
-            fused_load_weights(wf, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
+            fused_load_weights(wp, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
             ++w_issued;
           }
         }
       }
       __syncwarp();
     } else {
-      const bool valid = valid_s[r] != 0;
       for (int l = 0; l < kLayers; ++l) {
-        const uint32_t s  = step + (uint32_t)l;
-        const bool     ok = fused_wait(bar_mma + 8u * mc, s & 1u, abort_sm, err);
-        __syncwarp();
-        if (ok) {
+        const uint32_t s = step + (uint32_t)l;
+        for (int c = 0; c < kFTiles; ++c) {
+          const bool ok = fused_wait(bar_mma + 8u * c, s & 1u, abort_sm, err);
+          __syncwarp();
+          if (!ok) {
+            continue;
+          }
           tc_fence_after();
-          const float* bl = bias_s + l * kCh + hh * 32;
+          const int      pr  = c * 128 + q * 32 + lane;                 // window row pair
+          const uint32_t tad = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 128);
           if (l < kLayers - 1) {
-            // 32 output channels (chunks 4 hh .. 4 hh + 3) of row r: one TMEM load, the residual
+            // 32 output channels (chunks 4 hh .. 4 hh + 3) of one row: one TMEM load, the residual
             // and bias loads issued together, then straight-line arithmetic.
+            const int      plane  = cs >> 1, hh = cs & 1;
+            const bool     valid  = valid_s[2 * pr + plane] != 0;
             const bool     second = l >= 2 && (l & 1) == 0;
-            unsigned char* dst    = smem + ((l == 0 || second) ? 0u : kFActB);
-            uint4*         p      = reinterpret_cast<uint4*>(dst + (hh * 4) * kFChunkB) + (r + kFPad);
-            constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk column
+            unsigned char* dst    = (l & 1) ? buf_b : buf_a;
+            uint4*         p      = reinterpret_cast<uint4*>(dst + fused_line(plane, hh * 4, pr + 1));
+            constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk
+            const float*   bl     = bias_s + l * kCh + hh * 32;
             uint4          res[4];
             if (second) {
 #pragma unroll
@@ -554,7 +591,7 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
               }
             }
             float v[32];
-            tmem_ld32(tad, v);
+            tmem_ld32(tad + (uint32_t)(32 * cs), v);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
               const float4 b0 = reinterpret_cast<const float4*>(bl)[2 * k];
@@ -582,11 +619,15 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
               p[k * kStep] = pk;
             }
             fence_async_shared();
-          } else if (hh == 0) {
-            float v[16];
-            tmem_ld16(tad, v);
-            const int g = base + r;
-            if (r >= kFMargin && r < kFMargin + kFOut && g < R) {
+          } else if (cs < 2) {
+            const int    plane = cs;
+            const int    wr    = 2 * pr + plane; // window row
+            const bool   valid = valid_s[wr] != 0;
+            const float* bl    = bias_s + l * kCh;
+            float        v[16];
+            tmem_ld16(tad + (uint32_t)(kOutCh * plane), v);
+            const int g = base + wr;
+            if (wr >= kFMargin && wr < kFMargin + kFOut && g < R) {
 #pragma unroll
               for (int h = 0; h < 2; ++h) {
                 uint4 pk = make_uint4(0, 0, 0, 0);
@@ -604,7 +645,7 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
         tc_fence_before();
         __syncwarp();
         if (lane == 0) {
-          mbar_arrive(bar_epi + 8u * mc);
+          mbar_arrive(bar_epi);
         }
       }
     }
@@ -679,7 +720,7 @@ int fused_forward(pg_le_net* net, int R, cudaStream_t s)
   const int ntiles = (R + kFOut - 1) / kFOut;
   const int grid   = std::max(1, std::min(ntiles, net->ctx->sm_count));
   le_fused_forward_kernel<<<grid, kFThreads, kFSmem, s>>>(reinterpret_cast<const uint4*>(net->x), net->row_valid,
-                                                          net->wf, net->params, R, reinterpret_cast<uint4*>(net->y),
+                                                          net->wp, net->params, R, reinterpret_cast<uint4*>(net->y),
                                                           net->err);
   return pg::check_cuda(net->ctx, cudaGetLastError(), "le_fused_forward_kernel launch");
 }
@@ -739,7 +780,7 @@ int pack_launch(pg_le_net* net, int update, const pg_le_adam* opt, cudaStream_t 
     bc2 = 1.f - std::pow(b2, (float)net->step);
   }
   le_adam_kernel<<<(total + 255) / 256, 256, 0, s>>>(net->params, net->grads, net->adam_m, net->adam_v, net->wf,
-                                                     net->wt, total, update, lr, b1, b2, eps, wd, bc1, bc2);
+                                                     net->wt, net->wp, total, update, lr, b1, b2, eps, wd, bc1, bc2);
   return pg::check_cuda(net->ctx, cudaGetLastError(), "le_adam_kernel launch");
 }
 
@@ -862,7 +903,8 @@ int pg_le_create(pg_context* ctx, int max_rows, pg_le_net** out)
     return o;
   };
   const size_t o_p = take(P * 4), o_g = take(P * 4), o_m = take(P * 4), o_v = take(P * 4);
-  const size_t o_wf = take((size_t)T.npacked * 2), o_wt = take((size_t)T.npacked * 2);
+  const size_t o_wf = take((size_t)T.npacked * 2), o_wt = take((size_t)T.npacked * 2),
+               o_wp = take((size_t)T.npacked * 2);
   const size_t o_x = take(R * 32), o_y = take(R * 32), o_dy = take(R * 32);
   size_t o_act[8] = {}, o_mid[kBlocks] = {};
   for (int i = 1; i <= kBlocks + 1; ++i) {
@@ -904,6 +946,7 @@ int pg_le_create(pg_context* ctx, int max_rows, pg_le_net** out)
   n->adam_v    = reinterpret_cast<float*>(b + o_v);
   n->wf        = reinterpret_cast<uint16_t*>(b + o_wf);
   n->wt        = reinterpret_cast<uint16_t*>(b + o_wt);
+  n->wp        = reinterpret_cast<uint16_t*>(b + o_wp);
   n->x         = reinterpret_cast<uint16_t*>(b + o_x);
   n->y         = reinterpret_cast<uint16_t*>(b + o_y);
   n->dy        = reinterpret_cast<uint16_t*>(b + o_dy);
