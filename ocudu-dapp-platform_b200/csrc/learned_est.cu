@@ -353,6 +353,7 @@ constexpr int      kFWin      = 2 * kFPairs;
 constexpr int      kFPRows    = kFPairs + 2; // + one pad pair before and after, per plane
 constexpr int      kFMargin   = 2 * kLayers;
 constexpr int      kFOut      = kFWin - 2 * kFMargin;
+constexpr int      kFOutHalf  = kFWin / 2 - 2 * kFMargin; // exact rows of a one-tile window
 constexpr int      kFEpiWarps = 16;
 constexpr int      kFThreads  = 32 * (kFEpiWarps + 1); // + producer warp
 constexpr uint32_t kFChunkB   = kFPRows * 16;         // one 8-channel chunk of one plane
@@ -362,7 +363,7 @@ constexpr uint32_t kFOffW     = 2 * kFActB;
 constexpr uint32_t kFOffBias  = kFOffW + 2 * kFWB;
 constexpr uint32_t kFOffVal   = kFOffBias + kLayers * kCh * 4;
 constexpr uint32_t kFOffBar   = kFOffVal + kFWin;
-constexpr int      kFBars     = kFTiles + 3; // MMA done [2], epilogue done, weights [2]
+constexpr int      kFBars     = 2 * kFTiles + 2; // MMA done [2], epilogue done [2], weights [2]
 constexpr size_t   kFSmem     = kFOffBar + 8 * kFBars + 16;
 constexpr uint32_t kFCopy     = 16384; // bytes per bulk copy
 constexpr uint32_t kFCols     = 256;   // TMEM columns: 128 per M tile
@@ -386,40 +387,54 @@ __device__ __forceinline__ void fused_load_weights(const uint16_t* __restrict__ 
   }
 }
 
-// The MMAs of M tile c of one layer, committed to `bar`. The descriptors are formed once; each
-// MMA adds its constant offset (16-byte units) to the start-address field, which stays below 2^14
-// (shared memory < 256 KB), so no carry reaches the LBO field.
-template <int CIN, int COUT>
-__device__ __forceinline__ void fused_issue_tile(int c, uint32_t src, uint32_t wb, uint32_t tmem, uint32_t bar)
+// The MMAs of one input shift s (x[2 r' + s], all input chunks) of M tile c. The descriptors are
+// formed once; each MMA adds its constant offset (16-byte units) to the start-address field, which
+// stays below 2^14 (shared memory < 256 KB), so no carry reaches the LBO field. Shift -1 comes first
+// in each tile and initialises both halves of the accumulator (N = 2 cout, no accumulation on the
+// first chunk); every other MMA accumulates.
+template <int CIN, int COUT, int S>
+__device__ __forceinline__ void fused_issue_shift(uint64_t a0, uint64_t b0, uint32_t d)
 {
   constexpr uint32_t idesc_pair = make_idesc(128, 2 * COUT, false, false);
   constexpr uint32_t idesc_one  = make_idesc(128, COUT, false, false);
   constexpr uint32_t lbo_b      = (uint32_t)kTaps * COUT * 16; // between 8-channel chunks of the weights
-  const uint64_t     a0         = make_desc(src + (uint32_t)(c * 128) * 16u, kFChunkB, 128);
-  const uint64_t     b0         = make_desc(wb, lbo_b, 128);
-  const uint32_t     d          = tmem + (uint32_t)(c * 128);
+  constexpr uint32_t plane      = (uint32_t)(S & 1);
+  constexpr uint32_t pofs       = (uint32_t)(1 + (S >> 1));      // 1 + floor(S / 2), pairs
+  constexpr uint32_t tap_hi     = S == 3 ? 0u : (uint32_t)(2 - S); // first B tap block (descending taps)
 #pragma unroll
   for (int kc = 0; kc < CIN / 16; ++kc) {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      const int      s      = i == 0 ? 3 : i - 3; // 3, -2, -1, 0, 1, 2
-      const uint32_t plane  = (uint32_t)(s & 1);
-      const uint32_t pofs   = (uint32_t)(1 + (s >> 1)); // 1 + floor(s / 2), pairs
-      const uint32_t a_off  = (plane * 8u + 2u * (uint32_t)kc) * kFChunkB + pofs * 16u;
-      const uint32_t tap_hi = s == 3 ? 0u : (uint32_t)(2 - s); // first B tap block (descending taps)
-      const uint32_t b_off  = 2u * (uint32_t)kc * lbo_b + tap_hi * COUT * 16u;
-      const uint64_t ad     = a0 + (uint64_t)(a_off >> 4);
-      const uint64_t bd     = b0 + (uint64_t)(b_off >> 4);
-      if (s == 3) {
-        mma_bf16(d + COUT, ad, bd, idesc_one, kc != 0 ? 1u : 0u);
-      } else if (s == -2) {
-        mma_bf16(d, ad, bd, idesc_one, kc != 0 ? 1u : 0u);
-      } else {
-        mma_bf16(d, ad, bd, idesc_pair, 1u);
-      }
+    const uint32_t a_off = (plane * 8u + 2u * (uint32_t)kc) * kFChunkB + pofs * 16u;
+    const uint32_t b_off = 2u * (uint32_t)kc * lbo_b + tap_hi * COUT * 16u;
+    const uint64_t ad    = a0 + (uint64_t)(a_off >> 4);
+    const uint64_t bd    = b0 + (uint64_t)(b_off >> 4);
+    if (S == 3) {
+      mma_bf16(d + COUT, ad, bd, idesc_one, 1u);
+    } else if (S == -2) {
+      mma_bf16(d, ad, bd, idesc_one, 1u);
+    } else {
+      mma_bf16(d, ad, bd, idesc_pair, (S == -1 && kc == 0) ? 0u : 1u);
     }
   }
-  mma_commit(bar);
+}
+
+// The MMAs of M tile c of one layer: part 0 the shifts that read no pair beyond the tile's end
+// (-1, -2, 0, 1), part 1 the two that read the next tile's first pair (2, 3), part 2 all six.
+template <int CIN, int COUT>
+__device__ __forceinline__ void fused_issue_tile(int c, int part, uint32_t src, uint32_t wb, uint32_t tmem)
+{
+  const uint64_t a0 = make_desc(src + (uint32_t)(c * 128) * 16u, kFChunkB, 128);
+  const uint64_t b0 = make_desc(wb, (uint32_t)kTaps * COUT * 16, 128);
+  const uint32_t d  = tmem + (uint32_t)(c * 128);
+  if (part != 1) {
+    fused_issue_shift<CIN, COUT, -1>(a0, b0, d);
+    fused_issue_shift<CIN, COUT, -2>(a0, b0, d);
+    fused_issue_shift<CIN, COUT, 0>(a0, b0, d);
+    fused_issue_shift<CIN, COUT, 1>(a0, b0, d);
+  }
+  if (part != 0) {
+    fused_issue_shift<CIN, COUT, 2>(a0, b0, d);
+    fused_issue_shift<CIN, COUT, 3>(a0, b0, d);
+  }
 }
 
 // Bounded wait that gives up at once when another thread has recorded a failure.
@@ -446,7 +461,8 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
                                                                         const uint8_t* __restrict__ row_valid,
                                                                         const uint16_t* __restrict__ wp,
                                                                         const float* __restrict__ params, int R,
-                                                                        uint4* __restrict__ y, int* __restrict__ err)
+                                                                        int n_full, int n_win, uint4* __restrict__ y,
+                                                                        int* __restrict__ err)
 {
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned char*     buf_a    = smem;
@@ -459,8 +475,7 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   const int          tid      = threadIdx.x;
   const int          warp     = tid >> 5;
   const int          lane     = tid & 31;
-  const int          ntiles   = (R + kFOut - 1) / kFOut;
-  if ((int)blockIdx.x >= ntiles) {
+  if ((int)blockIdx.x >= n_win) {
     return;
   }
   // Pad pairs of every plane and chunk of both buffers: zero (those of B's first two chunks take
@@ -476,8 +491,8 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   }
   const bool     producer = warp == kFEpiWarps;
   const uint32_t bar_mma  = smem_u32(&bars[0]);           // + 8c
-  const uint32_t bar_epi  = smem_u32(&bars[kFTiles]);
-  const uint32_t bar_w    = smem_u32(&bars[kFTiles + 1]); // + 8b
+  const uint32_t bar_epi  = smem_u32(&bars[kFTiles]);     // + 8c
+  const uint32_t bar_w    = smem_u32(&bars[2 * kFTiles]); // + 8b
   const uint32_t wbuf0    = smem_u32(smem + kFOffW);
   const uint32_t act_a    = smem_u32(buf_a);
   const uint32_t act_b    = smem_u32(buf_b);
@@ -487,8 +502,8 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   if (producer && lane == 0) {
     for (int c = 0; c < kFTiles; ++c) {
       mbar_init(bar_mma + 8u * c, 1);
+      mbar_init(bar_epi + 8u * c, kFEpiWarps);
     }
-    mbar_init(bar_epi, kFEpiWarps);
     mbar_init(bar_w, 1);
     mbar_init(bar_w + 8u, 1);
     *abort_sm = 0;
@@ -507,11 +522,17 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
   uint32_t       w_issued   = 1; // producer: weight loads issued (load k went to buffer k & 1)
   uint32_t       mma_issued = 0; // producer: layer steps whose MMAs were issued
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int base = tile * kFOut - kFMargin; // global row of window row 0
-    // Input features: window rows -2 .. kFWin + 1 (pairs 0 .. kFPRows - 1 of both planes).
-    for (int i = tid; i < 2 * 2 * kFPRows; i += kFThreads) {
-      const int ch = i / (2 * kFPRows), w = i - ch * 2 * kFPRows - 2, g = base + w;
+  for (int win = blockIdx.x; win < n_win; win += gridDim.x) {
+    // Windows 0 .. n_full - 1 have two M tiles, the rest one (kFOutHalf exact rows): the host picks
+    // the split that evens out the work of the CTAs. A one-tile window keeps the barrier protocol
+    // of two (its tile-1 steps arrive without work), so every barrier phase stays in step.
+    const bool two  = win < n_full;
+    const int  nout = two ? kFOut : kFOutHalf;
+    const int  base = (two ? win * kFOut : n_full * kFOut + (win - n_full) * kFOutHalf) - kFMargin;
+    const int  nrow = two ? kFWin : kFWin / 2; // window rows computed
+    // Input features: window rows -2 .. nrow + 1 (pairs 0 .. nrow / 2 + 1 of both planes).
+    for (int i = tid; i < 2 * (nrow + 4); i += kFThreads) {
+      const int ch = i / (nrow + 4), w = i - ch * (nrow + 4) - 2, g = base + w;
       *reinterpret_cast<uint4*>(buf_b + fused_line(w & 1, ch, (w >> 1) + 1)) =
           (g >= 0 && g < R) ? x[(size_t)ch * R + g] : make_uint4(0, 0, 0, 0);
     }
@@ -534,30 +555,51 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
           if (!fused_wait(bar_w + 8u * (s & 1), (s >> 1) & 1u, abort_sm, err)) {
             break;
           }
-          // Layer 0 follows the window barrier; later layers wait for every epilogue of layer l - 1.
+          const uint32_t wb    = wbuf0 + (s & 1) * kFWB;
+          auto           issue = [&](int c, int part) {
+            if (l == 0) {
+              fused_issue_tile<kInCh, kCh>(c, part, src, wb, tmem);
+            } else if (l == kLayers - 1) {
+              fused_issue_tile<kCh, kOutCh>(c, part, src, wb, tmem);
+            } else {
+              fused_issue_tile<kCh, kCh>(c, part, src, wb, tmem);
+            }
+          };
+          // Layer 0 follows the window barrier. Later layers: tile 0's first part reads tile 0 of
+          // layer l - 1 only, its second part and tile 1 also read tile 1 (and tile 1 overwrites
+          // tile 1's accumulator), so the epilogue barriers are waited in between.
           if (l > 0) {
             if (!fused_wait(bar_epi, (s - 1) & 1u, abort_sm, err)) {
               break;
             }
             tc_fence_after();
           }
-          const uint32_t wb = wbuf0 + (s & 1) * kFWB;
-          for (int c = 0; c < kFTiles; ++c) {
-            if (l == 0) {
-              fused_issue_tile<kInCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
-            } else if (l == kLayers - 1) {
-              fused_issue_tile<kCh, kOutCh>(c, src, wb, tmem, bar_mma + 8u * c);
-            } else {
-              fused_issue_tile<kCh, kCh>(c, src, wb, tmem, bar_mma + 8u * c);
+          issue(0, 0);
+          if (l > 0) {
+            if (!fused_wait(bar_epi + 8u, (s - 1) & 1u, abort_sm, err)) {
+              // Tile 0's first part is in flight: both barriers take its completion, so that the
+              // wait after a failure below covers it.
+              mma_commit(bar_mma);
+              mma_commit(bar_mma + 8u);
+              mma_issued = s + 1;
+              break;
             }
+            tc_fence_after();
           }
-          mma_issued = s + 1;
-          // Every MMA of layer l - 1 has completed (its epilogues have arrived), so its weight
-          // buffer takes the next layer (layer 0 of the next window after the last layer).
-          if (l + 1 < kLayers || tile + (int)gridDim.x < ntiles) {
+          // Every MMA of layer l - 1 has completed (both of its epilogues have arrived; before layer
+          // 0, the window barrier), so its weight buffer takes the next layer (layer 0 of the next
+          // window after the last layer), in flight while this layer's MMAs run.
+          if (l + 1 < kLayers || win + (int)gridDim.x < n_win) {
             fused_load_weights(wp, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
             ++w_issued;
           }
+          issue(0, 1);
+          mma_commit(bar_mma);
+          if (two) {
+            issue(1, 2);
+          }
+          mma_commit(bar_mma + 8u);
+          mma_issued = s + 1;
         }
       }
       __syncwarp();
@@ -565,87 +607,91 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
       for (int l = 0; l < kLayers; ++l) {
         const uint32_t s = step + (uint32_t)l;
         for (int c = 0; c < kFTiles; ++c) {
-          const bool ok = fused_wait(bar_mma + 8u * c, s & 1u, abort_sm, err);
-          __syncwarp();
-          if (!ok) {
-            continue;
+          // One lane polls the barrier and tells the others: probes from all 32 lanes take
+          // shared-memory cycles from the tensor cores' operand reads (measured 13 % slower).
+          bool ok = false;
+          if (lane == 0) {
+            ok = fused_wait(bar_mma + 8u * c, s & 1u, abort_sm, err);
           }
-          tc_fence_after();
-          const int      pr  = c * 128 + q * 32 + lane;                 // window row pair
-          const uint32_t tad = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 128);
-          if (l < kLayers - 1) {
-            // 32 output channels (chunks 4 hh .. 4 hh + 3) of one row: one TMEM load, the residual
-            // and bias loads issued together, then straight-line arithmetic.
-            const int      plane  = cs >> 1, hh = cs & 1;
-            const bool     valid  = valid_s[2 * pr + plane] != 0;
-            const bool     second = l >= 2 && (l & 1) == 0;
-            unsigned char* dst    = (l & 1) ? buf_b : buf_a;
-            uint4*         p      = reinterpret_cast<uint4*>(dst + fused_line(plane, hh * 4, pr + 1));
-            constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk
-            const float*   bl     = bias_s + l * kCh + hh * 32;
-            uint4          res[4];
-            if (second) {
-#pragma unroll
-              for (int k = 0; k < 4; ++k) {
-                res[k] = p[k * kStep];
-              }
-            }
-            float v[32];
-            tmem_ld32(tad + (uint32_t)(32 * cs), v);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              const float4 b0 = reinterpret_cast<const float4*>(bl)[2 * k];
-              const float4 b1 = reinterpret_cast<const float4*>(bl)[2 * k + 1];
-              const float  bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-              float        o[8];
-#pragma unroll
-              for (int j = 0; j < 8; ++j) {
-                o[j] = v[8 * k + j] + bb[j];
-              }
+          ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+          if (ok && (two || c == 0)) {
+            tc_fence_after();
+            const int      pr  = c * 128 + q * 32 + lane;                 // window row pair
+            const uint32_t tad = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 128);
+            if (l < kLayers - 1) {
+              // 32 output channels (chunks 4 hh .. 4 hh + 3) of one row: one TMEM load, the residual
+              // and bias loads issued together, then straight-line arithmetic.
+              const int      plane  = cs >> 1, hh = cs & 1;
+              const bool     valid  = valid_s[2 * pr + plane] != 0;
+              const bool     second = l >= 2 && (l & 1) == 0;
+              unsigned char* dst    = (l & 1) ? buf_b : buf_a;
+              uint4*         p      = reinterpret_cast<uint4*>(dst + fused_line(plane, hh * 4, pr + 1));
+              constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk
+              const float*   bl     = bias_s + l * kCh + hh * 32;
+              uint4          res[4];
               if (second) {
-                const __nv_bfloat16* rb = reinterpret_cast<const __nv_bfloat16*>(&res[k]);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                  o[j] += __bfloat162float(rb[j]);
+  #pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                  res[k] = p[k * kStep];
                 }
               }
-              uint4 pk = make_uint4(0, 0, 0, 0);
-              if (valid) {
-                pk = make_uint4(pack_bf16x2(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f)),
-                                pack_bf16x2(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f)),
-                                pack_bf16x2(fmaxf(o[4], 0.f), fmaxf(o[5], 0.f)),
-                                pack_bf16x2(fmaxf(o[6], 0.f), fmaxf(o[7], 0.f)));
-              }
-              p[k * kStep] = pk;
-            }
-            fence_async_shared();
-          } else if (cs < 2) {
-            const int    plane = cs;
-            const int    wr    = 2 * pr + plane; // window row
-            const bool   valid = valid_s[wr] != 0;
-            const float* bl    = bias_s + l * kCh;
-            float        v[16];
-            tmem_ld16(tad + (uint32_t)(kOutCh * plane), v);
-            const int g = base + wr;
-            if (wr >= kFMargin && wr < kFMargin + kFOut && g < R) {
-#pragma unroll
-              for (int h = 0; h < 2; ++h) {
+              float v[32];
+              tmem_ld32(tad + (uint32_t)(32 * cs), v);
+  #pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const float4 b0 = reinterpret_cast<const float4*>(bl)[2 * k];
+                const float4 b1 = reinterpret_cast<const float4*>(bl)[2 * k + 1];
+                const float  bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+                float        o[8];
+  #pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                  o[j] = v[8 * k + j] + bb[j];
+                }
+                if (second) {
+                  const __nv_bfloat16* rb = reinterpret_cast<const __nv_bfloat16*>(&res[k]);
+  #pragma unroll
+                  for (int j = 0; j < 8; ++j) {
+                    o[j] += __bfloat162float(rb[j]);
+                  }
+                }
                 uint4 pk = make_uint4(0, 0, 0, 0);
                 if (valid) {
-                  const float* b8 = bl + 8 * h;
-                  const float* v8 = v + 8 * h;
-                  pk = make_uint4(pack_bf16x2(v8[0] + b8[0], v8[1] + b8[1]), pack_bf16x2(v8[2] + b8[2], v8[3] + b8[3]),
-                                  pack_bf16x2(v8[4] + b8[4], v8[5] + b8[5]), pack_bf16x2(v8[6] + b8[6], v8[7] + b8[7]));
+                  pk = make_uint4(pack_bf16x2(fmaxf(o[0], 0.f), fmaxf(o[1], 0.f)),
+                                  pack_bf16x2(fmaxf(o[2], 0.f), fmaxf(o[3], 0.f)),
+                                  pack_bf16x2(fmaxf(o[4], 0.f), fmaxf(o[5], 0.f)),
+                                  pack_bf16x2(fmaxf(o[6], 0.f), fmaxf(o[7], 0.f)));
                 }
-                y[(size_t)h * R + g] = pk;
+                p[k * kStep] = pk;
+              }
+              fence_async_shared();
+            } else if (cs < 2) {
+              const int    plane = cs;
+              const int    wr    = 2 * pr + plane; // window row
+              const bool   valid = valid_s[wr] != 0;
+              const float* bl    = bias_s + l * kCh;
+              float        v[16];
+              tmem_ld16(tad + (uint32_t)(kOutCh * plane), v);
+              const int g = base + wr;
+              if (wr >= kFMargin && wr < kFMargin + nout && g < R) {
+  #pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                  uint4 pk = make_uint4(0, 0, 0, 0);
+                  if (valid) {
+                    const float* b8 = bl + 8 * h;
+                    const float* v8 = v + 8 * h;
+                    pk = make_uint4(pack_bf16x2(v8[0] + b8[0], v8[1] + b8[1]), pack_bf16x2(v8[2] + b8[2], v8[3] + b8[3]),
+                                    pack_bf16x2(v8[4] + b8[4], v8[5] + b8[5]), pack_bf16x2(v8[6] + b8[6], v8[7] + b8[7]));
+                  }
+                  y[(size_t)h * R + g] = pk;
+                }
               }
             }
           }
-        }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) {
-          mbar_arrive(bar_epi);
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) {
+            mbar_arrive(bar_epi + 8u * c);
+          }
         }
       }
     }
@@ -712,16 +758,38 @@ int forward(pg_le_net* net, int R, cudaStream_t s)
   return rc;
 }
 
+// Windows of the fused kernel over R rows: n_full two-tile windows, then one-tile windows up to
+// n_win, dealt round-robin to min(n_win, sms) CTAs. CTA 0 has the most of both kinds, so its cost
+// (two-tile window 2, one-tile window 1) is the kernel's; the split with the lowest cost is taken,
+// with the most two-tile windows among equals.
+void fused_windows(int R, int sms, int* n_full, int* n_win)
+{
+  const int f0   = (R + kFOut - 1) / kFOut;
+  int       best = -1;
+  for (int f = f0; f >= std::max(0, f0 - sms); --f) {
+    const int rem  = R - f * kFOut;
+    const int w    = f + (rem > 0 ? (rem + kFOutHalf - 1) / kFOutHalf : 0);
+    const int g    = std::max(1, std::min(w, sms));
+    const int cost = (f + g - 1) / g + (w + g - 1) / g;
+    if (best < 0 || cost < best) {
+      best    = cost;
+      *n_full = f;
+      *n_win  = w;
+    }
+  }
+}
+
 int fused_forward(pg_le_net* net, int R, cudaStream_t s)
 {
   if (R <= 0) {
     return PG_OK;
   }
-  const int ntiles = (R + kFOut - 1) / kFOut;
-  const int grid   = std::max(1, std::min(ntiles, net->ctx->sm_count));
+  int n_full = 0, n_win = 0;
+  fused_windows(R, net->ctx->sm_count, &n_full, &n_win);
+  const int grid = std::max(1, std::min(n_win, net->ctx->sm_count));
   le_fused_forward_kernel<<<grid, kFThreads, kFSmem, s>>>(reinterpret_cast<const uint4*>(net->x), net->row_valid,
-                                                          net->wp, net->params, R, reinterpret_cast<uint4*>(net->y),
-                                                          net->err);
+                                                          net->wp, net->params, R, n_full, n_win,
+                                                          reinterpret_cast<uint4*>(net->y), net->err);
   return pg::check_cuda(net->ctx, cudaGetLastError(), "le_fused_forward_kernel launch");
 }
 

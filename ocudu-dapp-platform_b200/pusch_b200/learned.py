@@ -410,7 +410,7 @@ def main(argv=None):
     e.add_argument("--json", default=None)
     tm = sub.add_parser("time", help="time pg_le_refine_device on a batch of the training source")
     tm.add_argument("--rows", type=int, default=270_000)
-    tm.add_argument("--reps", type=int, default=10)
+    tm.add_argument("--reps", type=int, default=50)
     a = ap.parse_args(argv)
     ctx = _native.Context(0, 1024)
     if a.cmd == "time":

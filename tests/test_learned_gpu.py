@@ -76,9 +76,12 @@ def make_batch(ctx, seed, rows):
     return descs, est, ls, pr, h_true
 
 
-def test_refine_matches_oracle(ctx):
+@pytest.mark.parametrize("nrows", [20_000, 70_000])
+def test_refine_matches_oracle(ctx, nrows):
+    """20,000 rows run as one-tile windows of the fused network kernel only; 70,000 rows as
+    two-tile windows and one-tile windows after them."""
     import torch
-    descs, est, ls, pr, h_true = make_batch(ctx, 3, 20_000)
+    descs, est, ls, pr, h_true = make_batch(ctx, 3, nrows)
     n = len(descs)
     params = learned.init_params(11)
     params[-16 - 5 * 64 * 16:] *= 30.0
