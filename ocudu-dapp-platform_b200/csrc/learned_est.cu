@@ -366,7 +366,9 @@ constexpr uint32_t kFOffBar   = kFOffVal + kFWin;
 constexpr int      kFBars     = 2 * kFTiles + 2; // MMA done [2], epilogue done [2], weights [2]
 constexpr size_t   kFSmem     = kFOffBar + 8 * kFBars + 16;
 constexpr uint32_t kFCopy     = 16384; // bytes per bulk copy
-constexpr uint32_t kFCols     = 256;   // TMEM columns: 128 per M tile
+constexpr uint32_t kFCols     = 512;   // TMEM columns: 128 accumulators per M tile, then 64 per tile
+                                       // of packed bf16 block input (the residual two layers on)
+constexpr uint32_t kFColRes   = 256;
 static_assert(kFOffW % 16 == 0 && kFOffBias % 16 == 0 && kFOffBar % 8 == 0, "smem layout");
 static_assert(kFSmem <= 227 * 1024, "shared memory of the fused kernel");
 static_assert(kFChunkB % 16 == 0 && kFSmem < (1u << 18), "descriptor start addresses: 14 bits of 16-byte units");
@@ -575,6 +577,20 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
             tc_fence_after();
           }
           issue(0, 0);
+          // The MMAs of layer l - 1 are complete once its last commit (tile 1's barrier) has
+          // arrived, which precedes the epilogue waited next; before layer 0, the window barrier.
+          // Then its weight buffer takes the next layer (layer 0 of the next window after the
+          // last layer), in flight while this layer's MMAs run.
+          if (l > 0 && !fused_wait(bar_mma + 8u, (s - 1) & 1u, abort_sm, err)) {
+            mma_commit(bar_mma);
+            mma_commit(bar_mma + 8u);
+            mma_issued = s + 1;
+            break;
+          }
+          if (l + 1 < kLayers || win + (int)gridDim.x < n_win) {
+            fused_load_weights(wp, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
+            ++w_issued;
+          }
           if (l > 0) {
             if (!fused_wait(bar_epi + 8u, (s - 1) & 1u, abort_sm, err)) {
               // Tile 0's first part is in flight: both barriers take its completion, so that the
@@ -585,13 +601,6 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
               break;
             }
             tc_fence_after();
-          }
-          // Every MMA of layer l - 1 has completed (both of its epilogues have arrived; before layer
-          // 0, the window barrier), so its weight buffer takes the next layer (layer 0 of the next
-          // window after the last layer), in flight while this layer's MMAs run.
-          if (l + 1 < kLayers || win + (int)gridDim.x < n_win) {
-            fused_load_weights(wp, (l + 1) % kLayers, wbuf0 + ((s + 1) & 1) * kFWB, bar_w + 8u * ((s + 1) & 1));
-            ++w_issued;
           }
           issue(0, 1);
           mma_commit(bar_mma);
@@ -619,39 +628,47 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
             const int      pr  = c * 128 + q * 32 + lane;                 // window row pair
             const uint32_t tad = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 128);
             if (l < kLayers - 1) {
-              // 32 output channels (chunks 4 hh .. 4 hh + 3) of one row: one TMEM load, the residual
-              // and bias loads issued together, then straight-line arithmetic.
+              // 32 output channels (chunks 4 hh .. 4 hh + 3) of one row: one TMEM load of the
+              // accumulators, then straight-line arithmetic. Layers 0, 2, .. 12 write the block
+              // input, kept as packed bf16 in TMEM as well, where the second layer of the next block
+              // reads its residual (no shared-memory reads beside the tensor cores').
               const int      plane  = cs >> 1, hh = cs & 1;
               const bool     valid  = valid_s[2 * pr + plane] != 0;
               const bool     second = l >= 2 && (l & 1) == 0;
+              const bool     keep   = (l & 1) == 0;
               unsigned char* dst    = (l & 1) ? buf_b : buf_a;
               uint4*         p      = reinterpret_cast<uint4*>(dst + fused_line(plane, hh * 4, pr + 1));
               constexpr int  kStep  = kFChunkB / 16; // uint4 per chunk
               const float*   bl     = bias_s + l * kCh + hh * 32;
-              uint4          res[4];
+              const uint32_t tres   = tmem + ((uint32_t)(q * 32) << 16) + kFColRes + (uint32_t)(c * 64 + cs * 16);
+              uint32_t       res[16];
               if (second) {
-  #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                  res[k] = p[k * kStep];
+                float rf[16];
+                tmem_ld16(tres, rf);
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                  res[k] = __float_as_uint(rf[k]);
                 }
               }
               float v[32];
               tmem_ld32(tad + (uint32_t)(32 * cs), v);
-  #pragma unroll
+              uint32_t kept[16];
+#pragma unroll
               for (int k = 0; k < 4; ++k) {
                 const float4 b0 = reinterpret_cast<const float4*>(bl)[2 * k];
                 const float4 b1 = reinterpret_cast<const float4*>(bl)[2 * k + 1];
                 const float  bb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
                 float        o[8];
-  #pragma unroll
+#pragma unroll
                 for (int j = 0; j < 8; ++j) {
                   o[j] = v[8 * k + j] + bb[j];
                 }
                 if (second) {
-                  const __nv_bfloat16* rb = reinterpret_cast<const __nv_bfloat16*>(&res[k]);
-  #pragma unroll
-                  for (int j = 0; j < 8; ++j) {
-                    o[j] += __bfloat162float(rb[j]);
+#pragma unroll
+                  for (int j = 0; j < 4; ++j) {
+                    const __nv_bfloat162 rb = *reinterpret_cast<const __nv_bfloat162*>(&res[4 * k + j]);
+                    o[2 * j] += __low2float(rb);
+                    o[2 * j + 1] += __high2float(rb);
                   }
                 }
                 uint4 pk = make_uint4(0, 0, 0, 0);
@@ -662,6 +679,11 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
                                   pack_bf16x2(fmaxf(o[6], 0.f), fmaxf(o[7], 0.f)));
                 }
                 p[k * kStep] = pk;
+                kept[4 * k] = pk.x, kept[4 * k + 1] = pk.y, kept[4 * k + 2] = pk.z, kept[4 * k + 3] = pk.w;
+              }
+              if (keep) {
+                tmem_st16(tres, kept);
+                tmem_wait_st();
               }
               fence_async_shared();
             } else if (cs < 2) {
@@ -673,7 +695,7 @@ __global__ void __launch_bounds__(kFThreads, 1) le_fused_forward_kernel(const ui
               tmem_ld16(tad + (uint32_t)(kOutCh * plane), v);
               const int g = base + wr;
               if (wr >= kFMargin && wr < kFMargin + nout && g < R) {
-  #pragma unroll
+#pragma unroll
                 for (int h = 0; h < 2; ++h) {
                   uint4 pk = make_uint4(0, 0, 0, 0);
                   if (valid) {
