@@ -335,18 +335,21 @@ size_t al(size_t x)
 // in each tile, without accumulation, and initialise the two halves. Per 128-pair tile and 16 input
 // channels: 4 MMAs of N = 128 and 2 of N = 64, against 10 of N = 64 with one row per MMA row.
 //
-// Buffers: A (block input and output; the second layer of a block adds A and writes A in place,
-// row by row) and B (block middle; the 16 input features share its first two chunks, dead once
-// layer 0's MMAs have completed, which precedes every write of B).
+// Buffers: A (block input and output; the second layer of a block adds the block input, kept as
+// packed bf16 in tensor memory by the layer that wrote it, and writes A in place) and B (block
+// middle; the 16 input features share its first two chunks, dead once layer 0's MMAs have
+// completed, which precedes every write of B).
 //
 // Dataflow: the window is two M tiles of 128 pairs; the taps of either tile reach one pair into the
-// other, so every layer depends on both tiles of the previous one. A producer warp waits for the
-// epilogue barrier of layer l - 1, issues the MMAs of tile 0 and commits them to tile 0's barrier,
-// then those of tile 1. Sixteen epilogue warps (four per TMEM lane quarter, 32 accumulator columns
-// each) take tile 0 as soon as its MMAs complete - while tile 1's run - then tile 1: they add bias
-// and residual, apply the ReLU and the row mask, store bf16 to shared memory, make the stores
-// visible to the tensor cores and arrive once per layer. MMAs complete in issue order, so the
-// epilogue of layer l writes its destination only after every MMA of layer l - 1 that read it.
+// other. A producer warp waits for tile 0's epilogue barrier of layer l - 1 and issues the shifts
+// of tile 0 that read tile 0 only, loads the next layer's weights once layer l - 1's MMAs are
+// complete, waits for tile 1's epilogue barrier, issues tile 0's two remaining shifts (they read
+// tile 1's first pair) and commits tile 0, then issues and commits tile 1. Sixteen epilogue warps
+// (four per TMEM lane quarter, 32 accumulator columns each) take tile 0 as soon as its MMAs
+// complete - while tile 1's run - then tile 1: they add bias and residual, apply the ReLU and the
+// row mask, store bf16 to shared memory, make the stores visible to the tensor cores and arrive on
+// the tile's barrier. MMAs complete in issue order, so the epilogue of layer l writes its
+// destination only after every MMA of layer l - 1 that read it.
 constexpr int      kFTiles    = 2;
 constexpr int      kFPairs    = 128 * kFTiles;
 constexpr int      kFWin      = 2 * kFPairs;
