@@ -260,7 +260,7 @@ def run_reference_pusch(args):
         "metric": METRIC, "value": round(value, 3), "unit": "Mbit/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32/int8", "data": "synthetic (seeded simulator)", "impl": "reference",
-        "config": {"workload": PUSCH_WORKLOAD, "cells": N_CELLS, "ues": n_ues},
+        "config": pusch_config(slots, args.gpus, args.seed),
         "cpu_baseline": {"value": round(value, 3), "unit": "Mbit/s", "cores": cores, "kind": "reference",
                          "sample": f"the full {N_CELLS}-cell slot ({n_ues} UEs) per step through the reference's CPU "
                                    f"stage objects (oracle/_ref) on {cores} C++ threads, one UE per thread at a time"},
@@ -273,6 +273,20 @@ def run_reference_pusch(args):
 def pusch_workload(seed):
     from pusch_b200 import sim
     return sim.uneven_cells(seed=seed, nof_cells=N_CELLS)
+
+
+def pusch_config(slots, world, seed):
+    """The workload keys of the PUSCH line, identical in both arms: computed from the simulated
+    slots with the simulator's own (transmit-side) segmentation, so the reference arm needs no
+    part of the GPU library."""
+    from pusch_b200 import codec
+    from pusch_b200.sim import nof_ch_symbols
+    ues = [u for sl in slots for u in sl.ues]
+    cbs = sum(codec.segment_tx(u.tbs_bits, u.base_graph, u.modulation_order, u.nof_layers,
+                               nof_ch_symbols(u))["nof_cbs"] for u in ues)
+    return {"workload": PUSCH_WORKLOAD, "cells_per_rank": len(slots), "ues_per_rank": len(ues),
+            "codeblocks_per_rank": int(cbs), "tb_bits_per_rank": int(sum(u.tbs_bits for u in ues)),
+            "seed": seed, "max_iterations": MAX_ITER, "parallelism": f"replicas{world}"}
 
 
 def run_ours_pusch(args):
@@ -290,6 +304,7 @@ def run_ours_pusch(args):
     from pusch_b200 import learned as le_mod
 
     slots = pusch_workload(args.seed + rank)
+    config = pusch_config(slots, world, args.seed)
     truth = [t for sl in slots for t in sl.truth]
     ctx = _native.Context(device=dev, max_codeblocks=64)
     plan = PuschSlotPlan(ctx, slots, max_iterations=MAX_ITER, graph=True)
@@ -561,14 +576,13 @@ def run_ours_pusch(args):
             "metric": METRIC, "value": round(value, 3), "unit": "Mbit/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32/int8", "data": "synthetic (seeded simulator)",
-            "config": {"workload": PUSCH_WORKLOAD, "cells_per_rank": N_CELLS, "ues_per_rank": n,
-                       "codeblocks_per_rank": int(plan.info.nof_codeblocks), "tb_bits_per_rank": bits_all,
-                       "decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
-                       "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
-                       "parallelism": f"replicas{world}", "launch_shapes": tuning.as_dict(),
-                       "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
-                                     "plain LS + RC FIR + linear interpolation" if net is not None else
-                                     "plain (LS + RC FIR + linear interpolation)")},
+            "config": config,
+            "run": {"decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
+                    "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
+                    "launch_shapes": tuning.as_dict(),
+                    "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
+                                  "plain LS + RC FIR + linear interpolation" if net is not None else
+                                  "plain (LS + RC FIR + linear interpolation)")},
             "plain_per_ue": plain, "batched_plain": batched_plain,
             "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "ofh_bfp": bfp_line, "cpu_baseline": cpu,
             "clocks": clk,

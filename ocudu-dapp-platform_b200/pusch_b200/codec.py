@@ -190,6 +190,42 @@ def rate_match(bg, z, cw, e, rv=0, qm=2, nref=0, nof_filler_bits=0):
     return sel
 
 
+# TS 38.212 Table 5.3.2-1: the 51 lifting sizes, ascending.
+LIFTING_SIZES = tuple(sorted({a * (1 << j) for a in (2, 3, 5, 7, 9, 11, 13, 15) for j in range(8)
+                              if a * (1 << j) <= 384}))
+
+
+def segment_tx(tbs_bits, bg, qm, nof_layers, nof_ch_symbols):
+    """Transmit-side segmentation of one UL-SCH transport block: codeblock count and size
+    (TS 38.212 Section 5.2.2, with the K_b of Section 5.2.2 for base graph 2) and the
+    rate-matching lengths E of Section 5.4.2.1 (the first C - mod(G', C) codeblocks get the floor).
+    Returns the fields of pg_sch_segmentation as a dict. The simulator uses it to build its
+    codewords, so input generation does not depend on the receive library."""
+    if bg not in (1, 2) or tbs_bits <= 0 or not 1 <= nof_layers <= 4 or qm not in (1, 2, 4, 6, 8):
+        raise ValueError("invalid segmentation request")
+    if nof_ch_symbols % nof_layers:
+        raise ValueError("channel symbols not a multiple of the layers")
+    tb_crc = 16 if tbs_bits <= 3824 else 24
+    b = tbs_bits + tb_crc
+    kcb = 8448 if bg == 1 else 3840
+    c = 1 if b <= kcb else -(-b // (kcb - 24))
+    l = 24 if c > 1 else 0
+    b_out = b + c * l
+    if bg == 1:
+        kb = 22
+    else:
+        kb = 10 if b > 640 else (9 if b > 560 else (8 if b > 192 else 6))
+    z = next((ls for ls in LIFTING_SIZES if ls * c * kb >= b_out), 0)
+    if z == 0:
+        raise ValueError("transport block too large")
+    k = (22 if bg == 1 else 10) * z
+    k_prime = -(-b_out // c)
+    per_layer = nof_ch_symbols // nof_layers
+    return {"nof_cbs": c, "lifting_size": z, "cb_length": k, "nof_filler_bits": k - k_prime,
+            "cb_crc_bits": l, "tb_crc_bits": tb_crc, "nof_short_cbs": c - per_layer % c,
+            "e_short": (per_layer // c) * nof_layers * qm, "e_long": -(-per_layer // c) * nof_layers * qm}
+
+
 def ulsch_encode(tb_bits, bg, qm, nof_layers, nof_ch_symbols, seg, rv=0, nref=0):
     """Transport block bits -> codeword bits (G = nof_ch_symbols * Qm): TB CRC, code block
     segmentation with CB CRC24B, filler bits, LDPC encoding and rate matching (TS 38.212

@@ -147,7 +147,6 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
     UE) transmits given transport blocks instead, e.g. a HARQ retransmission with another rv."""
     from . import prg
     from .demod import to_cbf16
-    from .sch import segment
 
     rng = np.random.default_rng(seed)
     nsc_grid = 12 * nof_prb_grid
@@ -156,7 +155,7 @@ def make_pusch_slot(ues, nof_ports, nof_prb_grid=273, slot=0, seed=0, scs_khz=30
     beta = float(np.float32(10 ** (3 / 20)))
     for ue in ues:
         ncs = nof_ch_symbols(ue)
-        seg = segment(ue.tbs_bits, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs)
+        seg = codec.segment_tx(ue.tbs_bits, ue.base_graph, ue.modulation_order, ue.nof_layers, ncs)
         tb = rng.integers(0, 2, ue.tbs_bits, dtype=np.uint8)
         if tb_bits is not None:
             tb = np.asarray(tb_bits[len(truth)], np.uint8)

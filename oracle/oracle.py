@@ -162,6 +162,28 @@ class Ref:
         dt = self.lib.ref_pusch_decode_mt(ctypes.addressof(descs), n, _ptr(g), _ptr(tb), _ptr(ok), _ptr(it), threads)
         return ok.astype(bool), it, tb, float(dt)
 
+    def pusch_decode_detail(self, descs, grid, tb_bytes, nof_llrs, threads):
+        """pusch_decode_mt plus the stage taps (ref_pusch_decode_detail): returns a dict with ok
+        (bool per UE), mean_iters, tb (bytes), nof_cbs (per UE), cb_iters (one list per UE: the
+        ldpc_decoder result of every codeblock, 0 = not decoded) and llrs (the descrambled codeword
+        LLRs of every UE at its llr_offset)."""
+        n = len(descs)
+        g = np.ascontiguousarray(grid, np.uint32)
+        tb = np.zeros(max(tb_bytes, 1), np.uint8)
+        ok = np.zeros(n, np.int32)
+        it = np.zeros(n, np.float32)
+        cb_first = (np.arange(n, dtype=np.int32) * 160).astype(np.int32)  # at most 152 codeblocks per TB
+        cb_it = np.full(160 * n, -1, np.int32)
+        ncb = np.zeros(n, np.int32)
+        llrs = np.zeros(max(nof_llrs, 1), np.int8)
+        f = self.lib.ref_pusch_decode_detail
+        f.restype = ctypes.c_double
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 8 + [ctypes.c_int]
+        dt = f(ctypes.addressof(descs), n, _ptr(g), _ptr(tb), _ptr(ok), _ptr(it), _ptr(cb_first), _ptr(cb_it), _ptr(ncb),
+               _ptr(llrs), threads)
+        cbs = [cb_it[cb_first[i]:cb_first[i] + ncb[i]].copy() for i in range(n)]
+        return dict(ok=ok.astype(bool), mean_iters=it, tb=tb, nof_cbs=ncb, cb_iters=cbs, llrs=llrs, seconds=float(dt))
+
     def pusch_mcs(self, table, index):
         r = ctypes.c_float()
         qm = self.lib.ref_pusch_mcs(0 if table == 1 else 1, index, ctypes.byref(r))

@@ -643,13 +643,17 @@ int ref_base_graph(float rate, unsigned tbs_bits)
 /// counter (independent UE-level work, as the reference's PUSCH processor pool runs them).
 /// ues: pg_pusch_ue array (include/pusch_b200.h layout); grids: cbf16 words; tb_out: TB bytes at
 /// each UE's tb_out_offset (written when the TB CRC passes); ok / iters: per UE. Returns wall s.
-double ref_pusch_decode_mt(const pg_pusch_ue* ues,
-                           int                nof_ues,
-                           const uint32_t*    grids,
-                           uint8_t*           tb_out,
-                           int32_t*           ok,
-                           float*             mean_iters,
-                           int                nof_threads)
+static double pusch_decode_impl(const pg_pusch_ue* ues,
+                                int                nof_ues,
+                                const uint32_t*    grids,
+                                uint8_t*           tb_out,
+                                int32_t*           ok,
+                                float*             mean_iters,
+                                int                nof_threads,
+                                const int32_t*     cb_first,
+                                int32_t*           cb_iters,
+                                int32_t*           nof_cbs,
+                                int8_t*            llr_out)
 {
   std::atomic<int> next{0};
   auto worker = [&]() {
@@ -779,8 +783,14 @@ double ref_pusch_decode_mt(const pg_pusch_ue* ues,
       sc.nof_layers           = nl;
       sc.nof_ch_symbols       = g / qm;
       static_vector<described_rx_codeblock, MAX_NOF_SEGMENTS> cbs;
+      if (llr_out != nullptr) {
+        std::memcpy(llr_out + u.llr_offset, llr.data(), llr.size());
+      }
       seg->segment(cbs, llr, sc);
       const unsigned  C      = cbs.size();
+      if (nof_cbs != nullptr) {
+        nof_cbs[i] = static_cast<int32_t>(C);
+      }
       crc_calculator* cb_crc = C > 1 ? crc24b.get() : (u.tbs_bits <= 3824 ? crc16.get() : crc24a.get());
       std::vector<uint8_t> tb_bits;
       bool                 all_ok = true;
@@ -801,6 +811,9 @@ double ref_pusch_decode_mt(const pg_pusch_ue* ues,
         dynamic_bit_buffer           out(K);
         std::optional<unsigned>      r = dec->decode(out, rm, cb_crc, dc);
         all_ok                         = all_ok && r.has_value();
+        if (cb_iters != nullptr) {
+          cb_iters[cb_first[i] + c] = r.has_value() ? static_cast<int32_t>(*r) : 0;
+        }
         it_sum += r.has_value() ? *r : u.max_iterations;
         const unsigned payload = K - md.cb_specific.nof_filler_bits - (C > 1 ? 24 : 0);
         for (unsigned b = 0; b < payload; ++b) {
@@ -841,6 +854,38 @@ double ref_pusch_decode_mt(const pg_pusch_ue* ues,
     th.join();
   }
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+double ref_pusch_decode_mt(const pg_pusch_ue* ues,
+                           int                nof_ues,
+                           const uint32_t*    grids,
+                           uint8_t*           tb_out,
+                           int32_t*           ok,
+                           float*             mean_iters,
+                           int                nof_threads)
+{
+  return pusch_decode_impl(ues, nof_ues, grids, tb_out, ok, mean_iters, nof_threads, nullptr, nullptr, nullptr,
+                           nullptr);
+}
+
+/// ref_pusch_decode_mt with the stage taps a slot-level parity check needs: nof_cbs[u] = C of UE u,
+/// cb_iters[cb_first[u] + c] = the ldpc_decoder result of codeblock c (iterations, 0 = the
+/// reference's empty optional), and llr_out (may be NULL) = the descrambled codeword LLRs of every
+/// UE at its llr_offset - the soft bits pusch_processor hands to pusch_decoder.
+double ref_pusch_decode_detail(const pg_pusch_ue* ues,
+                               int                nof_ues,
+                               const uint32_t*    grids,
+                               uint8_t*           tb_out,
+                               int32_t*           ok,
+                               float*             mean_iters,
+                               const int32_t*     cb_first,
+                               int32_t*           cb_iters,
+                               int32_t*           nof_cbs,
+                               int8_t*            llr_out,
+                               int                nof_threads)
+{
+  return pusch_decode_impl(ues, nof_ues, grids, tb_out, ok, mean_iters, nof_threads, cb_first, cb_iters, nof_cbs,
+                           llr_out);
 }
 
 } // extern "C"

@@ -215,6 +215,26 @@ def est_cases(ref):
     return out
 
 
+def est_full_cell_case(ref):
+    """One full-cell allocation at the headline shape: 273 PRB, 4 receive ports, 2 layers, DM-RS at
+    symbols 2 and 11, exponential-PDP channel at 25 dB (estimate_273prb.npz, same keys as
+    estimate.npz)."""
+    from pusch_b200 import sim
+    out = {}
+    beta = float(np.float32(10 ** (3 / 20)))
+    ue = sim.PuschUe(rb_start=0, nof_rb=273, nof_layers=2, modulation_order=8, tbs_bits=417976, base_graph=1,
+                     dmrs_symbols=(2, 11), snr_db=25.0, channel="pdp", n_id=301, rnti=0x4711)
+    slot = sim.make_pusch_slot([ue], 4, nof_prb_grid=273, slot=7, seed=273)
+    out["c0_meta"] = np.array([0, 273, 2, 4, 7, 301, 0x4711, (1 << 2) | (1 << 11)], np.int32)
+    out["c0_grid"] = slot.grid
+    for p in range(4):
+        freq, sym, sc = ref.port_estimate(slot.grid, p, 7, 301, 0, 273, 2, [2, 11], beta)
+        out[f"c0_p{p}_freq"] = freq
+        out[f"c0_p{p}_sym"] = sym
+        out[f"c0_p{p}_scalars"] = np.array([sc["noise_var"], sc["epre"], sc["snr"], *sc["rsrp"]], np.float64)
+    return out
+
+
 def main():
     ref = Ref()
     rng = np.random.default_rng(20261203)
@@ -225,6 +245,7 @@ def main():
     np.savez_compressed(os.path.join(OUT, "demap.npz"), **demap_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "equalize.npz"), **eq_cases(ref, rng))
     np.savez_compressed(os.path.join(OUT, "estimate.npz"), **est_cases(ref))
+    np.savez_compressed(os.path.join(OUT, "estimate_273prb.npz"), **est_full_cell_case(ref))
     print("golden fixtures written; reference LDPC variant:", ref.variant)
 
 

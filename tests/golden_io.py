@@ -77,8 +77,14 @@ def eq_cases():
     return out
 
 
-def est_cases():
-    d = load("estimate.npz")
+def est_cases(names=("estimate.npz", "estimate_273prb.npz")):
+    out = []
+    for name in names:
+        out += _est_file(load(name))
+    return out
+
+
+def _est_file(d):
     out, i = [], 0
     while f"c{i}_meta" in d:
         rb0, nrb, nl, ports, slot, n_id, rnti, mask = (int(x) for x in d[f"c{i}_meta"])

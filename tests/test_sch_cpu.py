@@ -51,3 +51,21 @@ def test_rate_match_matches_reference(ref):
         a = ref.ldpc_encode_rm(bg, z, msg, e, rv=t % 4, qm=qm, Nref=nref, filler=f)
         b = codec.rate_match(bg, z, codec.ldpc_encode(bg, z, msg), e, rv=t % 4, qm=qm, nref=nref, nof_filler_bits=f)
         assert (a == b).all()
+
+
+def test_transmit_segmentation_matches_library_and_reference(ref):
+    """The simulator's own segmentation (codec.segment_tx, transmit side) equals the receive
+    library's (pg_sch_segment) and the reference's for random transport blocks and allocations."""
+    rng = np.random.default_rng(21)
+    for _ in range(400):
+        bg = int(rng.integers(1, 3))
+        tbs = 8 * int(rng.integers(3, 60000 if bg == 1 else 500))
+        qm = int(rng.choice([1, 2, 4, 6, 8]))
+        nl = int(rng.integers(1, 3))
+        nsym = nl * int(rng.integers(1, 40000))
+        a = codec.segment_tx(tbs, bg, qm, nl, nsym)
+        b = sch.segment(tbs, bg, qm, nl, nsym)
+        assert a == b, (tbs, bg, qm, nl, nsym)
+        r = ref.sch_segmentation(tbs, bg)
+        assert (r["C"], r["Z"], r["K"], r["tb_crc"]) == (a["nof_cbs"], a["lifting_size"], a["cb_length"],
+                                                          a["tb_crc_bits"])
