@@ -52,7 +52,12 @@ LE_FLOPS_PER_ROW = 2 * 5 * (16 * 64 + 12 * 64 * 64 + 64 * 16)  # 14 layers, kern
 WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) and BG2 Z=384 (K=3840, rate 1/5) "
             "mixed 50/50 by seed, CRC24B, BPSK/AWGN Eb/N0 U[1,3] dB, int8 LLRs (scale 4/LLR unit, sat +-127), "
             "max 10 iterations, CRC early stop")
-INT_OPS_PER_EDGE = 10  # algorithmic integer operations per edge update
+# Algorithmic integer operations per edge update: v2c saturating subtraction, infinity guard, abs,
+# three for the min1/min2 update, sign XOR, two for the message select and sign, promotion add.
+INT_OPS_PER_EDGE = 10
+# Integer-instruction throughput probe (the LDPC roofline denominator), built by
+# ocudu-dapp-platform_b200/measure/Makefile.
+PROBE_SO = os.path.join(ROOT, "ocudu-dapp-platform_b200", "measure", "_lib", "libpg_probe.so")
 
 
 def parse_args():
@@ -210,7 +215,7 @@ def int_peak(dev):
     figures (libpg_probe.so), or (None, None)."""
     import ctypes
     try:
-        probe = ctypes.CDLL(os.path.join(ROOT, "ocudu-dapp-platform_b200", "pusch_b200", "_lib", "libpg_probe.so"))
+        probe = ctypes.CDLL(PROBE_SO)
         probe.pg_probe_inst_classes.argtypes = [ctypes.c_int, ctypes.c_void_p]
         buf = (ctypes.c_double * 8)()
         if probe.pg_probe_inst_classes(dev, buf) == 0:
@@ -743,7 +748,7 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     # instruction throughput of this GPU (best of add.s32 / min.s32 in libpg_probe.so).
     peak_ops, classes = None, None
     try:
-        probe = ctypes.CDLL(os.path.join(ROOT, "ocudu-dapp-platform_b200", "pusch_b200", "_lib", "libpg_probe.so"))
+        probe = ctypes.CDLL(PROBE_SO)
         probe.pg_probe_inst_classes.argtypes = [ctypes.c_int, ctypes.c_void_p]
         buf = (ctypes.c_double * 8)()
         if probe.pg_probe_inst_classes(dev, buf) == 0:

@@ -110,8 +110,9 @@ int pg_ldpc_decode_batch_resident(pg_context* ctx, const pg_ldpc_cb* cbs_dev, in
  * a real-time PHY worker under a slot deadline, where an allocation's driver locks and device
  * synchronisation have no latency bound, and a process whose device memory was reserved at
  * start-up, which must not meet out-of-memory during traffic.
- * The first call on each device looks up the array's device address; make that first call before
- * any stream capture begins. All calls on a device share the one array: calls whose kernels may
+ * The array's device address is looked up when the context is created (pg_create), so the call
+ * itself makes no CUDA runtime call besides its launch (and, with kernel timing enabled, the two
+ * event records read by pg_last_kernel_ms). All calls on a device share the one array: calls whose kernels may
  * overlap in time (different streams without ordering, several host threads) race on it, so
  * order them on one stream or synchronise between them. */
 int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldpc_cb* cbs_dev, int nof_cbs, const int8_t* llrs,

@@ -989,6 +989,9 @@ __global__ void __launch_bounds__(kX2Threads, kX2MaxPerSm) ldpc_decode_x2_kernel
 
 } // namespace
 
+// Check-to-variable scratch of pg_ldpc_decode_batch_static_scratch (described with that entry).
+static __device__ __align__(256) int8_t g_static_c2v[(size_t)PG_STATIC_SCRATCH_MAX_CODEBLOCKS * pg::kC2vStride];
+
 namespace pg {
 
 int lifting_set_index(int Z)
@@ -1058,6 +1061,12 @@ int ldpc_upload_tables(pg_context* ctx)
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyToSymbol(c_row_deg, deg, sizeof(deg)), "cudaMemcpyToSymbol(row_deg)");
+  }
+  if (rc == PG_OK) {
+    // Device address of the static scratch on this context's device (current here), looked up
+    // once so that the static-scratch entry makes no runtime call besides its launch.
+    rc = check_cuda(ctx, cudaGetSymbolAddress((void**)&ctx->static_c2v, g_static_c2v),
+                    "cudaGetSymbolAddress(static check-to-variable scratch)");
   }
   return rc;
 }
@@ -1156,37 +1165,8 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
 // Nothing in the array has to start at zero: the first layered iteration of each codeblock writes
 // every check-to-variable message of the rows it processes before any later iteration reads one,
 // so what an earlier call left behind is never read. Every call on a device uses the same array;
-// kernels of two calls that run at the same time race on it.
-
-static __device__ __align__(256) int8_t g_static_c2v[(size_t)PG_STATIC_SCRATCH_MAX_CODEBLOCKS * pg::kC2vStride];
-
-namespace {
-
-constexpr int kStaticMaxDevices = 64;
-std::mutex    g_static_mu;
-int8_t*       g_static_c2v_addr[kStaticMaxDevices] = {};
-
-// Device address of g_static_c2v on ctx->device, looked up on the first call per device; the
-// caller has made ctx->device current.
-int static_scratch_address(pg_context* ctx, int8_t** out)
-{
-  if (ctx->device < 0 || ctx->device >= kStaticMaxDevices) {
-    return pg::set_error(ctx, PG_ERR_INVALID, "device ordinal beyond the static scratch table");
-  }
-  std::lock_guard<std::mutex> lock(g_static_mu);
-  if (g_static_c2v_addr[ctx->device] == nullptr) {
-    int8_t* ptr = nullptr;
-    if (int rc = pg::check_cuda(ctx, cudaGetSymbolAddress((void**)&ptr, g_static_c2v),
-                                "cudaGetSymbolAddress(static check-to-variable scratch)")) {
-      return rc;
-    }
-    g_static_c2v_addr[ctx->device] = ptr;
-  }
-  *out = g_static_c2v_addr[ctx->device];
-  return PG_OK;
-}
-
-} // namespace
+// kernels of two calls that run at the same time race on it. The array's device address is
+// looked up once per context, in ldpc_upload_tables (called by pg_create).
 
 extern "C" int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldpc_cb* cbs_dev, int nof_cbs,
                                                    const int8_t* llrs, uint8_t* bits, int32_t* iterations,
@@ -1218,12 +1198,16 @@ extern "C" int pg_ldpc_decode_batch_static_scratch(pg_context* ctx, const pg_ldp
       return rc;
     }
   }
-  int8_t* scratch = nullptr;
-  int     rc      = static_scratch_address(ctx, &scratch);
-  if (rc == PG_OK) {
-    ldpc_decode_kernel<<<nof_cbs, kThreads, 0, static_cast<cudaStream_t>(stream)>>>(
-        cbs_dev, llrs, bits, iterations, scratch, ctx->dev.crc_pow, nullptr, nof_cbs, nullptr, 0);
-    rc = pg::check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch (static scratch)");
+  const cudaStream_t s          = static_cast<cudaStream_t>(stream);
+  const unsigned int rec_flags  = pg::timing_record_flags(ctx, s);
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_start, s, rec_flags);
+  }
+  ldpc_decode_kernel<<<nof_cbs, kThreads, 0, s>>>(cbs_dev, llrs, bits, iterations, ctx->static_c2v, ctx->dev.crc_pow,
+                                                  nullptr, nof_cbs, nullptr, 0);
+  int rc = pg::check_cuda(ctx, cudaGetLastError(), "ldpc_decode_kernel launch (static scratch)");
+  if (ctx->timed) {
+    cudaEventRecordWithFlags(ctx->ev_stop, s, rec_flags);
   }
   if (prev != ctx->device) {
     cudaSetDevice(prev);

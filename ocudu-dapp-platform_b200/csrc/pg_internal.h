@@ -93,6 +93,7 @@ struct pg_context {
   void*               scratch_b      = nullptr;
   size_t              scratch_b_cap  = 0;
   bool                timed          = false;
+  int8_t*             static_c2v     = nullptr;  // device address of the module-static LDPC scratch
   std::string         last_error;
 };
 
