@@ -55,6 +55,9 @@ WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) an
 # Algorithmic integer operations per edge update: v2c saturating subtraction, infinity guard, abs,
 # three for the min1/min2 update, sign XOR, two for the message select and sign, promotion add.
 INT_OPS_PER_EDGE = 10
+LDPC_KERNEL_NAMES = ["ldpc_decode_kernel (one lifted lane per thread)",
+                     "ldpc_decode_x2_kernel (two lifted lanes per thread for even Z > 192)",
+                     "ldpc_decode_split_kernel (two lanes per thread pair, row edges split over the pair)"]
 # Integer-instruction throughput probe (the LDPC roofline denominator), built by
 # ocudu-dapp-platform_b200/measure/Makefile.
 PROBE_SO = os.path.join(ROOT, "ocudu-dapp-platform_b200", "measure", "_lib", "libpg_probe.so")
@@ -535,8 +538,7 @@ def run_ours_pusch(args):
     achieved = ops / (k_ms * 1e-3) / 1e12
     roofline = {
         "bound": "int",
-        "kernel": ("ldpc_decode_x2_kernel (every codeblock; two lifted lanes per thread for Z > 192)"
-                   if tuning.as_dict().get("ldpc_z384_two_lanes") else "ldpc_decode_kernel"),
+        "kernel": LDPC_KERNEL_NAMES[tuning.as_dict().get("ldpc_kernel", 0)],
         "achieved": round(achieved, 3), "peak": round(peak, 3),
         "unit": "Tops/s", "frac": round(achieved / peak, 4),
         "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"

@@ -136,6 +136,20 @@ int pg_set_kernel_timing(pg_context* ctx, int enabled);
  * or a negative value when none was recorded. */
 float pg_last_kernel_ms(pg_context* ctx);
 
+/* LDPC decoding kernels; every one gives the same bits and iteration counts. No counterpart in the
+ * reference, whose decoder runs one codeblock per CPU task. */
+enum pg_ldpc_kernel {
+  PG_LDPC_KERNEL_ONE_LANE  = 0, /* 384 threads per codeblock, one lifted lane per thread, two CTAs per SM */
+  PG_LDPC_KERNEL_TWO_LANES = 1, /* 192 threads per codeblock; even Z > 192: two lanes per thread as f16x2
+                                   halves; four CTAs per SM */
+  PG_LDPC_KERNEL_SPLIT     = 2  /* 384 threads per codeblock; even Z > 192: two lanes per thread pair, each
+                                   row's edges split between the two threads; two CTAs per SM */
+};
+
+/* Selects the kernel of the context's batch decodes (pg_ldpc_decode_batch_{host,device,resident}
+ * and pg_sch_decode_batch_host); slot plans choose theirs through their tuning. */
+int pg_set_ldpc_kernel(pg_context* ctx, int kernel);
+
 
 /* ---------------------------------------------------------------------------------------- */
 /* Rate dematching                                                                           */
@@ -349,6 +363,46 @@ int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ue
 int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, uint32_t* out,
                                      void* stream);
 
+/* One receive port of one allocation for port_channel_estimator::compute
+ * (include/ocudu/phy/upper/signal_processors/channel_estimator/port_channel_estimator.h:86-89): the
+ * fields of its configuration the estimator reads. DM-RS type 1, CDM group 0 (one or two layers), one
+ * or two DM-RS symbols, contiguous resource blocks, no frequency hopping, normal cyclic prefix. */
+typedef struct pg_port_estimate_cfg {
+  uint32_t grid_nof_subc;    /* subcarriers of each grid row */
+  float    scaling;          /* DM-RS amplitude relative to data (configuration::scaling) */
+  uint16_t rb_start;
+  uint16_t nof_rb;
+  uint16_t dmrs_symbol_mask; /* bit s: OFDM symbol s carries DM-RS */
+  uint8_t  first_symbol;
+  uint8_t  nof_symbols;
+  uint8_t  nof_layers;       /* 1 or 2 */
+  uint8_t  scs_khz;          /* 15, 30, 60 or 120 */
+  uint8_t  reserved[2];
+} pg_port_estimate_cfg;
+
+/* The scalars of port_channel_estimator_results (port_channel_estimator.h:107-139). */
+typedef struct pg_port_estimate_result {
+  float  noise_var;
+  float  epre;
+  float  snr;
+  float  rsrp[2];
+  float  cfo_hz;           /* NaN with one DM-RS symbol (the reference's empty optional) */
+  double time_alignment_s; /* DFT-based time alignment estimate */
+} pg_port_estimate_result;
+
+/* port_channel_estimator::compute with FD "filter", TD "interpolate", no CFO compensation, for one
+ * port, from and to host memory: grid cbf16 [14][grid_nof_subc] (that port's slot), pilots complex
+ * float [dmrs symbol][layer][6 nof_rb] (the caller's DM-RS sequences, as dmrs_pusch_estimator
+ * builds them). Writes the FP32 frequency response freq_response [dmrs symbol][layer][12 nof_rb],
+ * optionally the per-symbol estimates symbol_estimates cbf16 [14][layer][12 nof_rb] (what
+ * get_symbol_ch_estimate returns), and the scalars, including the CFO
+ * (port_channel_estimator_average_impl.cpp:593-615) and the time alignment of
+ * time_alignment_estimator_dft (lib/phy/support/time_alignment_estimator/
+ * time_alignment_estimator_dft_impl.cpp:97-233). */
+int pg_port_channel_estimate_host(pg_context* ctx, const pg_port_estimate_cfg* cfg, const uint32_t* grid,
+                                  const float* pilots, float* freq_response, uint32_t* symbol_estimates,
+                                  pg_port_estimate_result* result);
+
 /* Demodulation of every UE: per data RE the channel estimate of its OFDM symbol (time interpolation
  * between DM-RS symbols, rounded to bf16, DC subcarrier zeroed), equalisation (one layer: MRC with
  * per-port noise; two layers: MMSE with the largest port noise), soft demapping and descrambling
@@ -421,9 +475,8 @@ typedef struct pg_pusch_plan_tuning {
   int demod_block;          /* demodulation: threads per CTA, 64, 128 or 256 (default 256) */
   int ldpc_ctas_per_sm;     /* persistent LDPC decoders: CTAs per SM, 1..4 (default 2; the one-lane-per-
                                thread decoder holds at most 2) */
-  int ldpc_z384_two_lanes;  /* 1: every codeblock on the 192-thread decoder, two lifted lanes per
-                               thread for even Z > 192 (up to 384) and one lane per thread below;
-                               0: every codeblock on the 384-thread one-lane decoder (default 0) */
+  int ldpc_kernel;          /* LDPC decoder (pg_ldpc_kernel): PG_LDPC_KERNEL_ONE_LANE, _TWO_LANES or _SPLIT
+                               (default PG_LDPC_KERNEL_SPLIT) */
 } pg_pusch_plan_tuning;
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out);

@@ -3,10 +3,17 @@
 
 #include "../../include/pusch_b200.h"
 #include "ocudu/ocuduvec/bit.h"
+#include "ocudu/ocuduvec/copy.h"
+#include "ocudu/phy/support/resource_grid_reader.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_notifier.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_result.h"
+#include "ocudu/phy/upper/rx_buffer.h"
+#include "ocudu/ran/pusch/pusch_constants.h"
 #include "ocudu/ran/sch/modulation_scheme.h"
 #include "ocudu/support/error_handling.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 namespace ocudu {
@@ -247,6 +254,291 @@ void channel_equalizer_b200::equalize(span<cf_t>                       eq_symbol
 }
 
 // ---------------------------------------------------------------------------------------------
+// port_channel_estimator
+
+const port_channel_estimator_results& port_channel_estimator_b200::compute(const resource_grid_reader& grid,
+                                                                           unsigned                    port,
+                                                                           const dmrs_symbol_list&     pilots,
+                                                                           const configuration&        cfg)
+{
+  static_assert(sizeof(cbf16_t) == sizeof(uint32_t), "cbf16_t is two bf16 values");
+  report_fatal_error_if_not(!cfg.dmrs_pattern.empty() && cfg.dmrs_pattern.size() <= 2,
+                            "pusch_b200: the estimator supports one or two layers.");
+  report_fatal_error_if_not(cfg.cp == cyclic_prefix::NORMAL, "pusch_b200: only the normal cyclic prefix is supported.");
+  const layer_dmrs_pattern& pattern = cfg.dmrs_pattern.front();
+  report_fatal_error_if_not(!pattern.hopping_symbol_index.has_value(), "pusch_b200: frequency hopping not supported.");
+  report_fatal_error_if_not(pattern.rb_mask.is_contiguous() && pattern.rb_mask.any(),
+                            "pusch_b200: the allocation must be contiguous.");
+  for (unsigned k = 0; k != NOF_SUBCARRIERS_PER_RB; ++k) {
+    report_fatal_error_if_not(pattern.re_pattern.test(k) == (k % 2 == 0),
+                              "pusch_b200: DM-RS type 1, CDM group 0 only.");
+  }
+  nof_layers             = static_cast<unsigned>(cfg.dmrs_pattern.size());
+  const unsigned nd      = static_cast<unsigned>(pattern.symbols.count());
+  const unsigned rb0     = static_cast<unsigned>(pattern.rb_mask.find_lowest());
+  const unsigned nof_rb  = static_cast<unsigned>(pattern.rb_mask.count());
+  const unsigned npil    = 6 * nof_rb;
+  const unsigned rx_port = cfg.rx_ports.empty() ? port : cfg.rx_ports[port];
+  report_fatal_error_if_not(nd >= 1 && nd <= 2, "pusch_b200: one or two DM-RS symbols.");
+  report_fatal_error_if_not(pilots.size().nof_subc == npil && pilots.size().nof_symbols == nd &&
+                                pilots.size().nof_slices == nof_layers,
+                            "pusch_b200: pilot list does not match the configuration.");
+
+  nof_subc = 12 * nof_rb;
+  const unsigned grid_subc = grid.get_nof_subc();
+  grid_rows.assign(static_cast<size_t>(MAX_NSYMB_PER_SLOT) * grid_subc, 0);
+  uint16_t mask = 0;
+  for (unsigned s = 0; s != MAX_NSYMB_PER_SLOT; ++s) {
+    if (s < pattern.symbols.size() && pattern.symbols.test(s)) {
+      mask |= static_cast<uint16_t>(1U << s);
+      span<const cbf16_t> row = grid.get_view(rx_port, s);
+      std::memcpy(grid_rows.data() + static_cast<size_t>(s) * grid_subc, row.data(), grid_subc * sizeof(cbf16_t));
+    }
+  }
+  pilot_buf.resize(static_cast<size_t>(nd) * nof_layers * npil);
+  for (unsigned d = 0; d != nd; ++d) {
+    for (unsigned l = 0; l != nof_layers; ++l) {
+      span<const cf_t> p = pilots.get_symbol(d, l);
+      std::copy(p.begin(), p.end(), pilot_buf.begin() + (static_cast<size_t>(d) * nof_layers + l) * npil);
+    }
+  }
+
+  pg_port_estimate_cfg pc = {};
+  pc.grid_nof_subc        = grid_subc;
+  pc.scaling              = cfg.scaling;
+  pc.rb_start             = static_cast<uint16_t>(rb0);
+  pc.nof_rb               = static_cast<uint16_t>(nof_rb);
+  pc.dmrs_symbol_mask     = mask;
+  pc.first_symbol         = static_cast<uint8_t>(cfg.first_symbol);
+  pc.nof_symbols          = static_cast<uint8_t>(cfg.nof_symbols);
+  pc.nof_layers           = static_cast<uint8_t>(nof_layers);
+  pc.scs_khz              = static_cast<uint8_t>(scs_to_khz(cfg.scs));
+  freq_response.resize(static_cast<size_t>(nd) * nof_layers * nof_subc);
+  symbol_estimates.resize(static_cast<size_t>(MAX_NSYMB_PER_SLOT) * nof_layers * nof_subc);
+  pg_port_estimate_result r = {};
+  ctx.check(pg_port_channel_estimate_host(ctx.get(), &pc, grid_rows.data(), reinterpret_cast<const float*>(pilot_buf.data()),
+                                          reinterpret_cast<float*>(freq_response.data()), symbol_estimates.data(), &r),
+            "pg_port_channel_estimate_host");
+  noise_var = r.noise_var;
+  epre      = r.epre;
+  snr       = r.snr;
+  rsrp      = {r.rsrp[0], r.rsrp[1]};
+  cfo_hz    = std::isnan(r.cfo_hz) ? std::nullopt : std::optional<float>(r.cfo_hz);
+  // The reference keeps the estimate in a float (port_channel_estimator_average_impl.h:230).
+  time_alignment_s = static_cast<float>(r.time_alignment_s);
+  return *this;
+}
+
+void port_channel_estimator_b200::get_symbol_ch_estimate(span<cbf16_t> symbol, unsigned i_symbol, unsigned tx_layer) const
+{
+  report_fatal_error_if_not(symbol.size() == nof_subc && i_symbol < MAX_NSYMB_PER_SLOT && tx_layer < nof_layers,
+                            "pusch_b200: invalid symbol estimate request.");
+  std::memcpy(symbol.data(), symbol_estimates.data() + (static_cast<size_t>(i_symbol) * nof_layers + tx_layer) * nof_subc,
+              nof_subc * sizeof(cbf16_t));
+}
+
+void port_channel_estimator_b200::get_symbol_ch_estimate(span<cbf16_t>                              symbol,
+                                                         unsigned                                   i_symbol,
+                                                         unsigned                                   tx_layer,
+                                                         const bounded_bitset<MAX_NOF_SUBCARRIERS>& re_mask) const
+{
+  report_fatal_error_if_not(re_mask.size() == nof_subc && symbol.size() == re_mask.count() &&
+                                i_symbol < MAX_NSYMB_PER_SLOT && tx_layer < nof_layers,
+                            "pusch_b200: invalid symbol estimate request.");
+  const uint32_t* src = symbol_estimates.data() + (static_cast<size_t>(i_symbol) * nof_layers + tx_layer) * nof_subc;
+  unsigned        o   = 0;
+  re_mask.for_each(0, re_mask.size(), [&](unsigned i_re) { std::memcpy(&symbol[o++], src + i_re, sizeof(cbf16_t)); });
+}
+
+// ---------------------------------------------------------------------------------------------
+// pusch_decoder
+
+pusch_decoder_b200::pusch_decoder_b200(const device_config& cfg, unsigned max_softbits) :
+  ctx(cfg), softbits(max_softbits), cb_stats(MAX_NOF_SEGMENTS, 0)
+{
+}
+
+pusch_decoder_buffer& pusch_decoder_b200::new_data(span<uint8_t>           transport_block_,
+                                                   unique_rx_buffer        rm_buffer_,
+                                                   pusch_decoder_notifier& notifier_,
+                                                   const configuration&    cfg)
+{
+  transport_block = transport_block_;
+  rm_buffer       = std::move(rm_buffer_);
+  notifier        = &notifier_;
+  current         = cfg;
+  softbits_count  = 0;
+  nof_ulsch_softbits.reset();
+  if (current.new_data) {
+    span<bool> crcs = rm_buffer->get_codeblocks_crc();
+    std::fill(crcs.begin(), crcs.end(), false);
+  }
+  return *this;
+}
+
+void pusch_decoder_b200::set_nof_softbits(units::bits nof_softbits)
+{
+  nof_ulsch_softbits = static_cast<unsigned>(nof_softbits.value());
+}
+
+span<log_likelihood_ratio> pusch_decoder_b200::get_next_block_view(unsigned block_size)
+{
+  report_fatal_error_if_not(softbits_count + block_size <= softbits.size(), "pusch_b200: codeword too long.");
+  return span<log_likelihood_ratio>(softbits).subspan(softbits_count, block_size);
+}
+
+void pusch_decoder_b200::on_new_softbits(span<const log_likelihood_ratio> in)
+{
+  span<log_likelihood_ratio> block = get_next_block_view(static_cast<unsigned>(in.size()));
+  if (block.data() != in.data()) {
+    std::copy(in.begin(), in.end(), block.begin());
+  }
+  softbits_count += static_cast<unsigned>(in.size());
+}
+
+void pusch_decoder_b200::on_end_softbits()
+{
+  const unsigned qm  = get_bits_per_symbol(current.mod);
+  const unsigned G   = softbits_count;
+  const unsigned tbs = static_cast<unsigned>(transport_block.size()) * 8;
+  const int      bg  = to_pg_base_graph(current.base_graph);
+  report_fatal_error_if_not(!nof_ulsch_softbits.has_value() || *nof_ulsch_softbits == G,
+                            "pusch_b200: {} soft bits received, {} announced.", G, *nof_ulsch_softbits);
+  report_fatal_error_if_not(qm > 0 && G % qm == 0, "pusch_b200: codeword length not a multiple of Qm.");
+
+  pg_sch_segmentation seg = {};
+  ctx.check(pg_sch_segment(tbs, bg, static_cast<int>(qm), static_cast<int>(current.nof_layers), G / qm, &seg),
+            "pg_sch_segment");
+  const unsigned C      = seg.nof_cbs;
+  const unsigned Z      = seg.lifting_size;
+  const unsigned N      = (bg == 1 ? 66U : 50U) * Z;
+  const unsigned K      = (bg == 1 ? 22U : 10U) * Z;
+  const unsigned F      = seg.nof_filler_bits;
+  const unsigned L      = C > 1 ? 24U : seg.tb_crc_bits;
+  const unsigned n_data = K - L - F;
+  report_fatal_error_if_not(C == rm_buffer->get_nof_codeblocks(), "pusch_b200: rx buffer holds {} codeblocks, {} needed.",
+                            rm_buffer->get_nof_codeblocks(), C);
+  span<bool> cb_crcs = rm_buffer->get_codeblocks_crc();
+
+  // Rate dematching of every codeblock into its soft buffer (also those whose CRC already passed:
+  // their buffers keep combining, pusch_decoder_impl.cpp:409-423).
+  std::vector<pg_rm_cb> rm(C);
+  cb_buffers.resize(static_cast<size_t>(C) * N);
+  for (unsigned c = 0, off = 0; c != C; ++c) {
+    const unsigned e = c < seg.nof_short_cbs ? seg.e_short : seg.e_long;
+    rm[c]            = {off, e, c * N, current.Nref, static_cast<uint16_t>(Z), static_cast<uint16_t>(F),
+                        static_cast<uint8_t>(bg), static_cast<uint8_t>(current.rv), static_cast<uint8_t>(qm),
+                        static_cast<uint8_t>(current.new_data ? 1 : 0)};
+    off += e;
+    span<log_likelihood_ratio> soft = rm_buffer->get_codeblock_soft_bits(c, N);
+    std::memcpy(cb_buffers.data() + static_cast<size_t>(c) * N, soft.data(), N);
+  }
+  ctx.check(pg_rate_dematch_batch_host(ctx.get(), rm.data(), static_cast<int>(C), raw(span<const log_likelihood_ratio>(softbits).first(G)),
+                                       G, cb_buffers.data(), cb_buffers.size()),
+            "pg_rate_dematch_batch_host");
+  for (unsigned c = 0; c != C; ++c) {
+    span<log_likelihood_ratio> soft = rm_buffer->get_codeblock_soft_bits(c, N);
+    std::memcpy(soft.data(), cb_buffers.data() + static_cast<size_t>(c) * N, N);
+  }
+
+  // LDPC decoding of the codeblocks without a passed CRC.
+  const uint32_t poly = C > 1 ? PG_CRC24B : (tbs <= 3824 ? PG_CRC16 : PG_CRC24A);
+  std::vector<pg_ldpc_cb> ldpc;
+  std::vector<unsigned>   which;
+  const unsigned          out_bytes = static_cast<unsigned>(pg_ldpc_output_bytes(bg, static_cast<int>(Z)));
+  for (unsigned c = 0; c != C; ++c) {
+    if (cb_crcs[c]) {
+      continue;
+    }
+    pg_ldpc_cb d      = {};
+    d.llr_offset      = c * N;
+    d.nof_llrs        = N;
+    d.out_offset      = static_cast<uint32_t>(which.size()) * out_bytes;
+    d.lifting_size    = static_cast<uint16_t>(Z);
+    d.nof_filler_bits = static_cast<uint16_t>(F);
+    d.base_graph      = static_cast<uint8_t>(bg);
+    d.crc_poly        = static_cast<uint8_t>(current.use_early_stop ? poly : PG_CRC_NONE);
+    d.max_iterations  = static_cast<uint8_t>(current.nof_ldpc_iterations);
+    ldpc.push_back(d);
+    which.push_back(c);
+  }
+  if (!ldpc.empty()) {
+    cb_bits.assign(static_cast<size_t>(ldpc.size()) * out_bytes, 0);
+    std::vector<int32_t> iters(ldpc.size(), 0);
+    ctx.check(pg_ldpc_decode_batch_host(ctx.get(), ldpc.data(), static_cast<int>(ldpc.size()), cb_buffers.data(),
+                                        cb_buffers.size(), cb_bits.data(), cb_bits.size(), iters.data()),
+              "pg_ldpc_decode_batch_host");
+    for (size_t i = 0; i != which.size(); ++i) {
+      const unsigned c    = which[i];
+      const uint8_t* bits = cb_bits.data() + i * out_bytes;
+      int            it   = iters[i];
+      if (!current.use_early_stop && it > 0) {
+        // Without early stop the CRC follows a passed syndrome check (pusch_codeblock_decoder.cpp:50-63).
+        pg_crc_item item = {0, K - F, poly};
+        uint32_t    crc  = 1;
+        ctx.check(pg_crc_calculate_host(ctx.get(), &item, 1, bits, out_bytes, &crc), "pg_crc_calculate_host");
+        it = crc == 0 ? static_cast<int>(current.nof_ldpc_iterations) : 0;
+      }
+      bit_buffer message = rm_buffer->get_codeblock_data_bits(c, K);
+      std::memcpy(message.get_buffer().data(), bits, std::min<size_t>(message.get_buffer().size(), out_bytes));
+      if (it > 0) {
+        cb_crcs[c]  = true;
+        cb_stats[c] = static_cast<unsigned>(it);
+      } else {
+        cb_stats[c] = current.nof_ldpc_iterations;
+      }
+    }
+  }
+
+  // Join (pusch_decoder_impl.cpp:612-781).
+  pusch_decoder_result result;
+  result.tb_crc_ok            = false;
+  result.nof_codeblocks_total = C;
+  result.ldpc_decoder_stats.reset();
+  for (unsigned c = 0; c != C; ++c) {
+    result.ldpc_decoder_stats.update(cb_stats[c]);
+  }
+  if (C == 1) {
+    result.tb_crc_ok = cb_crcs[0];
+    if (result.tb_crc_ok) {
+      const bit_buffer data = rm_buffer->get_codeblock_data_bits(0, tbs);
+      std::memcpy(transport_block.data(), data.get_buffer().data(), transport_block.size());
+    }
+  } else if (std::all_of(cb_crcs.begin(), cb_crcs.end(), [](bool b) { return b; })) {
+    bit_buffer tb_data  = bit_buffer::from_bytes(transport_block);
+    unsigned   offset   = 0;
+    unsigned   checksum = 0;
+    for (unsigned c = 0; c != C; ++c) {
+      const unsigned   n_new = std::min(tbs - offset, n_data);
+      const bit_buffer data  = rm_buffer->get_codeblock_data_bits(c, n_data);
+      ocuduvec::copy_offset(tb_data, offset, data, 0, n_new);
+      if (c == C - 1) {
+        for (unsigned b = 0; b != 3; ++b) {
+          checksum = (checksum << 8U) | data.extract(n_new + b * 8, 8);
+        }
+      }
+      offset += n_new;
+    }
+    pg_crc_item item = {0, tbs, PG_CRC24A};
+    uint32_t    crc  = 0;
+    ctx.check(pg_crc_calculate_host(ctx.get(), &item, 1, transport_block.data(), transport_block.size(), &crc),
+              "pg_crc_calculate_host");
+    if (crc == checksum) {
+      result.tb_crc_ok = true;
+    } else {
+      rm_buffer->reset_codeblocks_crc();
+    }
+  }
+  if (result.tb_crc_ok) {
+    rm_buffer.release();
+  } else {
+    rm_buffer.unlock();
+  }
+  pusch_decoder_notifier* n = std::exchange(notifier, nullptr);
+  n->on_sch_data(result);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Factories
 
 namespace {
@@ -308,7 +600,51 @@ private:
   channel_equalizer_algorithm_type type;
 };
 
+class port_channel_estimator_factory_b200 : public port_channel_estimator_factory
+{
+public:
+  explicit port_channel_estimator_factory_b200(const device_config& dev_) : dev(dev_) {}
+  std::unique_ptr<port_channel_estimator> create(port_channel_estimator_fd_smoothing_strategy     fd,
+                                                 port_channel_estimator_td_interpolation_strategy td,
+                                                 bool                                             compensate_cfo) override
+  {
+    if (fd != port_channel_estimator_fd_smoothing_strategy::filter ||
+        td != port_channel_estimator_td_interpolation_strategy::interpolate || compensate_cfo) {
+      return nullptr;
+    }
+    return std::make_unique<port_channel_estimator_b200>(dev);
+  }
+
+private:
+  device_config dev;
+};
+
+class pusch_decoder_factory_b200 : public pusch_decoder_factory
+{
+public:
+  pusch_decoder_factory_b200(const device_config& dev_, unsigned max_softbits_) : dev(dev_), max_softbits(max_softbits_)
+  {
+  }
+  std::unique_ptr<pusch_decoder> create() override { return std::make_unique<pusch_decoder_b200>(dev, max_softbits); }
+
+private:
+  device_config dev;
+  unsigned      max_softbits;
+};
+
 } // namespace
+
+std::shared_ptr<port_channel_estimator_factory> create_port_channel_estimator_factory_b200(const device_config& dev)
+{
+  return std::make_shared<port_channel_estimator_factory_b200>(dev);
+}
+
+std::shared_ptr<pusch_decoder_factory>
+create_pusch_decoder_factory_b200(const device_config& dev, unsigned max_nof_prb, unsigned max_nof_layers)
+{
+  return std::make_shared<pusch_decoder_factory_b200>(
+      dev, static_cast<unsigned>(pusch_constants::get_max_codeword_size(max_nof_prb, max_nof_layers).value()));
+}
 
 std::shared_ptr<ldpc_decoder_factory>
 create_ldpc_decoder_factory_b200(const device_config&                                            dev,

@@ -19,7 +19,14 @@
 #include "ocudu/phy/upper/channel_modulation/demodulation_mapper.h"
 #include "ocudu/phy/upper/equalization/channel_equalizer.h"
 #include "ocudu/phy/upper/equalization/equalization_factories.h"
+#include "ocudu/phy/upper/channel_processors/pusch/factories.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_buffer.h"
+#include "ocudu/phy/upper/signal_processors/channel_estimator/factories.h"
+#include "ocudu/phy/upper/signal_processors/channel_estimator/port_channel_estimator.h"
+#include "ocudu/phy/upper/unique_rx_buffer.h"
 
+#include <array>
 #include <memory>
 #include <vector>
 
@@ -142,6 +149,84 @@ private:
   std::vector<uint32_t>            symbols, estimates;
 };
 
+/// port_channel_estimator (include/ocudu/phy/upper/signal_processors/channel_estimator/
+/// port_channel_estimator.h:63-139) with frequency smoothing "filter", time interpolation
+/// "interpolate" and no CFO compensation: one port per compute() call, on the GPU entry
+/// pg_port_channel_estimate_host, with the pilots the caller gives (dmrs_pusch_estimator's). It is
+/// also its own results object, valid until the next compute(). Supported: DM-RS type 1, CDM group
+/// 0 (one or two layers), one or two DM-RS symbols, contiguous resource blocks, no frequency hopping,
+/// normal cyclic prefix; anything else ends the process.
+class port_channel_estimator_b200 : public port_channel_estimator, private port_channel_estimator_results
+{
+public:
+  explicit port_channel_estimator_b200(const device_config& cfg) : ctx(cfg) {}
+
+  const port_channel_estimator_results&
+  compute(const resource_grid_reader& grid, unsigned port, const dmrs_symbol_list& pilots, const configuration& cfg)
+      override;
+
+private:
+  void  get_symbol_ch_estimate(span<cbf16_t> symbol, unsigned i_symbol, unsigned tx_layer) const override;
+  void  get_symbol_ch_estimate(span<cbf16_t>                              symbol,
+                               unsigned                                   i_symbol,
+                               unsigned                                   tx_layer,
+                               const bounded_bitset<MAX_NOF_SUBCARRIERS>& re_mask) const override;
+  float get_epre() const override { return epre; }
+  float get_noise_variance() const override { return noise_var; }
+  float get_snr() const override { return snr; }
+  float get_rsrp(unsigned tx_layer) const override { return rsrp[tx_layer]; }
+  std::optional<float> get_cfo_Hz() const override { return cfo_hz; }
+  phy_time_unit        get_time_alignment() const override { return phy_time_unit::from_seconds(time_alignment_s); }
+
+  context_handle        ctx;
+  std::vector<uint32_t> grid_rows, symbol_estimates;
+  std::vector<cf_t>     pilot_buf, freq_response;
+  unsigned              nof_layers = 1, nof_subc = 0;
+  float                 noise_var = 0, epre = 0, snr = 0;
+  std::array<float, 2>  rsrp     = {};
+  std::optional<float>  cfo_hz;
+  float                 time_alignment_s = 0;
+};
+
+/// pusch_decoder (include/ocudu/phy/upper/channel_processors/pusch/pusch_decoder.h:38-145): the soft
+/// bits arrive through the pusch_decoder_buffer interface and, at on_end_softbits(), every codeblock
+/// of the transport block is rate dematched into its rx_buffer soft buffer (saturating combination
+/// for retransmissions) and the ones without a passed CRC are LDPC decoded, in one GPU batch each;
+/// then the TB is joined, its CRC checked on the GPU and the notifier called, with the reference's
+/// rules for the codeblock CRC flags, the decoded-bit storage and the iteration statistics
+/// (lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.cpp:80-145, :390-477, :612-781).
+/// Decoding completes inside on_end_softbits() (the reference's synchronous mode, no executor).
+class pusch_decoder_b200 : public pusch_decoder, private pusch_decoder_buffer
+{
+public:
+  /// max_softbits: the largest codeword (G) of one transport block.
+  pusch_decoder_b200(const device_config& cfg, unsigned max_softbits);
+
+  pusch_decoder_buffer& new_data(span<uint8_t>           transport_block,
+                                 unique_rx_buffer        rm_buffer,
+                                 pusch_decoder_notifier& notifier,
+                                 const configuration&    cfg) override;
+  void                  set_nof_softbits(units::bits nof_softbits) override;
+
+private:
+  span<log_likelihood_ratio> get_next_block_view(unsigned block_size) override;
+  void                       on_new_softbits(span<const log_likelihood_ratio> softbits) override;
+  void                       on_end_softbits() override;
+
+  context_handle                    ctx;
+  std::vector<log_likelihood_ratio> softbits;
+  unsigned                          softbits_count = 0;
+  std::optional<unsigned>           nof_ulsch_softbits;
+  span<uint8_t>                     transport_block;
+  unique_rx_buffer                  rm_buffer;
+  pusch_decoder_notifier*           notifier = nullptr;
+  configuration                     current;
+  /// Iterations of each codeblock index, kept across transport blocks as the reference keeps them.
+  std::vector<unsigned> cb_stats;
+  std::vector<int8_t>   cb_buffers;
+  std::vector<uint8_t>  cb_bits;
+};
+
 /// Factories in the shape of the reference's *_sw factories.
 std::shared_ptr<ldpc_decoder_factory>
 create_ldpc_decoder_factory_b200(const device_config&                                            dev,
@@ -151,6 +236,11 @@ std::shared_ptr<crc_calculator_factory>      create_crc_calculator_factory_b200(
 std::shared_ptr<demodulation_mapper_factory> create_demodulation_mapper_factory_b200(const device_config& dev);
 std::shared_ptr<channel_equalizer_factory>
 create_channel_equalizer_factory_b200(const device_config& dev, channel_equalizer_algorithm_type type);
+/// Estimators with FD "filter", TD "interpolate" and no CFO compensation; other strategies give nullptr.
+std::shared_ptr<port_channel_estimator_factory> create_port_channel_estimator_factory_b200(const device_config& dev);
+/// Decoders for codewords of up to the largest PUSCH codeword of max_nof_prb PRBs and max_nof_layers layers.
+std::shared_ptr<pusch_decoder_factory>
+create_pusch_decoder_factory_b200(const device_config& dev, unsigned max_nof_prb, unsigned max_nof_layers);
 
 } // namespace b200
 } // namespace ocudu

@@ -39,6 +39,13 @@ constexpr int kThreads = 384;
 __constant__ uint8_t  c_edge_col[2][pg::kBg1Edges];
 __constant__ uint16_t c_edge_v[2][pg::kBg1Edges][8];
 __constant__ uint8_t  c_row_deg[2][pg::kBg1Rows];
+// Layer steps: runs of consecutive base-graph rows whose columns are pairwise disjoint. The rows of
+// a step touch disjoint soft bits, so running them between the same two barriers gives exactly
+// the results of the reference's one-row-at-a-time order (BG1: 46 rows in 32 steps, BG2: 42 in 28).
+__constant__ uint8_t  c_step_row0[2][pg::kBg1Rows]; // first row of each step
+__constant__ uint8_t  c_step_nrows[2][pg::kBg1Rows];
+__constant__ uint8_t  c_nsteps[2];
+__constant__ uint16_t c_row_e0[2][pg::kBg1Rows + 1]; // first edge of each row (prefix sums of the degrees)
 
 __device__ __forceinline__ int dev_set_index(int Z)
 {
@@ -54,6 +61,34 @@ __device__ __forceinline__ int dev_set_index(int Z)
     }
   }
   return -1;
+}
+
+// Steps of a codeblock that processes nof_layers rows: those whose first row is below nof_layers.
+__device__ __forceinline__ int steps_for_layers(int g, int nof_layers)
+{
+  int n = 0;
+  while (n < c_nsteps[g] && c_step_row0[g][n] < nof_layers) {
+    ++n;
+  }
+  return n;
+}
+
+// Pulls the check-to-variable messages of step st (rows up to nof_layers) into L1 ahead of their
+// use: one prefetch per 128-byte line, thread `tid` taking line tid. Message rows are
+// row_bytes apart (one per edge) starting at base.
+__device__ __forceinline__ void prefetch_step(const int g, const int st, const int nof_layers, const int tid,
+                                              const char* base, const int row_bytes)
+{
+  const int r0    = c_step_row0[g][st];
+  const int r1    = min(r0 + (int)c_step_nrows[g][st], nof_layers);
+  const int ea    = c_row_e0[g][r0];
+  const int lpe   = (row_bytes + 127) >> 7;
+  const int lines = (c_row_e0[g][r1] - ea) * lpe;
+  if (tid < lines) {
+    const int e = tid / lpe;
+    const char* p = base + (size_t)(ea + e) * row_bytes + ((tid - e * lpe) << 7);
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+  }
 }
 
 __device__ __forceinline__ int scale_mag(int m)
@@ -323,19 +358,27 @@ __device__ __forceinline__ void decode_codeblock(const pg_ldpc_cb& d, smem_scala
 
   int result = 0;
   const int max_it = d.max_iterations;
+  const int nsteps = steps_for_layers(g, nof_layers);
   for (int it = 0; it < max_it; ++it) {
-    int e0 = 0;
-    for (int r = 0; r < nof_layers; ++r) {
-      const int deg = c_row_deg[g][r];
+    for (int st = 0; st < nsteps; ++st) {
+      // Messages are read from the second iteration on: prefetch the next step's.
+      if (it > 0 || st + 1 == nsteps) {
+        prefetch_step(g, st + 1 < nsteps ? st + 1 : 0, nof_layers, tid, reinterpret_cast<const char*>(c2v), Z);
+      }
+      const int r0 = c_step_row0[g][st];
+      const int r1 = min(r0 + (int)c_step_nrows[g][st], nof_layers);
       if (tid < Z) {
-        int8_t* c2v_row = c2v + (size_t)e0 * Z + tid;
-        if (it == 0) {
-          row_dispatch<true, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
-        } else {
-          row_dispatch<false, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+        for (int r = r0; r < r1; ++r) {
+          const int deg     = c_row_deg[g][r];
+          const int e0      = c_row_e0[g][r];
+          int8_t*   c2v_row = c2v + (size_t)e0 * Z + tid;
+          if (it == 0) {
+            row_dispatch<true, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+          } else {
+            row_dispatch<false, ZT, NT>(deg, tid, Z, soft, edge + e0, c2v_row, sm.mbuf);
+          }
         }
       }
-      e0 += deg;
       __syncthreads();
     }
 
@@ -525,17 +568,29 @@ constexpr int kX2Threads  = 192; // = kMaxZ / 2
 constexpr int kScaleTab   = 1408;
 constexpr int kX2MaxPerSm = 4;   // resident CTAs per SM (registers)
 
-struct __align__(16) smem_pair_t {
+template <int NT>
+struct __align__(16) smem_pair_nt_t {
   uint16_t D[pg::kMaxNodes * pg::kMaxZ]; // soft-bit pairs, column stride Z
   uint32_t edge[pg::kBg1Edges];          // col*Z << 16 | s
   uint32_t hard[(22 * pg::kMaxZ) / 32];
-  uint32_t red[kX2Threads / 32];
+  uint32_t red[NT / 32];
   int      s_last;
   int      s_done;
 };
+using smem_pair_t      = smem_pair_nt_t<kX2Threads>;
 using smem_x2_scalar_t = smem_scalar_t<kX2Threads, kX2Threads>;
 constexpr size_t kX2Smem = sizeof(smem_pair_t) > sizeof(smem_x2_scalar_t) ? sizeof(smem_pair_t)
                                                                            : sizeof(smem_x2_scalar_t);
+
+// Split decoder: 384 threads per codeblock. Pair mode (even Z > 192) runs two threads per lane
+// pair, each taking every second edge of a row; other lifting sizes run the one-lane arithmetic
+// with one thread per lane.
+constexpr int kSplitThreads  = 384;
+constexpr int kSplitMaxPerSm = 2;
+using smem_split_pair_t      = smem_pair_nt_t<kSplitThreads>;
+using smem_split_scalar_t    = smem_scalar_t<kSplitThreads, pg::kMaxZ>;
+constexpr size_t kSplitSmem  = sizeof(smem_split_pair_t) > sizeof(smem_split_scalar_t) ? sizeof(smem_split_pair_t)
+                                                                                        : sizeof(smem_split_scalar_t);
 
 __device__ __forceinline__ uint32_t h2_sub(uint32_t a, uint32_t b)
 {
@@ -698,6 +753,88 @@ __device__ __forceinline__ void row_update_pair(const unsigned j, const unsigned
   }
 }
 
+// One layer for lane pair j split over two threads: thread t (0 or 1) takes edges t, t + 2, ... of
+// the row (a thread with an odd-degree row's missing last edge contributes +120, which changes no
+// minimum and no sign), the two partial (min1, min2, sign) meet through one shuffle, and each
+// thread updates its own edges. With at most ten edges per thread every row keeps its v2c, soft-bit
+// positions and partner positions in registers. Threads past the last lane pair (j >= H) run the
+// row without loads or stores, so that every shuffle has its whole warp.
+template <int DEG, bool FIRST>
+__device__ __forceinline__ void row_update_split(const unsigned j, const unsigned t, const unsigned Z, const unsigned H,
+                                                 uint16_t* __restrict__ D, const uint32_t* __restrict__ edge,
+                                                 uint16_t* __restrict__ c2v_row, const uint16_t* __restrict__ tab)
+{
+  constexpr int NE     = (DEG + 1) / 2;
+  const bool    active = j < H;
+  uint32_t      v[NE];
+  unsigned      pos[NE], par[NE];
+  uint32_t      min1 = kH120, min2 = kH120;
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const unsigned e     = 2 * k + t;
+    const bool     valid = active && ((DEG % 2) == 0 || k + 1 < NE || e < DEG);
+    const uint32_t ed    = edge[valid ? e : 0];
+    const unsigned p0    = j + (ed & 0xffffu);
+    const unsigned w     = min(p0, p0 - Z); // (j + s) mod Z
+    const unsigned p     = w + (ed >> 16);
+    pos[k]               = p;
+    par[k]               = w < H ? p + H : p - H;
+    uint32_t vv          = kH120;
+    if (valid) {
+      vv = pair_v2c<FIRST>(bytes_to_h2(D[p]), c2v_row + e * kX2Threads);
+    }
+    v[k]             = vv;
+    const uint32_t x = h2_max_xs(min1, vv);
+    min2             = h2_min_xs(min2, x);
+    min1             = h2_min_xs(min1, vv);
+  }
+  const uint32_t o1 = __shfl_xor_sync(0xffffffffu, min1, 1);
+  const uint32_t o2 = __shfl_xor_sync(0xffffffffu, min2, 1);
+  min2              = h2_min_xs(h2_min_xs(min2, o2), h2_max_xs(min1, o1));
+  min1              = h2_min_xs(min1, o1);
+  const uint32_t m1  = min1 & kAbs;
+  const uint32_t s1  = x2_scale(tab, m1);
+  const uint32_t s2  = x2_scale(tab, min2 & kAbs);
+  const uint32_t nds = h2_sub(s1, s2);
+  const uint32_t sgn = min1 & kSign; // sign product of every v2c of the row
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const unsigned e     = 2 * k + t;
+    const bool     valid = active && ((DEG % 2) == 0 || k + 1 < NE || e < DEG);
+    if (valid) {
+      const uint32_t vv  = v[k];
+      const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
+      const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
+      c2v_row[e * kX2Threads] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+      const uint32_t tt  = h2_add(c, vv);
+      const uint32_t cl  = h2_min(h2_max(tt, kHm120), kH120);
+      uint32_t       u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
+      u                  = h2_min(h2_max(u, kHm127), kH127);
+      const uint32_t ub  = h2_to_bytes_biased(u);
+      D[pos[k]]          = (uint16_t)__byte_perm(ub, 0, 0x0020);
+      D[par[k]]          = (uint16_t)__byte_perm(ub, 0, 0x0002);
+    }
+  }
+}
+
+template <bool FIRST>
+__device__ __forceinline__ void row_dispatch_split(int deg, unsigned j, unsigned t, unsigned Z, unsigned H,
+                                                   uint16_t* D, const uint32_t* edge, uint16_t* c2v_row,
+                                                   const uint16_t* tab)
+{
+  switch (deg) {
+    case 3: row_update_split<3, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 4: row_update_split<4, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 5: row_update_split<5, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 6: row_update_split<6, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 7: row_update_split<7, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 8: row_update_split<8, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 9: row_update_split<9, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    case 10: row_update_split<10, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+    default: row_update_split<19, FIRST>(j, t, Z, H, D, edge, c2v_row, tab); break;
+  }
+}
+
 template <bool FIRST>
 __device__ __forceinline__ void row_dispatch_pair(int deg, unsigned j, unsigned Z, unsigned H, uint16_t* D,
                                                   const uint32_t* edge, uint16_t* c2v_row, const uint16_t* tab)
@@ -752,12 +889,15 @@ __device__ __forceinline__ void fetch8(const int8_t* __restrict__ in, int k, int
   }
 }
 
-// Decodes codeblock cb (even Z > 192) with check-to-variable slab `slab`.
-__device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, const int8_t* __restrict__ llrs,
+// Decodes codeblock cb (even Z > 192) with check-to-variable slab `slab`: NT threads, T threads per
+// lane pair (NT = 192 * T).
+template <int NT, int T>
+__device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& sm, const int8_t* __restrict__ llrs,
                                       uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
                                       int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
                                       const uint16_t* __restrict__ scale_tab, const int cb, const int slab)
 {
+  static_assert(NT == kX2Threads * T && (T == 1 || T == 2), "one or two threads per lane pair");
   const int tid = threadIdx.x;
   const int bg  = d.base_graph;
   const int Z   = (int)d.lifting_size;
@@ -784,7 +924,7 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
   const int     nwords   = (msg_len + 31) / 32;
   uint16_t*     D        = sm.D;
 
-  for (int e = tid; e < nedges; e += kX2Threads) {
+  for (int e = tid; e < nedges; e += NT) {
     const int col = c_edge_col[g][e];
     const int s   = c_edge_v[g][e][set] % Z;
     sm.edge[e]    = ((uint32_t)(col * Z) << 16) | (uint32_t)s;
@@ -805,7 +945,7 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
     const bool aligned  = (reinterpret_cast<uintptr_t>(in) & 7u) == 0;
     int        last     = 0;
 #pragma unroll 4
-    for (int q = tid; q < nchunks; q += kX2Threads) {
+    for (int q = tid; q < nchunks; q += NT) {
       const int col = q / per_col;
       const int w0  = (q - col * per_col) * 8;
       const int k   = (col - 2) * Z + w0;
@@ -833,7 +973,7 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
 
   const int input_size = sm.s_last;
   if (input_size < msg_len) {
-    for (int b = tid; b < nbytes; b += kX2Threads) {
+    for (int b = tid; b < nbytes; b += NT) {
       out[b] = 0xff;
     }
     if (tid == 0) {
@@ -857,19 +997,40 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
   const int      max_it = d.max_iterations;
   const int      lane   = tid & 31;
   const unsigned j      = (unsigned)tid;
+  const int nsteps = steps_for_layers(g, nof_layers);
   for (int it = 0; it < max_it; ++it) {
-    int e0 = 0;
-    for (int r = 0; r < nof_layers; ++r) {
-      const int deg = c_row_deg[g][r];
-      if (tid < H) {
-        uint16_t* c2v_row = c2v + (size_t)e0 * kX2Threads + tid;
-        if (it == 0) {
-          row_dispatch_pair<true>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
-        } else {
-          row_dispatch_pair<false>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+    for (int st = 0; st < nsteps; ++st) {
+      // Messages are read from the second iteration on: prefetch the next step's.
+      if (it > 0 || st + 1 == nsteps) {
+        prefetch_step(g, st + 1 < nsteps ? st + 1 : 0, nof_layers, tid, reinterpret_cast<const char*>(c2v),
+                      kX2Threads * 2);
+      }
+      const int r0 = c_step_row0[g][st];
+      const int r1 = min(r0 + (int)c_step_nrows[g][st], nof_layers);
+      if (T == 1 && tid < H) {
+        for (int r = r0; r < r1; ++r) {
+          const int deg     = c_row_deg[g][r];
+          const int e0      = c_row_e0[g][r];
+          uint16_t* c2v_row = c2v + (size_t)e0 * kX2Threads + tid;
+          if (it == 0) {
+            row_dispatch_pair<true>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+          } else {
+            row_dispatch_pair<false>(deg, j, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+          }
+        }
+      } else if (T == 2 && tid < ((2 * H + 31) & ~31)) {
+        const unsigned jp = (unsigned)tid >> 1, tp = (unsigned)tid & 1u;
+        for (int r = r0; r < r1; ++r) {
+          const int deg     = c_row_deg[g][r];
+          const int e0      = c_row_e0[g][r];
+          uint16_t* c2v_row = c2v + (size_t)e0 * kX2Threads + jp;
+          if (it == 0) {
+            row_dispatch_split<true>(deg, jp, tp, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+          } else {
+            row_dispatch_split<false>(deg, jp, tp, (unsigned)Z, (unsigned)H, D, sm.edge + e0, c2v_row, scale_tab);
+          }
         }
       }
-      e0 += deg;
       __syncthreads();
     }
 
@@ -878,7 +1039,7 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
     // after the reversal); each set bit within the CRC length adds x^e mod g.
     int      zero = 0;
     uint32_t crc  = 0;
-    for (int wi = tid >> 5; wi < nwords; wi += kX2Threads / 32) {
+    for (int wi = tid >> 5; wi < nwords; wi += NT / 32) {
       const int      idx = 32 * wi + lane;
       const uint32_t b   = idx < msg_len ? (D[idx] & 0xffu) : 0xffu;
       const bool     bit = b <= 128u;
@@ -899,7 +1060,7 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
     __syncthreads();
     if (tid == 0) {
       uint32_t t = 0;
-      for (int w = 0; w < kX2Threads / 32; ++w) {
+      for (int w = 0; w < NT / 32; ++w) {
         t ^= sm.red[w];
       }
       sm.s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
@@ -933,14 +1094,14 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_t& sm, cons
     }
     bad      = __syncthreads_or(bad);
     int zero = 0;
-    for (int i = tid; i < msg_len; i += kX2Threads) {
+    for (int i = tid; i < msg_len; i += NT) {
       zero |= (D[i] & 0xffu) == 128u;
     }
     zero   = __syncthreads_or(zero);
     result = (!bad && !zero) ? max_it : 0;
   }
 
-  for (int b = tid; b < nbytes; b += kX2Threads) {
+  for (int b = tid; b < nbytes; b += NT) {
     out[b] = (uint8_t)(sm.hard[b >> 2] >> (24 - 8 * (b & 3)));
   }
   if (tid == 0) {
@@ -977,11 +1138,47 @@ __global__ void __launch_bounds__(kX2Threads, kX2MaxPerSm) ldpc_decode_x2_kernel
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
     if (d.lifting_size > kX2Threads) {
-      decode_codeblock_pair(d, *reinterpret_cast<smem_pair_t*>(smem_x2_raw), llrs, bits, iterations, c2v_all,
-                            crc_pow, scale_tab, cb, blockIdx.x);
+      decode_codeblock_pair<kX2Threads, 1>(d, *reinterpret_cast<smem_pair_t*>(smem_x2_raw), llrs, bits, iterations,
+                                           c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
     } else {
       decode_codeblock<0, kX2Threads, kX2Threads>(d, *reinterpret_cast<smem_x2_scalar_t*>(smem_x2_raw), llrs, bits,
                                                   iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      __syncthreads();
+    }
+  }
+}
+
+// Persistent split decoder of a work list, every lifting size: 384 threads per codeblock, pair mode
+// with two threads per lane pair for even Z > 192, the one-lane arithmetic otherwise.
+__global__ void __launch_bounds__(kSplitThreads, kSplitMaxPerSm) ldpc_decode_split_kernel(
+    const pg_ldpc_cb* __restrict__ descs, const int8_t* __restrict__ llrs, uint8_t* __restrict__ bits,
+    int32_t* __restrict__ iterations, int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
+    const uint16_t* __restrict__ scale_tab, const uint32_t* __restrict__ order, int n, int* __restrict__ counter)
+{
+  extern __shared__ __align__(16) unsigned char smem_split_raw[];
+  __shared__ int s_work;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_work = atomicAdd(counter, 1);
+    }
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= n) {
+      break;
+    }
+    const int        cb = order != nullptr ? (int)order[w] : w;
+    const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size > kX2Threads && (d.lifting_size & 1) == 0) {
+      decode_codeblock_pair<kSplitThreads, 2>(d, *reinterpret_cast<smem_split_pair_t*>(smem_split_raw), llrs, bits,
+                                              iterations, c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
+    } else if (d.lifting_size == 384) {
+      decode_codeblock<384, kSplitThreads, pg::kMaxZ>(d, *reinterpret_cast<smem_split_scalar_t*>(smem_split_raw), llrs,
+                                                      bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      __syncthreads();
+    } else {
+      decode_codeblock<0, kSplitThreads, pg::kMaxZ>(d, *reinterpret_cast<smem_split_scalar_t*>(smem_split_raw), llrs,
+                                                    bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
       __syncthreads();
     }
   }
@@ -1057,10 +1254,57 @@ int ldpc_upload_tables(pg_context* ctx)
                     "cudaFuncSetAttribute(ldpc_decode_x2_kernel)");
   }
   if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaFuncSetAttribute(ldpc_decode_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kSplitSmem),
+                    "cudaFuncSetAttribute(ldpc_decode_split_kernel)");
+  }
+  if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_v, v, sizeof(v)), "cudaMemcpyToSymbol(edge_v)");
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemcpyToSymbol(c_row_deg, deg, sizeof(deg)), "cudaMemcpyToSymbol(row_deg)");
+  }
+  // Layer steps: greedy runs of consecutive rows with pairwise disjoint columns.
+  uint8_t  step_row0[2][kBg1Rows] = {}, step_nrows[2][kBg1Rows] = {}, nsteps[2] = {};
+  uint16_t row_e0[2][kBg1Rows + 1] = {};
+  for (int gi = 0; gi < 2; ++gi) {
+    const int rows = gi == 0 ? PG_BG1_ROWS : PG_BG2_ROWS;
+    for (int r = 0; r < rows; ++r) {
+      row_e0[gi][r + 1] = (uint16_t)(row_e0[gi][r] + deg[gi][r]);
+    }
+    uint64_t used[2] = {0, 0}; // columns 0..67 of the current step
+    int      ns      = 0;
+    for (int r = 0; r < rows; ++r) {
+      uint64_t cols[2] = {0, 0};
+      for (int e = row_e0[gi][r]; e < row_e0[gi][r + 1]; ++e) {
+        cols[col[gi][e] >> 6] |= 1ull << (col[gi][e] & 63);
+      }
+      if (r == 0 || (cols[0] & used[0]) != 0 || (cols[1] & used[1]) != 0) {
+        step_row0[gi][ns]  = (uint8_t)r;
+        step_nrows[gi][ns] = 1;
+        ++ns;
+        used[0] = cols[0];
+        used[1] = cols[1];
+      } else {
+        ++step_nrows[gi][ns - 1];
+        used[0] |= cols[0];
+        used[1] |= cols[1];
+      }
+    }
+    nsteps[gi] = (uint8_t)ns;
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_step_row0, step_row0, sizeof(step_row0)), "cudaMemcpyToSymbol(steps)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_step_nrows, step_nrows, sizeof(step_nrows)), "cudaMemcpyToSymbol(steps)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_nsteps, nsteps, sizeof(nsteps)), "cudaMemcpyToSymbol(steps)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_row_e0, row_e0, sizeof(row_e0)), "cudaMemcpyToSymbol(row_e0)");
   }
   if (rc == PG_OK) {
     // Device address of the static scratch on this context's device (current here), looked up
@@ -1112,7 +1356,7 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
                            cudaStream_t stream)
 {
   return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, counter, stream,
-                                kX2MaxPerSm * ctx->sm_count, PG_LDPC_KIND_ALL | PG_LDPC_ROUTE_X2);
+                                kX2MaxPerSm * ctx->sm_count, PG_LDPC_KIND_ALL | ldpc_route(ctx->ldpc_kernel));
 }
 
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
@@ -1129,11 +1373,17 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  // With PG_LDPC_ROUTE_X2 the two-lanes-per-thread kernel decodes every codeblock (four CTAs per
-  // SM); without it ldpc_decode_kernel does (two per SM). The caller provides a slab per CTA
-  // (min(n, max_ctas) slabs, max_ctas <= four per SM).
+  // PG_LDPC_ROUTE_SPLIT: the split kernel decodes every codeblock (two CTAs per SM);
+  // PG_LDPC_ROUTE_X2: the two-lanes-per-thread kernel (four per SM); neither: ldpc_decode_kernel
+  // (two per SM). The caller provides a slab per CTA (min(n, max_ctas) slabs, max_ctas <= four
+  // per SM).
   int rc = PG_OK;
-  if (kinds & PG_LDPC_ROUTE_X2) {
+  if (kinds & PG_LDPC_ROUTE_SPLIT) {
+    const int grid_s = std::max(1, std::min(n, std::min(max_ctas, kSplitMaxPerSm * ctx->sm_count)));
+    ldpc_decode_split_kernel<<<grid_s, kSplitThreads, kSplitSmem, stream>>>(
+        descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
+    rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_split_kernel launch");
+  } else if (kinds & PG_LDPC_ROUTE_X2) {
     const int grid_x2 = std::max(1, std::min(n, std::min(max_ctas, kX2MaxPerSm * ctx->sm_count)));
     ldpc_decode_x2_kernel<<<grid_x2, kX2Threads, kX2Smem, stream>>>(
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);

@@ -505,6 +505,18 @@ int pg_set_kernel_timing(pg_context* ctx, int enabled)
   return PG_OK;
 }
 
+int pg_set_ldpc_kernel(pg_context* ctx, int kernel)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (kernel < PG_LDPC_KERNEL_ONE_LANE || kernel > PG_LDPC_KERNEL_SPLIT) {
+    return set_error(ctx, PG_ERR_INVALID, "unknown LDPC kernel " + std::to_string(kernel));
+  }
+  ctx->ldpc_kernel = kernel;
+  return PG_OK;
+}
+
 static float elapsed_ms(cudaEvent_t a, cudaEvent_t b)
 {
   float ms = -1.0f;

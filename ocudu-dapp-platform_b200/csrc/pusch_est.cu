@@ -199,7 +199,9 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
                                                                      float2* __restrict__ ls_all,
                                                                      pg_port_result* __restrict__ results,
                                                                      const uint32_t* __restrict__ gold,
-                                                                     uint32_t gold_words, int npil_max)
+                                                                     uint32_t gold_words, int npil_max,
+                                                                     const float2* __restrict__ pilots,
+                                                                     float2* __restrict__ cfo_acc)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const est_layout  sm   = est_carve(smem_raw, npil_max);
@@ -231,6 +233,16 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   auto rxp = [&](int d, int k) {
     return cbf16_load(grid + (size_t)dsym[d] * ue.grid_nof_subc + 12 * ue.rb_start + 2 * k);
   };
+  // Pilot of layer l at DM-RS symbol d, pilot k: given by the caller ([d][l][k], dmrs_pusch_estimator's
+  // sequences) or generated here (QPSK of the Gold sequence, the frequency OCC on layer 1).
+  const float a = 0.707106781186547524f; // 1/sqrt(2) (M_SQRT1_2 in float)
+  auto pilot = [&](int d, int l, int k) {
+    if (pilots != nullptr) {
+      return pilots[((size_t)d * nl + l) * npil + k];
+    }
+    const float2 p0 = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
+    return (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
+  };
 
   // Pilot bits c(2 m0) .. c(2 m0 + 2 npil - 1) per DM-RS symbol, m0 = 6 rb_start.
   const int nwords = (2 * npil + 31) / 32;
@@ -246,21 +258,35 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
 
   // LS estimates.
   const float inv_beta = 1.0f / beta;
-  const float a        = 0.707106781186547524f; // 1/sqrt(2) (M_SQRT1_2 in float)
   float       epre     = 0.f;
   for (int i = tid; i < nd * npil; i += kEstThreads) {
     const int    d  = i / npil;
     const int    k  = i - d * npil;
     const float2 y  = rxp(d, k);
     epre += y.x * y.x + y.y * y.y;
-    const float2 p0 = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
-    ext(d, 0)[kMaxV + k] = cmulconjf(y, p0);
+    ext(d, 0)[kMaxV + k] = cmulconjf(y, pilot(d, 0, k));
     if (nl > 1) {
-      const float2 p1      = (k & 1) ? make_float2(-p0.x, -p0.y) : p0;
-      ext(d, 1)[kMaxV + k] = cmulconjf(y, p1);
+      ext(d, 1)[kMaxV + k] = cmulconjf(y, pilot(d, 1, k));
     }
   }
   __syncthreads();
+  if (cfo_acc != nullptr && nd == 2) {
+    // CFO observation: the sum over layers and pilots of LS(second DM-RS symbol) x conj(LS(first)),
+    // before any averaging (port_channel_estimator_average_impl.cpp:593-615).
+    float cr = 0.f, ci = 0.f;
+    for (int i = tid; i < nl * npil; i += kEstThreads) {
+      const int    l  = i / npil;
+      const int    k  = i - l * npil;
+      const float2 q  = cmulconjf(ext(1, l)[kMaxV + k], ext(0, l)[kMaxV + k]);
+      cr += q.x;
+      ci += q.y;
+    }
+    const float tr = block_sum(cr, sm.red, 0);
+    const float ti = block_sum(ci, sm.red, 0);
+    if (tid == 0) {
+      cfo_acc[(size_t)u * 4 + port] = make_float2(tr, ti);
+    }
+  }
   for (int i = tid; i < nd * nl * (npil / 2); i += kEstThreads) {
     const int d  = i / (nl * (npil / 2));
     const int r  = i - d * nl * (npil / 2);
@@ -344,7 +370,6 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   for (int i = tid; i < nd * npil; i += kEstThreads) {
     const int    d    = i / npil;
     const int    k    = i - d * npil;
-    const float2 p0   = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
     float2       pred = make_float2(0.f, 0.f);
     for (int l = 0; l < nl; ++l) {
       float2 sacc = make_float2(0.f, 0.f);
@@ -353,8 +378,7 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
         sacc.x += f.x * sf;
         sacc.y += f.y * sf;
       }
-      const float2 p = (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
-      const float2 q = cmulf(sacc, p);
+      const float2 q = cmulf(sacc, pilot(d, l, k));
       pred.x += q.x;
       pred.y += q.y;
     }
@@ -406,6 +430,105 @@ __global__ void symbol_estimates_kernel(pg_pusch_ue ue, const float2* __restrict
       v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
     }
     out[(((size_t)p * 14 + s) * nl + l) * nsc + j] = float_to_bf16_rne(v.x) | (float_to_bf16_rne(v.y) << 16);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Time alignment of one receive port (time_alignment_estimator_dft_impl.cpp:97-233, called by
+// port_channel_estimator_helpers.cpp:235-272 with the smoothed pilots and stride 2).
+constexpr int kTaMaxDft = 4096; // pow2(log2_ceil(MAX_NOF_SUBCARRIERS = 3300))
+
+// Power of the inverse DFT of every (DM-RS symbol, layer) sequence of smoothed pilots, summed over
+// the sequences: corr[n] = sum_q |sum_k x_q[k] e^{+j 2 pi k n / N}|^2 (the pilots zero-padded to
+// N, a power of two). x_q[k] = est[q][2 k], the filter output at pilot k.
+__global__ void ta_correlation_kernel(const float2* __restrict__ est, int nseq, int nsc, int npil, int N,
+                                      float* __restrict__ corr)
+{
+  __shared__ float2 tw[kTaMaxDft];
+  for (int m = threadIdx.x; m < N; m += blockDim.x) {
+    float sn, cs;
+    sincospif(2.0f * (float)m / (float)N, &sn, &cs);
+    tw[m] = make_float2(cs, sn);
+  }
+  __syncthreads();
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) {
+    return;
+  }
+  float power = 0.f;
+  for (int q = 0; q < nseq; ++q) {
+    const float2* x   = est + (size_t)q * nsc;
+    float         re  = 0.f, im = 0.f;
+    unsigned      idx = 0; // k n mod N
+    for (int k = 0; k < npil; ++k) {
+      const float2 v = __ldg(x + 2 * k);
+      const float2 w = tw[idx];
+      re += v.x * w.x - v.y * w.y;
+      im += v.x * w.y + v.y * w.x;
+      idx = (idx + (unsigned)n) & (unsigned)(N - 1);
+    }
+    power += re * re + im * im;
+  }
+  corr[n] = power;
+}
+
+struct ta_cfo_out {
+  double time_alignment_s;
+  float  cfo_hz;
+  float  pad;
+};
+
+// Peak of the correlation among the max_ta delayed and the max_ta advanced samples, refined by the
+// reference's five- (three-) point curve fit (lib/support/math/curve_fitting_find_max.cpp) unless N
+// is the largest DFT size; and the CFO from the phase of the DM-RS-symbol correlation:
+// arg / (2 pi (epoch_1 - epoch_0)) * scs (port_channel_estimator_average_impl.cpp:612-615, :53).
+__global__ void ta_cfo_kernel(const float* __restrict__ corr, int N, int max_ta, double fs,
+                              const float2* __restrict__ cfo_acc, float epoch_diff, float scs_hz,
+                              ta_cfo_out* __restrict__ out)
+{
+  if (threadIdx.x != 0 || blockIdx.x != 0) {
+    return;
+  }
+  int   di = 0, ai = 0;
+  float dv = 0.f, av = 0.f;
+  for (int i = 0; i < max_ta; ++i) {
+    const float v = corr[i];
+    if (i == 0 || v > dv) {
+      dv = v;
+      di = i;
+    }
+    const float w = corr[N - max_ta + i];
+    if (i == 0 || w > av) {
+      av = w;
+      ai = i;
+    }
+  }
+  int idx = -(max_ta - ai);
+  if (dv >= av) {
+    idx = di;
+  }
+  float frac = 0.f;
+  if (N != kTaMaxDft) {
+    const float nw5[5] = {-0.400000f, -0.200000f, 0.000000f, 0.200000f, 0.400000f};
+    const float dw5[5] = {0.571429f, -0.285714f, -0.571429f, -0.285714f, 0.571429f};
+    const float nw3[3] = {-0.5f, 0.0f, 0.5f};
+    const float dw3[3] = {0.5f, -1.0f, 0.5f};
+    const int   taps   = max_ta > 2 ? 5 : 3;
+    float       num = 0.f, den = 0.f;
+    for (int i = 0; i < taps; ++i) {
+      const float smp = corr[(unsigned)(idx + i + N - taps / 2) & (unsigned)(N - 1)];
+      num             = __fadd_rn(num, __fmul_rn(taps == 5 ? nw5[i] : nw3[i], smp));
+      den             = __fadd_rn(den, __fmul_rn(taps == 5 ? dw5[i] : dw3[i], smp));
+    }
+    const float r = -(taps == 5 ? 1.0f : 0.5f) * num / den;
+    frac          = (isnan(r) || isinf(r) || fabsf(r) > 1.0f) ? 0.f : r;
+  }
+  out->time_alignment_s = ((double)idx + (double)frac) / fs;
+  if (cfo_acc != nullptr) {
+    const float2 c = cfo_acc[0];
+    out->cfo_hz    = atan2f(c.y, c.x) / 6.28318530717959f / epoch_diff * scs_hz;
+  } else {
+    out->cfo_hz = __int_as_float(0x7fc00000); // NaN: one DM-RS symbol, no CFO observation
   }
 }
 
@@ -490,7 +613,7 @@ int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_
   const int npil_max = 6 * std::max(1, std::min(max_rb, 275));
   pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, est_smem_bytes(npil_max), s>>>(
       ues_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls), results, ctx->dev.gold,
-      kGoldWords, npil_max);
+      kGoldWords, npil_max, nullptr, nullptr);
   return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
 }
 
@@ -579,6 +702,156 @@ int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, con
                             static_cast<cudaStream_t>(stream)>>>(*ue, reinterpret_cast<const float2*>(est), out, nd,
                                                                  d0, d1);
   return check_cuda(ctx, cudaGetLastError(), "symbol_estimates_kernel launch");
+}
+
+int pg_port_channel_estimate_host(pg_context* ctx, const pg_port_estimate_cfg* cfg, const uint32_t* grid,
+                                  const float* pilots, float* freq_response, uint32_t* symbol_estimates,
+                                  pg_port_estimate_result* result)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (cfg == nullptr || grid == nullptr || pilots == nullptr || freq_response == nullptr || result == nullptr) {
+    return set_error(ctx, PG_ERR_INVALID, "null argument");
+  }
+  const int mu = cfg->scs_khz == 15 ? 0 : cfg->scs_khz == 30 ? 1 : cfg->scs_khz == 60 ? 2 : cfg->scs_khz == 120 ? 3 : -1;
+  if (mu < 0) {
+    return set_error(ctx, PG_ERR_INVALID, "subcarrier spacing must be 15, 30, 60 or 120 kHz");
+  }
+  pg_pusch_ue ue       = {};
+  ue.grid_nof_subc     = cfg->grid_nof_subc;
+  ue.dmrs_scaling      = cfg->scaling;
+  ue.rb_start          = cfg->rb_start;
+  ue.nof_rb            = cfg->nof_rb;
+  ue.dmrs_symbol_mask  = cfg->dmrs_symbol_mask;
+  ue.first_symbol      = cfg->first_symbol;
+  ue.nof_symbols       = cfg->nof_symbols;
+  ue.nof_rx_ports      = 1;
+  ue.nof_layers        = cfg->nof_layers;
+  ue.modulation_order  = 2;
+  ue.dc_subcarrier     = -1;
+  if (int rc = validate_ues(ctx, &ue, 1)) {
+    return rc;
+  }
+  int       d0 = 0, d1 = 0;
+  const int nd   = dmrs_count(ue, &d0, &d1);
+  const int nl   = ue.nof_layers;
+  const int npil = 6 * ue.nof_rb;
+  const int nsc  = 12 * ue.nof_rb;
+
+  // Inverse-DFT size of the time-alignment estimator: the pilot count scaled by 4096 / 3300 (guard
+  // against circular interference), rounded up to a power of two, at least 128
+  // (time_alignment_estimator_dft_impl.cpp:19-24, :160-175).
+  unsigned req = (unsigned)npil * kTaMaxDft / 3300u;
+  unsigned N   = 1;
+  while (N < req) {
+    N <<= 1;
+  }
+  N = std::max(N, 128u);
+  // Sampling rate of the correlation (stride 2 for the type-1 comb) and the window of half a cyclic
+  // prefix (144 kappa / 2^(mu + 1)), with the reference's double arithmetic.
+  const double tc          = 1.0 / (480000.0 * 4096.0);
+  const double fs          = (double)((uint64_t)N * cfg->scs_khz * 1000u * 2u);
+  const int    max_ta      = (int)std::floor((double)((144 * 64) >> (mu + 1)) * tc * fs);
+  // OFDM symbol start epochs in useful-symbol durations (normal cyclic prefix): the first symbol of
+  // each half subframe has 16 kappa more cyclic prefix.
+  auto epoch = [&](int sym) {
+    double e = 0.0;
+    for (int i = 0; i <= sym; ++i) {
+      const int  per_half = 7 << mu;
+      const bool longcp   = (i % per_half) == 0;
+      const double cp_tc  = (double)((144 * 64) >> mu) + (longcp ? 16.0 * 64.0 : 0.0);
+      e += (i == 0 ? 0.0 : 1.0) + cp_tc / (double)((2048 * 64) >> mu);
+    }
+    return (float)e;
+  };
+  const float epoch_diff = nd == 2 ? epoch(d1) - epoch(d0) : 0.f;
+
+  const size_t grid_words = (size_t)14 * cfg->grid_nof_subc;
+  const size_t pil_bytes  = (size_t)nd * nl * npil * 8;
+  const size_t est_bytes  = (size_t)nd * nl * nsc * 8;
+  const size_t sym_bytes  = (size_t)14 * nl * nsc * 4;
+  auto al                 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t o_pil      = al(grid_words * 4);
+  const size_t o_est      = o_pil + al(pil_bytes);
+  const size_t o_sym      = o_est + al(est_bytes);
+  const size_t o_res      = o_sym + al(sym_bytes);
+  const size_t o_cfo      = o_res + al(4 * sizeof(pg_port_result));
+  const size_t o_corr     = o_cfo + al(4 * sizeof(float2));
+  const size_t o_out      = o_corr + al((size_t)kTaMaxDft * 4);
+  const size_t total      = o_out + al(sizeof(ta_cfo_out));
+  cudaStream_t s          = ctx->stream;
+  int          rc         = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc == PG_OK) {
+    rc = ensure_scratch(ctx, &ctx->scratch_a, &ctx->scratch_a_cap, total, "cudaMalloc(port estimate)");
+  }
+  if (rc != PG_OK) {
+    return rc;
+  }
+  char* b = static_cast<char*>(ctx->scratch_a);
+  rc      = check_cuda(ctx, cudaMemcpyAsync(b, grid, grid_words * 4, cudaMemcpyHostToDevice, s), "H2D grid");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(b + o_pil, pilots, pil_bytes, cudaMemcpyHostToDevice, s), "H2D pilots");
+  }
+  void* dev = nullptr;
+  if (rc == PG_OK) {
+    rc = stage_slot(ctx, SLOT_UE, &ue, sizeof(ue), s, &dev);
+  }
+  if (rc == PG_OK) {
+    pusch_estimate_kernel<<<dim3(1, 1), kEstThreads, est_smem_bytes(npil), s>>>(
+        static_cast<const pg_pusch_ue*>(dev), reinterpret_cast<const uint32_t*>(b), reinterpret_cast<float2*>(b + o_est),
+        nullptr, reinterpret_cast<pg_port_result*>(b + o_res), ctx->dev.gold, kGoldWords, npil,
+        reinterpret_cast<const float2*>(b + o_pil), reinterpret_cast<float2*>(b + o_cfo));
+    rc = check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
+  }
+  if (rc == PG_OK && symbol_estimates != nullptr) {
+    symbol_estimates_kernel<<<dim3((nl * nsc + 255) / 256, 14, 1), 256, 0, s>>>(
+        ue, reinterpret_cast<const float2*>(b + o_est), reinterpret_cast<uint32_t*>(b + o_sym), nd, d0, d1);
+    rc = check_cuda(ctx, cudaGetLastError(), "symbol_estimates_kernel launch");
+  }
+  if (rc == PG_OK) {
+    ta_correlation_kernel<<<(N + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float2*>(b + o_est), nd * nl, nsc,
+                                                          npil, (int)N, reinterpret_cast<float*>(b + o_corr));
+    rc = check_cuda(ctx, cudaGetLastError(), "ta_correlation_kernel launch");
+  }
+  if (rc == PG_OK) {
+    ta_cfo_kernel<<<1, 32, 0, s>>>(reinterpret_cast<const float*>(b + o_corr), (int)N, max_ta, fs,
+                                   nd == 2 ? reinterpret_cast<const float2*>(b + o_cfo) : nullptr, epoch_diff,
+                                   (float)cfg->scs_khz * 1000.0f, reinterpret_cast<ta_cfo_out*>(b + o_out));
+    rc = check_cuda(ctx, cudaGetLastError(), "ta_cfo_kernel launch");
+  }
+  pg_port_result pr  = {};
+  ta_cfo_out     tco = {};
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(freq_response, b + o_est, est_bytes, cudaMemcpyDeviceToHost, s), "D2H est");
+  }
+  if (rc == PG_OK && symbol_estimates != nullptr) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(symbol_estimates, b + o_sym, sym_bytes, cudaMemcpyDeviceToHost, s),
+                    "D2H symbol estimates");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(&pr, b + o_res, sizeof(pr), cudaMemcpyDeviceToHost, s), "D2H result");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(&tco, b + o_out, sizeof(tco), cudaMemcpyDeviceToHost, s), "D2H TA");
+  }
+  if (rc == PG_OK) {
+    rc = release_slot_after(ctx, SLOT_UE, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  }
+  if (rc != PG_OK) {
+    return rc;
+  }
+  result->noise_var        = pr.noise_var;
+  result->epre             = pr.epre;
+  result->snr              = pr.snr;
+  result->rsrp[0]          = pr.rsrp[0];
+  result->rsrp[1]          = pr.rsrp[1];
+  result->cfo_hz           = tco.cfo_hz;
+  result->time_alignment_s = tco.time_alignment_s;
+  return PG_OK;
 }
 
 } // extern "C"

@@ -77,7 +77,7 @@ struct pg_pusch_plan {
   int             le_nseq   = 0;
   int             le_rows   = 0;
   // Launch shapes (defaults, or the autotuner's choice).
-  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, 0};
+  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, PG_LDPC_KERNEL_SPLIT};
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -149,7 +149,7 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
                                 p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count,
-                                p->ldpc_kinds | (p->tuning.ldpc_z384_two_lanes ? PG_LDPC_ROUTE_X2 : 0));
+                                p->ldpc_kinds | ldpc_route(p->tuning.ldpc_kernel));
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
@@ -509,7 +509,7 @@ static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
          t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
          t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm <= 4 &&
-         (t.ldpc_z384_two_lanes == 0 || t.ldpc_z384_two_lanes == 1);
+         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_SPLIT;
 }
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
@@ -655,9 +655,9 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
       c.ldpc_ctas_per_sm     = v;
       if (rc == PG_OK) rc = try_set(c);
     }
-    for (int v : {0, 1}) {
+    for (int v : {PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT}) {
       pg_pusch_plan_tuning c = cur;
-      c.ldpc_z384_two_lanes  = v;
+      c.ldpc_kernel          = v;
       if (rc == PG_OK) rc = try_set(c);
     }
   }

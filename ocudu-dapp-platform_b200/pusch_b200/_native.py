@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libpusch_b200.so")
 PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_CAPACITY, PG_ERR_TIMEOUT, PG_ERR_NO_DEVICE = range(6)
 PG_CRC16, PG_CRC24A, PG_CRC24B = 0, 1, 2
 PG_CRC_NONE = 255
+# pg_ldpc_kernel: one lifted lane per thread, two lanes per thread (f16x2), two lanes per thread pair.
+PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT = 0, 1, 2
 
 STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_INVALID", 2: "PG_ERR_CUDA", 3: "PG_ERR_CAPACITY", 4: "PG_ERR_TIMEOUT",
                 5: "PG_ERR_NO_DEVICE"}
@@ -79,7 +81,7 @@ class PgLeAdam(ctypes.Structure):
 
 class PgPuschPlanTuning(ctypes.Structure):
     _fields_ = [("rm_ctas_per_cb", ctypes.c_int), ("demod_res_per_thread", ctypes.c_int),
-                ("demod_block", ctypes.c_int), ("ldpc_ctas_per_sm", ctypes.c_int), ("ldpc_z384_two_lanes", ctypes.c_int)]
+                ("demod_block", ctypes.c_int), ("ldpc_ctas_per_sm", ctypes.c_int), ("ldpc_kernel", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -100,6 +102,21 @@ class PgUlschDemuxConfig(ctypes.Structure):
 class PgUciShortBlock(ctypes.Structure):
     _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("out_offset", ctypes.c_uint32),
                 ("nof_bits", ctypes.c_uint8), ("modulation_order", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 2)]
+
+
+class PgPortEstimateCfg(ctypes.Structure):
+    _fields_ = [("grid_nof_subc", ctypes.c_uint32), ("scaling", ctypes.c_float), ("rb_start", ctypes.c_uint16),
+                ("nof_rb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16), ("first_symbol", ctypes.c_uint8),
+                ("nof_symbols", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8), ("scs_khz", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8 * 2)]
+
+
+class PgPortEstimateResult(ctypes.Structure):
+    _fields_ = [("noise_var", ctypes.c_float), ("epre", ctypes.c_float), ("snr", ctypes.c_float),
+                ("rsrp", ctypes.c_float * 2), ("cfo_hz", ctypes.c_float), ("time_alignment_s", ctypes.c_double)]
+
+
+assert ctypes.sizeof(PgPortEstimateCfg) == 20 and ctypes.sizeof(PgPortEstimateResult) == 32
 
 
 class PgPuschPlanInfo(ctypes.Structure):
@@ -185,6 +202,8 @@ SIGNATURES = {
     "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
+    "pg_set_ldpc_kernel": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "pg_port_channel_estimate_host": (ctypes.c_int, [_VP] * 7),
 }
 
 _lib = None

@@ -134,6 +134,10 @@ class LdpcBatchDecoder:
                                                     stream_ptr)
         self.ctx.check(rc)
 
+    def set_kernel(self, kernel: int):
+        """Selects the decoding kernel (_native.PG_LDPC_KERNEL_*); results do not depend on it."""
+        self.ctx.check(self.lib.pg_set_ldpc_kernel(self.ctx.handle, int(kernel)))
+
     def set_kernel_timing(self, enabled: bool):
         self.ctx.check(self.lib.pg_set_kernel_timing(self.ctx.handle, int(enabled)))
 

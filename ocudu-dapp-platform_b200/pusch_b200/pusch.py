@@ -109,6 +109,48 @@ class PuschProcessor:
         return out
 
 
+@dataclass
+class PortEstimate:
+    """port_channel_estimator_results of one receive port."""
+    freq_response: np.ndarray      # complex64 [dmrs symbol][layer][12 nof_rb], FP32
+    symbol_estimates: np.ndarray   # uint32 cbf16 [14][layer][12 nof_rb]
+    noise_var: float
+    epre: float
+    snr: float
+    rsrp: np.ndarray
+    cfo_hz: Optional[float]
+    time_alignment_s: float
+
+
+class PortChannelEstimator:
+    """Mirror of ``port_channel_estimator::compute`` (port_channel_estimator.h:86-89) for one port,
+    FD "filter", TD "interpolate": the caller gives that port's grid and the DM-RS pilots."""
+
+    def __init__(self, context: _native.Context):
+        self.ctx = context
+        self.lib = context.lib
+
+    def compute(self, grid_port, pilots, rb_start, nof_rb, dmrs_symbols, scaling, first_symbol=0, nof_symbols=14,
+                scs_khz=30) -> PortEstimate:
+        """grid_port: uint32 cbf16 [14][nsubc]; pilots: complex64 [dmrs symbol][layer][6 nof_rb]."""
+        g = np.ascontiguousarray(grid_port, np.uint32)
+        pil = np.ascontiguousarray(pilots, np.complex64)
+        nd, nl = pil.shape[0], pil.shape[1]
+        cfg = _native.PgPortEstimateCfg()
+        cfg.grid_nof_subc, cfg.scaling, cfg.rb_start, cfg.nof_rb = g.shape[1], scaling, rb_start, nof_rb
+        cfg.dmrs_symbol_mask = sum(1 << s for s in dmrs_symbols)
+        cfg.first_symbol, cfg.nof_symbols, cfg.nof_layers, cfg.scs_khz = first_symbol, nof_symbols, nl, scs_khz
+        freq = np.zeros((nd, nl, 12 * nof_rb), np.complex64)
+        sym = np.zeros((14, nl, 12 * nof_rb), np.uint32)
+        res = _native.PgPortEstimateResult()
+        self.ctx.check(self.lib.pg_port_channel_estimate_host(
+            self.ctx.handle, ctypes.byref(cfg), g.ctypes.data_as(ctypes.c_void_p), pil.ctypes.data_as(ctypes.c_void_p),
+            freq.ctypes.data_as(ctypes.c_void_p), sym.ctypes.data_as(ctypes.c_void_p), ctypes.byref(res)))
+        cfo = None if np.isnan(res.cfo_hz) else float(res.cfo_hz)
+        return PortEstimate(freq, sym, float(res.noise_var), float(res.epre), float(res.snr),
+                            np.array(res.rsrp[:nl], np.float64), cfo, float(res.time_alignment_s))
+
+
 def batch_descriptors(slots: Sequence[PuschSlot], max_iterations=6, dc_subcarrier=-1):
     """pg_pusch_ue array of every UE of every slot (one cell per slot), grids concatenated in slot
     order, TBs packed back to back. Returns (descriptors, grid words, TB bytes, UE list)."""

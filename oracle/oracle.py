@@ -148,6 +148,26 @@ class Ref:
         return freq, sym, dict(noise_var=float(sc[0]), epre=float(sc[1]), snr=float(sc[2]),
                                rsrp=sc[3:].astype(np.float64))
 
+    def port_estimate_full(self, grid, port, slot, n_id, rb_start, nof_rb, nof_layers, dmrs_symbols, scaling,
+                           n_scid=0):
+        """port_estimate plus the pilots the reference used (complex64 [nd][nl][6 nof_rb]) and its
+        CFO (Hz, NaN when none) and time alignment (s) in the scalars dict."""
+        g = np.ascontiguousarray(grid, np.uint32)
+        nports, _, nsubc = g.shape
+        nd = len(dmrs_symbols)
+        freq = np.zeros((nd, nof_layers, 12 * nof_rb), np.complex64)
+        sym = np.zeros((14, nof_layers, 12 * nof_rb), np.uint32)
+        sc = np.zeros(3 + nof_layers, np.float32)
+        pil = np.zeros((nd, nof_layers, 6 * nof_rb), np.complex64)
+        ct = np.zeros(2, np.float64)
+        mask = sum(1 << s for s in dmrs_symbols)
+        f = self.lib.ref_port_estimate_full
+        f.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 9 + [ctypes.c_uint32, ctypes.c_float] + [ctypes.c_void_p] * 5
+        f(_ptr(g), nports, nsubc, port, slot, n_id, n_scid, rb_start, nof_rb, nof_layers, mask, ctypes.c_float(scaling),
+          _ptr(freq), _ptr(sym), _ptr(sc), _ptr(pil), _ptr(ct))
+        return freq, sym, dict(noise_var=float(sc[0]), epre=float(sc[1]), snr=float(sc[2]),
+                               rsrp=sc[3:].astype(np.float64), cfo_hz=float(ct[0]), ta_s=float(ct[1]), pilots=pil)
+
     def pusch_decode_mt(self, descs, grid, tb_bytes, threads):
         """The reference's CPU receive path over a pg_pusch_ue array (ctypes) and its grids.
         Returns (ok flags, mean iterations, TB bytes, wall seconds)."""

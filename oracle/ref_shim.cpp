@@ -506,21 +506,23 @@ extern "C" {
 /// Outputs: freq (complex float [nof_dmrs][nof_layers][12*nof_rb], the FP32 response),
 /// sym_est (cbf16 [14][nof_layers][12*nof_rb], the public per-symbol estimates) and
 /// scalars {noise_var, epre, snr, rsrp[layer]...}.
-int ref_port_estimate(const uint32_t* grid,
-                      int             nports,
-                      int             nsubc,
-                      int             port,
-                      int             slot,
-                      int             n_id,
-                      int             n_scid,
-                      int             rb_start,
-                      int             nof_rb,
-                      int             nof_layers,
-                      uint32_t        dmrs_symbol_mask,
-                      float           scaling,
-                      float*          freq,
-                      uint32_t*       sym_est,
-                      float*          scalars)
+static int port_estimate_impl(const uint32_t* grid,
+                              int             nports,
+                              int             nsubc,
+                              int             port,
+                              int             slot,
+                              int             n_id,
+                              int             n_scid,
+                              int             rb_start,
+                              int             nof_rb,
+                              int             nof_layers,
+                              uint32_t        dmrs_symbol_mask,
+                              float           scaling,
+                              float*          freq,
+                              uint32_t*       sym_est,
+                              float*          scalars,
+                              float*          pilots_out,
+                              double*         cfo_ta)
 {
   array_grid_reader reader(grid, nports, 14, nsubc);
   auto              prg = create_pseudo_random_generator_sw_factory()->create();
@@ -598,7 +600,65 @@ int ref_port_estimate(const uint32_t* grid,
   for (int l = 0; l < nof_layers; ++l) {
     scalars[3 + l] = res.get_rsrp(l);
   }
+  if (pilots_out != nullptr) {
+    for (unsigned d = 0; d != nof_dmrs; ++d) {
+      for (int l = 0; l < nof_layers; ++l) {
+        span<const cf_t> pl = pilots.get_symbol(d, l);
+        std::memcpy(pilots_out + ((size_t)d * nof_layers + l) * 2 * npil, pl.data(), npil * sizeof(cf_t));
+      }
+    }
+  }
+  if (cfo_ta != nullptr) {
+    std::optional<float> cfo = res.get_cfo_Hz();
+    cfo_ta[0]                = cfo.has_value() ? static_cast<double>(*cfo) : std::nan("");
+    cfo_ta[1]                = res.get_time_alignment().to_seconds();
+  }
   return 0;
+}
+
+int ref_port_estimate(const uint32_t* grid,
+                      int             nports,
+                      int             nsubc,
+                      int             port,
+                      int             slot,
+                      int             n_id,
+                      int             n_scid,
+                      int             rb_start,
+                      int             nof_rb,
+                      int             nof_layers,
+                      uint32_t        dmrs_symbol_mask,
+                      float           scaling,
+                      float*          freq,
+                      uint32_t*       sym_est,
+                      float*          scalars)
+{
+  return port_estimate_impl(grid, nports, nsubc, port, slot, n_id, n_scid, rb_start, nof_rb, nof_layers,
+                            dmrs_symbol_mask, scaling, freq, sym_est, scalars, nullptr, nullptr);
+}
+
+/// ref_port_estimate that also returns the pilots it used (cf32 [nof_dmrs][nof_layers][6*nof_rb],
+/// dmrs_pusch_estimator_impl's sequences) and the reference's CFO in Hz (NaN when it has none) and
+/// time alignment in seconds (cfo_ta[0], cfo_ta[1]).
+int ref_port_estimate_full(const uint32_t* grid,
+                           int             nports,
+                           int             nsubc,
+                           int             port,
+                           int             slot,
+                           int             n_id,
+                           int             n_scid,
+                           int             rb_start,
+                           int             nof_rb,
+                           int             nof_layers,
+                           uint32_t        dmrs_symbol_mask,
+                           float           scaling,
+                           float*          freq,
+                           uint32_t*       sym_est,
+                           float*          scalars,
+                           float*          pilots_out,
+                           double*         cfo_ta)
+{
+  return port_estimate_impl(grid, nports, nsubc, port, slot, n_id, n_scid, rb_start, nof_rb, nof_layers,
+                            dmrs_symbol_mask, scaling, freq, sym_est, scalars, pilots_out, cfo_ta);
 }
 
 /// PUSCH MCS (TS 38.214 Tables 5.1.3.1-1/2; table 0 = qam64, 1 = qam256), no transform

@@ -8,8 +8,25 @@
 //   crc_calculator       equal checksums from calculate / calculate_byte / calculate_bit
 //   demodulation_mapper  |difference| <= 1 LSB, at least 99.9 % equal
 //   channel_equalizer    relative error <= 2.5e-4 (the reference's 14-bit reciprocal estimate)
+//   port_channel_estimator  noise, EPRE, SNR, RSRP within 1e-4; per-symbol bf16 estimates equal or
+//                        one unit apart (over 99 % equal); CFO within 1e-3 Hz (or 1e-3 relative);
+//                        time alignment within one T_c
+//   pusch_decoder        (with a codeword file, argv[1]) bit-exact TBs, CRC flags, codeblock counts,
+//                        iteration statistics and rx-buffer soft bits over two transmissions (HARQ)
 // Test infrastructure: it links the reference's compiled code (oracle/_ref).
 #include "../../ocudu-dapp-platform_b200/adapters/b200_phy_adapters.h"
+
+#include "lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.h"
+#include "lib/phy/upper/signal_processors/dmrs_helper.h"
+#include "ocudu/phy/generic_functions/generic_functions_factories.h"
+#include "ocudu/phy/support/resource_grid_reader.h"
+#include "ocudu/phy/support/time_alignment_estimator/time_alignment_estimator_factories.h"
+#include "ocudu/phy/upper/channel_coding/ldpc/ldpc_segmenter_rx.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_notifier.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_result.h"
+#include "ocudu/phy/upper/rx_buffer_pool.h"
+#include "ocudu/phy/upper/sequence_generators/sequence_generator_factories.h"
+#include "ocudu/phy/upper/signal_processors/channel_estimator/factories.h"
 
 #include "ocudu/adt/bit_buffer.h"
 #include "ocudu/ocuduvec/bit.h"
@@ -313,7 +330,339 @@ void check_equalizer(const b200::device_config& dev)
 
 } // namespace
 
-int main()
+// ---------------------------------------------------------------------------------------------
+// A resource_grid_reader over a cbf16 array [port][symbol][subcarrier].
+class vector_grid_reader : public resource_grid_reader
+{
+public:
+  vector_grid_reader(const std::vector<cbf16_t>& data, unsigned nports, unsigned nsubc) :
+    data_(data), nports_(nports), nsubc_(nsubc)
+  {
+  }
+  unsigned     get_nof_ports() const override { return nports_; }
+  unsigned     get_nof_subc() const override { return nsubc_; }
+  unsigned     get_nof_symbols() const override { return MAX_NSYMB_PER_SLOT; }
+  bool         is_empty(unsigned) const override { return false; }
+  bool         is_empty() const override { return false; }
+  crb_interval get_allocation_range(unsigned, unsigned) const override { return {0, nsubc_ / 12}; }
+  span<cf_t>   get(span<cf_t> symbols, unsigned port, unsigned l, unsigned k_init,
+                   const bounded_bitset<MAX_NOF_SUBCARRIERS>& mask) const override
+  {
+    mask.for_each(0, mask.size(), [&](unsigned k) {
+      symbols.front() = to_cf(view(port, l)[k_init + k]);
+      symbols         = symbols.last(symbols.size() - 1);
+    });
+    return symbols;
+  }
+  span<cbf16_t> get(span<cbf16_t> symbols, unsigned port, unsigned l, unsigned k_init,
+                    const bounded_bitset<MAX_NOF_SUBCARRIERS>& mask) const override
+  {
+    mask.for_each(0, mask.size(), [&](unsigned k) {
+      symbols.front() = view(port, l)[k_init + k];
+      symbols         = symbols.last(symbols.size() - 1);
+    });
+    return symbols;
+  }
+  void get(span<cf_t> symbols, unsigned port, unsigned l, unsigned k_init, unsigned stride) const override
+  {
+    for (unsigned i = 0; i != symbols.size(); ++i) {
+      symbols[i] = to_cf(view(port, l)[k_init + i * stride]);
+    }
+  }
+  void get(span<cbf16_t> symbols, unsigned port, unsigned l, unsigned k_init) const override
+  {
+    std::copy_n(view(port, l).begin() + k_init, symbols.size(), symbols.begin());
+  }
+  span<const cbf16_t> get_view(unsigned port, unsigned l) const override { return view(port, l); }
+
+private:
+  span<const cbf16_t> view(unsigned port, unsigned l) const
+  {
+    return span<const cbf16_t>(data_.data() + (static_cast<size_t>(port) * MAX_NSYMB_PER_SLOT + l) * nsubc_, nsubc_);
+  }
+  const std::vector<cbf16_t>& data_;
+  unsigned                    nports_, nsubc_;
+};
+
+// port_channel_estimator: seeded slots (random PRB allocation, one or two layers, one or two DM-RS
+// symbols, a multipath channel with a delay and a frequency offset, noise), both estimators on every
+// receive port with the same pilots.
+void check_port_estimator(const b200::device_config& dev)
+{
+  auto ta_factory = create_time_alignment_estimator_dft_factory(create_dft_processor_factory_generic());
+  auto ref_est    = create_port_channel_estimator_factory_sw(ta_factory)
+                     ->create(port_channel_estimator_fd_smoothing_strategy::filter,
+                              port_channel_estimator_td_interpolation_strategy::interpolate, false);
+  auto b200_est = b200::create_port_channel_estimator_factory_b200(dev)->create(
+      port_channel_estimator_fd_smoothing_strategy::filter, port_channel_estimator_td_interpolation_strategy::interpolate,
+      false);
+  auto   prg     = create_pseudo_random_generator_sw_factory()->create();
+  int    ports   = 0, bad = 0;
+  double worst_s = 0, worst_ta = 0, worst_cfo = 0;
+  for (int t = 0; t < 24; ++t) {
+    const unsigned nof_prb_grid = 273, nsubc = 12 * nof_prb_grid, nports = 4;
+    const unsigned nof_rb   = static_cast<unsigned>(uniform(1, 273));
+    const unsigned rb_start = static_cast<unsigned>(uniform(0, static_cast<int>(nof_prb_grid - nof_rb)));
+    const unsigned nl       = static_cast<unsigned>(uniform(1, 2));
+    const bool     two      = uniform(0, 3) != 0;
+    const unsigned n_id = static_cast<unsigned>(uniform(0, 1007)), slot = static_cast<unsigned>(uniform(0, 19));
+    bounded_bitset<MAX_NSYMB_PER_SLOT> symbols(MAX_NSYMB_PER_SLOT);
+    symbols.set(2);
+    if (two) {
+      symbols.set(11);
+    }
+    crb_bitmap rb_mask(rb_start + nof_rb);
+    rb_mask.fill(rb_start, rb_start + nof_rb);
+    const unsigned   nd = two ? 2 : 1, npil = 6 * nof_rb;
+    dmrs_symbol_list pilots({npil, nd, nl});
+    for (unsigned d = 0, s = 0; s < MAX_NSYMB_PER_SLOT; ++s) {
+      if (!symbols.test(s)) {
+        continue;
+      }
+      prg->init(((14 * slot + s + 1) * (2 * n_id + 1) * (1U << 17) + 2 * n_id) % (1U << 31));
+      dmrs_sequence_generate(pilots.get_symbol(d, 0), *prg, M_SQRT1_2, 0, 6, rb_mask);
+      if (nl > 1) {
+        dmrs_pxsch_parameters p1 = get_pxsch_dmrs_params(dmrs_config_type::type1, 1);
+        span<cf_t>            dst = pilots.get_symbol(d, 1);
+        span<const cf_t>      src = pilots.get_symbol(d, 0);
+        std::copy(src.begin(), src.end(), dst.begin());
+        for (unsigned k = 1; k < dst.size(); k += 2) {
+          dst[k] *= p1.w_f[1];
+        }
+      }
+      ++d;
+    }
+    port_channel_estimator::configuration cfg;
+    cfg.scs          = subcarrier_spacing::kHz30;
+    cfg.cp           = cyclic_prefix::NORMAL;
+    cfg.first_symbol = 0;
+    cfg.nof_symbols  = MAX_NSYMB_PER_SLOT;
+    cfg.scaling      = 1.41254f;
+    for (unsigned p = 0; p != nports; ++p) {
+      cfg.rx_ports.push_back(static_cast<uint8_t>(p));
+    }
+    for (unsigned l = 0; l != nl; ++l) {
+      cfg.dmrs_pattern.push_back(
+          {symbols, rb_mask, {}, std::nullopt, get_pxsch_dmrs_params(dmrs_config_type::type1, l).re_pattern});
+    }
+    // Grid: per port and layer a two-tap channel with a delay, a slow CFO rotation, pilots on the
+    // DM-RS comb, noise everywhere.
+    std::vector<cbf16_t> grid(static_cast<size_t>(nports) * MAX_NSYMB_PER_SLOT * nsubc);
+    const float          snr = std::pow(10.f, static_cast<float>(uniform(0, 30)) / 10.f);
+    const float          sig = std::sqrt(0.5f / snr);
+    const float          cfo = static_cast<float>(uniform(-300, 300)); // Hz
+    for (unsigned p = 0; p != nports; ++p) {
+      cf_t  a[2][2];
+      float tau[2];
+      for (unsigned l = 0; l != 2; ++l) {
+        a[l][0] = {gauss() * 0.6f, gauss() * 0.6f};
+        a[l][1] = {gauss() * 0.4f, gauss() * 0.4f};
+        tau[l]  = static_cast<float>(uniform(0, 400)) * 1e-9f;
+      }
+      for (unsigned s = 0; s != MAX_NSYMB_PER_SLOT; ++s) {
+        const cf_t rot = std::polar(1.f, 6.2831853f * cfo * static_cast<float>(s) * 35.7e-6f);
+        for (unsigned k = 0; k != nsubc; ++k) {
+          cf_t y = {sig * gauss(), sig * gauss()};
+          if (k >= 12 * rb_start && k < 12 * (rb_start + nof_rb)) {
+            const unsigned j = k - 12 * rb_start;
+            if (symbols.test(s) && (j % 2) == 0) {
+              const unsigned d = (s == 2) ? 0 : 1;
+              for (unsigned l = 0; l != nl; ++l) {
+                const float f = 30e3f * static_cast<float>(j);
+                const cf_t  h = a[l][0] + a[l][1] * std::polar(1.f, -6.2831853f * f * tau[l]);
+                y += h * pilots.get_symbol(d, l)[j / 2] * cfg.scaling * rot;
+              }
+            } else if (!symbols.test(s)) {
+              y += cf_t{(uniform(0, 1) ? 0.7071f : -0.7071f), (uniform(0, 1) ? 0.7071f : -0.7071f)};
+            }
+          }
+          grid[(static_cast<size_t>(p) * MAX_NSYMB_PER_SLOT + s) * nsubc + k] = to_cbf16(y);
+        }
+      }
+    }
+    vector_grid_reader reader(grid, nports, nsubc);
+    std::vector<cbf16_t> a_sym(12 * nof_rb), b_sym(12 * nof_rb);
+    for (unsigned p = 0; p != nports; ++p, ++ports) {
+      const port_channel_estimator_results& r = ref_est->compute(reader, p, pilots, cfg);
+      const port_channel_estimator_results& g = b200_est->compute(reader, p, pilots, cfg);
+      auto rel = [](float x, float y) { return std::abs(x - y) / std::max(std::abs(y), 1e-30f); };
+      double e = std::max({rel(g.get_noise_variance(), r.get_noise_variance()), rel(g.get_epre(), r.get_epre()),
+                           rel(g.get_snr(), r.get_snr()), rel(g.get_rsrp(0), r.get_rsrp(0))});
+      if (nl > 1) {
+        e = std::max<double>(e, rel(g.get_rsrp(1), r.get_rsrp(1)));
+      }
+      worst_s = std::max(worst_s, e);
+      const double ta = std::abs(static_cast<double>(g.get_time_alignment().to_Tc() - r.get_time_alignment().to_Tc()));
+      worst_ta        = std::max(worst_ta, ta);
+      bool ok         = e <= 1e-4 && ta <= 1;
+      if (r.get_cfo_Hz().has_value() != g.get_cfo_Hz().has_value()) {
+        ok = false;
+      } else if (r.get_cfo_Hz().has_value()) {
+        const double d = std::abs(*g.get_cfo_Hz() - *r.get_cfo_Hz());
+        worst_cfo      = std::max(worst_cfo, d);
+        ok             = ok && d <= std::max(1e-3, 1e-3 * std::abs(*r.get_cfo_Hz()));
+      }
+      unsigned diff1 = 0, equal = 0, total = 0;
+      for (unsigned s = 0; s != MAX_NSYMB_PER_SLOT; ++s) {
+        for (unsigned l = 0; l != nl; ++l) {
+          r.get_symbol_ch_estimate(a_sym, s, l);
+          g.get_symbol_ch_estimate(b_sym, s, l);
+          for (unsigned k = 0; k != a_sym.size(); ++k) {
+            uint32_t x, y;
+            std::memcpy(&x, &a_sym[k], 4);
+            std::memcpy(&y, &b_sym[k], 4);
+            for (int part = 0; part < 32; part += 16) {
+              const int dx = std::abs(static_cast<int>((x >> part) & 0xffff) - static_cast<int>((y >> part) & 0xffff));
+              diff1 += dx > 1;
+              equal += dx == 0;
+              ++total;
+            }
+          }
+        }
+      }
+      ok = ok && diff1 == 0 && equal > 0.99 * total;
+      bad += ok ? 0 : 1;
+    }
+  }
+  char detail[200];
+  std::snprintf(detail, sizeof(detail), "%d ports, worst scalar rel %.2e, TA %.0f Tc, CFO %.2e Hz, %d off", ports,
+                worst_s, worst_ta, worst_cfo, bad);
+  report("port_channel_estimator", bad == 0, detail);
+}
+
+// pusch_decoder: codewords from a file (written by tests/test_dropin.py with the project's
+// transmit-side codec): per transport block its parameters and two transmissions of soft bits.
+// Both decoders get rx buffers of their own pool with the same identifiers.
+struct sch_notifier : public pusch_decoder_notifier {
+  pusch_decoder_result result;
+  bool                 called = false;
+  void                 on_sch_data(const pusch_decoder_result& r) override
+  {
+    result = r;
+    called = true;
+  }
+};
+
+void check_pusch_decoder(const b200::device_config& dev, const char* path)
+{
+  FILE* f = std::fopen(path, "rb");
+  if (f == nullptr) {
+    report("pusch_decoder", false, "cannot open the codeword file");
+    return;
+  }
+  auto crcf = create_crc_calculator_factory_sw("auto");
+  pusch_codeblock_decoder::sch_crc cb_crcs{crcf->create(crc_generator_poly::CRC16),
+                                           crcf->create(crc_generator_poly::CRC24A),
+                                           crcf->create(crc_generator_poly::CRC24B)};
+  ldpc_decoder_factory::ldpc_decoder_factory_configuration fcfg = {false, false};
+  std::vector<std::unique_ptr<pusch_codeblock_decoder>>   cbd;
+  cbd.push_back(std::make_unique<pusch_codeblock_decoder>(create_ldpc_rate_dematcher_factory_sw("auto")->create(),
+                                                          create_ldpc_decoder_factory_sw("auto", fcfg)->create(),
+                                                          cb_crcs));
+  auto pool = std::make_shared<pusch_decoder_impl::codeblock_decoder_pool>(span<std::unique_ptr<pusch_codeblock_decoder>>(cbd));
+  pusch_decoder_impl ref_dec(create_ldpc_segmenter_rx_factory_sw()->create(), pool,
+                             {crcf->create(crc_generator_poly::CRC16), crcf->create(crc_generator_poly::CRC24A),
+                              crcf->create(crc_generator_poly::CRC24B)},
+                             nullptr, 273, 2);
+  auto b200_dec = b200::create_pusch_decoder_factory_b200(dev, 273, 2)->create();
+
+  rx_buffer_pool_config pcfg = {};
+  pcfg.max_codeblock_size    = 66 * 384;
+  pcfg.nof_buffers           = 8;
+  pcfg.nof_codeblocks        = 400;
+  pcfg.expire_timeout_slots  = 100;
+  pcfg.external_soft_bits    = false;
+  auto ref_pool  = create_rx_buffer_pool(pcfg);
+  auto b200_pool = create_rx_buffer_pool(pcfg);
+
+  int32_t ntb = 0;
+  bool    ok  = std::fread(&ntb, 4, 1, f) == 1;
+  int     tbs_ok = 0, tx = 0, mismatches = 0;
+  for (int i = 0; ok && i < ntb; ++i) {
+    int32_t h[8]; // tbs bytes, bg, qm, layers, nref, G, C, transmissions
+    ok = std::fread(h, 4, 8, f) == 8;
+    if (!ok) {
+      break;
+    }
+    std::vector<uint8_t> tb_a(h[0]), tb_b(h[0]);
+    for (int x = 0; ok && x < h[7]; ++x, ++tx) {
+      int32_t rv_nd[2];
+      ok = std::fread(rv_nd, 4, 2, f) == 2;
+      std::vector<log_likelihood_ratio> llrs(h[5]);
+      ok = ok && std::fread(llrs.data(), 1, h[5], f) == static_cast<size_t>(h[5]);
+      if (!ok) {
+        break;
+      }
+      pusch_decoder::configuration dc;
+      dc.base_graph          = h[1] == 1 ? ldpc_base_graph_type::BG1 : ldpc_base_graph_type::BG2;
+      dc.rv                  = static_cast<unsigned>(rv_nd[0]);
+      dc.mod                 = h[2] == 2 ? modulation_scheme::QPSK
+                                         : (h[2] == 4 ? modulation_scheme::QAM16
+                                                      : (h[2] == 6 ? modulation_scheme::QAM64 : modulation_scheme::QAM256));
+      dc.Nref                = static_cast<unsigned>(h[4]);
+      dc.nof_layers          = static_cast<unsigned>(h[3]);
+      dc.nof_ldpc_iterations = 6;
+      dc.use_early_stop      = true;
+      dc.new_data            = rv_nd[1] != 0;
+      const slot_point sl(1, static_cast<uint32_t>(2 * i + x));
+      unique_rx_buffer ra = ref_pool->get_pool().reserve(sl, trx_buffer_identifier(to_rnti(0x4601 + i), 0), h[6], dc.new_data);
+      unique_rx_buffer rb = b200_pool->get_pool().reserve(sl, trx_buffer_identifier(to_rnti(0x4601 + i), 0), h[6], dc.new_data);
+      if (!ra.is_valid() || !rb.is_valid()) {
+        ok = false;
+        break;
+      }
+      rx_buffer&   buf_a = *ra;
+      rx_buffer&   buf_b = *rb;
+      sch_notifier na, nb;
+      pusch_decoder_buffer& ia = ref_dec.new_data(tb_a, std::move(ra), na, dc);
+      pusch_decoder_buffer& ib = b200_dec->new_data(tb_b, std::move(rb), nb, dc);
+      ref_dec.set_nof_softbits(units::bits(h[5]));
+      b200_dec->set_nof_softbits(units::bits(h[5]));
+      for (unsigned off = 0; off < static_cast<unsigned>(h[5]); off += 4096) {
+        const unsigned                   n   = std::min(4096U, static_cast<unsigned>(h[5]) - off);
+        span<const log_likelihood_ratio> blk = span<const log_likelihood_ratio>(llrs).subspan(off, n);
+        span<log_likelihood_ratio>       va  = ia.get_next_block_view(n);
+        std::copy(blk.begin(), blk.end(), va.begin());
+        ia.on_new_softbits(va);
+        ib.on_new_softbits(blk);
+      }
+      ia.on_end_softbits();
+      ib.on_end_softbits();
+      bool same = na.called && nb.called && na.result.tb_crc_ok == nb.result.tb_crc_ok &&
+                  na.result.nof_codeblocks_total == nb.result.nof_codeblocks_total &&
+                  na.result.ldpc_decoder_stats.get_nof_observations() ==
+                      nb.result.ldpc_decoder_stats.get_nof_observations() &&
+                  na.result.ldpc_decoder_stats.get_min() == nb.result.ldpc_decoder_stats.get_min() &&
+                  na.result.ldpc_decoder_stats.get_max() == nb.result.ldpc_decoder_stats.get_max() &&
+                  na.result.ldpc_decoder_stats.get_mean() == nb.result.ldpc_decoder_stats.get_mean();
+      if (same && na.result.tb_crc_ok) {
+        same = tb_a == tb_b;
+        ++tbs_ok;
+      }
+      // The buffers: CRC flags and soft bits (unlocked buffers keep them for the retransmission).
+      if (same && !na.result.tb_crc_ok) {
+        span<bool> ca = buf_a.get_codeblocks_crc(), cb = buf_b.get_codeblocks_crc();
+        same = std::equal(ca.begin(), ca.end(), cb.begin());
+        const unsigned z = 384, n_cb = (h[1] == 1 ? 66U : 50U);
+        (void)z;
+        for (unsigned c = 0; same && c < static_cast<unsigned>(h[6]); ++c) {
+          const unsigned n = buf_a.get_codeblock_soft_bits(c, 0).size();
+          (void)n_cb;
+          span<log_likelihood_ratio> sa = buf_a.get_codeblock_soft_bits(c, n), sb = buf_b.get_codeblock_soft_bits(c, n);
+          same = std::equal(sa.begin(), sa.end(), sb.begin());
+        }
+      }
+      mismatches += same ? 0 : 1;
+    }
+  }
+  std::fclose(f);
+  char detail[200];
+  std::snprintf(detail, sizeof(detail), "%d transport blocks, %d transmissions, %d decoded, %d mismatches%s", ntb, tx,
+                tbs_ok, mismatches, ok ? "" : " (input error)");
+  report("pusch_decoder", ok && mismatches == 0 && tx > 0, detail);
+}
+
+int main(int argc, char** argv)
 {
   b200::device_config dev;
   dev.device         = 0;
@@ -323,6 +672,12 @@ int main()
   check_crc(dev);
   check_demapper(dev);
   check_equalizer(dev);
+  check_port_estimator(dev);
+  if (argc > 1) {
+    b200::device_config dec_dev = dev;
+    dec_dev.max_codeblocks      = 160;
+    check_pusch_decoder(dec_dev, argv[1]);
+  }
   std::printf("%s\n", failures == 0 ? "ALL OK" : "FAILED");
   return failures == 0 ? 0 : 1;
 }
