@@ -271,6 +271,17 @@ typedef struct pg_sch_result {
 int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* llrs,
                              size_t nof_llrs_total, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
 
+/* pg_sch_decode_batch_host with the codeword soft bits already in device memory (llrs, a device
+ * buffer of nof_llrs_total soft bits; the TBs, results and tb_out are host memory): the
+ * transport-block decode of pusch_resident_codeblock_decoder::decode_resident_softbits
+ * (include/ocudu/phy/upper/channel_processors/pusch/pusch_resident_codeblock_decoder.h:126-137).
+ * c_init (host, one per TB, may be NULL): the soft bits are still scrambled and are descrambled on the
+ * device with the Gold sequence of that initialisation from position bit_offset[t] (NULL: 0) -
+ * TS 38.211 Section 6.3.1.1; the caller's buffer is left unchanged. */
+int pg_sch_decode_batch_resident(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* llrs,
+                                 size_t nof_llrs_total, const uint32_t* c_init, const uint32_t* bit_offset,
+                                 uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
+
 /* ---------------------------------------------------------------------------------------- */
 /* Equalisation and soft demapping                                                           */
 

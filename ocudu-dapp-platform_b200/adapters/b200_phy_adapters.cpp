@@ -539,6 +539,186 @@ void pusch_decoder_b200::on_end_softbits()
 }
 
 // ---------------------------------------------------------------------------------------------
+// pusch_resident_codeblock_decoder
+
+std::vector<pusch_resident_codeblock_decoder::codeblock_result>
+pusch_resident_codeblock_decoder_b200::decode_batch(span<const described_rx_codeblock> codeblock_llrs,
+                                                    span<bit_buffer>                   cb_data_buffers,
+                                                    span<span<log_likelihood_ratio>>   rm_buffers,
+                                                    bool                               new_data,
+                                                    crc_generator_poly                 crc_poly,
+                                                    bool                               use_early_stop,
+                                                    unsigned                           nof_ldpc_iterations)
+{
+  const size_t n = codeblock_llrs.size();
+  report_fatal_error_if_not(cb_data_buffers.size() == n && rm_buffers.size() == n,
+                            "pusch_b200: inconsistent batch sizes.");
+  std::vector<codeblock_result> out(n);
+  if (n == 0) {
+    return out;
+  }
+  // Rate dematching of the batch into the caller's soft buffers (pusch_codeblock_decoder::rate_match).
+  std::vector<pg_rm_cb>   rm(n);
+  std::vector<int8_t>     in;
+  std::vector<uint32_t>   buf_off(n);
+  size_t                  total = 0;
+  for (size_t i = 0; i != n; ++i) {
+    const codeblock_metadata& md = codeblock_llrs[i].second;
+    span<const log_likelihood_ratio> e = codeblock_llrs[i].first;
+    rm[i]            = {static_cast<uint32_t>(in.size()), static_cast<uint32_t>(e.size()), static_cast<uint32_t>(total),
+                        md.tb_common.Nref, static_cast<uint16_t>(md.tb_common.lifting_size),
+                        static_cast<uint16_t>(md.cb_specific.nof_filler_bits),
+                        static_cast<uint8_t>(to_pg_base_graph(md.tb_common.base_graph)),
+                        static_cast<uint8_t>(md.tb_common.rv), static_cast<uint8_t>(get_bits_per_symbol(md.tb_common.mod)),
+                        static_cast<uint8_t>(new_data ? 1 : 0)};
+    const int8_t* p = raw(e);
+    in.insert(in.end(), p, p + e.size());
+    buf_off[i] = static_cast<uint32_t>(total);
+    total += (rm_buffers[i].size() + 15) & ~static_cast<size_t>(15);
+  }
+  buffers.assign(total, 0);
+  for (size_t i = 0; i != n; ++i) {
+    std::memcpy(buffers.data() + buf_off[i], rm_buffers[i].data(), rm_buffers[i].size());
+  }
+  if (in.empty()) {
+    in.push_back(0);
+  }
+  ctx.check(pg_rate_dematch_batch_host(ctx.get(), rm.data(), static_cast<int>(n), in.data(), in.size(), buffers.data(),
+                                       buffers.size()),
+            "pg_rate_dematch_batch_host");
+  for (size_t i = 0; i != n; ++i) {
+    std::memcpy(rm_buffers[i].data(), buffers.data() + buf_off[i], rm_buffers[i].size());
+  }
+  // LDPC decoding with CRC early stop, or syndrome check then CRC (pusch_codeblock_decoder::decode).
+  const uint32_t          poly = to_pg_poly(crc_poly);
+  std::vector<pg_ldpc_cb> ldpc(n);
+  std::vector<uint32_t>   out_off(n);
+  size_t                  bytes = 0;
+  for (size_t i = 0; i != n; ++i) {
+    const codeblock_metadata& md = codeblock_llrs[i].second;
+    const int                 bg = to_pg_base_graph(md.tb_common.base_graph);
+    const unsigned            z  = static_cast<unsigned>(md.tb_common.lifting_size);
+    ldpc[i]                      = {buf_off[i], static_cast<uint32_t>(rm_buffers[i].size()), static_cast<uint32_t>(bytes),
+                                    static_cast<uint16_t>(z), static_cast<uint16_t>(md.cb_specific.nof_filler_bits),
+                                    static_cast<uint8_t>(bg), static_cast<uint8_t>(use_early_stop ? poly : PG_CRC_NONE),
+                                    static_cast<uint8_t>(nof_ldpc_iterations), 0};
+    out_off[i] = static_cast<uint32_t>(bytes);
+    bytes += static_cast<size_t>(pg_ldpc_output_bytes(bg, static_cast<int>(z)));
+  }
+  bits.assign(bytes, 0);
+  std::vector<int32_t> iters(n, 0);
+  ctx.check(pg_ldpc_decode_batch_host(ctx.get(), ldpc.data(), static_cast<int>(n), buffers.data(), buffers.size(),
+                                      bits.data(), bits.size(), iters.data()),
+            "pg_ldpc_decode_batch_host");
+  for (size_t i = 0; i != n; ++i) {
+    const codeblock_metadata& md = codeblock_llrs[i].second;
+    const unsigned            k  = (to_pg_base_graph(md.tb_common.base_graph) == 1 ? 22U : 10U) *
+                       static_cast<unsigned>(md.tb_common.lifting_size);
+    const unsigned obytes = static_cast<unsigned>(
+        pg_ldpc_output_bytes(to_pg_base_graph(md.tb_common.base_graph), static_cast<int>(md.tb_common.lifting_size)));
+    int it = iters[i];
+    if (!use_early_stop && it > 0) {
+      pg_crc_item item = {0, k - md.cb_specific.nof_filler_bits, poly};
+      uint32_t    crc  = 1;
+      ctx.check(pg_crc_calculate_host(ctx.get(), &item, 1, bits.data() + out_off[i], obytes, &crc),
+                "pg_crc_calculate_host");
+      it = crc == 0 ? static_cast<int>(nof_ldpc_iterations) : 0;
+    }
+    span<uint8_t> dst = cb_data_buffers[i].get_buffer();
+    std::memcpy(dst.data(), bits.data() + out_off[i], std::min<size_t>(dst.size(), obytes));
+    out[i].crc_ok         = it > 0;
+    out[i].nof_iterations = it > 0 ? static_cast<unsigned>(it) : nof_ldpc_iterations;
+  }
+  timing.nof_cbs = static_cast<unsigned>(n);
+  return out;
+}
+
+void pusch_resident_codeblock_decoder_b200::rate_dematch_only(span<const log_likelihood_ratio> cb_llrs,
+                                                              span<log_likelihood_ratio>       rm_buffer,
+                                                              bool                             new_data,
+                                                              const codeblock_metadata&        md)
+{
+  pg_rm_cb d = {0, static_cast<uint32_t>(cb_llrs.size()), 0, md.tb_common.Nref,
+                static_cast<uint16_t>(md.tb_common.lifting_size), static_cast<uint16_t>(md.cb_specific.nof_filler_bits),
+                static_cast<uint8_t>(to_pg_base_graph(md.tb_common.base_graph)), static_cast<uint8_t>(md.tb_common.rv),
+                static_cast<uint8_t>(get_bits_per_symbol(md.tb_common.mod)), static_cast<uint8_t>(new_data ? 1 : 0)};
+  ctx.check(pg_rate_dematch_batch_host(ctx.get(), &d, 1, raw(cb_llrs), cb_llrs.size(), raw(rm_buffer), rm_buffer.size()),
+            "pg_rate_dematch_batch_host");
+}
+
+pusch_resident_codeblock_decoder::tb_decode_result pusch_resident_codeblock_decoder_b200::decode_resident_softbits(
+    void*                                                resident_llrs,
+    size_t                                               nof_softbits,
+    const scrambling_config*                             scrambling_cfg,
+    const codeblock_metadata::tb_common_metadata&        tb_common,
+    span<const codeblock_metadata::cb_specific_metadata> cb_specific,
+    span<uint8_t>                                        tb_output,
+    crc_generator_poly                                   cb_crc_poly,
+    unsigned                                             nof_ldpc_iterations,
+    void*                                                execution_context,
+    int                                                  buffer_index)
+{
+  (void)cb_crc_poly; // implied by the transport block size and the codeblock count
+  (void)execution_context;
+  (void)buffer_index;
+  const unsigned qm = get_bits_per_symbol(tb_common.mod);
+  report_fatal_error_if_not(qm > 0 && nof_softbits % qm == 0 && !cb_specific.empty(),
+                            "pusch_b200: invalid resident codeword.");
+  // The layer count is not part of the metadata: take the one whose TS 38.212 split reproduces the
+  // codeblocks' rate-matching lengths.
+  const unsigned tbs = static_cast<unsigned>(tb_output.size()) * 8;
+  const int      bg  = to_pg_base_graph(tb_common.base_graph);
+  unsigned       nl  = 0;
+  for (unsigned l = 1; l <= 4 && nl == 0; ++l) {
+    pg_sch_segmentation sg = {};
+    if ((nof_softbits / qm) % l != 0 ||
+        pg_sch_segment(tbs, bg, static_cast<int>(qm), static_cast<int>(l), static_cast<uint32_t>(nof_softbits / qm), &sg) !=
+            PG_OK ||
+        sg.nof_cbs != cb_specific.size()) {
+      continue;
+    }
+    bool match = true;
+    for (unsigned c = 0; c != sg.nof_cbs; ++c) {
+      match = match && cb_specific[c].rm_length == (c < sg.nof_short_cbs ? sg.e_short : sg.e_long);
+    }
+    nl = match ? l : 0;
+  }
+  report_fatal_error_if_not(nl != 0, "pusch_b200: codeblock lengths match no layer count.");
+  pg_sch_tb tb      = {};
+  tb.llr_offset     = 0;
+  tb.nof_ch_symbols = static_cast<uint32_t>(nof_softbits / qm);
+  tb.tbs_bits       = tbs;
+  tb.tb_out_offset  = 0;
+  tb.nref           = tb_common.Nref;
+  tb.base_graph     = static_cast<uint8_t>(bg);
+  tb.modulation_order = static_cast<uint8_t>(qm);
+  tb.nof_layers       = static_cast<uint8_t>(nl);
+  tb.rv               = static_cast<uint8_t>(tb_common.rv);
+  tb.max_iterations   = static_cast<uint8_t>(nof_ldpc_iterations);
+  uint32_t c_init = 0, offset = 0;
+  if (scrambling_cfg != nullptr) {
+    // TS 38.211 Section 6.3.1.1 (PUSCH): c_init = n_RNTI 2^15 + n_ID.
+    c_init = (static_cast<uint32_t>(scrambling_cfg->n_rnti) << 15) + (static_cast<uint32_t>(scrambling_cfg->q) << 14) +
+             scrambling_cfg->n_id;
+    offset = scrambling_cfg->bit_offset;
+  }
+  pg_sch_result r = {};
+  ctx.check(pg_sch_decode_batch_resident(ctx.get(), &tb, 1, static_cast<const int8_t*>(resident_llrs), nof_softbits,
+                                         scrambling_cfg != nullptr ? &c_init : nullptr,
+                                         scrambling_cfg != nullptr ? &offset : nullptr, tb_output.data(),
+                                         tb_output.size(), &r),
+            "pg_sch_decode_batch_resident");
+  timing.nof_cbs = r.nof_cbs;
+  return {r.tb_crc_ok != 0, r.nof_cbs_crc_ok == r.nof_cbs, static_cast<unsigned>(std::lround(r.mean_iterations))};
+}
+
+void pusch_resident_codeblock_decoder_b200::set_ldpc_decoder_algorithm(const std::string& algorithm)
+{
+  report_fatal_error_if_not(algorithm.empty() || algorithm == "layered_min_sum",
+                            "pusch_b200: LDPC algorithm '{}' is not supported.", algorithm);
+}
+
+// ---------------------------------------------------------------------------------------------
 // Factories
 
 namespace {

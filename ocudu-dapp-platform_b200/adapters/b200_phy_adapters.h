@@ -22,6 +22,7 @@
 #include "ocudu/phy/upper/channel_processors/pusch/factories.h"
 #include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder.h"
 #include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_buffer.h"
+#include "ocudu/phy/upper/channel_processors/pusch/pusch_resident_codeblock_decoder.h"
 #include "ocudu/phy/upper/signal_processors/channel_estimator/factories.h"
 #include "ocudu/phy/upper/signal_processors/channel_estimator/port_channel_estimator.h"
 #include "ocudu/phy/upper/unique_rx_buffer.h"
@@ -225,6 +226,59 @@ private:
   std::vector<unsigned> cb_stats;
   std::vector<int8_t>   cb_buffers;
   std::vector<uint8_t>  cb_bits;
+};
+
+/// pusch_resident_codeblock_decoder (include/ocudu/phy/upper/channel_processors/pusch/
+/// pusch_resident_codeblock_decoder.h:61-150), the batch hook of pusch_decoder_impl
+/// (lib/phy/upper/channel_processors/pusch/pusch_decoder_impl.cpp:492-600): decode_batch dematches
+/// every codeblock into its host soft buffer and decodes them in one GPU batch each;
+/// decode_resident_softbits decodes a transport block whose soft bits are already in device memory
+/// (int8 LLRs, descrambled on the device when a scrambling configuration is given) through
+/// pg_sch_decode_batch_resident. The dematched soft bits of a resident decode stay in the library's
+/// scratch, so export_resident_softbits reports that none can be exported (the interface's contract
+/// for that case: the caller resets the HARQ buffers).
+class pusch_resident_codeblock_decoder_b200 : public pusch_resident_codeblock_decoder
+{
+public:
+  explicit pusch_resident_codeblock_decoder_b200(const device_config& cfg) : ctx(cfg) {}
+
+  std::vector<codeblock_result> decode_batch(span<const described_rx_codeblock> codeblock_llrs,
+                                             span<bit_buffer>                   cb_data_buffers,
+                                             span<span<log_likelihood_ratio>>   rm_buffers,
+                                             bool                               new_data,
+                                             crc_generator_poly                 crc_poly,
+                                             bool                               use_early_stop,
+                                             unsigned                           nof_ldpc_iterations) override;
+  void rate_dematch_only(span<const log_likelihood_ratio> cb_llrs,
+                         span<log_likelihood_ratio>       rm_buffer,
+                         bool                             new_data,
+                         const codeblock_metadata&        metadata) override;
+  bool export_resident_softbits(span<span<log_likelihood_ratio>> rm_buffers) override { return false; }
+  tb_decode_result decode_resident_softbits(void*                                                resident_llrs,
+                                            size_t                                               nof_softbits,
+                                            const scrambling_config*                             scrambling_cfg,
+                                            const codeblock_metadata::tb_common_metadata&        tb_common,
+                                            span<const codeblock_metadata::cb_specific_metadata> cb_specific,
+                                            span<uint8_t>                                        tb_output,
+                                            crc_generator_poly                                   cb_crc_poly,
+                                            unsigned                                             nof_ldpc_iterations,
+                                            void*                                                execution_context,
+                                            int                                                  buffer_index) override;
+  const pusch_resident_codeblock_decoder_timing_stats& get_last_timing_stats() const override { return timing; }
+  void set_demod_timing(float grid_staging_us, float demod_sync_us) override
+  {
+    timing.grid_staging_us = grid_staging_us;
+    timing.demod_sync_us   = demod_sync_us;
+  }
+  void set_timing_enabled(bool enable) override { timing.timing_enabled = enable; }
+  /// "" or "layered_min_sum" (the only algorithm: the reference's layered normalised min-sum).
+  void set_ldpc_decoder_algorithm(const std::string& algorithm) override;
+
+private:
+  context_handle                                 ctx;
+  pusch_resident_codeblock_decoder_timing_stats  timing;
+  std::vector<int8_t>                            buffers;
+  std::vector<uint8_t>                           bits;
 };
 
 /// Factories in the shape of the reference's *_sw factories.

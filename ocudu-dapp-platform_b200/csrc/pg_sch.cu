@@ -1,10 +1,34 @@
 // C ABI of the rate-dematching, CRC, TB-assembly and TB-decoding entry points, and the UL-SCH
 // segmentation (host code).
 #include "pg_internal.h"
+#include "pg_device.cuh"
 
 #include <algorithm>
 #include <cstring>
 #include <vector>
+
+namespace {
+
+// Descrambling of n soft bits: out[i] = -in[i] where c(bit_offset + i) = 1 (TS 38.211 Section 6.3.1.1,
+// the Gold sequence of Section 5.2.1 with initialisation c_init), one 32-bit sequence word per thread.
+__global__ void descramble_kernel(const int8_t* __restrict__ in, int8_t* __restrict__ out, uint32_t n, uint32_t c_init,
+                                  uint32_t bit_offset, const uint32_t* __restrict__ gold, uint32_t gold_words)
+{
+  const uint32_t words = (n + 31) / 32;
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+    const uint32_t seq = pg::gold_word(gold, gold_words, c_init, bit_offset + 32u * w);
+#pragma unroll 4
+    for (uint32_t b = 0; b < 32; ++b) {
+      const uint32_t k = 32u * w + b;
+      if (k < n) {
+        const int v = in[k];
+        out[k]      = (int8_t)(((seq >> b) & 1u) ? -v : v);
+      }
+    }
+  }
+}
+
+} // namespace
 
 namespace pg {
 
@@ -284,6 +308,48 @@ int pg_sch_decode_batch_host(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs,
   }
   return sch_decode_device_llrs(ctx, tbs, nof_tbs, static_cast<const int8_t*>(ctx->scratch_a), nof_llrs_total, tb_out,
                                 tb_out_len, results);
+}
+
+int pg_sch_decode_batch_resident(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* llrs,
+                                 size_t nof_llrs_total, const uint32_t* c_init, const uint32_t* bit_offset,
+                                 uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results)
+{
+  if (ctx == nullptr || nof_tbs < 0 || (nof_tbs > 0 && (tbs == nullptr || results == nullptr || llrs == nullptr))) {
+    return ctx ? set_error(ctx, PG_ERR_INVALID, "invalid arguments") : PG_ERR_INVALID;
+  }
+  if (nof_tbs == 0) {
+    return PG_OK;
+  }
+  if (int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice")) {
+    return rc;
+  }
+  const int8_t* d_llrs = llrs;
+  if (c_init != nullptr) {
+    // Descrambled copy of every TB's soft bits (the caller's buffer stays untouched).
+    for (int t = 0; t < nof_tbs; ++t) {
+      const uint64_t g   = (uint64_t)tbs[t].nof_ch_symbols * tbs[t].modulation_order;
+      const uint64_t off = bit_offset != nullptr ? bit_offset[t] : 0;
+      if (tbs[t].llr_offset + g > nof_llrs_total || off + g + 64 > 32ull * (kGoldWords - 2)) {
+        return set_error(ctx, PG_ERR_INVALID, "transport block " + std::to_string(t) + ": soft bits out of range");
+      }
+    }
+    if (int rc = ensure_scratch(ctx, &ctx->scratch_a, &ctx->scratch_a_cap, std::max<size_t>(nof_llrs_total, 256),
+                                "cudaMalloc(descrambled llrs)")) {
+      return rc;
+    }
+    int8_t* d = static_cast<int8_t*>(ctx->scratch_a);
+    for (int t = 0; t < nof_tbs; ++t) {
+      const uint32_t g = tbs[t].nof_ch_symbols * tbs[t].modulation_order;
+      descramble_kernel<<<(g / 32 + 255) / 256 + 1, 256, 0, ctx->stream>>>(
+          llrs + tbs[t].llr_offset, d + tbs[t].llr_offset, g, c_init[t], bit_offset != nullptr ? bit_offset[t] : 0,
+          ctx->dev.gold, kGoldWords);
+      if (int rc = check_cuda(ctx, cudaGetLastError(), "descramble_kernel launch")) {
+        return rc;
+      }
+    }
+    d_llrs = d;
+  }
+  return sch_decode_device_llrs(ctx, tbs, nof_tbs, d_llrs, nof_llrs_total, tb_out, tb_out_len, results);
 }
 
 } // extern "C"

@@ -167,3 +167,37 @@ class PuschDecoder:
                                      float(r.mean_iterations), int(r.max_iterations_run),
                                      out[o:o + t.tbs_bits // 8].copy() if r.tb_crc_ok else None))
         return results
+
+    def decode_resident(self, tbs: Sequence[SchTransportBlock], offsets, llrs_ptr, nof_llrs, c_init=None,
+                        bit_offset=None) -> List[SchResult]:
+        """pg_sch_decode_batch_resident: the TBs' soft bits are already in device memory (llrs_ptr,
+        TB i from offsets[i]; the llrs fields of `tbs` only give their lengths). c_init: per TB, the
+        soft bits are still scrambled with that initialisation (from bit_offset[i], default 0)."""
+        n = len(tbs)
+        if n == 0:
+            return []
+        descs = (PgSchTb * n)()
+        out_off = 0
+        for i, t in enumerate(tbs):
+            qm = t.modulation_order
+            d = descs[i]
+            d.llr_offset, d.nof_ch_symbols, d.tbs_bits, d.tb_out_offset, d.nref = (
+                int(offsets[i]), t.llrs.size // qm, t.tbs_bits, out_off, t.nref)
+            d.base_graph, d.modulation_order, d.nof_layers, d.rv, d.max_iterations = (
+                t.base_graph, qm, t.nof_layers, t.rv, t.max_iterations)
+            out_off += t.tbs_bits // 8
+        ci = None if c_init is None else (ctypes.c_uint32 * n)(*[int(x) for x in c_init])
+        bo = None if bit_offset is None else (ctypes.c_uint32 * n)(*[int(x) for x in bit_offset])
+        out = np.zeros(max(out_off, 1), np.uint8)
+        res = (PgSchResult * n)()
+        self.ctx.check(self.lib.pg_sch_decode_batch_resident(self.ctx.handle, ctypes.addressof(descs), n, llrs_ptr,
+                                                             nof_llrs, ci, bo, out.ctypes.data_as(ctypes.c_void_p),
+                                                             out.size, ctypes.addressof(res)))
+        results = []
+        for i, t in enumerate(tbs):
+            r = res[i]
+            o = descs[i].tb_out_offset
+            results.append(SchResult(bool(r.tb_crc_ok), int(r.nof_cbs), int(r.nof_cbs_crc_ok),
+                                     float(r.mean_iterations), int(r.max_iterations_run),
+                                     out[o:o + t.tbs_bits // 8].copy() if r.tb_crc_ok else None))
+        return results

@@ -13,6 +13,8 @@
 //                        time alignment within one T_c
 //   pusch_decoder        (with a codeword file, argv[1]) bit-exact TBs, CRC flags, codeblock counts,
 //                        iteration statistics and rx-buffer soft bits over two transmissions (HARQ)
+//   resident_decoder     (same file) pusch_resident_codeblock_decoder::decode_batch bit-exact with the
+//                        reference's codeblock decoder: CRC verdicts, iterations, bits, soft buffers
 // Test infrastructure: it links the reference's compiled code (oracle/_ref).
 #include "../../ocudu-dapp-platform_b200/adapters/b200_phy_adapters.h"
 
@@ -662,6 +664,101 @@ void check_pusch_decoder(const b200::device_config& dev, const char* path)
   report("pusch_decoder", ok && mismatches == 0 && tx > 0, detail);
 }
 
+// pusch_resident_codeblock_decoder::decode_batch against the reference's pusch_codeblock_decoder on
+// the codeblocks of the same codewords (segmented by the reference's ldpc_segmenter_rx): CRC
+// verdicts, iteration counts, decoded bits and the soft buffers, over both transmissions.
+void check_resident_decoder(const b200::device_config& dev, const char* path)
+{
+  FILE* f = std::fopen(path, "rb");
+  if (f == nullptr) {
+    report("resident_decoder", false, "cannot open the codeword file");
+    return;
+  }
+  auto                             crcf = create_crc_calculator_factory_sw("auto");
+  pusch_codeblock_decoder::sch_crc cb_crcs{crcf->create(crc_generator_poly::CRC16),
+                                           crcf->create(crc_generator_poly::CRC24A),
+                                           crcf->create(crc_generator_poly::CRC24B)};
+  ldpc_decoder_factory::ldpc_decoder_factory_configuration fcfg = {false, false};
+  pusch_codeblock_decoder ref_cb(create_ldpc_rate_dematcher_factory_sw("auto")->create(),
+                                 create_ldpc_decoder_factory_sw("auto", fcfg)->create(), cb_crcs);
+  b200::pusch_resident_codeblock_decoder_b200 res(dev);
+  auto                                        seg = create_ldpc_segmenter_rx_factory_sw()->create();
+  int32_t                                     ntb = 0;
+  bool                                        ok  = std::fread(&ntb, 4, 1, f) == 1;
+  int                                         cbs = 0, decoded = 0, mismatches = 0;
+  for (int i = 0; ok && i < ntb; ++i) {
+    int32_t h[8];
+    ok = std::fread(h, 4, 8, f) == 8;
+    if (!ok) {
+      break;
+    }
+    const unsigned                                 N = 0;
+    std::vector<std::vector<log_likelihood_ratio>> ref_bufs, b200_bufs;
+    for (int x = 0; ok && x < h[7]; ++x) {
+      int32_t rv_nd[2];
+      ok = std::fread(rv_nd, 4, 2, f) == 2;
+      std::vector<log_likelihood_ratio> llrs(h[5]);
+      ok = ok && std::fread(llrs.data(), 1, h[5], f) == static_cast<size_t>(h[5]);
+      if (!ok) {
+        break;
+      }
+      segmenter_config sc;
+      sc.transport_block_size = units::bytes(h[0]);
+      sc.base_graph           = h[1] == 1 ? ldpc_base_graph_type::BG1 : ldpc_base_graph_type::BG2;
+      sc.rv                   = static_cast<unsigned>(rv_nd[0]);
+      sc.mod                  = h[2] == 2 ? modulation_scheme::QPSK
+                                          : (h[2] == 4 ? modulation_scheme::QAM16
+                                                       : (h[2] == 6 ? modulation_scheme::QAM64 : modulation_scheme::QAM256));
+      sc.Nref                 = static_cast<unsigned>(h[4]);
+      sc.nof_layers           = static_cast<unsigned>(h[3]);
+      sc.nof_ch_symbols       = static_cast<unsigned>(h[5]) / static_cast<unsigned>(h[2]);
+      static_vector<described_rx_codeblock, MAX_NOF_SEGMENTS> cbl;
+      seg->segment(cbl, llrs, sc);
+      const unsigned C       = static_cast<unsigned>(cbl.size());
+      const bool     newdata = rv_nd[1] != 0;
+      const unsigned n_full  = cbl[0].second.cb_specific.full_length;
+      if (newdata) {
+        ref_bufs.assign(C, std::vector<log_likelihood_ratio>(n_full));
+        b200_bufs.assign(C, std::vector<log_likelihood_ratio>(n_full));
+      }
+      const crc_generator_poly poly =
+          C > 1 ? crc_generator_poly::CRC24B : (8 * h[0] <= 3824 ? crc_generator_poly::CRC16 : crc_generator_poly::CRC24A);
+      const unsigned                      k = n_full / (h[1] == 1 ? 3 : 5);
+      std::vector<dynamic_bit_buffer>     ref_bits, b200_bits;
+      std::vector<bit_buffer>             b200_views;
+      std::vector<span<log_likelihood_ratio>> b200_rm;
+      for (unsigned c = 0; c != C; ++c) {
+        ref_bits.emplace_back(k);
+        b200_bits.emplace_back(k);
+      }
+      for (unsigned c = 0; c != C; ++c) {
+        b200_views.push_back(b200_bits[c]);
+        b200_rm.push_back(b200_bufs[c]);
+      }
+      std::vector<pusch_resident_codeblock_decoder::codeblock_result> got =
+          res.decode_batch(span<const described_rx_codeblock>(cbl.data(), C), b200_views, b200_rm, newdata, poly, true, 6);
+      for (unsigned c = 0; c != C; ++c, ++cbs) {
+        std::optional<unsigned> want = ref_cb.decode(ref_bits[c], ref_bufs[c], cbl[c].first, newdata, poly, true, 6,
+                                                     cbl[c].second);
+        bool same = got[c].crc_ok == want.has_value() && got[c].nof_iterations == (want.has_value() ? *want : 6U) &&
+                    ref_bufs[c] == b200_bufs[c];
+        if (same && want.has_value()) {
+          same = std::equal(ref_bits[c].get_buffer().begin(), ref_bits[c].get_buffer().end(),
+                            b200_bits[c].get_buffer().begin());
+          ++decoded;
+        }
+        mismatches += same ? 0 : 1;
+      }
+      (void)N;
+    }
+  }
+  std::fclose(f);
+  char detail[200];
+  std::snprintf(detail, sizeof(detail), "%d codeblocks, %d decoded, %d mismatches%s", cbs, decoded, mismatches,
+                ok ? "" : " (input error)");
+  report("resident_decoder", ok && mismatches == 0 && cbs > 0, detail);
+}
+
 int main(int argc, char** argv)
 {
   b200::device_config dev;
@@ -677,6 +774,7 @@ int main(int argc, char** argv)
     b200::device_config dec_dev = dev;
     dec_dev.max_codeblocks      = 160;
     check_pusch_decoder(dec_dev, argv[1]);
+    check_resident_decoder(dec_dev, argv[1]);
   }
   std::printf("%s\n", failures == 0 ? "ALL OK" : "FAILED");
   return failures == 0 ? 0 : 1;

@@ -63,5 +63,5 @@ def test_adapters_match_reference_implementations(tmp_path):
     print(r.stdout)
     assert r.returncode == 0, r.stdout + r.stderr
     for iface in ("ldpc_decoder", "ldpc_rate_dematcher", "crc_calculator", "demodulation_mapper", "channel_equalizer",
-                  "port_channel_estimator", "pusch_decoder"):
+                  "port_channel_estimator", "pusch_decoder", "resident_decoder"):
         assert any(line.startswith(iface) and " OK " in line for line in r.stdout.splitlines()), iface

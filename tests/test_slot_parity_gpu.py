@@ -171,6 +171,27 @@ def test_back_half_bit_exact_on_reference_llrs(ctx, slot_case):
         if g.tb_crc_ok:
             assert np.array_equal(g.transport_block, tb_of(r["tb"], d))
 
+    # The same soft bits scrambled again and left in device memory: the resident entry descrambles
+    # them on the device and decodes the same TBs.
+    import torch
+    from pusch_b200 import prg
+    scrambled = llrs[:c["nllr"]].astype(np.int16).copy()
+    c_init = []
+    for d, ue in zip(c["descs"], c["ues"]):
+        g = sim.nof_ch_symbols(ue) * ue.modulation_order
+        seq = prg.scrambling(ue.rnti, ue.n_id_data, g).astype(bool)
+        seg_llr = scrambled[d.llr_offset:d.llr_offset + g]
+        seg_llr[seq] = -seg_llr[seq]
+        c_init.append((ue.rnti << 15) + ue.n_id_data)
+    d_llrs = torch.from_numpy(scrambled.astype(np.int8)).cuda()
+    res_r = PuschDecoder(ctx).decode_resident(tbs, [d.llr_offset for d in c["descs"]], d_llrs.data_ptr(), c["nllr"],
+                                              c_init=c_init)
+    for u, (g, w) in enumerate(zip(res_r, res)):
+        assert (g.tb_crc_ok, g.nof_codeblocks_crc_ok, g.mean_iterations) == (
+            w.tb_crc_ok, w.nof_codeblocks_crc_ok, w.mean_iterations), (c["name"], u)
+        if g.tb_crc_ok:
+            assert np.array_equal(g.transport_block, w.transport_block)
+
     # Per codeblock: segmentation (pg_sch_segment), the rate dematcher and the LDPC batch decoder.
     dem, dec = LdpcRateDematcher(ctx), LdpcBatchDecoder(context=ctx)
     jobs, want = [], []
