@@ -230,6 +230,88 @@ def int_peak(dev):
     return None, None
 
 
+SUB_CONFIGS = {
+    "c1_20mhz_single_ue": ("Plain single-UE slot: 20 MHz / 30 kHz, 51 PRB, DM-RS symbol 2, 1 layer, 2 rx, QPSK "
+                           "(MCS table 1 index 5, TBS 5888), flat Rayleigh, 10 dB, max 6 LDPC iterations"),
+    "c3_100mhz_full_cell": ("Plain full-cell slot: 100 MHz / 30 kHz, 273 PRB, DM-RS symbols 2 and 11, 2 layers, 4 rx, "
+                            "256QAM (MCS table 2 index 20, TBS 417976, 50 codeblocks), exponential PDP (100 ns RMS, "
+                            "8 taps), 25 dB, max 6 LDPC iterations"),
+}
+
+
+def sub_config_lines(ctx, seed, steps, warmup, with_cpu):
+    """The two single-slot configurations as sub-lines of the PUSCH line: one slot plan each (plain
+    estimator, CUDA graph), device time per slot with CUDA events (L2 flushed between slots), decoded
+    Mbit/s and slots/s; with the CPU baseline, the reference's CPU receive path on one thread on the
+    same slot (Mbit/s) and whether its per-UE CRC flags, mean iterations and TBs equal the plan's."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from pusch_b200 import sim
+    from pusch_b200._native import PgSchResult
+    from pusch_b200.pusch import PuschSlotPlan, results_from
+
+    out = {}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    for name, slot in (("c1_20mhz_single_ue", sim.single_ue_slot(seed=seed)),
+                       ("c3_100mhz_full_cell", sim.full_cell_slot(seed=seed))):
+        plan = PuschSlotPlan(ctx, [slot], max_iterations=MAX_ITER, graph=True)
+        n = plan.n
+        d_grid = torch.from_numpy(plan.grid.view(np.int32)).cuda()
+        d_tb = torch.zeros(max(plan.tb_bytes, 1), dtype=torch.uint8, device="cuda")
+        d_res = torch.zeros(n * ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
+        plan.autotune(d_grid.data_ptr(), reps=3)
+        with torch.cuda.stream(stream):
+            for _ in range(max(warmup, 3)):
+                flush.fill_(1)
+                plan.execute_device(d_grid.data_ptr(), d_tb.data_ptr(), d_res.data_ptr(), None, stream.cuda_stream)
+            torch.cuda.synchronize()
+            ts = []
+            for k in range(steps):
+                flush.fill_(k & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                plan.execute_device(d_grid.data_ptr(), d_tb.data_ptr(), d_res.data_ptr(), None, stream.cuda_stream)
+                b.record(stream)
+                stream.synchronize()
+                ts.append(a.elapsed_time(b))
+        res_arr = (PgSchResult * n).from_buffer_copy(d_res.cpu().numpy().tobytes())
+        res = results_from(plan.descs, res_arr, None, d_tb.cpu().numpy())
+        good = [r.tb_crc_ok and bool((np.unpackbits(r.transport_block) == t).all()) for r, t in zip(res, slot.truth)]
+        bits = int(sum(u.tbs_bits for u, g in zip(plan.ues, good) if g))
+        ms = statistics.mean(ts)
+        line = {"workload": SUB_CONFIGS[name], "value": round(bits / (ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
+                "slots_per_s": round(1e3 / ms, 1), "ms_per_slot": round(ms, 4), "codeblocks": int(plan.info.nof_codeblocks),
+                "bler": round(1.0 - sum(good) / n, 4), "estimator": "plain", "launch_shapes": plan.tuning().as_dict()}
+        if with_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            from oracle import Ref  # CPU baseline and parity flags only
+            ref = Ref()
+            descs = plan.descs
+            r = ref.pusch_decode_detail(descs, plan.grid, plan.tb_bytes, int(plan.info.nof_llrs), 1)
+            same = all(g.tb_crc_ok == bool(o) and g.mean_iterations == float(it) and
+                       (not g.tb_crc_ok or np.array_equal(g.transport_block,
+                                                          r["tb"][d.tb_out_offset:d.tb_out_offset + d.tbs_bits // 8]))
+                       for g, o, it, d in zip(res, r["ok"], r["mean_iters"], descs))
+            total, passes = 0.0, 0
+            while total < 2.0 or passes < 3:
+                ok, _, _, dt = ref.pusch_decode_mt(descs, plan.grid, plan.tb_bytes, 1)
+                total += dt
+                passes += 1
+            ref_bits = int(sum(u.tbs_bits for u, o in zip(plan.ues, ok) if o))
+            line["reference_matches"] = bool(same)
+            line["cpu_baseline"] = {"value": round(ref_bits * passes / total / 1e6, 3), "unit": "Mbit/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": f"{passes} passes over the slot through the reference's CPU stage objects "
+                                              f"(oracle/_ref) on 1 thread, {total:.2f} s"}
+        out[name] = line
+        plan.close()
+    return out
+
+
 def reference_pusch(slots, seconds, cores, min_passes=1):
     """The reference's CPU receive path (oracle/_ref: the reference's own stage objects, one UE
     per thread) over the whole slot until `seconds` of decoding are timed. Returns (decoded bits
@@ -577,6 +659,11 @@ def run_ours_pusch(args):
         cpu = {"value": round(b * passes / dt / 1e6, 3), "unit": "Mbit/s", "cores": cores, "kind": "reference",
                "sample": f"{passes} passes over the full {N_CELLS}-cell slot ({n_ues} UEs) through the reference's "
                          f"CPU stage objects (oracle/_ref) on {cores} C++ threads, {dt:.1f} s"}
+        b1, dt1, passes1, _ = reference_pusch(slots, max(2.0, args.cpu_seconds / 4), 1)
+        cpu["one_thread"] = {"value": round(b1 * passes1 / dt1 / 1e6, 3), "unit": "Mbit/s", "cores": 1,
+                             "sample": f"{passes1} passes over the same slot on 1 thread, {dt1:.1f} s"}
+    sub_lines = sub_config_lines(ctx, args.seed + rank, max(10, min(args.steps, 100)), args.warmup,
+                                 rank == 0 and world == 1 and not args.no_cpu_baseline) if rank == 0 else None
 
     if rank == 0:
         line = {
@@ -590,6 +677,8 @@ def run_ours_pusch(args):
                     "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
                                   "plain LS + RC FIR + linear interpolation" if net is not None else
                                   "plain (LS + RC FIR + linear interpolation)")},
+            "slots_per_s": round(1e3 / ms_max * world, 1),
+            "configs": sub_lines,
             "plain_per_ue": plain, "batched_plain": batched_plain,
             "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "ofh_bfp": bfp_line, "cpu_baseline": cpu,
             "clocks": clk,

@@ -26,6 +26,7 @@ void plan(const pg_pusch_ue* ues, int n, slot_layout& L, bool assign_offsets)
     const uint32_t g = ue_codeword_bits(u);
     if (assign_offsets) {
       u.est_offset = (uint32_t)L.est_total;
+      L.llr_total  = (L.llr_total + 15) & ~(size_t)15; // 16-byte aligned codewords: vector LLR stores
       u.llr_offset = (uint32_t)L.llr_total;
     }
     L.est_total += pg_pusch_est_size(&u);

@@ -266,10 +266,41 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
   const uint32_t sh   = bit0 & 31u;
   const uint32_t cbits = sh ? ((wa >> sh) | (wb << (32 - sh))) : wa;
   int8_t* out = llr_out + ue.llr_offset + bit0;
+  // The RE's descrambled LLRs packed four to a word, stored with the widest store their address
+  // allows (codewords of plans and batched calls start on 16-byte boundaries, so an RE's NB bytes
+  // are NB-aligned for NB = 2, 4, 8, 16 and 4-aligned for 12).
+  constexpr int NB = L * QM;
+  uint32_t      wd[(NB + 3) / 4];
 #pragma unroll
-  for (int b = 0; b < L * QM; ++b) {
+  for (int k = 0; k < (NB + 3) / 4; ++k) {
+    wd[k] = 0;
+  }
+#pragma unroll
+  for (int b = 0; b < NB; ++b) {
     const int v = llr[b];
-    out[b]      = (int8_t)(((cbits >> b) & 1u) ? -v : v);
+    wd[b / 4] |= (uint32_t)(uint8_t)(int8_t)(((cbits >> b) & 1u) ? -v : v) << (8 * (b % 4));
+  }
+  const uintptr_t a = reinterpret_cast<uintptr_t>(out);
+  if (NB == 16 && (a & 15u) == 0) {
+    *reinterpret_cast<uint4*>(out) = make_uint4(wd[0], wd[1 % ((NB + 3) / 4)], wd[2 % ((NB + 3) / 4)],
+                                                wd[3 % ((NB + 3) / 4)]);
+  } else if (NB == 8 && (a & 7u) == 0) {
+    *reinterpret_cast<uint2*>(out) = make_uint2(wd[0], wd[1 % ((NB + 3) / 4)]);
+  } else if ((NB == 4 || NB == 12) && (a & 3u) == 0) {
+#pragma unroll
+    for (int k = 0; k < NB / 4; ++k) {
+      reinterpret_cast<uint32_t*>(out)[k] = wd[k];
+    }
+  } else if ((NB == 2 || NB == 6) && (a & 1u) == 0) {
+#pragma unroll
+    for (int k = 0; k < NB / 2; ++k) {
+      reinterpret_cast<uint16_t*>(out)[k] = (uint16_t)(wd[k / 2] >> (16 * (k % 2)));
+    }
+  } else {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      out[b] = (int8_t)(wd[b / 4] >> (8 * (b % 4)));
+    }
   }
 }
 

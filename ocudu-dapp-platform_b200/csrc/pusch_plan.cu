@@ -231,6 +231,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     }
     const uint32_t g = ue_codeword_bits(u);
     u.est_offset     = (uint32_t)est_total;
+    p->nof_llrs      = (p->nof_llrs + 15) & ~(size_t)15; // 16-byte aligned codewords: vector LLR stores
     u.llr_offset     = (uint32_t)p->nof_llrs;
     est_total += pg_pusch_est_size(&u);
     p->nof_llrs += g;

@@ -9,8 +9,9 @@
 // cycle of length V = N_cb - F; position p with valid index v receives the de-interleaved inputs
 // t = (v - v0) mod V, t + V, t + 2V, ... < E, summed in that order onto 0 (new data) or onto the
 // previous buffer content (soft combining). Filler positions hold +127; positions at or beyond N_cb
-// are zeroed on new data and untouched otherwise. kRmGridY CTAs per codeblock, threads stride
-// the N output positions (coalesced stores).
+// are zeroed on new data and untouched otherwise. kRmGridY CTAs per codeblock. Without repetition
+// (E <= V, the usual case) the kernel reads the input in coalesced tiles and transposes them through
+// shared memory; with repetition every output position is computed independently.
 #include "pg_internal.h"
 
 #include <algorithm>
@@ -35,10 +36,15 @@ __device__ __forceinline__ int llr_sum(int a, int b)
   return max(-120, min(120, a + b));
 }
 
+// Rows of the de-interleaver matrix per tile of the transposing path: a tile reads rows*Qm <= 2 KB
+// of input.
+constexpr int kRmTileRows = 256;
+
 __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb* __restrict__ cbs,
                                                                   const int8_t* __restrict__ in_all,
                                                                   int8_t* __restrict__ out_all)
 {
+  __shared__ int8_t tile[kRmTileRows * 8];
   const pg_rm_cb d   = cbs[blockIdx.x];
   const int      bg  = d.base_graph;
   const int      Z   = d.lifting_size;
@@ -60,8 +66,56 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   int8_t*        out = out_all + d.out_offset;
   const bool     nd  = d.new_data != 0;
 
-  // De-interleaver index src = (t mod Kq) * Qm + t div Kq with the quotient from a float
-  // reciprocal, corrected to the exact value (t < 2^24).
+  if (E <= V) {
+    // No repetition: each buffer position receives at most one input. The input, row i holding
+    // the Qm LLRs of de-interleaver column i, is read a tile of rows at a time (coalesced) and
+    // transposed through shared memory; bit plane j of rows i0.. lands on consecutive buffer
+    // positions (t = j Kq + i, valid index (v0 + t) mod V, past the fillers), so the stores are
+    // coalesced too. Positions no input reaches are written by the per-position loop below.
+    const int ntiles = (Kq + kRmTileRows - 1) / kRmTileRows;
+    for (int tl = blockIdx.y; tl < ntiles; tl += gridDim.y) {
+      const int i0   = tl * kRmTileRows;
+      const int rows = min(kRmTileRows, Kq - i0);
+      __syncthreads();
+      for (int k = threadIdx.x; k < rows * Qm; k += kRmThreads) {
+        tile[k] = in[i0 * Qm + k];
+      }
+      __syncthreads();
+      for (int k = threadIdx.x; k < rows * Qm; k += kRmThreads) {
+        const int j = k / rows;
+        const int i = k - j * rows;
+        const int t = j * Kq + i0 + i;
+        int       v = v0 + t;
+        v           = v >= V ? v - V : v;
+        const int p = v < inf ? v : v + F;
+        const int x = tile[i * Qm + j];
+        out[p]      = (int8_t)llr_sum(nd ? 0 : (int)out[p], x);
+      }
+    }
+    for (int p = blockIdx.y * kRmThreads + threadIdx.x; p < N; p += gridDim.y * kRmThreads) {
+      if (p >= inf && p < sys) {
+        out[p] = 127;
+        continue;
+      }
+      if (p >= Ncb) {
+        if (nd) {
+          out[p] = 0;
+        }
+        continue;
+      }
+      const int v = p < inf ? p : p - F;
+      int       t = v - v0;
+      t           = t < 0 ? t + V : t;
+      if (t >= E && nd) {
+        out[p] = 0;
+      }
+    }
+    return;
+  }
+
+  // Repetition (E > V): position p receives t, t + V, ... in that order. De-interleaver index
+  // src = (t mod Kq) * Qm + t div Kq with the quotient from a float reciprocal, corrected to the
+  // exact value (t < 2^24).
   const float inv_kq = 1.0f / (float)(Kq > 0 ? Kq : 1);
   for (int p = blockIdx.y * kRmThreads + threadIdx.x; p < N; p += gridDim.y * kRmThreads) {
     if (p >= inf && p < sys) {
