@@ -77,6 +77,8 @@ def parse_args():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-ldpc", action="store_true")
     p.add_argument("--no-learned", action="store_true", help="plain estimator only")
+    p.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning run)")
+    p.add_argument("--no-configs", action="store_true", help="skip the single-slot configuration sub-lines")
     return p.parse_args()
 
 
@@ -239,7 +241,7 @@ SUB_CONFIGS = {
 }
 
 
-def sub_config_lines(ctx, seed, steps, warmup, with_cpu):
+def sub_config_lines(ctx, seed, steps, warmup, with_cpu, autotune=True):
     """The two single-slot configurations as sub-lines of the PUSCH line: one slot plan each (plain
     estimator, CUDA graph), device time per slot with CUDA events (L2 flushed between slots), decoded
     Mbit/s and slots/s; with the CPU baseline, the reference's CPU receive path on one thread on the
@@ -263,7 +265,8 @@ def sub_config_lines(ctx, seed, steps, warmup, with_cpu):
         d_grid = torch.from_numpy(plan.grid.view(np.int32)).cuda()
         d_tb = torch.zeros(max(plan.tb_bytes, 1), dtype=torch.uint8, device="cuda")
         d_res = torch.zeros(n * ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
-        plan.autotune(d_grid.data_ptr(), reps=3)
+        if autotune:
+            plan.autotune(d_grid.data_ptr(), reps=3)
         with torch.cuda.stream(stream):
             for _ in range(max(warmup, 3)):
                 flush.fill_(1)
@@ -452,7 +455,7 @@ def run_ours_pusch(args):
     # Launch shapes picked by the autotuner on this slot (with the estimator that is timed next).
     if net is not None:
         plan.set_learned(net)
-    tuning, _ = plan.autotune(d_grid.data_ptr(), reps=5)
+    tuning = plan.tuning() if args.no_autotune else plan.autotune(d_grid.data_ptr(), reps=5)[0]
     if net is not None:
         plan.set_learned(None)
     ctx.lib.pg_set_kernel_timing(ctx.handle, 1)
@@ -663,7 +666,8 @@ def run_ours_pusch(args):
         cpu["one_thread"] = {"value": round(b1 * passes1 / dt1 / 1e6, 3), "unit": "Mbit/s", "cores": 1,
                              "sample": f"{passes1} passes over the same slot on 1 thread, {dt1:.1f} s"}
     sub_lines = sub_config_lines(ctx, args.seed + rank, max(10, min(args.steps, 100)), args.warmup,
-                                 rank == 0 and world == 1 and not args.no_cpu_baseline) if rank == 0 else None
+                                 rank == 0 and world == 1 and not args.no_cpu_baseline,
+                                 not args.no_autotune) if rank == 0 and not args.no_configs else None
 
     if rank == 0:
         line = {

@@ -325,19 +325,14 @@ __device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_u
                                              const float2* __restrict__ est_all,
                                              const pg_port_result* __restrict__ port_results,
                                              const uint32_t* __restrict__ seq_offsets, const uint32_t* __restrict__ seq,
-                                             int8_t* __restrict__ llrs, const demap_tables& tb)
+                                             int8_t* __restrict__ llrs, const demap_tables& tb, int u_first)
 {
-  // UE of this RE: the last u with re_off[u] <= rg.
-  int lo = 0, hi = nof_ues - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(re_off + mid) <= rg) {
-      lo = mid;
-    } else {
-      hi = mid - 1;
-    }
+  // UE of this RE: the last u with re_off[u] <= rg, searched forward from the UE of the CTA's first
+  // RE (a CTA's REs span one or a few UEs).
+  int u = u_first;
+  while (u + 1 < nof_ues && __ldg(re_off + u + 1) <= rg) {
+    ++u;
   }
-  const int         u   = lo;
   const pg_pusch_ue ue  = ues[u];
   const int         nsc = 12 * ue.nof_rb;
   const int         r   = (int)(rg - __ldg(re_off + u));
@@ -403,16 +398,32 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
   if (threadIdx.x < 3) {
     s_width[threadIdx.x] = c_width_d[threadIdx.x];
   }
+  __shared__ int     s_u0;
+  const uint32_t     first = blockIdx.x * blockDim.x * (uint32_t)res_per_thread;
+  if (threadIdx.x == 0) {
+    // UE of the CTA's first RE: the last u with re_off[u] <= first.
+    int lo = 0, hi = nof_ues - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(re_off + mid) <= first) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    s_u0 = lo;
+  }
   __syncthreads();
   const demap_tables tb    = {s_slope, s_icpt, s_width};
   const uint32_t     total = __ldg(re_off + nof_ues);
-  const uint32_t     base  = blockIdx.x * blockDim.x * (uint32_t)res_per_thread + threadIdx.x;
+  const uint32_t     base  = first + threadIdx.x;
+  const int          u0    = s_u0;
   for (int k = 0; k < res_per_thread; ++k) {
     const uint32_t rg = base + (uint32_t)k * blockDim.x;
     if (rg >= total) {
       break;
     }
-    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, port_results, seq_offsets, seq, llrs, tb);
+    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, port_results, seq_offsets, seq, llrs, tb, u0);
   }
 }
 
