@@ -370,8 +370,11 @@ int pg_pusch_estimate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ue
 /* Per-symbol channel estimates of one UE as the reference's
  * port_channel_estimator_results::get_symbol_ch_estimate returns them: cbf16 [port][symbol][layer]
  * [12 nof_rb] for symbols 0..13 (time interpolation between DM-RS symbols, rounded to bf16).
- * Device pointers. */
-int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, uint32_t* out,
+ * basis (may be NULL): the learned estimator's time-basis coefficients of the UE (same layout as
+ * est, see pg_le_refine_device), added to the interpolation with two DM-RS symbols. Device
+ * pointers. */
+int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, const float* basis,
+                                     uint32_t* out,
                                      void* stream);
 
 /* One receive port of one allocation for port_channel_estimator::compute
@@ -596,12 +599,19 @@ int pg_le_forward_device(pg_le_net* net, const void* x, const uint8_t* row_valid
 int pg_le_backward_device(pg_le_net* net, const void* dy, int rows, void* stream);
 
 /* Refines est (as written by pg_pusch_estimate_ls_device, with its LS output ls and port results)
- * in place for the UEs with use[u] != 0 (use may be NULL: every UE). ues: host array with the
- * est_offset of each UE. */
+ * in place for the UEs with use[u] != 0 (use may be NULL: every UE), and, for UEs with two DM-RS
+ * symbols, writes the network's time-basis coefficients to basis (may be NULL; same layout and
+ * offsets as est, the slots of DM-RS symbols 0 and 1 holding a_1 and a_2). The channel at OFDM
+ * symbol s is then h(s) = h_0 + (h_1 - h_0) w + a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1) with
+ * w = (s - d0) / (d1 - d0): the reference's linear time interpolation between the DM-RS symbols d0
+ * and d1 (port_channel_estimator_average_impl.cpp:705-767) plus two terms the network learns, which
+ * vanish at the DM-RS symbols. ues: host array with the est_offset of each UE. */
 int pg_le_refine_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, float* est,
-                        const pg_port_result* port_results, const uint8_t* use, void* stream);
-/* One training step on a batch of UEs: features -> forward -> mean squared error of the
- * correction against the true responses h_true (same layout as est) -> backward -> Adam.
+                        float* basis, const pg_port_result* port_results, const uint8_t* use, void* stream);
+/* One training step on a batch of UEs: features -> forward -> mean squared error, over every data
+ * symbol of the slot, of the channel the outputs give (refined DM-RS responses and time-basis terms,
+ * as pg_le_refine_device applies them) against the true channel h_true ([port][14][layer]
+ * [12 nof_rb] per UE, UEs back to back in the order given) -> backward -> Adam.
  * loss (device, 2 floats, may be NULL): the network's MSE and the plain estimator's MSE, both in
  * units of the allocations' mean channel power. */
 int pg_le_train_step_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, const float* est,

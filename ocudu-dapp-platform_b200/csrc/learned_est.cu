@@ -181,18 +181,24 @@ __global__ void le_features_kernel(const le_seq* __restrict__ seqs, int nseq, in
   row_valid[r]        = valid ? 1 : 0;
 }
 
-__device__ __forceinline__ void unpack4(const uint4 v, float* o)
+// The eight bf16 channels of one 16-byte activation row.
+__device__ __forceinline__ void unpack8(const uint4 v, float* o)
 {
   const __nv_bfloat16* b = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
+  for (int j = 0; j < 8; ++j) {
     o[j] = __bfloat162float(b[j]);
   }
 }
 
-// est += correction / g on the DM-RS symbols of every valid row (finite corrections only).
+// Corrected estimates: est += correction / g at the DM-RS symbols; with two DM-RS symbols and a
+// basis buffer (same layout as est), the time-basis coefficients a_1, a_2 / g of the rows go to
+// basis[(port, b, layer)] (b = 0, 1): the channel at OFDM symbol s is then
+//   h(s) = h_0 + (h_1 - h_0) w + a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1),  w = (s - d0) / (d1 - d0),
+// the linear interpolation of the reference's estimator plus two terms that vanish at the DM-RS
+// symbols.
 __global__ void le_apply_kernel(const le_seq* __restrict__ seqs, int nseq, int R, const uint4* __restrict__ y,
-                                const float* __restrict__ gseq, float2* __restrict__ est)
+                                const float* __restrict__ gseq, float2* __restrict__ est, float2* __restrict__ basis)
 {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R) {
@@ -205,8 +211,8 @@ __global__ void le_apply_kernel(const le_seq* __restrict__ seqs, int nseq, int R
   if (k < 0 || k >= (int)q.len || !(g > 0.f)) {
     return;
   }
-  float o[4];
-  unpack4(y[r], o);
+  float o[8];
+  unpack8(y[r], o);
   const float inv = 1.f / g;
   for (int d = 0; d < q.nd; ++d) {
     const float dx = o[2 * d] * inv, dyv = o[2 * d + 1] * inv;
@@ -216,13 +222,27 @@ __global__ void le_apply_kernel(const le_seq* __restrict__ seqs, int nseq, int R
       e.y += dyv;
     }
   }
+  if (basis != nullptr && q.nd == 2) {
+    for (int b = 0; b < 2; ++b) {
+      float ax = o[4 + 2 * b] * inv, ay = o[5 + 2 * b] * inv;
+      if (!isfinite(ax) || !isfinite(ay)) {
+        ax = ay = 0.f;
+      }
+      basis[q.est0 + (size_t)b * q.dstride + k] = make_float2(ax, ay);
+    }
+  }
 }
 
-// MSE of the correction against g (H - plain): dy = 2 (y - t) inv_n on the used channels, zero
-// elsewhere; loss[0] += sum (y - t)^2 inv_n, loss[1] += sum t^2 inv_n (the plain estimator's error).
+// Mean squared error of the channel the network's outputs give at every data symbol of the slot
+// (the DM-RS symbols carry no data) against the true channel, in the units of the features (x g):
+// target t(s) = g (H(s) - plain(s)), plain(s) = the reference's linear interpolation of the plain
+// estimates, prediction p(s) = c_0 + (c_1 - c_0) w + a_1 phi_1(w) + a_2 phi_2(w) with the output pairs
+// (0,1) c_0, (2,3) c_1, (4,5) a_1, (6,7) a_2 (one DM-RS symbol: p(s) = c_0). dy = the gradient of
+// sum |p - t|^2 inv_n; loss[0] += sum |p - t|^2 inv_n, loss[1] += sum |t|^2 inv_n (the plain
+// estimator's error). h_full: [port][14][layer][subcarrier] per UE (le_seq::h0).
 __global__ void le_loss_kernel(const le_seq* __restrict__ seqs, int nseq, int R, const uint4* __restrict__ y,
                                const float* __restrict__ gseq, const float2* __restrict__ est,
-                               const float2* __restrict__ h_true, float inv_n, uint4* __restrict__ dy,
+                               const float2* __restrict__ h_full, float inv_n, uint4* __restrict__ dy,
                                float* __restrict__ loss)
 {
   const int r   = blockIdx.x * blockDim.x + threadIdx.x;
@@ -232,22 +252,45 @@ __global__ void le_loss_kernel(const le_seq* __restrict__ seqs, int nseq, int R,
     const le_seq q = seqs[s];
     const int    k = r - (int)q.row0;
     const float  g = gseq[s];
-    float        d4[4] = {0.f, 0.f, 0.f, 0.f};
+    float        d8[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (k >= 0 && k < (int)q.len && g > 0.f) {
-      float o[4];
-      unpack4(y[r], o);
-      for (int d = 0; d < q.nd; ++d) {
-        const size_t i  = q.est0 + (size_t)d * q.dstride + k;
-        const float2 p  = est[i], h = h_true[i];
-        const float  tx = g * (h.x - p.x), ty = g * (h.y - p.y);
-        const float  ex = o[2 * d] - tx, ey = o[2 * d + 1] - ty;
-        d4[2 * d]       = 2.f * ex * inv_n;
-        d4[2 * d + 1]   = 2.f * ey * inv_n;
-        l0 += (ex * ex + ey * ey) * inv_n;
+      float o[8];
+      unpack8(y[r], o);
+      const int    d0 = q.dsym & 15, d1 = q.dsym >> 4;
+      const float2 p0 = est[q.est0 + k];
+      const float2 p1 = q.nd > 1 ? est[q.est0 + q.dstride + k] : p0;
+      for (int sy = 0; sy < 14; ++sy) {
+        if (sy == d0 || (q.nd > 1 && sy == d1)) {
+          continue;
+        }
+        const float  w  = q.nd > 1 ? (float)(sy - d0) / (float)(d1 - d0) : 0.f;
+        const float  f1 = q.nd > 1 ? w * (1.f - w) : 0.f;
+        const float  f2 = f1 * (2.f * w - 1.f);
+        const float2 h  = h_full[q.h0 + (size_t)sy * q.dstride + k];
+        const float  tx = g * (h.x - (p0.x + (p1.x - p0.x) * w));
+        const float  ty = g * (h.y - (p0.y + (p1.y - p0.y) * w));
+        const float  px = q.nd > 1 ? o[0] + (o[2] - o[0]) * w + o[4] * f1 + o[6] * f2 : o[0];
+        const float  py = q.nd > 1 ? o[1] + (o[3] - o[1]) * w + o[5] * f1 + o[7] * f2 : o[1];
+        const float  ex = (px - tx) * 2.f * inv_n, ey = (py - ty) * 2.f * inv_n;
+        if (q.nd > 1) {
+          d8[0] += ex * (1.f - w);
+          d8[1] += ey * (1.f - w);
+          d8[2] += ex * w;
+          d8[3] += ey * w;
+          d8[4] += ex * f1;
+          d8[5] += ey * f1;
+          d8[6] += ex * f2;
+          d8[7] += ey * f2;
+        } else {
+          d8[0] += ex;
+          d8[1] += ey;
+        }
+        l0 += ((px - tx) * (px - tx) + (py - ty) * (py - ty)) * inv_n;
         l1 += (tx * tx + ty * ty) * inv_n;
       }
     }
-    dy[r]             = make_uint4(pack_bf16x2(d4[0], d4[1]), pack_bf16x2(d4[2], d4[3]), 0u, 0u);
+    dy[r]             = make_uint4(pack_bf16x2(d8[0], d8[1]), pack_bf16x2(d8[2], d8[3]), pack_bf16x2(d8[4], d8[5]),
+                                   pack_bf16x2(d8[6], d8[7]));
     dy[(size_t)R + r] = make_uint4(0, 0, 0, 0);
   }
 #pragma unroll
@@ -886,9 +929,10 @@ namespace pg {
 size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vector<le_seq>& out, size_t* terms)
 {
   out.clear();
-  size_t row = 0, nterms = 0;
+  size_t row = 0, nterms = 0, h_base = 0;
   for (int u = 0; u < n; ++u) {
     if (use != nullptr && use[u] == 0) {
+      h_base += (size_t)ues[u].nof_rx_ports * 14 * ues[u].nof_layers * 12 * ues[u].nof_rb;
       continue;
     }
     const pg_pusch_ue& ue = ues[u];
@@ -908,11 +952,14 @@ size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vec
         q.layer      = (uint8_t)l;
         q.nof_layers = ue.nof_layers;
         q.nd         = (uint8_t)std::min(nd, 2);
+        q.dsym       = (uint8_t)(d0 | ((q.nd > 1 ? d1 : d0) << 4));
+        q.h0         = (uint32_t)(h_base + (size_t)((p * 14) * ue.nof_layers + l) * nsc);
         out.push_back(q);
         row += nsc;
-        nterms += (size_t)nsc * 2 * q.nd;
+        nterms += (size_t)nsc * 2 * (14 - q.nd);
       }
     }
+    h_base += (size_t)ue.nof_rx_ports * 14 * ue.nof_layers * nsc;
   }
   if (terms != nullptr) {
     *terms = nterms;
@@ -921,7 +968,7 @@ size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vec
 }
 
 int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, const float* ls, float* est,
-                     const pg_port_result* pr, cudaStream_t s)
+                     float* basis, const pg_port_result* pr, cudaStream_t s)
 {
   if (nseq == 0 || R == 0) {
     return PG_OK;
@@ -935,7 +982,8 @@ int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, co
   }
   if (rc == PG_OK) {
     le_apply_kernel<<<(R + 255) / 256, 256, 0, s>>>(seqs_dev, nseq, R, reinterpret_cast<const uint4*>(net->y),
-                                                    net->gseq, reinterpret_cast<float2*>(est));
+                                                    net->gseq, reinterpret_cast<float2*>(est),
+                                                    reinterpret_cast<float2*>(basis));
     rc = check_cuda(net->ctx, cudaGetLastError(), "le_apply_kernel launch");
   }
   return rc;
@@ -1214,7 +1262,7 @@ static int stage_seqs(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const
 }
 
 int pg_le_refine_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, float* est,
-                        const pg_port_result* port_results, const uint8_t* use, void* stream)
+                        float* basis, const pg_port_result* port_results, const uint8_t* use, void* stream)
 {
   if (net == nullptr) {
     return PG_ERR_INVALID;
@@ -1227,7 +1275,7 @@ int pg_le_refine_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, con
   if (int rc = stage_seqs(net, ues, nof_ues, use, &nseq, &R, nullptr, s)) {
     return rc;
   }
-  return le_refine_launch(net, net->seqs, nseq, R, ls, est, port_results, s);
+  return le_refine_launch(net, net->seqs, nseq, R, ls, est, basis, port_results, s);
 }
 
 int pg_le_train_step_device(pg_le_net* net, const pg_pusch_ue* ues, int nof_ues, const float* ls, const float* est,

@@ -166,11 +166,14 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s);
-// Same with `block` threads per CTA (64, 128 or 256) and res_per_thread REs per thread (1..8).
+// Same with `block` threads per CTA (64, 128 or 256) and res_per_thread REs per thread (1..8), and
+// the learned estimator's time-basis coefficients (basis, same layout as est; may be NULL) for the
+// UEs with basis_use[u] != 0.
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
-                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread);
+                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis = nullptr,
+                      const uint8_t* basis_use = nullptr);
 // Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
 // uses scratch_b; results and TB payloads land in host memory.
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
@@ -232,19 +235,22 @@ struct le_seq {
   uint32_t dstride; // complex floats from DM-RS symbol 0 to 1 (layers x 12 nof_rb)
   uint32_t pr;      // port-result index (u * 4 + port)
   float    beta;    // DM-RS amplitude
-  uint8_t  layer, nof_layers, nd, pad;
-  uint32_t pad2;
+  uint32_t h0;      // complex-float offset of (port, OFDM symbol 0, layer) in the full-grid truth of training
+                    // ([port][14][layer][12 nof_rb] per UE, UEs back to back); symbol stride dstride
+  uint8_t  layer, nof_layers, nd;
+  uint8_t  dsym;    // DM-RS symbols: first in bits 0-3, second in bits 4-7
 };
 static_assert(sizeof(le_seq) == 32, "le_seq layout");
 
 // Sequences of the UEs with use[u] != 0 (all when use is null), est_offset already assigned;
-// returns the rows of the layout (0 without sequences) and, in *terms, the loss terms.
+// returns the rows of the layout (0 without sequences) and, in *terms, the loss terms (two per
+// subcarrier and data symbol).
 size_t le_build_seqs(const pg_pusch_ue* ues, int n, const uint8_t* use, std::vector<le_seq>& out, size_t* terms);
 // PG_OK when the net's buffers hold `rows` rows and `nseq` sequences, else PG_ERR_CAPACITY.
 int le_capacity(const pg_le_net* net, size_t rows, int nseq);
 pg_context* le_context(const pg_le_net* net);
 // Features -> network -> est += correction, for sequences already in device memory.
-int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, const float* ls, float* est,
+int le_refine_launch(pg_le_net* net, const le_seq* seqs_dev, int nseq, int R, const float* ls, float* est, float* basis,
                      const pg_port_result* pr, cudaStream_t s);
 // Event-record flags for timing events on stream s: under stream capture the records become event
 // nodes of the graph (external records).

@@ -139,9 +139,10 @@ struct demap_tables {
 
 template <int L, int P, int QM>
 __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* __restrict__ grid,
-                                         const float2* __restrict__ est, const pg_port_result* __restrict__ pres,
-                                         int nd, float w, int sym, int re_idx, int j, const uint32_t* __restrict__ seq,
-                                         int8_t* __restrict__ llr_out, const demap_tables& tb)
+                                         const float2* __restrict__ est, const float2* __restrict__ basis,
+                                         const pg_port_result* __restrict__ pres, int nd, float w, int sym, int re_idx,
+                                         int j, const uint32_t* __restrict__ seq, int8_t* __restrict__ llr_out,
+                                         const demap_tables& tb)
 {
   const int nsc     = 12 * ue.nof_rb;
   const int sc      = 12 * ue.rb_start + j;
@@ -158,6 +159,15 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
       if (nd == 2) {
         const float2 v1 = f0[(size_t)L * nsc + j];
         v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
+        if (basis != nullptr) {
+          // The learned estimator's time-basis terms a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1).
+          const float2* b0 = basis + (((size_t)p * nd) * L + l) * nsc;
+          const float2  a1 = b0[j], a2 = b0[(size_t)L * nsc + j];
+          const float   f1 = __fmul_rn(w, __fsub_rn(1.f, w));
+          const float   f2 = __fmul_rn(f1, __fsub_rn(__fmul_rn(2.f, w), 1.f));
+          v                = make_float2(__fmaf_rn(a2.x, f2, __fmaf_rn(a1.x, f1, v.x)),
+                                         __fmaf_rn(a2.y, f2, __fmaf_rn(a1.y, f1, v.y)));
+        }
       }
       h[p][l] = is_dc ? cf{0.f, 0.f} : cf{bf16_round(v.x), bf16_round(v.y)};
     }
@@ -306,14 +316,15 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
 
 template <int L, int P>
 __device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const uint32_t* grid, const float2* est,
-                                                  const pg_port_result* pres, int nd, float w, int sym, int re_idx,
-                                                  int j, const uint32_t* seq, int8_t* llrs, const demap_tables& tb)
+                                                  const float2* bas, const pg_port_result* pres, int nd, float w,
+                                                  int sym, int re_idx, int j, const uint32_t* seq, int8_t* llrs,
+                                                  const demap_tables& tb)
 {
   switch (ue.modulation_order) {
-    case 2: demod_re<L, P, 2>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    case 4: demod_re<L, P, 4>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    case 6: demod_re<L, P, 6>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    default: demod_re<L, P, 8>(ue, grid, est, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 2: demod_re<L, P, 2>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 4: demod_re<L, P, 4>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 6: demod_re<L, P, 6>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    default: demod_re<L, P, 8>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
   }
 }
 
@@ -323,6 +334,8 @@ __device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const u
 __device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_ue* __restrict__ ues, int nof_ues,
                                              const uint32_t* __restrict__ re_off, const uint32_t* __restrict__ grids,
                                              const float2* __restrict__ est_all,
+                                             const float2* __restrict__ basis_all,
+                                             const uint8_t* __restrict__ basis_use,
                                              const pg_port_result* __restrict__ port_results,
                                              const uint32_t* __restrict__ seq_offsets, const uint32_t* __restrict__ seq,
                                              int8_t* __restrict__ llrs, const demap_tables& tb, int u_first)
@@ -362,18 +375,21 @@ __device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_u
   const float           w    = nd == 2 ? (float)(sym - d0) / (float)(d1 - d0) : 0.f;
   const uint32_t*       grid = grids + ue.grid_offset;
   const float2*         est  = est_all + ue.est_offset;
+  const float2*         bas  = (basis_all != nullptr && basis_use != nullptr && nd == 2 && basis_use[u] != 0)
+                                   ? basis_all + ue.est_offset
+                                   : nullptr;
   const pg_port_result* pres = port_results + (size_t)u * 4;
   const uint32_t*       sq   = seq + seq_offsets[u];
   if (ue.nof_layers == 1) {
     switch (ue.nof_rx_ports) {
-      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      default: demod_dispatch_qm<1, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      default: demod_dispatch_qm<1, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
     }
   } else {
     switch (ue.nof_rx_ports) {
-      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      default: demod_dispatch_qm<2, 4>(ue, grid, est, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      default: demod_dispatch_qm<2, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
     }
   }
 }
@@ -383,6 +399,8 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
                                                           const uint32_t* __restrict__ re_off,
                                                           const uint32_t* __restrict__ grids,
                                                           const float2* __restrict__ est_all,
+                                                          const float2* __restrict__ basis_all,
+                                                          const uint8_t* __restrict__ basis_use,
                                                           const pg_port_result* __restrict__ port_results,
                                                           const uint32_t* __restrict__ seq_offsets,
                                                           const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs,
@@ -423,7 +441,8 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
     if (rg >= total) {
       break;
     }
-    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, port_results, seq_offsets, seq, llrs, tb, u0);
+    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, basis_all, basis_use, port_results, seq_offsets, seq, llrs,
+                 tb, u0);
   }
 }
 
@@ -475,7 +494,8 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
-                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread)
+                      int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis,
+                      const uint8_t* basis_use)
 {
   if (n == 0 || total_re == 0) {
     return PG_OK;
@@ -485,9 +505,9 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
   }
   res_per_thread       = std::max(1, std::min(8, res_per_thread));
   const uint32_t per   = (uint32_t)block * (uint32_t)res_per_thread;
-  pusch_demod_kernel<<<(total_re + per - 1) / per, block, 0, s>>>(ues_dev, n, re_off_dev, grids,
-                                                                  reinterpret_cast<const float2*>(est), port_results,
-                                                                  seq_offsets_dev, seq_dev, llrs, res_per_thread);
+  pusch_demod_kernel<<<(total_re + per - 1) / per, block, 0, s>>>(
+      ues_dev, n, re_off_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
+      basis_use, port_results, seq_offsets_dev, seq_dev, llrs, res_per_thread);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 

@@ -407,9 +407,12 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
 }
 
 // Per-symbol estimates of one UE: f[i] + (f[i+1] - f[i]) w rounded to bf16 (the reference's
-// apply_td_domain_strategy + conversion to cbf16_t).
-__global__ void symbol_estimates_kernel(pg_pusch_ue ue, const float2* __restrict__ est, uint32_t* __restrict__ out,
-                                        int nd, int dsym0, int dsym1)
+// apply_td_domain_strategy + conversion to cbf16_t); with the learned estimator's time-basis
+// coefficients (basis, two DM-RS symbols) + a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1) before the
+// rounding, in the demodulator's operation order.
+__global__ void symbol_estimates_kernel(pg_pusch_ue ue, const float2* __restrict__ est,
+                                        const float2* __restrict__ basis, uint32_t* __restrict__ out, int nd,
+                                        int dsym0, int dsym1)
 {
   const int nsc = 12 * ue.nof_rb;
   const int nl  = ue.nof_layers;
@@ -428,6 +431,16 @@ __global__ void symbol_estimates_kernel(pg_pusch_ue ue, const float2* __restrict
     if (nd == 2) {
       const float2 v1 = f0[(size_t)nl * nsc + j];
       v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
+      if (basis != nullptr) {
+        const int L = nl;
+          // The learned estimator's time-basis terms a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1).
+          const float2* b0 = basis + (((size_t)p * nd) * L + l) * nsc;
+          const float2  a1 = b0[j], a2 = b0[(size_t)L * nsc + j];
+          const float   f1 = __fmul_rn(w, __fsub_rn(1.f, w));
+          const float   f2 = __fmul_rn(f1, __fsub_rn(__fmul_rn(2.f, w), 1.f));
+          v                = make_float2(__fmaf_rn(a2.x, f2, __fmaf_rn(a1.x, f1, v.x)),
+                                         __fmaf_rn(a2.y, f2, __fmaf_rn(a1.y, f1, v.y)));
+      }
     }
     out[(((size_t)p * 14 + s) * nl + l) * nsc + j] = float_to_bf16_rne(v.x) | (float_to_bf16_rne(v.y) << 16);
   }
@@ -687,8 +700,8 @@ int pg_pusch_estimate_ls_device(pg_context* ctx, const pg_pusch_ue* ues, int nof
   return release_slot_after(ctx, SLOT_UE, s);
 }
 
-int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, uint32_t* out,
-                                     void* stream)
+int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, const float* basis,
+                                     uint32_t* out, void* stream)
 {
   if (ctx == nullptr || ue == nullptr) {
     return PG_ERR_INVALID;
@@ -699,8 +712,9 @@ int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, con
   int       d0 = 0, d1 = 0;
   const int nd = dmrs_count(*ue, &d0, &d1);
   symbol_estimates_kernel<<<dim3((ue->nof_layers * 12 * ue->nof_rb + 255) / 256, 14, ue->nof_rx_ports), 256, 0,
-                            static_cast<cudaStream_t>(stream)>>>(*ue, reinterpret_cast<const float2*>(est), out, nd,
-                                                                 d0, d1);
+                            static_cast<cudaStream_t>(stream)>>>(*ue, reinterpret_cast<const float2*>(est),
+                                                                 reinterpret_cast<const float2*>(basis), out, nd, d0,
+                                                                 d1);
   return check_cuda(ctx, cudaGetLastError(), "symbol_estimates_kernel launch");
 }
 
@@ -806,7 +820,7 @@ int pg_port_channel_estimate_host(pg_context* ctx, const pg_port_estimate_cfg* c
   }
   if (rc == PG_OK && symbol_estimates != nullptr) {
     symbol_estimates_kernel<<<dim3((nl * nsc + 255) / 256, 14, 1), 256, 0, s>>>(
-        ue, reinterpret_cast<const float2*>(b + o_est), reinterpret_cast<uint32_t*>(b + o_sym), nd, d0, d1);
+        ue, reinterpret_cast<const float2*>(b + o_est), nullptr, reinterpret_cast<uint32_t*>(b + o_sym), nd, d0, d1);
     rc = check_cuda(ctx, cudaGetLastError(), "symbol_estimates_kernel launch");
   }
   if (rc == PG_OK) {

@@ -69,10 +69,13 @@ struct pg_pusch_plan {
   void*           host_slot[2]  = {nullptr, nullptr};
   uint64_t        submitted     = 0;
   uint64_t        collected     = 0;
-  // Learned estimator: the net, the LS estimates and the sequences of the refined UEs.
-  pg_le_net*      le_net    = nullptr;
-  void*           le_dev    = nullptr;
-  float*          d_ls      = nullptr;
+  // Learned estimator: the net, the LS estimates, the time-basis coefficients (same layout as
+  // d_est) with the per-UE flags of the UEs that use them, and the sequences of the refined UEs.
+  pg_le_net*      le_net      = nullptr;
+  void*           le_dev      = nullptr;
+  float*          d_ls        = nullptr;
+  float*          d_basis     = nullptr;
+  uint8_t*        d_basis_use = nullptr;
   le_seq*         d_le_seqs = nullptr;
   int             le_nseq   = 0;
   int             le_rows   = 0;
@@ -133,7 +136,8 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     if (ctx->timed) {
       cudaEventRecordWithFlags(ctx->ev_le_start, s, flags);
     }
-    rc = le_refine_launch(p->le_net, p->d_le_seqs, p->le_nseq, p->le_rows, p->d_ls, p->d_est, port_results, s);
+    rc = le_refine_launch(p->le_net, p->d_le_seqs, p->le_nseq, p->le_rows, p->d_ls, p->d_est, p->d_basis,
+                          port_results, s);
     if (ctx->timed) {
       cudaEventRecordWithFlags(ctx->ev_le_stop, s, flags);
       ctx->le_recorded = true;
@@ -141,7 +145,9 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
   }
   if (rc == PG_OK) {
     rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
-                           p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread);
+                           p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread,
+                           p->le_net != nullptr ? p->d_basis : nullptr,
+                           p->le_net != nullptr ? p->d_basis_use : nullptr);
   }
   if (rc == PG_OK) {
     rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb);
@@ -427,10 +433,12 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
     plan->exec = nullptr;
   }
   cudaFree(plan->le_dev);
-  plan->le_dev    = nullptr;
-  plan->le_net    = nullptr;
-  plan->d_ls      = nullptr;
-  plan->d_le_seqs = nullptr;
+  plan->le_dev      = nullptr;
+  plan->le_net      = nullptr;
+  plan->d_ls        = nullptr;
+  plan->d_basis     = nullptr;
+  plan->d_basis_use = nullptr;
+  plan->d_le_seqs   = nullptr;
   plan->le_nseq = plan->le_rows = 0;
   if (net == nullptr) {
     return PG_OK;
@@ -441,9 +449,25 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
     return set_error(ctx, PG_ERR_CAPACITY,
                      "learned estimator: the plan needs " + std::to_string(rows) + " rows, more than the net holds");
   }
-  const size_t o_seq = al(plan->est_total * 8);
-  const size_t bytes = o_seq + al(std::max<size_t>(1, seqs.size()) * sizeof(le_seq));
-  int          rc    = check_cuda(ctx, cudaMalloc(&plan->le_dev, bytes), "cudaMalloc(plan learned estimator)");
+  const size_t o_basis = al(plan->est_total * 8);
+  const size_t o_use   = o_basis + al(plan->est_total * 8);
+  const size_t o_seq   = o_use + al((size_t)plan->nof_ues);
+  const size_t bytes   = o_seq + al(std::max<size_t>(1, seqs.size()) * sizeof(le_seq));
+  int          rc      = check_cuda(ctx, cudaMalloc(&plan->le_dev, bytes), "cudaMalloc(plan learned estimator)");
+  std::vector<uint8_t> use_flags(plan->nof_ues);
+  for (int u = 0; u < plan->nof_ues; ++u) {
+    use_flags[u] = (use == nullptr || use[u] != 0) ? 1 : 0;
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemset(static_cast<uint8_t*>(plan->le_dev) + o_basis, 0, plan->est_total * 8),
+                    "cudaMemset(plan time-basis coefficients)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaMemcpy(static_cast<uint8_t*>(plan->le_dev) + o_use, use_flags.data(), use_flags.size(),
+                               cudaMemcpyHostToDevice),
+                    "H2D plan learned-estimator flags");
+  }
   if (rc == PG_OK && !seqs.empty()) {
     rc = check_cuda(ctx,
                     cudaMemcpy(static_cast<uint8_t*>(plan->le_dev) + o_seq, seqs.data(), seqs.size() * sizeof(le_seq),
@@ -455,8 +479,10 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
     plan->le_dev = nullptr;
     return rc;
   }
-  plan->d_ls      = static_cast<float*>(plan->le_dev);
-  plan->d_le_seqs = reinterpret_cast<le_seq*>(static_cast<uint8_t*>(plan->le_dev) + o_seq);
+  plan->d_ls        = static_cast<float*>(plan->le_dev);
+  plan->d_basis     = reinterpret_cast<float*>(static_cast<uint8_t*>(plan->le_dev) + o_basis);
+  plan->d_basis_use = static_cast<uint8_t*>(plan->le_dev) + o_use;
+  plan->d_le_seqs   = reinterpret_cast<le_seq*>(static_cast<uint8_t*>(plan->le_dev) + o_seq);
   plan->le_nseq   = (int)seqs.size();
   plan->le_rows   = (int)rows;
   plan->le_net    = net;

@@ -158,7 +158,7 @@ SIGNATURES = {
     "pg_demodulate_soft_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     "pg_pusch_est_size": (ctypes.c_size_t, [_VP]),
     "pg_pusch_estimate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
-    "pg_pusch_symbol_estimates_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    "pg_pusch_symbol_estimates_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_demodulate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_process_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _VP,
                                              _VP]),
@@ -185,7 +185,7 @@ SIGNATURES = {
     "pg_le_status": (ctypes.c_int, [_VP]),
     "pg_le_forward_device": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, _VP, _VP]),
     "pg_le_backward_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP]),
-    "pg_le_refine_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
+    "pg_le_refine_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_le_train_step_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_estimate_ls_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_pusch_plan_set_learned": (ctypes.c_int, [_VP, _VP, _VP]),

@@ -87,11 +87,13 @@ class LearnedEstimator:
     def backward(self, dy_ptr, rows, stream=0):
         self.ctx.check(self.lib.pg_le_backward_device(self.handle, dy_ptr, rows, stream))
 
-    def refine(self, descs, ls_ptr, est_ptr, pr_ptr, use=None, stream=0):
+    def refine(self, descs, ls_ptr, est_ptr, pr_ptr, use=None, basis_ptr=None, stream=0):
+        """Corrects est in place; with basis_ptr (a buffer of est's size), writes the time-basis
+        coefficients of the UEs with two DM-RS symbols there (pg_le_refine_device)."""
         n = len(descs)
         u = None if use is None else (ctypes.c_uint8 * n)(*[int(bool(v)) for v in use])
-        self.ctx.check(self.lib.pg_le_refine_device(self.handle, ctypes.addressof(descs), n, ls_ptr, est_ptr, pr_ptr,
-                                                    u, stream))
+        self.ctx.check(self.lib.pg_le_refine_device(self.handle, ctypes.addressof(descs), n, ls_ptr, est_ptr,
+                                                    basis_ptr, pr_ptr, u, stream))
 
     def train_step(self, descs, ls_ptr, est_ptr, pr_ptr, h_ptr, opt: PgLeAdam, loss_ptr, stream=0):
         self.ctx.check(self.lib.pg_le_train_step_device(self.handle, ctypes.addressof(descs), len(descs), ls_ptr,
@@ -139,7 +141,8 @@ def cbf16_words(torch, re, im):
 
 class DmrsTrainingSource:
     """Seeded batches of UEs with DM-RS-only grids (symbols 2 and 11, 4 receive ports) and their
-    true frequency responses at the DM-RS symbols, in the estimator's layout. Per UE: allocation
+    true channel at all 14 OFDM symbols ([port][symbol][layer][12 nof_rb] per UE, the layout
+    pg_le_train_step_device reads). Per UE: allocation
     1-273 PRB (half log-uniform, half uniform), 1 or 2 layers, SNR U[snr_db], exponential PDP of 8
     taps with RMS delay U[delay_ns], Rayleigh taps with Jakes' Doppler spectrum (16 sinusoids)
     at a maximum Doppler U[doppler_hz]."""
@@ -156,7 +159,7 @@ class DmrsTrainingSource:
         self.n_ids = n_ids
         self.device = device
         t = np.arange(14) * (1e-3 / (scs_khz / 15) / 14)
-        self.t_dmrs = torch.tensor(t[list(DMRS_SYMBOLS)], dtype=torch.float32, device=device)
+        self.t_sym = torch.tensor(t, dtype=torch.float32, device=device)
 
     def draw_ue(self):
         r = self.rng
@@ -194,7 +197,7 @@ class DmrsTrainingSource:
             d.slot, d.n_scid, d.first_symbol, d.nof_symbols = u["slot"], 0, 0, 14
             d.nof_rx_ports, d.nof_layers, d.modulation_order = P, L, 2
             d.base_graph, d.rv, d.max_iterations = 1, 0, 1
-            h = self.channel(u, K, L)                                  # [P][L][2][K] complex64
+            h = self.channel(u, K, L)                                  # [P][L][14][K] complex64
             g = torch.zeros((P, 14, K), dtype=torch.int32, device=self.device)
             nv = 10 ** (-u["snr"] / 10)
             for di, s in enumerate(DMRS_SYMBOLS):
@@ -203,11 +206,11 @@ class DmrsTrainingSource:
                 if L > 1:
                     pl[1, 1::2] *= -1
                 rx = torch.zeros((P, K), dtype=torch.complex64, device=self.device)
-                rx[:, 0::2] = (h[:, :, di, 0::2] * pl.unsqueeze(0)).sum(1) * BETA
+                rx[:, 0::2] = (h[:, :, s, 0::2] * pl.unsqueeze(0)).sum(1) * BETA
                 noise = torch.randn((2, P, K), generator=self.gen, device=self.device) * math.sqrt(nv / 2)
                 g[:, s, :] = cbf16_words(torch, rx.real + noise[0], rx.imag + noise[1])
             grids.append(g.reshape(-1))
-            hs.append(h.permute(0, 2, 1, 3).reshape(-1))            # [P][d][L][K]
+            hs.append(h.permute(0, 2, 1, 3).reshape(-1))            # [P][14][L][K]
             grid_off += P * 14 * K
             est_off += P * 2 * L * K
         grid = torch.cat(grids)
@@ -224,8 +227,8 @@ class DmrsTrainingSource:
         steer = torch.exp(-2j * math.pi * (tau[:, None] * f[None, :]).to(torch.complex64))          # [T][K]
         ang = torch.rand((P, L, T, M), generator=self.gen, device=self.device) * 2 * math.pi
         ph = torch.rand((P, L, T, M), generator=self.gen, device=self.device) * 2 * math.pi
-        arg = 2 * math.pi * u["doppler"] * torch.cos(ang)[..., None] * self.t_dmrs + ph[..., None]   # [P][L][T][M][2]
-        a = torch.exp(1j * arg.to(torch.complex64)).sum(3) / math.sqrt(M)                         # [P][L][T][2]
+        arg = 2 * math.pi * u["doppler"] * torch.cos(ang)[..., None] * self.t_sym + ph[..., None]    # [P][L][T][M][14]
+        a = torch.exp(1j * arg.to(torch.complex64)).sum(3) / math.sqrt(M)                         # [P][L][T][14]
         a = a * torch.sqrt(pw)[None, None, :, None]
         return torch.einsum("pltd,tk->pldk", a, steer)
 
@@ -288,19 +291,72 @@ def tb_errors(results, truths):
     return [not (r.tb_crc_ok and bool((np.unpackbits(r.transport_block) == t).all())) for r, t in zip(results, truths)]
 
 
-def _true_dmrs_response(slot, u, nd_syms):
+def cbf16_to_complex(words):
+    """uint32/int32 complex bf16 words (numpy) -> complex64."""
+    w = np.asarray(words).astype(np.uint32)
+    re = (w << 16).view(np.float32)
+    im = (w & 0xFFFF0000).view(np.float32)
+    return re + 1j * im
+
+
+def grid_estimates(ctx, descs, est, basis=None):
+    """The channel estimate of every UE at all 14 OFDM symbols, as the demodulator uses it
+    (pg_pusch_symbol_estimates_device: time interpolation between the DM-RS symbols, plus the
+    time-basis terms when basis is given, rounded to bf16): one complex64 array per UE,
+    [port][14][layer][12 nof_rb]."""
+    import torch
+    lib = _native.load()
+    out = []
+    for i in range(len(descs)):
+        d = descs[i]
+        P, L, K = d.nof_rx_ports, d.nof_layers, 12 * d.nof_rb
+        sym = torch.empty((P, 14, L, K), dtype=torch.int32, device="cuda")
+        bp = None if basis is None else basis.data_ptr() + 8 * d.est_offset
+        ctx.check(lib.pg_pusch_symbol_estimates_device(ctx.handle, ctypes.byref(d), est.data_ptr() + 8 * d.est_offset,
+                                                       bp, sym.data_ptr(), None))
+        out.append(cbf16_to_complex(sym.cpu().numpy()))
+    return out
+
+
+def data_symbol_nmse(descs, grids, truths):
+    """Normalised squared error of per-UE [port][14][layer][K] estimates against the true channel
+    over the symbols that carry no DM-RS."""
+    err = sig = 0.0
+    for i, (g, t) in enumerate(zip(grids, truths)):
+        mask = descs[i].dmrs_symbol_mask
+        data = [s for s in range(14) if not (mask >> s) & 1]
+        e = g[:, data] - t[:, data]
+        err += float(np.sum(np.abs(e) ** 2))
+        sig += float(np.sum(np.abs(t[:, data]) ** 2))
+    return err / sig
+
+
+def split_truth(descs, h_true):
+    """h_true of DmrsTrainingSource.make (real pairs, UEs back to back) -> per-UE complex
+    [port][14][layer][K] arrays."""
+    h = h_true.cpu().numpy().view(np.complex64).reshape(-1)
+    out, off = [], 0
+    for i in range(len(descs)):
+        d = descs[i]
+        shape = (d.nof_rx_ports, 14, d.nof_layers, 12 * d.nof_rb)
+        m = int(np.prod(shape))
+        out.append(h[off:off + m].reshape(shape))
+        off += m
+    return out
+
+
+def _true_channel(slot, u):
     h = slot.channels[u]                                        # [P][L][nsc] or [P][L][14][nsc]
     if h.ndim == 3:
-        hs = np.stack([h] * len(nd_syms), axis=1)               # [P][d][L][nsc]
-    else:
-        hs = np.stack([h[:, :, s, :] for s in nd_syms], axis=1)
-    return hs.reshape(-1)
+        h = np.stack([h] * 14, axis=2)
+    return h.transpose(0, 2, 1, 3)                              # [P][14][L][nsc]
 
 
 def estimate_quality(ctx, slots, net=None, max_iterations=6):
-    """EVM of the MMSE-equalised data symbols and NMSE of the DM-RS frequency responses, with the
-    plain estimates and (when net is given) the refined ones, through the library's stage entries:
-    estimation (pg_pusch_estimate_ls_device), refinement (pg_le_refine_device), per-symbol estimates
+    """EVM of the MMSE-equalised data symbols and NMSE of the channel estimate over the data
+    symbols, with the plain estimates and (when net is given) the refined ones with their
+    time-basis terms, through the library's stage entries: estimation
+    (pg_pusch_estimate_ls_device), refinement (pg_le_refine_device), per-symbol estimates
     (pg_pusch_symbol_estimates_device) and equalisation (pg_equalize_device)."""
     import torch
     from .pusch import batch_descriptors
@@ -313,36 +369,36 @@ def estimate_quality(ctx, slots, net=None, max_iterations=6):
         descs[i].est_offset = off
         off += 4 * len(ues[i].dmrs_symbols) * ues[i].nof_layers * 12 * ues[i].nof_rb
     d_grid = torch.from_numpy(grid.view(np.int32)).cuda()
-    est_size = sum(4 * len(ue.dmrs_symbols) * ue.nof_layers * 12 * ue.nof_rb for ue in ues)
+    est_size = off
     est = torch.empty(2 * est_size, dtype=torch.float32, device="cuda")
     ls = torch.empty_like(est)
     pr = torch.empty((4 * n, 5), dtype=torch.float32, device="cuda")
     ctx.check(lib.pg_pusch_estimate_ls_device(ctx.handle, ctypes.addressof(descs), n, d_grid.data_ptr(),
                                               est.data_ptr(), ls.data_ptr(), pr.data_ptr(), None))
-    variants = {"plain": est}
+    variants = {"plain": (est, None)}
     if net is not None:
         est_l = est.clone()
-        net.refine(descs, ls.data_ptr(), est_l.data_ptr(), pr.data_ptr())
-        variants["learned"] = est_l
+        basis = torch.zeros_like(est)
+        net.refine(descs, ls.data_ptr(), est_l.data_ptr(), pr.data_ptr(), basis_ptr=basis.data_ptr())
+        variants["learned"] = (est_l, basis)
     torch.cuda.synchronize()
     prh = pr.cpu().numpy().reshape(n, 4, 5)
     slot_of = [(si, u) for si, sl in enumerate(slots) for u in range(len(sl.ues))]
+    truths = [_true_channel(slots[si], u) for si, u in slot_of]
     out = {}
-    for name, e in variants.items():
-        err = sig = herr = hsig = 0.0
-        e_host = e.cpu().numpy().view(np.complex64)
+    for name, (e, bas) in variants.items():
+        err = sig = 0.0
+        g_all = grid_estimates(ctx, descs, e, bas)
         for i in range(n):
             d, ue = descs[i], ues[i]
             sl = slots[slot_of[i][0]]
             P, L, K = d.nof_rx_ports, d.nof_layers, 12 * d.nof_rb
-            nd = len(ue.dmrs_symbols)
-            sym = torch.empty((P, 14, L, K), dtype=torch.int32, device="cuda")
-            ctx.check(lib.pg_pusch_symbol_estimates_device(ctx.handle, ctypes.byref(d), e.data_ptr() + 8 * d.est_offset,
-                                                           sym.data_ptr(), None))
             data_syms = [s for s in range(14) if s not in ue.dmrs_symbols]
             g = d_grid[d.grid_offset:d.grid_offset + P * 14 * d.grid_nof_subc].view(P, 14, d.grid_nof_subc)
             y = g[:, data_syms, 12 * d.rb_start:12 * d.rb_start + K].reshape(P, -1).contiguous()
-            hh = sym[:, data_syms].permute(0, 2, 1, 3).reshape(P, L, -1).contiguous()
+            words = torch.from_numpy(g_all[i].astype(np.complex64).view(np.float32).reshape(P, 14, L, K, 2))
+            hh = cbf16_words(torch, words[..., 0], words[..., 1])[:, data_syms].permute(0, 2, 1, 3)
+            hh = hh.reshape(P, L, -1).contiguous().cuda()
             nre = y.shape[1]
             eq = torch.empty((nre, L, 2), dtype=torch.float32, device="cuda")
             nv = torch.empty((nre, L), dtype=torch.float32, device="cuda")
@@ -355,11 +411,7 @@ def estimate_quality(ctx, slots, net=None, max_iterations=6):
             x = sl.symbols[slot_of[i][1]]
             err += float(np.sum(np.abs(z - x) ** 2))
             sig += float(np.sum(np.abs(x) ** 2))
-            ht = _true_dmrs_response(sl, slot_of[i][1], ue.dmrs_symbols)
-            he = e_host[d.est_offset:d.est_offset + ht.size]
-            herr += float(np.sum(np.abs(he - ht) ** 2))
-            hsig += float(np.sum(np.abs(ht) ** 2))
-        out[name] = dict(evm=math.sqrt(err / sig), nmse=herr / hsig)
+        out[name] = dict(evm=math.sqrt(err / sig), nmse=data_symbol_nmse(descs, g_all, truths))
     return out
 
 

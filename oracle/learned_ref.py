@@ -161,12 +161,19 @@ def features(seqs, rows, est, ls, noise_var, rsrp, beta):
 
 
 def refine(seqs, est, y, gains):
-    """est + correction / g at the DM-RS symbols (a copy)."""
+    """est + correction / g at the DM-RS symbols (a copy), and the time-basis coefficients
+    a_1 / g, a_2 / g (outputs 4-7) of the sequences with two DM-RS symbols in a buffer of est's
+    layout (zero elsewhere): the channel at symbol s is then h_0 + (h_1 - h_0) w + a_1 w (1 - w)
+    + a_2 w (1 - w) (2 w - 1), w = (s - d0) / (d1 - d0)."""
     out = est.copy()
+    basis = np.zeros_like(est)
     for (r0, n, e0, ds, u, p, l, nd), g in zip(seqs, gains):
         if g <= 0:
             continue
         for d in range(nd):
             c = (y[r0:r0 + n, 2 * d] + 1j * y[r0:r0 + n, 2 * d + 1]) / g
             out[e0 + d * ds:e0 + d * ds + n] += c
-    return out
+        if nd == 2:
+            for b in range(2):
+                basis[e0 + b * ds:e0 + b * ds + n] = (y[r0:r0 + n, 4 + 2 * b] + 1j * y[r0:r0 + n, 5 + 2 * b]) / g
+    return out, basis

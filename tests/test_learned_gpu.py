@@ -1,7 +1,8 @@
 """Learned channel estimator on the GPU: forward pass and gradients of the tensor-core network
 against the float64 restatement (oracle/learned_ref.py, bf16 rounding at the same points), the
-refinement path (features -> network -> corrected estimates) against the restatement, and what
-training on the GPU gains over the plain estimator."""
+refinement path (features -> network -> corrected estimates and time-basis coefficients) against
+the restatement, and what training on the GPU gains over the plain estimator on the channel at
+every data symbol of the slot."""
 import ctypes
 
 import numpy as np
@@ -91,8 +92,10 @@ def test_refine_matches_oracle(ctx, nrows):
     est_h = est.cpu().numpy().view(np.complex64).astype(np.complex128)
     ls_h = ls.cpu().numpy().view(np.complex64).astype(np.complex128)
     prh = pr.cpu().numpy().reshape(n, 4, 5)
-    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr(), use=use)
+    basis = torch.full_like(est, 7.0)
+    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr(), use=use, basis_ptr=basis.data_ptr())
     got = est.cpu().numpy().view(np.complex64).astype(np.complex128)
+    got_b = basis.cpu().numpy().view(np.complex64).astype(np.complex128)
     net.status()
     # Restatement over the used UEs only (the layout skips the others).
     sel = [i for i in range(n) if use[i]]
@@ -102,33 +105,44 @@ def test_refine_matches_oracle(ctx, nrows):
     x, valid, gains = lr.features(seqs, R, est_h, ls_h, prh[sel, :, 0], prh[sel, :, 3:5],
                                   [descs[i].dmrs_scaling for i in sel])
     y, _ = lr.forward(params.astype(np.float64), x, valid, bf16_acts=True)
-    want = lr.refine(seqs, est_h, y, gains)
+    want, want_b = lr.refine(seqs, est_h, y, gains)
     corr = want - est_h
     err = np.linalg.norm(got - want) / max(np.linalg.norm(corr), 1e-12)
     assert err < 3e-2, err
+    used = np.zeros(got.size, bool)
     for i in range(n):
+        o = descs[i].est_offset
+        m = 4 * 2 * descs[i].nof_layers * 12 * descs[i].nof_rb
         if not use[i]:
-            o = descs[i].est_offset
-            m = 4 * 2 * descs[i].nof_layers * 12 * descs[i].nof_rb
             assert np.array_equal(got[o:o + m], est_h[o:o + m])
+            assert (got_b[o:o + m] == 7 + 7j).all()      # untouched
+        else:
+            used[o:o + m] = True
+    err_b = np.linalg.norm(got_b[used] - want_b[used]) / max(np.linalg.norm(want_b[used]), 1e-12)
+    assert err_b < 3e-2, err_b
     net.close()
 
 
-def nmse(est, h_true):
-    e = est.view(-1, 2) - h_true.view(-1, 2)
-    return float((e ** 2).sum() / (h_true ** 2).sum())
+def full_grid_nmse(ctx, net, descs, est, ls, pr, h_true):
+    """(plain, learned) NMSE of the channel at the data symbols, as the demodulator uses it."""
+    import torch
+    truth = learned.split_truth(descs, h_true)
+    before = learned.data_symbol_nmse(descs, learned.grid_estimates(ctx, descs, est), truth)
+    basis = torch.zeros_like(est)
+    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr(), basis_ptr=basis.data_ptr())
+    after = learned.data_symbol_nmse(descs, learned.grid_estimates(ctx, descs, est, basis), truth)
+    net.status()
+    return before, after
 
 
 def test_training_on_gpu_beats_plain_estimator(ctx):
     """A short training run on the GPU (the library's own forward/backward kernels and Adam)
-    lowers the channel-estimate error below the plain estimator's on held-out batches."""
+    lowers the error of the channel at the data symbols below the plain estimator's on held-out
+    batches."""
     net, hist = learned.train(ctx, steps=400, rows_per_step=40_000, seed=1, lr=1e-3, log_every=100, verbose=False)
     assert hist[-1][1] < hist[0][1]
     descs, est, ls, pr, h_true = make_batch(ctx, 999, 60_000)
-    before = nmse(est, h_true)
-    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
-    after = nmse(est, h_true)
-    net.status()
+    before, after = full_grid_nmse(ctx, net, descs, est, ls, pr, h_true)
     assert after < 0.9 * before, (before, after)
     net.close()
 
@@ -142,9 +156,6 @@ def test_committed_weights_gain_over_plain(ctx):
     descs, est, ls, pr, h_true = make_batch(ctx, 4242, 80_000)
     rows = int(ctx.lib.pg_le_rows(ctypes.addressof(descs), len(descs)))
     net = learned.LearnedEstimator(ctx, max_rows=rows, params=params)
-    before = nmse(est, h_true)
-    net.refine(descs, ls.data_ptr(), est.data_ptr(), pr.data_ptr())
-    after = nmse(est, h_true)
-    net.status()
+    before, after = full_grid_nmse(ctx, net, descs, est, ls, pr, h_true)
     assert after < 0.7 * before, (before, after)
     net.close()

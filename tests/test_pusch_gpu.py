@@ -67,7 +67,7 @@ def test_symbol_estimates_match_reference_bf16(ctx):
         nl, nsc = c["nof_layers"], 12 * c["nof_rb"]
         d_sym = torch.zeros(c["ports"] * 14 * nl * nsc, dtype=torch.int32, device="cuda")
         s = torch.cuda.current_stream()
-        rc = ctx.lib.pg_pusch_symbol_estimates_device(ctx.handle, ctypes.addressof(descs), d_est.data_ptr(),
+        rc = ctx.lib.pg_pusch_symbol_estimates_device(ctx.handle, ctypes.addressof(descs), d_est.data_ptr(), None,
                                                       d_sym.data_ptr(), s.cuda_stream)
         ctx.check(rc)
         s.synchronize()
