@@ -744,8 +744,14 @@ int pg_port_channel_estimate_host(pg_context* ctx, const pg_port_estimate_cfg* c
   ue.nof_layers        = cfg->nof_layers;
   ue.modulation_order  = 2;
   ue.dc_subcarrier     = -1;
-  if (int rc = validate_ues(ctx, &ue, 1)) {
-    return rc;
+  {
+    // One receive port is estimated whatever the layer count: validate the allocation as if the
+    // UE had enough ports for its layers.
+    pg_pusch_ue chk  = ue;
+    chk.nof_rx_ports = 4;
+    if (int rc = validate_ues(ctx, &chk, 1)) {
+      return rc;
+    }
   }
   int       d0 = 0, d1 = 0;
   const int nd   = dmrs_count(ue, &d0, &d1);

@@ -272,19 +272,18 @@ def train(ctx, steps=3000, rows_per_step=96_000, seed=0, lr=1e-3, lr_min=2e-5, l
 
 EVAL_DELAY_NS = (30.0, 300.0)
 EVAL_DOPPLER_HZ = (0.0, 500.0)
+EVAL_MARGINS_DB = (0.0, 2.0, 4.0, 6.0, 8.0)
+EVAL_BLER_TARGET = 0.1
+SLOT_S = 0.5e-3
 
 
-EVAL_LA_MARGIN_DB = 4.0
-
-
-def eval_slots(snr_db, seed=0, cells=4):
+def eval_slots(snr_db, seed=0, cells=4, la_margin_db=4.0):
     """Uneven slots (sim.uneven_cells) with every UE at snr_db, RMS delay spread U[30, 300] ns and
-    maximum Doppler U[0, 500] Hz; the link adaptation of sim.uneven_cells with a margin of
-    EVAL_LA_MARGIN_DB for these harder channels (its thresholds are calibrated on 100 ns without
-    Doppler)."""
+    maximum Doppler U[0, 500] Hz; the link adaptation of sim.uneven_cells with its thresholds
+    raised by la_margin_db (they are calibrated on 100 ns without Doppler)."""
     from . import sim
     return sim.uneven_cells(seed, nof_cells=cells, snr_range=(snr_db, snr_db), delay_range_ns=EVAL_DELAY_NS,
-                            doppler_range_hz=EVAL_DOPPLER_HZ, la_margin_db=EVAL_LA_MARGIN_DB)
+                            doppler_range_hz=EVAL_DOPPLER_HZ, la_margin_db=la_margin_db)
 
 
 def tb_errors(results, truths):
@@ -415,29 +414,61 @@ def estimate_quality(ctx, slots, net=None, max_iterations=6):
     return out
 
 
-def evaluate(ctx, net, snrs_db, seed=0, cells=4, max_iterations=6, verbose=True):
-    """Per SNR: BLER (TB CRC and payload against the transmitted bits) of the slot plan with the
-    plain and with the learned estimator, EVM and channel NMSE of both."""
+def run_plan(ctx, slots, net, max_iterations):
+    """(TB error flags, decoded bits) of every UE of the slots through a slot plan, with the plain
+    estimator (net None) or the learned one."""
     from .pusch import PuschSlotPlan
+    truths = [t for sl in slots for t in sl.truth]
+    plan = PuschSlotPlan(ctx, slots, max_iterations=max_iterations)
+    if net is not None:
+        plan.set_learned(net)
+    err = tb_errors(plan.execute_host(), truths)
+    if net is not None:
+        plan.set_learned(None)
+    plan.close()
+    bits = sum(len(t) for t, e in zip(truths, err) if not e)
+    return err, bits
+
+
+def la_point(per_margin, key):
+    """Outer-loop link adaptation: the smallest margin whose BLER is at most EVAL_BLER_TARGET (the
+    largest margin when none is)."""
+    for m in per_margin:
+        if m["bler_" + key] <= EVAL_BLER_TARGET:
+            return m
+    return per_margin[-1]
+
+
+def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, margins_db=EVAL_MARGINS_DB, verbose=True):
+    """Per SNR and link-adaptation margin: BLER (TB CRC and payload against the transmitted bits)
+    of the slot plan with the plain and with the learned estimator on the same slots, and the
+    decoded Mbit/s per cell. Each estimator then gets its own margin, the smallest with BLER at
+    most 10 % (outer-loop link adaptation), and its goodput there; EVM and data-symbol channel
+    NMSE of both at the plain estimator's margin."""
     rows = []
     for k, snr in enumerate(snrs_db):
-        slots = eval_slots(snr, seed + k, cells)
-        truths = [t for sl in slots for t in sl.truth]
-        plan = PuschSlotPlan(ctx, slots, max_iterations=max_iterations)
-        bl_p = tb_errors(plan.execute_host(), truths)
-        plan.set_learned(net)
-        bl_l = tb_errors(plan.execute_host(), truths)
-        plan.set_learned(None)
-        plan.close()
-        q = estimate_quality(ctx, slots, net, max_iterations)
-        row = dict(snr_db=float(snr), ues=len(truths), bler_plain=float(np.mean(bl_p)), bler_learned=float(np.mean(bl_l)),
+        per_margin = []
+        for m in margins_db:
+            slots = eval_slots(snr, seed + k, cells, la_margin_db=m)
+            e_p, b_p = run_plan(ctx, slots, None, max_iterations)
+            e_l, b_l = run_plan(ctx, slots, net, max_iterations)
+            per_margin.append(dict(margin_db=float(m), ues=len(e_p), bler_plain=float(np.mean(e_p)),
+                                   bler_learned=float(np.mean(e_l)),
+                                   mbps_plain=b_p / (cells * SLOT_S) / 1e6, mbps_learned=b_l / (cells * SLOT_S) / 1e6))
+        lp, ll = la_point(per_margin, "plain"), la_point(per_margin, "learned")
+        q = estimate_quality(ctx, eval_slots(snr, seed + k, cells, la_margin_db=lp["margin_db"]), net,
+                             max_iterations)
+        row = dict(snr_db=float(snr), ues=lp["ues"], margin_plain=lp["margin_db"], margin_learned=ll["margin_db"],
+                   bler_plain=lp["bler_plain"], bler_learned_same_mcs=lp["bler_learned"],
+                   bler_learned=ll["bler_learned"], mbps_plain=lp["mbps_plain"], mbps_learned=ll["mbps_learned"],
                    evm_plain=q["plain"]["evm"], evm_learned=q["learned"]["evm"], nmse_plain=q["plain"]["nmse"],
-                   nmse_learned=q["learned"]["nmse"])
+                   nmse_learned=q["learned"]["nmse"], per_margin=per_margin)
         rows.append(row)
         if verbose:
-            print(("SNR {snr_db:4.1f} dB  UEs {ues:3d}  BLER plain {bler_plain:.3f} learned {bler_learned:.3f}  "
-                   "EVM plain {evm_plain:.4f} learned {evm_learned:.4f}  NMSE plain {nmse_plain:.5f} "
-                   "learned {nmse_learned:.5f}").format(**row), flush=True)
+            print(("SNR {snr_db:4.1f} dB  UEs {ues:3d}  plain: margin {margin_plain:.0f} BLER {bler_plain:.3f} "
+                   "{mbps_plain:7.1f} Mbit/s  learned: same-MCS BLER {bler_learned_same_mcs:.3f}, margin "
+                   "{margin_learned:.0f} BLER {bler_learned:.3f} {mbps_learned:7.1f} Mbit/s  EVM {evm_plain:.4f}/"
+                   "{evm_learned:.4f}  NMSE {nmse_plain:.5f}/{nmse_learned:.5f}").format(**row), flush=True)
     return rows
 
 
@@ -454,10 +485,11 @@ def main(argv=None):
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--time-budget", type=float, default=None, help="stop after this many seconds")
     t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--init", default=None, help="start from the parameters in this file (default: fresh)")
     e = sub.add_parser("evaluate", help="BLER / EVM / NMSE of the plain and learned estimators per SNR")
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--snrs", default="0:30:2", help="first:last:step in dB")
-    e.add_argument("--cells", type=int, default=4)
+    e.add_argument("--cells", type=int, default=48, help="cells per SNR point and margin (about 10 UEs each)")
     e.add_argument("--seed", type=int, default=100)
     e.add_argument("--json", default=None)
     tm = sub.add_parser("time", help="time pg_le_refine_device on a batch of the training source")
@@ -493,7 +525,11 @@ def main(argv=None):
         net.close()
     elif a.cmd == "train":
         t0 = time.time()
-        net, hist = train(ctx, steps=a.steps, rows_per_step=a.rows, seed=a.seed, lr=a.lr, time_budget_s=a.time_budget)
+        init = load_params(a.init) if a.init else None
+        if a.init and init is None:
+            raise SystemExit(f"no parameters at {a.init}")
+        net, hist = train(ctx, steps=a.steps, rows_per_step=a.rows, seed=a.seed, lr=a.lr, time_budget_s=a.time_budget,
+                          params=init)
         ues_seen = hist[-1][0] * a.rows / (4 * 1.5 * 12 * 92)
         net.save(a.out, history=np.array(hist), steps=hist[-1][0], rows_per_step=a.rows, seed=a.seed,
                  train_seconds=time.time() - t0)

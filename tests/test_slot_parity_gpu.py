@@ -118,13 +118,25 @@ def per_modulation(c, diff):
     return {qm: np.concatenate(v) for qm, v in out.items()}
 
 
+# Largest LLR difference of the whole front end per modulation order. The GPU estimator's FP32
+# responses differ from the reference's in the last bits (summation order), so after the bf16
+# rounding of the per-symbol estimates a small fraction of the channel coefficients are one bf16
+# unit (2^-8 relative) apart; a 256QAM LLR that is not saturated moves by a few LSB with such a
+# coefficient (slope up to 8/sqrt(170) per 1/noise variance at 25 dB, 6 LSB per LLR unit). With the
+# reference's own estimates the demodulator is within +-1 LSB for every order
+# (test_fused_demodulator_on_reference_estimates).
+FRONT_END_MAX_DIFF = {2: 1, 4: 1, 6: 2, 8: 8}
+
+
 def test_front_end_llrs_match_reference(ctx, slot_case):
     c, r = slot_case, slot_case["ref"]
     got = gpu_front_end(ctx, c)
     diff = np.abs(got - r["llrs"][:c["nllr"]].astype(np.int16))
     for qm, d in per_modulation(c, diff).items():
-        assert d.max() <= 1, (c["name"], qm, int(d.max()))
-        assert (d == 0).mean() > 0.99, (c["name"], qm, float((d == 0).mean()))
+        stats = (c["name"], qm, int(d.max()), float((d == 0).mean()), float((d <= 1).mean()))
+        assert d.max() <= FRONT_END_MAX_DIFF[qm], stats
+        assert (d == 0).mean() > 0.99, stats
+        assert (d <= 1).mean() > 0.9999, stats
 
 
 def test_fused_demodulator_on_reference_estimates(ctx, ref, slot_case):
