@@ -142,13 +142,20 @@ enum pg_ldpc_kernel {
   PG_LDPC_KERNEL_ONE_LANE  = 0, /* 384 threads per codeblock, one lifted lane per thread, two CTAs per SM */
   PG_LDPC_KERNEL_TWO_LANES = 1, /* 192 threads per codeblock; even Z > 192: two lanes per thread as f16x2
                                    halves; four CTAs per SM */
-  PG_LDPC_KERNEL_SPLIT     = 2  /* 384 threads per codeblock; even Z > 192: two lanes per thread pair, each
+  PG_LDPC_KERNEL_SPLIT     = 2, /* 384 threads per codeblock; even Z > 192: two lanes per thread pair, each
                                    row's edges split between the two threads; two CTAs per SM */
+  PG_LDPC_KERNEL_Z384      = 3  /* 192 threads per codeblock; Z = 384 with the edge tables fixed at compile
+                                   time and f16 soft-bit pairs stored once, other Z as TWO_LANES; four
+                                   CTAs per SM */
 };
 
 /* Selects the kernel of the context's batch decodes (pg_ldpc_decode_batch_{host,device,resident}
  * and pg_sch_decode_batch_host); slot plans choose theirs through their tuning. */
 int pg_set_ldpc_kernel(pg_context* ctx, int kernel);
+/* Resident CTAs per SM of the context's batch decodes (1-4, capped by the kernel's own limit; 0:
+ * the kernel's limit, the default). Fewer CTAs than codeblocks make the persistent CTAs share the
+ * codeblocks dynamically; more make every codeblock start at once. */
+int pg_set_ldpc_ctas_per_sm(pg_context* ctx, int ctas_per_sm);
 
 
 /* ---------------------------------------------------------------------------------------- */

@@ -1110,6 +1110,386 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& s
   __syncthreads();
 }
 
+// ---------------------------------------------------------------------------------------------
+// Lifting size 384 (every large transport block): the two-lanes-per-thread arithmetic above with
+// everything that depends on Z fixed at compile time and the soft bits stored once, as f16.
+//
+// Thread j (0 <= j < 192) carries check lanes j and j + 192. Soft bits: E[col][k] = (soft[col][k],
+// soft[col][k + 192]) as one f16x2 word, 0 <= k < 192 (52 KB for BG1, so four CTAs share an SM).
+// For an edge of shift s, lane j reads variable lane (j + s) mod 384 and lane j + 192 reads
+// (j + 192 + s) mod 384: both are halves of the same word k = (j + s') mod 192 with s' = s mod 192,
+// swapped when (j + s' >= 192) differs from (s >= 192). Per edge the constant tables give 4 s', the
+// column's byte offset and the byte-permute selector of the wrapped case (c_z_*, set for Z = 384
+// at table upload); the selector of the unwrapped case differs from it by 0x2222.
+// The 0.8 scaling, floor(m * 52428 / 2^16) for integer 0 <= m <= 120, is
+// max(fma(m, f16(0.8), 1023.5) - 1024, 0) in f16: the fused multiply-add rounds once, to an integer
+// (the spacing of f16 in [1024, 2048)), and f16(0.8) = 0.7998046875 errs by at most 0.024 at
+// m = 120, inside the 0.1 margin of every rounding decision (checked for every m).
+constexpr int kZ384      = 384;
+constexpr int kZH        = 192;
+constexpr int kZThreads  = 192;
+constexpr int kZMaxPerSm = 4;
+constexpr int kZ19Keep   = 8; // v2c kept in registers for the degree-19 rows
+
+__constant__ uint32_t c_z_sp4[2][pg::kBg1Edges]; // 4 (s mod 192)
+__constant__ uint32_t c_z_col[2][pg::kBg1Edges]; // byte offset of the edge's column in E
+__constant__ uint32_t c_z_sel[2][pg::kBg1Edges]; // selector when j + s' >= 192
+
+struct __align__(16) smem_z_t {
+  uint32_t E[pg::kMaxNodes * kZH];
+  uint32_t hard[(22 * kZ384) / 32];
+  uint32_t red[kZThreads / 32];
+  int      s_last;
+  int      s_done;
+};
+
+constexpr uint32_t kH0p8     = 0x3a663a66u; // f16(0.8) = 0.7998046875
+constexpr uint32_t kH1023p5  = 0x63ff63ffu; // 1023.5
+constexpr uint32_t kHm1024   = 0xe400e400u; // -1024
+
+__device__ __forceinline__ uint32_t z_scale(uint32_t m)
+{
+  return h2_max(h2_add(h2_fma(m, kH0p8, kH1023p5), kHm1024), 0u);
+}
+
+__device__ __forceinline__ uint32_t lds_u32(const unsigned char* base, uint32_t off)
+{
+  return *reinterpret_cast<const uint32_t*>(base + off);
+}
+__device__ __forceinline__ void sts_u32(unsigned char* base, uint32_t off, uint32_t v)
+{
+  *reinterpret_cast<uint32_t*>(base + off) = v;
+}
+
+// Byte offset in E and byte-permute selector of edge e (global edge index) for thread j (j4 = 4 j).
+__device__ __forceinline__ void z_edge(const int g, const int e, const uint32_t j4, uint32_t& adr, uint32_t& sel)
+{
+  const uint32_t t4 = j4 + c_z_sp4[g][e];
+  const uint32_t k4 = __viaddmin_u32(t4, 0u - 4u * kZH, t4); // (j + s') mod 192, times 4
+  const uint32_t sw = c_z_sel[g][e];
+  sel               = k4 == t4 ? sw ^ 0x2222u : sw;
+  adr               = k4 + c_z_col[g][e];
+}
+
+// One layer (base-graph row of degree DEG, first edge e0) for thread j. Rows of degree up to ten
+// keep each edge's v2c, address and selector from the first pass; the degree-19 rows keep the
+// v2c of their first NV edges and recompute the rest (the soft bits and messages they read are
+// not yet overwritten), so that four CTAs fit an SM without spills.
+template <int DEG, bool FIRST>
+__device__ __forceinline__ void row_update_z(const int g, const int e0, const uint32_t j4, unsigned char* E,
+                                             uint16_t* __restrict__ c2v_row)
+{
+  constexpr bool KEEP = DEG <= 10;
+  constexpr int  NV   = KEEP ? DEG : kZ19Keep;
+  uint32_t       v[NV];
+  uint32_t       adr[KEEP ? DEG : 1], sel[KEEP ? DEG : 1];
+  uint32_t       min1 = kH120, min2 = kH120;
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    uint32_t a, s;
+    z_edge(g, e0 + e, j4, a, s);
+    if constexpr (KEEP) {
+      adr[e] = a;
+      sel[e] = s;
+    }
+    const uint32_t vv = pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+    if (e < NV) {
+      v[e < NV ? e : 0] = vv;
+    }
+    const uint32_t t  = h2_max_xs(min1, vv);
+    min2              = h2_min_xs(min2, t);
+    min1              = h2_min_xs(min1, vv);
+  }
+  const uint32_t m1  = min1 & kAbs;
+  const uint32_t s1  = z_scale(m1);
+  const uint32_t s2  = z_scale(min2 & kAbs);
+  const uint32_t nds = h2_sub(s1, s2);
+  const uint32_t sgn = min1 & kSign; // sign product of every v2c of the row
+#pragma unroll
+  for (int e = 0; e < DEG; ++e) {
+    uint32_t a, s;
+    if constexpr (KEEP) {
+      a = adr[e];
+      s = sel[e];
+    } else {
+      z_edge(g, e0 + e, j4, a, s);
+    }
+    const uint32_t vv  = e < NV ? v[e < NV ? e : 0]
+                                : pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+    const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
+    const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
+    c2v_row[e * kZThreads] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+    const uint32_t tt  = h2_add(c, vv);
+    const uint32_t cl  = h2_min(h2_max(tt, kHm120), kH120);
+    uint32_t       u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
+    u                  = h2_min(h2_max(u, kHm127), kH127);
+    sts_u32(E, a, __byte_perm(u, 0, s));
+  }
+}
+
+template <bool FIRST>
+__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint16_t* c2v_row)
+{
+  switch (deg) {
+    case 3: row_update_z<3, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 4: row_update_z<4, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 5: row_update_z<5, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 6: row_update_z<6, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 7: row_update_z<7, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 8: row_update_z<8, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 9: row_update_z<9, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 10: row_update_z<10, FIRST>(g, e0, j4, E, c2v_row); break;
+    default: row_update_z<19, FIRST>(g, e0, j4, E, c2v_row); break;
+  }
+}
+
+// f16 soft bit -> hard bit: soft <= 0 (either zero counts as 0).
+__device__ __forceinline__ bool z_hard(uint32_t h)
+{
+  return (h & 0x8000u) != 0 || (h & 0x7fffu) == 0;
+}
+
+// Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`.
+__device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const int8_t* __restrict__ llrs,
+                                      uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
+                                      int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow, const int cb,
+                                      const int slab)
+{
+  const int tid = threadIdx.x;
+  const int bg  = d.base_graph;
+  if (bg != 1 && bg != 2) {
+    if (tid == 0) {
+      iterations[cb] = -1;
+    }
+    return;
+  }
+  const int      g        = bg - 1;
+  const int      Kb       = bg == 1 ? 22 : 10;
+  const int      nrows    = bg == 1 ? pg::kBg1Rows : pg::kBg2Rows;
+  const int      nfull    = bg == 1 ? 68 : 52;
+  const int      msg_len  = Kb * kZ384;
+  const int      n        = (int)d.nof_llrs;
+  const int8_t*  in       = llrs + d.llr_offset;
+  uint16_t*      c2v      = reinterpret_cast<uint16_t*>(c2v_all + (size_t)slab * pg::kC2vStride);
+  const int      nbytes   = msg_len / 8;
+  uint8_t*       out      = bits + d.out_offset;
+  const int      crc_poly = d.crc_poly;
+  const int      nwords   = msg_len / 32;
+  unsigned char* E        = reinterpret_cast<unsigned char*>(sm.E);
+  const uint32_t j4       = 4u * (uint32_t)tid;
+
+  if (tid == 0) {
+    sm.s_last = 0;
+    sm.s_done = 0;
+  }
+  __syncthreads();
+
+  // Soft bits as f16 pairs, eight pairs per thread step (2Z punctured zeros, then the input).
+  {
+    constexpr int per_col  = kZH / 8;
+    const int     nchunks  = nfull * per_col;
+    const int     nof_full = (n / kZ384) * kZ384;
+    const bool    aligned  = (reinterpret_cast<uintptr_t>(in) & 7u) == 0;
+    int           last     = 0;
+#pragma unroll 2
+    for (int q = tid; q < nchunks; q += kZThreads) {
+      const int col = q / per_col;
+      const int w0  = (q - col * per_col) * 8;
+      const int k   = (col - 2) * kZ384 + w0;
+      uint32_t  l0, l1, h0, h1;
+      fetch8(in, k, n, nof_full, aligned, last, l0, l1);
+      fetch8(in, k + kZH, n, nof_full, aligned, last, h0, h1);
+      const uint32_t p0 = __byte_perm(l0, h0, 0x5140), p1 = __byte_perm(l0, h0, 0x7362);
+      const uint32_t p2 = __byte_perm(l1, h1, 0x5140), p3 = __byte_perm(l1, h1, 0x7362);
+      uint4          a, b;
+      a.x = bytes_to_h2(p0);
+      a.y = bytes_to_h2(p0 >> 16);
+      a.z = bytes_to_h2(p1);
+      a.w = bytes_to_h2(p1 >> 16);
+      b.x = bytes_to_h2(p2);
+      b.y = bytes_to_h2(p2 >> 16);
+      b.z = bytes_to_h2(p3);
+      b.w = bytes_to_h2(p3 >> 16);
+      *reinterpret_cast<uint4*>(sm.E + col * kZH + w0)     = a;
+      *reinterpret_cast<uint4*>(sm.E + col * kZH + w0 + 4) = b;
+    }
+    last = warp_max(last);
+    if ((tid & 31) == 0 && last > 0) {
+      atomicMax(&sm.s_last, last);
+    }
+  }
+  __syncthreads();
+
+  const int input_size = sm.s_last;
+  if (input_size < msg_len) {
+    for (int b = tid; b < nbytes; b += kZThreads) {
+      out[b] = 0xff;
+    }
+    if (tid == 0) {
+      iterations[cb] = 0;
+    }
+    __syncthreads();
+    return;
+  }
+  int cb_len = max(input_size + 2 * kZ384, (Kb + 4) * kZ384);
+  cb_len     = ((cb_len + kZ384 - 1) / kZ384) * kZ384;
+  const int nof_layers = min(cb_len / kZ384 - Kb, nrows);
+
+  int order = 24;
+  if (crc_poly == PG_CRC16) {
+    order = 16;
+  }
+  const uint32_t* pow_tab = crc_pow + (size_t)(crc_poly <= PG_CRC24B ? crc_poly : 0) * pg::kCrcPowLen;
+  const int       crc_len = msg_len - (int)d.nof_filler_bits;
+
+  int       result = 0;
+  const int max_it = d.max_iterations;
+  const int lane   = tid & 31;
+  const int nsteps = steps_for_layers(g, nof_layers);
+  for (int it = 0; it < max_it; ++it) {
+    for (int st = 0; st < nsteps; ++st) {
+      if (it > 0 || st + 1 == nsteps) {
+        prefetch_step(g, st + 1 < nsteps ? st + 1 : 0, nof_layers, tid, reinterpret_cast<const char*>(c2v),
+                      kZThreads * 2);
+      }
+      const int r0 = c_step_row0[g][st];
+      const int r1 = min(r0 + (int)c_step_nrows[g][st], nof_layers);
+      for (int r = r0; r < r1; ++r) {
+        const int deg     = c_row_deg[g][r];
+        const int e0      = c_row_e0[g][r];
+        uint16_t* c2v_row = c2v + (size_t)e0 * kZThreads + tid;
+        if (it == 0) {
+          row_dispatch_z<true>(deg, g, e0, j4, E, c2v_row);
+        } else {
+          row_dispatch_z<false>(deg, g, e0, j4, E, c2v_row);
+        }
+      }
+      __syncthreads();
+    }
+
+    // Hard decisions (soft <= 0), zero check and CRC: one 32-bit word per warp step, lane k
+    // holding bit 32 wi + k (MSB first after the reversal); message bit i of column c = i / 384,
+    // lane w = i mod 384 is half (w >= 192) of E[c][w mod 192].
+    int      zero = 0;
+    uint32_t crc  = 0;
+    for (int wi = tid >> 5; wi < nwords; wi += kZThreads / 32) {
+      const int      idx = 32 * wi + lane;
+      const int      col = idx / kZ384;
+      const int      w   = idx - col * kZ384;
+      const uint32_t x   = sm.E[col * kZH + (w < kZH ? w : w - kZH)];
+      const uint32_t h   = w < kZH ? (x & 0xffffu) : (x >> 16);
+      const bool     bit = z_hard(h);
+      zero |= (h & 0x7fffu) == 0;
+      const uint32_t wd = __brev(__ballot_sync(0xffffffffu, bit));
+      if (lane == 0) {
+        sm.hard[wi] = wd;
+      }
+      if (crc_poly != PG_CRC_NONE && bit && idx < crc_len) {
+        crc ^= __ldg(pow_tab + (crc_len - 1 - idx + order));
+      }
+    }
+    zero = __syncthreads_or(zero);
+    crc  = warp_xor(crc);
+    if (lane == 0) {
+      sm.red[tid >> 5] = crc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < kZThreads / 32; ++w) {
+        t ^= sm.red[w];
+      }
+      sm.s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
+    }
+    __syncthreads();
+    if (sm.s_done) {
+      result = it + 1;
+      break;
+    }
+  }
+
+  if (crc_poly == PG_CRC_NONE) {
+    // Syndrome check over the processed rows (ldpc_decoder_impl.cpp:329-387), both lanes.
+    int bad = 0;
+    int e0  = 0;
+    for (int r = 0; r < nof_layers; ++r) {
+      const int deg    = c_row_deg[g][r];
+      uint32_t  parity = 0;
+      for (int e = 0; e < deg; ++e) {
+        uint32_t a, s;
+        z_edge(g, e0 + e, j4, a, s);
+        const uint32_t x  = __byte_perm(lds_u32(E, a), 0, s);
+        const uint32_t lo = x & 0xffffu, hi = x >> 16;
+        bad |= ((lo & 0x7fffu) == 0) | ((hi & 0x7fffu) == 0);
+        parity ^= (uint32_t)z_hard(lo) | ((uint32_t)z_hard(hi) << 1);
+      }
+      bad |= parity != 0;
+      e0 += deg;
+    }
+    bad      = __syncthreads_or(bad);
+    int zero = 0;
+    for (int i = tid; i < msg_len; i += kZThreads) {
+      const int      col = i / kZ384;
+      const int      w   = i - col * kZ384;
+      const uint32_t x   = sm.E[col * kZH + (w < kZH ? w : w - kZH)];
+      zero |= (((w < kZH ? x : x >> 16) & 0x7fffu) == 0);
+    }
+    zero   = __syncthreads_or(zero);
+    result = (!bad && !zero) ? max_it : 0;
+  }
+
+  for (int b = tid; b < nbytes; b += kZThreads) {
+    out[b] = (uint8_t)(sm.hard[b >> 2] >> (24 - 8 * (b & 3)));
+  }
+  if (tid == 0) {
+    iterations[cb] = result;
+  }
+  __syncthreads();
+}
+
+constexpr size_t kZSmem = sizeof(smem_z_t) > kX2Smem ? sizeof(smem_z_t) : kX2Smem;
+
+// Persistent decoder of a work list, every lifting size: Z = 384 through decode_codeblock_z384,
+// other even Z > 192 in pair mode, Z <= 192 with the one-lane arithmetic (192 threads, four CTAs
+// per SM).
+__global__ void __launch_bounds__(kZThreads, kZMaxPerSm) ldpc_decode_z_kernel(const pg_ldpc_cb* __restrict__ descs,
+                                                                      const int8_t* __restrict__ llrs,
+                                                                      uint8_t* __restrict__ bits,
+                                                                      int32_t* __restrict__ iterations,
+                                                                      int8_t* __restrict__ c2v_all,
+                                                                      const uint32_t* __restrict__ crc_pow,
+                                                                      const uint16_t* __restrict__ scale_tab,
+                                                                      const uint32_t* __restrict__ order, int n,
+                                                                      int* __restrict__ counter)
+{
+  extern __shared__ __align__(16) unsigned char smem_z_raw[];
+  __shared__ int s_work;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_work = atomicAdd(counter, 1);
+    }
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= n) {
+      break;
+    }
+    const int        cb = order != nullptr ? (int)order[w] : w;
+    const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size == kZ384) {
+      decode_codeblock_z384(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), llrs, bits, iterations, c2v_all, crc_pow, cb,
+                            blockIdx.x);
+    } else if (d.lifting_size > kX2Threads) {
+      decode_codeblock_pair<kX2Threads, 1>(d, *reinterpret_cast<smem_pair_t*>(smem_z_raw), llrs, bits, iterations,
+                                           c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
+    } else {
+      decode_codeblock<0, kX2Threads, kX2Threads>(d, *reinterpret_cast<smem_x2_scalar_t*>(smem_z_raw), llrs, bits,
+                                                  iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      __syncthreads();
+    }
+  }
+}
+
 // Persistent decoder of a work list, every lifting size: each CTA takes the next work index from
 // *counter, decodes codeblock order[w] (or w) in pair mode (even Z > 192) or scalar mode (Z <= 192)
 // with slab blockIdx.x, and stops when the n codeblocks are taken.
@@ -1239,7 +1619,35 @@ int ldpc_upload_tables(pg_context* ctx)
     const uint16_t key = __half_as_ushort(__float2half_rn((float)m)) >> 4;
     scale[key]         = __half_as_ushort(__float2half_rn((float)((m * 52428) >> 16)));
   }
+  // Edge tables of the Z = 384 decoder (lifting set index 1): 4 (s mod 192), the column's byte
+  // offset in the f16-pair soft bits and the byte-permute selector of the wrapped case (halves
+  // swapped unless s >= 192).
+  uint32_t z_sp4[2][kBg1Edges] = {}, z_col[2][kBg1Edges] = {}, z_sel[2][kBg1Edges] = {};
+  for (int gi = 0; gi < 2; ++gi) {
+    const int ne = gi == 0 ? PG_BG1_EDGES : PG_BG2_EDGES;
+    for (int e = 0; e < ne; ++e) {
+      const uint32_t s = (uint32_t)v[gi][e][1] % (uint32_t)kZ384;
+      z_sp4[gi][e]     = 4u * (s % (uint32_t)kZH);
+      z_col[gi][e]     = 4u * (uint32_t)kZH * col[gi][e];
+      z_sel[gi][e]     = s >= (uint32_t)kZH ? 0x3210u : 0x1032u;
+    }
+  }
   int rc = check_cuda(ctx, cudaMemcpyToSymbol(c_edge_col, col, sizeof(col)), "cudaMemcpyToSymbol(edge_col)");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_z_sp4, z_sp4, sizeof(z_sp4)), "cudaMemcpyToSymbol(z_sp4)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_z_col, z_col, sizeof(z_col)), "cudaMemcpyToSymbol(z_col)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyToSymbol(c_z_sel, z_sel, sizeof(z_sel)), "cudaMemcpyToSymbol(z_sel)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaFuncSetAttribute(ldpc_decode_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kZSmem),
+                    "cudaFuncSetAttribute(ldpc_decode_z_kernel)");
+  }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_scale, sizeof(scale)), "cudaMalloc(scale table)");
   }
@@ -1355,8 +1763,9 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
                            int32_t* iterations, int8_t* c2v, const uint32_t* order, int* counter,
                            cudaStream_t stream)
 {
+  const int per_sm = ctx->ldpc_ctas_per_sm > 0 ? ctx->ldpc_ctas_per_sm : kX2MaxPerSm;
   return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, counter, stream,
-                                kX2MaxPerSm * ctx->sm_count, PG_LDPC_KIND_ALL | ldpc_route(ctx->ldpc_kernel));
+                                per_sm * ctx->sm_count, PG_LDPC_KIND_ALL | ldpc_route(ctx->ldpc_kernel));
 }
 
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
@@ -1373,12 +1782,19 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
+  // PG_LDPC_ROUTE_Z: the Z = 384 kernel (four per SM, pair mode and one-lane arithmetic for the
+  // other lifting sizes);
   // PG_LDPC_ROUTE_SPLIT: the split kernel decodes every codeblock (two CTAs per SM);
   // PG_LDPC_ROUTE_X2: the two-lanes-per-thread kernel (four per SM); neither: ldpc_decode_kernel
   // (two per SM). The caller provides a slab per CTA (min(n, max_ctas) slabs, max_ctas <= four
   // per SM).
   int rc = PG_OK;
-  if (kinds & PG_LDPC_ROUTE_SPLIT) {
+  if (kinds & PG_LDPC_ROUTE_Z) {
+    const int grid_z = std::max(1, std::min(n, std::min(max_ctas, kZMaxPerSm * ctx->sm_count)));
+    ldpc_decode_z_kernel<<<grid_z, kZThreads, kZSmem, stream>>>(
+        descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
+    rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_z_kernel launch");
+  } else if (kinds & PG_LDPC_ROUTE_SPLIT) {
     const int grid_s = std::max(1, std::min(n, std::min(max_ctas, kSplitMaxPerSm * ctx->sm_count)));
     ldpc_decode_split_kernel<<<grid_s, kSplitThreads, kSplitSmem, stream>>>(
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);

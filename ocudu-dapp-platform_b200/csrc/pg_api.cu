@@ -510,10 +510,22 @@ int pg_set_ldpc_kernel(pg_context* ctx, int kernel)
   if (ctx == nullptr) {
     return PG_ERR_INVALID;
   }
-  if (kernel < PG_LDPC_KERNEL_ONE_LANE || kernel > PG_LDPC_KERNEL_SPLIT) {
+  if (kernel < PG_LDPC_KERNEL_ONE_LANE || kernel > PG_LDPC_KERNEL_Z384) {
     return set_error(ctx, PG_ERR_INVALID, "unknown LDPC kernel " + std::to_string(kernel));
   }
   ctx->ldpc_kernel = kernel;
+  return PG_OK;
+}
+
+int pg_set_ldpc_ctas_per_sm(pg_context* ctx, int ctas_per_sm)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (ctas_per_sm < 0 || ctas_per_sm > 4) {
+    return set_error(ctx, PG_ERR_INVALID, "LDPC CTAs per SM must be 0-4, not " + std::to_string(ctas_per_sm));
+  }
+  ctx->ldpc_ctas_per_sm = ctas_per_sm;
   return PG_OK;
 }
 

@@ -95,6 +95,7 @@ struct pg_context {
   bool                timed          = false;
   int8_t*             static_c2v     = nullptr;  // device address of the module-static LDPC scratch
   int                 ldpc_kernel    = PG_LDPC_KERNEL_SPLIT; // kernel of the batch decodes (pg_ldpc_kernel)
+  int                 ldpc_ctas_per_sm = 0;   // resident CTAs per SM of the batch decodes (0: kernel limit)
   std::string         last_error;
 };
 
@@ -202,11 +203,21 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
 // Kinds of codeblocks a work list may hold: Z = 384 (two-lanes-per-thread decoder) and others.
 // PG_LDPC_ROUTE_X2 routes the Z = 384 codeblocks to the two-lanes-per-thread decoder; without it
 // ldpc_decode_kernel decodes every codeblock.
-enum { PG_LDPC_KIND_OTHER = 1, PG_LDPC_KIND_Z384 = 2, PG_LDPC_KIND_ALL = 3, PG_LDPC_ROUTE_X2 = 4, PG_LDPC_ROUTE_SPLIT = 8 };
+enum {
+  PG_LDPC_KIND_OTHER  = 1,
+  PG_LDPC_KIND_Z384   = 2,
+  PG_LDPC_KIND_ALL    = 3,
+  PG_LDPC_ROUTE_X2    = 4,
+  PG_LDPC_ROUTE_SPLIT = 8,
+  PG_LDPC_ROUTE_Z     = 16
+};
 // Route flags of a pg_ldpc_kernel value.
 inline int ldpc_route(int kernel)
 {
-  return kernel == PG_LDPC_KERNEL_TWO_LANES ? PG_LDPC_ROUTE_X2 : (kernel == PG_LDPC_KERNEL_SPLIT ? PG_LDPC_ROUTE_SPLIT : 0);
+  return kernel == PG_LDPC_KERNEL_TWO_LANES ? PG_LDPC_ROUTE_X2
+         : kernel == PG_LDPC_KERNEL_SPLIT   ? PG_LDPC_ROUTE_SPLIT
+         : kernel == PG_LDPC_KERNEL_Z384    ? PG_LDPC_ROUTE_Z
+                                            : 0;
 }
 // Same with at most max_ctas CTAs per decoder kernel, launching only the decoders of `kinds`.
 // counter: two device ints; c2v: one slab (kC2vStride bytes) per CTA.

@@ -536,7 +536,7 @@ static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
          t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
          t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm <= 4 &&
-         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_SPLIT;
+         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_Z384;
 }
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
@@ -682,7 +682,7 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
       c.ldpc_ctas_per_sm     = v;
       if (rc == PG_OK) rc = try_set(c);
     }
-    for (int v : {PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT}) {
+    for (int v : {PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384}) {
       pg_pusch_plan_tuning c = cur;
       c.ldpc_kernel          = v;
       if (rc == PG_OK) rc = try_set(c);

@@ -15,12 +15,25 @@ def f16_bits(v):
 
 def test_f16x2_constants_are_exact():
     text = open(SRC).read()
-    found = re.findall(r"constexpr uint32_t (kHm?\w+)\s*=\s*0x([0-9a-f]+)u; // (-?\d+)", text)
-    assert len(found) >= 10
+    found = re.findall(r"constexpr uint32_t (kHm?\w+)\s*=\s*0x([0-9a-f]+)u; // (-?\d+(?:\.\d+)?)(?=\s|$)", text, re.M)
+    assert len(found) >= 12
     for name, hexv, val in found:
-        assert float(np.float16(int(val))) == int(val), name
-        w = f16_bits(int(val))
+        assert float(np.float16(float(val))) == float(val), name
+        w = f16_bits(float(val))
         assert int(hexv, 16) == (w | (w << 16)), (name, hexv, val)
+    # f16(0.8), the one constant that is not exact.
+    m = re.search(r"constexpr uint32_t kH0p8\s*=\s*0x([0-9a-f]+)u;", text)
+    w = f16_bits(0.8)
+    assert int(m.group(1), 16) == (w | (w << 16))
+
+
+def test_scale_as_f16_fma():
+    """The Z = 384 decoder's 0.8 scaling max(fma(m, f16(0.8), 1023.5) - 1024, 0), rounded to f16 at
+    each step, equals the reference's (m * 52428) >> 16 for every magnitude 0 <= m <= 120."""
+    m = np.arange(0, 121)
+    r = fma16(m, np.float16(0.8), 1023.5)
+    s = np.maximum((r.astype(np.float64) - 1024).astype(np.float16), 0)
+    assert (s.astype(np.int64) == (m * 52428) >> 16).all()
 
 
 def fma16(a, b, c):
