@@ -80,6 +80,10 @@ def parse_args():
     p.add_argument("--no-learned", action="store_true", help="plain estimator only")
     p.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning run)")
     p.add_argument("--no-configs", action="store_true", help="skip the single-slot configuration sub-lines")
+    p.add_argument("--ldpc-kernel", type=int, default=None,
+                   help="LDPC batch kernel of the --workload ldpc line (pg_ldpc_kernel; default: the library's)")
+    p.add_argument("--ldpc-ctas-per-sm", type=int, default=0,
+                   help="resident LDPC CTAs per SM of the --workload ldpc line (0: the kernel's limit)")
     return p.parse_args()
 
 
@@ -772,6 +776,10 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     batch = sim.ldpc_batch(seed=args.seed + rank, n=N_CBS)
     descs, llrs, nbytes = make_descriptors(batch.jobs)
     dec = LdpcBatchDecoder(device=dev, max_codeblocks=N_CBS)
+    if args.ldpc_kernel is not None:
+        dec.set_kernel(args.ldpc_kernel)
+    dec.set_ctas_per_sm(args.ldpc_ctas_per_sm)
+    kernel_id = args.ldpc_kernel if args.ldpc_kernel is not None else int(dec.ctx.lib.pg_get_ldpc_kernel(dec.ctx.handle))
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
 
@@ -860,7 +868,8 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     peak = peak_ops / 1e12 if peak_ops else nominal
     roofline = {
         "bound": "int",
-        "kernel": "ldpc_decode_x2_kernel (every codeblock of the batch has Z=384)",
+        "kernel": LDPC_KERNEL_NAMES[kernel_id] + " (every codeblock of the batch has Z=384)",
+        "ctas_per_sm": args.ldpc_ctas_per_sm or "kernel limit",
         "achieved": round(achieved, 3), "peak": round(peak, 3),
         "unit": "Tops/s", "frac": round(achieved / peak, 4),
         "peak_source": ("measured: full-rate int32 instruction throughput (add.s32/min.s32 probe, libpg_probe.so)"

@@ -152,6 +152,8 @@ enum pg_ldpc_kernel {
 /* Selects the kernel of the context's batch decodes (pg_ldpc_decode_batch_{host,device,resident}
  * and pg_sch_decode_batch_host); slot plans choose theirs through their tuning. */
 int pg_set_ldpc_kernel(pg_context* ctx, int kernel);
+/* The kernel of the context's batch decodes (pg_ldpc_kernel), or a negative error code. */
+int pg_get_ldpc_kernel(const pg_context* ctx);
 /* Resident CTAs per SM of the context's batch decodes (1-4, capped by the kernel's own limit; 0:
  * the kernel's limit, the default). Fewer CTAs than codeblocks make the persistent CTAs share the
  * codeblocks dynamically; more make every codeblock start at once. */

@@ -517,6 +517,11 @@ int pg_set_ldpc_kernel(pg_context* ctx, int kernel)
   return PG_OK;
 }
 
+int pg_get_ldpc_kernel(const pg_context* ctx)
+{
+  return ctx == nullptr ? PG_ERR_INVALID : ctx->ldpc_kernel;
+}
+
 int pg_set_ldpc_ctas_per_sm(pg_context* ctx, int ctas_per_sm)
 {
   if (ctx == nullptr) {

@@ -203,6 +203,7 @@ SIGNATURES = {
     "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
     "pg_set_ldpc_ctas_per_sm": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "pg_get_ldpc_kernel": (ctypes.c_int, [_VP]),
     "pg_set_ldpc_kernel": (ctypes.c_int, [_VP, ctypes.c_int]),
     "pg_port_channel_estimate_host": (ctypes.c_int, [_VP] * 7),
     "pg_sch_decode_batch_resident": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, _VP, _VP,
