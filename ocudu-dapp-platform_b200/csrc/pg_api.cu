@@ -373,6 +373,7 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.crc_tabs);
   cudaFree(ctx->dev.gold);
   cudaFree(ctx->scratch_a);
+  cudaFree(ctx->est_partials);
   cudaFree(ctx->scratch_b);
   free_slots(ctx);
   cudaFree(ctx->dev.llrs);

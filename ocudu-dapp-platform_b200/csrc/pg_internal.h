@@ -88,6 +88,8 @@ struct pg_context {
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
   pg::staging_slot    slots[7];                  // rate-dematch, CRC, TB, PUSCH, UE and UCI work lists
+  void*               est_partials     = nullptr;  // partial sums of the batched channel estimation
+  size_t              est_partials_cap = 0;
   void*               scratch_a      = nullptr;  // growable device scratch of the _host entries
   size_t              scratch_a_cap  = 0;
   void*               scratch_b      = nullptr;
@@ -180,9 +182,17 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
                            size_t nof_llrs, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
 int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
-// max_rb: the largest nof_rb of the UEs (sizes the kernel's shared memory).
-int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
-                    float* ls, pg_port_result* results, cudaStream_t s);
+// Channel estimation of a batch (pusch_estimate_chunk_kernel + pusch_estimate_finish_kernel).
+// est_work_build writes the work list of the UEs (one item per (UE, port, chunk of pilots)) followed
+// by the first item of every (UE, port) (4 n + 1 entries) and returns the item count; work_dev
+// holds that blob on the device, partials nwork float4.
+int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob);
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
+                    void* partials, const uint32_t* grids, float* est, float* ls, pg_port_result* results,
+                    cudaStream_t s);
+// The same from host UEs: stages the UEs and their work list (SLOT_UE), partials in the context.
+int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const uint32_t* grids, float* est, float* ls,
+                         pg_port_result* results, cudaStream_t s);
 int max_nof_rb(const pg_pusch_ue* ues, int n);
 int dmrs_count(const pg_pusch_ue& u, int* d0, int* d1);
 int equalize_launch(pg_context* ctx, int nof_re, int nof_ports, int nof_layers, const uint32_t* y, const uint32_t* h,

@@ -140,13 +140,12 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
     rc = check_cuda(ctx, cudaMemcpyAsync(d_off, L.offs.data(), L.offs.size() * 4, cudaMemcpyHostToDevice, s),
                     "H2D offsets");
   }
+  if (rc == PG_OK) {
+    rc = estimate_launch_host(ctx, L.ues.data(), nof_ues, d_grid, d_est, nullptr, d_pr, s);
+  }
   void* d_ues = nullptr;
   if (rc == PG_OK) {
     rc = stage_slot(ctx, SLOT_UE, L.ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue), s, &d_ues);
-  }
-  if (rc == PG_OK) {
-    rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, max_nof_rb(ues, nof_ues), d_grid, d_est, nullptr,
-                         d_pr, s);
   }
   if (rc == PG_OK) {
     rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_re, d_off + nof_ues,

@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 namespace {
@@ -406,6 +407,263 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
   }
 }
 
+// Chunked form of pusch_estimate_kernel for batches: one CTA per (UE, receive port, chunk of
+// kChunk pilots), so that a slot of many allocations runs as one short wave of small CTAs instead
+// of one long CTA per (UE, port). Each CTA computes the LS estimates of its chunk plus a halo of
+// kHalo pilots either side (the smoothing filter's reach), the virtual pilots where the filter
+// reaches past either end of the allocation, the smoothed estimates of its own pilots and of the
+// next one (for the frequency interpolation of its last odd subcarrier), and its partial sums of
+// RSRP, EPRE and noise. Per element the arithmetic and its order are those of
+// pusch_estimate_kernel, so the frequency responses are identical; pusch_estimate_finish_kernel
+// then adds each (UE, port)'s partial sums in chunk order (deterministic) and forms the scalars.
+constexpr int kChunk        = 128;
+constexpr int kHalo         = 8;  // even, >= the largest filter half-length (7)
+constexpr int kTileOff      = 16; // tile position of pilot k is k - (k0 - kTileOff)
+constexpr int kChunkTile    = kChunk + 2 * kTileOff;
+constexpr int kChunkThreads = 128;
+
+__global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(const pg_pusch_ue* __restrict__ ues,
+                                                                             const uint32_t* __restrict__ work,
+                                                                             const uint32_t* __restrict__ grids,
+                                                                             float2* __restrict__ est_all,
+                                                                             float2* __restrict__ ls_all,
+                                                                             float4* __restrict__ partials,
+                                                                             const uint32_t* __restrict__ gold,
+                                                                             uint32_t gold_words)
+{
+  __shared__ uint32_t s_bits[kMaxDmrs][(2 * kChunkTile) / 32 + 2];
+  __shared__ float2   s_ls[kMaxDmrs][2][kChunkTile];
+  __shared__ float2   s_sm[kMaxDmrs][2][kChunk + 1];
+  __shared__ float    s_red[kChunkThreads / 32][4];
+
+  const uint32_t    wi   = work[blockIdx.x];
+  const int         u    = (int)(wi & 0xffffu);
+  const int         port = (int)((wi >> 16) & 0xfu);
+  const int         ch   = (int)(wi >> 20);
+  const pg_pusch_ue ue   = ues[u];
+  const int         tid  = threadIdx.x;
+  const int         nl   = ue.nof_layers;
+  const int         nrb  = ue.nof_rb;
+  const int         npil = 6 * nrb;
+  const int         nsc  = 12 * nrb;
+  const int         k0   = ch * kChunk;
+  const int         k1   = min(npil, k0 + kChunk);
+  const int         t0   = k0 - kTileOff;
+  const int         pb   = max(0, k0 - kHalo);   // first LS pilot of the tile (even)
+  const int         pe   = min(npil, k1 + kHalo); // one past the last (even)
+  int dsym[kMaxDmrs];
+  int nd = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && nd < kMaxDmrs; ++s) {
+    if ((ue.dmrs_symbol_mask >> s) & 1) {
+      dsym[nd++] = s;
+    }
+  }
+  const float     beta = ue.dmrs_scaling;
+  const uint32_t* grid = grids + ue.grid_offset + (size_t)port * 14 * ue.grid_nof_subc;
+  auto rxp = [&](int d, int k) {
+    return cbf16_load(grid + (size_t)dsym[d] * ue.grid_nof_subc + 12 * ue.rb_start + 2 * k);
+  };
+  const float a = 0.707106781186547524f;
+  auto bit = [&](int d, int i) { // pilot bit i of the allocation, i >= 2 pb
+    const int j = i - 2 * pb;
+    return (s_bits[d][j >> 5] >> (j & 31)) & 1u;
+  };
+  auto pilot = [&](int d, int l, int k) {
+    const float2 p0 = make_float2(bit(d, 2 * k) ? -a : a, bit(d, 2 * k + 1) ? -a : a);
+    return (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
+  };
+
+  // Pilot bits c(2 (m0 + pb)) .. of the tile, m0 = 6 rb_start.
+  const int nwords = (2 * (pe - pb) + 31) / 32;
+  for (int i = tid; i < nd * nwords; i += kChunkThreads) {
+    const int      d      = i / nwords;
+    const int      w      = i - d * nwords;
+    const uint32_t c_init = (uint32_t)(((14ull * ue.slot + dsym[d] + 1) * (2ull * ue.n_id + 1) * (1ull << 17) +
+                                        (2ull * ue.n_id + ue.n_scid)) %
+                                       (1ull << 31));
+    s_bits[d][w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 2u * pb + 32u * w);
+  }
+  __syncthreads();
+
+  // LS estimates of the tile, a pilot pair (k, k + 1) per thread step: averaged over the pair with
+  // two layers (the frequency OCC), scaled by 1/beta.
+  const float inv_beta = 1.0f / beta;
+  float       epre     = 0.f;
+  const int   npairs   = (pe - pb) / 2;
+  for (int i = tid; i < nd * npairs; i += kChunkThreads) {
+    const int    d  = i / npairs;
+    const int    k  = pb + 2 * (i - d * npairs);
+    const float2 y0 = rxp(d, k), y1 = rxp(d, k + 1);
+    if (k >= k0 && k < k1) {
+      epre += y0.x * y0.x + y0.y * y0.y;
+      epre += y1.x * y1.x + y1.y * y1.y;
+    }
+    for (int l = 0; l < nl; ++l) {
+      float2 v0 = cmulconjf(y0, pilot(d, l, k)), v1 = cmulconjf(y1, pilot(d, l, k + 1));
+      if (nl > 1) {
+        const float2 av = make_float2((v0.x + v1.x) / 2.0f, (v0.y + v1.y) / 2.0f);
+        v0 = v1 = av;
+      }
+      v0                       = make_float2(v0.x * inv_beta, v0.y * inv_beta);
+      v1                       = make_float2(v1.x * inv_beta, v1.y * inv_beta);
+      s_ls[d][l][k - t0]       = v0;
+      s_ls[d][l][k + 1 - t0]   = v1;
+      if (ls_all != nullptr && k >= k0 && k < k1) {
+        float2* ls = ls_all + ue.est_offset + (size_t)port * nd * nl * nsc + ((size_t)d * nl + l) * nsc;
+        ls[2 * k]     = v0;
+        ls[2 * k + 1] = make_float2(0.f, 0.f);
+        ls[2 * k + 2] = v1;
+        ls[2 * k + 3] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  __syncthreads();
+
+  // Virtual pilots where the filter reaches past the allocation's ends.
+  const int tsel  = nrb >= 3 ? 2 : nrb - 1;
+  const int ntaps = tsel == 2 ? 15 : (tsel == 1 ? 11 : 5);
+  const int mid   = ntaps / 2;
+  const int nv    = nrb == 1 ? npil : mid;
+  const int ks    = min(k1 + 1, npil); // smoothed pilots k0 .. ks - 1
+  if (tid < nd * nl * 2) {
+    const int d = tid / (nl * 2), l = (tid / 2) % nl, side = tid & 1;
+    float2*   e = s_ls[d][l];
+    if (side == 0 && k0 == 0) {
+      virtual_pilots(e - nv - t0, e - t0, nv, true);
+    } else if (side == 1 && ks - 1 + mid >= npil) {
+      virtual_pilots(e + npil - t0, e + npil - nv - t0, nv, false);
+    }
+  }
+  __syncthreads();
+
+  // Smoothing: pilots k0 .. ks - 1; the chunk's own ones go to the even subcarriers of the output.
+  float2* est          = est_all + ue.est_offset + (size_t)port * nd * nl * nsc;
+  float   rsrp_part[2] = {0.f, 0.f};
+  const int nsm        = ks - k0;
+  for (int i = tid; i < nd * nl * nsm; i += kChunkThreads) {
+    const int     d   = i / (nl * nsm);
+    const int     r   = i - d * nl * nsm;
+    const int     l   = r / nsm;
+    const int     k   = k0 + r - l * nsm;
+    const float2* e   = s_ls[d][l];
+    float2        acc = make_float2(0.f, 0.f);
+    for (int t = 0; t < ntaps; ++t) {
+      const float2 x = e[k - mid + t - t0];
+      acc.x += x.x * c_rc_taps[tsel][t];
+      acc.y += x.y * c_rc_taps[tsel][t];
+    }
+    s_sm[d][l][k - k0] = acc;
+    if (k < k1) {
+      est[((size_t)d * nl + l) * nsc + 2 * k] = acc;
+      rsrp_part[l] += acc.x * acc.x + acc.y * acc.y;
+    }
+  }
+  __syncthreads();
+
+  // Frequency interpolation to the odd subcarriers and noise, own pilots.
+  for (int i = tid; i < nd * nl * (k1 - k0); i += kChunkThreads) {
+    const int d = i / (nl * (k1 - k0));
+    const int r = i - d * nl * (k1 - k0);
+    const int l = r / (k1 - k0);
+    const int k = k0 + r - l * (k1 - k0);
+    float2    v = s_sm[d][l][k - k0];
+    if (k + 1 < npil) {
+      const float2 n = s_sm[d][l][k + 1 - k0];
+      v              = make_float2((n.x - v.x) * 0.5f + v.x, (n.y - v.y) * 0.5f + v.y);
+    }
+    est[((size_t)d * nl + l) * nsc + 2 * k + 1] = v;
+  }
+  float       noise = 0.f;
+  const float sf    = beta / (float)nd;
+  for (int i = tid; i < nd * (k1 - k0); i += kChunkThreads) {
+    const int d    = i / (k1 - k0);
+    const int k    = k0 + i - d * (k1 - k0);
+    float2    pred = make_float2(0.f, 0.f);
+    for (int l = 0; l < nl; ++l) {
+      float2 sacc = make_float2(0.f, 0.f);
+      for (int dd = 0; dd < nd; ++dd) {
+        const float2 f = s_sm[dd][l][k - k0];
+        sacc.x += f.x * sf;
+        sacc.y += f.y * sf;
+      }
+      const float2 q = cmulf(sacc, pilot(d, l, k));
+      pred.x += q.x;
+      pred.y += q.y;
+    }
+    const float2 y = rxp(d, k);
+    const float2 e = make_float2(pred.x - y.x, pred.y - y.y);
+    noise += e.x * e.x + e.y * e.y;
+  }
+  float v4[4] = {rsrp_part[0], rsrp_part[1], epre, noise};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v4[q] += __shfl_xor_sync(0xffffffffu, v4[q], o);
+    }
+  }
+  if ((tid & 31) == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      s_red[tid >> 5][q] = v4[q];
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int w = 0; w < kChunkThreads / 32; ++w) {
+      t.x += s_red[w][0];
+      t.y += s_red[w][1];
+      t.z += s_red[w][2];
+      t.w += s_red[w][3];
+    }
+    partials[blockIdx.x] = t;
+  }
+}
+
+// Port results of every (UE, port): partial sums of the port's chunks (work items first[i] ..
+// first[i + 1] - 1, i = 4 u + port) in chunk order, then the scalars of pusch_estimate_kernel.
+__global__ void pusch_estimate_finish_kernel(const pg_pusch_ue* __restrict__ ues, int n,
+                                             const uint32_t* __restrict__ first, const float4* __restrict__ partials,
+                                             pg_port_result* __restrict__ results)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 4 * n) {
+    return;
+  }
+  const int         u    = i >> 2;
+  const int         port = i & 3;
+  const pg_pusch_ue ue   = ues[u];
+  if (port >= ue.nof_rx_ports) {
+    return;
+  }
+  int nd = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && nd < kMaxDmrs; ++s) {
+    nd += (ue.dmrs_symbol_mask >> s) & 1;
+  }
+  float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (uint32_t w = first[i]; w < first[i + 1]; ++w) {
+    const float4 p = partials[w];
+    t.x += p.x;
+    t.y += p.y;
+    t.z += p.z;
+    t.w += p.w;
+  }
+  const int      nl    = ue.nof_layers;
+  const float    beta  = ue.dmrs_scaling;
+  const float    n_pil = (float)(6 * ue.nof_rb * nd);
+  pg_port_result pr;
+  pr.rsrp[0]       = t.x * beta * beta / n_pil;
+  pr.rsrp[1]       = nl > 1 ? t.y * beta * beta / n_pil : 0.f;
+  pr.epre          = t.z / n_pil;
+  const float ravg = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
+  float       nvar = (pg::is_normal(t.w) ? t.w : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
+  nvar             = fmaxf(ravg / 1e10f, nvar);
+  pr.noise_var     = nvar;
+  pr.snr           = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
+  results[i]       = pr;
+}
+
 // Per-symbol estimates of one UE: f[i] + (f[i+1] - f[i]) w rounded to bf16 (the reference's
 // apply_td_domain_strategy + conversion to cbf16_t); with the learned estimator's time-basis
 // coefficients (basis, two DM-RS symbols) + a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1) before the
@@ -617,17 +875,69 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
   return PG_OK;
 }
 
-int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, int max_rb, const uint32_t* grids, float* est,
-                    float* ls, pg_port_result* results, cudaStream_t s)
+int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob)
+{
+  std::vector<uint32_t> first((size_t)4 * n + 1);
+  blob.clear();
+  for (int u = 0; u < n; ++u) {
+    const int nch = (6 * (int)ues[u].nof_rb + kChunk - 1) / kChunk;
+    for (int p = 0; p < 4; ++p) {
+      first[(size_t)4 * u + p] = (uint32_t)blob.size();
+      if (p < ues[u].nof_rx_ports) {
+        for (int c = 0; c < nch; ++c) {
+          blob.push_back((uint32_t)u | ((uint32_t)p << 16) | ((uint32_t)c << 20));
+        }
+      }
+    }
+  }
+  first[(size_t)4 * n] = (uint32_t)blob.size();
+  const int nwork      = (int)blob.size();
+  blob.insert(blob.end(), first.begin(), first.end());
+  return nwork;
+}
+
+int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
+                    void* partials, const uint32_t* grids, float* est, float* ls, pg_port_result* results,
+                    cudaStream_t s)
 {
   if (n == 0) {
     return PG_OK;
   }
-  const int npil_max = 6 * std::max(1, std::min(max_rb, 275));
-  pusch_estimate_kernel<<<dim3(n, 4), kEstThreads, est_smem_bytes(npil_max), s>>>(
-      ues_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls), results, ctx->dev.gold,
-      kGoldWords, npil_max, nullptr, nullptr);
-  return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_kernel launch");
+  if (nwork > 0) {
+    pusch_estimate_chunk_kernel<<<nwork, kChunkThreads, 0, s>>>(
+        ues_dev, work_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls),
+        static_cast<float4*>(partials), ctx->dev.gold, kGoldWords);
+    if (int rc = check_cuda(ctx, cudaGetLastError(), "pusch_estimate_chunk_kernel launch")) {
+      return rc;
+    }
+  }
+  pusch_estimate_finish_kernel<<<(4 * n + 127) / 128, 128, 0, s>>>(ues_dev, n, work_dev + nwork,
+                                                                    static_cast<const float4*>(partials), results);
+  return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_finish_kernel launch");
+}
+
+int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const uint32_t* grids, float* est, float* ls,
+                         pg_port_result* results, cudaStream_t s)
+{
+  std::vector<uint32_t> blob;
+  const int             nwork = est_work_build(ues, n, blob);
+  std::vector<uint8_t>  staged((size_t)n * sizeof(pg_pusch_ue) + blob.size() * 4);
+  std::memcpy(staged.data(), ues, (size_t)n * sizeof(pg_pusch_ue));
+  std::memcpy(staged.data() + (size_t)n * sizeof(pg_pusch_ue), blob.data(), blob.size() * 4);
+  void* dev = nullptr;
+  if (int rc = stage_slot(ctx, SLOT_UE, staged.data(), staged.size(), s, &dev)) {
+    return rc;
+  }
+  if (int rc = ensure_scratch(ctx, &ctx->est_partials, &ctx->est_partials_cap,
+                              std::max<size_t>(16, (size_t)nwork * sizeof(float4)), "cudaMalloc(estimate partials)")) {
+    return rc;
+  }
+  const pg_pusch_ue* d_ues  = static_cast<const pg_pusch_ue*>(dev);
+  const uint32_t*    d_work = reinterpret_cast<const uint32_t*>(static_cast<uint8_t*>(dev) + (size_t)n * sizeof(pg_pusch_ue));
+  if (int rc = estimate_launch(ctx, d_ues, n, d_work, nwork, ctx->est_partials, grids, est, ls, results, s)) {
+    return rc;
+  }
+  return release_slot_after(ctx, SLOT_UE, s);
 }
 
 int max_nof_rb(const pg_pusch_ue* ues, int n)
@@ -688,16 +998,7 @@ int pg_pusch_estimate_ls_device(pg_context* ctx, const pg_pusch_ue* ues, int nof
   if (nof_ues == 0) {
     return PG_OK;
   }
-  cudaStream_t s   = static_cast<cudaStream_t>(stream);
-  void*        dev = nullptr;
-  if (int rc = stage_slot(ctx, SLOT_UE, ues, (size_t)nof_ues * sizeof(pg_pusch_ue), s, &dev)) {
-    return rc;
-  }
-  if (int rc = estimate_launch(ctx, static_cast<const pg_pusch_ue*>(dev), nof_ues, max_nof_rb(ues, nof_ues), grids, est,
-                               ls, results, s)) {
-    return rc;
-  }
-  return release_slot_after(ctx, SLOT_UE, s);
+  return estimate_launch_host(ctx, ues, nof_ues, grids, est, ls, results, static_cast<cudaStream_t>(stream));
 }
 
 int pg_pusch_symbol_estimates_device(pg_context* ctx, const pg_pusch_ue* ue, const float* est, const float* basis,

@@ -33,6 +33,9 @@ struct pg_pusch_plan {
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
   pg_pusch_ue*    d_ues    = nullptr;
+  uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
+  void*           d_est_part = nullptr; // its partial sums
+  int             est_nwork  = 0;
   pg_rm_cb*       d_rm     = nullptr;
   pg_ldpc_cb*     d_ldpc   = nullptr;
   pg_tb_desc*     d_tb     = nullptr;
@@ -129,8 +132,8 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
             pg_port_result* port_results, cudaStream_t s)
 {
   pg_context* ctx = p->ctx;
-  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->max_rb, grids, p->d_est,
-                                    p->le_net != nullptr ? p->d_ls : nullptr, port_results, s);
+  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->d_est_work, p->est_nwork, p->d_est_part, grids,
+                                    p->d_est, p->le_net != nullptr ? p->d_ls : nullptr, port_results, s);
   if (rc == PG_OK && p->le_net != nullptr) {
     const unsigned int flags = timing_record_flags(ctx, s);
     if (ctx->timed) {
@@ -299,7 +302,10 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_order  = o_cb_off + al(w.cb_bit_off.size() * 4);
   const size_t o_seqoff = o_order + al(order.size() * 4);
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
-  const size_t desc_end = o_reoff + al(re_off.size() * 4);
+  std::vector<uint32_t> est_work;
+  p->est_nwork          = est_work_build(p->ues.data(), nof_ues, est_work);
+  const size_t o_ework  = o_reoff + al(re_off.size() * 4);
+  const size_t desc_end = o_ework + al(est_work.size() * 4);
   const size_t o_seq    = desc_end;
   const size_t o_est    = o_seq + al(seq_total * 4);
   const size_t o_pr     = o_est + al(est_total * 8);
@@ -313,7 +319,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_grid   = o_c2v + al((size_t)ldpc_slabs * kC2vStride);
   const size_t o_tbout  = o_grid + al(grid_words * 4);
   const size_t o_res    = o_tbout + al(p->tb_bytes);
-  p->dev_bytes          = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
+  const size_t o_epart  = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
+  p->dev_bytes          = o_epart + al((size_t)std::max(1, p->est_nwork) * 16);
 
   const size_t h_res  = 0;
   const size_t h_pr   = h_res + al((size_t)nof_ues * sizeof(pg_sch_result));
@@ -353,6 +360,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
   p->d_tb_out  = b + o_tbout;
   p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);
+  p->d_est_work = reinterpret_cast<uint32_t*>(b + o_ework);
+  p->d_est_part = b + o_epart;
 
   // Descriptor image in pinned memory, one upload.
   uint8_t* h = static_cast<uint8_t*>(p->host);
@@ -365,6 +374,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_order, order.data(), order.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, re_off.data(), re_off.size() * 4);
+  std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
   cudaStream_t s = ctx->stream;
   rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
   if (rc == PG_OK) {
