@@ -272,7 +272,8 @@ def train(ctx, steps=3000, rows_per_step=96_000, seed=0, lr=1e-3, lr_min=2e-5, l
 
 EVAL_DELAY_NS = (30.0, 300.0)
 EVAL_DOPPLER_HZ = (0.0, 500.0)
-EVAL_MARGINS_DB = (0.0, 2.0, 4.0, 6.0, 8.0)
+EVAL_MARGIN_STEP_DB = 1.0
+EVAL_MARGIN_MAX_DB = 14.0
 EVAL_BLER_TARGET = 0.1
 SLOT_S = 0.5e-3
 
@@ -432,29 +433,36 @@ def run_plan(ctx, slots, net, max_iterations):
 
 def la_point(per_margin, key):
     """Outer-loop link adaptation: the smallest margin whose BLER is at most EVAL_BLER_TARGET (the
-    largest margin when none is)."""
+    largest margin tried when none is)."""
     for m in per_margin:
         if m["bler_" + key] <= EVAL_BLER_TARGET:
             return m
     return per_margin[-1]
 
 
-def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, margins_db=EVAL_MARGINS_DB, verbose=True):
-    """Per SNR and link-adaptation margin: BLER (TB CRC and payload against the transmitted bits)
-    of the slot plan with the plain and with the learned estimator on the same slots, and the
-    decoded Mbit/s per cell. Each estimator then gets its own margin, the smallest with BLER at
-    most 10 % (outer-loop link adaptation), and its goodput there; EVM and data-symbol channel
-    NMSE of both at the plain estimator's margin."""
+def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, step_db=EVAL_MARGIN_STEP_DB,
+             max_margin_db=EVAL_MARGIN_MAX_DB, verbose=True):
+    """Per SNR, link-adaptation margins 0, step_db, ... until both estimators reach BLER <= 10 % (or
+    max_margin_db): BLER (TB CRC and payload against the transmitted bits) of the slot plan with the
+    plain and with the learned estimator on the same slots, and the decoded Mbit/s per cell. Each
+    estimator then gets its own margin, the smallest with BLER at most 10 % (outer-loop link
+    adaptation), and its goodput there; EVM and data-symbol channel NMSE of both at the plain
+    estimator's margin."""
     rows = []
     for k, snr in enumerate(snrs_db):
-        per_margin = []
-        for m in margins_db:
+        per_margin, m = [], 0.0
+        while True:
             slots = eval_slots(snr, seed + k, cells, la_margin_db=m)
             e_p, b_p = run_plan(ctx, slots, None, max_iterations)
             e_l, b_l = run_plan(ctx, slots, net, max_iterations)
             per_margin.append(dict(margin_db=float(m), ues=len(e_p), bler_plain=float(np.mean(e_p)),
                                    bler_learned=float(np.mean(e_l)),
                                    mbps_plain=b_p / (cells * SLOT_S) / 1e6, mbps_learned=b_l / (cells * SLOT_S) / 1e6))
+            done = (any(p["bler_plain"] <= EVAL_BLER_TARGET for p in per_margin) and
+                    any(p["bler_learned"] <= EVAL_BLER_TARGET for p in per_margin))
+            if done or m + step_db > max_margin_db + 1e-9:
+                break
+            m += step_db
         lp, ll = la_point(per_margin, "plain"), la_point(per_margin, "learned")
         q = estimate_quality(ctx, eval_slots(snr, seed + k, cells, la_margin_db=lp["margin_db"]), net,
                              max_iterations)

@@ -504,6 +504,10 @@ void check_port_estimator(const b200::device_config& dev)
         worst_cfo      = std::max(worst_cfo, d);
         ok             = ok && d <= std::max(1e-3, 1e-3 * std::abs(*r.get_cfo_Hz()));
       }
+      // Per-symbol bf16 estimates: 99 % of the components bit-equal, every component within one bf16
+      // unit of its own magnitude plus 1e-4 of the coefficient's magnitude (a component much smaller
+      // than its coefficient carries the FP32 difference of the whole coefficient in many of its own
+      // units).
       unsigned diff1 = 0, equal = 0, total = 0;
       for (unsigned s = 0; s != MAX_NSYMB_PER_SLOT; ++s) {
         for (unsigned l = 0; l != nl; ++l) {
@@ -513,10 +517,19 @@ void check_port_estimator(const b200::device_config& dev)
             uint32_t x, y;
             std::memcpy(&x, &a_sym[k], 4);
             std::memcpy(&y, &b_sym[k], 4);
+            auto  val = [](uint32_t w, int part) {
+              const uint32_t b = part == 0 ? (w << 16) : (w & 0xffff0000u);
+              float          f;
+              std::memcpy(&f, &b, 4);
+              return static_cast<double>(f);
+            };
+            const double mag = std::hypot(val(x, 0), val(x, 16));
             for (int part = 0; part < 32; part += 16) {
-              const int dx = std::abs(static_cast<int>((x >> part) & 0xffff) - static_cast<int>((y >> part) & 0xffff));
-              diff1 += dx > 1;
-              equal += dx == 0;
+              const double a   = val(x, part), b = val(y, part);
+              const double top = std::max(std::abs(a), std::abs(b));
+              const double ulp = top > 0 ? std::ldexp(1.0, std::ilogb(top) - 7) : 0.0;
+              diff1 += std::abs(a - b) > ulp + 1e-4 * mag;
+              equal += a == b;
               ++total;
             }
           }
