@@ -130,9 +130,11 @@ int ensure_scratch(pg_context* ctx, void** buf, size_t* cap, size_t bytes, const
 int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_total, size_t out_total);
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
                         cudaStream_t stream);
-// Same with ctas_per_cb CTAs per codeblock (1..32).
+// Same with ctas_per_cb CTAs per codeblock (1..32). fill_only (may be NULL): per codeblock, 1 when
+// the demodulator stored its received LLRs directly (rm_direct); the kernel then writes only its
+// filler, unreached and beyond-N_cb positions.
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
-                        cudaStream_t stream, int ctas_per_cb);
+                        cudaStream_t stream, int ctas_per_cb, const uint8_t* fill_only = nullptr);
 void crc_tables_host(uint32_t* tab);
 int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8_t* data, uint32_t* out,
                cudaStream_t stream);
@@ -172,11 +174,21 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 // Same with `block` threads per CTA (64, 128 or 256) and res_per_thread REs per thread (1..8), and
 // the learned estimator's time-basis coefficients (basis, same layout as est; may be NULL) for the
 // UEs with basis_use[u] != 0.
+// Rate-dematch placement of one UE's codeword for the demodulator's direct stores (fused
+// demodulation and rate dematching): the UE's codeblocks hold new data without repetition
+// (E <= V = N_cb - F for each), so codeword bit g of codeblock r (E_r bits from off_r) lands in
+// circular-buffer position pos(t), t = (g - off_r) mod Qm * (E_r / Qm) + (g - off_r) div Qm, with
+// v = (v0 + t) mod V and pos = v < inf ? v : v + F (the placement of ldpc_rate_dematcher with
+// new_data). The first n_small codeblocks carry e_small bits, the others e_large; codeblock r's
+// buffer starts at out0 + r cb_len. enabled == 0: the UE's LLRs go to the codeword buffer instead.
+struct rm_direct {
+  uint32_t out0, cb_len, e_small, e_large, n_small, V, v0, inf, F, enabled;
+};
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis = nullptr,
-                      const uint8_t* basis_use = nullptr);
+                      const uint8_t* basis_use = nullptr, const rm_direct* direct = nullptr, int8_t* rm_out = nullptr);
 // Decodes transport blocks whose codeword LLRs are already in device memory (d_llrs, nof_llrs);
 // uses scratch_b; results and TB payloads land in host memory.
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,

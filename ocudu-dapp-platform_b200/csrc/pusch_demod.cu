@@ -142,7 +142,8 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
                                          const float2* __restrict__ est, const float2* __restrict__ basis,
                                          const pg_port_result* __restrict__ pres, int nd, float w, int sym, int re_idx,
                                          int j, const uint32_t* __restrict__ seq, int8_t* __restrict__ llr_out,
-                                         const demap_tables& tb)
+                                         const demap_tables& tb, const pg::rm_direct* __restrict__ dr,
+                                         int8_t* __restrict__ rm_out)
 {
   const int nsc     = 12 * ue.nof_rb;
   const int sc      = 12 * ue.rb_start + j;
@@ -275,6 +276,38 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
   const uint32_t wb   = __ldg(seq + (bit0 >> 5) + 1);
   const uint32_t sh   = bit0 & 31u;
   const uint32_t cbits = sh ? ((wa >> sh) | (wb << (32 - sh))) : wa;
+  if (dr != nullptr) {
+    // Fused rate dematching: the RE's L*QM bits lie in one codeblock (E is a multiple of L*QM);
+    // bit l*QM + b is de-interleaver row b, column i0 + l, placed in the circular buffer.
+    const uint32_t es = dr->e_small, el = dr->e_large, ns = dr->n_small;
+    const uint32_t lo = ns * es;
+    uint32_t       r, off, E;
+    if (bit0 < lo) {
+      r   = bit0 / es;
+      off = r * es;
+      E   = es;
+    } else {
+      r   = ns + (bit0 - lo) / el;
+      off = lo + (r - ns) * el;
+      E   = el;
+    }
+    const uint32_t kq  = E / QM;
+    const uint32_t i0  = (bit0 - off) / QM;
+    int8_t*        cbo = rm_out + dr->out0 + (size_t)r * dr->cb_len;
+#pragma unroll
+    for (int b = 0; b < QM; ++b) {
+#pragma unroll
+      for (int l = 0; l < L; ++l) {
+        uint32_t v = dr->v0 + (uint32_t)b * kq + i0 + (uint32_t)l;
+        v          = v >= dr->V ? v - dr->V : v;
+        const uint32_t pos = v < dr->inf ? v : v + dr->F;
+        const int      k   = l * QM + b;
+        const int      x   = llr[k];
+        cbo[pos]           = (int8_t)(((cbits >> k) & 1u) ? -x : x);
+      }
+    }
+    return;
+  }
   int8_t* out = llr_out + ue.llr_offset + bit0;
   // The RE's descrambled LLRs packed four to a word, stored with the widest store their address
   // allows (codewords of plans and batched calls start on 16-byte boundaries, so an RE's NB bytes
@@ -318,13 +351,13 @@ template <int L, int P>
 __device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const uint32_t* grid, const float2* est,
                                                   const float2* bas, const pg_port_result* pres, int nd, float w,
                                                   int sym, int re_idx, int j, const uint32_t* seq, int8_t* llrs,
-                                                  const demap_tables& tb)
+                                                  const demap_tables& tb, const pg::rm_direct* dr, int8_t* rm_out)
 {
   switch (ue.modulation_order) {
-    case 2: demod_re<L, P, 2>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    case 4: demod_re<L, P, 4>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    case 6: demod_re<L, P, 6>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
-    default: demod_re<L, P, 8>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb); break;
+    case 2: demod_re<L, P, 2>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
+    case 4: demod_re<L, P, 4>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
+    case 6: demod_re<L, P, 6>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
+    default: demod_re<L, P, 8>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
   }
 }
 
@@ -338,7 +371,8 @@ __device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_u
                                              const uint8_t* __restrict__ basis_use,
                                              const pg_port_result* __restrict__ port_results,
                                              const uint32_t* __restrict__ seq_offsets, const uint32_t* __restrict__ seq,
-                                             int8_t* __restrict__ llrs, const demap_tables& tb, int u_first)
+                                             int8_t* __restrict__ llrs, const demap_tables& tb, int u_first,
+                                             const pg::rm_direct* __restrict__ direct, int8_t* __restrict__ rm_out)
 {
   // UE of this RE: the last u with re_off[u] <= rg, searched forward from the UE of the CTA's first
   // RE (a CTA's REs span one or a few UEs).
@@ -380,16 +414,22 @@ __device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_u
                                    : nullptr;
   const pg_port_result* pres = port_results + (size_t)u * 4;
   const uint32_t*       sq   = seq + seq_offsets[u];
+  pg::rm_direct         drv;
+  const pg::rm_direct*  dr   = nullptr;
+  if (direct != nullptr && direct[u].enabled != 0) {
+    drv = direct[u];
+    dr  = &drv;
+  }
   if (ue.nof_layers == 1) {
     switch (ue.nof_rx_ports) {
-      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      default: demod_dispatch_qm<1, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
+      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
+      default: demod_dispatch_qm<1, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
     }
   } else {
     switch (ue.nof_rx_ports) {
-      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
-      default: demod_dispatch_qm<2, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb); break;
+      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
+      default: demod_dispatch_qm<2, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
     }
   }
 }
@@ -404,7 +444,8 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
                                                           const pg_port_result* __restrict__ port_results,
                                                           const uint32_t* __restrict__ seq_offsets,
                                                           const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs,
-                                                          int res_per_thread)
+                                                          int res_per_thread, const pg::rm_direct* __restrict__ direct,
+                                                          int8_t* __restrict__ rm_out)
 {
   __shared__ float s_slope[3 * 4 * 16];
   __shared__ float s_icpt[3 * 4 * 16];
@@ -442,7 +483,7 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
       break;
     }
     demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, basis_all, basis_use, port_results, seq_offsets, seq, llrs,
-                 tb, u0);
+                 tb, u0, direct, rm_out);
   }
 }
 
@@ -495,7 +536,7 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
                       const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis,
-                      const uint8_t* basis_use)
+                      const uint8_t* basis_use, const rm_direct* direct, int8_t* rm_out)
 {
   if (n == 0 || total_re == 0) {
     return PG_OK;
@@ -507,7 +548,7 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
   const uint32_t per   = (uint32_t)block * (uint32_t)res_per_thread;
   pusch_demod_kernel<<<(total_re + per - 1) / per, block, 0, s>>>(
       ues_dev, n, re_off_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
-      basis_use, port_results, seq_offsets_dev, seq_dev, llrs, res_per_thread);
+      basis_use, port_results, seq_offsets_dev, seq_dev, llrs, res_per_thread, direct, rm_out);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 

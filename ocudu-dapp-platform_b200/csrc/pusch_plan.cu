@@ -29,10 +29,14 @@ struct pg_pusch_plan {
   std::vector<pg_pusch_ue> ues;
   std::vector<pg_rm_cb>    rm;                 // rate-dematch descriptors (host copy, for HARQ updates)
   std::vector<int>         tb_first, tb_ncb;   // codeblocks of each UE
+  std::vector<rm_direct>   direct;             // host copies of d_direct / d_fill (rebuilt by set_harq)
+  std::vector<uint8_t>     fill;
   size_t                   rm_total = 0;       // bytes of dematched codeblocks (the soft buffers)
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
   pg_pusch_ue*    d_ues    = nullptr;
+  rm_direct*      d_direct   = nullptr; // per UE: fused rate-dematch placement of the demodulator
+  uint8_t*        d_fill     = nullptr; // per codeblock: 1 when the demodulator placed its LLRs
   uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
   void*           d_est_part = nullptr; // its partial sums
   int             est_nwork  = 0;
@@ -128,6 +132,73 @@ size_t al(size_t x)
   return (x + 255) & ~(size_t)255;
 }
 
+// Fused demodulation and rate dematching: per UE the placement of its codeword in the codeblock
+// buffers when every codeblock holds new data without repetition (E <= N_cb - F), as a
+// consecutive run of E values with the smaller ones first and buffers a constant stride apart;
+// other UEs keep the codeword buffer and the rate-dematch kernel. fill[c] = 1 for the codeblocks
+// of the enabled UEs (their dematch launch only writes the positions no LLR reaches).
+void build_direct(const std::vector<pg_pusch_ue>& ues, const std::vector<pg_rm_cb>& rm, const std::vector<int>& first,
+                  const std::vector<int>& ncb, std::vector<rm_direct>& direct, std::vector<uint8_t>& fill)
+{
+  direct.assign(ues.size(), rm_direct{});
+  fill.assign(rm.size(), 0);
+  for (size_t u = 0; u < ues.size(); ++u) {
+    const int c0 = first[u], n = ncb[u];
+    if (n <= 0) {
+      continue;
+    }
+    const pg_rm_cb& a   = rm[c0];
+    const int       bg  = a.base_graph;
+    const int       Z   = a.lifting_size;
+    const int       Kb  = bg == 1 ? 22 : 10;
+    const int       N   = (bg == 1 ? 66 : 50) * Z;
+    const int       Ncb = (a.nref > 0 && (int)a.nref < N) ? (int)a.nref : N;
+    const int       F   = a.nof_filler_bits;
+    const int       sys = (Kb - 2) * Z;
+    const int       inf = sys - F;
+    const int       V   = Ncb - F;
+    const int       sh  = bg == 1 ? (a.rv == 0 ? 0 : a.rv == 1 ? 17 : a.rv == 2 ? 33 : 56)
+                                  : (a.rv == 0 ? 0 : a.rv == 1 ? 13 : a.rv == 2 ? 25 : 43);
+    const int       k0  = (int)(((long long)sh * Ncb) / N) * Z;
+    const int       v0  = k0 < inf ? k0 : (k0 < sys ? inf : k0 - F);
+    const uint32_t  es  = a.rm_length;
+    const uint32_t  el  = rm[c0 + n - 1].rm_length;
+    uint32_t        ns  = 0;
+    while ((int)ns < n && rm[c0 + ns].rm_length == es) {
+      ++ns;
+    }
+    const pg_pusch_ue& ue = ues[u];
+    bool ok = ue.modulation_order == a.modulation_order && el <= (uint32_t)V && es <= el;
+    for (int k = 0; k < n && ok; ++k) {
+      const pg_rm_cb& c  = rm[c0 + k];
+      const uint32_t  e  = (uint32_t)k < ns ? es : el;
+      const uint32_t  in = ue.llr_offset + ((uint32_t)k < ns ? (uint32_t)k * es : ns * es + ((uint32_t)k - ns) * el);
+      ok = c.new_data != 0 && c.base_graph == a.base_graph && c.lifting_size == a.lifting_size &&
+           c.nof_filler_bits == a.nof_filler_bits && c.nref == a.nref && c.rv == a.rv &&
+           c.modulation_order == a.modulation_order && c.rm_length == e && c.in_offset == in &&
+           c.out_offset == a.out_offset + (uint32_t)k * (uint32_t)N &&
+           e % (uint32_t)(ue.nof_layers * ue.modulation_order) == 0;
+    }
+    if (!ok) {
+      continue;
+    }
+    rm_direct& d = direct[u];
+    d.out0       = a.out_offset;
+    d.cb_len     = (uint32_t)N;
+    d.e_small    = es;
+    d.e_large    = el;
+    d.n_small    = ns;
+    d.V          = (uint32_t)V;
+    d.v0         = (uint32_t)v0;
+    d.inf        = (uint32_t)inf;
+    d.F          = (uint32_t)F;
+    d.enabled    = 1;
+    for (int k = 0; k < n; ++k) {
+      fill[c0 + k] = 1;
+    }
+  }
+}
+
 int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_result* results,
             pg_port_result* port_results, cudaStream_t s)
 {
@@ -150,10 +221,11 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
                            p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread,
                            p->le_net != nullptr ? p->d_basis : nullptr,
-                           p->le_net != nullptr ? p->d_basis_use : nullptr);
+                           p->le_net != nullptr ? p->d_basis_use : nullptr, p->d_direct, p->d_rm_out);
   }
   if (rc == PG_OK) {
-    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb);
+    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb,
+                             p->d_fill);
   }
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
@@ -304,8 +376,15 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
   std::vector<uint32_t> est_work;
   p->est_nwork          = est_work_build(p->ues.data(), nof_ues, est_work);
+  std::vector<rm_direct> direct;
+  std::vector<uint8_t>   fill;
+  build_direct(p->ues, w.rm, w.tb_first, w.tb_ncb, direct, fill);
+  p->direct = direct;
+  p->fill   = fill;
   const size_t o_ework  = o_reoff + al(re_off.size() * 4);
-  const size_t desc_end = o_ework + al(est_work.size() * 4);
+  const size_t o_direct = o_ework + al(est_work.size() * 4);
+  const size_t o_fill   = o_direct + al(direct.size() * sizeof(rm_direct));
+  const size_t desc_end = o_fill + al(fill.size());
   const size_t o_seq    = desc_end;
   const size_t o_est    = o_seq + al(seq_total * 4);
   const size_t o_pr     = o_est + al(est_total * 8);
@@ -361,6 +440,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_tb_out  = b + o_tbout;
   p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);
   p->d_est_work = reinterpret_cast<uint32_t*>(b + o_ework);
+  p->d_direct   = reinterpret_cast<rm_direct*>(b + o_direct);
+  p->d_fill     = b + o_fill;
   p->d_est_part = b + o_epart;
 
   // Descriptor image in pinned memory, one upload.
@@ -375,6 +456,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, re_off.data(), re_off.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
+  std::memcpy(h + o_direct, direct.data(), direct.size() * sizeof(rm_direct));
+  std::memcpy(h + o_fill, fill.data(), fill.size());
   cudaStream_t s = ctx->stream;
   rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
   if (rc == PG_OK) {
@@ -523,12 +606,24 @@ int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const u
       }
     }
   }
+  // Soft combining (new_data == 0) takes a UE off the fused demodulation and rate dematching.
+  build_direct(plan->ues, plan->rm, plan->tb_first, plan->tb_ncb, plan->direct, plan->fill);
   // The kernels read the descriptors when they run, so a captured graph stays valid.
   cudaStream_t s  = ctx->stream;
   int          rc = check_cuda(ctx,
                                cudaMemcpyAsync(plan->d_rm, plan->rm.data(), plan->rm.size() * sizeof(pg_rm_cb),
                                                cudaMemcpyHostToDevice, s),
                                "H2D HARQ rate-dematch descriptors");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaMemcpyAsync(plan->d_direct, plan->direct.data(), plan->direct.size() * sizeof(rm_direct),
+                                    cudaMemcpyHostToDevice, s),
+                    "H2D HARQ demodulator placement");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_fill, plan->fill.data(), plan->fill.size(), cudaMemcpyHostToDevice, s),
+                    "H2D HARQ fill flags");
+  }
   if (rc == PG_OK) {
     rc = check_cuda(ctx,
                     cudaMemcpyAsync(plan->d_ues, plan->ues.data(), plan->ues.size() * sizeof(pg_pusch_ue),

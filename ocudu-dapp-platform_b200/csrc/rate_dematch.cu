@@ -42,7 +42,8 @@ constexpr int kRmTileRows = 256;
 
 __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb* __restrict__ cbs,
                                                                   const int8_t* __restrict__ in_all,
-                                                                  int8_t* __restrict__ out_all)
+                                                                  int8_t* __restrict__ out_all,
+                                                                  const uint8_t* __restrict__ fill_only)
 {
   __shared__ int8_t tile[kRmTileRows * 8];
   const pg_rm_cb d   = cbs[blockIdx.x];
@@ -67,12 +68,15 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   const bool     nd  = d.new_data != 0;
 
   if (E <= V) {
+    // Codeblocks whose LLRs the demodulator placed itself (new data, E <= V) need only the
+    // positions no input reaches.
+    const bool placed = fill_only != nullptr && fill_only[blockIdx.x] != 0;
     // No repetition: each buffer position receives at most one input. The input, row i holding
     // the Qm LLRs of de-interleaver column i, is read a tile of rows at a time (coalesced) and
     // transposed through shared memory; bit plane j of rows i0.. lands on consecutive buffer
     // positions (t = j Kq + i, valid index (v0 + t) mod V, past the fillers), so the stores are
     // coalesced too. Positions no input reaches are written by the per-position loop below.
-    const int ntiles = (Kq + kRmTileRows - 1) / kRmTileRows;
+    const int ntiles = placed ? 0 : (Kq + kRmTileRows - 1) / kRmTileRows;
     for (int tl = blockIdx.y; tl < ntiles; tl += gridDim.y) {
       const int i0   = tl * kRmTileRows;
       const int rows = min(kRmTileRows, Kq - i0);
@@ -204,14 +208,14 @@ int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const
 }
 
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
-                        cudaStream_t stream, int ctas_per_cb)
+                        cudaStream_t stream, int ctas_per_cb, const uint8_t* fill_only)
 {
   if (n == 0) {
     return PG_OK;
   }
   // Each codeblock's N <= 25,344 output positions spread over ctas_per_cb CTAs.
   ctas_per_cb = std::max(1, std::min(32, ctas_per_cb));
-  rate_dematch_kernel<<<dim3(n, ctas_per_cb), kRmThreads, 0, stream>>>(descs_dev, in, out);
+  rate_dematch_kernel<<<dim3(n, ctas_per_cb), kRmThreads, 0, stream>>>(descs_dev, in, out, fill_only);
   return check_cuda(ctx, cudaGetLastError(), "rate_dematch_kernel launch");
 }
 

@@ -455,8 +455,11 @@ def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, step_db=EVAL
             slots = eval_slots(snr, seed + k, cells, la_margin_db=m)
             e_p, b_p = run_plan(ctx, slots, None, max_iterations)
             e_l, b_l = run_plan(ctx, slots, net, max_iterations)
+            qm = np.array([ue.modulation_order for sl in slots for ue in sl.ues])
+            by_qm = {int(q): dict(ues=int((qm == q).sum()), plain=float(np.mean(np.array(e_p)[qm == q])),
+                                  learned=float(np.mean(np.array(e_l)[qm == q]))) for q in np.unique(qm)}
             per_margin.append(dict(margin_db=float(m), ues=len(e_p), bler_plain=float(np.mean(e_p)),
-                                   bler_learned=float(np.mean(e_l)),
+                                   bler_learned=float(np.mean(e_l)), bler_by_qm=by_qm,
                                    mbps_plain=b_p / (cells * SLOT_S) / 1e6, mbps_learned=b_l / (cells * SLOT_S) / 1e6))
             done = (any(p["bler_plain"] <= EVAL_BLER_TARGET for p in per_margin) and
                     any(p["bler_learned"] <= EVAL_BLER_TARGET for p in per_margin))
