@@ -145,12 +145,14 @@ int demap_upload_tables(pg_context* ctx);
 int est_upload_tables(pg_context* ctx);
 int demod_upload_tables(pg_context* ctx, const void* slope, const void* intercept, const void* width);
 uint32_t ue_codeword_bits(const pg_pusch_ue& u);
-int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_re,
-                 const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_tiles,
+                 const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                  const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
                  cudaStream_t s);
 // Prefix sums (n + 1 entries) of the UEs' data REs; returns the total.
-uint32_t data_re_offsets(const pg_pusch_ue* ues, int n, uint32_t* off);
+// Prefix sums (n + 1) of the UEs' demodulation tiles (groups of consecutive subcarriers that one
+// CTA demodulates over every data symbol); returns the total.
+uint32_t demod_tile_offsets(const pg_pusch_ue* ues, int n, uint32_t* off);
 // Host-side work lists of a batch of transport blocks: one rate-dematch and one LDPC descriptor
 // per codeblock, one TB descriptor per TB, the bit offset of each codeblock's decoded bits.
 struct sch_work {
@@ -167,11 +169,11 @@ int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t no
 int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,
                       const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s);
 // Demodulation with the scrambling sequences already generated.
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
-                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
+                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s);
-// Same with `block` threads per CTA (64, 128 or 256) and res_per_thread REs per thread (1..8), and
+// Same with `block` threads per CTA (64, 128 or 256) and res_per_thread tiles per CTA (1..8), and
 // the learned estimator's time-basis coefficients (basis, same layout as est; may be NULL) for the
 // UEs with basis_use[u] != 0.
 // Rate-dematch placement of one UE's codeword for the demodulator's direct stores (fused
@@ -184,8 +186,8 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 struct rm_direct {
   uint32_t out0, cb_len, e_small, e_large, n_small, V, v0, inf, F, enabled;
 };
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
-                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
+                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis = nullptr,
                       const uint8_t* basis_use = nullptr, const rm_direct* direct = nullptr, int8_t* rm_out = nullptr);

@@ -11,9 +11,9 @@ namespace {
 struct slot_layout {
   std::vector<pg_pusch_ue> ues;
   std::vector<uint32_t>    seq_off;
-  std::vector<uint32_t>    offs; // [seq offsets (n) | data RE offsets (n + 1)]
+  std::vector<uint32_t>    offs; // [seq offsets (n) | demodulation tile offsets (n + 1)]
   size_t                   est_total = 0, llr_total = 0, seq_total = 0;
-  uint32_t                 max_words = 0, total_re = 0;
+  uint32_t                 max_words = 0, total_tiles = 0;
 };
 
 // Assigns est/llr offsets and scrambling-sequence offsets.
@@ -38,7 +38,7 @@ void plan(const pg_pusch_ue* ues, int n, slot_layout& L, bool assign_offsets)
   }
   L.offs.assign(2 * (size_t)n + 1, 0);
   std::copy(L.seq_off.begin(), L.seq_off.end(), L.offs.begin());
-  L.total_re = data_re_offsets(L.ues.data(), n, L.offs.data() + n);
+  L.total_tiles = demod_tile_offsets(L.ues.data(), n, L.offs.data() + n);
 }
 
 } // namespace
@@ -75,7 +75,7 @@ int pg_pusch_demodulate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_
     rc = stage_slot(ctx, SLOT_UE, L.ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue), s, &d_ues);
   }
   if (rc == PG_OK) {
-    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_re,
+    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_tiles,
                       d_off + nof_ues, grids, est, port_results, d_off, d_seq, llrs, s);
   }
   if (rc == PG_OK) {
@@ -148,7 +148,7 @@ int pg_pusch_process_host(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, 
     rc = stage_slot(ctx, SLOT_UE, L.ues.data(), (size_t)nof_ues * sizeof(pg_pusch_ue), s, &d_ues);
   }
   if (rc == PG_OK) {
-    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_re, d_off + nof_ues,
+    rc = demod_launch(ctx, static_cast<const pg_pusch_ue*>(d_ues), nof_ues, L.max_words, L.total_tiles, d_off + nof_ues,
                       d_grid, d_est, d_pr, d_off, d_seq, d_llr, s);
   }
   if (rc == PG_OK) {

@@ -143,9 +143,11 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
                                          const pg_port_result* __restrict__ pres, int nd, float w, int sym, int re_idx,
                                          int j, const uint32_t* __restrict__ seq, int8_t* __restrict__ llr_out,
                                          const demap_tables& tb, const pg::rm_direct* __restrict__ dr,
-                                         int8_t* __restrict__ rm_out)
+                                         int8_t* __restrict__ rm_out, int estride, int je)
 {
-  const int nsc     = 12 * ue.nof_rb;
+  // est / basis: [port][DM-RS symbol][layer][estride], this RE's subcarrier at index je (the whole
+  // allocation, estride = 12 nof_rb and je = j, or a tile of it in shared memory).
+  const int nsc     = estride;
   const int sc      = 12 * ue.rb_start + j;
   const bool is_dc  = sc == ue.dc_subcarrier;
   cf        y[P];
@@ -156,14 +158,14 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
 #pragma unroll
     for (int l = 0; l < L; ++l) {
       const float2* f0 = est + (((size_t)p * nd) * L + l) * nsc;
-      float2        v  = f0[j];
+      float2        v  = f0[je];
       if (nd == 2) {
-        const float2 v1 = f0[(size_t)L * nsc + j];
+        const float2 v1 = f0[(size_t)L * nsc + je];
         v               = make_float2(__fmaf_rn(v1.x - v.x, w, v.x), __fmaf_rn(v1.y - v.y, w, v.y));
         if (basis != nullptr) {
           // The learned estimator's time-basis terms a_1 w (1 - w) + a_2 w (1 - w) (2 w - 1).
           const float2* b0 = basis + (((size_t)p * nd) * L + l) * nsc;
-          const float2  a1 = b0[j], a2 = b0[(size_t)L * nsc + j];
+          const float2  a1 = b0[je], a2 = b0[(size_t)L * nsc + je];
           const float   f1 = __fmul_rn(w, __fsub_rn(1.f, w));
           const float   f2 = __fmul_rn(f1, __fsub_rn(__fmul_rn(2.f, w), 1.f));
           v                = make_float2(__fmaf_rn(a2.x, f2, __fmaf_rn(a1.x, f1, v.x)),
@@ -347,96 +349,48 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
   }
 }
 
+// Demodulation in tiles: one CTA per (UE, kDemodTile consecutive subcarriers of its allocation)
+// over every data symbol. The CTA stages the tile's frequency responses (and the learned
+// estimator's time-basis coefficients) in shared memory once, so each is read from memory once
+// rather than once per data symbol; a warp's threads take consecutive subcarriers of one symbol,
+// so grid reads and LLR stores stay coalesced. tile_off[u] .. tile_off[u + 1] - 1 are UE u's tiles.
+constexpr int kDemodTile = 32;
+
+template <int L, int P, int QM>
+__device__ __forceinline__ void demod_tile(const pg_pusch_ue& ue, int u, int j0, int nt, int nd, const int* s_sym,
+                                           const float* s_w, int nds, const uint32_t* grid, const float2* s_est,
+                                           const float2* s_bas, const pg_port_result* pres, const uint32_t* sq,
+                                           int8_t* llrs, const demap_tables& tb, const pg::rm_direct* dr,
+                                           int8_t* rm_out)
+{
+  const int nsc = 12 * ue.nof_rb;
+  for (int q = threadIdx.x; q < nds * nt; q += blockDim.x) {
+    const int di = q / nt;
+    const int jj = q - di * nt;
+    const int j  = j0 + jj;
+    demod_re<L, P, QM>(ue, grid, s_est, s_bas, pres, nd, s_w[di], s_sym[di], di * nsc + j, j, sq, llrs, tb, dr, rm_out,
+                       kDemodTile, jj);
+  }
+}
+
 template <int L, int P>
-__device__ __forceinline__ void demod_dispatch_qm(const pg_pusch_ue& ue, const uint32_t* grid, const float2* est,
-                                                  const float2* bas, const pg_port_result* pres, int nd, float w,
-                                                  int sym, int re_idx, int j, const uint32_t* seq, int8_t* llrs,
-                                                  const demap_tables& tb, const pg::rm_direct* dr, int8_t* rm_out)
+__device__ __forceinline__ void demod_tile_qm(const pg_pusch_ue& ue, int u, int j0, int nt, int nd, const int* s_sym,
+                                              const float* s_w, int nds, const uint32_t* grid, const float2* s_est,
+                                              const float2* s_bas, const pg_port_result* pres, const uint32_t* sq,
+                                              int8_t* llrs, const demap_tables& tb, const pg::rm_direct* dr,
+                                              int8_t* rm_out)
 {
   switch (ue.modulation_order) {
-    case 2: demod_re<L, P, 2>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
-    case 4: demod_re<L, P, 4>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
-    case 6: demod_re<L, P, 6>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
-    default: demod_re<L, P, 8>(ue, grid, est, bas, pres, nd, w, sym, re_idx, j, seq, llrs, tb, dr, rm_out); break;
+    case 2: demod_tile<L, P, 2>(ue, u, j0, nt, nd, s_sym, s_w, nds, grid, s_est, s_bas, pres, sq, llrs, tb, dr, rm_out); break;
+    case 4: demod_tile<L, P, 4>(ue, u, j0, nt, nd, s_sym, s_w, nds, grid, s_est, s_bas, pres, sq, llrs, tb, dr, rm_out); break;
+    case 6: demod_tile<L, P, 6>(ue, u, j0, nt, nd, s_sym, s_w, nds, grid, s_est, s_bas, pres, sq, llrs, tb, dr, rm_out); break;
+    default: demod_tile<L, P, 8>(ue, u, j0, nt, nd, s_sym, s_w, nds, grid, s_est, s_bas, pres, sq, llrs, tb, dr, rm_out); break;
   }
 }
 
-// One thread per data resource element of the whole batch: re_off[u] .. re_off[u + 1] are the
-// data REs of UE u (data symbols x 12 nof_rb, symbol-major), so every CTA works on one or two
-// UEs and small UEs take no more threads than they have REs.
-__device__ __forceinline__ void demod_one_re(const uint32_t rg, const pg_pusch_ue* __restrict__ ues, int nof_ues,
-                                             const uint32_t* __restrict__ re_off, const uint32_t* __restrict__ grids,
-                                             const float2* __restrict__ est_all,
-                                             const float2* __restrict__ basis_all,
-                                             const uint8_t* __restrict__ basis_use,
-                                             const pg_port_result* __restrict__ port_results,
-                                             const uint32_t* __restrict__ seq_offsets, const uint32_t* __restrict__ seq,
-                                             int8_t* __restrict__ llrs, const demap_tables& tb, int u_first,
-                                             const pg::rm_direct* __restrict__ direct, int8_t* __restrict__ rm_out)
-{
-  // UE of this RE: the last u with re_off[u] <= rg, searched forward from the UE of the CTA's first
-  // RE (a CTA's REs span one or a few UEs).
-  int u = u_first;
-  while (u + 1 < nof_ues && __ldg(re_off + u + 1) <= rg) {
-    ++u;
-  }
-  const pg_pusch_ue ue  = ues[u];
-  const int         nsc = 12 * ue.nof_rb;
-  const int         r   = (int)(rg - __ldg(re_off + u));
-  int               d0 = -1, d1 = -1, nd = 0;
-  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-    if ((ue.dmrs_symbol_mask >> s) & 1) {
-      if (nd == 0) {
-        d0 = s;
-      } else if (nd == 1) {
-        d1 = s;
-      }
-      ++nd;
-    }
-  }
-  const int di = r / nsc;
-  const int j  = r - di * nsc;
-  // OFDM symbol of data-symbol index di.
-  int sym = ue.first_symbol, cnt = -1;
-  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-    if (!((ue.dmrs_symbol_mask >> s) & 1)) {
-      if (++cnt == di) {
-        sym = s;
-        break;
-      }
-    }
-  }
-  const float           w    = nd == 2 ? (float)(sym - d0) / (float)(d1 - d0) : 0.f;
-  const uint32_t*       grid = grids + ue.grid_offset;
-  const float2*         est  = est_all + ue.est_offset;
-  const float2*         bas  = (basis_all != nullptr && basis_use != nullptr && nd == 2 && basis_use[u] != 0)
-                                   ? basis_all + ue.est_offset
-                                   : nullptr;
-  const pg_port_result* pres = port_results + (size_t)u * 4;
-  const uint32_t*       sq   = seq + seq_offsets[u];
-  pg::rm_direct         drv;
-  const pg::rm_direct*  dr   = nullptr;
-  if (direct != nullptr && direct[u].enabled != 0) {
-    drv = direct[u];
-    dr  = &drv;
-  }
-  if (ue.nof_layers == 1) {
-    switch (ue.nof_rx_ports) {
-      case 1: demod_dispatch_qm<1, 1>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
-      case 2: demod_dispatch_qm<1, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
-      default: demod_dispatch_qm<1, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
-    }
-  } else {
-    switch (ue.nof_rx_ports) {
-      case 2: demod_dispatch_qm<2, 2>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
-      default: demod_dispatch_qm<2, 4>(ue, grid, est, bas, pres, nd, w, sym, r, j, sq, llrs, tb, dr, rm_out); break;
-    }
-  }
-}
-
-// res_per_thread consecutive blocks of blockDim.x REs per CTA (a launch-shape tunable).
+// tiles_per_cta consecutive tiles of the batch's tile list per CTA (a launch-shape tunable).
 __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, int nof_ues,
-                                                          const uint32_t* __restrict__ re_off,
+                                                          const uint32_t* __restrict__ tile_off,
                                                           const uint32_t* __restrict__ grids,
                                                           const float2* __restrict__ est_all,
                                                           const float2* __restrict__ basis_all,
@@ -444,12 +398,17 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
                                                           const pg_port_result* __restrict__ port_results,
                                                           const uint32_t* __restrict__ seq_offsets,
                                                           const uint32_t* __restrict__ seq, int8_t* __restrict__ llrs,
-                                                          int res_per_thread, const pg::rm_direct* __restrict__ direct,
+                                                          int tiles_per_cta, const pg::rm_direct* __restrict__ direct,
                                                           int8_t* __restrict__ rm_out)
 {
-  __shared__ float s_slope[3 * 4 * 16];
-  __shared__ float s_icpt[3 * 4 * 16];
-  __shared__ float s_width[3];
+  __shared__ float  s_slope[3 * 4 * 16];
+  __shared__ float  s_icpt[3 * 4 * 16];
+  __shared__ float  s_width[3];
+  __shared__ float2 s_est[4 * 2 * 2 * kDemodTile];
+  __shared__ float2 s_bas[4 * 2 * 2 * kDemodTile];
+  __shared__ int    s_sym[14];
+  __shared__ float  s_w[14];
+  __shared__ pg::rm_direct s_dr;
   for (int i = threadIdx.x; i < 3 * 4 * 16; i += blockDim.x) {
     s_slope[i] = (&c_slope_d[0][0][0])[i];
     s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
@@ -457,33 +416,93 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
   if (threadIdx.x < 3) {
     s_width[threadIdx.x] = c_width_d[threadIdx.x];
   }
-  __shared__ int     s_u0;
-  const uint32_t     first = blockIdx.x * blockDim.x * (uint32_t)res_per_thread;
-  if (threadIdx.x == 0) {
-    // UE of the CTA's first RE: the last u with re_off[u] <= first.
+  const demap_tables tb     = {s_slope, s_icpt, s_width};
+  const uint32_t     ntiles = __ldg(tile_off + nof_ues);
+  for (int k = 0; k < tiles_per_cta; ++k) {
+    const uint32_t t = blockIdx.x * (uint32_t)tiles_per_cta + (uint32_t)k;
+    if (t >= ntiles) {
+      break;
+    }
+    // UE of tile t: the last u with tile_off[u] <= t.
     int lo = 0, hi = nof_ues - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(re_off + mid) <= first) {
+      if (__ldg(tile_off + mid) <= t) {
         lo = mid;
       } else {
         hi = mid - 1;
       }
     }
-    s_u0 = lo;
-  }
-  __syncthreads();
-  const demap_tables tb    = {s_slope, s_icpt, s_width};
-  const uint32_t     total = __ldg(re_off + nof_ues);
-  const uint32_t     base  = first + threadIdx.x;
-  const int          u0    = s_u0;
-  for (int k = 0; k < res_per_thread; ++k) {
-    const uint32_t rg = base + (uint32_t)k * blockDim.x;
-    if (rg >= total) {
-      break;
+    const int         u   = lo;
+    const pg_pusch_ue ue  = ues[u];
+    const int         nsc = 12 * ue.nof_rb;
+    const int         j0  = (int)(t - __ldg(tile_off + u)) * kDemodTile;
+    const int         nt  = min(kDemodTile, nsc - j0);
+    int               d0 = -1, d1 = -1, nd = 0, nds = 0;
+    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+      if ((ue.dmrs_symbol_mask >> s) & 1) {
+        if (nd == 0) {
+          d0 = s;
+        } else if (nd == 1) {
+          d1 = s;
+        }
+        ++nd;
+      }
     }
-    demod_one_re(rg, ues, nof_ues, re_off, grids, est_all, basis_all, basis_use, port_results, seq_offsets, seq, llrs,
-                 tb, u0, direct, rm_out);
+    __syncthreads(); // the previous tile's readers are done with the shared arrays
+    const bool placed = direct != nullptr && direct[u].enabled != 0;
+    if (threadIdx.x == 0) {
+      if (placed) {
+        s_dr = direct[u];
+      }
+      for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+        if (!((ue.dmrs_symbol_mask >> s) & 1)) {
+          s_sym[nds] = s;
+          s_w[nds]   = nd == 2 ? (float)(s - d0) / (float)(d1 - d0) : 0.f;
+          ++nds;
+        }
+      }
+    }
+    const int ne = nd == 2 ? 2 : 1;
+    const bool use_basis = basis_all != nullptr && basis_use != nullptr && nd == 2 && basis_use[u] != 0;
+    const float2* est = est_all + ue.est_offset;
+    const float2* bas = use_basis ? basis_all + ue.est_offset : nullptr;
+    for (int i = threadIdx.x; i < ue.nof_rx_ports * ne * ue.nof_layers * nt; i += blockDim.x) {
+      const int row = i / nt;
+      const int jj  = i - row * nt;
+      // row = (p * ne + d) * L + l of the tile; the allocation's est rows are (p * nd + d) * L + l.
+      const int l  = row % ue.nof_layers;
+      const int pd = row / ue.nof_layers;
+      const int d  = pd % ne;
+      const int p  = pd / ne;
+      const size_t src = ((size_t)(p * nd + d) * ue.nof_layers + l) * nsc + j0 + jj;
+      s_est[row * kDemodTile + jj] = est[src];
+      if (bas != nullptr) {
+        s_bas[row * kDemodTile + jj] = bas[src];
+      }
+    }
+    __syncthreads();
+    nds = 0;
+    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
+      nds += !((ue.dmrs_symbol_mask >> s) & 1);
+    }
+    const pg::rm_direct*  dr   = placed ? &s_dr : nullptr;
+    const uint32_t*       grid = grids + ue.grid_offset;
+    const pg_port_result* pres = port_results + (size_t)u * 4;
+    const uint32_t*       sq   = seq + seq_offsets[u];
+    const float2*         sb   = bas != nullptr ? s_bas : nullptr;
+    if (ue.nof_layers == 1) {
+      switch (ue.nof_rx_ports) {
+        case 1: demod_tile_qm<1, 1>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+        case 2: demod_tile_qm<1, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+        default: demod_tile_qm<1, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+      }
+    } else {
+      switch (ue.nof_rx_ports) {
+        case 2: demod_tile_qm<2, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+        default: demod_tile_qm<2, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+      }
+    }
   }
 }
 
@@ -523,62 +542,57 @@ int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
   return check_cuda(ctx, cudaGetLastError(), "scrambling_kernel launch");
 }
 
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
-                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
+                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s)
 {
-  return demod_only_launch(ctx, ues_dev, n, total_re, re_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
+  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
                            llrs, s, 256, 1);
 }
 
-int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_re,
-                      const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
+                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis,
                       const uint8_t* basis_use, const rm_direct* direct, int8_t* rm_out)
 {
-  if (n == 0 || total_re == 0) {
+  if (n == 0 || total_tiles == 0) {
     return PG_OK;
   }
   if (block != 64 && block != 128 && block != 256) {
     block = 256;
   }
   res_per_thread       = std::max(1, std::min(8, res_per_thread));
-  const uint32_t per   = (uint32_t)block * (uint32_t)res_per_thread;
-  pusch_demod_kernel<<<(total_re + per - 1) / per, block, 0, s>>>(
-      ues_dev, n, re_off_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
+  const uint32_t per   = (uint32_t)res_per_thread; // tiles per CTA
+  pusch_demod_kernel<<<(total_tiles + per - 1) / per, block, 0, s>>>(
+      ues_dev, n, tile_off_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
       basis_use, port_results, seq_offsets_dev, seq_dev, llrs, res_per_thread, direct, rm_out);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 
 // Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
-// device scratch sized by the caller from ue_codeword_bits, re_off_dev holds n + 1 prefix sums of
-// the UEs' data REs (data_re_offsets).
-int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_re,
-                 const uint32_t* re_off_dev, const uint32_t* grids, const float* est,
+// device scratch sized by the caller from ue_codeword_bits, tile_off_dev holds n + 1 prefix sums of
+// the UEs' demodulation tiles (demod_tile_offsets).
+int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_tiles,
+                 const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
                  const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
                  cudaStream_t s)
 {
   if (int rc = scrambling_launch(ctx, ues_dev, n, max_words, seq_offsets_dev, seq_dev, s)) {
     return rc;
   }
-  return demod_only_launch(ctx, ues_dev, n, total_re, re_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
-                           llrs, s);
+  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_off_dev, grids, est, port_results, seq_offsets_dev,
+                           seq_dev, llrs, s);
 }
 
-// Prefix sums of the UEs' data REs (data symbols x 12 nof_rb); returns the total.
-uint32_t data_re_offsets(const pg_pusch_ue* ues, int n, uint32_t* off)
+// Prefix sums of the UEs' demodulation tiles (kDemodTile subcarriers each); returns the total.
+uint32_t demod_tile_offsets(const pg_pusch_ue* ues, int n, uint32_t* off)
 {
   uint32_t t = 0;
   for (int i = 0; i < n; ++i) {
-    off[i]        = t;
-    const auto& u = ues[i];
-    int         nd = 0;
-    for (int s = u.first_symbol; s < u.first_symbol + u.nof_symbols; ++s) {
-      nd += (u.dmrs_symbol_mask >> s) & 1;
-    }
-    t += (uint32_t)(u.nof_symbols - nd) * 12u * u.nof_rb;
+    off[i] = t;
+    t += (12u * ues[i].nof_rb + kDemodTile - 1) / kDemodTile;
   }
   off[n] = t;
   return t;

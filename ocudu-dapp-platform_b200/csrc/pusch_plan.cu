@@ -23,7 +23,7 @@ struct pg_pusch_plan {
   pg_context*              ctx = nullptr;
   int                      nof_ues = 0, nof_cbs = 0;
   size_t                   grid_words = 0, tb_bytes = 0, nof_llrs = 0, dev_bytes = 0, est_total = 0;
-  uint32_t                 total_re = 0;
+  uint32_t                 total_tiles = 0; // demodulation tiles
   int                      max_rb   = 1;
   int                      ldpc_kinds = 0; // PG_LDPC_KIND_* present in the plan
   std::vector<pg_pusch_ue> ues;
@@ -45,7 +45,7 @@ struct pg_pusch_plan {
   pg_tb_desc*     d_tb     = nullptr;
   uint32_t*       d_cb_off = nullptr;
   uint32_t*       d_seq_off = nullptr;
-  uint32_t*       d_re_off = nullptr;
+  uint32_t*       d_tile_off = nullptr;
   uint32_t*       d_seq    = nullptr;
   float*          d_est    = nullptr;
   pg_port_result* d_pr     = nullptr;
@@ -218,7 +218,7 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     }
   }
   if (rc == PG_OK) {
-    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_re, p->d_re_off, grids, p->d_est, port_results,
+    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_tiles, p->d_tile_off, grids, p->d_est, port_results,
                            p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread,
                            p->le_net != nullptr ? p->d_basis : nullptr,
                            p->le_net != nullptr ? p->d_basis_use : nullptr, p->d_direct, p->d_rm_out);
@@ -336,8 +336,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   }
   p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
   p->est_total = est_total;
-  std::vector<uint32_t> re_off(nof_ues + 1);
-  p->total_re = data_re_offsets(p->ues.data(), nof_ues, re_off.data());
+  std::vector<uint32_t> tile_off(nof_ues + 1);
+  p->total_tiles = demod_tile_offsets(p->ues.data(), nof_ues, tile_off.data());
   sch_work w;
   if (int rc = build_sch_work(ctx, tbs.data(), nof_ues, p->nof_llrs, p->tb_bytes, w)) {
     release(p);
@@ -381,7 +381,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   build_direct(p->ues, w.rm, w.tb_first, w.tb_ncb, direct, fill);
   p->direct = direct;
   p->fill   = fill;
-  const size_t o_ework  = o_reoff + al(re_off.size() * 4);
+  const size_t o_ework  = o_reoff + al(tile_off.size() * 4);
   const size_t o_direct = o_ework + al(est_work.size() * 4);
   const size_t o_fill   = o_direct + al(direct.size() * sizeof(rm_direct));
   const size_t desc_end = o_fill + al(fill.size());
@@ -424,7 +424,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_tb      = reinterpret_cast<pg_tb_desc*>(b + o_tb);
   p->d_cb_off  = reinterpret_cast<uint32_t*>(b + o_cb_off);
   p->d_seq_off = reinterpret_cast<uint32_t*>(b + o_seqoff);
-  p->d_re_off  = reinterpret_cast<uint32_t*>(b + o_reoff);
+  p->d_tile_off = reinterpret_cast<uint32_t*>(b + o_reoff);
   p->d_seq     = reinterpret_cast<uint32_t*>(b + o_seq);
   p->d_est     = reinterpret_cast<float*>(b + o_est);
   p->d_pr      = reinterpret_cast<pg_port_result*>(b + o_pr);
@@ -454,7 +454,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
   std::memcpy(h + o_order, order.data(), order.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
-  std::memcpy(h + o_reoff, re_off.data(), re_off.size() * 4);
+  std::memcpy(h + o_reoff, tile_off.data(), tile_off.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
   std::memcpy(h + o_direct, direct.data(), direct.size() * sizeof(rm_direct));
   std::memcpy(h + o_fill, fill.data(), fill.size());
