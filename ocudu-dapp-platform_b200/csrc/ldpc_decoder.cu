@@ -1125,11 +1125,21 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& s
 // max(fma(m, f16(0.8), 1023.5) - 1024, 0) in f16: the fused multiply-add rounds once, to an integer
 // (the spacing of f16 in [1024, 2048)), and f16(0.8) = 0.7998046875 errs by at most 0.024 at
 // m = 120, inside the 0.1 margin of every rounding decision (checked for every m).
+// Check-to-variable messages are f16x2 words in the L2 slab (no byte conversions), 242,688 bytes per
+// CTA, so that the slabs of two CTAs per SM (72 MB) stay in L2.
+// Saturation: the soft update keeps 8t - 7 clamp(t, +-120) without the final clamp to +-127, so a
+// soft bit the reference saturates to +-127 is here any magnitude of at least 128 (or f16
+// infinity). Such a value acts as +-127 everywhere it is used: its bounds 104x -+ 12984 are at least
+// 328 in magnitude, so its v2c stays at least 328 (no minimum, no message-magnitude tie, the sign
+// kept) and its next soft update is again at least 128 in magnitude; the hard decision reads only
+// the sign. The message magnitudes are at most 96 and finite, so no infinity meets its negative.
 constexpr int kZ384      = 384;
 constexpr int kZH        = 192;
 constexpr int kZThreads  = 192;
-constexpr int kZMaxPerSm = 4;
-constexpr int kZ19Keep   = 8; // v2c kept in registers for the degree-19 rows
+constexpr int kZMaxPerSm = 2;   // resident CTAs per SM: two slabs of f16 messages per SM in L2
+constexpr size_t kZSlab  = 2 * (size_t)pg::kC2vStride; // bytes of one CTA's message slab
+constexpr int kZ19Keep   = 8;  // v2c kept in registers by rows above kZKeepDeg edges
+constexpr int kZKeepDeg  = 19; // rows of up to this many edges keep v2c, address and selector
 
 __constant__ uint32_t c_z_sp4[2][pg::kBg1Edges]; // 4 (s mod 192)
 __constant__ uint32_t c_z_col[2][pg::kBg1Edges]; // byte offset of the edge's column in E
@@ -1171,15 +1181,27 @@ __device__ __forceinline__ void z_edge(const int g, const int e, const uint32_t 
   adr               = k4 + c_z_col[g][e];
 }
 
-// One layer (base-graph row of degree DEG, first edge e0) for thread j. Rows of degree up to ten
-// keep each edge's v2c, address and selector from the first pass; the degree-19 rows keep the
-// v2c of their first NV edges and recompute the rest (the soft bits and messages they read are
-// not yet overwritten), so that four CTAs fit an SM without spills.
+// One layer (base-graph row of degree DEG, first edge e0) for thread j. Rows of up to kZKeepDeg
+// edges keep each edge's v2c, address and selector from the first pass (151 registers at two CTAs
+// per SM); wider rows would keep the v2c of their first kZ19Keep edges and recompute the rest (the
+// soft bits and messages they read are not yet overwritten).
+// v2c of one edge from its soft-bit pair x and its f16x2 message (saturated soft bits as +-224 or
+// more).
+template <bool FIRST>
+__device__ __forceinline__ uint32_t z_v2c(const uint32_t x, const uint32_t* __restrict__ c2v)
+{
+  uint32_t d = x;
+  if (!FIRST) {
+    d = h2_min(h2_max(h2_sub(x, *c2v), kHm120), kH120);
+  }
+  return h2_min(h2_max(d, h2_fma(x, kH104, kHm12984)), h2_fma(x, kH104, kH12984));
+}
+
 template <int DEG, bool FIRST>
 __device__ __forceinline__ void row_update_z(const int g, const int e0, const uint32_t j4, unsigned char* E,
-                                             uint16_t* __restrict__ c2v_row)
+                                             uint32_t* __restrict__ c2v_row)
 {
-  constexpr bool KEEP = DEG <= 10;
+  constexpr bool KEEP = DEG <= kZKeepDeg;
   constexpr int  NV   = KEEP ? DEG : kZ19Keep;
   uint32_t       v[NV];
   uint32_t       adr[KEEP ? DEG : 1], sel[KEEP ? DEG : 1];
@@ -1192,7 +1214,7 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
       adr[e] = a;
       sel[e] = s;
     }
-    const uint32_t vv = pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+    const uint32_t vv = z_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
     if (e < NV) {
       v[e < NV ? e : 0] = vv;
     }
@@ -1215,20 +1237,19 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
       z_edge(g, e0 + e, j4, a, s);
     }
     const uint32_t vv  = e < NV ? v[e < NV ? e : 0]
-                                : pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+                                : z_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
     const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
     const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
-    c2v_row[e * kZThreads] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+    c2v_row[e * kZThreads] = c;
     const uint32_t tt  = h2_add(c, vv);
     const uint32_t cl  = h2_min(h2_max(tt, kHm120), kH120);
-    uint32_t       u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
-    u                  = h2_min(h2_max(u, kHm127), kH127);
+    const uint32_t u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
     sts_u32(E, a, __byte_perm(u, 0, s));
   }
 }
 
 template <bool FIRST>
-__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint16_t* c2v_row)
+__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint32_t* c2v_row)
 {
   switch (deg) {
     case 3: row_update_z<3, FIRST>(g, e0, j4, E, c2v_row); break;
@@ -1270,7 +1291,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
   const int      msg_len  = Kb * kZ384;
   const int      n        = (int)d.nof_llrs;
   const int8_t*  in       = llrs + d.llr_offset;
-  uint16_t*      c2v      = reinterpret_cast<uint16_t*>(c2v_all + (size_t)slab * pg::kC2vStride);
+  uint32_t*      c2v      = reinterpret_cast<uint32_t*>(c2v_all + (size_t)slab * kZSlab);
   const int      nbytes   = msg_len / 8;
   uint8_t*       out      = bits + d.out_offset;
   const int      crc_poly = d.crc_poly;
@@ -1350,14 +1371,14 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     for (int st = 0; st < nsteps; ++st) {
       if (it > 0 || st + 1 == nsteps) {
         prefetch_step(g, st + 1 < nsteps ? st + 1 : 0, nof_layers, tid, reinterpret_cast<const char*>(c2v),
-                      kZThreads * 2);
+                      kZThreads * 4);
       }
       const int r0 = c_step_row0[g][st];
       const int r1 = min(r0 + (int)c_step_nrows[g][st], nof_layers);
       for (int r = r0; r < r1; ++r) {
         const int deg     = c_row_deg[g][r];
         const int e0      = c_row_e0[g][r];
-        uint16_t* c2v_row = c2v + (size_t)e0 * kZThreads + tid;
+        uint32_t* c2v_row = c2v + (size_t)e0 * kZThreads + tid;
         if (it == 0) {
           row_dispatch_z<true>(deg, g, e0, j4, E, c2v_row);
         } else {
@@ -1476,15 +1497,16 @@ __global__ void __launch_bounds__(kZThreads, kZMaxPerSm) ldpc_decode_z_kernel(co
     }
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
+    // Slab: kZSlab bytes per CTA (two byte-message slabs for the other lifting sizes).
     if (d.lifting_size == kZ384) {
       decode_codeblock_z384(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), llrs, bits, iterations, c2v_all, crc_pow, cb,
                             blockIdx.x);
     } else if (d.lifting_size > kX2Threads) {
       decode_codeblock_pair<kX2Threads, 1>(d, *reinterpret_cast<smem_pair_t*>(smem_z_raw), llrs, bits, iterations,
-                                           c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
+                                           c2v_all, crc_pow, scale_tab, cb, 2 * blockIdx.x);
     } else {
       decode_codeblock<0, kX2Threads, kX2Threads>(d, *reinterpret_cast<smem_x2_scalar_t*>(smem_z_raw), llrs, bits,
-                                                  iterations, c2v_all, crc_pow, cb, blockIdx.x);
+                                                  iterations, c2v_all, crc_pow, cb, 2 * blockIdx.x);
       __syncthreads();
     }
   }
@@ -1561,6 +1583,100 @@ __global__ void __launch_bounds__(kSplitThreads, kSplitMaxPerSm) ldpc_decode_spl
                                                     bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
       __syncthreads();
     }
+  }
+}
+
+
+// Longest-first work order of a batch for the persistent decoders. A codeblock's expected decoding
+// time is its work per iteration (lifting size times the check rows its input reaches, as the
+// decoder counts them from the last non-zero LLR) over its input confidence (the mean magnitude of
+// its finite non-zero LLRs, which falls as the iterations it needs rise); both come from a sample
+// of at most ~2,048 input positions. The key is 255 - 16 log2(1 + that cost), clamped to 0..255
+// (no non-zero LLR: 255), and the order lists the codeblocks by ascending key, so that the long
+// decodes start first and the short ones fill the tail. The order only schedules: every
+// codeblock's result is independent of it.
+__global__ void ldpc_score_kernel(const pg_ldpc_cb* __restrict__ descs, int n, const int8_t* __restrict__ llrs,
+                                  uint8_t* __restrict__ keys)
+{
+  const int w    = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= n) {
+    return;
+  }
+  const pg_ldpc_cb d      = descs[w];
+  const int8_t*    in     = llrs + d.llr_offset;
+  const int        len    = (int)d.nof_llrs;
+  const int        stride = max(1, len / 2048);
+  uint32_t         sum = 0, cnt = 0;
+  int              last = 0;
+  for (int k = lane * stride; k < len; k += 32 * stride) {
+    const int v = abs((int)__ldg(in + k));
+    if (v != 0) {
+      last = k + 1;
+      if (v < 127) {
+        sum += (uint32_t)v;
+        ++cnt;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
+  }
+  if (lane == 0) {
+    uint32_t key = 255u;
+    if (cnt > 0) {
+      const int   Z    = max(1, (int)d.lifting_size);
+      const int   Kb   = d.base_graph == 1 ? 22 : 10;
+      const int   nr   = d.base_graph == 1 ? pg::kBg1Rows : pg::kBg2Rows;
+      const int   rows = min(max((last + 2 * Z) / Z, Kb + 4) - Kb, nr);
+      const float mean = (float)sum / (float)cnt;
+      const float cost = (float)(rows * Z) / mean;
+      key              = 255u - (uint32_t)min(255.f, 16.f * log2f(1.f + cost));
+    }
+    keys[w] = (uint8_t)key;
+  }
+}
+
+// Counting sort of the keys in one CTA: order[0..n) = codeblocks by ascending key.
+__global__ void __launch_bounds__(1024) ldpc_sort_kernel(const uint8_t* __restrict__ keys, int n,
+                                                         uint32_t* __restrict__ order)
+{
+  __shared__ uint32_t bin[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    bin[i] = 0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    atomicAdd(&bin[keys[k]], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // Exclusive prefix sum of the 256 bins: eight per lane, then across the warp.
+    uint32_t v[8], t = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = bin[8 * threadIdx.x + i];
+      t += v[i];
+    }
+    uint32_t inc = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      inc += threadIdx.x >= (unsigned)o ? y : 0u;
+    }
+    uint32_t run = inc - t;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      bin[8 * threadIdx.x + i] = run;
+      run += v[i];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    order[atomicAdd(&bin[keys[k]], 1u)] = (uint32_t)k;
   }
 }
 
@@ -1732,8 +1848,28 @@ int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_
 int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                         int32_t* iterations, int8_t* c2v, cudaStream_t stream)
 {
-  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, nullptr, ctx->dev.ldpc_counter,
-                                stream);
+  const uint32_t* order = nullptr;
+  if (n > 1 && n <= ctx->max_codeblocks) {
+    if (int rc = ldpc_order_launch(ctx, descs_dev, n, llrs, ctx->dev.ldpc_keys, ctx->dev.ldpc_order, stream)) {
+      return rc;
+    }
+    order = ctx->dev.ldpc_order;
+  }
+  return ldpc_launch_persistent(ctx, descs_dev, n, llrs, bits, iterations, c2v, order, ctx->dev.ldpc_counter, stream);
+}
+
+int ldpc_order_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* keys,
+                      uint32_t* order, cudaStream_t stream)
+{
+  if (n <= 0) {
+    return PG_OK;
+  }
+  ldpc_score_kernel<<<(n + 7) / 8, 256, 0, stream>>>(descs_dev, n, llrs, keys);
+  if (int rc = check_cuda(ctx, cudaGetLastError(), "ldpc_score_kernel launch")) {
+    return rc;
+  }
+  ldpc_sort_kernel<<<1, 1024, 0, stream>>>(keys, n, order);
+  return check_cuda(ctx, cudaGetLastError(), "ldpc_sort_kernel launch");
 }
 
 unsigned int timing_record_flags(pg_context* ctx, cudaStream_t s)

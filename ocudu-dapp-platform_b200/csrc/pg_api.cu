@@ -2,6 +2,8 @@
 // argument validation, staging and launches.
 #include "pg_internal.h"
 
+#include <algorithm>
+
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -275,8 +277,10 @@ int pg_create(const pg_config* cfg, pg_context** out)
     rc = check_cuda(ctx, cudaEventCreateWithFlags(&ctx->ev_desc, cudaEventDisableTiming), "cudaEventCreate");
   }
   if (rc == PG_OK) {
+    // One slab per resident decoder CTA: at most four per SM (two of twice the size for the Z = 384
+    // decoder), and at most one per codeblock.
     rc = check_cuda(ctx,
-                    cudaMalloc(&ctx->dev.c2v, (size_t)cfg->max_codeblocks * kC2vStride),
+                    cudaMalloc(&ctx->dev.c2v, (size_t)std::max(cfg->max_codeblocks, 4 * ctx->sm_count) * kC2vStride),
                     "cudaMalloc(check-to-variable scratch)");
   }
   if (rc == PG_OK) {
@@ -293,6 +297,13 @@ int pg_create(const pg_config* cfg, pg_context** out)
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_counter, 2 * sizeof(int)), "cudaMalloc(ldpc counter)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_keys, (size_t)cfg->max_codeblocks), "cudaMalloc(ldpc keys)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_order, (size_t)cfg->max_codeblocks * sizeof(uint32_t)),
+                    "cudaMalloc(ldpc order)");
   }
   if (rc == PG_OK) {
     ctx->ldpc_ctas = ldpc_resident_ctas(ctx);
@@ -380,6 +391,8 @@ void pg_destroy(pg_context* ctx)
   cudaFree(ctx->dev.bits);
   cudaFree(ctx->dev.iterations);
   cudaFree(ctx->dev.ldpc_counter);
+  cudaFree(ctx->dev.ldpc_keys);
+  cudaFree(ctx->dev.ldpc_order);
   cudaFree(ctx->dev.ldpc_scale);
   if (ctx->host_descs) {
     cudaFreeHost(ctx->host_descs);

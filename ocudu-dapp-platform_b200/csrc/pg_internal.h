@@ -63,6 +63,8 @@ struct device_buffers {
   uint8_t*     bits        = nullptr;
   int32_t*     iterations  = nullptr;
   int*         ldpc_counter = nullptr; // work counters of the persistent decoders (two ints)
+  uint8_t*     ldpc_keys    = nullptr; // max_codeblocks work-order keys of the batch decodes
+  uint32_t*    ldpc_order   = nullptr; // max_codeblocks work-order entries
   uint16_t*    ldpc_scale   = nullptr; // scale table of the two-lanes-per-thread decoder
   size_t       llr_cap     = 0;
   size_t       bits_cap    = 0;
@@ -96,7 +98,7 @@ struct pg_context {
   size_t              scratch_b_cap  = 0;
   bool                timed          = false;
   int8_t*             static_c2v     = nullptr;  // device address of the module-static LDPC scratch
-  int                 ldpc_kernel    = PG_LDPC_KERNEL_SPLIT; // kernel of the batch decodes (pg_ldpc_kernel)
+  int                 ldpc_kernel    = PG_LDPC_KERNEL_Z384; // kernel of the batch decodes (pg_ldpc_kernel)
   int                 ldpc_ctas_per_sm = 0;   // resident CTAs per SM of the batch decodes (0: kernel limit)
   std::string         last_error;
 };
@@ -219,6 +221,9 @@ int ldpc_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_
 // Same with a caller-provided check-to-variable scratch of min(n, ldpc_ctas) * kC2vStride bytes.
 int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,
                         int32_t* iterations, int8_t* c2v, cudaStream_t stream);
+// Hardest-first work order (ldpc_score_kernel + ldpc_sort_kernel): keys n bytes, order n entries.
+int ldpc_order_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* keys,
+                      uint32_t* order, cudaStream_t stream);
 // Persistent launch: min(n, ldpc_ctas) CTAs take codeblocks order[0..n) (identity when order is
 // null) from *counter (device int, zeroed here on the stream); c2v holds one slab per CTA.
 int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const int8_t* llrs, uint8_t* bits,

@@ -55,7 +55,8 @@ struct pg_pusch_plan {
   uint32_t*       d_tb_crc = nullptr;
   int32_t*        d_iters  = nullptr;
   int8_t*         d_c2v    = nullptr;
-  uint32_t*       d_order  = nullptr; // LDPC work order: largest codeblocks first
+  uint32_t*       d_order  = nullptr;
+  uint8_t*        d_keys   = nullptr; // work-order keys of the codeblocks // LDPC work order: largest codeblocks first
   int*            d_counter = nullptr; // work counter of the persistent decoder
   uint32_t*       d_grid   = nullptr; // grids of execute_host
   uint8_t*        d_tb_out = nullptr; // TBs of execute_host
@@ -87,7 +88,7 @@ struct pg_pusch_plan {
   int             le_nseq   = 0;
   int             le_rows   = 0;
   // Launch shapes (defaults, or the autotuner's choice).
-  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, PG_LDPC_KERNEL_SPLIT};
+  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, PG_LDPC_KERNEL_Z384};
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -227,6 +228,10 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb,
                              p->d_fill);
   }
+  if (rc == PG_OK && p->nof_cbs > 1) {
+    // Hardest first: the decoders take the codeblocks in ascending order of input confidence.
+    rc = ldpc_order_launch(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_keys, p->d_order, s);
+  }
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
                                 p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count,
@@ -362,8 +367,9 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   for (const pg_ldpc_cb& l : w.ldpc) {
     p->ldpc_kinds |= l.lifting_size == 384 ? PG_LDPC_KIND_Z384 : PG_LDPC_KIND_OTHER;
   }
-  // One check-to-variable slab per decoder CTA: up to four per SM (the Z = 384 decoder).
-  const int ldpc_slabs = std::max(1, std::min(p->nof_cbs, 4 * ctx->sm_count));
+  // One check-to-variable slab per decoder CTA: up to four per SM, or two of twice the size (the
+  // Z = 384 decoder's f16 messages), at most one CTA per codeblock.
+  const int ldpc_slabs = std::max(2, 2 * std::min(p->nof_cbs, 2 * ctx->sm_count));
 
   // Device image: descriptors first (uploaded once), then the workspace.
   const size_t o_ues    = 0;
@@ -393,7 +399,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_bits   = o_rmout + al(w.rm_total);
   const size_t o_crc    = o_bits + al(w.bits_total);
   const size_t o_it     = o_crc + al((size_t)nof_ues * 4);
-  const size_t o_cnt    = o_it + al((size_t)p->nof_cbs * 4);
+  const size_t o_keys   = o_it + al((size_t)p->nof_cbs * 4);
+  const size_t o_cnt    = o_keys + al((size_t)p->nof_cbs);
   const size_t o_c2v    = o_cnt + al(sizeof(int));
   const size_t o_grid   = o_c2v + al((size_t)ldpc_slabs * kC2vStride);
   const size_t o_tbout  = o_grid + al(grid_words * 4);
@@ -436,6 +443,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_c2v     = reinterpret_cast<int8_t*>(b + o_c2v);
   p->d_order   = reinterpret_cast<uint32_t*>(b + o_order);
   p->d_counter = reinterpret_cast<int*>(b + o_cnt);
+  p->d_keys    = b + o_keys;
   p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
   p->d_tb_out  = b + o_tbout;
   p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);

@@ -168,3 +168,57 @@ def test_pair_fill_layout():
                 assert a == col * Z + wp - 2 * Z and b == a + H
                 soft.update((a, b))
             assert soft == set(range(-2 * Z, (nfull - 2) * Z))
+
+
+def z_kernel_v(x, c, first):
+    """The Z = 384 decoder's v: as kernel_v, on soft bits that may also be saturated as any
+    magnitude of at least 128 or f16 infinity."""
+    x16 = x.astype(np.float16)
+    with np.errstate(over="ignore", invalid="ignore"):
+        d = x16 if first else np.clip((x16.astype(np.float64) - c).astype(np.float16), -120, 120).astype(np.float16)
+        lo = (x16.astype(np.float64) * 104 - 12984).astype(np.float16)
+        hi = (x16.astype(np.float64) * 104 + 12984).astype(np.float16)
+    return np.minimum(np.maximum(d, lo), hi)
+
+
+def z_kernel_soft(v, cnew):
+    """The Z = 384 decoder's soft update: 8t - 7 clamp(t, +-120) without the final clamp."""
+    with np.errstate(over="ignore", invalid="ignore"):
+        t = (cnew.astype(np.float64) + v.astype(np.float64)).astype(np.float16)
+        cl = np.clip(t, -120, 120).astype(np.float16)
+        t8 = (t.astype(np.float64) * 8).astype(np.float16)
+        return (cl.astype(np.float64) * -7 + t8.astype(np.float64)).astype(np.float16)
+
+
+def test_z384_unclamped_saturation_acts_as_127():
+    """Soft bits the reference saturates to +-127 are, in the Z = 384 decoder, any magnitude of at
+    least 128 or infinity (no clamp after the soft update). Over every finite soft bit, saturated
+    ones of many magnitudes, every stored message c and new message cnew (|.| <= 96): the v2c has
+    the reference's sign, acts alike in the minimum search (start 120) and the message-magnitude
+    test, and the soft update gives the reference's value, saturated ones as magnitudes >= 128,
+    never a NaN and never a magnitude in (120, 128)."""
+    big = [128, 129, 200, 1000, 2047, 5000, 60000, np.inf]
+    for first in (True, False):
+        fin = list(range(-126, 127)) if first else list(range(-120, 121))
+        xs = np.array(fin + [127, -127] + big + [-b for b in big], np.float64)
+        cs = np.array([0]) if first else np.arange(-96, 97)
+        cnew = np.arange(-96, 97)
+        x, c, cn = np.meshgrid(xs, cs, cnew, indexing="ij")
+        x, c, cn = x.ravel(), c.ravel(), cn.ravel()
+        sat = np.abs(x) >= 127
+        xr = np.where(sat, np.sign(x) * 127, x)                      # the reference's soft bit
+        ref_v = xr if first else np.where(sat, xr, np.clip(xr - c, -120, 120))
+        v = z_kernel_v(x, c, first).astype(np.float64)
+        assert not np.isnan(v).any()
+        assert (np.sign(v) == np.sign(ref_v)).all()
+        assert (np.minimum(np.abs(v), 120) == np.minimum(np.abs(ref_v), 120)).all()
+        fin_v = np.abs(ref_v) < 127
+        assert (v[fin_v] == ref_v[fin_v]).all()
+        assert (np.abs(v[~fin_v]) >= 217).all()
+        ref_t = cn + ref_v
+        ref_soft = np.where(np.abs(ref_v) == 127, ref_v, np.where(np.abs(ref_t) > 120, np.sign(ref_t) * 127, ref_t))
+        u = z_kernel_soft(v, cn).astype(np.float64)
+        assert not np.isnan(u).any()
+        assert not ((np.abs(u) > 120) & (np.abs(u) < 128)).any()
+        got = np.where(np.abs(u) >= 128, np.sign(u) * 127, u)
+        assert (got == ref_soft).all()
