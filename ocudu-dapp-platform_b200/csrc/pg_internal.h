@@ -201,11 +201,12 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
 // Channel estimation of a batch (pusch_estimate_chunk_kernel + pusch_estimate_finish_kernel).
 // est_work_build writes the work list of the UEs (one item per (UE, port, chunk of pilots)) followed
 // by the first item of every (UE, port) (4 n + 1 entries) and returns the item count; work_dev
-// holds that blob on the device, partials nwork float4.
+// holds that blob on the device, partials nwork float4, arrivals 4 n ints that are zero before the
+// launch (and again after it).
 int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob);
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
-                    void* partials, const uint32_t* grids, float* est, float* ls, pg_port_result* results,
-                    cudaStream_t s);
+                    void* partials, int* arrivals, const uint32_t* grids, float* est, float* ls,
+                    pg_port_result* results, cudaStream_t s);
 // The same from host UEs: stages the UEs and their work list (SLOT_UE), partials in the context.
 int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const uint32_t* grids, float* est, float* ls,
                          pg_port_result* results, cudaStream_t s);

@@ -414,8 +414,9 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
 // reaches past either end of the allocation, the smoothed estimates of its own pilots and of the
 // next one (for the frequency interpolation of its last odd subcarrier), and its partial sums of
 // RSRP, EPRE and noise. Per element the arithmetic and its order are those of
-// pusch_estimate_kernel, so the frequency responses are identical; pusch_estimate_finish_kernel
-// then adds each (UE, port)'s partial sums in chunk order (deterministic) and forms the scalars.
+// pusch_estimate_kernel, so the frequency responses are identical. The last CTA of each (UE, port)
+// to finish (a per-port arrival counter, reset by that CTA for the next launch) adds the port's
+// partial sums in chunk order (deterministic) and forms the scalars.
 constexpr int kChunk        = 128;
 constexpr int kHalo         = 8;  // even, >= the largest filter half-length (7)
 constexpr int kTileOff      = 16; // tile position of pilot k is k - (k0 - kTileOff)
@@ -429,7 +430,9 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
                                                                              float2* __restrict__ ls_all,
                                                                              float4* __restrict__ partials,
                                                                              const uint32_t* __restrict__ gold,
-                                                                             uint32_t gold_words)
+                                                                             uint32_t gold_words,
+                                                                             int* __restrict__ arrivals,
+                                                                             pg_port_result* __restrict__ results)
 {
   __shared__ uint32_t s_bits[kMaxDmrs][(2 * kChunkTile) / 32 + 2];
   __shared__ float2   s_ls[kMaxDmrs][2][kChunkTile];
@@ -618,50 +621,34 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
       t.w += s_red[w][3];
     }
     partials[blockIdx.x] = t;
+    __threadfence();
+    const int       pi    = 4 * u + port;
+    const uint32_t* first = work + gridDim.x; // the work list (one item per CTA), then each port's first item
+    const int       nch   = (int)(first[pi + 1] - first[pi]);
+    if (atomicAdd(&arrivals[pi], 1) == nch - 1) {
+      // Last chunk of this port: every other chunk's partials are visible (fence before arrival).
+      float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (uint32_t w = first[pi]; w < first[pi + 1]; ++w) {
+        const float4 p = __ldcg(partials + w);
+        s.x += p.x;
+        s.y += p.y;
+        s.z += p.z;
+        s.w += p.w;
+      }
+      arrivals[pi]     = 0;
+      const float n_pil = (float)(npil * nd);
+      pg_port_result pr;
+      pr.rsrp[0]       = s.x * beta * beta / n_pil;
+      pr.rsrp[1]       = nl > 1 ? s.y * beta * beta / n_pil : 0.f;
+      pr.epre          = s.z / n_pil;
+      const float ravg = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
+      float       nvar = (pg::is_normal(s.w) ? s.w : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
+      nvar             = fmaxf(ravg / 1e10f, nvar);
+      pr.noise_var     = nvar;
+      pr.snr           = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
+      results[pi]      = pr;
+    }
   }
-}
-
-// Port results of every (UE, port): partial sums of the port's chunks (work items first[i] ..
-// first[i + 1] - 1, i = 4 u + port) in chunk order, then the scalars of pusch_estimate_kernel.
-__global__ void pusch_estimate_finish_kernel(const pg_pusch_ue* __restrict__ ues, int n,
-                                             const uint32_t* __restrict__ first, const float4* __restrict__ partials,
-                                             pg_port_result* __restrict__ results)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 4 * n) {
-    return;
-  }
-  const int         u    = i >> 2;
-  const int         port = i & 3;
-  const pg_pusch_ue ue   = ues[u];
-  if (port >= ue.nof_rx_ports) {
-    return;
-  }
-  int nd = 0;
-  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && nd < kMaxDmrs; ++s) {
-    nd += (ue.dmrs_symbol_mask >> s) & 1;
-  }
-  float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-  for (uint32_t w = first[i]; w < first[i + 1]; ++w) {
-    const float4 p = partials[w];
-    t.x += p.x;
-    t.y += p.y;
-    t.z += p.z;
-    t.w += p.w;
-  }
-  const int      nl    = ue.nof_layers;
-  const float    beta  = ue.dmrs_scaling;
-  const float    n_pil = (float)(6 * ue.nof_rb * nd);
-  pg_port_result pr;
-  pr.rsrp[0]       = t.x * beta * beta / n_pil;
-  pr.rsrp[1]       = nl > 1 ? t.y * beta * beta / n_pil : 0.f;
-  pr.epre          = t.z / n_pil;
-  const float ravg = nl > 1 ? (pr.rsrp[0] + pr.rsrp[1]) / 2.f : pr.rsrp[0];
-  float       nvar = (pg::is_normal(t.w) ? t.w : 0.f) / (n_pil * (float)((nl + 1) / 2) - 1.f);
-  nvar             = fmaxf(ravg / 1e10f, nvar);
-  pr.noise_var     = nvar;
-  pr.snr           = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
-  results[i]       = pr;
 }
 
 // Per-symbol estimates of one UE: f[i] + (f[i+1] - f[i]) w rounded to bf16 (the reference's
@@ -897,23 +884,16 @@ int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob)
 }
 
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
-                    void* partials, const uint32_t* grids, float* est, float* ls, pg_port_result* results,
-                    cudaStream_t s)
+                    void* partials, int* arrivals, const uint32_t* grids, float* est, float* ls,
+                    pg_port_result* results, cudaStream_t s)
 {
-  if (n == 0) {
+  if (n == 0 || nwork == 0) {
     return PG_OK;
   }
-  if (nwork > 0) {
-    pusch_estimate_chunk_kernel<<<nwork, kChunkThreads, 0, s>>>(
-        ues_dev, work_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls),
-        static_cast<float4*>(partials), ctx->dev.gold, kGoldWords);
-    if (int rc = check_cuda(ctx, cudaGetLastError(), "pusch_estimate_chunk_kernel launch")) {
-      return rc;
-    }
-  }
-  pusch_estimate_finish_kernel<<<(4 * n + 127) / 128, 128, 0, s>>>(ues_dev, n, work_dev + nwork,
-                                                                    static_cast<const float4*>(partials), results);
-  return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_finish_kernel launch");
+  pusch_estimate_chunk_kernel<<<nwork, kChunkThreads, 0, s>>>(
+      ues_dev, work_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls),
+      static_cast<float4*>(partials), ctx->dev.gold, kGoldWords, arrivals, results);
+  return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_chunk_kernel launch");
 }
 
 int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const uint32_t* grids, float* est, float* ls,
@@ -928,13 +908,20 @@ int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const u
   if (int rc = stage_slot(ctx, SLOT_UE, staged.data(), staged.size(), s, &dev)) {
     return rc;
   }
+  // Partial sums (nwork float4), then the per-port arrival counters (4 n ints, zeroed here; each
+  // port's last chunk leaves its counter at zero again).
+  const size_t part_bytes = (size_t)nwork * sizeof(float4);
   if (int rc = ensure_scratch(ctx, &ctx->est_partials, &ctx->est_partials_cap,
-                              std::max<size_t>(16, (size_t)nwork * sizeof(float4)), "cudaMalloc(estimate partials)")) {
+                              std::max<size_t>(16, part_bytes + (size_t)16 * n), "cudaMalloc(estimate partials)")) {
+    return rc;
+  }
+  int* arrivals = reinterpret_cast<int*>(static_cast<uint8_t*>(ctx->est_partials) + part_bytes);
+  if (int rc = check_cuda(ctx, cudaMemsetAsync(arrivals, 0, (size_t)16 * n, s), "cudaMemsetAsync(arrivals)")) {
     return rc;
   }
   const pg_pusch_ue* d_ues  = static_cast<const pg_pusch_ue*>(dev);
   const uint32_t*    d_work = reinterpret_cast<const uint32_t*>(static_cast<uint8_t*>(dev) + (size_t)n * sizeof(pg_pusch_ue));
-  if (int rc = estimate_launch(ctx, d_ues, n, d_work, nwork, ctx->est_partials, grids, est, ls, results, s)) {
+  if (int rc = estimate_launch(ctx, d_ues, n, d_work, nwork, ctx->est_partials, arrivals, grids, est, ls, results, s)) {
     return rc;
   }
   return release_slot_after(ctx, SLOT_UE, s);

@@ -39,6 +39,7 @@ struct pg_pusch_plan {
   uint8_t*        d_fill     = nullptr; // per codeblock: 1 when the demodulator placed its LLRs
   uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
   void*           d_est_part = nullptr; // its partial sums
+  int*            d_est_arr  = nullptr; // per-(UE, port) arrival counters, zero between executions
   int             est_nwork  = 0;
   pg_rm_cb*       d_rm     = nullptr;
   pg_ldpc_cb*     d_ldpc   = nullptr;
@@ -204,8 +205,9 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
             pg_port_result* port_results, cudaStream_t s)
 {
   pg_context* ctx = p->ctx;
-  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->d_est_work, p->est_nwork, p->d_est_part, grids,
-                                    p->d_est, p->le_net != nullptr ? p->d_ls : nullptr, port_results, s);
+  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->d_est_work, p->est_nwork, p->d_est_part,
+                                    p->d_est_arr, grids, p->d_est, p->le_net != nullptr ? p->d_ls : nullptr,
+                                    port_results, s);
   if (rc == PG_OK && p->le_net != nullptr) {
     const unsigned int flags = timing_record_flags(ctx, s);
     if (ctx->timed) {
@@ -406,7 +408,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_tbout  = o_grid + al(grid_words * 4);
   const size_t o_res    = o_tbout + al(p->tb_bytes);
   const size_t o_epart  = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
-  p->dev_bytes          = o_epart + al((size_t)std::max(1, p->est_nwork) * 16);
+  const size_t o_earr   = o_epart + al((size_t)std::max(1, p->est_nwork) * 16);
+  p->dev_bytes          = o_earr + al((size_t)nof_ues * 16);
 
   const size_t h_res  = 0;
   const size_t h_pr   = h_res + al((size_t)nof_ues * sizeof(pg_sch_result));
@@ -451,6 +454,7 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_direct   = reinterpret_cast<rm_direct*>(b + o_direct);
   p->d_fill     = b + o_fill;
   p->d_est_part = b + o_epart;
+  p->d_est_arr  = reinterpret_cast<int*>(b + o_earr);
 
   // Descriptor image in pinned memory, one upload.
   uint8_t* h = static_cast<uint8_t*>(p->host);
@@ -470,6 +474,9 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(b + o_seq, 0, al(seq_total * 4), s), "cudaMemsetAsync(sequences)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemsetAsync(b + o_earr, 0, (size_t)nof_ues * 16, s), "cudaMemsetAsync(arrivals)");
   }
   if (rc == PG_OK) {
     rc = scrambling_launch(ctx, p->d_ues, nof_ues, max_words, p->d_seq_off, p->d_seq, s);

@@ -67,16 +67,91 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   int8_t*        out = out_all + d.out_offset;
   const bool     nd  = d.new_data != 0;
 
+  if (E <= V && fill_only != nullptr && fill_only[blockIdx.x] != 0) {
+    // The demodulator placed this codeblock's LLRs itself (new data, E <= V): they occupy the valid
+    // indices [v0, v0 + E) mod V, up to four position intervals past the fillers. Every other
+    // position is a filler (+127) or unreached / beyond N_cb (0). The buffer is written in 16-byte
+    // chunks: chunks of placed LLRs only are skipped, chunks without any are stored whole, and the
+    // few chunks that mix them are merged byte by byte.
+    int       ka[4], kb[4], nk = 0;
+    const int e_end = v0 + E;
+    auto add_v = [&](int a, int b) {
+      const int b1 = min(b, inf);
+      if (a < b1) {
+        ka[nk] = a;
+        kb[nk] = b1;
+        ++nk;
+      }
+      const int a2 = max(a, inf);
+      if (a2 < b) {
+        ka[nk] = a2 + F;
+        kb[nk] = b + F;
+        ++nk;
+      }
+    };
+    if (e_end <= V) {
+      add_v(v0, e_end);
+    } else {
+      add_v(v0, V);
+      add_v(0, e_end - V);
+    }
+    auto placed_at = [&](int p) {
+      bool k = false;
+      for (int i = 0; i < nk; ++i) {
+        k |= p >= ka[i] && p < kb[i];
+      }
+      return k;
+    };
+    auto fill_value = [&](int p) { return (int8_t)((p >= inf && p < sys) ? 127 : 0); };
+    const int head  = (int)((16u - (unsigned)(reinterpret_cast<uintptr_t>(out) & 15u)) & 15u);
+    const int first = min(head, N);
+    const int nch   = (N - first) / 16;
+    const int tail  = first + 16 * nch;
+    for (int p = blockIdx.y * kRmThreads + threadIdx.x; p < first; p += gridDim.y * kRmThreads) {
+      if (!placed_at(p)) {
+        out[p] = fill_value(p);
+      }
+    }
+    for (int p = tail + blockIdx.y * kRmThreads + threadIdx.x; p < N; p += gridDim.y * kRmThreads) {
+      if (!placed_at(p)) {
+        out[p] = fill_value(p);
+      }
+    }
+    for (int q = blockIdx.y * kRmThreads + threadIdx.x; q < nch; q += gridDim.y * kRmThreads) {
+      const int c = first + 16 * q;
+      int       kept = 0;
+      for (int i = 0; i < nk; ++i) {
+        kept += max(0, min(c + 16, kb[i]) - max(c, ka[i]));
+      }
+      if (kept == 16) {
+        continue;
+      }
+      const int fil = max(0, min(c + 16, sys) - max(c, inf));
+      uint4*    dst = reinterpret_cast<uint4*>(out + c);
+      if (kept == 0 && fil == 0) {
+        *dst = make_uint4(0u, 0u, 0u, 0u);
+      } else if (kept == 0 && fil == 16) {
+        *dst = make_uint4(0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu);
+      } else {
+        uint4   w = *dst;
+        int8_t* b = reinterpret_cast<int8_t*>(&w);
+        for (int i = 0; i < 16; ++i) {
+          if (!placed_at(c + i)) {
+            b[i] = fill_value(c + i);
+          }
+        }
+        *dst = w;
+      }
+    }
+    return;
+  }
   if (E <= V) {
-    // Codeblocks whose LLRs the demodulator placed itself (new data, E <= V) need only the
-    // positions no input reaches.
-    const bool placed = fill_only != nullptr && fill_only[blockIdx.x] != 0;
     // No repetition: each buffer position receives at most one input. The input, row i holding
     // the Qm LLRs of de-interleaver column i, is read a tile of rows at a time (coalesced) and
     // transposed through shared memory; bit plane j of rows i0.. lands on consecutive buffer
     // positions (t = j Kq + i, valid index (v0 + t) mod V, past the fillers), so the stores are
     // coalesced too. Positions no input reaches are written by the per-position loop below.
-    const int ntiles = placed ? 0 : (Kq + kRmTileRows - 1) / kRmTileRows;
+    const int ntiles = (Kq + kRmTileRows - 1) / kRmTileRows;
     for (int tl = blockIdx.y; tl < ntiles; tl += gridDim.y) {
       const int i0   = tl * kRmTileRows;
       const int rows = min(kRmTileRows, Kq - i0);
