@@ -58,7 +58,8 @@ INT_OPS_PER_EDGE = 10
 LDPC_KERNEL_NAMES = ["ldpc_decode_kernel (one lifted lane per thread)",
                      "ldpc_decode_x2_kernel (two lifted lanes per thread for even Z > 192)",
                      "ldpc_decode_split_kernel (two lanes per thread pair, row edges split over the pair)",
-                     "ldpc_decode_z_kernel (two lifted lanes per thread, Z = 384 specialised, f16 soft-bit pairs)"]
+                     "ldpc_decode_z_kernel (two lifted lanes per thread, Z = 384 specialised, f16 soft-bit pairs)",
+                     "ldpc_decode_zs_kernel (Z = 384 specialised, row edges split over a thread pair)"]
 # Integer-instruction throughput probe (the LDPC roofline denominator), built by
 # ocudu-dapp-platform_b200/measure/Makefile.
 PROBE_SO = os.path.join(ROOT, "ocudu-dapp-platform_b200", "measure", "_lib", "libpg_probe.so")

@@ -1125,8 +1125,8 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& s
 // max(fma(m, f16(0.8), 1023.5) - 1024, 0) in f16: the fused multiply-add rounds once, to an integer
 // (the spacing of f16 in [1024, 2048)), and f16(0.8) = 0.7998046875 errs by at most 0.024 at
 // m = 120, inside the 0.1 margin of every rounding decision (checked for every m).
-// Check-to-variable messages are f16x2 words in the L2 slab (no byte conversions), 242,688 bytes per
-// CTA, so that the slabs of two CTAs per SM (72 MB) stay in L2.
+// Check-to-variable messages are offset-binary byte pairs per (edge, thread) in the L2 slab, as in
+// the two-lanes-per-thread decoder.
 // Saturation: the soft update keeps 8t - 7 clamp(t, +-120) without the final clamp to +-127, so a
 // soft bit the reference saturates to +-127 is here any magnitude of at least 128 (or f16
 // infinity). Such a value acts as +-127 everywhere it is used: its bounds 104x -+ 12984 are at least
@@ -1136,22 +1136,23 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& s
 constexpr int kZ384      = 384;
 constexpr int kZH        = 192;
 constexpr int kZThreads  = 192;
-constexpr int kZMaxPerSm = 2;   // resident CTAs per SM: two slabs of f16 messages per SM in L2
-constexpr size_t kZSlab  = 2 * (size_t)pg::kC2vStride; // bytes of one CTA's message slab
+constexpr int kZMaxPerSm = 4;   // resident CTAs per SM (registers and shared memory)
 constexpr int kZ19Keep   = 8;  // v2c kept in registers by rows above kZKeepDeg edges
-constexpr int kZKeepDeg  = 19; // rows of up to this many edges keep v2c, address and selector
+constexpr int kZKeepDeg  = 10; // rows of up to this many edges keep v2c, address and selector
 
 __constant__ uint32_t c_z_sp4[2][pg::kBg1Edges]; // 4 (s mod 192)
 __constant__ uint32_t c_z_col[2][pg::kBg1Edges]; // byte offset of the edge's column in E
 __constant__ uint32_t c_z_sel[2][pg::kBg1Edges]; // selector when j + s' >= 192
 
-struct __align__(16) smem_z_t {
+template <int NT>
+struct __align__(16) smem_z_nt_t {
   uint32_t E[pg::kMaxNodes * kZH];
   uint32_t hard[(22 * kZ384) / 32];
-  uint32_t red[kZThreads / 32];
+  uint32_t red[NT / 32];
   int      s_last;
   int      s_done;
 };
+using smem_z_t = smem_z_nt_t<kZThreads>;
 
 constexpr uint32_t kH0p8     = 0x3a663a66u; // f16(0.8) = 0.7998046875
 constexpr uint32_t kH1023p5  = 0x63ff63ffu; // 1023.5
@@ -1182,24 +1183,12 @@ __device__ __forceinline__ void z_edge(const int g, const int e, const uint32_t 
 }
 
 // One layer (base-graph row of degree DEG, first edge e0) for thread j. Rows of up to kZKeepDeg
-// edges keep each edge's v2c, address and selector from the first pass (151 registers at two CTAs
-// per SM); wider rows would keep the v2c of their first kZ19Keep edges and recompute the rest (the
-// soft bits and messages they read are not yet overwritten).
-// v2c of one edge from its soft-bit pair x and its f16x2 message (saturated soft bits as +-224 or
-// more).
-template <bool FIRST>
-__device__ __forceinline__ uint32_t z_v2c(const uint32_t x, const uint32_t* __restrict__ c2v)
-{
-  uint32_t d = x;
-  if (!FIRST) {
-    d = h2_min(h2_max(h2_sub(x, *c2v), kHm120), kH120);
-  }
-  return h2_min(h2_max(d, h2_fma(x, kH104, kHm12984)), h2_fma(x, kH104, kH12984));
-}
-
+// edges keep each edge's v2c, address and selector from the first pass; the degree-19 rows keep
+// the v2c of their first kZ19Keep edges and recompute the rest (the soft bits and messages they
+// read are not yet overwritten), so that four CTAs fit an SM without spills.
 template <int DEG, bool FIRST>
 __device__ __forceinline__ void row_update_z(const int g, const int e0, const uint32_t j4, unsigned char* E,
-                                             uint32_t* __restrict__ c2v_row)
+                                             uint16_t* __restrict__ c2v_row)
 {
   constexpr bool KEEP = DEG <= kZKeepDeg;
   constexpr int  NV   = KEEP ? DEG : kZ19Keep;
@@ -1214,7 +1203,7 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
       adr[e] = a;
       sel[e] = s;
     }
-    const uint32_t vv = z_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+    const uint32_t vv = pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZH);
     if (e < NV) {
       v[e < NV ? e : 0] = vv;
     }
@@ -1237,10 +1226,10 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
       z_edge(g, e0 + e, j4, a, s);
     }
     const uint32_t vv  = e < NV ? v[e < NV ? e : 0]
-                                : z_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZThreads);
+                                : pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZH);
     const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
     const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
-    c2v_row[e * kZThreads] = c;
+    c2v_row[e * kZH] = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
     const uint32_t tt  = h2_add(c, vv);
     const uint32_t cl  = h2_min(h2_max(tt, kHm120), kH120);
     const uint32_t u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
@@ -1248,8 +1237,89 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
   }
 }
 
+// The same layer split over the two threads of lane pair j (t = 0, 1): thread t takes edges t,
+// t + 2, ... (a missing last edge of an odd-degree row contributes +120, which changes no minimum
+// and no sign), the two partial (min1, min2, sign) meet through one shuffle, and each thread updates
+// its own edges.
+template <int DEG, bool FIRST>
+__device__ __forceinline__ void row_update_z_split(const int g, const int e0, const uint32_t j4, const int t,
+                                                   unsigned char* E, uint16_t* __restrict__ c2v_row)
+{
+  constexpr int  NE   = (DEG + 1) / 2;
+  constexpr bool KEEP = NE <= 3; // wider rows recompute address and selector (register budget)
+  uint32_t       v[NE], adr[KEEP ? NE : 1], sel[KEEP ? NE : 1];
+  uint32_t       min1 = kH120, min2 = kH120;
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const int  e     = 2 * k + t;
+    const bool valid = (DEG % 2) == 0 || k + 1 < NE || e < DEG;
+    uint32_t   vv    = kH120;
+    if (valid) {
+      uint32_t a, s;
+      z_edge(g, e0 + e, j4, a, s);
+      if constexpr (KEEP) {
+        adr[k] = a;
+        sel[k] = s;
+      }
+      vv = pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZH);
+    }
+    v[k]             = vv;
+    const uint32_t x = h2_max_xs(min1, vv);
+    min2             = h2_min_xs(min2, x);
+    min1             = h2_min_xs(min1, vv);
+  }
+  const uint32_t o1 = __shfl_xor_sync(0xffffffffu, min1, 1);
+  const uint32_t o2 = __shfl_xor_sync(0xffffffffu, min2, 1);
+  min2              = h2_min_xs(h2_min_xs(min2, o2), h2_max_xs(min1, o1));
+  min1              = h2_min_xs(min1, o1);
+  const uint32_t m1  = min1 & kAbs;
+  const uint32_t s1  = z_scale(m1);
+  const uint32_t s2  = z_scale(min2 & kAbs);
+  const uint32_t nds = h2_sub(s1, s2);
+  const uint32_t sgn = min1 & kSign; // sign product of every v2c of the row
+#pragma unroll
+  for (int k = 0; k < NE; ++k) {
+    const int  e     = 2 * k + t;
+    const bool valid = (DEG % 2) == 0 || k + 1 < NE || e < DEG;
+    if (valid) {
+      uint32_t a, s;
+      if constexpr (KEEP) {
+        a = adr[k];
+        s = sel[k];
+      } else {
+        z_edge(g, e0 + e, j4, a, s);
+      }
+      const uint32_t vv  = v[k];
+      const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
+      const uint32_t c   = mag ^ ((sgn ^ vv) & kSign);
+      c2v_row[e * kZH]   = (uint16_t)__byte_perm(h2_to_bytes_biased(c), 0, 0x0020);
+      const uint32_t tt  = h2_add(c, vv);
+      const uint32_t cl  = h2_min(h2_max(tt, kHm120), kH120);
+      const uint32_t u   = h2_fma(cl, kHm7, h2_mul(tt, kH8));
+      sts_u32(E, a, __byte_perm(u, 0, s));
+    }
+  }
+}
+
 template <bool FIRST>
-__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint32_t* c2v_row)
+__device__ __forceinline__ void row_dispatch_z_split(int deg, int g, int e0, uint32_t j4, int t, unsigned char* E,
+                                                     uint16_t* c2v_row)
+{
+  switch (deg) {
+    case 3: row_update_z_split<3, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 4: row_update_z_split<4, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 5: row_update_z_split<5, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 6: row_update_z_split<6, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 7: row_update_z_split<7, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 8: row_update_z_split<8, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 9: row_update_z_split<9, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 10: row_update_z_split<10, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    default: row_update_z_split<19, FIRST>(g, e0, j4, t, E, c2v_row); break;
+  }
+}
+
+template <bool FIRST>
+__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint16_t* c2v_row)
 {
   switch (deg) {
     case 3: row_update_z<3, FIRST>(g, e0, j4, E, c2v_row); break;
@@ -1270,12 +1340,16 @@ __device__ __forceinline__ bool z_hard(uint32_t h)
   return (h & 0x8000u) != 0 || (h & 0x7fffu) == 0;
 }
 
-// Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`.
-__device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const int8_t* __restrict__ llrs,
+// Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`: NT threads, T = NT / 192 per
+// lane pair (T = 2: each row's edges split between the pair's two threads).
+template <int NT>
+__device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, const int8_t* __restrict__ llrs,
                                       uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
                                       int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow, const int cb,
                                       const int slab)
 {
+  constexpr int T = NT / kZH;
+  static_assert(NT == kZH || NT == 2 * kZH, "one or two threads per lane pair");
   const int tid = threadIdx.x;
   const int bg  = d.base_graph;
   if (bg != 1 && bg != 2) {
@@ -1291,13 +1365,15 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
   const int      msg_len  = Kb * kZ384;
   const int      n        = (int)d.nof_llrs;
   const int8_t*  in       = llrs + d.llr_offset;
-  uint32_t*      c2v      = reinterpret_cast<uint32_t*>(c2v_all + (size_t)slab * kZSlab);
+  uint16_t*      c2v      = reinterpret_cast<uint16_t*>(c2v_all + (size_t)slab * pg::kC2vStride);
   const int      nbytes   = msg_len / 8;
   uint8_t*       out      = bits + d.out_offset;
   const int      crc_poly = d.crc_poly;
   const int      nwords   = msg_len / 32;
   unsigned char* E        = reinterpret_cast<unsigned char*>(sm.E);
-  const uint32_t j4       = 4u * (uint32_t)tid;
+  const int      jp       = T == 1 ? tid : tid >> 1; // lane pair
+  const int      tp       = T == 1 ? 0 : tid & 1;
+  const uint32_t j4       = 4u * (uint32_t)jp;
 
   if (tid == 0) {
     sm.s_last = 0;
@@ -1313,7 +1389,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     const bool    aligned  = (reinterpret_cast<uintptr_t>(in) & 7u) == 0;
     int           last     = 0;
 #pragma unroll 2
-    for (int q = tid; q < nchunks; q += kZThreads) {
+    for (int q = tid; q < nchunks; q += NT) {
       const int col = q / per_col;
       const int w0  = (q - col * per_col) * 8;
       const int k   = (col - 2) * kZ384 + w0;
@@ -1343,7 +1419,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
 
   const int input_size = sm.s_last;
   if (input_size < msg_len) {
-    for (int b = tid; b < nbytes; b += kZThreads) {
+    for (int b = tid; b < nbytes; b += NT) {
       out[b] = 0xff;
     }
     if (tid == 0) {
@@ -1371,18 +1447,26 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     for (int st = 0; st < nsteps; ++st) {
       if (it > 0 || st + 1 == nsteps) {
         prefetch_step(g, st + 1 < nsteps ? st + 1 : 0, nof_layers, tid, reinterpret_cast<const char*>(c2v),
-                      kZThreads * 4);
+                      kZH * 2);
       }
       const int r0 = c_step_row0[g][st];
       const int r1 = min(r0 + (int)c_step_nrows[g][st], nof_layers);
       for (int r = r0; r < r1; ++r) {
         const int deg     = c_row_deg[g][r];
         const int e0      = c_row_e0[g][r];
-        uint32_t* c2v_row = c2v + (size_t)e0 * kZThreads + tid;
-        if (it == 0) {
-          row_dispatch_z<true>(deg, g, e0, j4, E, c2v_row);
+        uint16_t* c2v_row = c2v + (size_t)e0 * kZH + jp;
+        if (T == 1) {
+          if (it == 0) {
+            row_dispatch_z<true>(deg, g, e0, j4, E, c2v_row);
+          } else {
+            row_dispatch_z<false>(deg, g, e0, j4, E, c2v_row);
+          }
         } else {
-          row_dispatch_z<false>(deg, g, e0, j4, E, c2v_row);
+          if (it == 0) {
+            row_dispatch_z_split<true>(deg, g, e0, j4, tp, E, c2v_row);
+          } else {
+            row_dispatch_z_split<false>(deg, g, e0, j4, tp, E, c2v_row);
+          }
         }
       }
       __syncthreads();
@@ -1393,7 +1477,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     // lane w = i mod 384 is half (w >= 192) of E[c][w mod 192].
     int      zero = 0;
     uint32_t crc  = 0;
-    for (int wi = tid >> 5; wi < nwords; wi += kZThreads / 32) {
+    for (int wi = tid >> 5; wi < nwords; wi += NT / 32) {
       const int      idx = 32 * wi + lane;
       const int      col = idx / kZ384;
       const int      w   = idx - col * kZ384;
@@ -1417,7 +1501,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     __syncthreads();
     if (tid == 0) {
       uint32_t t = 0;
-      for (int w = 0; w < kZThreads / 32; ++w) {
+      for (int w = 0; w < NT / 32; ++w) {
         t ^= sm.red[w];
       }
       sm.s_done = (crc_poly != PG_CRC_NONE && !zero && t == 0) ? 1 : 0;
@@ -1433,12 +1517,12 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     // Syndrome check over the processed rows (ldpc_decoder_impl.cpp:329-387), both lanes.
     int bad = 0;
     int e0  = 0;
-    for (int r = 0; r < nof_layers; ++r) {
+    for (int r = 0; r < nof_layers && tid < kZH; ++r) {
       const int deg    = c_row_deg[g][r];
       uint32_t  parity = 0;
       for (int e = 0; e < deg; ++e) {
         uint32_t a, s;
-        z_edge(g, e0 + e, j4, a, s);
+        z_edge(g, e0 + e, 4u * (uint32_t)tid, a, s);
         const uint32_t x  = __byte_perm(lds_u32(E, a), 0, s);
         const uint32_t lo = x & 0xffffu, hi = x >> 16;
         bad |= ((lo & 0x7fffu) == 0) | ((hi & 0x7fffu) == 0);
@@ -1449,7 +1533,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     }
     bad      = __syncthreads_or(bad);
     int zero = 0;
-    for (int i = tid; i < msg_len; i += kZThreads) {
+    for (int i = tid; i < msg_len; i += NT) {
       const int      col = i / kZ384;
       const int      w   = i - col * kZ384;
       const uint32_t x   = sm.E[col * kZH + (w < kZH ? w : w - kZH)];
@@ -1459,7 +1543,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_t& sm, const i
     result = (!bad && !zero) ? max_it : 0;
   }
 
-  for (int b = tid; b < nbytes; b += kZThreads) {
+  for (int b = tid; b < nbytes; b += NT) {
     out[b] = (uint8_t)(sm.hard[b >> 2] >> (24 - 8 * (b & 3)));
   }
   if (tid == 0) {
@@ -1497,16 +1581,55 @@ __global__ void __launch_bounds__(kZThreads, kZMaxPerSm) ldpc_decode_z_kernel(co
     }
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
-    // Slab: kZSlab bytes per CTA (two byte-message slabs for the other lifting sizes).
     if (d.lifting_size == kZ384) {
-      decode_codeblock_z384(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), llrs, bits, iterations, c2v_all, crc_pow, cb,
-                            blockIdx.x);
+      decode_codeblock_z384<kZThreads>(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), llrs, bits, iterations, c2v_all,
+                                       crc_pow, cb, blockIdx.x);
     } else if (d.lifting_size > kX2Threads) {
       decode_codeblock_pair<kX2Threads, 1>(d, *reinterpret_cast<smem_pair_t*>(smem_z_raw), llrs, bits, iterations,
-                                           c2v_all, crc_pow, scale_tab, cb, 2 * blockIdx.x);
+                                           c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
     } else {
       decode_codeblock<0, kX2Threads, kX2Threads>(d, *reinterpret_cast<smem_x2_scalar_t*>(smem_z_raw), llrs, bits,
-                                                  iterations, c2v_all, crc_pow, cb, 2 * blockIdx.x);
+                                                  iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      __syncthreads();
+    }
+  }
+}
+
+// The Z = 384 decoder with two threads per lane pair (384 threads, two CTAs per SM): each row's
+// edges are split between the pair, which halves the latency of a layer, for batches whose time is
+// set by their slowest codeblocks. Other lifting sizes as ldpc_decode_split_kernel.
+constexpr int    kZsThreads  = 2 * kZH;
+constexpr int    kZsMaxPerSm = 2;
+constexpr size_t kZsSmem     = std::max(sizeof(smem_z_nt_t<kZsThreads>), kSplitSmem);
+
+__global__ void __launch_bounds__(kZsThreads, kZsMaxPerSm) ldpc_decode_zs_kernel(
+    const pg_ldpc_cb* __restrict__ descs, const int8_t* __restrict__ llrs, uint8_t* __restrict__ bits,
+    int32_t* __restrict__ iterations, int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow,
+    const uint16_t* __restrict__ scale_tab, const uint32_t* __restrict__ order, int n, int* __restrict__ counter)
+{
+  extern __shared__ __align__(16) unsigned char smem_zs_raw[];
+  __shared__ int s_work;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_work = atomicAdd(counter, 1);
+    }
+    __syncthreads();
+    const int w = s_work;
+    __syncthreads();
+    if (w >= n) {
+      break;
+    }
+    const int        cb = order != nullptr ? (int)order[w] : w;
+    const pg_ldpc_cb d  = descs[cb];
+    if (d.lifting_size == kZ384) {
+      decode_codeblock_z384<kZsThreads>(d, *reinterpret_cast<smem_z_nt_t<kZsThreads>*>(smem_zs_raw), llrs, bits,
+                                        iterations, c2v_all, crc_pow, cb, blockIdx.x);
+    } else if (d.lifting_size > kX2Threads && (d.lifting_size & 1) == 0) {
+      decode_codeblock_pair<kSplitThreads, 2>(d, *reinterpret_cast<smem_split_pair_t*>(smem_zs_raw), llrs, bits,
+                                              iterations, c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
+    } else {
+      decode_codeblock<0, kSplitThreads, pg::kMaxZ>(d, *reinterpret_cast<smem_split_scalar_t*>(smem_zs_raw), llrs,
+                                                    bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
       __syncthreads();
     }
   }
@@ -1591,7 +1714,7 @@ __global__ void __launch_bounds__(kSplitThreads, kSplitMaxPerSm) ldpc_decode_spl
 // time is its work per iteration (lifting size times the check rows its input reaches, as the
 // decoder counts them from the last non-zero LLR) over its input confidence (the mean magnitude of
 // its finite non-zero LLRs, which falls as the iterations it needs rise); both come from a sample
-// of at most ~2,048 input positions. The key is 255 - 16 log2(1 + that cost), clamped to 0..255
+// of 256 input positions spread over the codeblock. The key is 255 - 16 log2(1 + that cost), clamped to 0..255
 // (no non-zero LLR: 255), and the order lists the codeblocks by ascending key, so that the long
 // decodes start first and the short ones fill the tail. The order only schedules: every
 // codeblock's result is independent of it.
@@ -1606,15 +1729,22 @@ __global__ void ldpc_score_kernel(const pg_ldpc_cb* __restrict__ descs, int n, c
   const pg_ldpc_cb d      = descs[w];
   const int8_t*    in     = llrs + d.llr_offset;
   const int        len    = (int)d.nof_llrs;
-  const int        stride = max(1, len / 2048);
+  const int        stride = max(1, (len + 255) / 256);
   uint32_t         sum = 0, cnt = 0;
   int              last = 0;
-  for (int k = lane * stride; k < len; k += 32 * stride) {
-    const int v = abs((int)__ldg(in + k));
-    if (v != 0) {
+  int              v8[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int k = (lane + 32 * i) * stride;
+    v8[i]       = k < len ? abs((int)__ldg(in + k)) : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int k = (lane + 32 * i) * stride;
+    if (v8[i] != 0) {
       last = k + 1;
-      if (v < 127) {
-        sum += (uint32_t)v;
+      if (v8[i] < 127) {
+        sum += (uint32_t)v8[i];
         ++cnt;
       }
     }
@@ -1763,6 +1893,12 @@ int ldpc_upload_tables(pg_context* ctx)
                     cudaFuncSetAttribute(ldpc_decode_z_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kZSmem),
                     "cudaFuncSetAttribute(ldpc_decode_z_kernel)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx,
+                    cudaFuncSetAttribute(ldpc_decode_zs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kZsSmem),
+                    "cudaFuncSetAttribute(ldpc_decode_zs_kernel)");
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMalloc(&ctx->dev.ldpc_scale, sizeof(scale)), "cudaMalloc(scale table)");
@@ -1925,7 +2061,12 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   // (two per SM). The caller provides a slab per CTA (min(n, max_ctas) slabs, max_ctas <= four
   // per SM).
   int rc = PG_OK;
-  if (kinds & PG_LDPC_ROUTE_Z) {
+  if (kinds & PG_LDPC_ROUTE_ZS) {
+    const int grid_zs = std::max(1, std::min(n, std::min(max_ctas, kZsMaxPerSm * ctx->sm_count)));
+    ldpc_decode_zs_kernel<<<grid_zs, kZsThreads, kZsSmem, stream>>>(
+        descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
+    rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_zs_kernel launch");
+  } else if (kinds & PG_LDPC_ROUTE_Z) {
     const int grid_z = std::max(1, std::min(n, std::min(max_ctas, kZMaxPerSm * ctx->sm_count)));
     ldpc_decode_z_kernel<<<grid_z, kZThreads, kZSmem, stream>>>(
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);

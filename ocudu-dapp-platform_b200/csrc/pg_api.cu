@@ -524,7 +524,7 @@ int pg_set_ldpc_kernel(pg_context* ctx, int kernel)
   if (ctx == nullptr) {
     return PG_ERR_INVALID;
   }
-  if (kernel < PG_LDPC_KERNEL_ONE_LANE || kernel > PG_LDPC_KERNEL_Z384) {
+  if (kernel < PG_LDPC_KERNEL_ONE_LANE || kernel > PG_LDPC_KERNEL_Z384_SPLIT) {
     return set_error(ctx, PG_ERR_INVALID, "unknown LDPC kernel " + std::to_string(kernel));
   }
   ctx->ldpc_kernel = kernel;

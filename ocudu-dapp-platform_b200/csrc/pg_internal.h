@@ -239,7 +239,8 @@ enum {
   PG_LDPC_KIND_ALL    = 3,
   PG_LDPC_ROUTE_X2    = 4,
   PG_LDPC_ROUTE_SPLIT = 8,
-  PG_LDPC_ROUTE_Z     = 16
+  PG_LDPC_ROUTE_Z     = 16,
+  PG_LDPC_ROUTE_ZS    = 32
 };
 // Route flags of a pg_ldpc_kernel value.
 inline int ldpc_route(int kernel)
@@ -247,6 +248,7 @@ inline int ldpc_route(int kernel)
   return kernel == PG_LDPC_KERNEL_TWO_LANES ? PG_LDPC_ROUTE_X2
          : kernel == PG_LDPC_KERNEL_SPLIT   ? PG_LDPC_ROUTE_SPLIT
          : kernel == PG_LDPC_KERNEL_Z384    ? PG_LDPC_ROUTE_Z
+         : kernel == PG_LDPC_KERNEL_Z384_SPLIT ? PG_LDPC_ROUTE_ZS
                                             : 0;
 }
 // Same with at most max_ctas CTAs per decoder kernel, launching only the decoders of `kinds`.

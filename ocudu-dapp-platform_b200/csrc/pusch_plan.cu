@@ -369,9 +369,8 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   for (const pg_ldpc_cb& l : w.ldpc) {
     p->ldpc_kinds |= l.lifting_size == 384 ? PG_LDPC_KIND_Z384 : PG_LDPC_KIND_OTHER;
   }
-  // One check-to-variable slab per decoder CTA: up to four per SM, or two of twice the size (the
-  // Z = 384 decoder's f16 messages), at most one CTA per codeblock.
-  const int ldpc_slabs = std::max(2, 2 * std::min(p->nof_cbs, 2 * ctx->sm_count));
+  // One check-to-variable slab per decoder CTA: up to four per SM, at most one per codeblock.
+  const int ldpc_slabs = std::max(1, std::min(p->nof_cbs, 4 * ctx->sm_count));
 
   // Device image: descriptors first (uploaded once), then the workspace.
   const size_t o_ues    = 0;
@@ -656,7 +655,7 @@ static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
          t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
          t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm <= 4 &&
-         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_Z384;
+         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_Z384_SPLIT;
 }
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
@@ -802,7 +801,8 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
       c.ldpc_ctas_per_sm     = v;
       if (rc == PG_OK) rc = try_set(c);
     }
-    for (int v : {PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384}) {
+    for (int v : {PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384,
+                  PG_LDPC_KERNEL_Z384_SPLIT}) {
       pg_pusch_plan_tuning c = cur;
       c.ldpc_kernel          = v;
       if (rc == PG_OK) rc = try_set(c);

@@ -14,7 +14,8 @@ PG_OK, PG_ERR_INVALID, PG_ERR_CUDA, PG_ERR_CAPACITY, PG_ERR_TIMEOUT, PG_ERR_NO_D
 PG_CRC16, PG_CRC24A, PG_CRC24B = 0, 1, 2
 PG_CRC_NONE = 255
 # pg_ldpc_kernel: one lifted lane per thread, two lanes per thread (f16x2), two lanes per thread pair.
-PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384 = 0, 1, 2, 3
+(PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384,
+ PG_LDPC_KERNEL_Z384_SPLIT) = 0, 1, 2, 3, 4
 
 STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_INVALID", 2: "PG_ERR_CUDA", 3: "PG_ERR_CAPACITY", 4: "PG_ERR_TIMEOUT",
                 5: "PG_ERR_NO_DEVICE"}

@@ -194,10 +194,12 @@ def test_pair_mode_saturation_and_short_inputs_match_port(batch_decoder, port):
 
 
 @pytest.mark.parametrize("kernel", [_native.PG_LDPC_KERNEL_ONE_LANE, _native.PG_LDPC_KERNEL_TWO_LANES,
-                                    _native.PG_LDPC_KERNEL_SPLIT, _native.PG_LDPC_KERNEL_Z384])
+                                    _native.PG_LDPC_KERNEL_SPLIT, _native.PG_LDPC_KERNEL_Z384,
+                                    _native.PG_LDPC_KERNEL_Z384_SPLIT])
 def test_every_kernel_bit_exact(batch_decoder, port, kernel):
-    """The four decoding kernels (one lane per thread; two lanes per thread; two lanes per thread
-    pair with the rows split over the pair; the Z = 384 specialisation) on the golden cases, a random
+    """The five decoding kernels (one lane per thread; two lanes per thread; two lanes per thread
+    pair with the rows split over the pair; the Z = 384 specialisation, with one or two threads per
+    lane pair) on the golden cases, a random
     mixed batch of 19 lifting sizes and the 512-codeblock BG1/BG2 Z=384 batch: bits and iteration
     counts equal the reference's and the restatement's."""
     batch_decoder.set_kernel(kernel)
