@@ -50,14 +50,22 @@ __device__ __forceinline__ cf cbf16(uint32_t v)
 {
   return {__uint_as_float(v << 16), __uint_as_float(v & 0xffff0000u)};
 }
-__device__ __forceinline__ float bf16_round(float f)
+// A complex FP32 value rounded to bf16 (round to nearest even, both parts in one conversion) and
+// widened back to FP32.
+__device__ __forceinline__ cf bf16_round2(float re, float im)
 {
-  uint32_t u = __float_as_uint(f);
-  if ((u & 0x7fffffffu) > 0x7f800000u) {
-    return f;
-  }
-  u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
-  return __uint_as_float(u);
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(im), "f"(re));
+  return {__uint_as_float(r << 16), __uint_as_float(r & 0xffff0000u)};
+}
+
+// Hardware reciprocal estimate (relative error below 2^-22): the equaliser and the demapper use
+// it where the reference itself uses a 14-bit reciprocal estimate or a division.
+__device__ __forceinline__ float rcp_est(float x)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
 }
 
 __device__ __forceinline__ int8_t quantize(float v, float scale)
@@ -74,7 +82,7 @@ template <int QM>
 __device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* llr, const float* s_slope,
                                       const float* s_icpt, const float* s_width)
 {
-  const float rcp = (nvar > 0.f) ? __frcp_rn(nvar) : 0.f;
+  const float rcp = (nvar > 0.f) ? rcp_est(nvar) : 0.f;
   if (QM == 2) {
     const float g = 2.0f * 1.41421353816986083984375f;
     llr[0]        = quantize(__fmul_rn(__fmul_rn(g, xr), rcp), 5.0f);
@@ -98,11 +106,14 @@ __device__ __forceinline__ void demap(float xr, float xi, float nvar, int8_t* ll
   }
   constexpr int t     = QM == 6 ? 1 : 2;
   constexpr int nint  = QM == 6 ? 8 : 16;
-  const float   width = s_width[t];
-  const float   x[2]  = {xr, xi};
+  // Interval index floor(x / width) as x times the stored reciprocal width: where the two differ
+  // (x / width within an ulp of an integer) the neighbouring interval's line meets this one at
+  // the boundary (the interval functions are continuous), so the LLR is the same within rounding.
+  const float   iwidth = s_width[3 + t];
+  const float   x[2]   = {xr, xi};
 #pragma unroll
   for (int c = 0; c < 2; ++c) {
-    int idx      = (int)floorf(__fdiv_rn(x[c], width)) + nint / 2;
+    int idx      = (int)floorf(__fmul_rn(x[c], iwidth)) + nint / 2;
     idx          = idx < 0 ? 0 : (idx > nint - 1 ? nint - 1 : idx);
     const bool z = fabsf(x[c]) <= 1e-9f;
 #pragma unroll
@@ -172,7 +183,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
                                          __fmaf_rn(a2.y, f2, __fmaf_rn(a1.y, f1, v.y)));
         }
       }
-      h[p][l] = is_dc ? cf{0.f, 0.f} : cf{bf16_round(v.x), bf16_round(v.y)};
+      h[p][l] = is_dc ? cf{0.f, 0.f} : bf16_round2(v.x, v.y);
     }
   }
   cf    s[L];
@@ -190,7 +201,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
       }
     }
     const bool  ok  = (ch_mod > 0.f) && (ch_mod < INFINITY);
-    const float rcp = __frcp_rn(ch_mod);
+    const float rcp = rcp_est(ch_mod);
     s[0]            = ok ? cscale(acc, rcp) : cf{0.f, 0.f};
     nv[0]           = ok ? __fmul_rn(nacc, __fmul_rn(rcp, rcp)) : INFINITY;
   } else {
@@ -205,12 +216,18 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
     for (int i = 0; i < L; ++i) {
 #pragma unroll
       for (int k = 0; k < L; ++k) {
-        cf acc = {0.f, 0.f};
+        if (k < i) {
+          // Hermitian: conj(h_i) h_k and conj(h_k) h_i have equal real parts and opposite
+          // imaginary parts in IEEE arithmetic (products commute, a - b = -(b - a)).
+          G[i][k] = cf{G[k][i].r, -G[k][i].i};
+        } else {
+          cf acc = {0.f, 0.f};
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-          acc = cadd(acc, cconjmul(h[p][i], h[p][k]));
+          for (int p = 0; p < P; ++p) {
+            acc = cadd(acc, cconjmul(h[p][i], h[p][k]));
+          }
+          G[i][k] = acc;
         }
-        G[i][k]  = acc;
         Gi[i][k] = cf{i == k ? 1.f : 0.f, 0.f};
       }
       ok        = ok && (G[i][i].r > 0.f);
@@ -221,7 +238,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
       const cf    piv  = G[i][i];
       const float pn   = cnorm(piv);
       ok               = ok && (pn > 0.f);
-      const cf    pinv = cscale(cf{piv.r, -piv.i}, __frcp_rn(pn));
+      const cf    pinv = cscale(cf{piv.r, -piv.i}, rcp_est(pn));
       Gi[i][i]         = cf{1.f, 0.f};
 #pragma unroll
       for (int k = i + 1; k < L; ++k) {
@@ -262,7 +279,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
         acc  = cadd(acc, cmul(wv, y[p]));
         corr = __fadd_rn(corr, cmul(wv, h[p][l]).r);
       }
-      const float c = __frcp_rn(corr);
+      const float c = rcp_est(corr);
       s[l]          = ok ? cscale(acc, c) : cf{0.f, 0.f};
       nv[l]         = ok ? __fsub_rn(c, 1.f) : INFINITY;
     }
@@ -403,7 +420,7 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
 {
   __shared__ float  s_slope[3 * 4 * 16];
   __shared__ float  s_icpt[3 * 4 * 16];
-  __shared__ float  s_width[3];
+  __shared__ float  s_width[6]; // interval widths, then their reciprocals
   __shared__ float2 s_est[4 * 2 * 2 * kDemodTile];
   __shared__ float2 s_bas[4 * 2 * 2 * kDemodTile];
   __shared__ int    s_sym[14];
@@ -414,7 +431,8 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
     s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
   }
   if (threadIdx.x < 3) {
-    s_width[threadIdx.x] = c_width_d[threadIdx.x];
+    s_width[threadIdx.x]     = c_width_d[threadIdx.x];
+    s_width[3 + threadIdx.x] = 1.0f / c_width_d[threadIdx.x];
   }
   const demap_tables tb     = {s_slope, s_icpt, s_width};
   const uint32_t     ntiles = __ldg(tile_off + nof_ues);

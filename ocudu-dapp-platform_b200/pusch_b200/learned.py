@@ -415,14 +415,20 @@ def estimate_quality(ctx, slots, net=None, max_iterations=6):
     return out
 
 
-def run_plan(ctx, slots, net, max_iterations):
+def learned_use(slots, min_qm=0):
+    """Per UE of the slots: True where the learned refinement applies (modulation order at least
+    min_qm; 0: every UE)."""
+    return [ue.modulation_order >= min_qm for sl in slots for ue in sl.ues]
+
+
+def run_plan(ctx, slots, net, max_iterations, min_qm=0):
     """(TB error flags, decoded bits) of every UE of the slots through a slot plan, with the plain
-    estimator (net None) or the learned one."""
+    estimator (net None) or the learned one (for the UEs of modulation order min_qm and above)."""
     from .pusch import PuschSlotPlan
     truths = [t for sl in slots for t in sl.truth]
     plan = PuschSlotPlan(ctx, slots, max_iterations=max_iterations)
     if net is not None:
-        plan.set_learned(net)
+        plan.set_learned(net, use=None if min_qm <= 0 else learned_use(slots, min_qm))
     err = tb_errors(plan.execute_host(), truths)
     if net is not None:
         plan.set_learned(None)
@@ -441,7 +447,7 @@ def la_point(per_margin, key):
 
 
 def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, step_db=EVAL_MARGIN_STEP_DB,
-             max_margin_db=EVAL_MARGIN_MAX_DB, verbose=True):
+             max_margin_db=EVAL_MARGIN_MAX_DB, verbose=True, min_qm=0):
     """Per SNR, link-adaptation margins 0, step_db, ... until both estimators reach BLER <= 10 % (or
     max_margin_db): BLER (TB CRC and payload against the transmitted bits) of the slot plan with the
     plain and with the learned estimator on the same slots, and the decoded Mbit/s per cell. Each
@@ -454,7 +460,7 @@ def evaluate(ctx, net, snrs_db, seed=0, cells=48, max_iterations=6, step_db=EVAL
         while True:
             slots = eval_slots(snr, seed + k, cells, la_margin_db=m)
             e_p, b_p = run_plan(ctx, slots, None, max_iterations)
-            e_l, b_l = run_plan(ctx, slots, net, max_iterations)
+            e_l, b_l = run_plan(ctx, slots, net, max_iterations, min_qm)
             qm = np.array([ue.modulation_order for sl in slots for ue in sl.ues])
             by_qm = {int(q): dict(ues=int((qm == q).sum()), plain=float(np.mean(np.array(e_p)[qm == q])),
                                   learned=float(np.mean(np.array(e_l)[qm == q]))) for q in np.unique(qm)}
@@ -503,6 +509,7 @@ def main(argv=None):
     e.add_argument("--cells", type=int, default=48, help="cells per SNR point and margin (about 10 UEs each)")
     e.add_argument("--seed", type=int, default=100)
     e.add_argument("--json", default=None)
+    e.add_argument("--min-qm", type=int, default=0, help="refine only UEs of this modulation order and above")
     tm = sub.add_parser("time", help="time pg_le_refine_device on a batch of the training source")
     tm.add_argument("--rows", type=int, default=270_000)
     tm.add_argument("--reps", type=int, default=50)
@@ -556,7 +563,7 @@ def main(argv=None):
         # A cell holds at most 273 PRB x 4 ports x 2 layers of subcarrier rows, plus the gaps of
         # up to 16 UEs x 8 allocations.
         net = LearnedEstimator(ctx, max_rows=a.cells * (4 * 2 * 12 * 273 + 16 * 8 * 2), params=params)
-        rows = evaluate(ctx, net, snrs, seed=a.seed, cells=a.cells)
+        rows = evaluate(ctx, net, snrs, seed=a.seed, cells=a.cells, min_qm=a.min_qm)
         if a.json:
             with open(a.json, "w") as f:
                 json.dump(rows, f, indent=1)
