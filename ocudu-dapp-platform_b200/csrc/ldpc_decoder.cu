@@ -1713,41 +1713,50 @@ __global__ void __launch_bounds__(kSplitThreads, kSplitMaxPerSm) ldpc_decode_spl
 // Longest-first work order of a batch for the persistent decoders. A codeblock's expected decoding
 // time is its work per iteration (lifting size times the check rows its input reaches, as the
 // decoder counts them from the last non-zero LLR) over its input confidence (the mean magnitude of
-// its finite non-zero LLRs, which falls as the iterations it needs rise); both come from a sample
-// of 256 input positions spread over the codeblock. The key is 255 - 16 log2(1 + that cost), clamped to 0..255
-// (no non-zero LLR: 255), and the order lists the codeblocks by ascending key, so that the long
-// decodes start first and the short ones fill the tail. The order only schedules: every
-// codeblock's result is independent of it.
-__global__ void ldpc_score_kernel(const pg_ldpc_cb* __restrict__ descs, int n, const int8_t* __restrict__ llrs,
-                                  uint8_t* __restrict__ keys)
+// its non-zero LLRs, which falls as the iterations it needs rise). The key is
+// 255 - 16 log2(1 + that cost), clamped to 0..255 (no non-zero LLR: 255), and the order lists the
+// codeblocks by ascending key, so that the long decodes start first and the short ones fill the
+// tail. The order only schedules: every codeblock's result is independent of it. One CTA per
+// codeblock reads its whole input, 16 bytes per load in the aligned body.
+constexpr int kScoreThreads = 128;
+
+__device__ __forceinline__ void score_word(uint32_t w, int idx, uint32_t& sum, uint32_t& cnt, int& last)
 {
-  const int w    = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (w >= n) {
-    return;
+  const uint32_t a  = __vabsss4(w);                    // |x| per byte (saturating, -128 -> 127)
+  const uint32_t nz = __vcmpne4(w, 0u) & 0x01010101u;  // 1 per non-zero byte
+  sum               = __dp4a(a, 0x01010101u, sum);
+  cnt               = __dp4a(nz, 0x01010101u, cnt);
+  if (w != 0) {
+    last = max(last, idx + 4 - (__clz(w) >> 3));     // one past the highest non-zero byte
   }
-  const pg_ldpc_cb d      = descs[w];
-  const int8_t*    in     = llrs + d.llr_offset;
-  const int        len    = (int)d.nof_llrs;
-  const int        stride = max(1, (len + 255) / 256);
+}
+
+__global__ void __launch_bounds__(kScoreThreads) ldpc_score_kernel(const pg_ldpc_cb* __restrict__ descs, int n,
+                                                                  const int8_t* __restrict__ llrs,
+                                                                  uint8_t* __restrict__ keys)
+{
+  __shared__ uint32_t s_red[3][kScoreThreads / 32];
+  const pg_ldpc_cb d    = descs[blockIdx.x];
+  const int8_t*    in   = llrs + d.llr_offset;
+  const int        len  = (int)d.nof_llrs;
+  const int        head = min(len, (int)((16u - (unsigned)(reinterpret_cast<uintptr_t>(in) & 15u)) & 15u));
+  const int        nvec = (len - head) / 16;
   uint32_t         sum = 0, cnt = 0;
   int              last = 0;
-  int              v8[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int k = (lane + 32 * i) * stride;
-    v8[i]       = k < len ? abs((int)__ldg(in + k)) : 0;
+  for (int k = threadIdx.x; k < head; k += kScoreThreads) {
+    score_word((uint32_t)(uint8_t)__ldg(in + k), k, sum, cnt, last);
   }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int k = (lane + 32 * i) * stride;
-    if (v8[i] != 0) {
-      last = k + 1;
-      if (v8[i] < 127) {
-        sum += (uint32_t)v8[i];
-        ++cnt;
-      }
-    }
+  const uint4* body = reinterpret_cast<const uint4*>(in + head);
+  for (int q = threadIdx.x; q < nvec; q += kScoreThreads) {
+    const uint4 v  = __ldg(body + q);
+    const int   k0 = head + 16 * q;
+    score_word(v.x, k0, sum, cnt, last);
+    score_word(v.y, k0 + 4, sum, cnt, last);
+    score_word(v.z, k0 + 8, sum, cnt, last);
+    score_word(v.w, k0 + 12, sum, cnt, last);
+  }
+  for (int k = head + 16 * nvec + threadIdx.x; k < len; k += kScoreThreads) {
+    score_word((uint32_t)(uint8_t)__ldg(in + k), k, sum, cnt, last);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -1755,19 +1764,33 @@ __global__ void ldpc_score_kernel(const pg_ldpc_cb* __restrict__ descs, int n, c
     cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
   }
-  if (lane == 0) {
+  if ((threadIdx.x & 31) == 0) {
+    s_red[0][threadIdx.x >> 5] = sum;
+    s_red[1][threadIdx.x >> 5] = cnt;
+    s_red[2][threadIdx.x >> 5] = (uint32_t)last;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t ts = 0, tc = 0;
+    int      tl = 0;
+    for (int w = 0; w < kScoreThreads / 32; ++w) {
+      ts += s_red[0][w];
+      tc += s_red[1][w];
+      tl = max(tl, (int)s_red[2][w]);
+    }
     uint32_t key = 255u;
-    if (cnt > 0) {
+    if (tc > 0) {
       const int   Z    = max(1, (int)d.lifting_size);
       const int   Kb   = d.base_graph == 1 ? 22 : 10;
       const int   nr   = d.base_graph == 1 ? pg::kBg1Rows : pg::kBg2Rows;
-      const int   rows = min(max((last + 2 * Z) / Z, Kb + 4) - Kb, nr);
-      const float mean = (float)sum / (float)cnt;
+      const int   rows = min(max((tl + 2 * Z) / Z, Kb + 4) - Kb, nr);
+      const float mean = (float)ts / (float)tc;
       const float cost = (float)(rows * Z) / mean;
       key              = 255u - (uint32_t)min(255.f, 16.f * log2f(1.f + cost));
     }
-    keys[w] = (uint8_t)key;
+    keys[blockIdx.x] = (uint8_t)key;
   }
+  (void)n;
 }
 
 // Counting sort of the keys in one CTA: order[0..n) = codeblocks by ascending key.
@@ -2000,7 +2023,7 @@ int ldpc_order_launch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, const
   if (n <= 0) {
     return PG_OK;
   }
-  ldpc_score_kernel<<<(n + 7) / 8, 256, 0, stream>>>(descs_dev, n, llrs, keys);
+  ldpc_score_kernel<<<n, kScoreThreads, 0, stream>>>(descs_dev, n, llrs, keys);
   if (int rc = check_cuda(ctx, cudaGetLastError(), "ldpc_score_kernel launch")) {
     return rc;
   }
