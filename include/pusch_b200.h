@@ -154,6 +154,12 @@ enum pg_ldpc_kernel {
 /* Selects the kernel of the context's batch decodes (pg_ldpc_decode_batch_{host,device,resident}
  * and pg_sch_decode_batch_host); slot plans choose theirs through their tuning. */
 int pg_set_ldpc_kernel(pg_context* ctx, int kernel);
+/* Work order of the context's batch decodes: the codeblocks as given, or longest first (the
+ * default): an estimate of each codeblock's decoding time from its input (the edges its rows cover
+ * times Z, over the LLR magnitude per message bit) orders the persistent decoders' work list, so that
+ * the long decodes start first. Results do not depend on the order. */
+enum pg_ldpc_order { PG_LDPC_ORDER_GIVEN = 0, PG_LDPC_ORDER_LONGEST_FIRST = 1 };
+int pg_set_ldpc_order(pg_context* ctx, int mode);
 /* The kernel of the context's batch decodes (pg_ldpc_kernel), or a negative error code. */
 int pg_get_ldpc_kernel(const pg_context* ctx);
 /* Resident CTAs per SM of the context's batch decodes (1-4, capped by the kernel's own limit; 0:

@@ -1711,10 +1711,12 @@ __global__ void __launch_bounds__(kSplitThreads, kSplitMaxPerSm) ldpc_decode_spl
 
 
 // Longest-first work order of a batch for the persistent decoders. A codeblock's expected decoding
-// time is its work per iteration (lifting size times the check rows its input reaches, as the
-// decoder counts them from the last non-zero LLR) over its input confidence (the mean magnitude of
-// its non-zero LLRs, which falls as the iterations it needs rise). The key is
-// 255 - 16 log2(1 + that cost), clamped to 0..255 (no non-zero LLR: 255), and the order lists the
+// time is its work per iteration (the edges of the check rows its input reaches, as the decoder
+// counts them from the last non-zero LLR, times Z) times the iterations it needs, which fall as its
+// information per message bit rises: the sum of its LLR magnitudes over its K = Kb Z message bits
+// (the mean LLR magnitude over the code rate; on the 512-codeblock BG1/BG2 batch the iterations
+// correlate with it at -0.9 within each graph). Cost = edges Z K / sum |LLR|; the key is
+// 255 - 16 log2(1 + cost), clamped to 0..255 (no non-zero LLR: 255), and the order lists the
 // codeblocks by ascending key, so that the long decodes start first and the short ones fill the
 // tail. The order only schedules: every codeblock's result is independent of it. One CTA per
 // codeblock reads its whole input, 16 bytes per load in the aligned body.
@@ -1783,10 +1785,10 @@ __global__ void __launch_bounds__(kScoreThreads) ldpc_score_kernel(const pg_ldpc
       const int   Z    = max(1, (int)d.lifting_size);
       const int   Kb   = d.base_graph == 1 ? 22 : 10;
       const int   nr   = d.base_graph == 1 ? pg::kBg1Rows : pg::kBg2Rows;
-      const int   rows = min(max((tl + 2 * Z) / Z, Kb + 4) - Kb, nr);
-      const float mean = (float)ts / (float)tc;
-      const float cost = (float)(rows * Z) / mean;
-      key              = 255u - (uint32_t)min(255.f, 16.f * log2f(1.f + cost));
+      const int   rows  = min(max((tl + 2 * Z) / Z, Kb + 4) - Kb, nr);
+      const int   edges = c_row_e0[d.base_graph == 2 ? 1 : 0][rows];
+      const float cost  = (float)edges * (float)Z * (float)(Kb * Z) / (float)max(ts, 1u);
+      key               = 255u - (uint32_t)min(255.f, 16.f * log2f(1.f + cost));
     }
     keys[blockIdx.x] = (uint8_t)key;
   }
@@ -2008,7 +2010,7 @@ int ldpc_launch_scratch(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, con
                         int32_t* iterations, int8_t* c2v, cudaStream_t stream)
 {
   const uint32_t* order = nullptr;
-  if (n > 1 && n <= ctx->max_codeblocks) {
+  if (ctx->ldpc_order_mode == PG_LDPC_ORDER_LONGEST_FIRST && n > 1 && n <= ctx->max_codeblocks) {
     if (int rc = ldpc_order_launch(ctx, descs_dev, n, llrs, ctx->dev.ldpc_keys, ctx->dev.ldpc_order, stream)) {
       return rc;
     }

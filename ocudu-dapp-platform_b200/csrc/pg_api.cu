@@ -531,6 +531,18 @@ int pg_set_ldpc_kernel(pg_context* ctx, int kernel)
   return PG_OK;
 }
 
+int pg_set_ldpc_order(pg_context* ctx, int mode)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (mode != PG_LDPC_ORDER_GIVEN && mode != PG_LDPC_ORDER_LONGEST_FIRST) {
+    return set_error(ctx, PG_ERR_INVALID, "unknown LDPC work order " + std::to_string(mode));
+  }
+  ctx->ldpc_order_mode = mode;
+  return PG_OK;
+}
+
 int pg_get_ldpc_kernel(const pg_context* ctx)
 {
   return ctx == nullptr ? PG_ERR_INVALID : ctx->ldpc_kernel;

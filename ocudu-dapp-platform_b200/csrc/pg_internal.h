@@ -100,6 +100,7 @@ struct pg_context {
   int8_t*             static_c2v     = nullptr;  // device address of the module-static LDPC scratch
   int                 ldpc_kernel    = PG_LDPC_KERNEL_Z384; // kernel of the batch decodes (pg_ldpc_kernel)
   int                 ldpc_ctas_per_sm = 0;   // resident CTAs per SM of the batch decodes (0: kernel limit)
+  int                 ldpc_order_mode  = PG_LDPC_ORDER_LONGEST_FIRST; // work order of the batch decodes
   std::string         last_error;
 };
 

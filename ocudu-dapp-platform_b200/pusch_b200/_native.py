@@ -16,6 +16,7 @@ PG_CRC_NONE = 255
 # pg_ldpc_kernel: one lifted lane per thread, two lanes per thread (f16x2), two lanes per thread pair.
 (PG_LDPC_KERNEL_ONE_LANE, PG_LDPC_KERNEL_TWO_LANES, PG_LDPC_KERNEL_SPLIT, PG_LDPC_KERNEL_Z384,
  PG_LDPC_KERNEL_Z384_SPLIT) = 0, 1, 2, 3, 4
+PG_LDPC_ORDER_GIVEN, PG_LDPC_ORDER_LONGEST_FIRST = 0, 1
 
 STATUS_NAMES = {0: "PG_OK", 1: "PG_ERR_INVALID", 2: "PG_ERR_CUDA", 3: "PG_ERR_CAPACITY", 4: "PG_ERR_TIMEOUT",
                 5: "PG_ERR_NO_DEVICE"}
@@ -205,6 +206,7 @@ SIGNATURES = {
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),
     "pg_set_ldpc_ctas_per_sm": (ctypes.c_int, [_VP, ctypes.c_int]),
     "pg_get_ldpc_kernel": (ctypes.c_int, [_VP]),
+    "pg_set_ldpc_order": (ctypes.c_int, [_VP, ctypes.c_int]),
     "pg_set_ldpc_kernel": (ctypes.c_int, [_VP, ctypes.c_int]),
     "pg_port_channel_estimate_host": (ctypes.c_int, [_VP] * 7),
     "pg_sch_decode_batch_resident": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, _VP, _VP,

@@ -138,6 +138,10 @@ class LdpcBatchDecoder:
         """Selects the decoding kernel (_native.PG_LDPC_KERNEL_*); results do not depend on it."""
         self.ctx.check(self.lib.pg_set_ldpc_kernel(self.ctx.handle, int(kernel)))
 
+    def set_order(self, mode: int):
+        """Work order of the batch decodes (_native.PG_LDPC_ORDER_*); results do not depend on it."""
+        self.ctx.check(self.lib.pg_set_ldpc_order(self.ctx.handle, int(mode)))
+
     def set_ctas_per_sm(self, ctas_per_sm: int):
         """Resident CTAs per SM of the batch decodes (0: the kernel's limit); results do not depend on it."""
         self.ctx.check(self.lib.pg_set_ldpc_ctas_per_sm(self.ctx.handle, int(ctas_per_sm)))
