@@ -81,6 +81,8 @@ def parse_args():
     p.add_argument("--no-learned", action="store_true", help="plain estimator only")
     p.add_argument("--no-autotune", action="store_true", help="default launch shapes (no autotuning run)")
     p.add_argument("--no-configs", action="store_true", help="skip the single-slot configuration sub-lines")
+    p.add_argument("--learned-min-qm", type=int, default=6,
+                   help="refine the UEs of this modulation order and above with the learned estimator (0: every UE)")
     p.add_argument("--ldpc-kernel", type=int, default=None,
                    help="LDPC batch kernel of the --workload ldpc line (pg_ldpc_kernel; default: the library's)")
     p.add_argument("--ldpc-ctas-per-sm", type=int, default=0,
@@ -415,11 +417,15 @@ def run_ours_pusch(args):
     d_res = torch.zeros(n * ctypes.sizeof(PgSchResult), dtype=torch.uint8, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > 126 MB L2
 
-    # The learned estimator (trained parameters committed with the package) refines every UE's
-    # channel estimates inside the plan; without parameters the plan runs the plain estimator.
+    # The learned estimator (trained parameters committed with the package) refines the channel
+    # estimates of the UEs at 64QAM and 256QAM inside the plan (--learned-min-qm): its evaluation
+    # (python -m pusch_b200.learned evaluate --min-qm 6) gives the same BLER and goodput as refining
+    # every UE from 12 dB up, and the same goodput below. Without parameters the plan runs the plain
+    # estimator.
     params = None if args.no_learned else le_mod.load_params()
-    le_rows = plan.le_rows()
-    net = le_mod.LearnedEstimator(ctx, max_rows=le_rows, params=params) if params is not None else None
+    le_use = [ue.modulation_order >= args.learned_min_qm for ue in plan.ues]
+    le_rows = plan.le_rows(le_use)
+    net = le_mod.LearnedEstimator(ctx, max_rows=max(le_rows, 1), params=params) if params is not None else None
 
     def step():
         plan.execute_device(d_grid.data_ptr(), d_tb.data_ptr(), d_res.data_ptr(), None, sptr)
@@ -460,7 +466,7 @@ def run_ours_pusch(args):
 
     # Launch shapes picked by the autotuner on this slot (with the estimator that is timed next).
     if net is not None:
-        plan.set_learned(net)
+        plan.set_learned(net, use=le_use)
     tuning = plan.tuning() if args.no_autotune else plan.autotune(d_grid.data_ptr(), reps=5)[0]
     if net is not None:
         plan.set_learned(None)
@@ -474,7 +480,7 @@ def run_ours_pusch(args):
         batched_plain = {"value": round(p_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 4),
                          "bler": round(1.0 - sum(p_ok) / n, 4),
                          "what": "the same slot plan with the plain estimator (LS + RC FIR + linear interpolation)"}
-        plan.set_learned(net)
+        plan.set_learned(net, use=le_use)
     step_ms, ldpc_ms, learned_ms, clk = timed(args.steps, sample_clocks=True)
     ms = statistics.mean(step_ms)
     results, good, bits_ok = decoded()
@@ -684,9 +690,12 @@ def run_ours_pusch(args):
             "run": {"decoded_bits_per_rank": bits_ok, "bler": round(bler, 4),
                     "l2": "flushed between steps (256 MiB write)", "graph": "one CUDA graph per step",
                     "launch_shapes": tuning.as_dict(),
-                    "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores) on the "
-                                  "plain LS + RC FIR + linear interpolation" if net is not None else
-                                  "plain (LS + RC FIR + linear interpolation)")},
+                    "estimator": ("learned (residual 1-D CNN, 6 blocks x 64 ch, k=5, BF16 tensor cores; DM-RS "
+                                  "corrections and time-basis terms over the slot) on the plain LS + RC FIR + "
+                                  "linear interpolation" if net is not None else
+                                  "plain (LS + RC FIR + linear interpolation)"),
+                    "learned_ues": (f"modulation order >= {args.learned_min_qm}: {sum(le_use)} of {n} UEs, "
+                                    f"{le_rows} estimator rows" if net is not None else None)},
             "slots_per_s": round(1e3 / ms_max * world, 1),
             "configs": sub_lines,
             "plain_per_ue": plain, "batched_plain": batched_plain,
