@@ -85,8 +85,8 @@ def parse_args():
                    help="refine the UEs of this modulation order and above with the learned estimator (0: every UE)")
     p.add_argument("--ldpc-kernel", type=int, default=None,
                    help="LDPC batch kernel of the --workload ldpc line (pg_ldpc_kernel; default: the library's)")
-    p.add_argument("--ldpc-ctas-per-sm", type=int, default=0,
-                   help="resident LDPC CTAs per SM of the --workload ldpc line (0: the kernel's limit)")
+    p.add_argument("--ldpc-ctas-per-sm", type=int, default=2,
+                   help="resident LDPC CTAs per SM of the --workload ldpc line (0: the kernel limit)")
     return p.parse_args()
 
 

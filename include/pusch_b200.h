@@ -479,6 +479,39 @@ typedef struct pg_pusch_plan_info_t {
  * grid_nof_subc. */
 int  pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, size_t grid_words,
                           pg_pusch_plan** out);
+
+/* UCI multiplexed on one UE's PUSCH (HARQ-ACK and CSI Part 1 of 1 to 11 bits each): the fields of
+ * the reference's ulsch_demultiplex::configuration (include/ocudu/phy/upper/channel_processors/
+ * pusch/ulsch_demultiplex.h:31-90) that pg_pusch_ue does not carry. All zero: no UCI. */
+typedef struct pg_pusch_uci {
+  uint32_t nof_harq_ack_rvd;            /* G^HARQ-ACK_rvd, reserved HARQ-ACK soft bits */
+  uint32_t nof_enc_harq_ack_bits;       /* G^HARQ-ACK */
+  uint32_t nof_enc_csi_part1_bits;      /* G^CSI-1 */
+  uint8_t  nof_harq_ack_bits;           /* O^HARQ-ACK, 0..11 */
+  uint8_t  nof_csi_part1_bits;          /* O^CSI-1, 0..11 */
+  uint8_t  nof_cdm_groups_without_data; /* DM-RS type 1: 1 or 2 */
+  uint8_t  reserved;
+} pg_pusch_uci;
+
+/* Decoded UCI of one UE after an execution: the bits of each message (one per byte, message bit i
+ * at index i) and the short-block detector's validity (1: the reference's detection test passes;
+ * 0 also when the UE carries no such message). */
+typedef struct pg_pusch_uci_result {
+  uint8_t harq_ack[11];
+  uint8_t csi_part1[11];
+  uint8_t harq_ack_valid;
+  uint8_t csi_part1_valid;
+} pg_pusch_uci_result;
+
+/* pg_pusch_plan_create with UCI on PUSCH: uci holds one entry per UE (NULL: none). Each execution
+ * demultiplexes the UCI UEs' codewords on the GPU (as pusch_processor_impl.cpp:616-712 configures
+ * it: ulsch_demultiplex, the UL-SCH stream to the decoder, the UCI streams to the UCI decoders),
+ * decodes the UL-SCH stream as usual and detects the short-block messages. */
+int  pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_pusch_uci* uci, int nof_ues,
+                              size_t grid_words, pg_pusch_plan** out);
+/* UCI results of the plan's last execution (nof_ues entries, host memory). Reads device memory
+ * synchronously: call after that execution's stream has completed. */
+int  pg_pusch_plan_uci_results(pg_pusch_plan* plan, pg_pusch_uci_result* out);
 void pg_pusch_plan_destroy(pg_pusch_plan* plan);
 int  pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info);
 

@@ -4,6 +4,7 @@
 #include "../../include/pusch_b200.h"
 
 #include <cuda_runtime.h>
+#include <array>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -115,6 +116,21 @@ int validate_ldpc_descs(pg_context* ctx, const pg_ldpc_cb* cbs, int n, size_t no
 // Uploads the constant base-graph tables (once per process and device).
 int ldpc_upload_tables(pg_context* ctx);
 int uci_upload_tables(pg_context* ctx);
+// UL-SCH demultiplexing of n codewords (uci.cu): the device blob [UE table | symbol table | work
+// items] that the kernel reads, built on the host; sizes (may be null) receives each codeword's
+// UL-SCH, HARQ-ACK and CSI Part 1 soft bits. Returns an error text (empty: consistent).
+struct uci_demux_work {
+  size_t o_syms = 0, o_items = 0;
+  int    nitems = 0;
+};
+std::string uci_demux_blob(const pg_ulsch_demux_config* cfgs, int n, std::vector<uint8_t>& blob, uci_demux_work& w,
+                           std::vector<std::array<uint32_t, 3>>* sizes);
+int uci_demux_launch(pg_context* ctx, const void* blob_dev, const uci_demux_work& w, const int8_t* llrs, int8_t* sch,
+                     int8_t* harq_ack, int8_t* csi_part1, cudaStream_t s);
+// Short-block UCI detection: the device items blob of n messages, and the launch.
+std::string uci_short_blob(const pg_uci_short_block* items, int n, std::vector<uint8_t>& blob);
+int uci_detect_launch(pg_context* ctx, const void* items_dev, int n, const int8_t* llrs, uint8_t* bits, uint8_t* valid,
+                      cudaStream_t s);
 // Open Fronthaul BFP: compressed bytes per PRB, and decompression of nof_prb PRBs into cbf16.
 int bfp_prb_bytes(int data_width);
 int bfp_decompress_launch(pg_context* ctx, const uint8_t* in, uint32_t nof_prb, int data_width, uint32_t* out,

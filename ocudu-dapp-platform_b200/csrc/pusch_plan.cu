@@ -35,6 +35,16 @@ struct pg_pusch_plan {
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
   pg_pusch_ue*    d_ues    = nullptr;
+  // UCI on PUSCH: the demultiplexer's device blob and work shape, the detector's message items,
+  // the UCI soft bits, detected bits (pg_pusch_uci_result layout per UE) and validity per message.
+  void*           d_uci_blob  = nullptr;
+  uci_demux_work  uci_w;
+  void*           d_uci_items = nullptr;
+  int             uci_nmsg    = 0;
+  int8_t*         d_uci_llr   = nullptr;
+  uint8_t*        d_uci_bits  = nullptr;
+  uint8_t*        d_uci_valid = nullptr;
+  std::vector<int> uci_msg_ue, uci_msg_kind; // per message: UE and 0 HARQ-ACK / 1 CSI Part 1
   rm_direct*      d_direct   = nullptr; // per UE: fused rate-dematch placement of the demodulator
   uint8_t*        d_fill     = nullptr; // per codeblock: 1 when the demodulator placed its LLRs
   uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
@@ -226,6 +236,14 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
                            p->le_net != nullptr ? p->d_basis : nullptr,
                            p->le_net != nullptr ? p->d_basis_use : nullptr, p->d_direct, p->d_rm_out);
   }
+  if (rc == PG_OK && p->uci_w.nitems > 0) {
+    // UCI UEs: their codewords into the UL-SCH stream (in the codeword buffer, after the codewords)
+    // and the HARQ-ACK / CSI Part 1 streams, then the short-block detection of the messages.
+    rc = uci_demux_launch(ctx, p->d_uci_blob, p->uci_w, p->d_llr, p->d_llr, p->d_uci_llr, p->d_uci_llr, s);
+    if (rc == PG_OK) {
+      rc = uci_detect_launch(ctx, p->d_uci_items, p->uci_nmsg, p->d_uci_llr, p->d_uci_bits, p->d_uci_valid, s);
+    }
+  }
   if (rc == PG_OK) {
     rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb,
                              p->d_fill);
@@ -287,6 +305,12 @@ extern "C" {
 
 int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, size_t grid_words, pg_pusch_plan** out)
 {
+  return pg_pusch_plan_create_uci(ctx, ues, nullptr, nof_ues, grid_words, out);
+}
+
+int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_pusch_uci* uci, int nof_ues,
+                             size_t grid_words, pg_pusch_plan** out)
+{
   if (ctx == nullptr || out == nullptr) {
     return PG_ERR_INVALID;
   }
@@ -341,6 +365,80 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
     t.rv               = u.rv;
     t.max_iterations   = u.max_iterations;
   }
+  // UCI UEs: the demultiplexer's configuration, the UL-SCH stream in the codeword buffer after
+  // the codewords (the TB decodes from there), the HARQ-ACK and CSI Part 1 streams in their own
+  // buffer, one short-block message per field.
+  std::vector<pg_ulsch_demux_config> ucfg;
+  std::vector<pg_uci_short_block>    umsg;
+  size_t                             uci_llr_total = 0;
+  for (int i = 0; uci != nullptr && i < nof_ues; ++i) {
+    const pg_pusch_uci& q = uci[i];
+    if (q.nof_harq_ack_bits == 0 && q.nof_csi_part1_bits == 0) {
+      continue;
+    }
+    const pg_pusch_ue&    u = p->ues[i];
+    pg_ulsch_demux_config c = {};
+    c.llr_offset            = u.llr_offset;
+    c.nof_llrs              = ue_codeword_bits(u);
+    c.c_init                = ((uint32_t)u.rnti << 15) + u.n_id_data;
+    c.nof_harq_ack_rvd      = q.nof_harq_ack_rvd;
+    c.nof_enc_harq_ack_bits = q.nof_enc_harq_ack_bits;
+    c.nof_enc_csi_part1_bits = q.nof_enc_csi_part1_bits;
+    c.nof_prb               = u.nof_rb;
+    c.dmrs_symbol_mask      = u.dmrs_symbol_mask;
+    c.modulation_order      = u.modulation_order;
+    c.nof_layers            = u.nof_layers;
+    c.start_symbol_index    = u.first_symbol;
+    c.nof_symbols           = u.nof_symbols;
+    c.dmrs_type             = 1;
+    c.nof_cdm_groups_without_data = q.nof_cdm_groups_without_data;
+    c.nof_harq_ack_bits     = q.nof_harq_ack_bits;
+    c.nof_csi_part1_bits    = q.nof_csi_part1_bits;
+    uint32_t sz[3]          = {0, 0, 0};
+    if (pg_ulsch_demultiplex_sizes(&c, sz) != PG_OK) {
+      release(p);
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": inconsistent UCI configuration");
+    }
+    if ((q.nof_harq_ack_bits > 11) || (q.nof_csi_part1_bits > 11)) {
+      release(p);
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": UCI fields of 1 to 11 bits");
+    }
+    p->nof_llrs      = (p->nof_llrs + 15) & ~(size_t)15;
+    c.sch_offset     = (uint32_t)p->nof_llrs;
+    p->nof_llrs += sz[0];
+    c.harq_ack_offset  = (uint32_t)uci_llr_total;
+    c.csi_part1_offset = (uint32_t)(uci_llr_total + sz[1]);
+    for (int k = 0; k < 2; ++k) {
+      const uint8_t nbits = k == 0 ? q.nof_harq_ack_bits : q.nof_csi_part1_bits;
+      if (nbits > 0) {
+        pg_uci_short_block m = {};
+        m.llr_offset         = k == 0 ? c.harq_ack_offset : c.csi_part1_offset;
+        m.nof_llrs           = sz[1 + k];
+        m.out_offset         = (uint32_t)(i * sizeof(pg_pusch_uci_result)) + (k == 0 ? 0u : 11u);
+        m.nof_bits           = nbits;
+        m.modulation_order   = u.modulation_order;
+        umsg.push_back(m);
+        p->uci_msg_ue.push_back(i);
+        p->uci_msg_kind.push_back(k);
+      }
+    }
+    uci_llr_total += sz[1] + sz[2];
+    tbs[i].llr_offset     = c.sch_offset;
+    tbs[i].nof_ch_symbols = sz[0] / u.modulation_order;
+    ucfg.push_back(c);
+  }
+  std::vector<uint8_t> uci_blob, uci_items;
+  if (!ucfg.empty()) {
+    std::string err = uci_demux_blob(ucfg.data(), (int)ucfg.size(), uci_blob, p->uci_w, nullptr);
+    if (err.empty()) {
+      err = uci_short_blob(umsg.data(), (int)umsg.size(), uci_items);
+    }
+    if (!err.empty()) {
+      release(p);
+      return set_error(ctx, PG_ERR_INVALID, err);
+    }
+    p->uci_nmsg = (int)umsg.size();
+  }
   p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
   p->est_total = est_total;
   std::vector<uint32_t> tile_off(nof_ues + 1);
@@ -389,7 +487,9 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->direct = direct;
   p->fill   = fill;
   const size_t o_ework  = o_reoff + al(tile_off.size() * 4);
-  const size_t o_direct = o_ework + al(est_work.size() * 4);
+  const size_t o_ublob  = o_ework + al(est_work.size() * 4);
+  const size_t o_uitems = o_ublob + al(uci_blob.size());
+  const size_t o_direct = o_uitems + al(uci_items.size());
   const size_t o_fill   = o_direct + al(direct.size() * sizeof(rm_direct));
   const size_t desc_end = o_fill + al(fill.size());
   const size_t o_seq    = desc_end;
@@ -408,7 +508,10 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   const size_t o_res    = o_tbout + al(p->tb_bytes);
   const size_t o_epart  = o_res + al((size_t)nof_ues * sizeof(pg_sch_result));
   const size_t o_earr   = o_epart + al((size_t)std::max(1, p->est_nwork) * 16);
-  p->dev_bytes          = o_earr + al((size_t)nof_ues * 16);
+  const size_t o_ullr   = o_earr + al((size_t)nof_ues * 16);
+  const size_t o_ubits  = o_ullr + al(uci_llr_total);
+  const size_t o_uvalid = o_ubits + al((size_t)nof_ues * sizeof(pg_pusch_uci_result));
+  p->dev_bytes          = o_uvalid + al((size_t)std::max(1, p->uci_nmsg));
 
   const size_t h_res  = 0;
   const size_t h_pr   = h_res + al((size_t)nof_ues * sizeof(pg_sch_result));
@@ -454,6 +557,11 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   p->d_fill     = b + o_fill;
   p->d_est_part = b + o_epart;
   p->d_est_arr  = reinterpret_cast<int*>(b + o_earr);
+  p->d_uci_blob  = b + o_ublob;
+  p->d_uci_items = b + o_uitems;
+  p->d_uci_llr   = reinterpret_cast<int8_t*>(b + o_ullr);
+  p->d_uci_bits  = b + o_ubits;
+  p->d_uci_valid = b + o_uvalid;
 
   // Descriptor image in pinned memory, one upload.
   uint8_t* h = static_cast<uint8_t*>(p->host);
@@ -467,6 +575,10 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, tile_off.data(), tile_off.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
+  if (!uci_blob.empty()) {
+    std::memcpy(h + o_ublob, uci_blob.data(), uci_blob.size());
+    std::memcpy(h + o_uitems, uci_items.data(), uci_items.size());
+  }
   std::memcpy(h + o_direct, direct.data(), direct.size() * sizeof(rm_direct));
   std::memcpy(h + o_fill, fill.data(), fill.size());
   cudaStream_t s = ctx->stream;
@@ -476,6 +588,10 @@ int pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, s
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(b + o_earr, 0, (size_t)nof_ues * 16, s), "cudaMemsetAsync(arrivals)");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemsetAsync(b + o_ubits, 0, (size_t)nof_ues * sizeof(pg_pusch_uci_result), s),
+                    "cudaMemsetAsync(UCI results)");
   }
   if (rc == PG_OK) {
     rc = scrambling_launch(ctx, p->d_ues, nof_ues, max_words, p->d_seq_off, p->d_seq, s);
@@ -593,6 +709,37 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
   plan->le_nseq   = (int)seqs.size();
   plan->le_rows   = (int)rows;
   plan->le_net    = net;
+  return PG_OK;
+}
+
+int pg_pusch_plan_uci_results(pg_pusch_plan* plan, pg_pusch_uci_result* out)
+{
+  if (plan == nullptr || out == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  std::vector<pg_pusch_uci_result> r(plan->nof_ues);
+  std::vector<uint8_t>             valid(std::max(1, plan->uci_nmsg));
+  int rc = check_cuda(ctx,
+                      cudaMemcpy(r.data(), plan->d_uci_bits, r.size() * sizeof(pg_pusch_uci_result),
+                                 cudaMemcpyDeviceToHost),
+                      "D2H UCI bits");
+  if (rc == PG_OK && plan->uci_nmsg > 0) {
+    rc = check_cuda(ctx, cudaMemcpy(valid.data(), plan->d_uci_valid, (size_t)plan->uci_nmsg, cudaMemcpyDeviceToHost),
+                    "D2H UCI validity");
+  }
+  if (rc != PG_OK) {
+    return rc;
+  }
+  for (int u = 0; u < plan->nof_ues; ++u) {
+    r[u].harq_ack_valid  = 0;
+    r[u].csi_part1_valid = 0;
+  }
+  for (int m = 0; m < plan->uci_nmsg; ++m) {
+    pg_pusch_uci_result& x = r[plan->uci_msg_ue[m]];
+    (plan->uci_msg_kind[m] == 0 ? x.harq_ack_valid : x.csi_part1_valid) = valid[m];
+  }
+  std::memcpy(out, r.data(), r.size() * sizeof(pg_pusch_uci_result));
   return PG_OK;
 }
 

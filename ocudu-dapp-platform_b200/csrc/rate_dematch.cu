@@ -68,6 +68,10 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   const bool     nd  = d.new_data != 0;
 
   if (E <= V && fill_only != nullptr && fill_only[blockIdx.x] != 0) {
+    // One CTA per codeblock suffices for this fill (at most N / 16 chunks); the others leave.
+    if (blockIdx.y != 0) {
+      return;
+    }
     // The demodulator placed this codeblock's LLRs itself (new data, E <= V): they occupy the valid
     // indices [v0, v0 + E) mod V, up to four position intervals past the fillers. Every other
     // position is a filler (+127) or unreached / beyond N_cb (0). The buffer is written in 16-byte
@@ -107,17 +111,17 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
     const int first = min(head, N);
     const int nch   = (N - first) / 16;
     const int tail  = first + 16 * nch;
-    for (int p = blockIdx.y * kRmThreads + threadIdx.x; p < first; p += gridDim.y * kRmThreads) {
+    for (int p = threadIdx.x; p < first; p += kRmThreads) {
       if (!placed_at(p)) {
         out[p] = fill_value(p);
       }
     }
-    for (int p = tail + blockIdx.y * kRmThreads + threadIdx.x; p < N; p += gridDim.y * kRmThreads) {
+    for (int p = tail + threadIdx.x; p < N; p += kRmThreads) {
       if (!placed_at(p)) {
         out[p] = fill_value(p);
       }
     }
-    for (int q = blockIdx.y * kRmThreads + threadIdx.x; q < nch; q += gridDim.y * kRmThreads) {
+    for (int q = threadIdx.x; q < nch; q += kRmThreads) {
       const int c = first + 16 * q;
       int       kept = 0;
       for (int i = 0; i < nk; ++i) {

@@ -26,6 +26,8 @@
 #include "pg_device.cuh"
 #include "pg_internal.h"
 
+#include <array>
+
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
@@ -490,6 +492,109 @@ std::string ulsch_demux_layout(const pg_ulsch_demux_config& c, demux_layout& out
 
 using namespace pg;
 
+namespace pg {
+
+std::string uci_demux_blob(const pg_ulsch_demux_config* cfgs, int n, std::vector<uint8_t>& blob, uci_demux_work& w,
+                           std::vector<std::array<uint32_t, 3>>* sizes)
+{
+  if (sizes != nullptr) {
+    sizes->assign((size_t)n, std::array<uint32_t, 3>{0, 0, 0});
+  }
+  std::vector<demux_ue>  ues(n);
+  std::vector<demux_sym> syms;
+  for (int u = 0; u < n; ++u) {
+    demux_layout      L;
+    const std::string err = ulsch_demux_layout(cfgs[u], L);
+    if (!err.empty()) {
+      return "UE " + std::to_string(u) + ": " + err;
+    }
+    if (sizes != nullptr) {
+      for (int k = 0; k < 3; ++k) {
+        (*sizes)[u][k] = L.sizes[k];
+      }
+    }
+    demux_ue& d  = ues[u];
+    d.llr_offset = cfgs[u].llr_offset;
+    d.sch_offset = cfgs[u].sch_offset;
+    d.ack_offset = cfgs[u].harq_ack_offset;
+    d.csi_offset = cfgs[u].csi_part1_offset;
+    d.c_init     = cfgs[u].c_init;
+    d.sym0       = (uint16_t)syms.size();
+    d.nsym       = (uint16_t)L.syms.size();
+    d.bpr        = (uint8_t)(cfgs[u].modulation_order * cfgs[u].nof_layers);
+    d.qm         = cfgs[u].modulation_order;
+    d.ack_bits   = (uint8_t)cfgs[u].nof_harq_ack_bits;
+    d.csi_bits   = (uint8_t)cfgs[u].nof_csi_part1_bits;
+    for (demux_sym sy : L.syms) {
+      sy.ue = (uint32_t)u;
+      syms.push_back(sy);
+    }
+  }
+  std::vector<uint2> items;
+  for (size_t k = 0; k < syms.size(); ++k) {
+    for (uint32_t r0 = 0; r0 < syms[k].nre; r0 += kDemuxChunk) {
+      const uint32_t r1 = std::min<uint32_t>(syms[k].nre, r0 + kDemuxChunk);
+      items.push_back(make_uint2((uint32_t)k, r0 | (r1 << 16)));
+    }
+  }
+  // [UEs | symbols | items], the items (8-byte vectors) on a 16-byte boundary.
+  const size_t b_ues = ues.size() * sizeof(demux_ue), b_syms = syms.size() * sizeof(demux_sym);
+  w.o_syms           = b_ues;
+  w.o_items          = (b_ues + b_syms + 15) & ~(size_t)15;
+  w.nitems           = (int)items.size();
+  blob.assign(w.o_items + items.size() * sizeof(uint2), 0);
+  std::memcpy(blob.data(), ues.data(), b_ues);
+  std::memcpy(blob.data() + b_ues, syms.data(), b_syms);
+  std::memcpy(blob.data() + w.o_items, items.data(), items.size() * sizeof(uint2));
+  return std::string();
+}
+
+int uci_demux_launch(pg_context* ctx, const void* blob_dev, const uci_demux_work& w, const int8_t* llrs, int8_t* sch,
+                     int8_t* harq_ack, int8_t* csi_part1, cudaStream_t s)
+{
+  if (w.nitems == 0) {
+    return PG_OK;
+  }
+  const uint8_t* b = static_cast<const uint8_t*>(blob_dev);
+  ulsch_demux_kernel<<<(unsigned)w.nitems, kDemuxChunk, 0, s>>>(
+      reinterpret_cast<const demux_ue*>(b), reinterpret_cast<const demux_sym*>(b + w.o_syms),
+      reinterpret_cast<const uint2*>(b + w.o_items), llrs, sch, harq_ack, csi_part1, ctx->dev.gold);
+  return check_cuda(ctx, cudaGetLastError(), "ulsch_demux_kernel launch");
+}
+
+std::string uci_short_blob(const pg_uci_short_block* items, int n, std::vector<uint8_t>& blob)
+{
+  std::vector<short_item> v(n);
+  for (int i = 0; i < n; ++i) {
+    const pg_uci_short_block& it = items[i];
+    const unsigned            qm = it.modulation_order;
+    if (it.nof_bits < 1 || it.nof_bits > 11) {
+      return "message " + std::to_string(i) + ": 1 to 11 bits";
+    }
+    if (qm != 1 && qm != 2 && qm != 4 && qm != 6 && qm != 8) {
+      return "message " + std::to_string(i) + ": invalid modulation order";
+    }
+    v[i] = short_item{it.llr_offset, it.nof_llrs, it.out_offset, it.nof_bits, (uint8_t)qm, {0, 0}};
+  }
+  blob.resize(v.size() * sizeof(short_item));
+  std::memcpy(blob.data(), v.data(), blob.size());
+  return std::string();
+}
+
+int uci_detect_launch(pg_context* ctx, const void* items_dev, int n, const int8_t* llrs, uint8_t* bits, uint8_t* valid,
+                      cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  const unsigned warps_per_cta = 4;
+  uci_short_block_kernel<<<(unsigned)((n + warps_per_cta - 1) / warps_per_cta), 32 * warps_per_cta, 0, s>>>(
+      static_cast<const short_item*>(items_dev), n, llrs, bits, valid);
+  return check_cuda(ctx, cudaGetLastError(), "uci_short_block_kernel launch");
+}
+
+} // namespace pg
+
 extern "C" {
 
 int pg_ulsch_demultiplex_sizes(const pg_ulsch_demux_config* cfg, uint32_t* sizes)
@@ -516,66 +621,31 @@ int pg_ulsch_demultiplex_device(pg_context* ctx, const pg_ulsch_demux_config* cf
   if (n < 0 || (n > 0 && (cfgs == nullptr || llrs == nullptr || sch == nullptr))) {
     return set_error(ctx, PG_ERR_INVALID, "null argument");
   }
-  std::vector<demux_ue>  ues(n);
-  std::vector<demux_sym> syms;
+  std::vector<uint8_t>                 blob;
+  uci_demux_work                       w;
+  std::vector<std::array<uint32_t, 3>> sizes;
+  const std::string                    err = uci_demux_blob(cfgs, n, blob, w, &sizes);
+  if (!err.empty()) {
+    return set_error(ctx, PG_ERR_INVALID, err);
+  }
   for (int u = 0; u < n; ++u) {
-    demux_layout      L;
-    const std::string err = ulsch_demux_layout(cfgs[u], L);
-    if (!err.empty()) {
-      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(u) + ": " + err);
-    }
-    if ((L.sizes[1] > 0 && harq_ack == nullptr) || (L.sizes[2] > 0 && csi_part1 == nullptr)) {
+    if ((sizes[u][1] > 0 && harq_ack == nullptr) || (sizes[u][2] > 0 && csi_part1 == nullptr)) {
       return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(u) + ": null UCI output");
     }
-    demux_ue& d  = ues[u];
-    d.llr_offset = cfgs[u].llr_offset;
-    d.sch_offset = cfgs[u].sch_offset;
-    d.ack_offset = cfgs[u].harq_ack_offset;
-    d.csi_offset = cfgs[u].csi_part1_offset;
-    d.c_init     = cfgs[u].c_init;
-    d.sym0       = (uint16_t)syms.size();
-    d.nsym       = (uint16_t)L.syms.size();
-    d.bpr        = (uint8_t)(cfgs[u].modulation_order * cfgs[u].nof_layers);
-    d.qm         = cfgs[u].modulation_order;
-    d.ack_bits   = (uint8_t)cfgs[u].nof_harq_ack_bits;
-    d.csi_bits   = (uint8_t)cfgs[u].nof_csi_part1_bits;
-    for (demux_sym s : L.syms) {
-      s.ue = (uint32_t)u;
-      syms.push_back(s);
-    }
   }
-  if (syms.empty()) {
+  if (w.nitems == 0) {
     return PG_OK;
   }
-  std::vector<uint2> items;
-  for (size_t k = 0; k < syms.size(); ++k) {
-    for (uint32_t r0 = 0; r0 < syms[k].nre; r0 += kDemuxChunk) {
-      const uint32_t r1 = std::min<uint32_t>(syms[k].nre, r0 + kDemuxChunk);
-      items.push_back(make_uint2((uint32_t)k, r0 | (r1 << 16)));
-    }
-  }
-  // [UEs | symbols | items], the items (8-byte vectors) on a 16-byte boundary.
-  const size_t         b_ues = ues.size() * sizeof(demux_ue), b_syms = syms.size() * sizeof(demux_sym);
-  const size_t         o_items = (b_ues + b_syms + 15) & ~(size_t)15;
-  std::vector<uint8_t> blob(o_items + items.size() * sizeof(uint2));
-  std::memcpy(blob.data(), ues.data(), b_ues);
-  std::memcpy(blob.data() + b_ues, syms.data(), b_syms);
-  std::memcpy(blob.data() + o_items, items.data(), items.size() * sizeof(uint2));
   cudaStream_t s   = static_cast<cudaStream_t>(stream);
   void*        dev = nullptr;
   if (int rc = stage_slot(ctx, SLOT_UCI, blob.data(), blob.size(), s, &dev)) {
     return rc;
   }
-  const demux_ue*  d_ues  = static_cast<const demux_ue*>(dev);
-  const demux_sym* d_syms  = reinterpret_cast<const demux_sym*>(static_cast<uint8_t*>(dev) + b_ues);
-  const uint2*     d_items = reinterpret_cast<const uint2*>(static_cast<uint8_t*>(dev) + o_items);
   const unsigned int rec = timing_record_flags(ctx, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, s, rec);
   }
-  ulsch_demux_kernel<<<(unsigned)items.size(), kDemuxChunk, 0, s>>>(d_ues, d_syms, d_items, llrs, sch, harq_ack,
-                                                                     csi_part1, ctx->dev.gold);
-  const int rc = check_cuda(ctx, cudaGetLastError(), "ulsch_demux_kernel launch");
+  const int rc = uci_demux_launch(ctx, dev, w, llrs, sch, harq_ack, csi_part1, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
   }
@@ -594,31 +664,21 @@ int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* 
   if (n == 0) {
     return PG_OK;
   }
-  std::vector<short_item> v(n);
-  for (int i = 0; i < n; ++i) {
-    const pg_uci_short_block& it = items[i];
-    const unsigned            qm = it.modulation_order;
-    if (it.nof_bits < 1 || it.nof_bits > 11) {
-      return set_error(ctx, PG_ERR_INVALID, "message " + std::to_string(i) + ": 1 to 11 bits");
-    }
-    if (qm != 1 && qm != 2 && qm != 4 && qm != 6 && qm != 8) {
-      return set_error(ctx, PG_ERR_INVALID, "message " + std::to_string(i) + ": invalid modulation order");
-    }
-    v[i] = short_item{it.llr_offset, it.nof_llrs, it.out_offset, it.nof_bits, (uint8_t)qm, {0, 0}};
+  std::vector<uint8_t> blob;
+  const std::string    err = uci_short_blob(items, n, blob);
+  if (!err.empty()) {
+    return set_error(ctx, PG_ERR_INVALID, err);
   }
   cudaStream_t s   = static_cast<cudaStream_t>(stream);
   void*        dev = nullptr;
-  if (int rc = stage_slot(ctx, SLOT_UCI_SHORT, v.data(), v.size() * sizeof(short_item), s, &dev)) {
+  if (int rc = stage_slot(ctx, SLOT_UCI_SHORT, blob.data(), blob.size(), s, &dev)) {
     return rc;
   }
-  const unsigned warps_per_cta = 4;
-  const unsigned int rec           = timing_record_flags(ctx, s);
+  const unsigned int rec = timing_record_flags(ctx, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, s, rec);
   }
-  uci_short_block_kernel<<<(unsigned)((n + warps_per_cta - 1) / warps_per_cta), 32 * warps_per_cta, 0, s>>>(
-      static_cast<const short_item*>(dev), n, llrs, bits, valid);
-  const int rc = check_cuda(ctx, cudaGetLastError(), "uci_short_block_kernel launch");
+  const int rc = uci_detect_launch(ctx, dev, n, llrs, bits, valid, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
   }

@@ -101,6 +101,18 @@ class PgUlschDemuxConfig(ctypes.Structure):
                 ("nof_csi_part1_bits", ctypes.c_uint8)]
 
 
+class PgPuschUci(ctypes.Structure):
+    _fields_ = [("nof_harq_ack_rvd", ctypes.c_uint32), ("nof_enc_harq_ack_bits", ctypes.c_uint32),
+                ("nof_enc_csi_part1_bits", ctypes.c_uint32), ("nof_harq_ack_bits", ctypes.c_uint8),
+                ("nof_csi_part1_bits", ctypes.c_uint8), ("nof_cdm_groups_without_data", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8)]
+
+
+class PgPuschUciResult(ctypes.Structure):
+    _fields_ = [("harq_ack", ctypes.c_uint8 * 11), ("csi_part1", ctypes.c_uint8 * 11), ("harq_ack_valid", ctypes.c_uint8),
+                ("csi_part1_valid", ctypes.c_uint8)]
+
+
 class PgUciShortBlock(ctypes.Structure):
     _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("out_offset", ctypes.c_uint32),
                 ("nof_bits", ctypes.c_uint8), ("modulation_order", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 2)]
@@ -165,6 +177,8 @@ SIGNATURES = {
     "pg_pusch_process_host": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, ctypes.c_size_t, _VP, ctypes.c_size_t, _VP,
                                              _VP]),
     "pg_pusch_plan_create": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
+    "pg_pusch_plan_create_uci": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
+    "pg_pusch_plan_uci_results": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_destroy": (None, [_VP]),
     "pg_pusch_plan_info": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_graph": (ctypes.c_int, [_VP, ctypes.c_int]),

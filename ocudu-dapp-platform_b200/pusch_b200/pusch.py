@@ -172,14 +172,22 @@ class PuschSlotPlan:
     pusch_processor::process (pusch_processor.h:199-203)."""
 
     def __init__(self, context: _native.Context, slots: Sequence[PuschSlot], max_iterations=6, dc_subcarrier=-1,
-                 graph=False):
+                 graph=False, uci=None):
+        """uci: None, or one _native.PgPuschUci per UE (UCI multiplexed on the UE's PUSCH; all-zero
+        entries carry none)."""
         self.ctx = context
         self.lib = _native.load()
         self.descs, self.grid, self.tb_bytes, self.ues = batch_descriptors(slots, max_iterations, dc_subcarrier)
         self.n = len(self.ues)
         h = ctypes.c_void_p()
-        self.ctx.check(self.lib.pg_pusch_plan_create(self.ctx.handle, ctypes.addressof(self.descs), self.n,
-                                                     self.grid.size, ctypes.byref(h)))
+        if uci is None:
+            self.ctx.check(self.lib.pg_pusch_plan_create(self.ctx.handle, ctypes.addressof(self.descs), self.n,
+                                                         self.grid.size, ctypes.byref(h)))
+        else:
+            arr = (_native.PgPuschUci * self.n)(*uci)
+            self.ctx.check(self.lib.pg_pusch_plan_create_uci(self.ctx.handle, ctypes.addressof(self.descs),
+                                                             ctypes.addressof(arr), self.n, self.grid.size,
+                                                             ctypes.byref(h)))
         self.handle = h
         info = PgPuschPlanInfo()
         self.ctx.check(self.lib.pg_pusch_plan_info(self.handle, ctypes.byref(info)))
@@ -188,6 +196,13 @@ class PuschSlotPlan:
 
     def set_graph(self, enabled: bool):
         self.ctx.check(self.lib.pg_pusch_plan_set_graph(self.handle, int(bool(enabled))))
+
+    def uci_results(self):
+        """UCI of the last execution per UE: (harq_ack bits, valid, csi_part1 bits, valid), the bit
+        arrays of each message's length (empty when the UE carries no such field)."""
+        res = (_native.PgPuschUciResult * self.n)()
+        self.ctx.check(self.lib.pg_pusch_plan_uci_results(self.handle, ctypes.addressof(res)))
+        return res
 
     def set_learned(self, net, use=None):
         """Refines the channel estimates with a LearnedEstimator (None: the plain estimator only)
