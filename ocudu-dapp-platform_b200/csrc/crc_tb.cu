@@ -139,6 +139,9 @@ __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_de
   __shared__ uint32_t byte_tab[256];
   __shared__ uint32_t red[kCrcThreads / 32];
   const pg_tb_desc    d = tbs[blockIdx.x];
+  if (blockIdx.y * (uint64_t)kTbChunkWords * 32u >= (uint64_t)d.cb_payload_bits * d.nof_cbs) {
+    return; // no chunk of this TB for this CTA (the whole CTA leaves: no barrier is pending)
+  }
   uint32_t            g;
   int                 order;
   pg::crc_poly_params(d.crc_poly, &g, &order);

@@ -22,6 +22,7 @@ __device__ __forceinline__ uint32_t gold_word(const uint32_t* __restrict__ tab, 
   const uint32_t w  = bit >> 5;
   const uint32_t sh = bit & 31u;
   uint32_t       lo = __ldg(tab + w), hi = __ldg(tab + w + 1);
+#pragma unroll
   for (int i = 0; i < 31; ++i) {
     if ((c_init >> i) & 1u) {
       const uint32_t* b = tab + (size_t)(i + 1) * words;

@@ -149,11 +149,15 @@ int ensure_scratch(pg_context* ctx, void** buf, size_t* cap, size_t bytes, const
 int validate_rm_descs(pg_context* ctx, const pg_rm_cb* cbs, int n, size_t in_total, size_t out_total);
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
                         cudaStream_t stream);
-// Same with ctas_per_cb CTAs per codeblock (1..32). fill_only (may be NULL): per codeblock, 1 when
-// the demodulator stored its received LLRs directly (rm_direct); the kernel then writes only its
-// filler, unreached and beyond-N_cb positions.
+// Same with ctas_per_cb CTAs per codeblock (1..32), over the n codeblocks list[0 .. n - 1] of
+// descs_dev when list is not NULL (a plan's codeblocks that the demodulator does not store in place).
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
-                        cudaStream_t stream, int ctas_per_cb, const uint8_t* fill_only = nullptr);
+                        cudaStream_t stream, int ctas_per_cb, const uint32_t* list = nullptr);
+// Writes what rate dematching leaves at the positions no LLR reaches (+127 at the fillers, 0
+// elsewhere) over the whole circular buffer of every codeblock with placed[c] = 1, to be done
+// before the demodulator stores those codeblocks' LLRs in place.
+int rm_prefill_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const uint8_t* placed, int8_t* out,
+                      cudaStream_t stream);
 void crc_tables_host(uint32_t* tab);
 int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8_t* data, uint32_t* out,
                cudaStream_t stream);
@@ -165,13 +169,15 @@ int est_upload_tables(pg_context* ctx);
 int demod_upload_tables(pg_context* ctx, const void* slope, const void* intercept, const void* width);
 uint32_t ue_codeword_bits(const pg_pusch_ue& u);
 int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_tiles,
-                 const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                 const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                  const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
                  cudaStream_t s);
-// Prefix sums (n + 1 entries) of the UEs' data REs; returns the total.
-// Prefix sums (n + 1) of the UEs' demodulation tiles (groups of consecutive subcarriers that one
-// CTA demodulates over every data symbol); returns the total.
-uint32_t demod_tile_offsets(const pg_pusch_ue* ues, int n, uint32_t* off);
+// The batch's demodulation tiles (groups of consecutive subcarriers that one CTA demodulates over
+// every data symbol), appended to `map` one word each: UE index | tile index within the UE's
+// allocation << 16. Returns the number of tiles (the launchers refuse batches of more than
+// kDemodMaxUes UEs).
+constexpr int kDemodMaxUes = 65535;
+uint32_t demod_tile_map(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& map);
 // Host-side work lists of a batch of transport blocks: one rate-dematch and one LDPC descriptor
 // per codeblock, one TB descriptor per TB, the bit offset of each codeblock's decoded bits.
 struct sch_work {
@@ -189,7 +195,7 @@ int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
                       const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s);
 // Demodulation with the scrambling sequences already generated.
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
-                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                      const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s);
 // Same with `block` threads per CTA (64, 128 or 256) and res_per_thread tiles per CTA (1..8), and
@@ -206,7 +212,7 @@ struct rm_direct {
   uint32_t out0, cb_len, e_small, e_large, n_small, V, v0, inf, F, enabled;
 };
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
-                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                      const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis = nullptr,
                       const uint8_t* basis_use = nullptr, const rm_direct* direct = nullptr, int8_t* rm_out = nullptr);
@@ -215,15 +221,20 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 int sch_decode_device_llrs(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, const int8_t* d_llrs,
                            size_t nof_llrs, uint8_t* tb_out, size_t tb_out_len, pg_sch_result* results);
 int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n);
-// Channel estimation of a batch (pusch_estimate_chunk_kernel + pusch_estimate_finish_kernel).
-// est_work_build writes the work list of the UEs (one item per (UE, port, chunk of pilots)) followed
-// by the first item of every (UE, port) (4 n + 1 entries) and returns the item count; work_dev
-// holds that blob on the device, partials nwork float4, arrivals 4 n ints that are zero before the
-// launch (and again after it).
-int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob);
+// Channel estimation of a batch (pusch_estimate_chunk_kernel). est_work_build writes the work list
+// of the UEs (one item per (UE, port, chunk of pilots)), then the first item of every (UE, port)
+// (4 n + 1 entries), then each UE's offset in the pilot-bit rows of dmrs_bits_launch (n entries,
+// *pilot_words words in total), and returns the item count. work_dev holds that blob on the device,
+// partials nwork float4, arrivals 4 n ints that are zero before the launch (and again after it).
+// pilot_bits (may be NULL: the kernel then forms the pilots from the Gold basis) holds the rows
+// written by dmrs_bits_launch for the same UEs and blob.
+int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob, uint32_t* pilot_words = nullptr);
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
                     void* partials, int* arrivals, const uint32_t* grids, float* est, float* ls,
-                    pg_port_result* results, cudaStream_t s);
+                    pg_port_result* results, cudaStream_t s, const uint32_t* pilot_bits = nullptr);
+// The DM-RS sequence bits of every UE (their slot, N_ID, n_SCID and symbols), once per plan.
+int dmrs_bits_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
+                     uint32_t* bits_dev, cudaStream_t s);
 // The same from host UEs: stages the UEs and their work list (SLOT_UE), partials in the context.
 int estimate_launch_host(pg_context* ctx, const pg_pusch_ue* ues, int n, const uint32_t* grids, float* est, float* ls,
                          pg_port_result* results, cudaStream_t s);

@@ -36,9 +36,9 @@ void plan(const pg_pusch_ue* ues, int n, slot_layout& L, bool assign_offsets)
     L.seq_total += words;
     L.max_words = std::max(L.max_words, words);
   }
-  L.offs.assign(2 * (size_t)n + 1, 0);
-  std::copy(L.seq_off.begin(), L.seq_off.end(), L.offs.begin());
-  L.total_tiles = demod_tile_offsets(L.ues.data(), n, L.offs.data() + n);
+  // [sequence offsets (n) | demodulation tile map]
+  L.offs.assign(L.seq_off.begin(), L.seq_off.end());
+  L.total_tiles = demod_tile_map(L.ues.data(), n, L.offs);
 }
 
 } // namespace
@@ -60,7 +60,7 @@ int pg_pusch_demodulate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_
   slot_layout L;
   plan(ues, nof_ues, L, false);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // Scratch: [sequence offsets | data RE offsets | sequences].
+  // Scratch: [sequence offsets | demodulation tile map | sequences].
   const size_t noffs = L.offs.size();
   const size_t bytes = 256 + noffs * 4 + L.seq_total * 4;
   if (int rc = ensure_scratch(ctx, &ctx->scratch_b, &ctx->scratch_b_cap, bytes, "cudaMalloc(demod scratch)")) {

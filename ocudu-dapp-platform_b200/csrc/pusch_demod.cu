@@ -370,7 +370,7 @@ __device__ __forceinline__ void demod_re(const pg_pusch_ue& ue, const uint32_t* 
 // over every data symbol. The CTA stages the tile's frequency responses (and the learned
 // estimator's time-basis coefficients) in shared memory once, so each is read from memory once
 // rather than once per data symbol; a warp's threads take consecutive subcarriers of one symbol,
-// so grid reads and LLR stores stay coalesced. tile_off[u] .. tile_off[u + 1] - 1 are UE u's tiles.
+// so grid reads and LLR stores stay coalesced.
 constexpr int kDemodTile = 32;
 
 template <int L, int P, int QM>
@@ -380,13 +380,17 @@ __device__ __forceinline__ void demod_tile(const pg_pusch_ue& ue, int u, int j0,
                                            int8_t* llrs, const demap_tables& tb, const pg::rm_direct* dr,
                                            int8_t* rm_out)
 {
+  // Work item q = (data symbol q / kDemodTile, subcarrier j0 + q % kDemodTile); the missing
+  // subcarriers of a UE's last, narrower tile idle.
   const int nsc = 12 * ue.nof_rb;
-  for (int q = threadIdx.x; q < nds * nt; q += blockDim.x) {
-    const int di = q / nt;
-    const int jj = q - di * nt;
-    const int j  = j0 + jj;
-    demod_re<L, P, QM>(ue, grid, s_est, s_bas, pres, nd, s_w[di], s_sym[di], di * nsc + j, j, sq, llrs, tb, dr, rm_out,
-                       kDemodTile, jj);
+  for (int q = threadIdx.x; q < nds * kDemodTile; q += blockDim.x) {
+    const int di = q / kDemodTile;
+    const int jj = q % kDemodTile;
+    if (jj < nt) {
+      const int j = j0 + jj;
+      demod_re<L, P, QM>(ue, grid, s_est, s_bas, pres, nd, s_w[di], s_sym[di], di * nsc + j, j, sq, llrs, tb, dr,
+                         rm_out, kDemodTile, jj);
+    }
   }
 }
 
@@ -406,8 +410,9 @@ __device__ __forceinline__ void demod_tile_qm(const pg_pusch_ue& ue, int u, int 
 }
 
 // tiles_per_cta consecutive tiles of the batch's tile list per CTA (a launch-shape tunable).
-__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, int nof_ues,
-                                                          const uint32_t* __restrict__ tile_off,
+// tile_map[t] = UE index | tile index within the UE's allocation << 16.
+__global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __restrict__ ues, uint32_t ntiles,
+                                                          const uint32_t* __restrict__ tile_map,
                                                           const uint32_t* __restrict__ grids,
                                                           const float2* __restrict__ est_all,
                                                           const float2* __restrict__ basis_all,
@@ -425,7 +430,8 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
   __shared__ float2 s_bas[4 * 2 * 2 * kDemodTile];
   __shared__ int    s_sym[14];
   __shared__ float  s_w[14];
-  __shared__ pg::rm_direct s_dr;
+  __shared__ pg_port_result s_pres[4];
+  __shared__ pg::rm_direct  s_dr;
   for (int i = threadIdx.x; i < 3 * 4 * 16; i += blockDim.x) {
     s_slope[i] = (&c_slope_d[0][0][0])[i];
     s_icpt[i]  = (&c_intercept_d[0][0][0])[i];
@@ -434,91 +440,75 @@ __global__ void __launch_bounds__(256) pusch_demod_kernel(const pg_pusch_ue* __r
     s_width[threadIdx.x]     = c_width_d[threadIdx.x];
     s_width[3 + threadIdx.x] = 1.0f / c_width_d[threadIdx.x];
   }
-  const demap_tables tb     = {s_slope, s_icpt, s_width};
-  const uint32_t     ntiles = __ldg(tile_off + nof_ues);
+  const demap_tables tb = {s_slope, s_icpt, s_width};
   for (int k = 0; k < tiles_per_cta; ++k) {
     const uint32_t t = blockIdx.x * (uint32_t)tiles_per_cta + (uint32_t)k;
     if (t >= ntiles) {
       break;
     }
-    // UE of tile t: the last u with tile_off[u] <= t.
-    int lo = 0, hi = nof_ues - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(tile_off + mid) <= t) {
-        lo = mid;
-      } else {
-        hi = mid - 1;
-      }
-    }
-    const int         u   = lo;
+    const uint32_t    tm  = __ldg(tile_map + t);
+    const int         u   = (int)(tm & 0xffffu);
     const pg_pusch_ue ue  = ues[u];
     const int         nsc = 12 * ue.nof_rb;
-    const int         j0  = (int)(t - __ldg(tile_off + u)) * kDemodTile;
+    const int         j0  = (int)(tm >> 16) * kDemodTile;
     const int         nt  = min(kDemodTile, nsc - j0);
-    int               d0 = -1, d1 = -1, nd = 0, nds = 0;
-    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-      if ((ue.dmrs_symbol_mask >> s) & 1) {
-        if (nd == 0) {
-          d0 = s;
-        } else if (nd == 1) {
-          d1 = s;
-        }
-        ++nd;
-      }
-    }
+    // The allocation's DM-RS symbols (the first two are the interpolation's ends) and data symbols.
+    const uint32_t alloc = ((1u << (ue.first_symbol + ue.nof_symbols)) - 1u) & ~((1u << ue.first_symbol) - 1u);
+    const uint32_t dm    = ue.dmrs_symbol_mask & alloc;
+    const uint32_t data  = alloc & ~dm;
+    const int      nd    = __popc(dm);
+    const int      nds   = __popc(data);
+    const int      d0    = __ffs(dm) - 1;
+    const int      d1    = __ffs(dm & (dm - 1u)) - 1;
     __syncthreads(); // the previous tile's readers are done with the shared arrays
     const bool placed = direct != nullptr && direct[u].enabled != 0;
-    if (threadIdx.x == 0) {
-      if (placed) {
-        s_dr = direct[u];
-      }
-      for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-        if (!((ue.dmrs_symbol_mask >> s) & 1)) {
-          s_sym[nds] = s;
-          s_w[nds]   = nd == 2 ? (float)(s - d0) / (float)(d1 - d0) : 0.f;
-          ++nds;
-        }
-      }
+    if (placed && threadIdx.x < sizeof(pg::rm_direct) / 4) {
+      reinterpret_cast<uint32_t*>(&s_dr)[threadIdx.x] = reinterpret_cast<const uint32_t*>(direct + u)[threadIdx.x];
+    }
+    if (threadIdx.x < 14 && ((data >> threadIdx.x) & 1u)) {
+      const int s      = (int)threadIdx.x;
+      const int r      = __popc(data & ((1u << s) - 1u));
+      s_sym[r]         = s;
+      s_w[r]           = nd == 2 ? (float)(s - d0) / (float)(d1 - d0) : 0.f;
+    }
+    if (threadIdx.x >= 32 && threadIdx.x < 32 + ue.nof_rx_ports) {
+      s_pres[threadIdx.x - 32] = port_results[(size_t)u * 4 + threadIdx.x - 32];
     }
     const int ne = nd == 2 ? 2 : 1;
     const bool use_basis = basis_all != nullptr && basis_use != nullptr && nd == 2 && basis_use[u] != 0;
     const float2* est = est_all + ue.est_offset;
     const float2* bas = use_basis ? basis_all + ue.est_offset : nullptr;
-    for (int i = threadIdx.x; i < ue.nof_rx_ports * ne * ue.nof_layers * nt; i += blockDim.x) {
-      const int row = i / nt;
-      const int jj  = i - row * nt;
-      // row = (p * ne + d) * L + l of the tile; the allocation's est rows are (p * nd + d) * L + l.
-      const int l  = row % ue.nof_layers;
-      const int pd = row / ue.nof_layers;
-      const int d  = pd % ne;
-      const int p  = pd / ne;
-      const size_t src = ((size_t)(p * nd + d) * ue.nof_layers + l) * nsc + j0 + jj;
-      s_est[row * kDemodTile + jj] = est[src];
-      if (bas != nullptr) {
-        s_bas[row * kDemodTile + jj] = bas[src];
+    for (int i = threadIdx.x; i < ue.nof_rx_ports * ne * ue.nof_layers * kDemodTile; i += blockDim.x) {
+      const int row = i / kDemodTile;
+      const int jj  = i % kDemodTile;
+      if (jj < nt) {
+        // row = (p * ne + d) * L + l of the tile; the allocation's est rows are (p * nd + d) * L + l.
+        const int    l   = row % ue.nof_layers;
+        const int    pd  = row / ue.nof_layers;
+        const int    d   = pd % ne;
+        const int    p   = pd / ne;
+        const size_t src = ((size_t)(p * nd + d) * ue.nof_layers + l) * nsc + j0 + jj;
+        s_est[row * kDemodTile + jj] = est[src];
+        if (bas != nullptr) {
+          s_bas[row * kDemodTile + jj] = bas[src];
+        }
       }
     }
     __syncthreads();
-    nds = 0;
-    for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols; ++s) {
-      nds += !((ue.dmrs_symbol_mask >> s) & 1);
-    }
     const pg::rm_direct*  dr   = placed ? &s_dr : nullptr;
     const uint32_t*       grid = grids + ue.grid_offset;
-    const pg_port_result* pres = port_results + (size_t)u * 4;
     const uint32_t*       sq   = seq + seq_offsets[u];
     const float2*         sb   = bas != nullptr ? s_bas : nullptr;
     if (ue.nof_layers == 1) {
       switch (ue.nof_rx_ports) {
-        case 1: demod_tile_qm<1, 1>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
-        case 2: demod_tile_qm<1, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
-        default: demod_tile_qm<1, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+        case 1: demod_tile_qm<1, 1>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, s_pres, sq, llrs, tb, dr, rm_out); break;
+        case 2: demod_tile_qm<1, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, s_pres, sq, llrs, tb, dr, rm_out); break;
+        default: demod_tile_qm<1, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, s_pres, sq, llrs, tb, dr, rm_out); break;
       }
     } else {
       switch (ue.nof_rx_ports) {
-        case 2: demod_tile_qm<2, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
-        default: demod_tile_qm<2, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, pres, sq, llrs, tb, dr, rm_out); break;
+        case 2: demod_tile_qm<2, 2>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, s_pres, sq, llrs, tb, dr, rm_out); break;
+        default: demod_tile_qm<2, 4>(ue, u, j0, nt, ne, s_sym, s_w, nds, grid, s_est, sb, s_pres, sq, llrs, tb, dr, rm_out); break;
       }
     }
   }
@@ -561,16 +551,16 @@ int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
 }
 
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
-                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                      const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s)
 {
-  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_off_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
+  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_map_dev, grids, est, port_results, seq_offsets_dev, seq_dev,
                            llrs, s, 256, 1);
 }
 
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
-                      const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                      const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                       const pg_port_result* port_results, const uint32_t* seq_offsets_dev, const uint32_t* seq_dev,
                       int8_t* llrs, cudaStream_t s, int block, int res_per_thread, const float* basis,
                       const uint8_t* basis_use, const rm_direct* direct, int8_t* rm_out)
@@ -578,41 +568,46 @@ int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32
   if (n == 0 || total_tiles == 0) {
     return PG_OK;
   }
+  if (n > kDemodMaxUes) {
+    return set_error(ctx, PG_ERR_INVALID, "more than 65535 UEs in one demodulation batch");
+  }
   if (block != 64 && block != 128 && block != 256) {
     block = 256;
   }
   res_per_thread       = std::max(1, std::min(8, res_per_thread));
   const uint32_t per   = (uint32_t)res_per_thread; // tiles per CTA
   pusch_demod_kernel<<<(total_tiles + per - 1) / per, block, 0, s>>>(
-      ues_dev, n, tile_off_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
+      ues_dev, total_tiles, tile_map_dev, grids, reinterpret_cast<const float2*>(est), reinterpret_cast<const float2*>(basis),
       basis_use, port_results, seq_offsets_dev, seq_dev, llrs, res_per_thread, direct, rm_out);
   return check_cuda(ctx, cudaGetLastError(), "pusch_demod_kernel launch");
 }
 
 // Enqueues scrambling-sequence generation and demodulation; seq_offsets_dev / seq_dev are
-// device scratch sized by the caller from ue_codeword_bits, tile_off_dev holds n + 1 prefix sums of
-// the UEs' demodulation tiles (demod_tile_offsets).
+// device scratch sized by the caller from ue_codeword_bits, tile_map_dev holds the batch's
+// demodulation tiles (demod_tile_map).
 int demod_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words, uint32_t total_tiles,
-                 const uint32_t* tile_off_dev, const uint32_t* grids, const float* est,
+                 const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,
                  const pg_port_result* port_results, const uint32_t* seq_offsets_dev, uint32_t* seq_dev, int8_t* llrs,
                  cudaStream_t s)
 {
   if (int rc = scrambling_launch(ctx, ues_dev, n, max_words, seq_offsets_dev, seq_dev, s)) {
     return rc;
   }
-  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_off_dev, grids, est, port_results, seq_offsets_dev,
+  return demod_only_launch(ctx, ues_dev, n, total_tiles, tile_map_dev, grids, est, port_results, seq_offsets_dev,
                            seq_dev, llrs, s);
 }
 
-// Prefix sums of the UEs' demodulation tiles (kDemodTile subcarriers each); returns the total.
-uint32_t demod_tile_offsets(const pg_pusch_ue* ues, int n, uint32_t* off)
+// The batch's demodulation tiles (kDemodTile subcarriers each), UE by UE; returns their number.
+uint32_t demod_tile_map(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& map)
 {
   uint32_t t = 0;
   for (int i = 0; i < n; ++i) {
-    off[i] = t;
-    t += (12u * ues[i].nof_rb + kDemodTile - 1) / kDemodTile;
+    const uint32_t k = (12u * ues[i].nof_rb + kDemodTile - 1) / kDemodTile;
+    for (uint32_t j = 0; j < k; ++j) {
+      map.push_back((uint32_t)i | (j << 16));
+    }
+    t += k;
   }
-  off[n] = t;
   return t;
 }
 

@@ -417,6 +417,20 @@ __global__ void __launch_bounds__(kEstThreads) pusch_estimate_kernel(const pg_pu
 // pusch_estimate_kernel, so the frequency responses are identical. The last CTA of each (UE, port)
 // to finish (a per-port arrival counter, reset by that CTA for the next launch) adds the port's
 // partial sums in chunk order (deterministic) and forms the scalars.
+// c_init of the DM-RS sequence of OFDM symbol `sym` (TS 38.211 Section 6.4.1.1.1.1).
+__device__ __host__ __forceinline__ uint32_t dmrs_c_init(const pg_pusch_ue& ue, int sym)
+{
+  return (uint32_t)(((14ull * ue.slot + sym + 1) * (2ull * ue.n_id + 1) * (1ull << 17) + (2ull * ue.n_id + ue.n_scid)) %
+                    (1ull << 31));
+}
+
+// Words per DM-RS symbol of a UE's precomputed pilot bits: the allocation's 12 nof_rb sequence bits
+// plus two words, so that a 32-bit window at any bit offset below 12 nof_rb reads in bounds.
+__device__ __host__ __forceinline__ int dmrs_bit_words(int nof_rb)
+{
+  return (12 * nof_rb + 31) / 32 + 2;
+}
+
 constexpr int kChunk        = 128;
 constexpr int kHalo         = 8;  // even, >= the largest filter half-length (7)
 constexpr int kTileOff      = 16; // tile position of pilot k is k - (k0 - kTileOff)
@@ -432,9 +446,12 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
                                                                              const uint32_t* __restrict__ gold,
                                                                              uint32_t gold_words,
                                                                              int* __restrict__ arrivals,
-                                                                             pg_port_result* __restrict__ results)
+                                                                             pg_port_result* __restrict__ results,
+                                                                             const uint32_t* __restrict__ pilot_bits,
+                                                                             int nof_ues)
 {
   __shared__ uint32_t s_bits[kMaxDmrs][(2 * kChunkTile) / 32 + 2];
+  __shared__ float2   s_y[kMaxDmrs][kChunk]; // the received pilots of the chunk (LS, then noise)
   __shared__ float2   s_ls[kMaxDmrs][2][kChunkTile];
   __shared__ float2   s_sm[kMaxDmrs][2][kChunk + 1];
   __shared__ float    s_red[kChunkThreads / 32][4];
@@ -476,15 +493,26 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
     return (l == 1 && (k & 1)) ? make_float2(-p0.x, -p0.y) : p0;
   };
 
-  // Pilot bits c(2 (m0 + pb)) .. of the tile, m0 = 6 rb_start.
+  // Pilot bits c(2 (m0 + pb)) .. of the tile, m0 = 6 rb_start: from the UE's precomputed pilot
+  // bits (dmrs_bits_launch; bit b of symbol d's row = c(12 rb_start + b)) or from the Gold basis.
   const int nwords = (2 * (pe - pb) + 31) / 32;
-  for (int i = tid; i < nd * nwords; i += kChunkThreads) {
-    const int      d      = i / nwords;
-    const int      w      = i - d * nwords;
-    const uint32_t c_init = (uint32_t)(((14ull * ue.slot + dsym[d] + 1) * (2ull * ue.n_id + 1) * (1ull << 17) +
-                                        (2ull * ue.n_id + ue.n_scid)) %
-                                       (1ull << 31));
-    s_bits[d][w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 2u * pb + 32u * w);
+  if (pilot_bits != nullptr) {
+    const uint32_t* pbits = pilot_bits + work[gridDim.x + 4 * nof_ues + 1 + u];
+    const int       W     = dmrs_bit_words(nrb);
+    const int       w0    = (2 * pb) >> 5;
+    const int       sh    = (2 * pb) & 31;
+    for (int i = tid; i < nd * nwords; i += kChunkThreads) {
+      const int      d  = i / nwords;
+      const int      w  = i - d * nwords;
+      const uint32_t lo = __ldg(pbits + d * W + w0 + w), hi = __ldg(pbits + d * W + w0 + w + 1);
+      s_bits[d][w]      = sh ? __funnelshift_r(lo, hi, sh) : lo;
+    }
+  } else {
+    for (int i = tid; i < nd * nwords; i += kChunkThreads) {
+      const int      d      = i / nwords;
+      const int      w      = i - d * nwords;
+      s_bits[d][w] = pg::gold_word(gold, gold_words, dmrs_c_init(ue, dsym[d]), 12u * ue.rb_start + 2u * pb + 32u * w);
+    }
   }
   __syncthreads();
 
@@ -500,6 +528,8 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
     if (k >= k0 && k < k1) {
       epre += y0.x * y0.x + y0.y * y0.y;
       epre += y1.x * y1.x + y1.y * y1.y;
+      s_y[d][k - k0]     = y0;
+      s_y[d][k + 1 - k0] = y1;
     }
     for (int l = 0; l < nl; ++l) {
       float2 v0 = cmulconjf(y0, pilot(d, l, k)), v1 = cmulconjf(y1, pilot(d, l, k + 1));
@@ -593,7 +623,7 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
       pred.x += q.x;
       pred.y += q.y;
     }
-    const float2 y = rxp(d, k);
+    const float2 y = s_y[d][k - k0];
     const float2 e = make_float2(pred.x - y.x, pred.y - y.y);
     noise += e.x * e.x + e.y * e.y;
   }
@@ -612,6 +642,9 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
     }
   }
   __syncthreads();
+  __shared__ int s_last;
+  const int       pi    = 4 * u + port;
+  const uint32_t* first = work + gridDim.x; // the work list (one item per CTA), then each port's first item
   if (tid == 0) {
     float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int w = 0; w < kChunkThreads / 32; ++w) {
@@ -622,20 +655,32 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
     }
     partials[blockIdx.x] = t;
     __threadfence();
-    const int       pi    = 4 * u + port;
-    const uint32_t* first = work + gridDim.x; // the work list (one item per CTA), then each port's first item
-    const int       nch   = (int)(first[pi + 1] - first[pi]);
-    if (atomicAdd(&arrivals[pi], 1) == nch - 1) {
-      // Last chunk of this port: every other chunk's partials are visible (fence before arrival).
-      float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
-      for (uint32_t w = first[pi]; w < first[pi + 1]; ++w) {
-        const float4 p = __ldcg(partials + w);
-        s.x += p.x;
-        s.y += p.y;
-        s.z += p.z;
-        s.w += p.w;
-      }
-      arrivals[pi]     = 0;
+    const int nch = (int)(first[pi + 1] - first[pi]);
+    s_last        = atomicAdd(&arrivals[pi], 1) == nch - 1;
+  }
+  __syncthreads();
+  if (s_last && tid < 32) {
+    // Last chunk of this port: every other chunk's partials are visible (fence before arrival).
+    // The first warp loads them at once (lane i takes chunks i, i + 32, ...) and adds them in a
+    // fixed tree, so the port's scalars do not depend on which chunk arrived last.
+    __threadfence();
+    float4 s = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t w = first[pi] + tid; w < first[pi + 1]; w += 32) {
+      const float4 p = __ldcg(partials + w);
+      s.x += p.x;
+      s.y += p.y;
+      s.z += p.z;
+      s.w += p.w;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+      s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+      s.z += __shfl_xor_sync(0xffffffffu, s.z, o);
+      s.w += __shfl_xor_sync(0xffffffffu, s.w, o);
+    }
+    if (tid == 0) {
+      arrivals[pi]      = 0;
       const float n_pil = (float)(npil * nd);
       pg_port_result pr;
       pr.rsrp[0]       = s.x * beta * beta / n_pil;
@@ -647,6 +692,26 @@ __global__ void __launch_bounds__(kChunkThreads) pusch_estimate_chunk_kernel(con
       pr.noise_var     = nvar;
       pr.snr           = pg::is_normal(nvar) ? (ravg * (float)nl / beta / beta) / nvar : 0.f;
       results[pi]      = pr;
+    }
+  }
+}
+
+// Pilot bits of every UE of a plan, computed once: row d (DM-RS symbol d of the allocation) word w =
+// c(12 rb_start + 32 w) .. c(12 rb_start + 32 w + 31), rows of dmrs_bit_words(nof_rb) words from
+// off[u].
+__global__ void dmrs_bits_kernel(const pg_pusch_ue* __restrict__ ues, const uint32_t* __restrict__ off,
+                                 uint32_t* __restrict__ bits, const uint32_t* __restrict__ gold, uint32_t gold_words)
+{
+  const pg_pusch_ue ue = ues[blockIdx.y];
+  const int         W  = dmrs_bit_words(ue.nof_rb);
+  int               d  = 0;
+  for (int s = ue.first_symbol; s < ue.first_symbol + ue.nof_symbols && d < kMaxDmrs; ++s) {
+    if ((ue.dmrs_symbol_mask >> s) & 1) {
+      const uint32_t c_init = dmrs_c_init(ue, s);
+      for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < W; w += gridDim.x * blockDim.x) {
+        bits[off[blockIdx.y] + d * W + w] = pg::gold_word(gold, gold_words, c_init, 12u * ue.rb_start + 32u * w);
+      }
+      ++d;
     }
   }
 }
@@ -843,6 +908,10 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
   if (n < 0 || (n > 0 && ues == nullptr)) {
     return set_error(ctx, PG_ERR_INVALID, "invalid UE list");
   }
+  if (n > kDemodMaxUes) {
+    // The estimator's and demodulator's work lists carry the UE index in 16 bits.
+    return set_error(ctx, PG_ERR_INVALID, "more than 65535 UEs in one batch");
+  }
   for (int i = 0; i < n; ++i) {
     const pg_pusch_ue& u = ues[i];
     int                nd = 0;
@@ -862,7 +931,7 @@ int validate_ues(pg_context* ctx, const pg_pusch_ue* ues, int n)
   return PG_OK;
 }
 
-int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob)
+int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob, uint32_t* pilot_words)
 {
   std::vector<uint32_t> first((size_t)4 * n + 1);
   blob.clear();
@@ -880,19 +949,38 @@ int est_work_build(const pg_pusch_ue* ues, int n, std::vector<uint32_t>& blob)
   first[(size_t)4 * n] = (uint32_t)blob.size();
   const int nwork      = (int)blob.size();
   blob.insert(blob.end(), first.begin(), first.end());
+  uint32_t words = 0;
+  for (int u = 0; u < n; ++u) {
+    blob.push_back(words);
+    words += (uint32_t)(kMaxDmrs * dmrs_bit_words(ues[u].nof_rb));
+  }
+  if (pilot_words != nullptr) {
+    *pilot_words = words;
+  }
   return nwork;
+}
+
+int dmrs_bits_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
+                     uint32_t* bits_dev, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  dmrs_bits_kernel<<<dim3(1, n), 128, 0, s>>>(ues_dev, work_dev + nwork + 4 * (size_t)n + 1, bits_dev, ctx->dev.gold,
+                                              kGoldWords);
+  return check_cuda(ctx, cudaGetLastError(), "dmrs_bits_kernel launch");
 }
 
 int estimate_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, const uint32_t* work_dev, int nwork,
                     void* partials, int* arrivals, const uint32_t* grids, float* est, float* ls,
-                    pg_port_result* results, cudaStream_t s)
+                    pg_port_result* results, cudaStream_t s, const uint32_t* pilot_bits)
 {
   if (n == 0 || nwork == 0) {
     return PG_OK;
   }
   pusch_estimate_chunk_kernel<<<nwork, kChunkThreads, 0, s>>>(
       ues_dev, work_dev, grids, reinterpret_cast<float2*>(est), reinterpret_cast<float2*>(ls),
-      static_cast<float4*>(partials), ctx->dev.gold, kGoldWords, arrivals, results);
+      static_cast<float4*>(partials), ctx->dev.gold, kGoldWords, arrivals, results, pilot_bits, n);
   return check_cuda(ctx, cudaGetLastError(), "pusch_estimate_chunk_kernel launch");
 }
 

@@ -29,8 +29,9 @@ struct pg_pusch_plan {
   std::vector<pg_pusch_ue> ues;
   std::vector<pg_rm_cb>    rm;                 // rate-dematch descriptors (host copy, for HARQ updates)
   std::vector<int>         tb_first, tb_ncb;   // codeblocks of each UE
-  std::vector<rm_direct>   direct;             // host copies of d_direct / d_fill (rebuilt by set_harq)
-  std::vector<uint8_t>     fill;
+  std::vector<rm_direct>   direct;             // host copies of d_direct / d_placed (rebuilt by set_harq)
+  std::vector<uint8_t>     placed;
+  std::vector<uint32_t>    unplaced;           // the other codeblocks: the rate-dematch launch's list
   size_t                   rm_total = 0;       // bytes of dematched codeblocks (the soft buffers)
   // Device: descriptors, then workspace.
   void*           dev      = nullptr;
@@ -46,7 +47,14 @@ struct pg_pusch_plan {
   uint8_t*        d_uci_valid = nullptr;
   std::vector<int> uci_msg_ue, uci_msg_kind; // per message: UE and 0 HARQ-ACK / 1 CSI Part 1
   rm_direct*      d_direct   = nullptr; // per UE: fused rate-dematch placement of the demodulator
-  uint8_t*        d_fill     = nullptr; // per codeblock: 1 when the demodulator placed its LLRs
+  uint8_t*        d_placed   = nullptr; // per codeblock: 1 when the demodulator places its LLRs
+  uint32_t*       d_unplaced = nullptr; // capacity nof_cbs
+  uint32_t*       d_pilot_bits = nullptr; // DM-RS sequence bits of every UE (dmrs_bits_launch)
+  // Side branch of every execution: the in-place codeblocks' circular buffers are prefilled on
+  // `aux` (forked from and joined back into the execution's stream) beside the channel estimation.
+  cudaStream_t    aux        = nullptr;
+  cudaEvent_t     ev_fork    = nullptr;
+  cudaEvent_t     ev_join    = nullptr;
   uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
   void*           d_est_part = nullptr; // its partial sums
   int*            d_est_arr  = nullptr; // per-(UE, port) arrival counters, zero between executions
@@ -56,7 +64,7 @@ struct pg_pusch_plan {
   pg_tb_desc*     d_tb     = nullptr;
   uint32_t*       d_cb_off = nullptr;
   uint32_t*       d_seq_off = nullptr;
-  uint32_t*       d_tile_off = nullptr;
+  uint32_t*       d_tile_map = nullptr;
   uint32_t*       d_seq    = nullptr;
   float*          d_est    = nullptr;
   pg_port_result* d_pr     = nullptr;
@@ -147,13 +155,13 @@ size_t al(size_t x)
 // Fused demodulation and rate dematching: per UE the placement of its codeword in the codeblock
 // buffers when every codeblock holds new data without repetition (E <= N_cb - F), as a
 // consecutive run of E values with the smaller ones first and buffers a constant stride apart;
-// other UEs keep the codeword buffer and the rate-dematch kernel. fill[c] = 1 for the codeblocks
-// of the enabled UEs (their dematch launch only writes the positions no LLR reaches).
+// other UEs keep the codeword buffer and the rate-dematch kernel. placed[c] = 1 for the codeblocks
+// of the enabled UEs (prefilled with rm_prefill_launch, left alone by the rate-dematch kernel).
 void build_direct(const std::vector<pg_pusch_ue>& ues, const std::vector<pg_rm_cb>& rm, const std::vector<int>& first,
-                  const std::vector<int>& ncb, std::vector<rm_direct>& direct, std::vector<uint8_t>& fill)
+                  const std::vector<int>& ncb, std::vector<rm_direct>& direct, std::vector<uint8_t>& placed)
 {
   direct.assign(ues.size(), rm_direct{});
-  fill.assign(rm.size(), 0);
+  placed.assign(rm.size(), 0);
   for (size_t u = 0; u < ues.size(); ++u) {
     const int c0 = first[u], n = ncb[u];
     if (n <= 0) {
@@ -206,18 +214,43 @@ void build_direct(const std::vector<pg_pusch_ue>& ues, const std::vector<pg_rm_c
     d.F          = (uint32_t)F;
     d.enabled    = 1;
     for (int k = 0; k < n; ++k) {
-      fill[c0 + k] = 1;
+      placed[c0 + k] = 1;
     }
   }
+}
+
+// The codeblocks that the demodulator does not store in place, in codeblock order.
+std::vector<uint32_t> unplaced_list(const std::vector<uint8_t>& placed)
+{
+  std::vector<uint32_t> list;
+  for (size_t c = 0; c < placed.size(); ++c) {
+    if (placed[c] == 0) {
+      list.push_back((uint32_t)c);
+    }
+  }
+  return list;
 }
 
 int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_result* results,
             pg_port_result* port_results, cudaStream_t s)
 {
   pg_context* ctx = p->ctx;
-  int         rc  = estimate_launch(ctx, p->d_ues, p->nof_ues, p->d_est_work, p->est_nwork, p->d_est_part,
-                                    p->d_est_arr, grids, p->d_est, p->le_net != nullptr ? p->d_ls : nullptr,
-                                    port_results, s);
+  // Fork: the in-place codeblocks' prefill depends on nothing of this execution (the previous
+  // execution on this stream, whose decoder read the buffers, precedes the fork).
+  int rc = check_cuda(ctx, cudaEventRecord(p->ev_fork, s), "cudaEventRecord(fork)");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamWaitEvent(p->aux, p->ev_fork, 0), "cudaStreamWaitEvent(fork)");
+  }
+  if (rc == PG_OK) {
+    rc = rm_prefill_launch(ctx, p->d_rm, p->nof_cbs, p->d_placed, p->d_rm_out, p->aux);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaEventRecord(p->ev_join, p->aux), "cudaEventRecord(join)");
+  }
+  if (rc == PG_OK) {
+    rc = estimate_launch(ctx, p->d_ues, p->nof_ues, p->d_est_work, p->est_nwork, p->d_est_part, p->d_est_arr, grids,
+                         p->d_est, p->le_net != nullptr ? p->d_ls : nullptr, port_results, s, p->d_pilot_bits);
+  }
   if (rc == PG_OK && p->le_net != nullptr) {
     const unsigned int flags = timing_record_flags(ctx, s);
     if (ctx->timed) {
@@ -231,7 +264,10 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     }
   }
   if (rc == PG_OK) {
-    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_tiles, p->d_tile_off, grids, p->d_est, port_results,
+    rc = check_cuda(ctx, cudaStreamWaitEvent(s, p->ev_join, 0), "cudaStreamWaitEvent(join)");
+  }
+  if (rc == PG_OK) {
+    rc = demod_only_launch(ctx, p->d_ues, p->nof_ues, p->total_tiles, p->d_tile_map, grids, p->d_est, port_results,
                            p->d_seq_off, p->d_seq, p->d_llr, s, p->tuning.demod_block, p->tuning.demod_res_per_thread,
                            p->le_net != nullptr ? p->d_basis : nullptr,
                            p->le_net != nullptr ? p->d_basis_use : nullptr, p->d_direct, p->d_rm_out);
@@ -244,9 +280,9 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
       rc = uci_detect_launch(ctx, p->d_uci_items, p->uci_nmsg, p->d_uci_llr, p->d_uci_bits, p->d_uci_valid, s);
     }
   }
-  if (rc == PG_OK) {
-    rc = rate_dematch_launch(ctx, p->d_rm, p->nof_cbs, p->d_llr, p->d_rm_out, s, p->tuning.rm_ctas_per_cb,
-                             p->d_fill);
+  if (rc == PG_OK && !p->unplaced.empty()) {
+    rc = rate_dematch_launch(ctx, p->d_rm, (int)p->unplaced.size(), p->d_llr, p->d_rm_out, s,
+                             p->tuning.rm_ctas_per_cb, p->d_unplaced);
   }
   if (rc == PG_OK && p->nof_cbs > 1) {
     // Hardest first: the decoders take the codeblocks in ascending order of input confidence.
@@ -283,7 +319,10 @@ void release(pg_pusch_plan* p)
   if (p->copy_stream) {
     cudaStreamDestroy(p->copy_stream);
   }
-  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1]}) {
+  if (p->aux) {
+    cudaStreamDestroy(p->aux);
+  }
+  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1], p->ev_fork, p->ev_join}) {
     if (e) {
       cudaEventDestroy(e);
     }
@@ -441,8 +480,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   }
   p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
   p->est_total = est_total;
-  std::vector<uint32_t> tile_off(nof_ues + 1);
-  p->total_tiles = demod_tile_offsets(p->ues.data(), nof_ues, tile_off.data());
+  std::vector<uint32_t> tile_map;
+  p->total_tiles = demod_tile_map(p->ues.data(), nof_ues, tile_map);
   sch_work w;
   if (int rc = build_sch_work(ctx, tbs.data(), nof_ues, p->nof_llrs, p->tb_bytes, w)) {
     release(p);
@@ -480,18 +519,21 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_seqoff = o_order + al(order.size() * 4);
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
   std::vector<uint32_t> est_work;
-  p->est_nwork          = est_work_build(p->ues.data(), nof_ues, est_work);
+  uint32_t              pilot_words = 0;
+  p->est_nwork          = est_work_build(p->ues.data(), nof_ues, est_work, &pilot_words);
   std::vector<rm_direct> direct;
-  std::vector<uint8_t>   fill;
-  build_direct(p->ues, w.rm, w.tb_first, w.tb_ncb, direct, fill);
-  p->direct = direct;
-  p->fill   = fill;
-  const size_t o_ework  = o_reoff + al(tile_off.size() * 4);
+  std::vector<uint8_t>   placed;
+  build_direct(p->ues, w.rm, w.tb_first, w.tb_ncb, direct, placed);
+  p->direct     = direct;
+  p->placed     = placed;
+  p->unplaced   = unplaced_list(placed);
+  const size_t o_ework  = o_reoff + al(tile_map.size() * 4);
   const size_t o_ublob  = o_ework + al(est_work.size() * 4);
   const size_t o_uitems = o_ublob + al(uci_blob.size());
   const size_t o_direct = o_uitems + al(uci_items.size());
   const size_t o_fill   = o_direct + al(direct.size() * sizeof(rm_direct));
-  const size_t desc_end = o_fill + al(fill.size());
+  const size_t o_unpl   = o_fill + al(placed.size());
+  const size_t desc_end = o_unpl + al((size_t)p->nof_cbs * 4);
   const size_t o_seq    = desc_end;
   const size_t o_est    = o_seq + al(seq_total * 4);
   const size_t o_pr     = o_est + al(est_total * 8);
@@ -511,7 +553,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_ullr   = o_earr + al((size_t)nof_ues * 16);
   const size_t o_ubits  = o_ullr + al(uci_llr_total);
   const size_t o_uvalid = o_ubits + al((size_t)nof_ues * sizeof(pg_pusch_uci_result));
-  p->dev_bytes          = o_uvalid + al((size_t)std::max(1, p->uci_nmsg));
+  const size_t o_pbits  = o_uvalid + al((size_t)std::max(1, p->uci_nmsg));
+  p->dev_bytes          = o_pbits + al((size_t)pilot_words * 4);
 
   const size_t h_res  = 0;
   const size_t h_pr   = h_res + al((size_t)nof_ues * sizeof(pg_sch_result));
@@ -536,7 +579,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   p->d_tb      = reinterpret_cast<pg_tb_desc*>(b + o_tb);
   p->d_cb_off  = reinterpret_cast<uint32_t*>(b + o_cb_off);
   p->d_seq_off = reinterpret_cast<uint32_t*>(b + o_seqoff);
-  p->d_tile_off = reinterpret_cast<uint32_t*>(b + o_reoff);
+  p->d_tile_map = reinterpret_cast<uint32_t*>(b + o_reoff);
   p->d_seq     = reinterpret_cast<uint32_t*>(b + o_seq);
   p->d_est     = reinterpret_cast<float*>(b + o_est);
   p->d_pr      = reinterpret_cast<pg_port_result*>(b + o_pr);
@@ -554,7 +597,9 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   p->d_res     = reinterpret_cast<pg_sch_result*>(b + o_res);
   p->d_est_work = reinterpret_cast<uint32_t*>(b + o_ework);
   p->d_direct   = reinterpret_cast<rm_direct*>(b + o_direct);
-  p->d_fill     = b + o_fill;
+  p->d_placed   = b + o_fill;
+  p->d_unplaced = reinterpret_cast<uint32_t*>(b + o_unpl);
+  p->d_pilot_bits = reinterpret_cast<uint32_t*>(b + o_pbits);
   p->d_est_part = b + o_epart;
   p->d_est_arr  = reinterpret_cast<int*>(b + o_earr);
   p->d_uci_blob  = b + o_ublob;
@@ -573,16 +618,25 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
   std::memcpy(h + o_order, order.data(), order.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
-  std::memcpy(h + o_reoff, tile_off.data(), tile_off.size() * 4);
+  std::memcpy(h + o_reoff, tile_map.data(), tile_map.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
   if (!uci_blob.empty()) {
     std::memcpy(h + o_ublob, uci_blob.data(), uci_blob.size());
     std::memcpy(h + o_uitems, uci_items.data(), uci_items.size());
   }
   std::memcpy(h + o_direct, direct.data(), direct.size() * sizeof(rm_direct));
-  std::memcpy(h + o_fill, fill.data(), fill.size());
+  std::memcpy(h + o_fill, placed.data(), placed.size());
+  std::memcpy(h + o_unpl, p->unplaced.data(), p->unplaced.size() * 4);
   cudaStream_t s = ctx->stream;
   rc = check_cuda(ctx, cudaMemcpyAsync(p->dev, h, desc_end, cudaMemcpyHostToDevice, s), "H2D plan descriptors");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking), "cudaStreamCreate(aux)");
+  }
+  for (cudaEvent_t* e : {&p->ev_fork, &p->ev_join}) {
+    if (rc == PG_OK) {
+      rc = check_cuda(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate(fork/join)");
+    }
+  }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaMemsetAsync(b + o_seq, 0, al(seq_total * 4), s), "cudaMemsetAsync(sequences)");
   }
@@ -595,6 +649,9 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   }
   if (rc == PG_OK) {
     rc = scrambling_launch(ctx, p->d_ues, nof_ues, max_words, p->d_seq_off, p->d_seq, s);
+  }
+  if (rc == PG_OK) {
+    rc = dmrs_bits_launch(ctx, p->d_ues, nof_ues, p->d_est_work, p->est_nwork, p->d_pilot_bits, s);
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize(plan)");
@@ -768,8 +825,15 @@ int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const u
     }
   }
   // Soft combining (new_data == 0) takes a UE off the fused demodulation and rate dematching.
-  build_direct(plan->ues, plan->rm, plan->tb_first, plan->tb_ncb, plan->direct, plan->fill);
-  // The kernels read the descriptors when they run, so a captured graph stays valid.
+  build_direct(plan->ues, plan->rm, plan->tb_first, plan->tb_ncb, plan->direct, plan->placed);
+  std::vector<uint32_t> unplaced = unplaced_list(plan->placed);
+  if (unplaced.size() != plan->unplaced.size() && plan->exec != nullptr) {
+    // The rate-dematch launch changes shape: the next execution captures a new graph.
+    cudaGraphExecDestroy(plan->exec);
+    plan->exec = nullptr;
+  }
+  plan->unplaced = unplaced;
+  // Otherwise the kernels read the descriptors when they run, so a captured graph stays valid.
   cudaStream_t s  = ctx->stream;
   int          rc = check_cuda(ctx,
                                cudaMemcpyAsync(plan->d_rm, plan->rm.data(), plan->rm.size() * sizeof(pg_rm_cb),
@@ -782,8 +846,15 @@ int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const u
                     "H2D HARQ demodulator placement");
   }
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_fill, plan->fill.data(), plan->fill.size(), cudaMemcpyHostToDevice, s),
-                    "H2D HARQ fill flags");
+    rc = check_cuda(ctx,
+                    cudaMemcpyAsync(plan->d_placed, plan->placed.data(), plan->placed.size(), cudaMemcpyHostToDevice, s),
+                    "H2D HARQ in-place flags");
+  }
+  if (rc == PG_OK && !plan->unplaced.empty()) {
+    rc = check_cuda(ctx,
+                    cudaMemcpyAsync(plan->d_unplaced, plan->unplaced.data(), plan->unplaced.size() * 4,
+                                    cudaMemcpyHostToDevice, s),
+                    "H2D HARQ rate-dematch list");
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx,

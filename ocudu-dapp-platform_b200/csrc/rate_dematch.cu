@@ -43,10 +43,10 @@ constexpr int kRmTileRows = 256;
 __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb* __restrict__ cbs,
                                                                   const int8_t* __restrict__ in_all,
                                                                   int8_t* __restrict__ out_all,
-                                                                  const uint8_t* __restrict__ fill_only)
+                                                                  const uint32_t* __restrict__ list)
 {
   __shared__ int8_t tile[kRmTileRows * 8];
-  const pg_rm_cb d   = cbs[blockIdx.x];
+  const pg_rm_cb d   = cbs[list != nullptr ? list[blockIdx.x] : blockIdx.x];
   const int      bg  = d.base_graph;
   const int      Z   = d.lifting_size;
   const int      Kb  = bg == 1 ? 22 : 10;
@@ -67,88 +67,6 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   int8_t*        out = out_all + d.out_offset;
   const bool     nd  = d.new_data != 0;
 
-  if (E <= V && fill_only != nullptr && fill_only[blockIdx.x] != 0) {
-    // One CTA per codeblock suffices for this fill (at most N / 16 chunks); the others leave.
-    if (blockIdx.y != 0) {
-      return;
-    }
-    // The demodulator placed this codeblock's LLRs itself (new data, E <= V): they occupy the valid
-    // indices [v0, v0 + E) mod V, up to four position intervals past the fillers. Every other
-    // position is a filler (+127) or unreached / beyond N_cb (0). The buffer is written in 16-byte
-    // chunks: chunks of placed LLRs only are skipped, chunks without any are stored whole, and the
-    // few chunks that mix them are merged byte by byte.
-    int       ka[4], kb[4], nk = 0;
-    const int e_end = v0 + E;
-    auto add_v = [&](int a, int b) {
-      const int b1 = min(b, inf);
-      if (a < b1) {
-        ka[nk] = a;
-        kb[nk] = b1;
-        ++nk;
-      }
-      const int a2 = max(a, inf);
-      if (a2 < b) {
-        ka[nk] = a2 + F;
-        kb[nk] = b + F;
-        ++nk;
-      }
-    };
-    if (e_end <= V) {
-      add_v(v0, e_end);
-    } else {
-      add_v(v0, V);
-      add_v(0, e_end - V);
-    }
-    auto placed_at = [&](int p) {
-      bool k = false;
-      for (int i = 0; i < nk; ++i) {
-        k |= p >= ka[i] && p < kb[i];
-      }
-      return k;
-    };
-    auto fill_value = [&](int p) { return (int8_t)((p >= inf && p < sys) ? 127 : 0); };
-    const int head  = (int)((16u - (unsigned)(reinterpret_cast<uintptr_t>(out) & 15u)) & 15u);
-    const int first = min(head, N);
-    const int nch   = (N - first) / 16;
-    const int tail  = first + 16 * nch;
-    for (int p = threadIdx.x; p < first; p += kRmThreads) {
-      if (!placed_at(p)) {
-        out[p] = fill_value(p);
-      }
-    }
-    for (int p = tail + threadIdx.x; p < N; p += kRmThreads) {
-      if (!placed_at(p)) {
-        out[p] = fill_value(p);
-      }
-    }
-    for (int q = threadIdx.x; q < nch; q += kRmThreads) {
-      const int c = first + 16 * q;
-      int       kept = 0;
-      for (int i = 0; i < nk; ++i) {
-        kept += max(0, min(c + 16, kb[i]) - max(c, ka[i]));
-      }
-      if (kept == 16) {
-        continue;
-      }
-      const int fil = max(0, min(c + 16, sys) - max(c, inf));
-      uint4*    dst = reinterpret_cast<uint4*>(out + c);
-      if (kept == 0 && fil == 0) {
-        *dst = make_uint4(0u, 0u, 0u, 0u);
-      } else if (kept == 0 && fil == 16) {
-        *dst = make_uint4(0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu);
-      } else {
-        uint4   w = *dst;
-        int8_t* b = reinterpret_cast<int8_t*>(&w);
-        for (int i = 0; i < 16; ++i) {
-          if (!placed_at(c + i)) {
-            b[i] = fill_value(c + i);
-          }
-        }
-        *dst = w;
-      }
-    }
-    return;
-  }
   if (E <= V) {
     // No repetition: each buffer position receives at most one input. The input, row i holding
     // the Qm LLRs of de-interleaver column i, is read a tile of rows at a time (coalesced) and
@@ -235,6 +153,52 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
   }
 }
 
+// The circular buffers of the codeblocks whose LLRs the demodulator stores in place (placed[c]
+// = 1: new data, E <= V), before it does: +127 at the filler positions [inf, (Kb - 2) Z) and 0
+// everywhere else, which is what rate dematching leaves at every position that no LLR reaches.
+// 16-byte stores; the first and last bytes of a buffer that does not start or end on a 16-byte
+// boundary are stored one by one.
+__global__ void __launch_bounds__(kRmThreads) rm_prefill_kernel(const pg_rm_cb* __restrict__ cbs,
+                                                                const uint8_t* __restrict__ placed,
+                                                                int8_t* __restrict__ out_all)
+{
+  if (placed[blockIdx.x] == 0) {
+    return;
+  }
+  const pg_rm_cb d    = cbs[blockIdx.x];
+  const int      Z    = d.lifting_size;
+  const int      N    = (d.base_graph == 1 ? 66 : 50) * Z;
+  const int      sys  = ((d.base_graph == 1 ? 22 : 10) - 2) * Z;
+  const int      inf  = sys - (int)d.nof_filler_bits;
+  int8_t*        out  = out_all + d.out_offset;
+  const int      head = min(N, (int)((16u - (unsigned)(reinterpret_cast<uintptr_t>(out) & 15u)) & 15u));
+  const int      nch  = (N - head) / 16;
+  const int      tail = head + 16 * nch;
+  const int      tid  = blockIdx.y * kRmThreads + threadIdx.x;
+  const int      nthr = gridDim.y * kRmThreads;
+  auto value = [&](int p) { return (int8_t)((p >= inf && p < sys) ? 127 : 0); };
+  if (tid < head) {
+    out[tid] = value(tid);
+  }
+  if (tail + tid < N) {
+    out[tail + tid] = value(tail + tid);
+  }
+  for (int q = tid; q < nch; q += nthr) {
+    const int c   = head + 16 * q;
+    const int fil = max(0, min(c + 16, sys) - max(c, inf));
+    uint4     w   = make_uint4(0u, 0u, 0u, 0u);
+    if (fil == 16) {
+      w = make_uint4(0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu, 0x7f7f7f7fu);
+    } else if (fil > 0) {
+      int8_t* b = reinterpret_cast<int8_t*>(&w);
+      for (int i = 0; i < 16; ++i) {
+        b[i] = value(c + i);
+      }
+    }
+    *reinterpret_cast<uint4*>(out + c) = w;
+  }
+}
+
 } // namespace
 
 namespace pg {
@@ -287,15 +251,26 @@ int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const
 }
 
 int rate_dematch_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const int8_t* in, int8_t* out,
-                        cudaStream_t stream, int ctas_per_cb, const uint8_t* fill_only)
+                        cudaStream_t stream, int ctas_per_cb, const uint32_t* list)
 {
   if (n == 0) {
     return PG_OK;
   }
   // Each codeblock's N <= 25,344 output positions spread over ctas_per_cb CTAs.
   ctas_per_cb = std::max(1, std::min(32, ctas_per_cb));
-  rate_dematch_kernel<<<dim3(n, ctas_per_cb), kRmThreads, 0, stream>>>(descs_dev, in, out, fill_only);
+  rate_dematch_kernel<<<dim3(n, ctas_per_cb), kRmThreads, 0, stream>>>(descs_dev, in, out, list);
   return check_cuda(ctx, cudaGetLastError(), "rate_dematch_kernel launch");
+}
+
+int rm_prefill_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const uint8_t* placed, int8_t* out,
+                      cudaStream_t stream)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  // N <= 25,344 bytes = 1,584 chunks: two CTAs of 256 threads per codeblock, about three stores each.
+  rm_prefill_kernel<<<dim3(n, 2), kRmThreads, 0, stream>>>(descs_dev, placed, out);
+  return check_cuda(ctx, cudaGetLastError(), "rm_prefill_kernel launch");
 }
 
 } // namespace pg

@@ -65,3 +65,30 @@ def test_adapters_match_reference_implementations(tmp_path):
     for iface in ("ldpc_decoder", "ldpc_rate_dematcher", "crc_calculator", "demodulation_mapper", "channel_equalizer",
                   "port_channel_estimator", "pusch_decoder", "resident_decoder"):
         assert any(line.startswith(iface) and " OK " in line for line in r.stdout.splitlines()), iface
+
+
+DAPP_CHECK = os.path.join(ROOT, "oracle", "_ref", "dapp_check")
+DAPP_MODULE = os.path.join(ROOT, "ocudu-dapp-platform_b200", "adapters", "_lib", "libpg_dapp_b200.so")
+needs_dapp = pytest.mark.skipif(not (os.path.exists(DAPP_CHECK) and os.path.exists(DAPP_MODULE)),
+                                reason="oracle/_ref/dapp_check or the dApp module not built")
+
+
+@needs_dapp
+def test_dapp_module_descriptor_passes_reference_validator():
+    """The dApp plug-in module loads through ocudu_dapp_query_v1 and the reference's own ABI
+    validator accepts its descriptor: two Class-A interfaces (channel estimator v1, receiver v1)."""
+    r = subprocess.run([DAPP_CHECK, DAPP_MODULE, "--describe"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert any(line.startswith("dapp_module") and " OK " in line for line in r.stdout.splitlines())
+
+
+@needs_dapp
+@pytest.mark.gpu
+def test_dapp_module_matches_reference_chain():
+    """The module's channel estimator and receiver, invoked with the host hooks' tensors, against the
+    reference's native port_channel_estimator / channel_equalizer / demodulation_mapper."""
+    r = subprocess.run([DAPP_CHECK, DAPP_MODULE], capture_output=True, text=True, timeout=600)
+    print(r.stdout)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for name in ("dapp_module", "dapp_channel_estimator", "dapp_receiver", "dapp_bypass", "dapp_lifecycle"):
+        assert any(line.startswith(name) and " OK " in line for line in r.stdout.splitlines()), name
