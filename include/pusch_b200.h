@@ -327,6 +327,15 @@ int pg_demodulate_soft_device(pg_context* ctx, int modulation_order, int nof_sym
 int pg_demodulate_soft_host(pg_context* ctx, int modulation_order, int nof_symbols, const float* symbols,
                             const float* noise_vars, int8_t* llrs);
 
+/* Descrambling of soft bits (TS 38.211 Section 6.3.1.1, c_init = RNTI * 2^15 + n_ID): llrs_out[i]
+ * = -llrs_in[i] where the Gold sequence bit c(i) is 1, else llrs_in[i]; in place allowed. The step
+ * the reference's PUSCH demodulator applies after soft demapping (revert_scrambling,
+ * pusch_demodulator_impl.cpp:23-33,409-414) and its offline replay tool repeats
+ * (apps/tools/pusch_replay/ocudu_pusch_replay.cpp:266-296). At most 14 * 3276 * 2 * 8 soft bits. */
+int pg_descramble_device(pg_context* ctx, uint32_t c_init, const int8_t* llrs_in, int8_t* llrs_out, size_t n,
+                         void* stream);
+int pg_descramble_host(pg_context* ctx, uint32_t c_init, const int8_t* llrs_in, int8_t* llrs_out, size_t n);
+
 /* ---------------------------------------------------------------------------------------- */
 /* PUSCH slot processing: DM-RS channel estimation, demodulation, decoding                   */
 

@@ -193,6 +193,8 @@ int build_sch_work(pg_context* ctx, const pg_sch_tb* tbs, int nof_tbs, size_t no
 // Scrambling sequences of every UE (c_init = RNTI * 2^15 + n_ID), words at seq_offsets_dev[u].
 int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,
                       const uint32_t* seq_offsets_dev, uint32_t* seq_dev, cudaStream_t s);
+// Descrambling of n soft bits with the Gold sequence of c_init (in == out allowed).
+int descramble_launch(pg_context* ctx, uint32_t c_init, const int8_t* in, int8_t* out, size_t n, cudaStream_t s);
 // Demodulation with the scrambling sequences already generated.
 int demod_only_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t total_tiles,
                       const uint32_t* tile_map_dev, const uint32_t* grids, const float* est,

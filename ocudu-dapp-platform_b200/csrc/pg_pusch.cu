@@ -45,6 +45,50 @@ void plan(const pg_pusch_ue* ues, int n, slot_layout& L, bool assign_offsets)
 
 extern "C" {
 
+int pg_descramble_device(pg_context* ctx, uint32_t c_init, const int8_t* llrs_in, int8_t* llrs_out, size_t n,
+                         void* stream)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (n > 0 && (llrs_in == nullptr || llrs_out == nullptr)) {
+    return set_error(ctx, PG_ERR_INVALID, "null soft-bit buffer");
+  }
+  return descramble_launch(ctx, c_init, llrs_in, llrs_out, n, static_cast<cudaStream_t>(stream));
+}
+
+int pg_descramble_host(pg_context* ctx, uint32_t c_init, const int8_t* llrs_in, int8_t* llrs_out, size_t n)
+{
+  if (ctx == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  if (n == 0) {
+    return PG_OK;
+  }
+  if (llrs_in == nullptr || llrs_out == nullptr) {
+    return set_error(ctx, PG_ERR_INVALID, "null soft-bit buffer");
+  }
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc == PG_OK) {
+    rc = ensure_scratch(ctx, &ctx->scratch_a, &ctx->scratch_a_cap, std::max<size_t>(n, 256), "cudaMalloc(descramble)");
+  }
+  int8_t*      d = static_cast<int8_t*>(ctx->scratch_a);
+  cudaStream_t s = ctx->stream;
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(d, llrs_in, n, cudaMemcpyHostToDevice, s), "H2D soft bits");
+  }
+  if (rc == PG_OK) {
+    rc = descramble_launch(ctx, c_init, d, d, n, s);
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpyAsync(llrs_out, d, n, cudaMemcpyDeviceToHost, s), "D2H soft bits");
+  }
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "cudaStreamSynchronize");
+  }
+  return rc;
+}
+
 int pg_pusch_demodulate_device(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, const uint32_t* grids,
                                const float* est, const pg_port_result* port_results, int8_t* llrs, void* stream)
 {

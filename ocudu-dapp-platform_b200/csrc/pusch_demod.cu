@@ -142,6 +142,22 @@ __global__ void scrambling_kernel(const pg_pusch_ue* __restrict__ ues, const uin
   }
 }
 
+// Descrambling of a soft-bit stream: thread i takes soft bits 32 i .. 32 i + 31 and Gold word i.
+__global__ void descramble_kernel(uint32_t c_init, const int8_t* __restrict__ in, int8_t* __restrict__ out, size_t n,
+                                  const uint32_t* __restrict__ gold, uint32_t gold_words)
+{
+  const size_t w = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (32 * w >= n) {
+    return;
+  }
+  const uint32_t c   = pg::gold_word(gold, gold_words, c_init, 32u * (uint32_t)w);
+  const size_t   end = n - 32 * w < 32 ? n - 32 * w : 32;
+  for (size_t b = 0; b < end; ++b) {
+    const int x        = in[32 * w + b];
+    out[32 * w + b]    = (int8_t)(((c >> b) & 1u) ? -x : x);
+  }
+}
+
 struct demap_tables {
   const float* slope;
   const float* icpt;
@@ -537,6 +553,20 @@ uint32_t ue_codeword_bits(const pg_pusch_ue& u)
     ndmrs += (u.dmrs_symbol_mask >> s) & 1;
   }
   return (uint32_t)(u.nof_symbols - ndmrs) * 12u * u.nof_rb * u.nof_layers * u.modulation_order;
+}
+
+int descramble_launch(pg_context* ctx, uint32_t c_init, const int8_t* in, int8_t* out, size_t n, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  // The Gold basis covers kGoldWords - 2 words from position 0.
+  if ((n + 31) / 32 + 2 > kGoldWords) {
+    return set_error(ctx, PG_ERR_INVALID, "soft-bit stream longer than the scrambling sequence table");
+  }
+  const size_t words = (n + 31) / 32;
+  descramble_kernel<<<(unsigned)((words + 255) / 256), 256, 0, s>>>(c_init, in, out, n, ctx->dev.gold, kGoldWords);
+  return check_cuda(ctx, cudaGetLastError(), "descramble_kernel launch");
 }
 
 int scrambling_launch(pg_context* ctx, const pg_pusch_ue* ues_dev, int n, uint32_t max_words,

@@ -170,6 +170,8 @@ SIGNATURES = {
                                         ctypes.c_float, _VP, _VP]),
     "pg_demodulate_soft_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_demodulate_soft_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
+    "pg_descramble_device": (ctypes.c_int, [_VP, ctypes.c_uint32, _VP, _VP, ctypes.c_size_t, _VP]),
+    "pg_descramble_host": (ctypes.c_int, [_VP, ctypes.c_uint32, _VP, _VP, ctypes.c_size_t]),
     "pg_pusch_est_size": (ctypes.c_size_t, [_VP]),
     "pg_pusch_estimate_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_pusch_symbol_estimates_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP]),

@@ -301,3 +301,51 @@ def scale_grid_words(words, factor):
     f = np.stack([(w & 0xFFFF) << 16, w & 0xFFFF0000], axis=-1).astype(np.uint32).view(np.float32) * np.float32(factor)
     h = (f.view(np.uint32) >> 16).astype(np.uint32)
     return (h[..., 0] | (h[..., 1] << 16)).astype(np.uint32)
+
+
+# ----------------------------------------------------------------------------------------------
+# Replay bursts (the E3 pusch.symbols recording format of the reference's ocudu-pusch-replay).
+
+def synthetic_burst(seed=0, nof_prb=52, mcs_table=2, mcs_index=10, nof_layers=1, sinr_db=20.0, rv=0,
+                    crc_ok_reported=True, nof_dmrs=2):
+    """A recorded PUSCH burst in the form the reference's replay tool reads
+    (apps/tools/pusch_replay/ocudu_pusch_replay.cpp:93-137): the grant of one UE with 14 OFDM
+    symbols and DM-RS type 1 at symbols 2 (and 11), and its equalised data symbols - the scrambled
+    UL-SCH codeword of a random TB, QAM-modulated with unit energy, plus complex white noise of
+    variance 10^(-SINR/10). Returns (replay.Burst, transmitted TB bits)."""
+    from . import mcs as mcs_tables
+    from . import prg
+    from .replay import Burst
+
+    rng = np.random.default_rng(seed)
+    dmrs = (2, 11)[:nof_dmrs]
+    qm, r = mcs_tables.mcs(mcs_table, mcs_index)
+    tbs = mcs_tables.tbs(14, 12 * len(dmrs), 0, qm, r, nof_layers, nof_prb)
+    bg = mcs_tables.base_graph(r, tbs)
+    ncs = (14 - len(dmrs)) * 12 * nof_prb * nof_layers
+    seg = codec.segment_tx(tbs, bg, qm, nof_layers, ncs)
+    tb = rng.integers(0, 2, tbs, dtype=np.uint8)
+    # TBS_LBRM of TS 38.212 Section 5.4.2.1 for a 273-PRB, 4-layer, 256QAM carrier.
+    lbrm_bits = mcs_tables.tbs(14, 12, 0, 8, 948, 4, 273)
+    c = seg["nof_cbs"]
+    nref = min(lbrm_bits * 3 // (2 * c), 25344)
+    rnti, n_id = int(rng.integers(1, 0xFFEF)), int(rng.integers(0, 1024))
+    cw = codec.ulsch_encode(tb, bg, qm, nof_layers, ncs, seg, rv=rv, nref=nref)
+    cw = cw ^ prg.scrambling(rnti, n_id, cw.size)
+    x = codec.modulate(cw, qm)
+    nv = 10 ** (-sinr_db / 10)
+    y = x + np.sqrt(nv / 2) * (rng.standard_normal(x.size) + 1j * rng.standard_normal(x.size))
+    mask = 0
+    for s in dmrs:
+        mask |= 1 << s
+    grant = {"tbs_bytes": tbs // 8, "tbs_lbrm_bytes": lbrm_bits // 8, "ldpc_base_graph": bg, "rv": rv,
+             "harq_id": 0, "n_id": n_id, "mcs_index": mcs_index, "mcs_table": mcs_table,
+             "nof_harq_ack_bits": 0, "nof_csi_part1_bits": 0, "alpha_scaling": 1.0, "beta_offset_harq_ack": 20.0,
+             "beta_offset_csi_part1": 6.25, "beta_offset_csi_part2": 6.25, "start_symbol": 0, "nof_symbols": 14,
+             "dmrs_type": 1, "dmrs_symbol_mask": mask, "nof_cdm_groups_without_data": 2, "dc_position": None,
+             "prb_mask": "ff" * ((nof_prb + 7) // 8)}
+    burst = Burst(rnti=rnti, numerology=1, sfn=int(rng.integers(0, 1024)), slot=int(rng.integers(0, 20)),
+                  modulation_bits=qm, sinr_db=float(sinr_db), nof_prb=nof_prb, nof_layers=nof_layers,
+                  crc_known=crc_ok_reported is not None, crc_ok_reported=bool(crc_ok_reported),
+                  symbols_truncated=False, grant=grant, symbols=y.astype(np.complex64))
+    return burst, tb
