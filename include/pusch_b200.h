@@ -720,6 +720,47 @@ typedef struct pg_ulsch_demux_config {
   uint8_t  nof_csi_part1_bits;     /* O^CSI-1, 0..11 */
 } pg_ulsch_demux_config;
 
+/* The rate-matching sizes of UCI multiplexed on PUSCH (TS 38.212 Sections 6.3.2.4.1.1-3 and
+ * 6.3.2.4.2.1-3), replacing get_ulsch_information (include/ocudu/ran/pusch/ulsch_info.h:144,
+ * lib/ran/pusch/ulsch_info.cpp:137-342) for DM-RS type 1: from the grant, the encoded soft-bit counts
+ * of the UL-SCH, HARQ-ACK (and the reserved HARQ-ACK bits), CSI Part 1 and CSI Part 2 - the numbers
+ * a pg_ulsch_demux_config or pg_pusch_uci takes. Host computation, no GPU. */
+typedef struct pg_ulsch_info_config {
+  uint32_t tbs_bits;                    /* 0: no UL-SCH on this PUSCH */
+  float    target_code_rate;            /* R in (0, 1) (MCS rate / 1024); used without UL-SCH */
+  float    alpha_scaling;               /* alpha (0.5, 0.65, 0.8 or 1) */
+  float    beta_offset_harq_ack;        /* beta_offset values of TS 38.213 Table 9.3-1/2 */
+  float    beta_offset_csi_part1;
+  float    beta_offset_csi_part2;
+  uint16_t nof_harq_ack_bits;           /* O^HARQ-ACK */
+  uint16_t nof_csi_part1_bits;          /* O^CSI-1 */
+  uint16_t nof_csi_part2_bits;          /* O^CSI-2 */
+  uint16_t nof_rb;
+  uint16_t dmrs_symbol_mask;            /* bit s: slot symbol s carries DM-RS */
+  uint8_t  base_graph;                  /* LDPC base graph of the UL-SCH (1 or 2) */
+  uint8_t  modulation_order;            /* 1, 2, 4, 6, 8 */
+  uint8_t  nof_layers;                  /* 1..4 */
+  uint8_t  start_symbol;
+  uint8_t  nof_symbols;
+  uint8_t  nof_cdm_groups_without_data; /* 1 or 2 */
+  uint8_t  contains_dc;                 /* the allocation holds the DC subcarrier */
+  uint8_t  reserved[3];
+} pg_ulsch_info_config;
+
+typedef struct pg_ulsch_info {
+  uint32_t nof_ul_sch_bits;     /* G^UL-SCH */
+  uint32_t nof_harq_ack_bits;   /* G^HARQ-ACK */
+  uint32_t nof_harq_ack_rvd;    /* G^HARQ-ACK_rvd */
+  uint32_t nof_csi_part1_bits;  /* G^CSI-1 */
+  uint32_t nof_csi_part2_bits;  /* G^CSI-2 */
+  uint32_t nof_harq_ack_re;     /* Q'_ACK */
+  uint32_t nof_csi_part1_re;    /* Q'_CSI-1 */
+  uint32_t nof_csi_part2_re;    /* Q'_CSI-2 */
+  uint32_t nof_dc_overlap_bits; /* rate-matched bits on the DC subcarrier */
+} pg_ulsch_info;
+
+int pg_ulsch_information(const pg_ulsch_info_config* cfg, pg_ulsch_info* out);
+
 /* Soft bits of the UL-SCH, HARQ-ACK and CSI Part 1 streams of one codeword (host computation, no
  * GPU): sizes[0..2]. PG_ERR_INVALID when the configuration is inconsistent or unsupported. */
 int pg_ulsch_demultiplex_sizes(const pg_ulsch_demux_config* cfg, uint32_t* sizes);

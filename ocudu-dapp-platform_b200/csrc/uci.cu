@@ -26,6 +26,8 @@
 #include "pg_device.cuh"
 #include "pg_internal.h"
 
+#include <cmath>
+
 #include <array>
 
 #include <algorithm>
@@ -595,7 +597,124 @@ int uci_detect_launch(pg_context* ctx, const void* items_dev, int n, const int8_
 
 } // namespace pg
 
+namespace {
+
+// CRC bits attached to a UCI payload of n bits (TS 38.212 Section 6.3.2.1 via 5.2.1): none up to 11
+// bits, CRC6 up to 19, CRC11 above.
+unsigned uci_crc_bits(unsigned n)
+{
+  return n < 12 ? 0u : (n < 20 ? 6u : 11u);
+}
+
+// Resource elements of one UCI field with UL-SCH (TS 38.212 Sections 6.3.2.4.1.1-3): the
+// beta-offset share of the UCI-capable REs over the UL-SCH codeblock bits, capped. The single
+// precision and the operation order are those of lib/ran/pusch/ulsch_info.cpp:12-135, so that a
+// value on a rounding boundary gives the same count.
+unsigned uci_re_with_sch(unsigned bits, float beta, unsigned re_uci, unsigned sum_cb)
+{
+  return (unsigned)std::ceil((float)(bits + uci_crc_bits(bits)) * beta * (float)re_uci / (float)sum_cb);
+}
+
+unsigned uci_re_without_sch(unsigned bits, float beta, float rate, unsigned qm)
+{
+  return (unsigned)std::ceil((float)(bits + uci_crc_bits(bits)) * beta / (rate * (float)qm));
+}
+
+} // namespace
+
 extern "C" {
+
+int pg_ulsch_information(const pg_ulsch_info_config* cfg, pg_ulsch_info* out)
+{
+  if (cfg == nullptr || out == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  const pg_ulsch_info_config& c = *cfg;
+  const unsigned qm = c.modulation_order, nl = c.nof_layers;
+  const uint32_t alloc = ((1u << (c.start_symbol + c.nof_symbols)) - 1u) & ~((1u << c.start_symbol) - 1u);
+  const uint32_t dm    = c.dmrs_symbol_mask & 0x3fffu;
+  const bool     sch   = c.tbs_bits > 0;
+  if (!(qm == 1 || qm == 2 || qm == 4 || qm == 6 || qm == 8) || nl < 1 || nl > 4 || c.nof_rb == 0 ||
+      c.nof_symbols == 0 || c.start_symbol + c.nof_symbols > 14 || dm == 0 || (dm & ~alloc) != 0 ||
+      c.nof_cdm_groups_without_data < 1 || c.nof_cdm_groups_without_data > 2 ||
+      (sch && c.base_graph != 1 && c.base_graph != 2) || (!sch && !(c.target_code_rate > 0.f && c.target_code_rate < 1.f))) {
+    return PG_ERR_INVALID;
+  }
+  // Codeblocks of the UL-SCH: sum of K_r (including filler bits), TS 38.212 Section 5.2.2.
+  const unsigned nd         = (unsigned)__builtin_popcount(dm);
+  const unsigned re_dmrs_rb = nd * c.nof_cdm_groups_without_data * 6u; // DM-RS type 1: 6 REs per CDM group
+  const unsigned re_total   = c.nof_rb * (c.nof_symbols * 12u - re_dmrs_rb);
+  unsigned       sum_cb     = 0;
+  if (sch) {
+    pg_sch_segmentation seg = {};
+    if (pg_sch_segment(c.tbs_bits, c.base_graph, qm, (int)nl, re_total * nl, &seg) != PG_OK) {
+      return PG_ERR_INVALID;
+    }
+    sum_cb = seg.nof_cbs * seg.cb_length;
+  }
+  const unsigned re_uci     = (c.nof_symbols - nd) * c.nof_rb * 12u;
+  // UCI-capable REs from the first DM-RS symbol on.
+  unsigned re_uci_l0 = 0;
+  for (unsigned s = (unsigned)__builtin_ctz(dm); s < c.start_symbol + c.nof_symbols; ++s) {
+    re_uci_l0 += ((dm >> s) & 1u) ? 0u : c.nof_rb * 12u;
+  }
+  const unsigned cap_ack = (unsigned)std::ceil(c.alpha_scaling * (float)re_uci_l0);
+  auto ack_re = [&](unsigned bits) {
+    if (bits == 0) {
+      return 0u;
+    }
+    const unsigned left = sch ? uci_re_with_sch(bits, c.beta_offset_harq_ack, re_uci, sum_cb)
+                              : uci_re_without_sch(bits, c.beta_offset_harq_ack, c.target_code_rate, qm);
+    return std::min(left, cap_ack);
+  };
+  const unsigned harq_re = ack_re(c.nof_harq_ack_bits);
+  // Up to two HARQ-ACK bits reserve the REs of two.
+  unsigned rvd_re = 0;
+  if (c.nof_harq_ack_bits < 2) {
+    rvd_re = ack_re(2);
+  } else if (c.nof_harq_ack_bits == 2) {
+    rvd_re = harq_re;
+  }
+  const unsigned ack_for_csi1 = c.nof_harq_ack_bits <= 2 ? rvd_re : harq_re;
+  unsigned       csi1_re      = 0;
+  if (c.nof_csi_part1_bits > 0) {
+    if (sch) {
+      const unsigned left  = uci_re_with_sch(c.nof_csi_part1_bits, c.beta_offset_csi_part1, re_uci, sum_cb);
+      const unsigned right = (unsigned)std::ceil(c.alpha_scaling * (float)re_uci) - ack_for_csi1;
+      csi1_re              = std::min(left, right);
+    } else if (c.nof_csi_part2_bits == 0) {
+      csi1_re = re_uci - ack_for_csi1;
+    } else {
+      csi1_re = std::min(uci_re_without_sch(c.nof_csi_part1_bits, c.beta_offset_csi_part1, c.target_code_rate, qm),
+                         re_uci - ack_for_csi1);
+    }
+  }
+  const unsigned ack_for_csi2 = c.nof_harq_ack_bits <= 2 ? 0u : harq_re;
+  unsigned       csi2_re      = 0;
+  if (c.nof_csi_part2_bits > 0) {
+    if (sch) {
+      const unsigned left  = uci_re_with_sch(c.nof_csi_part2_bits, c.beta_offset_csi_part2, re_uci, sum_cb);
+      const unsigned right = (unsigned)std::ceil(c.alpha_scaling * (float)re_uci) - ack_for_csi2 - csi1_re;
+      csi2_re              = std::min(left, right);
+    } else {
+      csi2_re = re_uci - ack_for_csi2 - csi1_re;
+    }
+  }
+  const unsigned ack_used = c.nof_harq_ack_bits > 2 ? harq_re : 0u;
+  const unsigned sch_re   = sch ? re_total - ack_used - csi1_re - csi2_re : 0u;
+  const unsigned per_re   = nl * qm;
+  *out                     = pg_ulsch_info{};
+  out->nof_ul_sch_bits     = sch_re * per_re;
+  out->nof_harq_ack_bits   = harq_re * per_re;
+  out->nof_harq_ack_rvd    = rvd_re * per_re;
+  out->nof_csi_part1_bits  = csi1_re * per_re;
+  out->nof_csi_part2_bits  = csi2_re * per_re;
+  out->nof_harq_ack_re     = harq_re;
+  out->nof_csi_part1_re    = csi1_re;
+  out->nof_csi_part2_re    = csi2_re;
+  out->nof_dc_overlap_bits = c.contains_dc ? c.nof_symbols * qm : 0u;
+  return PG_OK;
+}
 
 int pg_ulsch_demultiplex_sizes(const pg_ulsch_demux_config* cfg, uint32_t* sizes)
 {

@@ -89,6 +89,23 @@ class PgPuschPlanTuning(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class PgUlschInfoConfig(ctypes.Structure):
+    _fields_ = [("tbs_bits", ctypes.c_uint32), ("target_code_rate", ctypes.c_float), ("alpha_scaling", ctypes.c_float),
+                ("beta_offset_harq_ack", ctypes.c_float), ("beta_offset_csi_part1", ctypes.c_float),
+                ("beta_offset_csi_part2", ctypes.c_float), ("nof_harq_ack_bits", ctypes.c_uint16),
+                ("nof_csi_part1_bits", ctypes.c_uint16), ("nof_csi_part2_bits", ctypes.c_uint16),
+                ("nof_rb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16), ("base_graph", ctypes.c_uint8),
+                ("modulation_order", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8), ("start_symbol", ctypes.c_uint8),
+                ("nof_symbols", ctypes.c_uint8), ("nof_cdm_groups_without_data", ctypes.c_uint8),
+                ("contains_dc", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3)]
+
+
+class PgUlschInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in ("nof_ul_sch_bits", "nof_harq_ack_bits", "nof_harq_ack_rvd",
+                                               "nof_csi_part1_bits", "nof_csi_part2_bits", "nof_harq_ack_re",
+                                               "nof_csi_part1_re", "nof_csi_part2_re", "nof_dc_overlap_bits")]
+
+
 class PgUlschDemuxConfig(ctypes.Structure):
     _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("sch_offset", ctypes.c_uint32),
                 ("harq_ack_offset", ctypes.c_uint32), ("csi_part1_offset", ctypes.c_uint32),
@@ -170,6 +187,7 @@ SIGNATURES = {
                                         ctypes.c_float, _VP, _VP]),
     "pg_demodulate_soft_device": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP, _VP]),
     "pg_demodulate_soft_host": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
+    "pg_ulsch_information": (ctypes.c_int, [_VP, _VP]),
     "pg_descramble_device": (ctypes.c_int, [_VP, ctypes.c_uint32, _VP, _VP, ctypes.c_size_t, _VP]),
     "pg_descramble_host": (ctypes.c_int, [_VP, ctypes.c_uint32, _VP, _VP, ctypes.c_size_t]),
     "pg_pusch_est_size": (ctypes.c_size_t, [_VP]),

@@ -5,7 +5,8 @@ of complex64 equalised data symbols ([OFDM symbol][RE][layer], the exporter's or
 runs through the receiver chain the gNB runs after equalisation - soft demapping with a flat noise
 variance from the reported post-equalisation SINR, descrambling, UL-SCH demultiplexing, rate
 dematching, LDPC decoding, TB CRC - here on the GPU (pg_demodulate_soft_host,
-pg_descramble_host, pg_ulsch_demultiplex_device for bursts that carry UCI, pg_sch_decode_batch_host),
+pg_descramble_host, pg_ulsch_demultiplex_device for bursts that carry UCI with the sizes of
+pg_ulsch_information, pg_sch_decode_batch_host),
 and the TB CRC is printed next to the one the gNB reported, so recordings can be validated and other
 front ends (channel estimation, equalisation) scored by writing their output as the same JSON + cf32
 pair.
@@ -25,9 +26,9 @@ from typing import Optional
 
 import numpy as np
 
-from . import _native
+from . import _native, uci
 from .demod import DemodulationMapper
-from .sch import PuschDecoder, SchTransportBlock, segment
+from .sch import PuschDecoder, SchTransportBlock
 
 # ldpc::MAX_CODEBLOCK_SIZE (include/ocudu/phy/upper/channel_coding/ldpc/ldpc.h): 66 * 384.
 MAX_CODEBLOCK_SIZE = 25344
@@ -114,8 +115,6 @@ def replay(ctx: _native.Context, burst: Burst, iterations=10) -> ReplayResult:
     nre_symbol = 12 * burst.nof_prb
     if burst.symbols.size % (nre_symbol * nl):
         raise ValueError(f"sample count {burst.symbols.size} is not a whole number of OFDM symbols")
-    if int(g.get("nof_harq_ack_bits", 0) or 0) or int(g.get("nof_csi_part1_bits", 0) or 0):
-        raise ValueError("bursts with UCI multiplexed on the PUSCH are not replayed (UL-SCH only)")
     tbs_bits = 8 * int(g["tbs_bytes"])
     bg = 2 if int(g["ldpc_base_graph"]) == 2 else 1
     c = nof_codeblocks(tbs_bits, bg)
@@ -127,14 +126,37 @@ def replay(ctx: _native.Context, burst: Burst, iterations=10) -> ReplayResult:
     c_init = ((burst.rnti << 15) + int(g["n_id"])) & 0xFFFFFFFF
     ctx.check(ctx.lib.pg_descramble_host(ctx.handle, c_init, llrs.ctypes.data_as(ctypes.c_void_p),
                                          llrs.ctypes.data_as(ctypes.c_void_p), llrs.size))
-    seg = segment(tbs_bits, bg, qm, nl, llrs.size // qm)
-    if seg["nof_cbs"] != c:
-        raise ValueError("codeblock count mismatch")
-    res = PuschDecoder(ctx).decode_batch([SchTransportBlock(llrs=llrs, tbs_bits=tbs_bits, base_graph=bg,
+    # UL-SCH information: how many soft bits carry data and how many UCI (TS 38.212 6.3.2.4), then the
+    # UL-SCH stream out of the codeword when UCI is multiplexed (ocudu_pusch_replay.cpp:152-188,255-263).
+    ack, csi1 = int(g.get("nof_harq_ack_bits") or 0), int(g.get("nof_csi_part1_bits") or 0)
+    mask = int(g["dmrs_symbol_mask"])
+    contains_dc = False
+    if g.get("dc_position") is not None:
+        dc_prb = int(g["dc_position"]) // 12
+        prb_mask = str(g["prb_mask"])
+        contains_dc = bool((int(prb_mask[2 * (dc_prb // 8):2 * (dc_prb // 8) + 2], 16) >> (dc_prb % 8)) & 1)
+    info = uci.ulsch_information(tbs_bits, bg, qm, nl, burst.nof_prb, int(g["start_symbol"]), int(g["nof_symbols"]),
+                                 mask, ack, csi1, 0, float(g["alpha_scaling"]), float(g["beta_offset_harq_ack"]),
+                                 float(g["beta_offset_csi_part1"]), float(g["beta_offset_csi_part2"]),
+                                 int(g["nof_cdm_groups_without_data"]), contains_dc=contains_dc)
+    sch_llrs = llrs
+    if ack or csi1:
+        cfg = uci.make_config(nof_llrs=llrs.size, c_init=c_init, nof_harq_ack_rvd=info["nof_harq_ack_rvd"],
+                              nof_enc_harq_ack_bits=info["nof_harq_ack_bits"],
+                              nof_enc_csi_part1_bits=info["nof_csi_part1_bits"], nof_prb=burst.nof_prb,
+                              dmrs_symbol_mask=mask, modulation_order=qm, nof_layers=nl,
+                              start_symbol_index=int(g["start_symbol"]), nof_symbols=int(g["nof_symbols"]),
+                              dmrs_type=int(g["dmrs_type"]),
+                              nof_cdm_groups_without_data=int(g["nof_cdm_groups_without_data"]),
+                              nof_harq_ack_bits=ack, nof_csi_part1_bits=csi1)
+        sch_llrs = uci.UlschDemultiplexer(ctx).demultiplex([cfg], [llrs])[0][0]
+    if sch_llrs.size != info["nof_ul_sch_bits"]:
+        raise ValueError(f"{llrs.size} soft bits for a grant of {info['nof_ul_sch_bits']} UL-SCH bits")
+    res = PuschDecoder(ctx).decode_batch([SchTransportBlock(llrs=sch_llrs, tbs_bits=tbs_bits, base_graph=bg,
                                                             modulation_order=qm, nof_layers=nl, rv=int(g["rv"]),
                                                             nref=nref, max_iterations=iterations)])[0]
-    return ReplayResult(res.tb_crc_ok, tbs_bits // 8, res.nof_codeblocks_total, llrs.size, res.mean_iterations,
-                        res.transport_block, llrs)
+    return ReplayResult(res.tb_crc_ok, tbs_bits // 8, res.nof_codeblocks_total, info["nof_ul_sch_bits"],
+                        res.mean_iterations, res.transport_block, llrs)
 
 
 def main(argv=None):

@@ -307,12 +307,14 @@ def scale_grid_words(words, factor):
 # Replay bursts (the E3 pusch.symbols recording format of the reference's ocudu-pusch-replay).
 
 def synthetic_burst(seed=0, nof_prb=52, mcs_table=2, mcs_index=10, nof_layers=1, sinr_db=20.0, rv=0,
-                    crc_ok_reported=True, nof_dmrs=2):
+                    crc_ok_reported=True, nof_dmrs=2, nof_harq_ack_bits=0, nof_csi_part1_bits=0):
     """A recorded PUSCH burst in the form the reference's replay tool reads
     (apps/tools/pusch_replay/ocudu_pusch_replay.cpp:93-137): the grant of one UE with 14 OFDM
     symbols and DM-RS type 1 at symbols 2 (and 11), and its equalised data symbols - the scrambled
     UL-SCH codeword of a random TB, QAM-modulated with unit energy, plus complex white noise of
-    variance 10^(-SINR/10). Returns (replay.Burst, transmitted TB bits)."""
+    variance 10^(-SINR/10). With UCI bits in the grant the symbols are random QPSK-scaled noise of
+    the same length (this simulator has no UCI transmit multiplexer), a burst for the replay's
+    accounting and demultiplexing, not for decoding. Returns (replay.Burst, transmitted TB bits)."""
     from . import mcs as mcs_tables
     from . import prg
     from .replay import Burst
@@ -333,6 +335,8 @@ def synthetic_burst(seed=0, nof_prb=52, mcs_table=2, mcs_index=10, nof_layers=1,
     cw = codec.ulsch_encode(tb, bg, qm, nof_layers, ncs, seg, rv=rv, nref=nref)
     cw = cw ^ prg.scrambling(rnti, n_id, cw.size)
     x = codec.modulate(cw, qm)
+    if nof_harq_ack_bits or nof_csi_part1_bits:
+        x = codec.modulate(rng.integers(0, 2, cw.size, dtype=np.uint8), qm)
     nv = 10 ** (-sinr_db / 10)
     y = x + np.sqrt(nv / 2) * (rng.standard_normal(x.size) + 1j * rng.standard_normal(x.size))
     mask = 0
@@ -340,7 +344,8 @@ def synthetic_burst(seed=0, nof_prb=52, mcs_table=2, mcs_index=10, nof_layers=1,
         mask |= 1 << s
     grant = {"tbs_bytes": tbs // 8, "tbs_lbrm_bytes": lbrm_bits // 8, "ldpc_base_graph": bg, "rv": rv,
              "harq_id": 0, "n_id": n_id, "mcs_index": mcs_index, "mcs_table": mcs_table,
-             "nof_harq_ack_bits": 0, "nof_csi_part1_bits": 0, "alpha_scaling": 1.0, "beta_offset_harq_ack": 20.0,
+             "nof_harq_ack_bits": nof_harq_ack_bits, "nof_csi_part1_bits": nof_csi_part1_bits, "alpha_scaling": 1.0,
+             "beta_offset_harq_ack": 20.0,
              "beta_offset_csi_part1": 6.25, "beta_offset_csi_part2": 6.25, "start_symbol": 0, "nof_symbols": 14,
              "dmrs_type": 1, "dmrs_symbol_mask": mask, "nof_cdm_groups_without_data": 2, "dc_position": None,
              "prb_mask": "ff" * ((nof_prb + 7) // 8)}

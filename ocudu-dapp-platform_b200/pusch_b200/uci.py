@@ -97,3 +97,28 @@ class ShortBlockDetector:
             out.append((bits[o:o + K].copy(), bool(valid[i])))
             o += K
         return out
+
+
+def ulsch_information(tbs_bits, base_graph, modulation_order, nof_layers, nof_rb, start_symbol, nof_symbols,
+                      dmrs_symbol_mask, nof_harq_ack_bits=0, nof_csi_part1_bits=0, nof_csi_part2_bits=0,
+                      alpha_scaling=1.0, beta_offset_harq_ack=20.0, beta_offset_csi_part1=6.25,
+                      beta_offset_csi_part2=6.25, nof_cdm_groups_without_data=2, target_code_rate=0.5,
+                      contains_dc=False) -> dict:
+    """pg_ulsch_information: the encoded soft-bit counts of UCI multiplexed on a PUSCH (the
+    reference's get_ulsch_information, include/ocudu/ran/pusch/ulsch_info.h:144)."""
+    from ._native import PgUlschInfo, PgUlschInfoConfig
+    c = PgUlschInfoConfig()
+    c.tbs_bits, c.target_code_rate, c.alpha_scaling = tbs_bits, target_code_rate, alpha_scaling
+    c.beta_offset_harq_ack, c.beta_offset_csi_part1, c.beta_offset_csi_part2 = (
+        beta_offset_harq_ack, beta_offset_csi_part1, beta_offset_csi_part2)
+    c.nof_harq_ack_bits, c.nof_csi_part1_bits, c.nof_csi_part2_bits = (
+        nof_harq_ack_bits, nof_csi_part1_bits, nof_csi_part2_bits)
+    c.nof_rb, c.dmrs_symbol_mask, c.base_graph = nof_rb, dmrs_symbol_mask, base_graph
+    c.modulation_order, c.nof_layers, c.start_symbol, c.nof_symbols = (
+        modulation_order, nof_layers, start_symbol, nof_symbols)
+    c.nof_cdm_groups_without_data, c.contains_dc = nof_cdm_groups_without_data, int(bool(contains_dc))
+    out = PgUlschInfo()
+    rc = _native.load().pg_ulsch_information(ctypes.byref(c), ctypes.byref(out))
+    if rc:
+        raise _native.PgError(rc, "invalid UL-SCH information request")
+    return {n: int(getattr(out, n)) for n, _ in PgUlschInfo._fields_}

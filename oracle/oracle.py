@@ -239,6 +239,20 @@ class Ref:
           _ptr(csi), G, _ptr(lens))
         return sch[:lens[0]].copy(), ack[:lens[1]].copy(), csi[:lens[2]].copy(), bool(lens[3])
 
+    def ulsch_information(self, tbs_bits, rate_x1024, qm, nof_layers, harq_ack, csi1, csi2, alpha, beta_ack,
+                          beta_csi1, beta_csi2, nof_rb, start, nof_symbols, dmrs_mask, nof_cdm, contains_dc=False):
+        """The reference's get_ulsch_information (lib/ran/pusch/ulsch_info.cpp) for DM-RS type 1:
+        (UL-SCH, HARQ-ACK, reserved HARQ-ACK, CSI-1, CSI-2 soft bits, HARQ-ACK, CSI-1, CSI-2 REs, DC
+        overlap bits)."""
+        out = np.zeros(9, np.uint32)
+        f = self.lib.ref_ulsch_information
+        f.argtypes = [ctypes.c_uint, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.c_uint,
+                      ctypes.c_uint, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_uint,
+                      ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, ctypes.c_void_p]
+        f(tbs_bits, rate_x1024, qm, nof_layers, harq_ack, csi1, csi2, alpha, beta_ack, beta_csi1, beta_csi2, nof_rb,
+          start, nof_symbols, dmrs_mask, nof_cdm, int(contains_dc), _ptr(out))
+        return tuple(int(x) for x in out)
+
     def short_block_encode(self, msg, E, qm):
         msg = np.ascontiguousarray(msg, dtype=np.uint8)
         out = np.zeros(E, np.uint8)

@@ -14,6 +14,7 @@
 #include "ocudu/ocuduvec/bit.h"
 #include "ocudu/phy/upper/channel_processors/pusch/pusch_decoder_buffer.h"
 #include "ocudu/phy/upper/sequence_generators/sequence_generator_factories.h"
+#include "ocudu/ran/pusch/ulsch_info.h"
 #include "ocudu/ran/uci/uci_info.h"
 #include <cstring>
 #include <memory>
@@ -170,3 +171,43 @@ int ref_uci_min_encoded_bits(int K)
 }
 
 } // extern "C"
+
+/// get_ulsch_information (lib/ran/pusch/ulsch_info.cpp) for DM-RS type 1: out[0..8] = UL-SCH,
+/// HARQ-ACK, reserved HARQ-ACK, CSI-1 and CSI-2 soft bits, HARQ-ACK, CSI-1 and CSI-2 REs, DC overlap
+/// bits. rate_x1024 is the MCS's target code rate times 1024.
+extern "C" int ref_ulsch_information(unsigned tbs_bits, float rate_x1024, int qm, int nof_layers, unsigned harq_ack,
+                                     unsigned csi1, unsigned csi2, float alpha, float beta_ack, float beta_csi1,
+                                     float beta_csi2, unsigned nof_rb, unsigned start, unsigned nof_symbols,
+                                     unsigned dmrs_mask, unsigned nof_cdm, int contains_dc, uint32_t* out)
+{
+  ulsch_configuration c;
+  c.tbs                          = units::bits(tbs_bits);
+  c.mcs_descr.modulation         = static_cast<modulation_scheme>(qm);
+  c.mcs_descr.target_code_rate   = rate_x1024;
+  c.nof_harq_ack_bits            = units::bits(harq_ack);
+  c.nof_csi_part1_bits           = units::bits(csi1);
+  c.nof_csi_part2_bits           = units::bits(csi2);
+  c.alpha_scaling                = alpha;
+  c.beta_offset_harq_ack         = beta_ack;
+  c.beta_offset_csi_part1        = beta_csi1;
+  c.beta_offset_csi_part2        = beta_csi2;
+  c.nof_rb                       = nof_rb;
+  c.start_symbol_index           = start;
+  c.nof_symbols                  = nof_symbols;
+  c.dmrs_type                    = dmrs_config_type::type1;
+  c.dmrs_symbol_mask             = bounded_bitset<MAX_NSYMB_PER_SLOT>(MAX_NSYMB_PER_SLOT);
+  for (unsigned s = 0; s != MAX_NSYMB_PER_SLOT; ++s) {
+    if ((dmrs_mask >> s) & 1U) {
+      c.dmrs_symbol_mask.set(s);
+    }
+  }
+  c.nof_cdm_groups_without_data = nof_cdm;
+  c.nof_layers                  = static_cast<unsigned>(nof_layers);
+  c.contains_dc                 = contains_dc != 0;
+  const ulsch_information i     = get_ulsch_information(c);
+  const uint32_t v[9] = {i.nof_ul_sch_bits.value(), i.nof_harq_ack_bits.value(), i.nof_harq_ack_rvd.value(),
+                         i.nof_csi_part1_bits.value(), i.nof_csi_part2_bits.value(), i.nof_harq_ack_re,
+                         i.nof_csi_part1_re, i.nof_csi_part2_re, i.nof_dc_overlap_bits.value()};
+  std::memcpy(out, v, sizeof(v));
+  return 0;
+}

@@ -20,11 +20,12 @@ needs_ref = pytest.mark.skipif(not os.path.exists(REF_REPLAY), reason="oracle/_r
 CASES = [(20.0, 2, 10, 1, 52, 0), (-3.0, 2, 10, 1, 52, 0), (30.0, 2, 25, 2, 273, 0), (15.0, 1, 5, 1, 20, 2)]
 
 
-def write_cases(tmp_path):
+def write_cases(tmp_path, uci=False):
     out = []
     for i, (sinr, table, index, nl, prb, rv) in enumerate(CASES):
+        ack, csi = ((0, 0), (2, 0), (5, 8), (1, 11))[i] if uci else (0, 0)
         b, tb = sim.synthetic_burst(seed=i, nof_prb=prb, mcs_table=table, mcs_index=index, nof_layers=nl,
-                                    sinr_db=sinr, rv=rv)
+                                    sinr_db=sinr, rv=rv, nof_harq_ack_bits=ack, nof_csi_part1_bits=csi)
         path = os.path.join(str(tmp_path), f"burst{i}.json")
         replay.write_burst(path, b)
         out.append((path, b, tb))

@@ -16,9 +16,12 @@ pytestmark = pytest.mark.gpu
 
 
 @needs_ref
-def test_replay_matches_reference_tool(tmp_path):
+@pytest.mark.parametrize("uci", [False, True])
+def test_replay_matches_reference_tool(tmp_path, uci):
+    """uci: the grants carry HARQ-ACK / CSI Part 1 (the UL-SCH bit count and demultiplexing follow the
+    UCI sizes; the symbols are noise, so both tools report the same failing CRC and iterations)."""
     env = dict(os.environ, PYTHONPATH=os.path.join(ROOT, "ocudu-dapp-platform_b200"))
-    for path, b, tb in write_cases(tmp_path):
+    for path, b, tb in write_cases(tmp_path, uci):
         ref = subprocess.run([REF_REPLAY, path, "--verbose"], capture_output=True, text=True, timeout=300)
         got = subprocess.run([sys.executable, "-m", "pusch_b200.replay", path, "--verbose"], capture_output=True,
                              text=True, timeout=300, env=env)
