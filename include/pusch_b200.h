@@ -548,8 +548,11 @@ typedef struct pg_pusch_plan_tuning {
   int demod_block;          /* demodulation: threads per CTA, 64, 128 or 256 (default 256) */
   int ldpc_ctas_per_sm;     /* persistent LDPC decoders: CTAs per SM, 1..4 (default 2; the one-lane-per-
                                thread decoder holds at most 2) */
-  int ldpc_kernel;          /* LDPC decoder (pg_ldpc_kernel): PG_LDPC_KERNEL_ONE_LANE, _TWO_LANES or _SPLIT
-                               (default PG_LDPC_KERNEL_SPLIT) */
+  int ldpc_kernel;          /* LDPC decoder (pg_ldpc_kernel), PG_LDPC_KERNEL_ONE_LANE .. _Z384_SPLIT
+                               (default PG_LDPC_KERNEL_Z384) */
+  int ldpc_order;           /* work order of the persistent decoders: 0 = largest codeblocks first, fixed
+                               when the plan is created; 1 = longest predicted decode first, from every
+                               execution's LLRs (pg_set_ldpc_order's estimate; default 1) */
 } pg_pusch_plan_tuning;
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out);

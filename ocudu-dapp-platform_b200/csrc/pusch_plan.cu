@@ -74,7 +74,8 @@ struct pg_pusch_plan {
   uint32_t*       d_tb_crc = nullptr;
   int32_t*        d_iters  = nullptr;
   int8_t*         d_c2v    = nullptr;
-  uint32_t*       d_order  = nullptr;
+  uint32_t*       d_order  = nullptr; // per-execution work order (device ordering)
+  uint32_t*       d_order_static = nullptr; // largest codeblocks first, fixed at creation
   uint8_t*        d_keys   = nullptr; // work-order keys of the codeblocks // LDPC work order: largest codeblocks first
   int*            d_counter = nullptr; // work counter of the persistent decoder
   uint32_t*       d_grid   = nullptr; // grids of execute_host
@@ -107,7 +108,7 @@ struct pg_pusch_plan {
   int             le_nseq   = 0;
   int             le_rows   = 0;
   // Launch shapes (defaults, or the autotuner's choice).
-  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, PG_LDPC_KERNEL_Z384};
+  pg_pusch_plan_tuning tuning = {8, 1, 256, 2, PG_LDPC_KERNEL_Z384, 1};
   // CUDA graph of execute_device.
   bool            use_graph = false;
   cudaGraphExec_t exec      = nullptr;
@@ -284,13 +285,15 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     rc = rate_dematch_launch(ctx, p->d_rm, (int)p->unplaced.size(), p->d_llr, p->d_rm_out, s,
                              p->tuning.rm_ctas_per_cb, p->d_unplaced);
   }
-  if (rc == PG_OK && p->nof_cbs > 1) {
-    // Hardest first: the decoders take the codeblocks in ascending order of input confidence.
-    rc = ldpc_order_launch(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_keys, p->d_order, s);
+  const uint32_t* order = p->d_order_static;
+  if (rc == PG_OK && p->nof_cbs > 1 && p->tuning.ldpc_order != 0) {
+    // Longest first: the decoders take the codeblocks by the predicted decoding time of their input.
+    rc    = ldpc_order_launch(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_keys, p->d_order, s);
+    order = p->d_order;
   }
   if (rc == PG_OK) {
     rc = ldpc_launch_persistent(ctx, p->d_ldpc, p->nof_cbs, p->d_rm_out, p->d_cb_bits, p->d_iters, p->d_c2v,
-                                p->d_order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count,
+                                order, p->d_counter, s, p->tuning.ldpc_ctas_per_sm * ctx->sm_count,
                                 p->ldpc_kinds | ldpc_route(p->tuning.ldpc_kernel));
   }
   if (rc == PG_OK) {
@@ -516,7 +519,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_tb     = o_ldpc + al(w.ldpc.size() * sizeof(pg_ldpc_cb));
   const size_t o_cb_off = o_tb + al(w.tbd.size() * sizeof(pg_tb_desc));
   const size_t o_order  = o_cb_off + al(w.cb_bit_off.size() * 4);
-  const size_t o_seqoff = o_order + al(order.size() * 4);
+  const size_t o_ostat  = o_order + al(order.size() * 4);
+  const size_t o_seqoff = o_ostat + al(order.size() * 4);
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
   std::vector<uint32_t> est_work;
   uint32_t              pilot_words = 0;
@@ -590,6 +594,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   p->d_iters   = reinterpret_cast<int32_t*>(b + o_it);
   p->d_c2v     = reinterpret_cast<int8_t*>(b + o_c2v);
   p->d_order   = reinterpret_cast<uint32_t*>(b + o_order);
+  p->d_order_static = reinterpret_cast<uint32_t*>(b + o_ostat);
   p->d_counter = reinterpret_cast<int*>(b + o_cnt);
   p->d_keys    = b + o_keys;
   p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
@@ -617,6 +622,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   std::memcpy(h + o_tb, w.tbd.data(), w.tbd.size() * sizeof(pg_tb_desc));
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
   std::memcpy(h + o_order, order.data(), order.size() * 4);
+  std::memcpy(h + o_ostat, order.data(), order.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, tile_map.data(), tile_map.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);
@@ -873,7 +879,8 @@ static bool tuning_valid(const pg_pusch_plan_tuning& t, const pg_context* ctx)
   return t.rm_ctas_per_cb >= 1 && t.rm_ctas_per_cb <= 32 && t.demod_res_per_thread >= 1 &&
          t.demod_res_per_thread <= 8 && (t.demod_block == 64 || t.demod_block == 128 || t.demod_block == 256) &&
          t.ldpc_ctas_per_sm >= 1 && t.ldpc_ctas_per_sm <= 4 &&
-         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_Z384_SPLIT;
+         t.ldpc_kernel >= PG_LDPC_KERNEL_ONE_LANE && t.ldpc_kernel <= PG_LDPC_KERNEL_Z384_SPLIT &&
+         (t.ldpc_order == 0 || t.ldpc_order == 1);
 }
 
 int pg_pusch_plan_get_tuning(const pg_pusch_plan* plan, pg_pusch_plan_tuning* out)
@@ -1023,6 +1030,11 @@ int pg_pusch_plan_autotune(pg_pusch_plan* plan, const uint32_t* grids, int reps,
                   PG_LDPC_KERNEL_Z384_SPLIT}) {
       pg_pusch_plan_tuning c = cur;
       c.ldpc_kernel          = v;
+      if (rc == PG_OK) rc = try_set(c);
+    }
+    for (int v : {0, 1}) {
+      pg_pusch_plan_tuning c = cur;
+      c.ldpc_order           = v;
       if (rc == PG_OK) rc = try_set(c);
     }
   }

@@ -83,7 +83,8 @@ class PgLeAdam(ctypes.Structure):
 
 class PgPuschPlanTuning(ctypes.Structure):
     _fields_ = [("rm_ctas_per_cb", ctypes.c_int), ("demod_res_per_thread", ctypes.c_int),
-                ("demod_block", ctypes.c_int), ("ldpc_ctas_per_sm", ctypes.c_int), ("ldpc_kernel", ctypes.c_int)]
+                ("demod_block", ctypes.c_int), ("ldpc_ctas_per_sm", ctypes.c_int), ("ldpc_kernel", ctypes.c_int),
+                ("ldpc_order", ctypes.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

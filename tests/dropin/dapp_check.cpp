@@ -475,37 +475,50 @@ void check_receiver(module_handle& mh, void* worker, uint32_t worker_id)
       ++bad;
       continue;
     }
-    // The reference's chain on the same grid and pilots.
-    vector_grid_reader         reader(a.grid, a.nports, kGridSubc);
-    dynamic_re_buffer<cbf16_t> y(P, nre);
-    dynamic_ch_est_list        h(nre, P, L);
-    std::vector<float>         nv(P);
-    std::vector<cbf16_t>       sym(N);
+    // The reference's chain on the same grid and pilots, one OFDM symbol at a time as
+    // pusch_demodulator_impl.cpp:330-420 runs it (its equaliser and demapper take one symbol's REs).
+    vector_grid_reader reader(a.grid, a.nports, kGridSubc);
+    std::vector<float> nv(P);
+    std::vector<std::vector<cbf16_t>> est_sym(static_cast<size_t>(P) * L * S, std::vector<cbf16_t>(N));
     for (unsigned p = 0; p != P; ++p) {
       const port_channel_estimator_results& r = ref->compute(reader, p, *a.pilots, a.cfg);
       nv[p]                                   = r.get_noise_variance();
       for (unsigned l = 0; l != L; ++l) {
-        unsigned cur = ~0u;
-        for (unsigned i = 0; i != nre; ++i) {
-          const unsigned s = in.data_re[i] / N, k = in.data_re[i] % N;
-          if (s != cur) {
-            r.get_symbol_ch_estimate(sym, a.first_symbol + s, l);
-            cur = s;
-          }
-          h.get_channel(p, l)[i] = sym[k];
+        for (unsigned s = 0; s != S; ++s) {
+          r.get_symbol_ch_estimate(est_sym[(static_cast<size_t>(p) * L + l) * S + s], a.first_symbol + s, l);
         }
-      }
-      for (unsigned i = 0; i != nre; ++i) {
-        const unsigned s = in.data_re[i] / N, k = in.data_re[i] % N;
-        y.get_slice(p)[i] =
-            a.grid[(static_cast<size_t>(p) * MAX_NSYMB_PER_SLOT + a.first_symbol + s) * kGridSubc + 12 * a.rb_start + k];
       }
     }
     std::vector<cf_t>                 eq(static_cast<size_t>(nre) * L);
     std::vector<float>                var(static_cast<size_t>(nre) * L);
     std::vector<log_likelihood_ratio> want(static_cast<size_t>(nre) * L * qm);
-    eq_ref->equalize(eq, var, y, h, nv, 1.0f);
-    demap->demodulate_soft(want, eq, var, static_cast<modulation_scheme>(qm));
+    for (unsigned i0 = 0; i0 != nre;) {
+      const unsigned s  = in.data_re[i0] / N;
+      unsigned       i1 = i0;
+      while (i1 != nre && in.data_re[i1] / N == s) {
+        ++i1;
+      }
+      const unsigned             n = i1 - i0;
+      dynamic_re_buffer<cbf16_t> y(P, n);
+      dynamic_ch_est_list        h(n, P, L);
+      for (unsigned p = 0; p != P; ++p) {
+        for (unsigned i = 0; i != n; ++i) {
+          const unsigned k  = in.data_re[i0 + i] % N;
+          y.get_slice(p)[i] = a.grid[(static_cast<size_t>(p) * MAX_NSYMB_PER_SLOT + a.first_symbol + s) * kGridSubc +
+                                     12 * a.rb_start + k];
+          for (unsigned l = 0; l != L; ++l) {
+            h.get_channel(p, l)[i] = est_sym[(static_cast<size_t>(p) * L + l) * S + s][k];
+          }
+        }
+      }
+      span<cf_t>  eq_s  = span<cf_t>(eq).subspan(static_cast<size_t>(i0) * L, static_cast<size_t>(n) * L);
+      span<float> var_s = span<float>(var).subspan(static_cast<size_t>(i0) * L, static_cast<size_t>(n) * L);
+      eq_ref->equalize(eq_s, var_s, y, h, nv, 1.0f);
+      demap->demodulate_soft(span<log_likelihood_ratio>(want).subspan(static_cast<size_t>(i0) * L * qm,
+                                                                      static_cast<size_t>(n) * L * qm),
+                             eq_s, var_s, static_cast<modulation_scheme>(qm));
+      i0 = i1;
+    }
     bool ok = true;
     for (size_t i = 0; i != want.size(); ++i) {
       const int d = std::abs(static_cast<int>(want[i].to_value_type()) - static_cast<int>(llrs[i]));
@@ -582,6 +595,7 @@ int main(int argc, char** argv)
     std::fprintf(stderr, "usage: dapp_check <module.so> [--describe]\n");
     return 2;
   }
+  std::setvbuf(stdout, nullptr, _IONBF, 0); // every line reaches the log, also if a check aborts
   const bool describe = argc > 2 && std::strcmp(argv[2], "--describe") == 0;
   void*      so       = dlopen(argv[1], RTLD_NOW | RTLD_LOCAL);
   if (so == nullptr) {

@@ -103,9 +103,10 @@ def test_autotuner_keeps_results(ctx):
     assert 1 <= best.rm_ctas_per_cb <= 32 and 1 <= best.demod_res_per_thread <= 8
     assert best.demod_block in (64, 128, 256) and best.ldpc_ctas_per_sm in (1, 2, 3, 4)
     assert plan.tuning().as_dict() == best.as_dict()
-    assert best.ldpc_kernel in range(5)
+    assert best.ldpc_kernel in range(5) and best.ldpc_order in (0, 1)
     for shape in (best, PgPuschPlanTuning(3, 3, 64, 1, 0), PgPuschPlanTuning(32, 8, 128, 2, 1),
-                  PgPuschPlanTuning(8, 1, 256, 4, 1), PgPuschPlanTuning(8, 1, 256, 1, 1)):
+                  PgPuschPlanTuning(8, 1, 256, 4, 1), PgPuschPlanTuning(8, 1, 256, 1, 1),
+                  PgPuschPlanTuning(8, 1, 256, 2, 3, 1), PgPuschPlanTuning(16, 1, 256, 2, 4, 0)):
         plan.set_tuning(shape)
         got = plan.execute_host()
         for g, r in zip(got, ref):
