@@ -60,6 +60,14 @@ LDPC_KERNEL_NAMES = ["ldpc_decode_kernel (one lifted lane per thread)",
                      "ldpc_decode_split_kernel (two lanes per thread pair, row edges split over the pair)",
                      "ldpc_decode_z_kernel (two lifted lanes per thread, Z = 384 specialised, f16 soft-bit pairs)",
                      "ldpc_decode_zs_kernel (Z = 384 specialised, row edges split over a thread pair)"]
+# ncu figures of one launch of the LDPC batch per kernel (pg_ldpc_kernel id): DRAM bytes read +
+# written, and pipe utilisation in % of active cycles. Kernel 1 at four CTAs per SM, kernel 3 at
+# two (the bench default).
+LDPC_NCU = {
+    1: {"traffic": 24246528, "pipes": {"alu": 55.5, "fma": 32.3, "lsu": 24.9, "issue_active": 59.6,
+                                       "sm_active_pct_of_elapsed": 60.4}},
+    3: {"traffic": 11592960, "pipes": {"alu": 48.3, "issue_active": 48.9, "sm_active_pct_of_elapsed": 82.2}},
+}
 # Integer-instruction throughput probe (the LDPC roofline denominator), built by
 # ocudu-dapp-platform_b200/measure/Makefile.
 PROBE_SO = os.path.join(ROOT, "ocudu-dapp-platform_b200", "measure", "_lib", "libpg_probe.so")
@@ -87,6 +95,8 @@ def parse_args():
                    help="LDPC batch kernel of the --workload ldpc line (pg_ldpc_kernel; default: the library's)")
     p.add_argument("--ldpc-ctas-per-sm", type=int, default=2,
                    help="resident LDPC CTAs per SM of the --workload ldpc line (0: the kernel limit)")
+    p.add_argument("--ldpc-order", default="longest", choices=["given", "longest"],
+                   help="work order of the --workload ldpc line's persistent decoders (pg_set_ldpc_order)")
     return p.parse_args()
 
 
@@ -789,6 +799,7 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
     if args.ldpc_kernel is not None:
         dec.set_kernel(args.ldpc_kernel)
     dec.set_ctas_per_sm(args.ldpc_ctas_per_sm)
+    dec.set_order(0 if args.ldpc_order == "given" else 1)
     kernel_id = args.ldpc_kernel if args.ldpc_kernel is not None else int(dec.ctx.lib.pg_get_ldpc_kernel(dec.ctx.handle))
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
@@ -886,12 +897,11 @@ def ldpc_core(args, dev, rank, world, with_cpu=True, with_e2e=True, steps=None):
                         if peak_ops else "nominal 148 SM x 128 lanes x max SM clock"),
         "nominal_peak": round(nominal, 3), "instruction_classes_tops": classes,
         "ops_per_edge_update": INT_OPS_PER_EDGE, "edge_updates_per_launch": edge_updates,
-        # dram__bytes_read.sum + dram__bytes_write.sum of one launch of ldpc_decode_x2_kernel on this
-        # workload, and its pipe utilisation (ncu --set full, one launch; summarised in
-        # profiles/ldpc_decode_kernel_ldpc-batch-512cb.md).
-        "traffic": 24246528,
-        "ncu_pipes_pct_of_active": {"alu": 55.5, "fma": 32.3, "lsu": 24.9, "issue_active": 59.6,
-                                    "sm_active_pct_of_elapsed": 60.4},
+        # dram__bytes_read.sum + dram__bytes_write.sum of one launch on this workload, and the pipe
+        # utilisation, for the kernels with an ncu capture (summarised in
+        # profiles/ldpc_decode_kernel_ldpc-batch-512cb.md); null for the others.
+        "traffic": LDPC_NCU.get(kernel_id, {}).get("traffic"),
+        "ncu_pipes_pct_of_active": LDPC_NCU.get(kernel_id, {}).get("pipes"),
         "hbm_bytes_per_launch": int(llrs.size + nbytes + 4 * N_CBS + 20 * N_CBS),
     }
 
