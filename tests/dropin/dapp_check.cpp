@@ -175,7 +175,7 @@ struct allocation {
   unsigned                             nports = 4, nlayers = 1, rb_start = 0, nof_rb = 0, first_symbol = 0, nof_symbols = 14;
   unsigned                             nd = 2, qm = 2;
   float                                scaling = 1.41254f;
-  bounded_bitset<MAX_NSYMB_PER_SLOT>   dmrs{MAX_NSYMB_PER_SLOT};
+  bounded_bitset<MAX_NSYMB_PER_SLOT>   dmrs = bounded_bitset<MAX_NSYMB_PER_SLOT>(MAX_NSYMB_PER_SLOT); // 14 symbols
   std::vector<cbf16_t>                 grid; // [port][14][3276]
   std::unique_ptr<dmrs_symbol_list>    pilots;
   port_channel_estimator::configuration cfg;
