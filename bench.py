@@ -46,8 +46,6 @@ PUSCH_WORKLOAD = ("Batched uneven slot: 16 cells x 273 PRB (100 MHz, 30 kHz SCS)
                   "PRB allocations, QPSK-256QAM (MCS table 2) with link adaptation to BLER<=10%, 1-2 layers, 4 rx, "
                   "per-UE SNR U[0,30] dB, DM-RS type 1 symbols {2,11}, exponential PDP (100 ns RMS, 8 taps), "
                   "max 6 LDPC iterations, CRC early stop")
-KERNELS_PER_PLAN = 6  # estimate, demodulate, rate dematch, LDPC, TB assembly, results
-LE_KERNELS = 3        # learned estimator: features, the fused 14-layer network, apply
 LE_FLOPS_PER_ROW = 2 * 5 * (16 * 64 + 12 * 64 * 64 + 64 * 16)  # 14 layers, kernel 5, per subcarrier row
 WORKLOAD = ("LDPC decoder batch: 512 codeblocks, BG1 Z=384 (K=8448, rate 1/3) and BG2 Z=384 (K=3840, rate 1/5) "
             "mixed 50/50 by seed, CRC24B, BPSK/AWGN Eb/N0 U[1,3] dB, int8 LLRs (scale 4/LLR unit, sat +-127), "
@@ -98,6 +96,16 @@ def parse_args():
     p.add_argument("--ldpc-order", default="longest", choices=["given", "longest"],
                    help="work order of the --workload ldpc line's persistent decoders (pg_set_ldpc_order)")
     return p.parse_args()
+
+
+def plan_kernels(plan):
+    """Kernels one execution of the plan launches with its current tuning and estimator
+    (pg_pusch_plan_info's count)."""
+    import ctypes
+    from pusch_b200._native import PgPuschPlanInfo
+    info = PgPuschPlanInfo()
+    plan.ctx.check(plan.lib.pg_pusch_plan_info(plan.handle, ctypes.byref(info)))
+    return int(info.nof_kernels)
 
 
 def dist_env():
@@ -534,7 +542,7 @@ def run_ours_pusch(args):
         # The per-UE plans decode what the batched plan with the plain estimator decodes.
         plain_bits = bits_ok if batched_plain is None else p_bits
         plain = {"value": round(plain_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s", "ms_per_step": round(p_ms, 3),
-                 "plans": len(per_ue), "kernels_per_step": KERNELS_PER_PLAN * len(per_ue),
+                 "plans": len(per_ue), "kernels_per_step": sum(plan_kernels(p) for p in per_ue),
                  "what": "one plan per UE executed in turn, host waits for each UE's result (no batching, no graph)"}
         for p in per_ue:
             p.close()
@@ -711,7 +719,7 @@ def run_ours_pusch(args):
             "plain_per_ue": plain, "batched_plain": batched_plain,
             "e2e": e2e, "roofline": roofline, "rooflines": rooflines, "ldpc": ldpc_line, "uci": uci_line, "ofh_bfp": bfp_line, "cpu_baseline": cpu,
             "clocks": clk,
-            "gpu_launches": (KERNELS_PER_PLAN + (LE_KERNELS if net is not None else 0)) * args.steps,
+            "gpu_launches": plan_kernels(plan) * args.steps,
             "step_ms": {"min": round(min(step_ms), 4), "max": round(max(step_ms), 4)},
         }
         print(json.dumps(line), flush=True)

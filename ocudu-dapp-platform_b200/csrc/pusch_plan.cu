@@ -690,6 +690,13 @@ int pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info)
   info->nof_llrs       = plan->nof_llrs;
   info->grid_words     = plan->grid_words;
   info->device_bytes   = plan->dev_bytes;
+  // The kernels enqueue() launches: prefill, estimation, [learned: features, network, corrections],
+  // demodulation, [UCI: demultiplexing, detection], [rate dematching of the codeblocks not placed],
+  // [device work order: score, sort], LDPC, TB assembly, results.
+  info->nof_kernels = 2u + (plan->le_net != nullptr ? 3u : 0u) + 1u + (plan->uci_w.nitems > 0 ? 2u : 0u) +
+                      (plan->unplaced.empty() ? 0u : 1u) + (plan->nof_cbs > 1 && plan->tuning.ldpc_order != 0 ? 2u : 0u) +
+                      3u;
+  info->reserved = 0;
   return PG_OK;
 }
 
