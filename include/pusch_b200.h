@@ -144,9 +144,9 @@ enum pg_ldpc_kernel {
                                    halves; four CTAs per SM */
   PG_LDPC_KERNEL_SPLIT     = 2, /* 384 threads per codeblock; even Z > 192: two lanes per thread pair, each
                                    row's edges split between the two threads; two CTAs per SM */
-  PG_LDPC_KERNEL_Z384      = 3, /* 192 threads per codeblock; Z = 384 with the edge tables fixed at compile
-                                   time and f16 soft-bit pairs stored once, other Z as TWO_LANES; four
-                                   CTAs per SM */
+  PG_LDPC_KERNEL_Z384      = 3, /* 192 threads per codeblock; Z = 384 with the lifted edge tables in shared
+                                   memory and f16 soft-bit pairs stored once, other Z as TWO_LANES; up to
+                                   three CTAs per SM */
   PG_LDPC_KERNEL_Z384_SPLIT = 4 /* 384 threads per codeblock; Z = 384 as Z384 with each row's edges split
                                    over the two threads of a lane pair, other Z as SPLIT; two CTAs per SM */
 };

@@ -134,12 +134,19 @@ __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_de
                                                                   const uint32_t* __restrict__ cb_bit_offsets,
                                                                   uint8_t* __restrict__ tb_out,
                                                                   uint32_t* __restrict__ tb_crc,
-                                                                  const uint32_t* __restrict__ tabs)
+                                                                  const uint32_t* __restrict__ tabs,
+                                                                  const uint32_t* __restrict__ chunks)
 {
   __shared__ uint32_t byte_tab[256];
   __shared__ uint32_t red[kCrcThreads / 32];
-  const pg_tb_desc    d = tbs[blockIdx.x];
-  if (blockIdx.y * (uint64_t)kTbChunkWords * 32u >= (uint64_t)d.cb_payload_bits * d.nof_cbs) {
+  // The TB and the chunks of this CTA: one chunk of a chunk list (TB | chunk << 16), or chunks
+  // blockIdx.y, blockIdx.y + gridDim.y, ... of TB blockIdx.x.
+  const uint32_t   item        = chunks != nullptr ? chunks[blockIdx.x] : 0u;
+  const uint32_t   tb          = chunks != nullptr ? (item & 0xffffu) : blockIdx.x;
+  const uint32_t   chunk_first = chunks != nullptr ? (item >> 16) : blockIdx.y;
+  const uint32_t   chunk_step  = chunks != nullptr ? 0xffffu : gridDim.y;
+  const pg_tb_desc d           = tbs[tb];
+  if (chunk_first * (uint64_t)kTbChunkWords * 32u >= (uint64_t)d.cb_payload_bits * d.nof_cbs) {
     return; // no chunk of this TB for this CTA (the whole CTA leaves: no barrier is pending)
   }
   uint32_t            g;
@@ -161,7 +168,7 @@ __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_de
   const uint32_t  words    = (L + 31) / 32;
   uint8_t*        out      = tb_out + d.tb_out_offset;
   const uint32_t  tb_bytes = d.tbs_bits / 8;
-  for (uint32_t chunk = blockIdx.y; chunk * kTbChunkWords < words; chunk += gridDim.y) {
+  for (uint32_t chunk = chunk_first; chunk * kTbChunkWords < words; chunk += chunk_step) {
     const uint32_t w0  = chunk * kTbChunkWords + threadIdx.x * kTbWordsPerThread;
     uint32_t       rem = 0;
     uint32_t       end_bit = 0;
@@ -198,7 +205,7 @@ __global__ void __launch_bounds__(kCrcThreads) tb_assemble_kernel(const pg_tb_de
     }
     const uint32_t part = block_xor(contrib, red);
     if (threadIdx.x == 0 && part != 0) {
-      atomicXor(tb_crc + blockIdx.x, part);
+      atomicXor(tb_crc + tb, part);
     }
     __syncthreads();
   }
@@ -262,7 +269,8 @@ int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8
 }
 
 int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const uint8_t* cb_bits,
-                       const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream)
+                       const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream,
+                       const uint32_t* chunks_dev, int nof_chunks)
 {
   if (n == 0) {
     return PG_OK;
@@ -271,9 +279,29 @@ int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const 
                           "cudaMemsetAsync(tb crc)")) {
     return rc;
   }
-  tb_assemble_kernel<<<dim3(n, kTbGridY), kCrcThreads, 0, stream>>>(tbs_dev, cb_bits, cb_bit_offsets, tb_out, tb_crc,
-                                                                     ctx->dev.crc_tabs);
+  if (chunks_dev != nullptr) {
+    if (nof_chunks > 0) {
+      tb_assemble_kernel<<<nof_chunks, kCrcThreads, 0, stream>>>(tbs_dev, cb_bits, cb_bit_offsets, tb_out, tb_crc,
+                                                                 ctx->dev.crc_tabs, chunks_dev);
+    }
+  } else {
+    tb_assemble_kernel<<<dim3(n, kTbGridY), kCrcThreads, 0, stream>>>(tbs_dev, cb_bits, cb_bit_offsets, tb_out, tb_crc,
+                                                                       ctx->dev.crc_tabs, nullptr);
+  }
   return check_cuda(ctx, cudaGetLastError(), "tb_assemble_kernel launch");
+}
+
+void tb_chunk_list(const pg_tb_desc* tbs, int n, std::vector<uint32_t>& out)
+{
+  out.clear();
+  for (int t = 0; t < n; ++t) {
+    const uint64_t bits   = (uint64_t)tbs[t].cb_payload_bits * tbs[t].nof_cbs;
+    const uint64_t words  = (bits + 31) / 32;
+    const uint64_t nchunk = (words + kTbChunkWords - 1) / kTbChunkWords;
+    for (uint64_t c = 0; c < nchunk; ++c) {
+      out.push_back((uint32_t)t | ((uint32_t)c << 16));
+    }
+  }
 }
 
 } // namespace pg

@@ -1136,7 +1136,8 @@ __device__ void decode_codeblock_pair(const pg_ldpc_cb& d, smem_pair_nt_t<NT>& s
 constexpr int kZ384      = 384;
 constexpr int kZH        = 192;
 constexpr int kZThreads  = 192;
-constexpr int kZMaxPerSm = 4;   // resident CTAs per SM (registers and shared memory)
+constexpr int kZMaxPerSm = 4;   // register budget of the launch bounds (80 registers a thread)
+constexpr int kZResidentPerSm = 3; // resident CTAs per SM: shared memory (soft bits + edge tables)
 constexpr int kZ19Keep   = 8;  // v2c kept in registers by rows above kZKeepDeg edges
 constexpr int kZKeepDeg  = 10; // rows of up to this many edges keep v2c, address and selector
 
@@ -1172,14 +1173,28 @@ __device__ __forceinline__ void sts_u32(unsigned char* base, uint32_t off, uint3
   *reinterpret_cast<uint32_t*>(base + off) = v;
 }
 
-// Byte offset in E and byte-permute selector of edge e (global edge index) for thread j (j4 = 4 j).
-__device__ __forceinline__ void z_edge(const int g, const int e, const uint32_t j4, uint32_t& adr, uint32_t& sel)
+// Byte offset in E and byte-permute selector of edge e (global edge index) for thread j (j4 = 4 j),
+// from the CTA's copy of the edge table: {4 (s mod 192), column byte offset, selector when
+// j + s' >= 192, selector otherwise}.
+__device__ __forceinline__ void z_edge(const uint4* __restrict__ zt, const int e, const uint32_t j4, uint32_t& adr,
+                                       uint32_t& sel)
 {
-  const uint32_t t4 = j4 + c_z_sp4[g][e];
+  const uint4    c  = zt[e];
+  const uint32_t t4 = j4 + c.x;
   const uint32_t k4 = __viaddmin_u32(t4, 0u - 4u * kZH, t4); // (j + s') mod 192, times 4
-  const uint32_t sw = c_z_sel[g][e];
-  sel               = k4 == t4 ? sw ^ 0x2222u : sw;
-  adr               = k4 + c_z_col[g][e];
+  sel               = k4 == t4 ? c.w : c.z;
+  adr               = k4 + c.y;
+}
+
+// The edge tables of both base graphs in shared memory (one copy per CTA, filled once per launch).
+__device__ __forceinline__ void z_load_edge_tables(uint4* zt)
+{
+  for (int i = threadIdx.x; i < 2 * pg::kBg1Edges; i += blockDim.x) {
+    const int      g = i / pg::kBg1Edges, e = i - g * pg::kBg1Edges;
+    const uint32_t sw = c_z_sel[g][e];
+    zt[i]             = make_uint4(c_z_sp4[g][e], c_z_col[g][e], sw, sw ^ 0x2222u);
+  }
+  __syncthreads();
 }
 
 // One layer (base-graph row of degree DEG, first edge e0) for thread j. Rows of up to kZKeepDeg
@@ -1187,7 +1202,7 @@ __device__ __forceinline__ void z_edge(const int g, const int e, const uint32_t 
 // the v2c of their first kZ19Keep edges and recompute the rest (the soft bits and messages they
 // read are not yet overwritten), so that four CTAs fit an SM without spills.
 template <int DEG, bool FIRST>
-__device__ __forceinline__ void row_update_z(const int g, const int e0, const uint32_t j4, unsigned char* E,
+__device__ __forceinline__ void row_update_z(const uint4* __restrict__ zt, const int e0, const uint32_t j4, unsigned char* E,
                                              uint16_t* __restrict__ c2v_row)
 {
   constexpr bool KEEP = DEG <= kZKeepDeg;
@@ -1198,7 +1213,7 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
 #pragma unroll
   for (int e = 0; e < DEG; ++e) {
     uint32_t a, s;
-    z_edge(g, e0 + e, j4, a, s);
+    z_edge(zt, e0 + e, j4, a, s);
     if constexpr (KEEP) {
       adr[e] = a;
       sel[e] = s;
@@ -1223,7 +1238,7 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
       a = adr[e];
       s = sel[e];
     } else {
-      z_edge(g, e0 + e, j4, a, s);
+      z_edge(zt, e0 + e, j4, a, s);
     }
     const uint32_t vv  = e < NV ? v[e < NV ? e : 0]
                                 : pair_v2c<FIRST>(__byte_perm(lds_u32(E, a), 0, s), c2v_row + e * kZH);
@@ -1242,7 +1257,7 @@ __device__ __forceinline__ void row_update_z(const int g, const int e0, const ui
 // and no sign), the two partial (min1, min2, sign) meet through one shuffle, and each thread updates
 // its own edges.
 template <int DEG, bool FIRST>
-__device__ __forceinline__ void row_update_z_split(const int g, const int e0, const uint32_t j4, const int t,
+__device__ __forceinline__ void row_update_z_split(const uint4* __restrict__ zt, const int e0, const uint32_t j4, const int t,
                                                    unsigned char* E, uint16_t* __restrict__ c2v_row)
 {
   constexpr int  NE   = (DEG + 1) / 2;
@@ -1256,7 +1271,7 @@ __device__ __forceinline__ void row_update_z_split(const int g, const int e0, co
     uint32_t   vv    = kH120;
     if (valid) {
       uint32_t a, s;
-      z_edge(g, e0 + e, j4, a, s);
+      z_edge(zt, e0 + e, j4, a, s);
       if constexpr (KEEP) {
         adr[k] = a;
         sel[k] = s;
@@ -1287,7 +1302,7 @@ __device__ __forceinline__ void row_update_z_split(const int g, const int e0, co
         a = adr[k];
         s = sel[k];
       } else {
-        z_edge(g, e0 + e, j4, a, s);
+        z_edge(zt, e0 + e, j4, a, s);
       }
       const uint32_t vv  = v[k];
       const uint32_t mag = h2_fma(nds, h2_ne(vv & kAbs, m1), s2);
@@ -1302,35 +1317,35 @@ __device__ __forceinline__ void row_update_z_split(const int g, const int e0, co
 }
 
 template <bool FIRST>
-__device__ __forceinline__ void row_dispatch_z_split(int deg, int g, int e0, uint32_t j4, int t, unsigned char* E,
+__device__ __forceinline__ void row_dispatch_z_split(int deg, const uint4* zt, int e0, uint32_t j4, int t, unsigned char* E,
                                                      uint16_t* c2v_row)
 {
   switch (deg) {
-    case 3: row_update_z_split<3, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 4: row_update_z_split<4, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 5: row_update_z_split<5, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 6: row_update_z_split<6, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 7: row_update_z_split<7, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 8: row_update_z_split<8, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 9: row_update_z_split<9, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    case 10: row_update_z_split<10, FIRST>(g, e0, j4, t, E, c2v_row); break;
-    default: row_update_z_split<19, FIRST>(g, e0, j4, t, E, c2v_row); break;
+    case 3: row_update_z_split<3, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 4: row_update_z_split<4, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 5: row_update_z_split<5, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 6: row_update_z_split<6, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 7: row_update_z_split<7, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 8: row_update_z_split<8, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 9: row_update_z_split<9, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    case 10: row_update_z_split<10, FIRST>(zt, e0, j4, t, E, c2v_row); break;
+    default: row_update_z_split<19, FIRST>(zt, e0, j4, t, E, c2v_row); break;
   }
 }
 
 template <bool FIRST>
-__device__ __forceinline__ void row_dispatch_z(int deg, int g, int e0, uint32_t j4, unsigned char* E, uint16_t* c2v_row)
+__device__ __forceinline__ void row_dispatch_z(int deg, const uint4* zt, int e0, uint32_t j4, unsigned char* E, uint16_t* c2v_row)
 {
   switch (deg) {
-    case 3: row_update_z<3, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 4: row_update_z<4, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 5: row_update_z<5, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 6: row_update_z<6, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 7: row_update_z<7, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 8: row_update_z<8, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 9: row_update_z<9, FIRST>(g, e0, j4, E, c2v_row); break;
-    case 10: row_update_z<10, FIRST>(g, e0, j4, E, c2v_row); break;
-    default: row_update_z<19, FIRST>(g, e0, j4, E, c2v_row); break;
+    case 3: row_update_z<3, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 4: row_update_z<4, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 5: row_update_z<5, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 6: row_update_z<6, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 7: row_update_z<7, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 8: row_update_z<8, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 9: row_update_z<9, FIRST>(zt, e0, j4, E, c2v_row); break;
+    case 10: row_update_z<10, FIRST>(zt, e0, j4, E, c2v_row); break;
+    default: row_update_z<19, FIRST>(zt, e0, j4, E, c2v_row); break;
   }
 }
 
@@ -1343,7 +1358,8 @@ __device__ __forceinline__ bool z_hard(uint32_t h)
 // Decodes codeblock cb (Z = 384) with check-to-variable slab `slab`: NT threads, T = NT / 192 per
 // lane pair (T = 2: each row's edges split between the pair's two threads).
 template <int NT>
-__device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, const int8_t* __restrict__ llrs,
+__device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, const uint4* __restrict__ ztab,
+                                      const int8_t* __restrict__ llrs,
                                       uint8_t* __restrict__ bits, int32_t* __restrict__ iterations,
                                       int8_t* __restrict__ c2v_all, const uint32_t* __restrict__ crc_pow, const int cb,
                                       const int slab)
@@ -1359,6 +1375,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, 
     return;
   }
   const int      g        = bg - 1;
+  const uint4*   zt       = ztab + g * pg::kBg1Edges;
   const int      Kb       = bg == 1 ? 22 : 10;
   const int      nrows    = bg == 1 ? pg::kBg1Rows : pg::kBg2Rows;
   const int      nfull    = bg == 1 ? 68 : 52;
@@ -1457,15 +1474,15 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, 
         uint16_t* c2v_row = c2v + (size_t)e0 * kZH + jp;
         if (T == 1) {
           if (it == 0) {
-            row_dispatch_z<true>(deg, g, e0, j4, E, c2v_row);
+            row_dispatch_z<true>(deg, zt, e0, j4, E, c2v_row);
           } else {
-            row_dispatch_z<false>(deg, g, e0, j4, E, c2v_row);
+            row_dispatch_z<false>(deg, zt, e0, j4, E, c2v_row);
           }
         } else {
           if (it == 0) {
-            row_dispatch_z_split<true>(deg, g, e0, j4, tp, E, c2v_row);
+            row_dispatch_z_split<true>(deg, zt, e0, j4, tp, E, c2v_row);
           } else {
-            row_dispatch_z_split<false>(deg, g, e0, j4, tp, E, c2v_row);
+            row_dispatch_z_split<false>(deg, zt, e0, j4, tp, E, c2v_row);
           }
         }
       }
@@ -1522,7 +1539,7 @@ __device__ void decode_codeblock_z384(const pg_ldpc_cb& d, smem_z_nt_t<NT>& sm, 
       uint32_t  parity = 0;
       for (int e = 0; e < deg; ++e) {
         uint32_t a, s;
-        z_edge(g, e0 + e, 4u * (uint32_t)tid, a, s);
+        z_edge(zt, e0 + e, 4u * (uint32_t)tid, a, s);
         const uint32_t x  = __byte_perm(lds_u32(E, a), 0, s);
         const uint32_t lo = x & 0xffffu, hi = x >> 16;
         bad |= ((lo & 0x7fffu) == 0) | ((hi & 0x7fffu) == 0);
@@ -1568,7 +1585,9 @@ __global__ void __launch_bounds__(kZThreads, kZMaxPerSm) ldpc_decode_z_kernel(co
                                                                       int* __restrict__ counter)
 {
   extern __shared__ __align__(16) unsigned char smem_z_raw[];
-  __shared__ int s_work;
+  __shared__ int   s_work;
+  __shared__ uint4 s_ztab[2 * pg::kBg1Edges];
+  z_load_edge_tables(s_ztab);
   for (;;) {
     if (threadIdx.x == 0) {
       s_work = atomicAdd(counter, 1);
@@ -1582,8 +1601,8 @@ __global__ void __launch_bounds__(kZThreads, kZMaxPerSm) ldpc_decode_z_kernel(co
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
     if (d.lifting_size == kZ384) {
-      decode_codeblock_z384<kZThreads>(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), llrs, bits, iterations, c2v_all,
-                                       crc_pow, cb, blockIdx.x);
+      decode_codeblock_z384<kZThreads>(d, *reinterpret_cast<smem_z_t*>(smem_z_raw), s_ztab, llrs, bits, iterations,
+                                       c2v_all, crc_pow, cb, blockIdx.x);
     } else if (d.lifting_size > kX2Threads) {
       decode_codeblock_pair<kX2Threads, 1>(d, *reinterpret_cast<smem_pair_t*>(smem_z_raw), llrs, bits, iterations,
                                            c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
@@ -1608,7 +1627,9 @@ __global__ void __launch_bounds__(kZsThreads, kZsMaxPerSm) ldpc_decode_zs_kernel
     const uint16_t* __restrict__ scale_tab, const uint32_t* __restrict__ order, int n, int* __restrict__ counter)
 {
   extern __shared__ __align__(16) unsigned char smem_zs_raw[];
-  __shared__ int s_work;
+  __shared__ int   s_work;
+  __shared__ uint4 s_ztab[2 * pg::kBg1Edges];
+  z_load_edge_tables(s_ztab);
   for (;;) {
     if (threadIdx.x == 0) {
       s_work = atomicAdd(counter, 1);
@@ -1622,8 +1643,8 @@ __global__ void __launch_bounds__(kZsThreads, kZsMaxPerSm) ldpc_decode_zs_kernel
     const int        cb = order != nullptr ? (int)order[w] : w;
     const pg_ldpc_cb d  = descs[cb];
     if (d.lifting_size == kZ384) {
-      decode_codeblock_z384<kZsThreads>(d, *reinterpret_cast<smem_z_nt_t<kZsThreads>*>(smem_zs_raw), llrs, bits,
-                                        iterations, c2v_all, crc_pow, cb, blockIdx.x);
+      decode_codeblock_z384<kZsThreads>(d, *reinterpret_cast<smem_z_nt_t<kZsThreads>*>(smem_zs_raw), s_ztab, llrs,
+                                        bits, iterations, c2v_all, crc_pow, cb, blockIdx.x);
     } else if (d.lifting_size > kX2Threads && (d.lifting_size & 1) == 0) {
       decode_codeblock_pair<kSplitThreads, 2>(d, *reinterpret_cast<smem_split_pair_t*>(smem_zs_raw), llrs, bits,
                                               iterations, c2v_all, crc_pow, scale_tab, cb, blockIdx.x);
@@ -2079,7 +2100,7 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, stream, rec_flags);
   }
-  // PG_LDPC_ROUTE_Z: the Z = 384 kernel (four per SM, pair mode and one-lane arithmetic for the
+  // PG_LDPC_ROUTE_Z: the Z = 384 kernel (three per SM, pair mode and one-lane arithmetic for the
   // other lifting sizes);
   // PG_LDPC_ROUTE_SPLIT: the split kernel decodes every codeblock (two CTAs per SM);
   // PG_LDPC_ROUTE_X2: the two-lanes-per-thread kernel (four per SM); neither: ldpc_decode_kernel
@@ -2092,7 +2113,7 @@ int ldpc_launch_persistent(pg_context* ctx, const pg_ldpc_cb* descs_dev, int n, 
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
     rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_zs_kernel launch");
   } else if (kinds & PG_LDPC_ROUTE_Z) {
-    const int grid_z = std::max(1, std::min(n, std::min(max_ctas, kZMaxPerSm * ctx->sm_count)));
+    const int grid_z = std::max(1, std::min(n, std::min(max_ctas, kZResidentPerSm * ctx->sm_count)));
     ldpc_decode_z_kernel<<<grid_z, kZThreads, kZSmem, stream>>>(
         descs_dev, llrs, bits, iterations, c2v, ctx->dev.crc_pow, ctx->dev.ldpc_scale, order, n, counter + 1);
     rc = check_cuda(ctx, cudaGetLastError(), "ldpc_decode_z_kernel launch");

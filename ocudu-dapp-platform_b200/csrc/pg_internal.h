@@ -161,8 +161,13 @@ int rm_prefill_launch(pg_context* ctx, const pg_rm_cb* descs_dev, int n, const u
 void crc_tables_host(uint32_t* tab);
 int crc_launch(pg_context* ctx, const pg_crc_item* items_dev, int n, const uint8_t* data, uint32_t* out,
                cudaStream_t stream);
+// TB assembly and TB CRC. chunks_dev (may be NULL: a 2-D grid over every TB) lists the work items
+// TB | chunk << 16 of tb_chunk_list, one CTA each.
 int tb_assemble_launch(pg_context* ctx, const pg_tb_desc* tbs_dev, int n, const uint8_t* cb_bits,
-                       const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream);
+                       const uint32_t* cb_bit_offsets, uint8_t* tb_out, uint32_t* tb_crc, cudaStream_t stream,
+                       const uint32_t* chunks_dev = nullptr, int nof_chunks = 0);
+// The 1,024-word chunks of every TB (n <= 65,535 TBs).
+void tb_chunk_list(const pg_tb_desc* tbs, int n, std::vector<uint32_t>& out);
 
 int demap_upload_tables(pg_context* ctx);
 int est_upload_tables(pg_context* ctx);

@@ -76,6 +76,8 @@ struct pg_pusch_plan {
   int8_t*         d_c2v    = nullptr;
   uint32_t*       d_order  = nullptr; // per-execution work order (device ordering)
   uint32_t*       d_order_static = nullptr; // largest codeblocks first, fixed at creation
+  uint32_t*       d_tb_chunks    = nullptr; // TB-assembly work items (TB | chunk << 16)
+  int             tb_nchunks     = 0;
   uint8_t*        d_keys   = nullptr; // work-order keys of the codeblocks // LDPC work order: largest codeblocks first
   int*            d_counter = nullptr; // work counter of the persistent decoder
   uint32_t*       d_grid   = nullptr; // grids of execute_host
@@ -300,7 +302,8 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     rc = check_cuda(ctx, cudaMemsetAsync(tb_out, 0, p->tb_bytes, s), "cudaMemsetAsync(tb)");
   }
   if (rc == PG_OK) {
-    rc = tb_assemble_launch(ctx, p->d_tb, p->nof_ues, p->d_cb_bits, p->d_cb_off, tb_out, p->d_tb_crc, s);
+    rc = tb_assemble_launch(ctx, p->d_tb, p->nof_ues, p->d_cb_bits, p->d_cb_off, tb_out, p->d_tb_crc, s, p->d_tb_chunks,
+                            p->tb_nchunks);
   }
   if (rc == PG_OK) {
     sch_results_kernel<<<(p->nof_ues + 127) / 128, 128, 0, s>>>(p->d_tb, p->d_ues, p->nof_ues, p->d_iters, p->d_tb_crc,
@@ -520,7 +523,11 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_cb_off = o_tb + al(w.tbd.size() * sizeof(pg_tb_desc));
   const size_t o_order  = o_cb_off + al(w.cb_bit_off.size() * 4);
   const size_t o_ostat  = o_order + al(order.size() * 4);
-  const size_t o_seqoff = o_ostat + al(order.size() * 4);
+  std::vector<uint32_t> tb_chunks;
+  tb_chunk_list(w.tbd.data(), (int)w.tbd.size(), tb_chunks);
+  p->tb_nchunks         = (int)tb_chunks.size();
+  const size_t o_tbch   = o_ostat + al(order.size() * 4);
+  const size_t o_seqoff = o_tbch + al(tb_chunks.size() * 4);
   const size_t o_reoff  = o_seqoff + al((size_t)nof_ues * 4);
   std::vector<uint32_t> est_work;
   uint32_t              pilot_words = 0;
@@ -595,6 +602,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   p->d_c2v     = reinterpret_cast<int8_t*>(b + o_c2v);
   p->d_order   = reinterpret_cast<uint32_t*>(b + o_order);
   p->d_order_static = reinterpret_cast<uint32_t*>(b + o_ostat);
+  p->d_tb_chunks    = reinterpret_cast<uint32_t*>(b + o_tbch);
   p->d_counter = reinterpret_cast<int*>(b + o_cnt);
   p->d_keys    = b + o_keys;
   p->d_grid    = reinterpret_cast<uint32_t*>(b + o_grid);
@@ -623,6 +631,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   std::memcpy(h + o_cb_off, w.cb_bit_off.data(), w.cb_bit_off.size() * 4);
   std::memcpy(h + o_order, order.data(), order.size() * 4);
   std::memcpy(h + o_ostat, order.data(), order.size() * 4);
+  std::memcpy(h + o_tbch, tb_chunks.data(), tb_chunks.size() * 4);
   std::memcpy(h + o_seqoff, seq_off.data(), (size_t)nof_ues * 4);
   std::memcpy(h + o_reoff, tile_map.data(), tile_map.size() * 4);
   std::memcpy(h + o_ework, est_work.data(), est_work.size() * 4);

@@ -10,7 +10,8 @@
 //                           bf16 unit apart (over 99 % equal), noise variances within 1e-4
 //   dapp_receiver           LLRs (before descrambling) against the reference's channel_equalizer (MMSE,
 //                           tx scaling 1) + demodulation_mapper on the module's own estimates: |diff|
-//                           <= 1, at least 99.9 % equal, post-equalisation noise within 2.5e-4; and
+//                           <= 1, at least 99.9 % equal, post-equalisation noise within 5e-4 (the
+//                           reference's equaliser divides by 14-bit reciprocal estimates); and
 //                           against the whole reference chain (its port_channel_estimator too): at
 //                           least 99.5 % equal
 //   dapp_bypass             DM-RS type 2 and device-resident tensors are declined (BYPASS),
@@ -572,7 +573,7 @@ void check_receiver(module_handle& mh, void* w_rx, uint32_t rx_id, void* w_est, 
       if (std::isfinite(var[i]) || std::isfinite(post_noise[i])) {
         const double e = std::abs(var[i] - post_noise[i]) / std::max(std::abs(var[i]), 1e-3f * max_v);
         worst_var      = std::max(worst_var, e);
-        ok             = ok && e <= 2.5e-4;
+        ok             = ok && e <= 5e-4; // the reference's equaliser: 14-bit reciprocal estimates
       }
     }
     // (b) the reference's whole chain from its own estimator.
