@@ -64,7 +64,7 @@ LDPC_KERNEL_NAMES = ["ldpc_decode_kernel (one lifted lane per thread)",
 LDPC_NCU = {
     1: {"traffic": 24246528, "pipes": {"alu": 55.5, "fma": 32.3, "lsu": 24.9, "issue_active": 59.6,
                                        "sm_active_pct_of_elapsed": 60.4}},
-    3: {"traffic": 11592960, "pipes": {"alu": 48.3, "issue_active": 48.9, "sm_active_pct_of_elapsed": 82.2}},
+    3: {"traffic": 11546880, "pipes": {"alu": 50.3, "issue_active": 53.3, "sm_active_pct_of_elapsed": 81.0}},
 }
 # Integer-instruction throughput probe (the LDPC roofline denominator), built by
 # ocudu-dapp-platform_b200/measure/Makefile.
