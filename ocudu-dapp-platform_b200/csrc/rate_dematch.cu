@@ -39,6 +39,7 @@ __device__ __forceinline__ int llr_sum(int a, int b)
 // Rows of the de-interleaver matrix per tile of the transposing path: a tile reads rows*Qm <= 2 KB
 // of input.
 constexpr int kRmTileRows = 256;
+constexpr int kRmRepBatch = 4; // repetitions whose loads a thread issues together
 
 __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb* __restrict__ cbs,
                                                                   const int8_t* __restrict__ in_all,
@@ -133,21 +134,33 @@ __global__ void __launch_bounds__(kRmThreads) rate_dematch_kernel(const pg_rm_cb
     int       t   = v - v0;
     t             = t < 0 ? t + V : t;
     int       acc = nd ? 0 : (int)out[p];
-    for (; t < E; t += V) {
-      int src = t;
-      if (Qm > 1) {
-        int q = __float2int_rz((float)t * inv_kq);
-        int r = t - q * Kq;
-        if (r < 0) {
-          --q;
-          r += Kq;
-        } else if (r >= Kq) {
-          ++q;
-          r -= Kq;
+    // Four repetitions per step: their loads are issued together, the sums taken in order.
+    for (; t < E; t += kRmRepBatch * V) {
+      int x[kRmRepBatch];
+#pragma unroll
+      for (int u = 0; u < kRmRepBatch; ++u) {
+        const int tu = t + u * V;
+        int       src = tu;
+        if (Qm > 1) {
+          int q = __float2int_rz((float)tu * inv_kq);
+          int r = tu - q * Kq;
+          if (r < 0) {
+            --q;
+            r += Kq;
+          } else if (r >= Kq) {
+            ++q;
+            r -= Kq;
+          }
+          src = r * Qm + q;
         }
-        src = r * Qm + q;
+        x[u] = tu < E ? (int)in[src] : 0;
       }
-      acc = llr_sum(acc, in[src]);
+#pragma unroll
+      for (int u = 0; u < kRmRepBatch; ++u) {
+        if (t + u * V < E) {
+          acc = llr_sum(acc, x[u]);
+        }
+      }
     }
     out[p] = (int8_t)acc;
   }
