@@ -796,6 +796,39 @@ typedef struct pg_uci_short_block {
 int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* items, int n, const int8_t* llrs,
                                      uint8_t* bits, uint8_t* valid, void* stream);
 
+/* One polar-coded UCI message of 12 to 1706 bits: uci_decoder_impl::decode_codeword_polar
+ * (lib/phy/upper/channel_processors/uci/uci_decoder_impl.cpp:25-99), called by
+ * uci_decoder_impl::decode above 11 bits (:101-111): segmentation into one or two codeblocks
+ * (include/ocudu/ran/uci/uci_info.h:22-47), per codeblock the polar code of polar_code_impl::set
+ * (lib/phy/upper/channel_coding/polar/polar_code_impl.cpp:432-480, uplink nMax = 10, channel
+ * interleaver present), rate dematching, simplified successive-cancellation decoding, deallocation
+ * and the CRC6 / CRC11 check. */
+typedef struct pg_uci_polar {
+  uint32_t llr_offset; /* demultiplexed soft bits */
+  uint32_t nof_llrs;   /* E of the message (both codeblocks) */
+  uint32_t out_offset; /* nof_bits output bytes, one bit per byte */
+  uint16_t nof_bits;   /* A, 12..1706 */
+  uint16_t reserved;
+} pg_uci_polar;
+
+/* Decodes n messages (items: host array; llrs, bits, valid: device buffers). valid[i] = 1 when
+ * every codeblock of message i passes its CRC (the reference's uci_status::valid). A message whose
+ * code the reference's polar_code_impl rejects (E above 8192 per codeblock, K outside 18..25 and
+ * 31..1023, E not above K + nPC) is PG_ERR_INVALID. */
+int pg_uci_polar_decode_device(pg_context* ctx, const pg_uci_polar* items, int n, const int8_t* llrs, uint8_t* bits,
+                               uint8_t* valid, void* stream);
+
+/* The polar code of one codeblock as pg_uci_polar_decode_device builds it (host computation, no
+ * GPU): polar_code_impl::set for K (payload + CRC + filler bits) and E. */
+typedef struct pg_polar_code_info {
+  uint16_t n, N, K, E;
+  uint8_t  nPC, nWmPC;
+  uint16_t pc_set[4];     /* sorted parity-check sub-channels, unused entries 1024 */
+  uint32_t k_set[32];     /* bit i of word i / 32: sub-channel i carries message, CRC or parity */
+  uint16_t subblock[1024]; /* sub-block interleaver J(0 .. N - 1) */
+} pg_polar_code_info;
+int pg_polar_code(uint32_t K, uint32_t E, pg_polar_code_info* out);
+
 
 /* Pipelined host execution of consecutive slots: pg_pusch_plan_submit_host enqueues one slot and
  * returns without waiting - the host-to-device copy of its grids runs on a stream of its own into

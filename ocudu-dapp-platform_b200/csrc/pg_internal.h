@@ -90,7 +90,7 @@ struct pg_context {
   bool                le_recorded    = false;
   cudaEvent_t         ev_desc        = nullptr; // completion of the last descriptor upload
   bool                desc_pending   = false;
-  pg::staging_slot    slots[7];                  // rate-dematch, CRC, TB, PUSCH, UE and UCI work lists
+  pg::staging_slot    slots[8];                  // rate-dematch, CRC, TB, PUSCH, UE and UCI work lists
   void*               est_partials     = nullptr;  // partial sums of the batched channel estimation
   size_t              est_partials_cap = 0;
   void*               scratch_a      = nullptr;  // growable device scratch of the _host entries
@@ -131,12 +131,15 @@ int uci_demux_launch(pg_context* ctx, const void* blob_dev, const uci_demux_work
 std::string uci_short_blob(const pg_uci_short_block* items, int n, std::vector<uint8_t>& blob);
 int uci_detect_launch(pg_context* ctx, const void* items_dev, int n, const int8_t* llrs, uint8_t* bits, uint8_t* valid,
                       cudaStream_t s);
+// Polar-coded UCI: decodes n messages (codes built on the host, descriptors staged, one launch).
+int uci_polar_launch(pg_context* ctx, const pg_uci_polar* items, int n, const int8_t* llrs, uint8_t* bits,
+                     uint8_t* valid, cudaStream_t s);
 // Open Fronthaul BFP: compressed bytes per PRB, and decompression of nof_prb PRBs into cbf16.
 int bfp_prb_bytes(int data_width);
 int bfp_decompress_launch(pg_context* ctx, const uint8_t* in, uint32_t nof_prb, int data_width, uint32_t* out,
                           cudaStream_t s);
 
-enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4, SLOT_UCI = 5, SLOT_UCI_SHORT = 6 };
+enum { SLOT_RM = 0, SLOT_CRC = 1, SLOT_TB = 2, SLOT_PUSCH = 3, SLOT_UE = 4, SLOT_UCI = 5, SLOT_UCI_SHORT = 6, SLOT_UCI_POLAR = 7 };
 
 // Copies `bytes` of host descriptors to the slot's device buffer on stream s (growing it when
 // needed); returns the device pointer in *dev. release_slot_after marks the slot busy until the

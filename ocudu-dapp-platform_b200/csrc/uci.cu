@@ -768,7 +768,8 @@ int pg_ulsch_demultiplex_device(pg_context* ctx, const pg_ulsch_demux_config* cf
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
   }
-  return rc;
+  // The staged blob stays in use until the kernel has read it.
+  return rc != PG_OK ? rc : release_slot_after(ctx, SLOT_UCI, s);
 }
 
 int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* items, int n, const int8_t* llrs,
@@ -801,7 +802,7 @@ int pg_uci_short_block_detect_device(pg_context* ctx, const pg_uci_short_block* 
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
   }
-  return rc;
+  return rc != PG_OK ? rc : release_slot_after(ctx, SLOT_UCI_SHORT, s);
 }
 
 } // extern "C"

@@ -136,6 +136,17 @@ class PgUciShortBlock(ctypes.Structure):
                 ("nof_bits", ctypes.c_uint8), ("modulation_order", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 2)]
 
 
+class PgUciPolar(ctypes.Structure):
+    _fields_ = [("llr_offset", ctypes.c_uint32), ("nof_llrs", ctypes.c_uint32), ("out_offset", ctypes.c_uint32),
+                ("nof_bits", ctypes.c_uint16), ("reserved", ctypes.c_uint16)]
+
+
+class PgPolarCodeInfo(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint16), ("N", ctypes.c_uint16), ("K", ctypes.c_uint16), ("E", ctypes.c_uint16),
+                ("nPC", ctypes.c_uint8), ("nWmPC", ctypes.c_uint8), ("pc_set", ctypes.c_uint16 * 4),
+                ("k_set", ctypes.c_uint32 * 32), ("subblock", ctypes.c_uint16 * 1024)]
+
+
 class PgPortEstimateCfg(ctypes.Structure):
     _fields_ = [("grid_nof_subc", ctypes.c_uint32), ("scaling", ctypes.c_float), ("rb_start", ctypes.c_uint16),
                 ("nof_rb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16), ("first_symbol", ctypes.c_uint8),
@@ -237,6 +248,8 @@ SIGNATURES = {
                                                       _VP, _VP]),
     "pg_ulsch_demultiplex_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP]),
     "pg_uci_short_block_detect_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_uci_polar_decode_device": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP, _VP, _VP]),
+    "pg_polar_code": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, _VP]),
     "pg_pusch_plan_get_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_tuning": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_autotune": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _VP, _VP]),

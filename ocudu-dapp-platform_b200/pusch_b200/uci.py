@@ -99,6 +99,56 @@ class ShortBlockDetector:
         return out
 
 
+class PolarUciDecoder:
+    """Polar-coded UCI messages of 12 to 1706 bits (pg_uci_polar_decode_device): the reference's
+    uci_decoder::decode above 11 bits (lib/phy/upper/channel_processors/uci/uci_decoder_impl.cpp:25-111)."""
+
+    def __init__(self, context: _native.Context):
+        self.ctx = context
+        self.lib = context.lib
+
+    def decode(self, messages: Sequence[Tuple[int, np.ndarray]]) -> List[Tuple[np.ndarray, bool]]:
+        """messages: (nof_bits, soft bits); returns (bits, valid) per message."""
+        import torch
+        n = len(messages)
+        if n == 0:
+            return []
+        items = (_native.PgUciPolar * n)()
+        off, out_off = 0, 0
+        for i, (A, llr) in enumerate(messages):
+            items[i].llr_offset, items[i].nof_llrs, items[i].out_offset = off, int(np.asarray(llr).size), out_off
+            items[i].nof_bits = A
+            off += int(np.asarray(llr).size)
+            out_off += A
+        d_in = torch.from_numpy(np.ascontiguousarray(np.concatenate([m[1] for m in messages]), dtype=np.int8)).cuda()
+        d_bits = torch.zeros(out_off, dtype=torch.uint8, device="cuda")
+        d_valid = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        st = torch.cuda.current_stream()
+        self.ctx.check(self.lib.pg_uci_polar_decode_device(self.ctx.handle, ctypes.addressof(items), n,
+                                                           d_in.data_ptr(), d_bits.data_ptr(), d_valid.data_ptr(),
+                                                           st.cuda_stream))
+        st.synchronize()
+        bits, valid = d_bits.cpu().numpy(), d_valid.cpu().numpy()
+        out, o = [], 0
+        for i, (A, _) in enumerate(messages):
+            out.append((bits[o:o + A].copy(), bool(valid[i])))
+            o += A
+        return out
+
+
+def polar_code(K, E):
+    """The polar code pg_uci_polar_decode_device builds for one codeblock (pg_polar_code; host only):
+    dict with n, N, nPC, nWmPC, k_set (0/1 per sub-channel), pc_set and subblock (N entries), or
+    None when the reference's polar_code_impl rejects (K, E)."""
+    info = _native.PgPolarCodeInfo()
+    if _native.load().pg_polar_code(K, E, ctypes.byref(info)) != 0:
+        return None
+    N = info.N
+    kset = np.array([(info.k_set[i >> 5] >> (i & 31)) & 1 for i in range(N)], np.uint8)
+    return dict(n=info.n, N=N, nPC=info.nPC, nWmPC=info.nWmPC, k_set=kset, pc_set=list(info.pc_set),
+                subblock=np.array(info.subblock[:N], np.uint16))
+
+
 def ulsch_information(tbs_bits, base_graph, modulation_order, nof_layers, nof_rb, start_symbol, nof_symbols,
                       dmrs_symbol_mask, nof_harq_ack_bits=0, nof_csi_part1_bits=0, nof_csi_part2_bits=0,
                       alpha_scaling=1.0, beta_offset_harq_ack=20.0, beta_offset_csi_part1=6.25,

@@ -270,6 +270,40 @@ class Ref:
         ok = self.lib.ref_short_block_detect(K, _ptr(llrs), llrs.size, qm, _ptr(out))
         return out, bool(ok)
 
+    def polar_code(self, K, E):
+        """The reference's polar_code_impl::set (uplink): dict as pusch_b200.uci.polar_code, or None."""
+        N = 1024
+        info = np.zeros(4, np.int32)
+        kset = np.zeros(N, np.uint8)
+        pc = np.zeros(4, np.uint16)
+        sub = np.zeros(N, np.uint16)
+        f = self.lib.ref_polar_code
+        f.argtypes = [ctypes.c_uint, ctypes.c_uint] + [ctypes.c_void_p] * 4
+        if not f(K, E, _ptr(info), _ptr(kset), _ptr(pc), _ptr(sub)):
+            return None
+        n_ = int(info[1])
+        return dict(n=int(info[0]), N=n_, nPC=int(info[2]), k_set=kset[:n_].copy(), pc_set=[int(x) for x in pc],
+                    subblock=sub[:n_].copy())
+
+    def uci_polar_encode(self, msg, E):
+        """Polar-coded UCI test vector: A message bits -> E bits (segmentation, CRC, polar encoding,
+        rate matching with the channel interleaver, all by the reference's pieces)."""
+        msg = np.ascontiguousarray(msg, dtype=np.uint8)
+        out = np.zeros(E, np.uint8)
+        f = self.lib.ref_uci_polar_encode
+        f.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+        f(msg.size, _ptr(msg), E, _ptr(out))
+        return out
+
+    def uci_polar_decode(self, A, llrs):
+        """The reference's uci_decoder::decode of an A-bit polar-coded message: (bits, valid)."""
+        llrs = np.ascontiguousarray(llrs, dtype=np.int8)
+        out = np.zeros(A, np.uint8)
+        f = self.lib.ref_uci_polar_decode
+        f.argtypes = [ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint, ctypes.c_void_p]
+        ok = f(A, _ptr(llrs), llrs.size, _ptr(out))
+        return out, bool(ok)
+
     def bfp_compress(self, width, iq_words, generic=False):
         """The reference's BFP compressor on complex bf16 words (12 per PRB): compressed bytes."""
         iq_words = np.ascontiguousarray(iq_words, dtype=np.uint32)

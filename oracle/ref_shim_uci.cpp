@@ -4,10 +4,22 @@
 //                                      (lib/phy/upper/channel_processors/pusch/ulsch_demultiplex_impl.cpp)
 //   short_block_detector::detect       include/ocudu/phy/upper/channel_coding/short/short_block_detector.h
 //   short_block_encoder::encode        include/ocudu/phy/upper/channel_coding/short/short_block_encoder.h
+//   uci_decoder::decode (polar)        lib/phy/upper/channel_processors/uci/uci_decoder_impl.cpp:25-111
+//   polar_code::set                    lib/phy/upper/channel_coding/polar/polar_code_impl.cpp:432-480
+//   a polar UCI test-vector encoder    polar_allocator, polar_encoder, polar_rate_matcher
 // The scrambling sequence handed to the demultiplexer is the reference's own pseudo-random
 // generator output for c_init, as pusch_demodulator_impl produces it.
 
+#include "lib/phy/upper/channel_coding/polar/polar_allocator_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_code_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_deallocator_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_decoder_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_encoder_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_rate_dematcher_impl.h"
+#include "lib/phy/upper/channel_coding/polar/polar_rate_matcher_impl.h"
 #include "lib/phy/upper/channel_coding/short/short_block_detector_impl.h"
+#include "lib/phy/upper/channel_processors/uci/uci_decoder_impl.h"
+#include "ocudu/phy/upper/channel_coding/channel_coding_factories.h"
 #include "lib/phy/upper/channel_coding/short/short_block_encoder_impl.h"
 #include "lib/phy/upper/channel_processors/pusch/ulsch_demultiplex_impl.h"
 #include "ocudu/adt/bit_buffer.h"
@@ -162,6 +174,88 @@ int ref_short_block_detect(int K, const int8_t* llrs, int E, int qm, uint8_t* ou
     in[i] = llrs[i];
   }
   return det.detect(span<uint8_t>(out, K), in, mod_from_qm(qm)) ? 1 : 0;
+}
+
+// polar_code_impl::set for (K, E) on the uplink (nMax 10, channel interleaver present): info[0..3] =
+// n, N, nPC, valid (0 when the reference's range checks fail); kset[0..N) = 1 for K_set
+// sub-channels; pc[0..4) = PC_set; subblock[0..N) = the sub-block interleaver.
+int ref_polar_code(unsigned K, unsigned E, int* info, uint8_t* kset, uint16_t* pc, uint16_t* subblock)
+{
+  if (E > polar_code::EMAX || K < 18 || (K > 25 && K < 31) || K > 1023 || !(K + (K <= 25 ? 3 : 0) < E)) {
+    info[3] = 0;
+    return 0;
+  }
+  polar_code_impl code;
+  code.set(K, E, 10, polar_code_ibil::present);
+  info[0] = (int)code.get_n();
+  info[1] = (int)code.get_N();
+  info[2] = (int)code.get_nPC();
+  info[3] = 1;
+  for (unsigned i = 0; i != code.get_N(); ++i) {
+    kset[i] = code.get_K_set().test(i) ? 1 : 0;
+  }
+  span<const uint16_t> pcs = code.get_PC_set();
+  for (unsigned i = 0; i != 4; ++i) {
+    pc[i] = i < pcs.size() ? pcs[i] : polar_code::NMAX;
+  }
+  span<const uint16_t> blk = code.get_blk_interleaver();
+  for (unsigned i = 0; i != code.get_N(); ++i) {
+    subblock[i] = blk[i];
+  }
+  return 1;
+}
+
+// Test-vector encoder for polar-coded UCI (TS 38.212 6.3.1.2-6.3.1.4 with the reference's pieces):
+// A message bits into E bits. Segmentation and CRC size of uci_info.h, a leading zero filler bit
+// when A is odd and split in two, the CRC of each codeblock by the reference's CRC calculator,
+// polar_allocator + polar_encoder + polar_rate_matcher with the channel interleaver.
+int ref_uci_polar_encode(unsigned A, const uint8_t* msg, unsigned E, uint8_t* out)
+{
+  const unsigned C  = get_nof_uci_codeblocks(A, E);
+  const unsigned L  = get_uci_crc_size(A);
+  auto           cf = create_crc_calculator_factory_sw("auto");
+  auto           crc = cf->create(L == 11 ? crc_generator_poly::CRC11 : crc_generator_poly::CRC6);
+  const unsigned A0 = A / C, E0 = E / C, F = A % C;
+  unsigned       msg_pos = 0;
+  for (unsigned c = 0; c != C; ++c) {
+    const unsigned       Ac = c == 0 ? A0 : (A + C - 1) / C;
+    const unsigned       Ec = c == 0 ? E0 : E - E0;
+    const unsigned       Fc = c == 0 ? F : 0;
+    const unsigned       K  = Fc + Ac + L;
+    std::vector<uint8_t> blk(K, 0);
+    std::memcpy(blk.data() + Fc, msg + msg_pos, Ac);
+    msg_pos += Ac;
+    const unsigned ck = crc->calculate_bit(span<const uint8_t>(blk.data(), Fc + Ac));
+    for (unsigned i = 0; i != L; ++i) {
+      blk[Fc + Ac + i] = (ck >> (L - 1 - i)) & 1U;
+    }
+    polar_code_impl code;
+    code.set(K, Ec, 10, polar_code_ibil::present);
+    std::vector<uint8_t> u(code.get_N()), x(code.get_N());
+    polar_allocator_impl().allocate(u, blk, code);
+    polar_encoder_impl().encode(x, u, code.get_n());
+    polar_rate_matcher_impl().rate_match(span<uint8_t>(out + (c == 0 ? 0 : E0), Ec), x, code);
+  }
+  return (int)C;
+}
+
+// uci_decoder_impl::decode of an A-bit message (12..1706 bits) from E soft bits into out (A
+// bytes); returns 1 when the reference declares it valid.
+int ref_uci_polar_decode(unsigned A, const int8_t* llrs, unsigned E, uint8_t* out)
+{
+  auto             cf = create_crc_calculator_factory_sw("auto");
+  uci_decoder_impl dec(std::make_unique<short_block_detector_impl>(), std::make_unique<polar_code_impl>(),
+                       std::make_unique<polar_rate_dematcher_impl>(),
+                       std::make_unique<polar_decoder_impl>(std::make_unique<polar_encoder_impl>(), 10),
+                       std::make_unique<polar_deallocator_impl>(), cf->create(crc_generator_poly::CRC6),
+                       cf->create(crc_generator_poly::CRC11));
+  std::vector<log_likelihood_ratio> in(E);
+  for (unsigned i = 0; i != E; ++i) {
+    in[i] = llrs[i];
+  }
+  uci_decoder::configuration cfg = {};
+  cfg.modulation                 = modulation_scheme::QPSK;
+  return dec.decode(span<uint8_t>(out, A), in, cfg) == uci_status::valid ? 1 : 0;
 }
 
 // The reference's minimum number of rate-matched bits for a K-bit short block.
