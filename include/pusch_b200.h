@@ -491,22 +491,23 @@ typedef struct pg_pusch_plan_info_t {
 int  pg_pusch_plan_create(pg_context* ctx, const pg_pusch_ue* ues, int nof_ues, size_t grid_words,
                           pg_pusch_plan** out);
 
-/* UCI multiplexed on one UE's PUSCH (HARQ-ACK and CSI Part 1 of 1 to 11 bits each): the fields of
+/* UCI multiplexed on one UE's PUSCH (HARQ-ACK and CSI Part 1 of 1 to 1706 bits each): the fields of
  * the reference's ulsch_demultiplex::configuration (include/ocudu/phy/upper/channel_processors/
  * pusch/ulsch_demultiplex.h:31-90) that pg_pusch_ue does not carry. All zero: no UCI. */
 typedef struct pg_pusch_uci {
   uint32_t nof_harq_ack_rvd;            /* G^HARQ-ACK_rvd, reserved HARQ-ACK soft bits */
   uint32_t nof_enc_harq_ack_bits;       /* G^HARQ-ACK */
   uint32_t nof_enc_csi_part1_bits;      /* G^CSI-1 */
-  uint8_t  nof_harq_ack_bits;           /* O^HARQ-ACK, 0..11 */
-  uint8_t  nof_csi_part1_bits;          /* O^CSI-1, 0..11 */
+  uint16_t nof_harq_ack_bits;           /* O^HARQ-ACK, 0..1706 (above 11: polar-coded) */
+  uint16_t nof_csi_part1_bits;          /* O^CSI-1, 0..1706 */
   uint8_t  nof_cdm_groups_without_data; /* DM-RS type 1: 1 or 2 */
-  uint8_t  reserved;
+  uint8_t  reserved[3];
 } pg_pusch_uci;
 
-/* Decoded UCI of one UE after an execution: the bits of each message (one per byte, message bit i
- * at index i) and the short-block detector's validity (1: the reference's detection test passes;
- * 0 also when the UE carries no such message). */
+/* Decoded UCI of one UE after an execution: the bits of each message of up to 11 bits (one per
+ * byte, message bit i at index i; zeros for a longer message, whose bits pg_pusch_plan_uci_message
+ * gives) and each message's validity (1: the reference's short-block detection test passes, or
+ * every polar codeblock passes its CRC; 0 also when the UE carries no such message). */
 typedef struct pg_pusch_uci_result {
   uint8_t harq_ack[11];
   uint8_t csi_part1[11];
@@ -517,12 +518,18 @@ typedef struct pg_pusch_uci_result {
 /* pg_pusch_plan_create with UCI on PUSCH: uci holds one entry per UE (NULL: none). Each execution
  * demultiplexes the UCI UEs' codewords on the GPU (as pusch_processor_impl.cpp:616-712 configures
  * it: ulsch_demultiplex, the UL-SCH stream to the decoder, the UCI streams to the UCI decoders),
- * decodes the UL-SCH stream as usual and detects the short-block messages. */
+ * decodes the UL-SCH stream as usual, detects the short-block messages (1 to 11 bits) and decodes
+ * the polar-coded ones (12 to 1706 bits; their codes are built when the plan is created, and a
+ * message without a polar code for its encoded size makes the creation PG_ERR_INVALID). */
 int  pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_pusch_uci* uci, int nof_ues,
                               size_t grid_words, pg_pusch_plan** out);
 /* UCI results of the plan's last execution (nof_ues entries, host memory). Reads device memory
  * synchronously: call after that execution's stream has completed. */
 int  pg_pusch_plan_uci_results(pg_pusch_plan* plan, pg_pusch_uci_result* out);
+/* One UCI message of the plan's last execution, any size: UE ue, field 0 HARQ-ACK / 1 CSI Part 1;
+ * bits receives the message's bits (one per byte; len at least its size) and *valid its validity.
+ * PG_ERR_INVALID when the UE carries no such message. Synchronous, as pg_pusch_plan_uci_results. */
+int  pg_pusch_plan_uci_message(pg_pusch_plan* plan, int ue, int field, uint8_t* bits, size_t len, uint8_t* valid);
 void pg_pusch_plan_destroy(pg_pusch_plan* plan);
 int  pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info);
 
@@ -696,8 +703,9 @@ int pg_pusch_plan_set_learned(pg_pusch_plan* plan, pg_le_net* net, const uint8_t
 
 
 /* ---------------------------------------------------------------------------------------------
- * UCI on PUSCH: HARQ-ACK and CSI Part 1 of up to 11 bits (short block codes). Messages of more
- * than 11 bits (polar codes) and CSI Part 2 are not supported (PG_ERR_INVALID). */
+ * UCI on PUSCH: HARQ-ACK and CSI Part 1 of up to 1706 bits (the placeholder and reserved-RE rules
+ * of messages of one or two bits; longer messages are demultiplexed alike). CSI Part 2 is not
+ * supported (PG_ERR_INVALID). */
 
 /* One codeword to demultiplex: the fields of ulsch_demultiplex::configuration
  * (include/ocudu/phy/upper/channel_processors/pusch/ulsch_demultiplex.h:31-58) plus the buffers.
@@ -721,8 +729,8 @@ typedef struct pg_ulsch_demux_config {
   uint8_t  nof_symbols;
   uint8_t  dmrs_type;              /* 1 or 2 */
   uint8_t  nof_cdm_groups_without_data;
-  uint8_t  nof_harq_ack_bits;      /* O^HARQ-ACK, 0..11 */
-  uint8_t  nof_csi_part1_bits;     /* O^CSI-1, 0..11 */
+  uint16_t nof_harq_ack_bits;      /* O^HARQ-ACK, 0..1706 */
+  uint16_t nof_csi_part1_bits;     /* O^CSI-1, 0..1706 */
 } pg_ulsch_demux_config;
 
 /* The rate-matching sizes of UCI multiplexed on PUSCH (TS 38.212 Sections 6.3.2.4.1.1-3 and

@@ -131,7 +131,11 @@ int uci_demux_launch(pg_context* ctx, const void* blob_dev, const uci_demux_work
 std::string uci_short_blob(const pg_uci_short_block* items, int n, std::vector<uint8_t>& blob);
 int uci_detect_launch(pg_context* ctx, const void* items_dev, int n, const int8_t* llrs, uint8_t* bits, uint8_t* valid,
                       cudaStream_t s);
-// Polar-coded UCI: decodes n messages (codes built on the host, descriptors staged, one launch).
+// Polar-coded UCI: the device descriptors of n messages (codes built on the host; an error text for
+// a message without a polar code), their launch, and both steps with the descriptors staged.
+std::string uci_polar_blob(const pg_uci_polar* items, int n, std::vector<uint8_t>& blob);
+int uci_polar_launch_dev(pg_context* ctx, const void* cbs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                         uint8_t* valid, cudaStream_t s);
 int uci_polar_launch(pg_context* ctx, const pg_uci_polar* items, int n, const int8_t* llrs, uint8_t* bits,
                      uint8_t* valid, cudaStream_t s);
 // Open Fronthaul BFP: compressed bytes per PRB, and decompression of nof_prb PRBs into cbf16.

@@ -46,6 +46,14 @@ struct pg_pusch_plan {
   uint8_t*        d_uci_bits  = nullptr;
   uint8_t*        d_uci_valid = nullptr;
   std::vector<int> uci_msg_ue, uci_msg_kind; // per message: UE and 0 HARQ-ACK / 1 CSI Part 1
+  // Polar-coded messages (after the short-block ones in the message order): their descriptors,
+  // their decoded bits, and per message the bit offset (in the short-block results or the polar
+  // bits) and the size.
+  int              uci_nshort   = 0;
+  int              polar_n      = 0;
+  void*            d_polar_cbs  = nullptr;
+  uint8_t*         d_polar_bits = nullptr;
+  std::vector<uint32_t> uci_msg_off, uci_msg_nbits;
   rm_direct*      d_direct   = nullptr; // per UE: fused rate-dematch placement of the demodulator
   uint8_t*        d_placed   = nullptr; // per codeblock: 1 when the demodulator places its LLRs
   uint32_t*       d_unplaced = nullptr; // capacity nof_cbs
@@ -280,7 +288,11 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
     // and the HARQ-ACK / CSI Part 1 streams, then the short-block detection of the messages.
     rc = uci_demux_launch(ctx, p->d_uci_blob, p->uci_w, p->d_llr, p->d_llr, p->d_uci_llr, p->d_uci_llr, s);
     if (rc == PG_OK) {
-      rc = uci_detect_launch(ctx, p->d_uci_items, p->uci_nmsg, p->d_uci_llr, p->d_uci_bits, p->d_uci_valid, s);
+      rc = uci_detect_launch(ctx, p->d_uci_items, p->uci_nshort, p->d_uci_llr, p->d_uci_bits, p->d_uci_valid, s);
+    }
+    if (rc == PG_OK && p->polar_n > 0) {
+      rc = uci_polar_launch_dev(ctx, p->d_polar_cbs, p->polar_n, p->d_uci_llr, p->d_polar_bits,
+                                p->d_uci_valid + p->uci_nshort, s);
     }
   }
   if (rc == PG_OK && !p->unplaced.empty()) {
@@ -415,7 +427,9 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   // buffer, one short-block message per field.
   std::vector<pg_ulsch_demux_config> ucfg;
   std::vector<pg_uci_short_block>    umsg;
-  size_t                             uci_llr_total = 0;
+  std::vector<pg_uci_polar>          pmsg;
+  std::vector<int>                   pmsg_ue, pmsg_kind;
+  size_t                             uci_llr_total = 0, polar_bits_total = 0;
   for (int i = 0; uci != nullptr && i < nof_ues; ++i) {
     const pg_pusch_uci& q = uci[i];
     if (q.nof_harq_ack_bits == 0 && q.nof_csi_part1_bits == 0) {
@@ -444,9 +458,9 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
       release(p);
       return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": inconsistent UCI configuration");
     }
-    if ((q.nof_harq_ack_bits > 11) || (q.nof_csi_part1_bits > 11)) {
+    if ((q.nof_harq_ack_bits > 1706) || (q.nof_csi_part1_bits > 1706)) {
       release(p);
-      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": UCI fields of 1 to 11 bits");
+      return set_error(ctx, PG_ERR_INVALID, "UE " + std::to_string(i) + ": UCI fields of 1 to 1706 bits");
     }
     p->nof_llrs      = (p->nof_llrs + 15) & ~(size_t)15;
     c.sch_offset     = (uint32_t)p->nof_llrs;
@@ -454,17 +468,29 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
     c.harq_ack_offset  = (uint32_t)uci_llr_total;
     c.csi_part1_offset = (uint32_t)(uci_llr_total + sz[1]);
     for (int k = 0; k < 2; ++k) {
-      const uint8_t nbits = k == 0 ? q.nof_harq_ack_bits : q.nof_csi_part1_bits;
-      if (nbits > 0) {
+      const unsigned nbits = k == 0 ? q.nof_harq_ack_bits : q.nof_csi_part1_bits;
+      if (nbits > 11) {
+        pg_uci_polar m = {};
+        m.llr_offset   = k == 0 ? c.harq_ack_offset : c.csi_part1_offset;
+        m.nof_llrs     = sz[1 + k];
+        m.out_offset   = (uint32_t)polar_bits_total;
+        m.nof_bits     = (uint16_t)nbits;
+        pmsg.push_back(m);
+        pmsg_ue.push_back(i);
+        pmsg_kind.push_back(k);
+        polar_bits_total += nbits;
+      } else if (nbits > 0) {
         pg_uci_short_block m = {};
         m.llr_offset         = k == 0 ? c.harq_ack_offset : c.csi_part1_offset;
         m.nof_llrs           = sz[1 + k];
         m.out_offset         = (uint32_t)(i * sizeof(pg_pusch_uci_result)) + (k == 0 ? 0u : 11u);
-        m.nof_bits           = nbits;
+        m.nof_bits           = (uint8_t)nbits;
         m.modulation_order   = u.modulation_order;
         umsg.push_back(m);
         p->uci_msg_ue.push_back(i);
         p->uci_msg_kind.push_back(k);
+        p->uci_msg_off.push_back(m.out_offset);
+        p->uci_msg_nbits.push_back(nbits);
       }
     }
     uci_llr_total += sz[1] + sz[2];
@@ -472,17 +498,28 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
     tbs[i].nof_ch_symbols = sz[0] / u.modulation_order;
     ucfg.push_back(c);
   }
-  std::vector<uint8_t> uci_blob, uci_items;
+  std::vector<uint8_t> uci_blob, uci_items, polar_blob;
   if (!ucfg.empty()) {
     std::string err = uci_demux_blob(ucfg.data(), (int)ucfg.size(), uci_blob, p->uci_w, nullptr);
     if (err.empty()) {
       err = uci_short_blob(umsg.data(), (int)umsg.size(), uci_items);
     }
+    if (err.empty()) {
+      err = uci_polar_blob(pmsg.data(), (int)pmsg.size(), polar_blob);
+    }
     if (!err.empty()) {
       release(p);
       return set_error(ctx, PG_ERR_INVALID, err);
     }
-    p->uci_nmsg = (int)umsg.size();
+    p->uci_nshort = (int)umsg.size();
+    p->polar_n    = (int)pmsg.size();
+    for (size_t m = 0; m < pmsg.size(); ++m) {
+      p->uci_msg_ue.push_back(pmsg_ue[m]);
+      p->uci_msg_kind.push_back(pmsg_kind[m]);
+      p->uci_msg_off.push_back(pmsg[m].out_offset);
+      p->uci_msg_nbits.push_back(pmsg[m].nof_bits);
+    }
+    p->uci_nmsg = p->uci_nshort + p->polar_n;
   }
   p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
   p->est_total = est_total;
@@ -541,7 +578,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_ework  = o_reoff + al(tile_map.size() * 4);
   const size_t o_ublob  = o_ework + al(est_work.size() * 4);
   const size_t o_uitems = o_ublob + al(uci_blob.size());
-  const size_t o_direct = o_uitems + al(uci_items.size());
+  const size_t o_pcbs   = o_uitems + al(uci_items.size());
+  const size_t o_direct = o_pcbs + al(polar_blob.size());
   const size_t o_fill   = o_direct + al(direct.size() * sizeof(rm_direct));
   const size_t o_unpl   = o_fill + al(placed.size());
   const size_t desc_end = o_unpl + al((size_t)p->nof_cbs * 4);
@@ -564,7 +602,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   const size_t o_ullr   = o_earr + al((size_t)nof_ues * 16);
   const size_t o_ubits  = o_ullr + al(uci_llr_total);
   const size_t o_uvalid = o_ubits + al((size_t)nof_ues * sizeof(pg_pusch_uci_result));
-  const size_t o_pbits  = o_uvalid + al((size_t)std::max(1, p->uci_nmsg));
+  const size_t o_polb   = o_uvalid + al((size_t)std::max(1, p->uci_nmsg));
+  const size_t o_pbits  = o_polb + al(polar_bits_total);
   p->dev_bytes          = o_pbits + al((size_t)pilot_words * 4);
 
   const size_t h_res  = 0;
@@ -620,6 +659,8 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   p->d_uci_llr   = reinterpret_cast<int8_t*>(b + o_ullr);
   p->d_uci_bits  = b + o_ubits;
   p->d_uci_valid = b + o_uvalid;
+  p->d_polar_cbs  = b + o_pcbs;
+  p->d_polar_bits = b + o_polb;
 
   // Descriptor image in pinned memory, one upload.
   uint8_t* h = static_cast<uint8_t*>(p->host);
@@ -638,6 +679,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   if (!uci_blob.empty()) {
     std::memcpy(h + o_ublob, uci_blob.data(), uci_blob.size());
     std::memcpy(h + o_uitems, uci_items.data(), uci_items.size());
+    std::memcpy(h + o_pcbs, polar_blob.data(), polar_blob.size());
   }
   std::memcpy(h + o_direct, direct.data(), direct.size() * sizeof(rm_direct));
   std::memcpy(h + o_fill, placed.data(), placed.size());
@@ -702,7 +744,8 @@ int pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info)
   // The kernels enqueue() launches: prefill, estimation, [learned: features, network, corrections],
   // demodulation, [UCI: demultiplexing, detection], [rate dematching of the codeblocks not placed],
   // [device work order: score, sort], LDPC, TB assembly, results.
-  info->nof_kernels = 2u + (plan->le_net != nullptr ? 3u : 0u) + 1u + (plan->uci_w.nitems > 0 ? 2u : 0u) +
+  info->nof_kernels = 2u + (plan->le_net != nullptr ? 3u : 0u) + 1u + (plan->uci_w.nitems > 0 ? 1u : 0u) +
+                      (plan->uci_nshort > 0 ? 1u : 0u) + (plan->polar_n > 0 ? 1u : 0u) +
                       (plan->unplaced.empty() ? 0u : 1u) + (plan->nof_cbs > 1 && plan->tuning.ldpc_order != 0 ? 2u : 0u) +
                       3u;
   info->reserved = 0;
@@ -820,6 +863,34 @@ int pg_pusch_plan_uci_results(pg_pusch_plan* plan, pg_pusch_uci_result* out)
   }
   std::memcpy(out, r.data(), r.size() * sizeof(pg_pusch_uci_result));
   return PG_OK;
+}
+
+int pg_pusch_plan_uci_message(pg_pusch_plan* plan, int ue, int field, uint8_t* bits, size_t len, uint8_t* valid)
+{
+  if (plan == nullptr) {
+    return PG_ERR_INVALID;
+  }
+  pg_context* ctx = plan->ctx;
+  if (bits == nullptr || valid == nullptr) {
+    return set_error(ctx, PG_ERR_INVALID, "null argument");
+  }
+  int m = 0;
+  while (m < plan->uci_nmsg && !(plan->uci_msg_ue[m] == ue && plan->uci_msg_kind[m] == field)) {
+    ++m;
+  }
+  if (m == plan->uci_nmsg) {
+    return set_error(ctx, PG_ERR_INVALID, "the UE carries no such UCI message");
+  }
+  const size_t nbits = plan->uci_msg_nbits[m];
+  if (len < nbits) {
+    return set_error(ctx, PG_ERR_INVALID, "bit buffer shorter than the message");
+  }
+  const uint8_t* src = (m < plan->uci_nshort ? plan->d_uci_bits : plan->d_polar_bits) + plan->uci_msg_off[m];
+  int            rc  = check_cuda(ctx, cudaMemcpy(bits, src, nbits, cudaMemcpyDeviceToHost), "D2H UCI message");
+  if (rc == PG_OK) {
+    rc = check_cuda(ctx, cudaMemcpy(valid, plan->d_uci_valid + m, 1, cudaMemcpyDeviceToHost), "D2H UCI validity");
+  }
+  return rc;
 }
 
 int pg_pusch_plan_set_harq(pg_pusch_plan* plan, const uint8_t* new_data, const uint8_t* rv)

@@ -375,8 +375,8 @@ std::string ulsch_demux_layout(const pg_ulsch_demux_config& c, demux_layout& out
   if ((c.dmrs_symbol_mask & 0x3fffu) == 0) {
     return "no DM-RS symbol";
   }
-  if (c.nof_harq_ack_bits > 11 || c.nof_csi_part1_bits > 11) {
-    return "UCI messages of more than 11 bits (polar-coded) are not supported";
+  if (c.nof_harq_ack_bits > 1706 || c.nof_csi_part1_bits > 1706) {
+    return "UCI messages of more than 1706 bits";
   }
   if (c.nof_harq_ack_rvd != 0 && c.nof_harq_ack_bits > 2) {
     return "reserved HARQ-ACK bits apply to messages of at most two bits";
@@ -525,8 +525,8 @@ std::string uci_demux_blob(const pg_ulsch_demux_config* cfgs, int n, std::vector
     d.nsym       = (uint16_t)L.syms.size();
     d.bpr        = (uint8_t)(cfgs[u].modulation_order * cfgs[u].nof_layers);
     d.qm         = cfgs[u].modulation_order;
-    d.ack_bits   = (uint8_t)cfgs[u].nof_harq_ack_bits;
-    d.csi_bits   = (uint8_t)cfgs[u].nof_csi_part1_bits;
+    d.ack_bits   = (uint8_t)std::min<unsigned>(cfgs[u].nof_harq_ack_bits, 255u); // only <= 2 matters
+    d.csi_bits   = (uint8_t)std::min<unsigned>(cfgs[u].nof_csi_part1_bits, 255u);
     for (demux_sym sy : L.syms) {
       sy.ue = (uint32_t)u;
       syms.push_back(sy);

@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kPolarThreads) uci_polar_kernel(const polar_cb
 
 // The device blob of n messages: two polar_cb per message (the second with E = 0 when the message
 // has one codeblock). Returns an error text for an invalid message.
-std::string uci_polar_blob(const pg_uci_polar* items, int n, std::vector<polar_cb>& cbs)
+std::string polar_blob_cbs(const pg_uci_polar* items, int n, std::vector<polar_cb>& cbs)
 {
   cbs.assign((size_t)2 * n, polar_cb{});
   for (int i = 0; i < n; ++i) {
@@ -504,20 +504,39 @@ std::string uci_polar_blob(const pg_uci_polar* items, int n, std::vector<polar_c
 
 namespace pg {
 
+std::string uci_polar_blob(const pg_uci_polar* items, int n, std::vector<uint8_t>& blob)
+{
+  std::vector<polar_cb> cbs;
+  const std::string     err = polar_blob_cbs(items, n, cbs);
+  blob.resize(cbs.size() * sizeof(polar_cb));
+  std::memcpy(blob.data(), cbs.data(), blob.size());
+  return err;
+}
+
+int uci_polar_launch_dev(pg_context* ctx, const void* cbs_dev, int n, const int8_t* llrs, uint8_t* bits,
+                         uint8_t* valid, cudaStream_t s)
+{
+  if (n == 0) {
+    return PG_OK;
+  }
+  uci_polar_kernel<<<(unsigned)n, kPolarThreads, 0, s>>>(static_cast<const polar_cb*>(cbs_dev), n, llrs, bits,
+                                                         valid);
+  return check_cuda(ctx, cudaGetLastError(), "uci_polar_kernel launch");
+}
+
 int uci_polar_launch(pg_context* ctx, const pg_uci_polar* items, int n, const int8_t* llrs, uint8_t* bits,
                      uint8_t* valid, cudaStream_t s)
 {
-  std::vector<polar_cb> cbs;
-  const std::string     err = uci_polar_blob(items, n, cbs);
+  std::vector<uint8_t> blob;
+  const std::string    err = uci_polar_blob(items, n, blob);
   if (!err.empty()) {
     return set_error(ctx, PG_ERR_INVALID, err);
   }
   void* dev = nullptr;
-  if (int rc = stage_slot(ctx, SLOT_UCI_POLAR, cbs.data(), cbs.size() * sizeof(polar_cb), s, &dev)) {
+  if (int rc = stage_slot(ctx, SLOT_UCI_POLAR, blob.data(), blob.size(), s, &dev)) {
     return rc;
   }
-  uci_polar_kernel<<<(unsigned)n, kPolarThreads, 0, s>>>(static_cast<const polar_cb*>(dev), n, llrs, bits, valid);
-  if (int rc = check_cuda(ctx, cudaGetLastError(), "uci_polar_kernel launch")) {
+  if (int rc = uci_polar_launch_dev(ctx, dev, n, llrs, bits, valid, s)) {
     return rc;
   }
   return release_slot_after(ctx, SLOT_UCI_POLAR, s);

@@ -115,15 +115,15 @@ class PgUlschDemuxConfig(ctypes.Structure):
                 ("nof_prb", ctypes.c_uint16), ("dmrs_symbol_mask", ctypes.c_uint16),
                 ("modulation_order", ctypes.c_uint8), ("nof_layers", ctypes.c_uint8),
                 ("start_symbol_index", ctypes.c_uint8), ("nof_symbols", ctypes.c_uint8), ("dmrs_type", ctypes.c_uint8),
-                ("nof_cdm_groups_without_data", ctypes.c_uint8), ("nof_harq_ack_bits", ctypes.c_uint8),
-                ("nof_csi_part1_bits", ctypes.c_uint8)]
+                ("nof_cdm_groups_without_data", ctypes.c_uint8), ("nof_harq_ack_bits", ctypes.c_uint16),
+                ("nof_csi_part1_bits", ctypes.c_uint16)]
 
 
 class PgPuschUci(ctypes.Structure):
     _fields_ = [("nof_harq_ack_rvd", ctypes.c_uint32), ("nof_enc_harq_ack_bits", ctypes.c_uint32),
-                ("nof_enc_csi_part1_bits", ctypes.c_uint32), ("nof_harq_ack_bits", ctypes.c_uint8),
-                ("nof_csi_part1_bits", ctypes.c_uint8), ("nof_cdm_groups_without_data", ctypes.c_uint8),
-                ("reserved", ctypes.c_uint8)]
+                ("nof_enc_csi_part1_bits", ctypes.c_uint32), ("nof_harq_ack_bits", ctypes.c_uint16),
+                ("nof_csi_part1_bits", ctypes.c_uint16), ("nof_cdm_groups_without_data", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8 * 3)]
 
 
 class PgPuschUciResult(ctypes.Structure):
@@ -212,6 +212,7 @@ SIGNATURES = {
     "pg_pusch_plan_create": (ctypes.c_int, [_VP, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
     "pg_pusch_plan_create_uci": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int, ctypes.c_size_t, _VP]),
     "pg_pusch_plan_uci_results": (ctypes.c_int, [_VP, _VP]),
+    "pg_pusch_plan_uci_message": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_size_t, _VP]),
     "pg_pusch_plan_destroy": (None, [_VP]),
     "pg_pusch_plan_info": (ctypes.c_int, [_VP, _VP]),
     "pg_pusch_plan_set_graph": (ctypes.c_int, [_VP, ctypes.c_int]),

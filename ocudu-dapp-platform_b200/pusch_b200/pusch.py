@@ -204,6 +204,16 @@ class PuschSlotPlan:
         self.ctx.check(self.lib.pg_pusch_plan_uci_results(self.handle, ctypes.addressof(res)))
         return res
 
+    def uci_message(self, ue, field, nbits):
+        """One UCI message of the last execution (field 0 HARQ-ACK, 1 CSI Part 1; any size, polar-coded
+        ones included): (bits, valid)."""
+        import numpy as np
+        buf = np.zeros(max(1, nbits), np.uint8)
+        valid = ctypes.c_uint8(0)
+        self.ctx.check(self.lib.pg_pusch_plan_uci_message(self.handle, ue, field, buf.ctypes.data_as(ctypes.c_void_p),
+                                                          buf.size, ctypes.byref(valid)))
+        return buf[:nbits].copy(), bool(valid.value)
+
     def set_learned(self, net, use=None):
         """Refines the channel estimates with a LearnedEstimator (None: the plain estimator only)
         for the UEs with use[u] true (all when use is None)."""

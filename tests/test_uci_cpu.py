@@ -57,7 +57,9 @@ def test_demux_rejects_unsupported(lib):
                 dmrs_type=1, nof_cdm_groups_without_data=2, nof_harq_ack_bits=5, nof_csi_part1_bits=0)
     base["nof_llrs"] = uci_cases.codeword_size(base)
     assert f(base) is not None
-    for bad in (dict(nof_harq_ack_bits=12), dict(nof_enc_harq_ack_bits=241), dict(nof_llrs=base["nof_llrs"] + 2),
+    # Polar-coded messages demultiplex as the short-block ones of 3 to 11 bits.
+    assert f(dict(base, nof_harq_ack_bits=12)) == f(base) == f(dict(base, nof_harq_ack_bits=1706))
+    for bad in (dict(nof_harq_ack_bits=1707), dict(nof_enc_harq_ack_bits=241), dict(nof_llrs=base["nof_llrs"] + 2),
                 dict(nof_harq_ack_rvd=4), dict(nof_enc_harq_ack_bits=10 ** 6), dict(dmrs_symbol_mask=0),
                 dict(modulation_order=3)):
         assert f(dict(base, **bad)) is None, bad

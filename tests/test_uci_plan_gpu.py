@@ -174,3 +174,76 @@ def test_plan_uci_rejects_inconsistent_configuration(ctx):
     from pusch_b200._native import PgError
     with pytest.raises(PgError):
         PuschSlotPlan(ctx, slots, max_iterations=MAX_ITER, uci=ucis)
+
+
+def test_plan_polar_uci_matches_stage_chain(ctx):
+    """Polar-coded HARQ-ACK and CSI Part 1 (12 to 200 bits) inside a plan: every message's bits and
+    validity (pg_pusch_plan_uci_message) equal the stage chain's - pg_ulsch_demultiplex_device on
+    the demodulated codewords, then pg_uci_polar_decode_device (tests/test_uci_polar_gpu.py pins it
+    to the reference's uci_decoder)."""
+    import torch
+    from pusch_b200.uci import PolarUciDecoder
+    rng = np.random.default_rng(5)
+    slots = sim.uneven_cells(seed=13, nof_cells=2)
+    descs, grid, tb_bytes, ues = batch_descriptors(slots, max_iterations=MAX_ITER)
+    ucis = []
+    for ue, d in zip(ues, descs):
+        q = PgPuschUci()
+        if rng.random() < 0.7:
+            bpr = ue.modulation_order * ue.nof_layers
+            q.nof_harq_ack_bits = int(rng.choice([3, 12, 20, 40]))
+            q.nof_csi_part1_bits = int(rng.choice([0, 19, 64, 200]))
+            enc = lambda A: 0 if A == 0 else bpr * (-(-2 * (A + 14) // bpr) + int(rng.integers(0, 20)))
+            q.nof_enc_harq_ack_bits = enc(q.nof_harq_ack_bits)
+            q.nof_enc_csi_part1_bits = enc(q.nof_csi_part1_bits)
+            q.nof_cdm_groups_without_data = 2
+            if sizes_of(ctx, demux_config(ue, d, q, 0, (0, 0, 0))) is None:
+                q = PgPuschUci()
+        ucis.append(q)
+    plan = PuschSlotPlan(ctx, slots, max_iterations=MAX_ITER, uci=ucis)
+    plan.execute_host()
+    sel = [i for i, q in enumerate(ucis) if q.nof_harq_ack_bits or q.nof_csi_part1_bits]
+    msgs = [(i, k, n) for i in sel for k, n in ((0, ucis[i].nof_harq_ack_bits), (1, ucis[i].nof_csi_part1_bits))
+            if n > 11]
+    assert len(msgs) >= 8
+    plan_out = {(i, k): plan.uci_message(i, k, n) for i, k, n in msgs}
+    plan.close()
+
+    n = len(ues)
+    llr_off, nllr, nest = [], 0, 0
+    for d, ue in zip(descs, ues):
+        d.llr_offset, d.est_offset = nllr, nest
+        llr_off.append(nllr)
+        nllr += sim.nof_ch_symbols(ue) * ue.modulation_order
+        nest += d.nof_rx_ports * len(ue.dmrs_symbols) * ue.nof_layers * 12 * ue.nof_rb
+    st = torch.cuda.current_stream()
+    d_grid = torch.from_numpy(grid.view(np.int32)).cuda()
+    d_est = torch.zeros(2 * nest, dtype=torch.float32, device="cuda")
+    d_pr = torch.zeros(n * 4 * 5, dtype=torch.float32, device="cuda")
+    d_llr = torch.zeros(nllr, dtype=torch.int8, device="cuda")
+    ctx.check(ctx.lib.pg_pusch_estimate_device(ctx.handle, ctypes.addressof(descs), n, d_grid.data_ptr(),
+                                               d_est.data_ptr(), d_pr.data_ptr(), st.cuda_stream))
+    ctx.check(ctx.lib.pg_pusch_demodulate_device(ctx.handle, ctypes.addressof(descs), n, d_grid.data_ptr(),
+                                                 d_est.data_ptr(), d_pr.data_ptr(), d_llr.data_ptr(), st.cuda_stream))
+    cfgs, spans, offs = [], {}, [0, 0, 0]
+    for i in sel:
+        c = demux_config(ues[i], descs[i], ucis[i], llr_off[i], tuple(offs))
+        sz = sizes_of(ctx, c)
+        cfgs.append(c)
+        spans[i] = [(offs[k], sz[k]) for k in range(3)]
+        offs = [offs[k] + sz[k] for k in range(3)]
+    arr = (uci_cases.PgUlschDemuxConfig * len(cfgs))(*[uci_cases.to_struct(c) for c in cfgs])
+    outs = [torch.zeros(max(1, offs[k]), dtype=torch.int8, device="cuda") for k in range(3)]
+    ctx.check(ctx.lib.pg_ulsch_demultiplex_device(ctx.handle, ctypes.addressof(arr), len(cfgs), d_llr.data_ptr(),
+                                                  outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(),
+                                                  st.cuda_stream))
+    st.synchronize()
+    streams = [outs[1].cpu().numpy(), outs[2].cpu().numpy()]
+    chain = PolarUciDecoder(ctx).decode([(nb, streams[k][spans[i][1 + k][0]:spans[i][1 + k][0] + spans[i][1 + k][1]])
+                                         for i, k, nb in msgs])
+    # The simulator carries no UCI in these REs (their soft bits are UL-SCH data), so the CRCs fail;
+    # the decoders' bits are still a function of the soft bits and must agree message by message.
+    for (i, k, nb), (bits, ok) in zip(msgs, chain):
+        pb, pok = plan_out[(i, k)]
+        assert pok == ok, (i, k)
+        assert np.array_equal(pb, bits), (i, k)
