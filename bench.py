@@ -1057,9 +1057,38 @@ def uci_measure(ctx, ues, peak_gbs):
             ks.append(float(lib.pg_last_kernel_ms(ctx.handle)))
         times[name] = statistics.mean(a.elapsed_time(b) for a, b in ev)
         kernel[name] = statistics.mean(ks)
+    # Polar-coded CSI Part 1: one 100-bit message of 400 soft bits per UE (CRC11, N = 512 with
+    # puncturing), synthetic soft bits.
+    from pusch_b200._native import PgUciPolar
+    pol = (PgUciPolar * n)()
+    for i in range(n):
+        pol[i].llr_offset, pol[i].nof_llrs, pol[i].out_offset, pol[i].nof_bits = 400 * i, 400, 100 * i, 100
+    p_in = torch.randint(-120, 121, (400 * n,), dtype=torch.int8, device="cuda", generator=gen)
+    p_bits = torch.zeros(100 * n, dtype=torch.uint8, device="cuda")
+
+    def polar():
+        ctx.check(lib.pg_uci_polar_decode_device(ctx.handle, ctypes.addressof(pol), n, p_in.data_ptr(),
+                                                 p_bits.data_ptr(), d_valid.data_ptr(), st.cuda_stream))
+
+    for name, fn in (("polar", polar),):
+        for _ in range(3):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(20)]
+        ks = []
+        for a, b in ev:
+            a.record(st)
+            fn()
+            b.record(st)
+            b.synchronize()
+            ks.append(float(lib.pg_last_kernel_ms(ctx.handle)))
+        times[name] = statistics.mean(a.elapsed_time(b) for a, b in ev)
+        kernel[name] = statistics.mean(ks)
     gbs = 2 * in_off / (kernel["demux"] * 1e-3) / 1e9
     return {"ues": n, "harq_ack_bits": 5, "csi_part1_bits": 8, "soft_bits": int(in_off),
-            "call_ms": {k: round(v, 4) for k, v in times.items()},
+            "polar": {"messages": n, "bits": 100, "soft_bits_per_message": 400, "kernel_ms": round(kernel["polar"], 4),
+                      "call_ms": round(times["polar"], 4),
+                      "note": "one CTA per message, one warp per codeblock; latency-bound (sequential SC tree walk)"},
+            "call_ms": {k: round(v, 4) for k, v in times.items() if k != "polar"},
             "demux_kernel_ms": round(kernel["demux"], 4), "detect_kernel_ms": round(kernel["detect"], 4),
             "demux_roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak_gbs, "unit": "GB/s",
                                "frac": round(gbs / peak_gbs, 4), "bytes_per_launch": int(2 * in_off)},
