@@ -63,6 +63,8 @@ struct pg_pusch_plan {
   cudaStream_t    aux        = nullptr;
   cudaEvent_t     ev_fork    = nullptr;
   cudaEvent_t     ev_join    = nullptr;
+  cudaEvent_t     ev_ufork   = nullptr; // polar UCI decoding on the aux stream, beside the UL-SCH stages
+  cudaEvent_t     ev_ujoin   = nullptr;
   uint32_t*       d_est_work = nullptr; // channel-estimation work list and per-(UE, port) first items
   void*           d_est_part = nullptr; // its partial sums
   int*            d_est_arr  = nullptr; // per-(UE, port) arrival counters, zero between executions
@@ -291,8 +293,19 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
       rc = uci_detect_launch(ctx, p->d_uci_items, p->uci_nshort, p->d_uci_llr, p->d_uci_bits, p->d_uci_valid, s);
     }
     if (rc == PG_OK && p->polar_n > 0) {
-      rc = uci_polar_launch_dev(ctx, p->d_polar_cbs, p->polar_n, p->d_uci_llr, p->d_polar_bits,
-                                p->d_uci_valid + p->uci_nshort, s);
+      // The polar decoders read only the demultiplexed UCI streams: a branch of their own that
+      // overlaps rate dematching and LDPC decoding, joined at the end.
+      rc = check_cuda(ctx, cudaEventRecord(p->ev_ufork, s), "cudaEventRecord(UCI fork)");
+      if (rc == PG_OK) {
+        rc = check_cuda(ctx, cudaStreamWaitEvent(p->aux, p->ev_ufork, 0), "cudaStreamWaitEvent(UCI fork)");
+      }
+      if (rc == PG_OK) {
+        rc = uci_polar_launch_dev(ctx, p->d_polar_cbs, p->polar_n, p->d_uci_llr, p->d_polar_bits,
+                                  p->d_uci_valid + p->uci_nshort, p->aux);
+      }
+      if (rc == PG_OK) {
+        rc = check_cuda(ctx, cudaEventRecord(p->ev_ujoin, p->aux), "cudaEventRecord(UCI join)");
+      }
     }
   }
   if (rc == PG_OK && !p->unplaced.empty()) {
@@ -322,6 +335,9 @@ int enqueue(pg_pusch_plan* p, const uint32_t* grids, uint8_t* tb_out, pg_sch_res
                                                                  results);
     rc = check_cuda(ctx, cudaGetLastError(), "sch_results_kernel launch");
   }
+  if (rc == PG_OK && p->uci_w.nitems > 0 && p->polar_n > 0) {
+    rc = check_cuda(ctx, cudaStreamWaitEvent(s, p->ev_ujoin, 0), "cudaStreamWaitEvent(UCI join)");
+  }
   return rc;
 }
 
@@ -340,7 +356,8 @@ void release(pg_pusch_plan* p)
   if (p->aux) {
     cudaStreamDestroy(p->aux);
   }
-  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1], p->ev_fork, p->ev_join}) {
+  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1], p->ev_fork, p->ev_join, p->ev_ufork,
+                        p->ev_ujoin}) {
     if (e) {
       cudaEventDestroy(e);
     }
@@ -689,7 +706,7 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking), "cudaStreamCreate(aux)");
   }
-  for (cudaEvent_t* e : {&p->ev_fork, &p->ev_join}) {
+  for (cudaEvent_t* e : {&p->ev_fork, &p->ev_join, &p->ev_ufork, &p->ev_ujoin}) {
     if (rc == PG_OK) {
       rc = check_cuda(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate(fork/join)");
     }

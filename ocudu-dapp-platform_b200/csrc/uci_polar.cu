@@ -219,31 +219,30 @@ struct polar_warp_smem {
   int8_t   llr[2 * kPolarNMax];    // stage s at offset 2^s - 1, 2^s values (s = 0 .. n)
   uint8_t  est[kPolarNMax];        // codeword estimates (partial sums)
   uint8_t  u[kPolarNMax];          // decoded sub-channel bits
+  uint8_t  type[2 * kPolarNMax];   // node types, stage s at offset 2N - (2N >> s)
   uint32_t info[kPolarNMax / 32];
   uint16_t pc[4];
   int      valid;
 };
 
-// Node type of stage s, index j (leaves [j 2^s, (j + 1) 2^s)): rate 0 when no leaf is in K_set,
-// rate 1 when all are, rate R otherwise (polar_decoder_impl.cpp:74-107).
-__device__ __forceinline__ int node_type(const uint32_t* info, int s, int j, int lane)
+// Node types of every stage (polar_decoder_impl.cpp:74-107): a leaf is rate 1 when it is in K_set,
+// rate 0 otherwise; a node of stage s is rate 0 (rate 1) when both children are, rate R otherwise.
+__device__ __forceinline__ void node_types(polar_warp_smem& sm, int n, int lane)
 {
-  if (s >= 5) {
-    const int w0 = (j << s) >> 5, nw = 1 << (s - 5);
-    bool      any = false, all = true;
-    for (int w = lane; w < nw; w += 32) {
-      const uint32_t x = info[w0 + w];
-      any |= x != 0u;
-      all &= x == 0xffffffffu;
-    }
-    any = __any_sync(0xffffffffu, any);
-    all = __all_sync(0xffffffffu, all);
-    return any ? (all ? kRate1 : kRateR) : kRate0;
+  const int N = 1 << n;
+  for (int j = lane; j < N; j += 32) {
+    sm.type[j] = ((sm.info[j >> 5] >> (j & 31)) & 1u) ? kRate1 : kRate0;
   }
-  const int      first = (j << s) & 31;
-  const uint32_t m     = (s == 5 ? 0xffffffffu : ((1u << (1 << s)) - 1u)) << first;
-  const uint32_t x     = info[(j << s) >> 5] & m;
-  return x == 0u ? kRate0 : (x == m ? kRate1 : kRateR);
+  __syncwarp();
+  for (int st = 1; st <= n; ++st) {
+    const uint8_t* c = sm.type + (2 * N - ((2 * N) >> (st - 1)));
+    uint8_t*       t = sm.type + (2 * N - ((2 * N) >> st));
+    for (int j = lane; j < (N >> st); j += 32) {
+      const int a = c[2 * j], b = c[2 * j + 1];
+      t[j]        = (uint8_t)(a == b && a != kRateR ? a : kRateR);
+    }
+    __syncwarp();
+  }
 }
 
 // One codeblock by one warp.
@@ -260,6 +259,8 @@ __device__ void polar_decode_codeblock(const polar_cb& d, polar_warp_smem& sm, c
   for (int w = lane; w < kPolarNMax / 32; w += 32) {
     sm.info[w] = d.info[w];
   }
+  __syncwarp();
+  node_types(sm, n, lane);
   if (lane < 4) {
     sm.pc[lane] = d.pc[lane];
   }
@@ -336,7 +337,7 @@ __device__ void polar_decode_codeblock(const polar_cb& d, polar_warp_smem& sm, c
     const int h      = (1 << s) >> 1;
     int8_t*   ls     = sm.llr + ((1 << s) - 1);
     if (ph == 0) {
-      const int t = node_type(sm.info, s, j, lane);
+      const int t = sm.type[2 * N - ((2 * N) >> s) + j];
       if (t == kRate1) {
         // Hard decisions of the node's LLRs, re-encoded into its message bits (:180-205).
         const int p0 = j << s, sz = 1 << s;
