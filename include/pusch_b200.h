@@ -840,10 +840,10 @@ int pg_polar_code(uint32_t K, uint32_t E, pg_polar_code_info* out);
 
 /* Pipelined host execution of consecutive slots: pg_pusch_plan_submit_host enqueues one slot and
  * returns without waiting - the host-to-device copy of its grids runs on a stream of its own into
- * a staging buffer, overlapping the previous slot's processing; the grids then move into the plan's
+ * one of two staging buffers, overlapping the processing of the slots before it; the grids then move into the plan's
  * grid buffer, the plan runs and its results come back to a pinned buffer of the slot.
  * pg_pusch_plan_collect_host waits for the oldest submitted slot and writes its results as
- * pg_pusch_plan_execute_host does. At most two slots are in flight (PG_ERR_INVALID beyond); the
+ * pg_pusch_plan_execute_host does. At most three slots are in flight (PG_ERR_INVALID beyond); the
  * grids of a slot are read asynchronously, so they stay untouched until its collect returns (pinned
  * host memory makes the copy asynchronous). The first submit allocates the staging and result
  * buffers. Do not mix with the plan's other execute calls while slots are in flight. */

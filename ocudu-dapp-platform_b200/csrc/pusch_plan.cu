@@ -19,6 +19,8 @@
 
 using namespace pg;
 
+constexpr int kPlanInFlight = 3; // slots pg_pusch_plan_submit_host may hold before a collect
+
 struct pg_pusch_plan {
   pg_context*              ctx = nullptr;
   int                      nof_ues = 0, nof_cbs = 0;
@@ -98,15 +100,16 @@ struct pg_pusch_plan {
   // Compressed grids of execute_host_bfp (allocated on its first call).
   uint8_t*        d_bfp     = nullptr;
   size_t          d_bfp_cap = 0;
-  // Pipelined host execution (submit_host / collect_host; allocated on the first submit): the
-  // staging buffer the next slot's grids are copied into while the current slot runs, the copy
-  // stream, and two pinned result slots.
-  uint32_t*       d_stage       = nullptr;
-  cudaStream_t    copy_stream   = nullptr;
-  cudaEvent_t     ev_h2d        = nullptr;
-  cudaEvent_t     ev_stage_free = nullptr;
-  cudaEvent_t     ev_done[2]    = {nullptr, nullptr};
-  void*           host_slot[2]  = {nullptr, nullptr};
+  // Pipelined host execution (submit_host / collect_host; allocated on the first submit): two
+  // staging buffers the next slots' grids are copied into while the current slot runs (each free
+  // again once its grids moved into the grid buffer), the copy stream, and a pinned result slot per
+  // slot in flight.
+  uint32_t*       d_stage[2]                  = {nullptr, nullptr};
+  cudaStream_t    copy_stream                 = nullptr;
+  cudaEvent_t     ev_h2d                      = nullptr;
+  cudaEvent_t     ev_stage_free[2]            = {nullptr, nullptr};
+  cudaEvent_t     ev_done[kPlanInFlight]      = {nullptr, nullptr, nullptr};
+  void*           host_slot[kPlanInFlight]    = {nullptr, nullptr, nullptr};
   uint64_t        submitted     = 0;
   uint64_t        collected     = 0;
   // Learned estimator: the net, the LS estimates, the time-basis coefficients (same layout as
@@ -349,15 +352,16 @@ void release(pg_pusch_plan* p)
   cudaFree(p->dev);
   cudaFree(p->le_dev);
   cudaFree(p->d_bfp);
-  cudaFree(p->d_stage);
+  cudaFree(p->d_stage[0]);
+  cudaFree(p->d_stage[1]);
   if (p->copy_stream) {
     cudaStreamDestroy(p->copy_stream);
   }
   if (p->aux) {
     cudaStreamDestroy(p->aux);
   }
-  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free, p->ev_done[0], p->ev_done[1], p->ev_fork, p->ev_join, p->ev_ufork,
-                        p->ev_ujoin}) {
+  for (cudaEvent_t e : {p->ev_h2d, p->ev_stage_free[0], p->ev_stage_free[1], p->ev_done[0], p->ev_done[1],
+                        p->ev_done[2], p->ev_fork, p->ev_join, p->ev_ufork, p->ev_ujoin}) {
     if (e) {
       cudaEventDestroy(e);
     }
@@ -1332,8 +1336,8 @@ int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
   if (grids == nullptr) {
     return set_error(ctx, PG_ERR_INVALID, "null host buffer");
   }
-  if (plan->submitted - plan->collected >= 2) {
-    return set_error(ctx, PG_ERR_INVALID, "two slots in flight: collect one before submitting another");
+  if (plan->submitted - plan->collected >= (uint64_t)kPlanInFlight) {
+    return set_error(ctx, PG_ERR_INVALID, "three slots in flight: collect one before submitting another");
   }
   const size_t grid_bytes = plan->grid_words * 4;
   const size_t n          = (size_t)plan->nof_ues;
@@ -1341,15 +1345,19 @@ int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
   int          rc         = PG_OK;
   if (plan->copy_stream == nullptr) {
     rc = check_cuda(ctx, cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (cudaEvent_t* e : {&plan->ev_h2d, &plan->ev_stage_free, &plan->ev_done[0], &plan->ev_done[1]}) {
+    for (cudaEvent_t* e : {&plan->ev_h2d, &plan->ev_stage_free[0], &plan->ev_stage_free[1], &plan->ev_done[0],
+                           &plan->ev_done[1], &plan->ev_done[2]}) {
       if (rc == PG_OK) {
         rc = check_cuda(ctx, cudaEventCreateWithFlags(e, cudaEventDisableTiming), "cudaEventCreate");
       }
     }
-    if (rc == PG_OK) {
-      rc = check_cuda(ctx, cudaMalloc(&plan->d_stage, std::max<size_t>(grid_bytes, 4)), "cudaMalloc(staging grids)");
+    for (uint32_t** d : {&plan->d_stage[0], &plan->d_stage[1]}) {
+      if (rc == PG_OK) {
+        rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(d), std::max<size_t>(grid_bytes, 4)),
+                        "cudaMalloc(staging grids)");
+      }
     }
-    for (void** h : {&plan->host_slot[0], &plan->host_slot[1]}) {
+    for (void** h : {&plan->host_slot[0], &plan->host_slot[1], &plan->host_slot[2]}) {
       if (rc == PG_OK) {
         rc = check_cuda(ctx, cudaMallocHost(h, std::max<size_t>(h_bytes, 64)), "cudaMallocHost(result slot)");
       }
@@ -1359,12 +1367,14 @@ int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
     }
   }
   cudaStream_t s    = ctx->stream;
-  const int    slot = (int)(plan->submitted & 1u);
-  // Copy stream: the staging buffer is free once the previous slot has moved it into the grid
-  // buffer; the H2D then overlaps whatever the compute stream runs.
-  rc = check_cuda(ctx, cudaStreamWaitEvent(plan->copy_stream, plan->ev_stage_free, 0), "cudaStreamWaitEvent");
+  const int    slot  = (int)(plan->submitted % (uint64_t)kPlanInFlight);
+  const int    stage = (int)(plan->submitted & 1u);
+  // Copy stream: a staging buffer is free once the slot two submissions back has moved it into the
+  // grid buffer; the H2D then overlaps whatever the compute stream runs, up to two slots ahead.
+  rc = check_cuda(ctx, cudaStreamWaitEvent(plan->copy_stream, plan->ev_stage_free[stage], 0), "cudaStreamWaitEvent");
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_stage, grids, grid_bytes, cudaMemcpyHostToDevice, plan->copy_stream),
+    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_stage[stage], grids, grid_bytes, cudaMemcpyHostToDevice,
+                                         plan->copy_stream),
                     "H2D grids");
   }
   if (rc == PG_OK) {
@@ -1376,11 +1386,11 @@ int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
     rc = check_cuda(ctx, cudaStreamWaitEvent(s, plan->ev_h2d, 0), "cudaStreamWaitEvent");
   }
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, plan->d_stage, grid_bytes, cudaMemcpyDeviceToDevice, s),
+    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, plan->d_stage[stage], grid_bytes, cudaMemcpyDeviceToDevice, s),
                     "D2D grids");
   }
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaEventRecord(plan->ev_stage_free, s), "cudaEventRecord");
+    rc = check_cuda(ctx, cudaEventRecord(plan->ev_stage_free[stage], s), "cudaEventRecord");
   }
   if (rc == PG_OK) {
     rc = pg_pusch_plan_execute_device(plan, plan->d_grid, plan->d_tb_out, plan->d_res, plan->d_pr, s);
@@ -1413,7 +1423,7 @@ int pg_pusch_plan_collect_host(pg_pusch_plan* plan, uint8_t* tb_out, size_t tb_o
   if (plan->collected == plan->submitted) {
     return set_error(ctx, PG_ERR_INVALID, "no slot submitted");
   }
-  const int slot = (int)(plan->collected & 1u);
+  const int slot = (int)(plan->collected % (uint64_t)kPlanInFlight);
   if (int rc = check_cuda(ctx, cudaEventSynchronize(plan->ev_done[slot]), "cudaEventSynchronize")) {
     return rc;
   }

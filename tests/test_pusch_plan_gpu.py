@@ -119,25 +119,26 @@ def test_autotuner_keeps_results(ctx):
 
 
 def test_pipelined_host_execution(ctx):
-    """submit_host / collect_host over three slots with two in flight give, slot by slot, the
+    """submit_host / collect_host over four slots with up to three in flight give, slot by slot, the
     results of execute_host on the same grids; the in-flight limit and an empty collect are errors."""
     from pusch_b200._native import PgError
     slots = sim.uneven_cells(seed=13, nof_cells=2)
     plan = PuschSlotPlan(ctx, slots, max_iterations=6)
     grids = [plan.grid] + [np.concatenate([np.ascontiguousarray(sl.grid, np.uint32).ravel()
                                            for sl in [same_config_slot(x, 200 + 10 * k + i) for i, x in enumerate(slots)]])
-                           for k in range(2)]
+                           for k in range(3)]
     want = [plan.execute_host(g) for g in grids]
     try:
         with pytest.raises(PgError):
             plan.collect_host()
         plan.submit_host(grids[0])
         plan.submit_host(grids[1])
-        with pytest.raises(PgError):
-            plan.submit_host(grids[2])
-        got = [plan.collect_host()]
         plan.submit_host(grids[2])
-        got += [plan.collect_host(), plan.collect_host()]
+        with pytest.raises(PgError):
+            plan.submit_host(grids[3])
+        got = [plan.collect_host()]
+        plan.submit_host(grids[3])
+        got += [plan.collect_host(), plan.collect_host(), plan.collect_host()]
         for g_slot, w_slot in zip(got, want):
             for g, w in zip(g_slot, w_slot):
                 assert (g.tb_crc_ok, g.nof_codeblocks_crc_ok, g.mean_iterations) == \
