@@ -575,7 +575,7 @@ def run_ours_pusch(args):
         assert e_ok == [r.tb_crc_ok for r in results]
         e_ms = max_over_ranks(e_ms, world)
         e2e = {"value": round(total_bits / (e_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
-               "h2d_bytes_per_step": int(plan.grid.size * 4),
+               "h2d_bytes_per_step": int(plan.info.h2d_grid_bytes),
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
                "ms_per_step": round(e_ms, 3), "entry": "pg_pusch_plan_execute_host"}
 
@@ -601,7 +601,7 @@ def run_ours_pusch(args):
         # The headline end-to-end figure is the pipelined one (consecutive slots, as a PHY runs them);
         # the one-call-at-a-time figure stays beside it.
         e2e = {"value": round(total_bits / (p_ms * 1e-3) / 1e6, 3), "unit": "Mbit/s",
-               "h2d_bytes_per_step": int(plan.grid.size * 4),
+               "h2d_bytes_per_step": int(plan.info.h2d_grid_bytes),
                "d2h_bytes_per_step": int(plan.tb_bytes + n * ctypes.sizeof(PgSchResult)),
                "ms_per_step": round(p_ms, 3),
                "slots_in_flight": args.e2e_depth,

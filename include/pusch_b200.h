@@ -482,7 +482,8 @@ typedef struct pg_pusch_plan_info_t {
   uint64_t grid_words;   /* cbf16 words of the grids buffer */
   uint64_t device_bytes; /* device memory the plan holds */
   uint32_t nof_kernels;  /* kernels one execution launches with the current tuning and estimator */
-  uint32_t reserved;
+  uint32_t h2d_grid_bytes; /* grid bytes a host execution copies: per cell grid, the subcarriers its
+                              UEs occupy on every port and symbol (no kernel reads the rest) */
 } pg_pusch_plan_info_t;
 
 /* ues: host array of nof_ues PDUs whose grids lie in a buffer of grid_words cbf16 words; the

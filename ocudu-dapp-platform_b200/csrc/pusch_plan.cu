@@ -21,6 +21,19 @@ using namespace pg;
 
 constexpr int kPlanInFlight = 3; // slots pg_pusch_plan_submit_host may hold before a collect
 
+// The part of one cell's grid ([port][symbol][subcarrier] words from `offset`) that the plan's UEs
+// occupy: subcarriers [sc0, sc0 + width) of every port and symbol. Host executions copy only these
+// spans; no kernel reads a grid word outside them.
+struct grid_span {
+  size_t offset; // first word copied: the grid's offset + sc0
+  size_t width;  // words per row
+  size_t pitch;  // words between rows (subcarriers of the grid)
+  size_t rows;   // ports x 14 symbols
+};
+extern "C" {
+static int copy_grid_spans(pg_pusch_plan* plan, uint32_t* dst, const uint32_t* src, cudaStream_t s);
+}
+
 struct pg_pusch_plan {
   pg_context*              ctx = nullptr;
   int                      nof_ues = 0, nof_cbs = 0;
@@ -112,6 +125,8 @@ struct pg_pusch_plan {
   void*           host_slot[kPlanInFlight]    = {nullptr, nullptr, nullptr};
   uint64_t        submitted     = 0;
   uint64_t        collected     = 0;
+  std::vector<grid_span> grid_spans;
+  size_t                 h2d_grid_bytes = 0;
   // Learned estimator: the net, the LS estimates, the time-basis coefficients (same layout as
   // d_est) with the per-UE flags of the UEs that use them, and the sequences of the refined UEs.
   pg_le_net*      le_net      = nullptr;
@@ -542,6 +557,34 @@ int pg_pusch_plan_create_uci(pg_context* ctx, const pg_pusch_ue* ues, const pg_p
     }
     p->uci_nmsg = p->uci_nshort + p->polar_n;
   }
+  {
+    // Per cell grid (UEs sharing grid_offset), the span of the subcarriers its UEs occupy.
+    std::vector<std::pair<uint32_t, grid_span>> cells;
+    for (int i = 0; i < nof_ues; ++i) {
+      const pg_pusch_ue& u   = p->ues[i];
+      const size_t       sc0 = 12u * (size_t)u.rb_start, sc1 = 12u * ((size_t)u.rb_start + u.nof_rb);
+      auto it = std::find_if(cells.begin(), cells.end(), [&](const auto& c) { return c.first == u.grid_offset; });
+      if (it == cells.end()) {
+        cells.push_back({u.grid_offset, grid_span{sc0, sc1 - sc0, u.grid_nof_subc, (size_t)u.nof_rx_ports * 14u}});
+        continue;
+      }
+      grid_span&   g   = it->second;
+      const size_t lo  = std::min(g.offset, sc0), hi = std::max(g.offset + g.width, sc1);
+      g.offset         = lo;
+      g.width          = hi - lo;
+      g.pitch          = std::max<size_t>(g.pitch, u.grid_nof_subc);
+      g.rows           = std::max<size_t>(g.rows, (size_t)u.nof_rx_ports * 14u);
+    }
+    for (auto& c : cells) {
+      grid_span g = c.second;
+      g.offset += c.first;
+      if (g.width > g.pitch || g.offset + (g.rows - 1) * g.pitch + g.width > grid_words) {
+        g = grid_span{c.first, c.second.pitch, c.second.pitch, c.second.rows}; // whole rows
+      }
+      p->grid_spans.push_back(g);
+      p->h2d_grid_bytes += 4 * g.width * g.rows;
+    }
+  }
   p->max_rb    = max_nof_rb(p->ues.data(), nof_ues);
   p->est_total = est_total;
   std::vector<uint32_t> tile_map;
@@ -769,7 +812,7 @@ int pg_pusch_plan_info(const pg_pusch_plan* plan, pg_pusch_plan_info_t* info)
                       (plan->uci_nshort > 0 ? 1u : 0u) + (plan->polar_n > 0 ? 1u : 0u) +
                       (plan->unplaced.empty() ? 0u : 1u) + (plan->nof_cbs > 1 && plan->tuning.ldpc_order != 0 ? 2u : 0u) +
                       3u;
-  info->reserved = 0;
+  info->h2d_grid_bytes = (uint32_t)std::min<size_t>(plan->h2d_grid_bytes, 0xffffffffu);
   return PG_OK;
 }
 
@@ -1234,9 +1277,7 @@ int pg_pusch_plan_execute_host(pg_pusch_plan* plan, const uint32_t* grids, uint8
   if (tb_out_len < plan->tb_bytes) {
     return set_error(ctx, PG_ERR_INVALID, "transport-block buffer smaller than the plan's TBs");
   }
-  const int rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_grid, grids, plan->grid_words * 4, cudaMemcpyHostToDevice,
-                                                 ctx->stream),
-                            "H2D grids");
+  const int rc = copy_grid_spans(plan, plan->d_grid, grids, ctx->stream);
   return execute_host_tail(plan, tb_out, results, port_results, rc);
 }
 
@@ -1327,6 +1368,20 @@ static int enqueue_results_d2h(pg_pusch_plan* plan, uint8_t* h, cudaStream_t s)
   return rc;
 }
 
+// Host grids to a device grid buffer of the plan's layout: one 2-D copy per cell span.
+static int copy_grid_spans(pg_pusch_plan* plan, uint32_t* dst, const uint32_t* src, cudaStream_t s)
+{
+  for (const grid_span& g : plan->grid_spans) {
+    if (int rc = check_cuda(plan->ctx,
+                            cudaMemcpy2DAsync(dst + g.offset, g.pitch * 4, src + g.offset, g.pitch * 4, g.width * 4,
+                                              g.rows, cudaMemcpyHostToDevice, s),
+                            "H2D grids")) {
+      return rc;
+    }
+  }
+  return PG_OK;
+}
+
 int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
 {
   if (plan == nullptr) {
@@ -1373,9 +1428,7 @@ int pg_pusch_plan_submit_host(pg_pusch_plan* plan, const uint32_t* grids)
   // grid buffer; the H2D then overlaps whatever the compute stream runs, up to two slots ahead.
   rc = check_cuda(ctx, cudaStreamWaitEvent(plan->copy_stream, plan->ev_stage_free[stage], 0), "cudaStreamWaitEvent");
   if (rc == PG_OK) {
-    rc = check_cuda(ctx, cudaMemcpyAsync(plan->d_stage[stage], grids, grid_bytes, cudaMemcpyHostToDevice,
-                                         plan->copy_stream),
-                    "H2D grids");
+    rc = copy_grid_spans(plan, plan->d_stage[stage], grids, plan->copy_stream);
   }
   if (rc == PG_OK) {
     rc = check_cuda(ctx, cudaEventRecord(plan->ev_h2d, plan->copy_stream), "cudaEventRecord");

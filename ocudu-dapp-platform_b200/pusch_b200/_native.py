@@ -165,7 +165,7 @@ assert ctypes.sizeof(PgPortEstimateCfg) == 20 and ctypes.sizeof(PgPortEstimateRe
 class PgPuschPlanInfo(ctypes.Structure):
     _fields_ = [("nof_ues", ctypes.c_uint32), ("nof_codeblocks", ctypes.c_uint32), ("tb_bytes", ctypes.c_uint64),
                 ("nof_llrs", ctypes.c_uint64), ("grid_words", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
-                ("nof_kernels", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("nof_kernels", ctypes.c_uint32), ("h2d_grid_bytes", ctypes.c_uint32)]
 
 
 assert ctypes.sizeof(PgRmCb) == 24 and ctypes.sizeof(PgSchTb) == 28 and ctypes.sizeof(PgTbDesc) == 24
